@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark of the AMR multigrid solve (AMRMultiGrid::solve over
+VCAMRPoissonOp2) on the 3-level variable-coefficient Helmholtz hierarchy:
+base 128^3, refinement ratio 2, blocking factor 8, max box 32, fill ratio 0.75,
+alpha = 1, beta = -1, coefficients exp of a seeded Fourier series in
+[0.1, 10], seeded Gaussian-bump right-hand side, homogeneous Dirichlet,
+4 + 4 red-black smooths, BiCGStab bottom, zero initial guess to a 1e-10
+relative residual.  One step = one full solve.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  Under torchrun every rank solves its own
+replica of the hierarchy (independent solves shard with no collective);
+timing is the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+ORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle")
+METRIC = "Poisson solves/s & p50/p99 latency at 1e-10 rel. residual; V-cycle HBM GB/s"
+WORKLOADS = {
+    "config1": {
+        "golden": "config1_vc_3lev_128",
+        "name": "3-level VC Helmholtz (VCAMRPoissonOp2 alpha=1 beta=-1), base 128^3, ratio 2, block 8, "
+                "max box 32, fill 0.75, Dirichlet, GSRB 4+4, BiCGStab bottom, rel. residual 1e-10",
+    },
+    "config0": {
+        "golden": "config0_poisson_64",
+        "name": "single-level Poisson (AMRPoissonOp alpha=0 beta=1), 64^3, max box 32, Dirichlet, "
+                "GSRB 4+4, BiCGStab bottom, rel. residual 1e-10",
+    },
+}
+
+
+def load_cmg():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("cmg", os.path.join(ROOT, "chombo_3.2_b200", "cmg.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def golden_meta(name):
+    return json.load(open(os.path.join(GOLDEN, name + ".json")))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sms = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sms)) if sms else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def write_boxfile(meta):
+    f = tempfile.NamedTemporaryFile("w", suffix=".boxes", delete=False)
+    f.write(f"{len(meta['boxes'])}\n")
+    for bl in meta["boxes"]:
+        f.write(f"{len(bl)}\n")
+        for b in bl:
+            f.write(" ".join(map(str, b)) + "\n")
+    f.close()
+    return f.name
+
+
+def oracle_args(meta, boxfile, iters, repeat):
+    return [ORACLE, f"n0={meta['n0']}", f"levels={len(meta['boxes'])}", f"maxbox={meta['maxbox']}",
+            f"block={meta['block']}", f"op={meta['op']}", f"alpha={meta['alpha']}", f"beta={meta['beta']}",
+            f"seed={meta['seed']}", f"pre={meta['pre']}", f"post={meta['post']}", f"bottom={meta['bottom']}",
+            f"eps={meta['eps']}", f"hang={meta['hang']}", f"iters={iters}", f"repeat={repeat}", "dumpphi=0",
+            f"boxfile={boxfile}", f"out={boxfile}.out"]
+
+
+def parse_repeats(text):
+    reps = []
+    for line in text.splitlines():
+        if line.startswith("repeat "):
+            w = line.split()
+            its = [float(x) for x in w[w.index("iterations") + 1:]]
+            reps.append({"seconds": float(w[3]), "setup": float(w[5]), "iterations": its})
+    return reps
+
+
+def extrapolate(rep, n_iter):
+    """Full-solve time from a capped solve: set-up + first iteration + the
+    remaining iterations at the later (steady) iteration time."""
+    its = rep["iterations"]
+    steady = its[-1] if len(its) > 1 else its[0]
+    return rep["setup"] + its[0] + (n_iter - 1) * steady
+
+
+def cpu_reference(meta, processes, repeats):
+    """The reference solve (oracle/_ref, the reference's C++ with the
+    restated ChF kernels) on host cores: `processes` concurrent single-thread
+    solves of the workload, each capped at 2 V-cycles per repeat and
+    extrapolated to the reference's own iteration count."""
+    if not os.path.exists(ORACLE):
+        return None
+    boxfile = write_boxfile(meta)
+    n_iter = len(meta["residual_history"]) - 1
+    procs = [subprocess.Popen(oracle_args(meta, boxfile, 2, repeats), stdout=subprocess.PIPE,
+                              stderr=subprocess.DEVNULL, text=True) for _ in range(processes)]
+    outs = [parse_repeats(p.communicate()[0]) for p in procs]
+    per_step = []
+    for k in range(repeats):
+        ts = [extrapolate(o[k], n_iter) for o in outs if len(o) > k]
+        per_step.append(len(ts) / max(ts) if ts else float("nan"))
+    return {"per_step": per_step, "n_iter": n_iter, "processes": processes,
+            "wall_step": [max(o[k]["seconds"] for o in outs if len(o) > k) for k in range(repeats)]}
+
+
+def run_reference_arm(args, meta, wl):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if not os.path.exists(ORACLE):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cmg_oracle not built (needs the "
+                          "reference sources at build time)"}))
+        return
+    cores = os.cpu_count() or 1
+    # each process holds ~3 GB for this workload; bound the concurrency
+    procs = max(1, min(cores, 8))
+    res = cpu_reference(meta, procs, args.warmup + args.steps)
+    timed = res["per_step"][args.warmup:]
+    value = float(np.mean(timed))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * float(np.mean(res["wall_step"][args.warmup:])),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["name"], "global_batch": 1, "parallelism": f"{procs} concurrent host processes"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "reference",
+                         "sample": f"each step: {procs} concurrent single-thread reference solves capped at 2 of "
+                                   f"{res['n_iter']} V-cycles, extrapolated to the full solve"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    meta = golden_meta(wl["golden"])
+    if args.impl == "reference":
+        return run_reference_arm(args, meta, wl)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    args.warmup = max(args.warmup, 3)
+
+    cmg = load_cmg()
+    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+    h.fill_synthetic(meta["seed"])
+    params = cmg.solve_params(pre=meta["pre"], post=meta["post"], bottom=meta["bottom"], iter_max=meta["iters"],
+                              eps=meta["eps"], hang=meta["hang"])
+    stream = torch.cuda.ExternalStream(h.stream())
+    ncells = [h.num_cells(l) for l in range(len(meta["boxes"]))]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        out = h.solve(params)
+    assert out["exit_status"] == meta["exit_status"], out
+    n_iter = out["iterations"]
+
+    # Device-resident timed region.  Working set (~2.5 GB of FP64 fields)
+    # exceeds L2, so no flush is needed between steps.
+    sampler = ClockSampler(local)
+    sampler.start()
+    h.profile_enable(True)
+    barrier()
+    launches0 = cmg.launch_count()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(args.steps):
+            h.solve(params)
+            ev[k + 1].record(stream)
+    barrier()
+    launches = cmg.launch_count() - launches0
+    clocks = sampler.stop()
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    gsrb = h.profile_read(0)
+    resid = h.profile_read(1)
+    h.profile_enable(False)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1000.0)
+
+    # End to end through the C ABI: every step uploads the right-hand side
+    # of every level from pinned host memory, solves, and reads phi back into
+    # pinned host memory.
+    host_rhs = [torch.empty(n, dtype=torch.float64, pin_memory=True) for n in ncells]
+    host_phi = [torch.empty(n, dtype=torch.float64, pin_memory=True) for n in ncells]
+    for l in range(len(ncells)):
+        h.get_rhs_ptr(l, host_rhs[l].data_ptr(), 0)
+    h2d = sum(ncells) * 8
+    d2h = sum(ncells) * 8
+    barrier()
+    e2e_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e2e_ev[0].record(stream)
+    for k in range(args.steps):
+        for l in range(len(ncells)):
+            h.set_rhs_ptr(l, host_rhs[l].data_ptr(), 0)
+        out = h.solve(params)
+        for l in range(len(ncells)):
+            h.get_phi_ptr(l, host_phi[l].data_ptr(), 0)
+    e2e_ev[1].record(stream)
+    barrier()
+    e2e_ms = e2e_ev[0].elapsed_time(e2e_ev[1])
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert out["exit_status"] == meta["exit_status"], out
+    e2e = {"value": world * args.steps / (e2e_ms / 1000.0), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h}
+
+    peak, peak_kind = measured_peaks()
+    n_gsrb, ms_gsrb, bytes_gsrb = gsrb
+    achieved = (bytes_gsrb / 1e9) / (ms_gsrb / 1e3) if ms_gsrb > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(args.workload)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "k_gsrb (red-black relaxation, one colour, every level)",
+                "peak_kind": peak_kind, "launches": n_gsrb,
+                "avg_launch_us": 1000.0 * ms_gsrb / max(n_gsrb, 1),
+                "bytes_per_launch": bytes_gsrb / max(n_gsrb, 1),
+                "residual_kernels_gbs": (resid[2] / 1e9) / (resid[1] / 1e3) if resid[1] > 0 else 0.0,
+                "gsrb_share_of_step": ms_gsrb / total_ms if total_ms > 0 else 0.0}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = cpu_reference(meta, 1, 1)
+        if res:
+            cpu = {"value": res["per_step"][0], "unit": "solves/s", "cores": 1, "kind": "reference",
+                   "sample": f"one single-thread reference solve capped at 2 of {res['n_iter']} V-cycles, "
+                             f"extrapolated to the full solve (set-up + first + (n-1) x later V-cycle)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["name"], "global_batch": world, "cells": sum(ncells),
+                       "levels": len(ncells), "boxes": [len(b) for b in meta["boxes"]],
+                       "vcycles_per_solve": n_iter, "l2": "working set > L2 (no flush)",
+                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
+            "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+            "vcycle_gbs": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    h.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,217 @@
+"""ctypes binding of libcmg.so (include/cmg.h) for the tests and the benchmark.
+
+The library is the product; this module only marshals numpy arrays and
+raises on any non-zero status.  It fails loudly when libcmg.so is missing:
+there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcmg.so")
+
+CMG_OK, CMG_EINVAL, CMG_ENOMEM, CMG_ECUDA, CMG_EINTERNAL = range(5)
+
+
+class CmgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cmg status {code}: {msg}")
+        self.code = code
+
+
+class Box(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3)]
+
+
+class SolveParams(ctypes.Structure):
+    _fields_ = [("pre", ctypes.c_int), ("post", ctypes.c_int), ("bottom", ctypes.c_int),
+                ("num_mg", ctypes.c_int), ("iter_max", ctypes.c_int), ("imin", ctypes.c_int),
+                ("eps", ctypes.c_double), ("hang", ctypes.c_double), ("norm_thresh", ctypes.c_double)]
+
+
+def solve_params(pre=4, post=4, bottom=4, num_mg=1, iter_max=100, imin=5, eps=1e-10, hang=1e-10,
+                 norm_thresh=1e-30):
+    return SolveParams(pre, post, bottom, num_mg, iter_max, imin, eps, hang, norm_thresh)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} not built: run `make -C chombo_3.2_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.cmg_last_error.restype = ctypes.c_char_p
+        L.cmg_fill_synthetic.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != CMG_OK:
+        raise CmgError(rc, lib().cmg_last_error().decode())
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def boxes_array(boxes):
+    arr = (Box * len(boxes))()
+    for i, b in enumerate(boxes):
+        arr[i].lo[:] = list(b[0:3])
+        arr[i].hi[:] = list(b[3:6])
+    return arr
+
+
+def domain_split(lo, hi, max_box, block_factor):
+    L = lib()
+    n = ctypes.c_int()
+    _check(L.cmg_domain_split((ctypes.c_int * 3)(*lo), (ctypes.c_int * 3)(*hi), max_box, block_factor, None, 0,
+                              ctypes.byref(n)))
+    out = (Box * n.value)()
+    _check(L.cmg_domain_split((ctypes.c_int * 3)(*lo), (ctypes.c_int * 3)(*hi), max_box, block_factor, out,
+                              n.value, ctypes.byref(n)))
+    return [tuple(b.lo) + tuple(b.hi) for b in out]
+
+
+def launch_count():
+    n = ctypes.c_int64()
+    _check(lib().cmg_launch_count(ctypes.byref(n)))
+    return n.value
+
+
+def _plan(fn, *args):
+    n = ctypes.c_int()
+    _check(fn(*args, None, 0, ctypes.byref(n)))
+    buf = np.zeros(14 * max(n.value, 1), dtype=np.int32)
+    _check(fn(*args, _ptr(buf), n.value, ctypes.byref(n)))
+    return buf[:14 * n.value].reshape(n.value, 14)
+
+
+def layout_exchange_plan(boxes):
+    arr = boxes_array(boxes)
+    return _plan(lib().cmg_layout_exchange_plan, arr, len(boxes))
+
+
+def layout_coarse_fine_plan(fine, coarse):
+    fa, ca = boxes_array(fine), boxes_array(coarse)
+    return _plan(lib().cmg_layout_coarse_fine_plan, fa, len(fine), ca, len(coarse))
+
+
+class Hierarchy:
+    """One AMR hierarchy with device-resident state (cmg_hierarchy)."""
+
+    def __init__(self, n0, level_boxes, op=0, alpha=0.0, beta=1.0, dx0=None):
+        L = lib()
+        self.nlev = len(level_boxes)
+        counts = (ctypes.c_int * self.nlev)(*[len(b) for b in level_boxes])
+        flat = [b for lev in level_boxes for b in lev]
+        arr = boxes_array(flat)
+        h = ctypes.c_void_p()
+        dx0 = 1.0 / n0 if dx0 is None else dx0
+        _check(L.cmg_hierarchy_create((ctypes.c_int * 3)(0, 0, 0), (ctypes.c_int * 3)(n0 - 1, n0 - 1, n0 - 1),
+                                      ctypes.c_double(dx0), self.nlev, counts, arr, op, ctypes.c_double(alpha),
+                                      ctypes.c_double(beta), ctypes.byref(h)))
+        self.h = h
+        self.op = op
+
+    def close(self):
+        if self.h:
+            _check(lib().cmg_hierarchy_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def num_cells(self, level):
+        n = ctypes.c_int64()
+        _check(lib().cmg_num_cells(self.h, level, ctypes.byref(n)))
+        return n.value
+
+    def num_faces(self, level, d):
+        n = ctypes.c_int64()
+        _check(lib().cmg_num_faces(self.h, level, d, ctypes.byref(n)))
+        return n.value
+
+    def boxes(self, level):
+        n = ctypes.c_int()
+        _check(lib().cmg_num_boxes(self.h, level, ctypes.byref(n)))
+        out = (Box * n.value)()
+        _check(lib().cmg_get_boxes(self.h, level, out, n.value))
+        return [tuple(b.lo) + tuple(b.hi) for b in out]
+
+    def fill_synthetic(self, seed):
+        _check(lib().cmg_fill_synthetic(self.h, ctypes.c_uint64(seed)))
+
+    def set_rhs(self, level, data):
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        _check(lib().cmg_set_rhs(self.h, level, _ptr(a), 0))
+
+    def set_acoef(self, level, data):
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        _check(lib().cmg_set_acoef(self.h, level, _ptr(a), 0))
+
+    def set_bcoef(self, level, d, data):
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        _check(lib().cmg_set_bcoef(self.h, level, d, _ptr(a), 0))
+
+    def finalize_coefficients(self):
+        _check(lib().cmg_finalize_coefficients(self.h))
+
+    def phi(self, level):
+        out = np.empty(self.num_cells(level), dtype=np.float64)
+        _check(lib().cmg_get_phi(self.h, level, _ptr(out), 0))
+        return out
+
+    def set_phi(self, level, data):
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        _check(lib().cmg_set_phi(self.h, level, _ptr(a), 0))
+
+    def solve(self, params=None, zero_phi=True):
+        p = params or solve_params()
+        hist = np.zeros(p.iter_max + 2, dtype=np.float64)
+        st, it, hl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().cmg_solve(self.h, ctypes.byref(p), int(zero_phi), ctypes.byref(st), ctypes.byref(it),
+                               _ptr(hist), len(hist), ctypes.byref(hl)))
+        return {"exit_status": st.value, "iterations": it.value, "history": hist[:hl.value].copy()}
+
+    def residual_norm(self):
+        r = ctypes.c_double()
+        _check(lib().cmg_residual_norm(self.h, ctypes.byref(r)))
+        return r.value
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        _check(lib().cmg_get_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+    def profile_enable(self, on=True):
+        _check(lib().cmg_profile_enable(self.h, int(on)))
+
+    def profile_read(self, kernel_class):
+        n, ms, b = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        _check(lib().cmg_profile_read(self.h, kernel_class, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(b)))
+        return n.value, ms.value, b.value
+
+    def set_rhs_ptr(self, level, ptr, on_device):
+        _check(lib().cmg_set_rhs(self.h, level, ctypes.c_void_p(ptr), int(on_device)))
+
+    def get_rhs_ptr(self, level, ptr, on_device):
+        _check(lib().cmg_get_rhs(self.h, level, ctypes.c_void_p(ptr), int(on_device)))
+
+    def get_phi_ptr(self, level, ptr, on_device):
+        _check(lib().cmg_get_phi(self.h, level, ctypes.c_void_p(ptr), int(on_device)))
+
+    def vcycle_bytes(self, params=None):
+        p = params or solve_params()
+        r = ctypes.c_double()
+        _check(lib().cmg_vcycle_bytes(self.h, ctypes.byref(p), ctypes.byref(r)))
+        return r.value

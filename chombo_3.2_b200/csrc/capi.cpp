@@ -1,0 +1,453 @@
+// C ABI over the solver (include/cmg.h).  Every entry point catches
+// exceptions and turns them into status codes; nothing aborts.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/cmg.h"
+#include "solver.H"
+#include "synthetic.H"
+
+struct cmg_hierarchy {
+  cudaStream_t stream = nullptr;
+  cmg::Solver* solver = nullptr;
+  cmg::HierarchyDesc desc;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+template <class F>
+int guard(F fn) {
+  try {
+    fn();
+    return CMG_OK;
+  } catch (const std::bad_alloc& e) {
+    return fail(CMG_ENOMEM, e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(CMG_EINVAL, e.what());
+  } catch (const std::runtime_error& e) {
+    std::string w = e.what();
+    if (w.find("cudaMalloc") != std::string::npos) return fail(CMG_ENOMEM, w);
+    if (w.find("cmg: ") == 0 && w.find(": ") != w.rfind(": ")) return fail(CMG_ECUDA, w);
+    return fail(CMG_EINTERNAL, w);
+  } catch (...) {
+    return fail(CMG_EINTERNAL, "unknown error");
+  }
+}
+
+void needLevel(const cmg_hierarchy* h, int level) {
+  if (!h || !h->solver) throw std::invalid_argument("cmg: null hierarchy");
+  if (level < 0 || level >= h->solver->numLevels()) throw std::invalid_argument("cmg: level out of range");
+}
+
+cmg::Box toBox(const cmg_box& b) { return cmg::Box(cmg::IV(b.lo[0], b.lo[1], b.lo[2]), cmg::IV(b.hi[0], b.hi[1], b.hi[2])); }
+
+void fromBox(const cmg::Box& b, cmg_box& o) {
+  for (int d = 0; d < 3; ++d) {
+    o.lo[d] = b.lo[d];
+    o.hi[d] = b.hi[d];
+  }
+}
+
+void putMotion(int* o, int from, int to, const cmg::Box& fr, const cmg::Box& tr) {
+  o[0] = from;
+  o[1] = to;
+  for (int d = 0; d < 3; ++d) {
+    o[2 + d] = fr.lo[d];
+    o[5 + d] = fr.hi[d];
+    o[8 + d] = tr.lo[d];
+    o[11 + d] = tr.hi[d];
+  }
+}
+
+template <class F>
+void parallelBoxes(size_t nbox, F fn) {
+  unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; ++t)
+    th.emplace_back([&, t]() {
+      for (size_t b = t; b < nbox; b += nt) fn(b);
+    });
+  for (auto& x : th) x.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cmg_last_error(void) { return g_err.c_str(); }
+
+int cmg_hierarchy_create(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels, const int* nboxes,
+                         const cmg_box* boxes, int op, double alpha, double beta, cmg_hierarchy** out) {
+  return guard([&]() {
+    if (!domain_lo || !domain_hi || !nboxes || !boxes || !out || nlevels < 1 || dx0 <= 0 || (op != 0 && op != 1))
+      throw std::invalid_argument("cmg: invalid hierarchy description");
+    *out = nullptr;
+    cmg::HierarchyDesc d;
+    d.domain = cmg::Box(cmg::IV(domain_lo[0], domain_lo[1], domain_lo[2]), cmg::IV(domain_hi[0], domain_hi[1], domain_hi[2]));
+    if (d.domain.empty()) throw std::invalid_argument("cmg: empty domain");
+    d.dx0 = dx0;
+    d.vc = op;
+    d.alpha = alpha;
+    d.beta = beta;
+    int k = 0;
+    cmg::Box dom = d.domain;
+    for (int l = 0; l < nlevels; ++l) {
+      if (nboxes[l] < 1) throw std::invalid_argument("cmg: a level has no boxes");
+      if (l > 0) dom = dom.refine(2);
+      std::vector<cmg::Box> v;
+      for (int b = 0; b < nboxes[l]; ++b, ++k) {
+        cmg::Box bx = toBox(boxes[k]);
+        if (bx.empty() || !dom.contains(bx)) throw std::invalid_argument("cmg: box empty or outside its level domain");
+        if (l > 0 && !bx.coarsenable(2)) throw std::invalid_argument("cmg: fine box not coarsenable by 2");
+        v.push_back(bx);
+      }
+      std::vector<cmg::Box> sorted = v;
+      std::sort(sorted.begin(), sorted.end());
+      for (size_t i = 0; i < sorted.size(); ++i)
+        for (size_t j = i + 1; j < sorted.size() && sorted[j].lo[0] <= sorted[i].hi[0]; ++j)
+          if (sorted[i].intersects(sorted[j])) throw std::invalid_argument("cmg: boxes of a level overlap");
+      d.boxes.push_back(v);
+    }
+    cmg_hierarchy* h = new cmg_hierarchy;
+    h->desc = d;
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete h;
+      throw std::runtime_error(std::string("cmg: stream: ") + cudaGetErrorString(e));
+    }
+    try {
+      h->solver = new cmg::Solver(d, h->stream);
+    } catch (...) {
+      cudaStreamDestroy(h->stream);
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int cmg_hierarchy_destroy(cmg_hierarchy* h) {
+  return guard([&]() {
+    if (!h) return;
+    delete h->solver;
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+  });
+}
+
+int cmg_num_levels(const cmg_hierarchy* h, int* out) {
+  return guard([&]() {
+    needLevel(h, 0);
+    *out = h->solver->numLevels();
+  });
+}
+
+int cmg_num_boxes(const cmg_hierarchy* h, int level, int* out) {
+  return guard([&]() {
+    needLevel(h, level);
+    *out = (int)h->solver->level(level).grids.size();
+  });
+}
+
+int cmg_get_boxes(const cmg_hierarchy* h, int level, cmg_box* out, int cap) {
+  return guard([&]() {
+    needLevel(h, level);
+    const auto& g = h->solver->level(level).grids;
+    if (!out || cap < (int)g.size()) throw std::invalid_argument("cmg: box buffer too small");
+    for (size_t b = 0; b < g.size(); ++b) fromBox(g[b], out[b]);
+  });
+}
+
+int cmg_num_cells(const cmg_hierarchy* h, int level, int64_t* out) {
+  return guard([&]() {
+    needLevel(h, level);
+    *out = h->solver->numValidCells(level);
+  });
+}
+
+int cmg_num_faces(const cmg_hierarchy* h, int level, int dir, int64_t* out) {
+  return guard([&]() {
+    needLevel(h, level);
+    if (dir < 0 || dir > 2) throw std::invalid_argument("cmg: direction out of range");
+    *out = h->solver->numFaces(level, dir);
+  });
+}
+
+int cmg_set_rhs(cmg_hierarchy* h, int level, const double* data, int on_device) {
+  return guard([&]() {
+    needLevel(h, level);
+    if (!data) throw std::invalid_argument("cmg: null data");
+    h->solver->setRHS(level, data, on_device != 0);
+  });
+}
+
+int cmg_set_acoef(cmg_hierarchy* h, int level, const double* data, int on_device) {
+  return guard([&]() {
+    needLevel(h, level);
+    if (!data) throw std::invalid_argument("cmg: null data");
+    if (!h->desc.vc) throw std::invalid_argument("cmg: operator has no a coefficient");
+    h->solver->setACoef(level, data, on_device != 0);
+  });
+}
+
+int cmg_set_bcoef(cmg_hierarchy* h, int level, int dir, const double* data, int on_device) {
+  return guard([&]() {
+    needLevel(h, level);
+    if (!data || dir < 0 || dir > 2) throw std::invalid_argument("cmg: bad b coefficient argument");
+    if (!h->desc.vc) throw std::invalid_argument("cmg: operator has no b coefficient");
+    h->solver->setBCoef(level, dir, data, on_device != 0);
+  });
+}
+
+int cmg_finalize_coefficients(cmg_hierarchy* h) {
+  return guard([&]() {
+    needLevel(h, 0);
+    h->solver->finalizeCoefficients();
+  });
+}
+
+int cmg_get_phi(cmg_hierarchy* h, int level, double* data, int on_device) {
+  return guard([&]() {
+    needLevel(h, level);
+    if (!data) throw std::invalid_argument("cmg: null data");
+    h->solver->getPhi(level, data, on_device != 0);
+  });
+}
+
+int cmg_get_rhs(cmg_hierarchy* h, int level, double* data, int on_device) {
+  return guard([&]() {
+    needLevel(h, level);
+    if (!data) throw std::invalid_argument("cmg: null data");
+    h->solver->getRHS(level, data, on_device != 0);
+  });
+}
+
+int cmg_set_phi(cmg_hierarchy* h, int level, const double* data, int on_device) {
+  return guard([&]() {
+    needLevel(h, level);
+    if (!data) throw std::invalid_argument("cmg: null data");
+    h->solver->setPhi(level, data, on_device != 0);
+  });
+}
+
+int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
+              double* history, int history_cap, int* history_len) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (!p) throw std::invalid_argument("cmg: null parameters");
+    cmg::SolveParams sp;
+    sp.pre = p->pre;
+    sp.post = p->post;
+    sp.bottom = p->bottom;
+    sp.numMG = p->num_mg;
+    sp.iterMax = p->iter_max;
+    sp.imin = p->imin;
+    sp.eps = p->eps;
+    sp.hang = p->hang;
+    sp.normThresh = p->norm_thresh;
+    if (sp.pre < 0 || sp.post < 0 || sp.bottom < 0 || sp.numMG < 1 || sp.iterMax < 0)
+      throw std::invalid_argument("cmg: invalid solver parameters");
+    cmg::SolveResult r = h->solver->solve(sp, zero_phi != 0);
+    if (exit_status) *exit_status = r.exitStatus;
+    if (iterations) *iterations = r.iterations;
+    int n = (int)r.history.size();
+    if (history_len) *history_len = n;
+    if (history)
+      for (int i = 0; i < n && i < history_cap; ++i) history[i] = r.history[i];
+  });
+}
+
+int cmg_residual_norm(cmg_hierarchy* h, double* out) {
+  return guard([&]() {
+    needLevel(h, 0);
+    *out = h->solver->residualNorm();
+  });
+}
+
+int cmg_fill_synthetic(cmg_hierarchy* h, uint64_t seed) {
+  return guard([&]() {
+    needLevel(h, 0);
+    cmg_synth::Problem prob(seed);
+    cmg::Solver& S = *h->solver;
+    for (int l = 0; l < S.numLevels(); ++l) {
+      const cmg::LevelPlan& L = S.level(l);
+      const double dx = L.dx;
+      std::vector<int64_t> off(L.grids.size() + 1, 0);
+      for (size_t b = 0; b < L.grids.size(); ++b) off[b + 1] = off[b] + L.grids[b].numPts();
+      std::vector<double> rhs(off.back()), a;
+      if (h->desc.vc) a.resize(off.back());
+      parallelBoxes(L.grids.size(), [&](size_t b) {
+        const cmg::Box& B = L.grids[b];
+        int64_t q = off[b];
+        for (int k = B.lo[2]; k <= B.hi[2]; ++k)
+          for (int j = B.lo[1]; j <= B.hi[1]; ++j)
+            for (int i = B.lo[0]; i <= B.hi[0]; ++i, ++q) {
+              double x = (i + 0.5) * dx, y = (j + 0.5) * dx, z = (k + 0.5) * dx;
+              rhs[q] = prob.bumps.eval(x, y, z);
+              if (!a.empty()) a[q] = prob.acoef.eval(x, y, z);
+            }
+      });
+      S.setRHS(l, rhs.data(), false);
+      if (!h->desc.vc) continue;
+      S.setACoef(l, a.data(), false);
+      for (int d = 0; d < 3; ++d) {
+        std::vector<int64_t> fo(L.grids.size() + 1, 0);
+        for (size_t b = 0; b < L.grids.size(); ++b) {
+          cmg::Box fb = L.grids[b];
+          fb.hi[d] += 1;
+          fo[b + 1] = fo[b] + fb.numPts();
+        }
+        std::vector<double> bc(fo.back());
+        parallelBoxes(L.grids.size(), [&](size_t b) {
+          cmg::Box fb = L.grids[b];
+          fb.hi[d] += 1;
+          int64_t q = fo[b];
+          for (int k = fb.lo[2]; k <= fb.hi[2]; ++k)
+            for (int j = fb.lo[1]; j <= fb.hi[1]; ++j)
+              for (int i = fb.lo[0]; i <= fb.hi[0]; ++i, ++q) {
+                int iv[3] = {i, j, k};
+                double x[3];
+                for (int e = 0; e < 3; ++e) x[e] = (e == d) ? iv[e] * dx : (iv[e] + 0.5) * dx;
+                bc[q] = prob.bcoef.eval(x[0], x[1], x[2]);
+              }
+        });
+        S.setBCoef(l, d, bc.data(), false);
+      }
+    }
+    if (h->desc.vc) S.finalizeCoefficients();
+  });
+}
+
+int cmg_domain_split(const int domain_lo[3], const int domain_hi[3], int max_box, int block_factor, cmg_box* out,
+                     int cap, int* n) {
+  return guard([&]() {
+    if (!domain_lo || !domain_hi || !n || block_factor < 1 || max_box < 0)
+      throw std::invalid_argument("cmg: invalid domainSplit arguments");
+    cmg::Box dom(cmg::IV(domain_lo[0], domain_lo[1], domain_lo[2]), cmg::IV(domain_hi[0], domain_hi[1], domain_hi[2]));
+    if (!dom.coarsenable(block_factor)) throw std::invalid_argument("cmg: domain not coarsenable by the blocking factor");
+    cmg::Layout l(cmg::domainSplit(dom, max_box, block_factor));
+    *n = (int)l.size();
+    if (out) {
+      if (cap < (int)l.size()) throw std::invalid_argument("cmg: box buffer too small");
+      for (size_t b = 0; b < l.size(); ++b) fromBox(l[b], out[b]);
+    }
+  });
+}
+
+int cmg_exchange_plan(const cmg_hierarchy* h, int level, int* items14, int cap, int* n) {
+  return guard([&]() {
+    needLevel(h, level);
+    auto plan = cmg::exchangePlan(h->solver->level(level).grids);
+    *n = (int)plan.size();
+    if (items14) {
+      if (cap < (int)plan.size()) throw std::invalid_argument("cmg: item buffer too small");
+      for (size_t i = 0; i < plan.size(); ++i)
+        putMotion(items14 + 14 * i, plan[i].from, plan[i].to, plan[i].fromRegion, plan[i].toRegion);
+    }
+  });
+}
+
+int cmg_coarse_fine_plan(const cmg_hierarchy* h, int level, int* items14, int cap, int* n) {
+  return guard([&]() {
+    needLevel(h, level);
+    if (level < 1) throw std::invalid_argument("cmg: level 0 has no coarser level");
+    const auto& F = h->solver->level(level);
+    *n = (int)F.toCoarse.size();
+    if (items14) {
+      if (cap < *n) throw std::invalid_argument("cmg: item buffer too small");
+      for (size_t i = 0; i < F.toCoarse.size(); ++i) {
+        const auto& it = F.toCoarse[i];
+        cmg::Box r(cmg::IV(it.lo[0], it.lo[1], it.lo[2]), cmg::IV(it.hi[0], it.hi[1], it.hi[2]));
+        putMotion(items14 + 14 * i, it.fbox, it.cbox, r, r);
+      }
+    }
+  });
+}
+
+int cmg_get_stream(const cmg_hierarchy* h, void** stream) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (!stream) throw std::invalid_argument("cmg: null output");
+    *stream = (void*)h->stream;
+  });
+}
+
+int cmg_launch_count(int64_t* out) {
+  return guard([&]() {
+    if (!out) throw std::invalid_argument("cmg: null output");
+    *out = (int64_t)cmg::launchCount();
+  });
+}
+
+int cmg_profile_enable(cmg_hierarchy* h, int on) {
+  return guard([&]() {
+    needLevel(h, 0);
+    h->solver->profileEnable(on != 0);
+  });
+}
+
+int cmg_profile_read(cmg_hierarchy* h, int kernel_class, int64_t* launches, double* ms, double* bytes) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (!launches || !ms || !bytes) throw std::invalid_argument("cmg: null output");
+    h->solver->profileRead(kernel_class, launches, ms, bytes);
+  });
+}
+
+int cmg_layout_exchange_plan(const cmg_box* boxes, int nbox, int* items14, int cap, int* n) {
+  return guard([&]() {
+    if (!boxes || nbox < 1 || !n) throw std::invalid_argument("cmg: invalid box list");
+    std::vector<cmg::Box> v;
+    for (int b = 0; b < nbox; ++b) v.push_back(toBox(boxes[b]));
+    auto plan = cmg::exchangePlan(cmg::Layout(v));
+    *n = (int)plan.size();
+    if (items14) {
+      if (cap < (int)plan.size()) throw std::invalid_argument("cmg: item buffer too small");
+      for (size_t i = 0; i < plan.size(); ++i)
+        putMotion(items14 + 14 * i, plan[i].from, plan[i].to, plan[i].fromRegion, plan[i].toRegion);
+    }
+  });
+}
+
+int cmg_layout_coarse_fine_plan(const cmg_box* fine, int nfine, const cmg_box* coarse, int ncoarse, int* items14,
+                                int cap, int* n) {
+  return guard([&]() {
+    if (!fine || !coarse || nfine < 1 || ncoarse < 1 || !n) throw std::invalid_argument("cmg: invalid box lists");
+    std::vector<cmg::Box> f, c;
+    for (int b = 0; b < nfine; ++b) f.push_back(toBox(fine[b]));
+    for (int b = 0; b < ncoarse; ++b) c.push_back(toBox(coarse[b]));
+    auto plan = cmg::copyPlan(cmg::Layout(f).coarsen(2), cmg::Layout(c));
+    *n = (int)plan.size();
+    if (items14) {
+      if (cap < (int)plan.size()) throw std::invalid_argument("cmg: item buffer too small");
+      for (size_t i = 0; i < plan.size(); ++i)
+        putMotion(items14 + 14 * i, plan[i].from, plan[i].to, plan[i].fromRegion, plan[i].toRegion);
+    }
+  });
+}
+
+int cmg_vcycle_bytes(const cmg_hierarchy* h, const cmg_solve_params* p, double* out) {
+  return guard([&]() {
+    needLevel(h, 0);
+    cmg::SolveParams sp;
+    sp.pre = p->pre;
+    sp.post = p->post;
+    *out = h->solver->vcycleBytes(sp);
+  });
+}
+
+}  // extern "C"

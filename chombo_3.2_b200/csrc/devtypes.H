@@ -1,0 +1,112 @@
+// Plain-old-data tables that the host plan builder writes and the CUDA
+// kernels read.  One level's fields all share one ghosted layout:
+//   every box owns a FAB of (nx+2) x (ny+2) x (nz+2) cells (one ghost layer),
+//   stored x-fastest with the x pitch padded to a multiple of 4 elements and
+//   the first valid cell at column XOFF+1 = 4, so every valid row starts on
+//   a 32-byte boundary for FP64 (16-byte for FP32).
+// Face-centred data (the b coefficient in direction d) uses the same layout:
+// the face on the low side of cell i in direction d is stored at cell i, so
+// faces lo..hi+1 fit in the valid region plus the high ghost layer.
+#ifndef CMG_DEVTYPES_H
+#define CMG_DEVTYPES_H
+
+#include <stdint.h>
+
+namespace cmg {
+
+enum { XOFF = 3 };
+
+struct BoxDesc {
+  int lo[3], hi[3];
+  int px, py;       // x pitch and y extent (ny + 2) of the ghosted FAB
+  int64_t off;      // element offset of ghost cell (lo0-1, lo1-1, lo2-1)
+};
+
+#if defined(__CUDACC__)
+#define CMG_HD __host__ __device__ __forceinline__
+#else
+#define CMG_HD inline
+#endif
+
+CMG_HD int64_t cellIndex(const BoxDesc& b, int i, int j, int k) {
+  return b.off + (int64_t)(i - b.lo[0] + 1 + XOFF) +
+         (int64_t)b.px * ((int64_t)(j - b.lo[1] + 1) + (int64_t)b.py * (k - b.lo[2] + 1));
+}
+
+// Ghost-layer work items executed by one kernel per fill (exchange copies,
+// physical boundary values, homogeneous coarse-fine values, zeroing).
+enum GhostKind {
+  G_COPY = 0,      // dst(cell) = src(cell), cells of region (Copier item)
+  G_BC = 1,        // homogeneous first-order Dirichlet: g = 2*0 - interior
+  G_CFQUAD = 2,    // homogeneous quadratic CF: g = c1*phi(1 in) + c2*phi(2 in)
+  G_CFLIN = 3,     // one-cell-wide box: g = f*phi(1 in)
+  G_ZERO = 4       // dst(cell) = 0 (covered cells before a norm)
+};
+
+struct GhostTask {
+  int kind, dst, src, dir, side;  // side = -1 (low) or +1 (high)
+  int lo[3], hi[3];
+};
+
+// Work decomposition of a box list into fixed-size chunks of cells (or of
+// one colour's cells for red-black sweeps): chunk c covers cells
+// [start, start + CHUNK) of box `box` in the enumeration used by the kernel.
+struct Chunk {
+  int box;
+  int start;
+};
+
+// Inhomogeneous quadratic coarse-fine interpolation (QuadCFInterp): one entry
+// per fine ghost cell.  Coarse data are read straight from the coarse level
+// through precomputed element offsets.
+struct CFDeriv {
+  int kind;   // 0: zero, 1: centred standard form, 2: weighted stencil
+  int n;      // number of (weight, offset) pairs for kind 2
+  int start;  // first pair in the pool; kind 1 uses pool offsets only
+};
+struct CFCoarse {
+  int64_t cc;      // offset of the coarse cell under the ghost
+  CFDeriv d1[2];   // first derivatives along the two tangential directions
+  CFDeriv d2[2];   // second derivatives
+  CFDeriv mx;      // mixed derivative
+};
+struct CFFine {
+  int64_t g;       // fine ghost cell
+  int64_t pa, pb;  // fine cells 2 and 1 inward of the ghost
+  double x1, x2;   // tangential offsets of the fine centre from the coarse centre
+  int coarse;      // CFCoarse index
+  int packed;      // 1: Fortran-form interpolation, 0: C++-form
+};
+
+// Flux-register correction of one uncovered coarse cell next to finer cells.
+struct RefluxCell {
+  int64_t c;       // coarse cell (coarse level layout)
+  int nco;         // coarse face terms (<= 6)
+  int nfi;         // fine face groups (<= 6), each of 4 fine faces
+  int start;       // first coarse term in the term pool
+  int fstart;      // first fine group in the group pool
+};
+struct RefluxCoarseTerm {
+  int64_t hi, lo;  // cells on each side of the coarse face
+  int64_t bface;   // face coefficient element (VC), -1 otherwise
+  int dir;
+  double sgn;      // +1 (low-side location) or -1 (high-side)
+};
+struct RefluxFineGroup {
+  int64_t hi[4], lo[4];  // cells on each side of the 4 fine faces, k-j-i order
+  int64_t bface[4];
+  int dir;
+  double scale;          // sign(side) * 1 / nRef^2
+};
+
+// Map between a fine level and its coarse parent: one item per (coarse box,
+// fine box) pair whose coarsened fine box meets the coarse box; region is in
+// coarse index space.
+struct CoarseFineItem {
+  int cbox, fbox;
+  int lo[3], hi[3];
+};
+
+}  // namespace cmg
+
+#endif

@@ -1,0 +1,104 @@
+// Device kernels of the AMR multigrid V-cycle (sm_100a).  Each launcher
+// applies one reference operation to every box of a level in one launch,
+// driven by the tables in devtypes.H.  T is the field precision (double for
+// the drop-in solve, float for the inner V-cycles of iterative refinement).
+#ifndef CMG_KERNELS_H
+#define CMG_KERNELS_H
+
+#include <cuda_runtime.h>
+
+#include "devtypes.H"
+
+namespace cmg {
+
+// Device-resident plan of one level (pointers into device memory).
+struct LevelDev {
+  const BoxDesc* boxes = nullptr;
+  int nbox = 0;
+  int64_t nelem = 0;
+  const GhostTask* ghost = nullptr;
+  int nExchBC = 0, nGhost = 0;
+  const GhostTask* zero = nullptr;
+  int nZero = 0;
+  const Chunk* chAll = nullptr;
+  int nAll = 0;
+  const Chunk* chColor[2] = {nullptr, nullptr};
+  int nColor[2] = {0, 0};
+  // coarse-fine interpolation from the coarser level
+  const CFCoarse* cfC = nullptr;
+  const CFFine* cfF = nullptr;
+  int nCfF = 0;
+  const double* cfW = nullptr;
+  const int64_t* cfOff = nullptr;
+  // coarse/fine maps to the coarser level
+  const CoarseFineItem* items = nullptr;
+  const Chunk* itemChC = nullptr;
+  int nItemChC = 0;
+  const Chunk* itemChF = nullptr;
+  int nItemChF = 0;
+  // flux-register correction from the finer level
+  const RefluxCell* rfCells = nullptr;
+  int nRf = 0;
+  const RefluxCoarseTerm* rfC = nullptr;
+  const RefluxFineGroup* rfF = nullptr;
+  double dx = 0, dxCrse = 0;
+};
+
+// Operator coefficients: L = alpha*phi + beta*Lap(phi) (constant, vc = 0) or
+// L = alpha*a*phi - beta*div(b grad phi) (variable, vc = 1).
+template <class T>
+struct Coef {
+  int vc = 0;
+  double alpha = 0, beta = 1;
+  const T* a = nullptr;
+  const T* b[3] = {nullptr, nullptr, nullptr};
+  const T* lambda = nullptr;
+};
+
+template <class T> void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s);
+template <class T> void zeroCovered(const LevelDev& L, T* f, cudaStream_t s);
+template <class T> void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s);
+// residualI form: r = rhs - L(phi) in the operator's own expression order.
+template <class T> void residual(const LevelDev& L, T* r, const T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s);
+// applyOpI form: lofphi = L(phi).
+template <class T> void applyOp(const LevelDev& L, T* lofphi, const T* phi, const Coef<T>& c, cudaStream_t s);
+// r = -lofphi + rhs over valid cells (LevelDataOps::axby(r, r, rhs, -1, 1)).
+template <class T> void negAdd(const LevelDev& L, T* r, const T* lofphi, const T* rhs, cudaStream_t s);
+// Multigrid restriction of the residual (RESTRICTRES), box b -> coarsened box b.
+template <class T> void restrictMG(const LevelDev& F, const LevelDev& C, T* resC, const T* phi, const T* rhs,
+                                   const Coef<T>& c, cudaStream_t s);
+// Multigrid piecewise-constant prolongation, box b <- coarsened box b.
+template <class T> void prolongMG(const LevelDev& F, const LevelDev& C, T* phi, const T* corrC, cudaStream_t s);
+// AMR restriction: coarse(c) = average of 8 fine values, over coarse/fine items.
+template <class T> void averageAMR(const LevelDev& F, const LevelDev& C, T* coarse, const T* fine, cudaStream_t s);
+// AMR prolongation: fine += coarse(i/2) over coarse/fine items.
+template <class T> void prolongAMR(const LevelDev& F, const LevelDev& C, T* fine, const T* coarse, cudaStream_t s);
+// Inhomogeneous quadratic coarse-fine ghost fill of phiF from phiC.
+template <class T> void quadCF(const LevelDev& F, T* phiF, const T* phiC, cudaStream_t s);
+// Flux-register correction of lofphiC from phiC and phiF (finer level).
+template <class T> void reflux(const LevelDev& C, T* lofphiC, const T* phiC, const T* phiF, const Coef<T>& cc,
+                               const Coef<T>& cf, cudaStream_t s);
+// lhs += scale * x over valid cells.
+template <class T> void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s);
+// Max |f| over valid cells, folded into *out (device scalar) with max().
+template <class T> void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s);
+
+// Work vectors of the bottom BiCGStab: r, r~, e, p, p~, s~, t, v (each one
+// level-sized array), per-box partial sums and a 2-int status (exit, iters).
+struct BottomWork {
+  double* v[8];
+  double* part;
+  int* status;
+};
+// BiCGStab bottom solve of L(phi) = rhs (homogeneous boundary conditions) on
+// one level, one thread block, reference summation order.  eps and metric are
+// the tolerance and convergence metric AMRMultiGrid hands its bottom solver.
+void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
+                 double eps, double metric, cudaStream_t s);
+
+// Number of kernel launches issued by the launchers above since load.
+long long launchCount();
+
+}  // namespace cmg
+
+#endif

@@ -1,0 +1,884 @@
+// Device kernels of the AMR multigrid V-cycle.  Each kernel states the
+// reference operation (ChF kernel or C++ routine, paths relative to the
+// Chombo lib/src tree) whose arithmetic it reproduces term for term, so the
+// FP64 build (compiled with --fmad=false) rounds exactly like the reference.
+#include <atomic>
+#include <cstdio>
+#include <stdexcept>
+
+#include "kernels.H"
+#include "plan.H"
+
+namespace cmg {
+
+namespace {
+
+inline void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "cmg: %s: %s", what, cudaGetErrorString(e));
+    throw std::runtime_error(buf);
+  }
+}
+std::atomic<long long> g_launches{0};
+#define CMG_LAUNCHED(name) (g_launches.fetch_add(1, std::memory_order_relaxed), check(cudaGetLastError(), name))
+
+struct Strides {
+  int64_t sy, sz;
+};
+__device__ __forceinline__ Strides strides(const BoxDesc& b) {
+  Strides s;
+  s.sy = b.px;
+  s.sz = (int64_t)b.px * b.py;
+  return s;
+}
+
+// Cell q of box b in x-fastest order.
+__device__ __forceinline__ bool allCell(const BoxDesc& b, int q, int& i, int& j, int& k) {
+  int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
+  if (q >= nx * ny * nz) return false;
+  i = b.lo[0] + q % nx;
+  int r = q / nx;
+  j = b.lo[1] + r % ny;
+  k = b.lo[2] + r / ny;
+  return true;
+}
+
+// q-th cell of colour `color` (cells with i+j+k = color mod 2), the cells the
+// GSRB kernels visit for redBlack = color (AMRPoissonOpF.ChF:151-158).
+__device__ __forceinline__ bool colorCell(const BoxDesc& b, int q, int color, int& i, int& j, int& k) {
+  int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
+  int half = (nx + 1) / 2;
+  int r = q / half;
+  if (r >= ny * nz) return false;
+  j = b.lo[1] + r % ny;
+  k = b.lo[2] + r / ny;
+  int par = ((b.lo[0] + j + k + color) % 2 + 2) % 2;
+  i = b.lo[0] + par + 2 * (q % half);
+  return i <= b.hi[0];
+}
+
+// ---------------------------------------------------------------- ghosts
+// Exchange copies (BoxLayoutData local copy), homogeneous Dirichlet faces
+// (BCFunc.cpp:25-32,294-354: ghost = 2*0 - near), homogeneous quadratic and
+// linear coarse-fine ghosts (InterpF.ChF:435-494) and zeroing.
+template <class T>
+__global__ void k_ghost(const BoxDesc* boxes, const GhostTask* tasks, T* f, T c1, T c2, T flin) {
+  const GhostTask t = tasks[blockIdx.x];
+  const BoxDesc db = boxes[t.dst];
+  int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1, nz = t.hi[2] - t.lo[2] + 1;
+  int n = nx * ny * nz;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    int i = t.lo[0] + q % nx, r = q / nx;
+    int j = t.lo[1] + r % ny, k = t.lo[2] + r / ny;
+    int64_t g = cellIndex(db, i, j, k);
+    if (t.kind == G_COPY) {
+      f[g] = f[cellIndex(boxes[t.src], i, j, k)];
+    } else if (t.kind == G_ZERO) {
+      f[g] = T(0);
+    } else {
+      int e[3] = {0, 0, 0};
+      e[t.dir] = -t.side;  // one cell inward
+      int64_t in1 = cellIndex(db, i + e[0], j + e[1], k + e[2]);
+      if (t.kind == G_BC) {
+        T zero = T(0);
+        f[g] = T(2) * zero - f[in1];
+      } else if (t.kind == G_CFLIN) {
+        f[g] = flin * f[in1];
+      } else {
+        int64_t in2 = cellIndex(db, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
+        f[g] = c1 * f[in1] + c2 * f[in2];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- stencils
+// Sum of the six neighbours in the ChF order (+x, -x, +y, -y, +z, -z).
+template <class T>
+__device__ __forceinline__ T nbrSum(const T* p, int64_t c, const Strides& s) {
+  return p[c + 1] + p[c - 1] + p[c + s.sy] + p[c - s.sy] + p[c + s.sz] + p[c - s.sz];
+}
+
+// Variable-coefficient divergence term of VCAMRPoissonOpF.ChF:93-111.
+template <class T>
+__device__ __forceinline__ T vcDiv(const T* p, const T* b0, const T* b1, const T* b2, int64_t c, const Strides& s) {
+  T pc = p[c];
+  return b0[c + 1] * (p[c + 1] - pc) - b0[c] * (pc - p[c - 1]) + b1[c + s.sy] * (p[c + s.sy] - pc) -
+         b1[c] * (pc - p[c - s.sy]) + b2[c + s.sz] * (p[c + s.sz] - pc) - b2[c] * (pc - p[c - s.sz]);
+}
+
+struct Scal {
+  double dxinv, lambda, alpha, beta;
+  int laplacian;
+};
+
+// GSRBLAPLACIAN / GSRBHELMHOLTZ (AMRPoissonOpF.ChF:51-198) and
+// GSRBHELMHOLTZVC3D (VCAMRPoissonOpF.ChF:57-125), one colour.
+template <class T, int VC>
+__global__ void k_gsrb(const BoxDesc* boxes, const Chunk* chunks, T* phi, const T* rhs, int color, Scal sc,
+                       const T* a, const T* b0, const T* b1, const T* b2, const T* lam) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  int i, j, k;
+  if (!colorCell(bd, ch.start + threadIdx.x, color, i, j, k)) return;
+  Strides s = strides(bd);
+  int64_t c = cellIndex(bd, i, j, k);
+  const T dxinv = T(sc.dxinv);
+  if (VC) {
+    T pc = phi[c];
+    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, c, s) * dxinv;
+    phi[c] = pc - lam[c] * (lofphi - rhs[c]);
+  } else if (sc.laplacian) {
+    T lphi = nbrSum(phi, c, s) * dxinv;
+    phi[c] = T(sc.lambda) * (rhs[c] - lphi);
+  } else {
+    T pc = phi[c];
+    T lphi = (nbrSum(phi, c, s) - T(2.0) * T(3) * pc) * dxinv;
+    T helmop = T(sc.alpha) * pc + T(sc.beta) * lphi;
+    phi[c] = pc + T(sc.lambda) * (helmop - rhs[c]);
+  }
+}
+
+// OPERATORLAPRES / OPERATORLAP (AMRPoissonOpF.ChF:287-377) and
+// VCCOMPUTERES3D / VCCOMPUTEOP3D (VCAMRPoissonOpF.ChF:148-312).
+// mode 0: r = rhs - L(phi) (residual form), mode 1: r = L(phi).
+template <class T, int VC, int MODE>
+__global__ void k_op(const BoxDesc* boxes, const Chunk* chunks, T* r, const T* phi, const T* rhs, Scal sc,
+                     const T* a, const T* b0, const T* b1, const T* b2) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  int i, j, k;
+  if (!allCell(bd, ch.start + threadIdx.x, i, j, k)) return;
+  Strides s = strides(bd);
+  int64_t c = cellIndex(bd, i, j, k);
+  const T dxinv = T(sc.dxinv);
+  T pc = phi[c];
+  if (VC) {
+    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, c, s) * dxinv;
+    r[c] = MODE == 0 ? rhs[c] - lofphi : lofphi;
+  } else {
+    T lap = (nbrSum(phi, c, s) - T(6) * pc) * dxinv;
+    if (MODE == 0)
+      r[c] = -(T(sc.alpha) * pc) - T(sc.beta) * lap + rhs[c];
+    else
+      r[c] = T(sc.alpha) * pc + T(sc.beta) * lap;
+  }
+}
+
+template <class T>
+__global__ void k_negadd(const BoxDesc* boxes, const Chunk* chunks, T* r, const T* lofphi, const T* rhs) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  int i, j, k;
+  if (!allCell(bd, ch.start + threadIdx.x, i, j, k)) return;
+  int64_t c = cellIndex(bd, i, j, k);
+  r[c] = lofphi[c] * T(-1) + rhs[c] * T(1);
+}
+
+template <class T>
+__global__ void k_incr(const BoxDesc* boxes, const Chunk* chunks, T* lhs, const T* x, T scale) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  int i, j, k;
+  if (!allCell(bd, ch.start + threadIdx.x, i, j, k)) return;
+  int64_t c = cellIndex(bd, i, j, k);
+  lhs[c] = lhs[c] + x[c] * scale;
+}
+
+__device__ __forceinline__ void atomicMaxPos(double* addr, double v) {
+  // v >= 0: the IEEE bit pattern of a non-negative double orders like an
+  // unsigned integer, so an integer max is a floating max.
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+template <class T>
+__global__ void k_maxnorm(const BoxDesc* boxes, const Chunk* chunks, const T* f, double* out) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  int i, j, k;
+  double v = 0.0;
+  if (allCell(bd, ch.start + threadIdx.x, i, j, k)) v = fabs((double)f[cellIndex(bd, i, j, k)]);
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __shared__ double red[CHUNK / 32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < CHUNK / 32 ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) atomicMaxPos(out, v);
+  }
+}
+
+// RESTRICTRES / RESTRICTRESVC3D (AMRPoissonOpF.ChF:394-438,
+// VCAMRPoissonOpF.ChF:337-413): res_c accumulates (rhs - L phi)/8 over its 8
+// fine cells in fine k-j-i order, starting from zero.
+template <class T, int VC>
+__global__ void k_restrictmg(const BoxDesc* fboxes, const BoxDesc* cboxes, const Chunk* chunks, T* resC,
+                             const T* phi, const T* rhs, Scal sc, const T* a, const T* b0, const T* b1,
+                             const T* b2) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc cb = cboxes[ch.box];
+  int I, J, K;
+  if (!allCell(cb, ch.start + threadIdx.x, I, J, K)) return;
+  const BoxDesc fb = fboxes[ch.box];
+  Strides s = strides(fb);
+  const T dxinv = T(sc.dxinv);
+  const T denom = T(8);
+  T acc = T(0);
+  for (int kk = 0; kk < 2; ++kk)
+    for (int jj = 0; jj < 2; ++jj)
+      for (int ii = 0; ii < 2; ++ii) {
+        int64_t c = cellIndex(fb, 2 * I + ii, 2 * J + jj, 2 * K + kk);
+        T pc = phi[c];
+        T lofphi;
+        if (VC)
+          lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, c, s) * dxinv;
+        else
+          lofphi = T(sc.alpha) * pc + T(sc.beta) * (nbrSum(phi, c, s) - pc * T(2) * T(3)) * dxinv;
+        acc = acc + (rhs[c] - lofphi) / denom;
+      }
+  resC[cellIndex(cb, I, J, K)] = acc;
+}
+
+// PROLONG (AMRPoissonOpF.ChF:453-478): phi += coarse(i/2), same box index.
+template <class T>
+__global__ void k_prolongmg(const BoxDesc* fboxes, const BoxDesc* cboxes, const Chunk* chunks, T* phi,
+                            const T* corrC) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc fb = fboxes[ch.box];
+  int i, j, k;
+  if (!allCell(fb, ch.start + threadIdx.x, i, j, k)) return;
+  int64_t c = cellIndex(fb, i, j, k);
+  phi[c] = phi[c] + corrC[cellIndex(cboxes[ch.box], i >> 1, j >> 1, k >> 1)];
+}
+
+// AVERAGE with refRatio 2 (AverageF.ChF:36-55) written straight into the
+// coarse level through the coarsened-fine -> coarse copy items.
+template <class T>
+__global__ void k_average(const BoxDesc* fboxes, const BoxDesc* cboxes, const CoarseFineItem* items,
+                          const Chunk* chunks, T* coarse, const T* fine) {
+  Chunk ch = chunks[blockIdx.x];
+  const CoarseFineItem it = items[ch.box];
+  int q = ch.start + threadIdx.x;
+  int nx = it.hi[0] - it.lo[0] + 1, ny = it.hi[1] - it.lo[1] + 1, nz = it.hi[2] - it.lo[2] + 1;
+  if (q >= nx * ny * nz) return;
+  int I = it.lo[0] + q % nx, r = q / nx, J = it.lo[1] + r % ny, K = it.lo[2] + r / ny;
+  const BoxDesc fb = fboxes[it.fbox];
+  Strides s = strides(fb);
+  int64_t f = cellIndex(fb, 2 * I, 2 * J, 2 * K);
+  T sum = fine[f] + fine[f + 1] + fine[f + s.sy] + fine[f + s.sy + 1] + fine[f + s.sz] + fine[f + s.sz + 1] +
+          fine[f + s.sz + s.sy] + fine[f + s.sz + s.sy + 1];
+  coarse[cellIndex(cboxes[it.cbox], I, J, K)] = T(0.125) * sum;
+}
+
+// AMRProlongS (AMRPoissonOp.cpp:959-990): fine += coarse(i/2).
+template <class T>
+__global__ void k_prolongamr(const BoxDesc* fboxes, const BoxDesc* cboxes, const CoarseFineItem* items,
+                             const Chunk* chunks, T* fine, const T* coarse) {
+  Chunk ch = chunks[blockIdx.x];
+  const CoarseFineItem it = items[ch.box];
+  int q = ch.start + threadIdx.x;
+  int nx = it.hi[0] - it.lo[0] + 1, ny = it.hi[1] - it.lo[1] + 1, nz = it.hi[2] - it.lo[2] + 1;
+  int cq = q >> 3, sub = q & 7;
+  if (cq >= nx * ny * nz) return;
+  int I = it.lo[0] + cq % nx, r = cq / nx, J = it.lo[1] + r % ny, K = it.lo[2] + r / ny;
+  int64_t f = cellIndex(fboxes[it.fbox], 2 * I + (sub & 1), 2 * J + ((sub >> 1) & 1), 2 * K + (sub >> 2));
+  fine[f] = fine[f] + coarse[cellIndex(cboxes[it.cbox], I, J, K)];
+}
+
+// QuadCFStencil derivatives (AMRTools/QuadCFStencil.cpp:33-260).
+template <class T>
+__device__ __forceinline__ T cfFirst(const CFDeriv& d, const double* w, const int64_t* off, const T* pc, T dxc) {
+  if (d.kind == 1) return (pc[off[d.start + 1]] - pc[off[d.start]]) / (T(2.0) * dxc);
+  if (d.kind == 0) return T(0);
+  T v = T(0);
+  for (int n = 0; n < d.n; ++n) v += T(w[d.start + n]) * pc[off[d.start + n]];
+  return v / dxc;
+}
+template <class T>
+__device__ __forceinline__ T cfSecond(const CFDeriv& d, const double* w, const int64_t* off, const T* pc, T dxc) {
+  if (d.kind == 1)
+    return (pc[off[d.start + 1]] + pc[off[d.start]] - T(2.0) * pc[off[d.start + 2]]) / (dxc * dxc);
+  if (d.kind == 0) return T(0);
+  T v = T(0);
+  for (int n = 0; n < d.n; ++n) v += T(w[d.start + n]) * pc[off[d.start + n]];
+  return v / (dxc * dxc);
+}
+template <class T>
+__device__ __forceinline__ T cfMixed(const CFDeriv& d, const double* w, const int64_t* off, const T* pc, T dxc) {
+  if (d.kind == 1) {
+    const int64_t* o = off + d.start;  // ur, ul, lr, ll
+    return (pc[o[0]] + pc[o[3]] - pc[o[2]] - pc[o[1]]) / (T(4.) * dxc * dxc);
+  }
+  if (d.kind == 0) return T(0);
+  T v = T(0);
+  for (int n = 0; n < d.n; ++n) v += T(w[d.start + n]) * pc[off[d.start + n]];
+  return v / (dxc * dxc);
+}
+
+// QuadCFInterp::getPhiStar + interpOnIVS (AMRTools/QuadCFInterp.cpp:569-839):
+// phistar from the coarse Taylor expansion, then the quadratic through
+// phistar and two fine cells, in the Fortran (packed face,
+// QuadCFInterpF.ChF:9-48) or C++ (unpacked face) arithmetic.
+template <class T>
+__global__ void k_quadcf(const CFFine* fine, int n, const CFCoarse* coarse, const double* w, const int64_t* off,
+                         T* phiF, const T* phiC, T h) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const CFFine e = fine[t];
+  const CFCoarse cc = coarse[e.coarse];
+  const T dxc = T(2) * h;
+  T s1 = cfFirst(cc.d1[0], w, off, phiC, dxc);
+  T c1 = cfSecond(cc.d2[0], w, off, phiC, dxc);
+  T s2 = cfFirst(cc.d1[1], w, off, phiC, dxc);
+  T c2 = cfSecond(cc.d2[1], w, off, phiC, dxc);
+  T mx = cfMixed(cc.mx, w, off, phiC, dxc);
+  const T x1 = T(e.x1), x2 = T(e.x2);
+  T update1 = x1 * s1 + T(0.5) * x1 * x1 * c1;
+  T update2 = x2 * s2 + T(0.5) * x2 * x2 * c2;
+  T update3 = x1 * x2 * mx;
+  T ps = phiC[cc.cc] + update1 + update2 + update3;
+  T pa = phiF[e.pa], pb = phiF[e.pb];
+  T r;
+  if (e.packed) {
+    T frac = T(2.0) / (h * h);
+    T denom = T(2 * 2 + 4 * 2 + 3);
+    T mult = frac / denom;
+    T invh = T(1.0) / h;
+    T x = T(2.0) * h;
+    T xsq = T(4.0) * h * h;
+    T a = mult * (T(2.0) * ps + T(2 + 1) * pa - T(2 + 3) * pb);
+    T b = (pb - pa) * invh - a * h;
+    r = xsq * a + b * x + pa;
+  } else {
+    T a = (T(2.) / h / h) * (T(2.) * ps + pa * (T(2) + T(1.0)) - pb * (T(2) + T(3.0))) / (T(2 * 2 + 4 * 2) + T(3.0));
+    T b = (pb - pa) / h - a * h;
+    T x = T(2.) * h;
+    r = a * x * x + b * x + pa;
+  }
+  phiF[e.g] = r;
+}
+
+// Flux-register correction (AMRPoissonOp::reflux, VCAMRPoissonOp2::reflux
+// and LevelFluxRegister incrementCoarse/incrementFine/reflux).
+template <class T, int VC>
+__global__ void k_reflux(const RefluxCell* cells, int n, const RefluxCoarseTerm* cterms, const RefluxFineGroup* fgroups,
+                         T* lofphi, const T* phiC, const T* phiF, const T* bc0, const T* bc1, const T* bc2,
+                         const T* bf0, const T* bf1, const T* bf2, T sc, T sf, T negs) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const RefluxCell rc = cells[t];
+  const T* bc[3] = {bc0, bc1, bc2};
+  const T* bf[3] = {bf0, bf1, bf2};
+  T u = lofphi[rc.c];
+  T coar = T(0);
+  for (int m = 0; m < rc.nco; ++m) {
+    const RefluxCoarseTerm ct = cterms[rc.start + m];
+    T flux;
+    if (VC)
+      flux = -bc[ct.dir][ct.bface] * ((phiC[ct.hi] - phiC[ct.lo]) * sc);
+    else
+      flux = (phiC[ct.hi] - phiC[ct.lo]) * sc;
+    coar = coar + flux * T(ct.sgn);
+  }
+  u = u + coar * negs;
+  for (int m = 0; m < rc.nfi; ++m) {
+    const RefluxFineGroup& g = fgroups[rc.fstart + m];
+    T reg = T(0);
+    for (int q = 0; q < 4; ++q) {
+      T ff;
+      if (VC)
+        ff = -bf[g.dir][g.bface[q]] * ((phiF[g.hi[q]] - phiF[g.lo[q]]) * sf);
+      else
+        ff = (phiF[g.hi[q]] - phiF[g.lo[q]]) * sf;
+      reg = reg + T(g.scale) * ff;
+    }
+    u = u + reg * negs;
+  }
+  lofphi[rc.c] = u;
+}
+
+// ---------------------------------------------------------------- bottom
+// BiCGStabSolver<T>::solve (AMRElliptic/BiCGStabSolver.H:199-515) on the
+// deepest multigrid level, run by one thread block so that every dot product
+// and norm is summed in the reference's order: per box in x-fastest order
+// (FArrayBox::dotProduct, FArrayBox.cpp:260-280; FArrayBox::sumPow pencil
+// order, FArrayBox.cpp:168-209), then box by box.
+struct BottomArgs {
+  LevelDev L;
+  Scal sc;
+  int vc;
+  const double *a, *b0, *b1, *b2, *lam;
+  double *phi;
+  const double* rhs;
+  double *r, *rt, *e, *p, *pt, *st, *t, *v, *part;
+  double eps, metric, reps, hang, small, mult;
+  int imax, numRestarts, nsmooth;
+  int* status;
+};
+
+__device__ void blkGhost(const BottomArgs& A, double* f) {
+  const LevelDev& L = A.L;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int ti = warp; ti < L.nGhost; ti += nw) {
+    const GhostTask t = L.ghost[ti];
+    const BoxDesc db = L.boxes[t.dst];
+    int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1, nz = t.hi[2] - t.lo[2] + 1;
+    for (int q = lane; q < nx * ny * nz; q += 32) {
+      int i = t.lo[0] + q % nx, r = q / nx, j = t.lo[1] + r % ny, k = t.lo[2] + r / ny;
+      int64_t g = cellIndex(db, i, j, k);
+      if (t.kind == G_COPY) {
+        f[g] = f[cellIndex(L.boxes[t.src], i, j, k)];
+      } else if (t.kind == G_BC) {
+        int e[3] = {0, 0, 0};
+        e[t.dir] = -t.side;
+        double zero = 0.0;
+        f[g] = 2.0 * zero - f[cellIndex(db, i + e[0], j + e[1], k + e[2])];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <class F>
+__device__ void blkCells(const LevelDev& L, F fn) {
+  int n = L.nAll * CHUNK;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    Chunk ch = L.chAll[idx / CHUNK];
+    const BoxDesc bd = L.boxes[ch.box];
+    int i, j, k;
+    if (allCell(bd, ch.start + idx % CHUNK, i, j, k)) fn(bd, cellIndex(bd, i, j, k));
+  }
+  __syncthreads();
+}
+
+__device__ void blkGsrb(const BottomArgs& A, double* phi, const double* rhs, int color) {
+  const LevelDev& L = A.L;
+  int n = L.nColor[color] * CHUNK;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    Chunk ch = L.chColor[color][idx / CHUNK];
+    const BoxDesc bd = L.boxes[ch.box];
+    int i, j, k;
+    if (!colorCell(bd, ch.start + idx % CHUNK, color, i, j, k)) continue;
+    Strides s = strides(bd);
+    int64_t c = cellIndex(bd, i, j, k);
+    const double dxinv = A.sc.dxinv;
+    if (A.vc) {
+      double pc = phi[c];
+      double lofphi = A.sc.alpha * A.a[c] * pc - A.sc.beta * vcDiv(phi, A.b0, A.b1, A.b2, c, s) * dxinv;
+      phi[c] = pc - A.lam[c] * (lofphi - rhs[c]);
+    } else if (A.sc.laplacian) {
+      double lphi = nbrSum(phi, c, s) * dxinv;
+      phi[c] = A.sc.lambda * (rhs[c] - lphi);
+    } else {
+      double pc = phi[c];
+      double lphi = (nbrSum(phi, c, s) - 2.0 * 3 * pc) * dxinv;
+      double helmop = A.sc.alpha * pc + A.sc.beta * lphi;
+      phi[c] = pc + A.sc.lambda * (helmop - rhs[c]);
+    }
+  }
+  __syncthreads();
+}
+
+// levelGSRB: per colour a ghost fill then the colour update.
+__device__ void blkRelax(const BottomArgs& A, double* phi, const double* rhs, int nit) {
+  for (int it = 0; it < nit; ++it)
+    for (int color = 0; color <= 1; ++color) {
+      blkGhost(A, phi);
+      blkGsrb(A, phi, rhs, color);
+    }
+}
+
+// residual (mode 0) or applyOp (mode 1) after a ghost fill.
+__device__ void blkOp(const BottomArgs& A, double* r, double* phi, const double* rhs, int mode) {
+  blkGhost(A, phi);
+  const double dxinv = A.sc.dxinv;
+  blkCells(A.L, [&](const BoxDesc& bd, int64_t c) {
+    Strides s = strides(bd);
+    double pc = phi[c];
+    if (A.vc) {
+      double lofphi = A.sc.alpha * A.a[c] * pc - A.sc.beta * vcDiv(phi, A.b0, A.b1, A.b2, c, s) * dxinv;
+      r[c] = mode == 0 ? rhs[c] - lofphi : lofphi;
+    } else {
+      double lap = (nbrSum(phi, c, s) - 6.0 * pc) * dxinv;
+      r[c] = mode == 0 ? -(A.sc.alpha * pc) - A.sc.beta * lap + rhs[c] : A.sc.alpha * pc + A.sc.beta * lap;
+    }
+  });
+}
+
+__device__ void blkPrecond(const BottomArgs& A, double* out, const double* in) {
+  blkCells(A.L, [&](const BoxDesc&, int64_t c) { out[c] = A.vc ? in[c] * A.lam[c] : in[c] * A.mult; });
+  blkRelax(A, out, in, 2);
+}
+
+__device__ double blkDot(const BottomArgs& A, const double* x, const double* y, bool pencil) {
+  const LevelDev& L = A.L;
+  for (int b = threadIdx.x; b < L.nbox; b += blockDim.x) {
+    const BoxDesc bd = L.boxes[b];
+    double s = 0.0;
+    if (!pencil) {
+      for (int k = bd.lo[2]; k <= bd.hi[2]; ++k)
+        for (int j = bd.lo[1]; j <= bd.hi[1]; ++j)
+          for (int i = bd.lo[0]; i <= bd.hi[0]; ++i) {
+            int64_t c = cellIndex(bd, i, j, k);
+            s += x[c] * y[c];
+          }
+    } else {
+      // sumPow(p=2): per-x accumulation over pencils, then across x.
+      for (int i = bd.lo[0]; i <= bd.hi[0]; ++i) {
+        double acc = 0.0;
+        bool first = true;
+        for (int k = bd.lo[2]; k <= bd.hi[2]; ++k)
+          for (int j = bd.lo[1]; j <= bd.hi[1]; ++j) {
+            double v = x[cellIndex(bd, i, j, k)];
+            acc = first ? v * v : acc + v * v;
+            first = false;
+          }
+        s = (i == bd.lo[0]) ? acc : s + acc;
+      }
+    }
+    A.part[b] = s;
+  }
+  __syncthreads();
+  __shared__ double tot;
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int b = 0; b < L.nbox; ++b) v += A.part[b];
+    tot = v;
+  }
+  __syncthreads();
+  double r = tot;
+  __syncthreads();
+  return r;
+}
+
+__device__ double blkNorm(const BottomArgs& A, const double* x) { return sqrt(blkDot(A, x, x, true)); }
+
+__global__ void k_bottom(BottomArgs A) {
+  const LevelDev& L = A.L;
+  auto zeroAll = [&](double* x) {
+    for (int64_t q = threadIdx.x; q < L.nelem; q += blockDim.x) x[q] = 0.0;
+    __syncthreads();
+  };
+  auto copyValid = [&](double* d, const double* s) { blkCells(L, [&](const BoxDesc&, int64_t c) { d[c] = s[c]; }); };
+  auto incrV = [&](double* y, const double* x, double sc) {
+    blkCells(L, [&](const BoxDesc&, int64_t c) { y[c] = y[c] + x[c] * sc; });
+  };
+  zeroAll(A.r);
+  blkOp(A, A.r, A.phi, A.rhs, 0);
+  copyValid(A.rt, A.r);
+  zeroAll(A.e);
+  zeroAll(A.pt);
+  zeroAll(A.st);
+  int iter = 0, recount = 0, restarts = 0, status = 0;
+  double rho[4] = {0, 0, 0, 0};
+  double norm[2];
+  norm[0] = blkNorm(A, A.r);
+  double initial_norm = norm[0];
+  const double initial_residual = norm[0];
+  norm[1] = norm[0];
+  double alpha[2] = {0, 0}, beta[2] = {0, 0}, omega[2] = {0, 0};
+  bool init = true;
+  if (A.metric > 0) initial_norm = A.metric;
+  while ((iter < A.imax && norm[0] > A.eps * norm[1]) && (norm[1] > 0)) {
+    iter++;
+    norm[1] = norm[0];
+    alpha[1] = alpha[0];
+    beta[1] = beta[0];
+    omega[1] = omega[0];
+    rho[3] = rho[2];
+    rho[2] = rho[1];
+    rho[1] = blkDot(A, A.rt, A.r, false);
+    if (rho[1] == 0.0) {
+      incrV(A.phi, A.e, 1.0);
+      if (threadIdx.x == 0) A.status[0] = 2, A.status[1] = iter;
+      return;
+    }
+    if (init) {
+      copyValid(A.p, A.r);
+      init = false;
+    } else {
+      beta[1] = (rho[1] / rho[2]) * (alpha[1] / omega[1]);
+      blkCells(L, [&](const BoxDesc&, int64_t c) { A.p[c] = A.p[c] * beta[1]; });
+      incrV(A.p, A.v, -beta[1] * omega[1]);
+      incrV(A.p, A.r, 1.0);
+    }
+    blkPrecond(A, A.pt, A.p);
+    zeroAll(A.v);
+    blkOp(A, A.v, A.pt, nullptr, 1);
+    double m = blkDot(A, A.rt, A.v, false);
+    alpha[0] = rho[1] / m;
+    if (fabs(m) > A.small * fabs(rho[1])) {
+      incrV(A.r, A.v, -alpha[0]);
+      norm[0] = blkNorm(A, A.r);
+      incrV(A.e, A.pt, alpha[0]);
+    } else {
+      zeroAll(A.r);
+      norm[0] = 0.0;
+    }
+    if (norm[0] > A.eps * initial_norm && norm[0] > A.reps * initial_residual) {
+      blkPrecond(A, A.st, A.r);
+      zeroAll(A.t);
+      blkOp(A, A.t, A.st, nullptr, 1);
+      double tr = blkDot(A, A.t, A.r, false);
+      double tt = blkDot(A, A.t, A.t, false);
+      omega[0] = tr / tt;
+      incrV(A.e, A.st, omega[0]);
+      incrV(A.r, A.t, -omega[0]);
+      norm[0] = blkNorm(A, A.r);
+    }
+    if (norm[0] <= A.eps * initial_norm || norm[0] <= A.reps * initial_residual) {
+      status = 1;
+      break;
+    }
+    if (omega[0] == 0.0 || norm[0] > (1 - A.hang) * norm[1]) {
+      if (recount == 0) {
+        recount = 1;
+      } else {
+        recount = 0;
+        incrV(A.phi, A.e, 1.0);
+        if (restarts == A.numRestarts) {
+          if (threadIdx.x == 0) A.status[0] = 3, A.status[1] = iter;
+          return;
+        }
+        blkOp(A, A.r, A.phi, A.rhs, 0);
+        norm[0] = blkNorm(A, A.r);
+        rho[1] = 0.0;
+        rho[2] = 0.0;
+        rho[3] = 0.0;
+        alpha[0] = 0;
+        beta[0] = 0;
+        omega[0] = 0;
+        copyValid(A.rt, A.r);
+        zeroAll(A.e);
+        restarts++;
+        init = true;
+      }
+    }
+  }
+  incrV(A.phi, A.e, 1.0);
+  if (threadIdx.x == 0) A.status[0] = status, A.status[1] = iter;
+}
+
+}  // namespace
+
+}  // namespace cmg
+
+namespace cmg {
+
+namespace {
+
+Scal scalars(double dx, double alpha, double beta, int vc) {
+  Scal s;
+  s.dxinv = 1.0 / (dx * dx);
+  double sum_b = 0.0;
+  for (int d = 0; d < 3; ++d) sum_b = sum_b + 2.0 * s.dxinv;
+  s.alpha = alpha;
+  s.beta = beta;
+  s.laplacian = (!vc && alpha == 0.0 && beta == 1.0) ? 1 : 0;
+  s.lambda = s.laplacian ? -1.0 / sum_b : -1.0 / (alpha - beta * sum_b);
+  return s;
+}
+
+}  // namespace
+
+template <class T>
+void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s) {
+  int n = withCF ? L.nGhost : L.nExchBC;
+  if (n == 0) return;
+  const double dx = L.dx, dxc = L.dxCrse;
+  T c1 = T(2 * (dxc - dx) / (dxc + dx));
+  T c2 = T(-(dxc - dx) / (dxc + 3 * dx));
+  T flin = T(1 - 2 * dx / (dx + dxc));
+  k_ghost<T><<<n, 128, 0, s>>>(L.boxes, L.ghost, f, c1, c2, flin);
+  CMG_LAUNCHED("ghostFill");
+}
+
+template <class T>
+void zeroCovered(const LevelDev& L, T* f, cudaStream_t s) {
+  if (L.nZero == 0) return;
+  k_ghost<T><<<L.nZero, 128, 0, s>>>(L.boxes, L.zero, f, T(0), T(0), T(0));
+  CMG_LAUNCHED("zeroCovered");
+}
+
+template <class T>
+void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s) {
+  int n = L.nColor[color];
+  if (n == 0) return;
+  Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
+  if (c.vc)
+    k_gsrb<T, 1><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, c.a, c.b[0], c.b[1], c.b[2],
+                                     c.lambda);
+  else
+    k_gsrb<T, 0><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, nullptr, nullptr, nullptr,
+                                     nullptr, nullptr);
+  CMG_LAUNCHED("gsrb");
+}
+
+template <class T>
+void residual(const LevelDev& L, T* r, const T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s) {
+  if (L.nAll == 0) return;
+  Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
+  if (c.vc)
+    k_op<T, 1, 0><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, r, phi, rhs, sc, c.a, c.b[0], c.b[1], c.b[2]);
+  else
+    k_op<T, 0, 0><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, r, phi, rhs, sc, nullptr, nullptr, nullptr, nullptr);
+  CMG_LAUNCHED("residual");
+}
+
+template <class T>
+void applyOp(const LevelDev& L, T* lofphi, const T* phi, const Coef<T>& c, cudaStream_t s) {
+  if (L.nAll == 0) return;
+  Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
+  if (c.vc)
+    k_op<T, 1, 1><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lofphi, phi, nullptr, sc, c.a, c.b[0], c.b[1], c.b[2]);
+  else
+    k_op<T, 0, 1><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lofphi, phi, nullptr, sc, nullptr, nullptr, nullptr,
+                                           nullptr);
+  CMG_LAUNCHED("applyOp");
+}
+
+template <class T>
+void negAdd(const LevelDev& L, T* r, const T* lofphi, const T* rhs, cudaStream_t s) {
+  if (L.nAll == 0) return;
+  k_negadd<T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, r, lofphi, rhs);
+  CMG_LAUNCHED("negAdd");
+}
+
+template <class T>
+void restrictMG(const LevelDev& F, const LevelDev& C, T* resC, const T* phi, const T* rhs, const Coef<T>& c,
+                cudaStream_t s) {
+  if (C.nAll == 0) return;
+  Scal sc = scalars(F.dx, c.alpha, c.beta, c.vc);
+  if (c.vc)
+    k_restrictmg<T, 1><<<C.nAll, CHUNK, 0, s>>>(F.boxes, C.boxes, C.chAll, resC, phi, rhs, sc, c.a, c.b[0], c.b[1],
+                                                c.b[2]);
+  else
+    k_restrictmg<T, 0><<<C.nAll, CHUNK, 0, s>>>(F.boxes, C.boxes, C.chAll, resC, phi, rhs, sc, nullptr, nullptr,
+                                                nullptr, nullptr);
+  CMG_LAUNCHED("restrictMG");
+}
+
+template <class T>
+void prolongMG(const LevelDev& F, const LevelDev& C, T* phi, const T* corrC, cudaStream_t s) {
+  if (F.nAll == 0) return;
+  k_prolongmg<T><<<F.nAll, CHUNK, 0, s>>>(F.boxes, C.boxes, F.chAll, phi, corrC);
+  CMG_LAUNCHED("prolongMG");
+}
+
+template <class T>
+void averageAMR(const LevelDev& F, const LevelDev& C, T* coarse, const T* fine, cudaStream_t s) {
+  if (F.nItemChC == 0) return;
+  k_average<T><<<F.nItemChC, CHUNK, 0, s>>>(F.boxes, C.boxes, F.items, F.itemChC, coarse, fine);
+  CMG_LAUNCHED("averageAMR");
+}
+
+template <class T>
+void prolongAMR(const LevelDev& F, const LevelDev& C, T* fine, const T* coarse, cudaStream_t s) {
+  if (F.nItemChF == 0) return;
+  k_prolongamr<T><<<F.nItemChF, CHUNK, 0, s>>>(F.boxes, C.boxes, F.items, F.itemChF, fine, coarse);
+  CMG_LAUNCHED("prolongAMR");
+}
+
+template <class T>
+void quadCF(const LevelDev& F, T* phiF, const T* phiC, cudaStream_t s) {
+  if (F.nCfF == 0) return;
+  int nb = (F.nCfF + 127) / 128;
+  k_quadcf<T><<<nb, 128, 0, s>>>(F.cfF, F.nCfF, F.cfC, F.cfW, F.cfOff, phiF, phiC, T(F.dx));
+  CMG_LAUNCHED("quadCF");
+}
+
+template <class T>
+void reflux(const LevelDev& C, T* lofphiC, const T* phiC, const T* phiF, const Coef<T>& cc, const Coef<T>& cf,
+            cudaStream_t s) {
+  if (C.nRf == 0) return;
+  int nb = (C.nRf + 127) / 128;
+  // getFlux scale beta * ref / dx with the coarse dx (AMRPoissonOp.cpp:1797-1851).
+  T sc = T(cc.beta * 1 / C.dx);
+  T sf = T(cc.beta * 2 / C.dx);
+  T negs = T(-(1.0 / C.dx));
+  if (cc.vc)
+    k_reflux<T, 1><<<nb, 128, 0, s>>>(C.rfCells, C.nRf, C.rfC, C.rfF, lofphiC, phiC, phiF, cc.b[0], cc.b[1],
+                                      cc.b[2], cf.b[0], cf.b[1], cf.b[2], sc, sf, negs);
+  else
+    k_reflux<T, 0><<<nb, 128, 0, s>>>(C.rfCells, C.nRf, C.rfC, C.rfF, lofphiC, phiC, phiF, nullptr, nullptr,
+                                      nullptr, nullptr, nullptr, nullptr, sc, sf, negs);
+  CMG_LAUNCHED("reflux");
+}
+
+template <class T>
+void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s) {
+  if (L.nAll == 0) return;
+  k_incr<T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lhs, x, T(scale));
+  CMG_LAUNCHED("incr");
+}
+
+template <class T>
+void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s) {
+  if (L.nAll == 0) return;
+  k_maxnorm<T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, f, out);
+  CMG_LAUNCHED("maxNorm");
+}
+
+
+long long launchCount() { return g_launches.load(std::memory_order_relaxed); }
+
+void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
+                 double eps, double metric, cudaStream_t s) {
+  BottomArgs A;
+  A.L = L;
+  A.sc = scalars(L.dx, c.alpha, c.beta, c.vc);
+  A.vc = c.vc;
+  A.a = c.a;
+  A.b0 = c.b[0];
+  A.b1 = c.b[1];
+  A.b2 = c.b[2];
+  A.lam = c.lambda;
+  A.phi = phi;
+  A.rhs = rhs;
+  A.r = w.v[0];
+  A.rt = w.v[1];
+  A.e = w.v[2];
+  A.p = w.v[3];
+  A.pt = w.v[4];
+  A.st = w.v[5];
+  A.t = w.v[6];
+  A.v = w.v[7];
+  A.part = w.part;
+  A.eps = eps;
+  A.metric = metric;
+  A.reps = 1.0e-12;
+  A.hang = 1e-8;
+  A.small = 1.0e-30;
+  A.imax = 80;
+  A.numRestarts = 5;
+  // AMRPoissonOp::preCond multiplier (AMRPoissonOp.cpp:304-329).
+  A.mult = 1.0 / (c.alpha - 2.0 * 3 * c.beta / (L.dx * L.dx));
+  A.status = w.status;
+  k_bottom<<<1, 1024, 0, s>>>(A);
+  CMG_LAUNCHED("bottomSolve");
+}
+
+#define CMG_INST(T)                                                                                       \
+  template void ghostFill<T>(const LevelDev&, T*, bool, cudaStream_t);                                     \
+  template void zeroCovered<T>(const LevelDev&, T*, cudaStream_t);                                         \
+  template void gsrb<T>(const LevelDev&, T*, const T*, const Coef<T>&, int, cudaStream_t);                 \
+  template void residual<T>(const LevelDev&, T*, const T*, const T*, const Coef<T>&, cudaStream_t);        \
+  template void applyOp<T>(const LevelDev&, T*, const T*, const Coef<T>&, cudaStream_t);                   \
+  template void negAdd<T>(const LevelDev&, T*, const T*, const T*, cudaStream_t);                          \
+  template void restrictMG<T>(const LevelDev&, const LevelDev&, T*, const T*, const T*, const Coef<T>&,    \
+                              cudaStream_t);                                                               \
+  template void prolongMG<T>(const LevelDev&, const LevelDev&, T*, const T*, cudaStream_t);                \
+  template void averageAMR<T>(const LevelDev&, const LevelDev&, T*, const T*, cudaStream_t);               \
+  template void prolongAMR<T>(const LevelDev&, const LevelDev&, T*, const T*, cudaStream_t);               \
+  template void quadCF<T>(const LevelDev&, T*, const T*, cudaStream_t);                                    \
+  template void reflux<T>(const LevelDev&, T*, const T*, const T*, const Coef<T>&, const Coef<T>&,         \
+                          cudaStream_t);                                                                   \
+  template void incr<T>(const LevelDev&, T*, const T*, double, cudaStream_t);                              \
+  template void maxNorm<T>(const LevelDev&, const T*, double*, cudaStream_t);
+
+CMG_INST(double)
+CMG_INST(float)
+
+}  // namespace cmg

@@ -1,0 +1,64 @@
+// Host-side plans for one hierarchy: per-level box tables, ghost work lists,
+// red-black work chunks, coarse-fine interpolation stencils, flux-register
+// correction lists and coarse-fine box maps.  Everything here is built once
+// per hierarchy shape and uploaded; the V-cycle only reads it.
+#ifndef CMG_PLAN_H
+#define CMG_PLAN_H
+
+#include <vector>
+
+#include "devtypes.H"
+#include "geom.H"
+
+namespace cmg {
+
+enum { CHUNK = 256 };
+
+struct LevelPlan {
+  Layout grids;
+  Box domain;
+  double dx = 0, dxCrse = 0;   // dxCrse: spacing of the coarser AMR level (2 dx)
+  std::vector<BoxDesc> boxes;
+  int64_t nelem = 0;           // elements per field on this level
+  // Ghost work: [0, nExchBC) exchange + physical BC, then homogeneous CF.
+  std::vector<GhostTask> ghost;
+  int nExchBC = 0;
+  std::vector<GhostTask> zeroCovered;  // covered by the next finer level
+  std::vector<Chunk> chunksAll, chunksColor[2];
+  // Coarse-fine interpolation from the next coarser level (levels >= 1).
+  std::vector<CFCoarse> cfCoarse;
+  std::vector<CFFine> cfFine;
+  std::vector<double> cfW;
+  std::vector<int64_t> cfOff;
+  // Maps to the next coarser level (levels >= 1): items in coarse index space.
+  std::vector<CoarseFineItem> toCoarse;
+  std::vector<Chunk> toCoarseChunksF;  // chunks over fine cells of items
+  std::vector<Chunk> toCoarseChunksC;  // chunks over coarse cells of items
+  // Flux-register correction of this level from the next finer level.
+  std::vector<RefluxCell> rfCells;
+  std::vector<RefluxCoarseTerm> rfCoarse;
+  std::vector<RefluxFineGroup> rfFine;
+};
+
+// Layout and ghost/chunk plans of one level (AMR level or multigrid depth).
+// dxCrse > 0 enables homogeneous coarse-fine ghost tasks on CF faces.
+void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse);
+// Coarse-fine interpolation tables of fine level F from coarse level C.
+void buildQuadCF(LevelPlan& F, const LevelPlan& C);
+// Coarse/fine box maps and zero-covered tasks (F fine, C coarse).
+void buildCoarseFine(LevelPlan& F, LevelPlan& C);
+// Flux-register lists for coarse level C with finer level F.  vc selects the
+// variable-coefficient flux (face coefficients are then addressed).
+void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc);
+
+// Cell index of (i,j,k) inside box b of level L.
+inline int64_t cellOf(const LevelPlan& L, int b, const IV& p) {
+  return cellIndex(L.boxes[b], p[0], p[1], p[2]);
+}
+
+// Finds the box of L containing p, or -1.
+int ownerOf(const LevelPlan& L, const IV& p);
+
+}  // namespace cmg
+
+#endif

@@ -1,0 +1,537 @@
+// Plan construction.  Each builder cites the reference code whose data it
+// reproduces; the kernels then apply these tables without any geometry logic.
+#include "plan.H"
+
+#include <map>
+#include <stdexcept>
+
+namespace cmg {
+
+namespace {
+
+void chunkCounts(std::vector<Chunk>& out, int box, int64_t n) {
+  for (int64_t s = 0; s < n; s += CHUNK) out.push_back(Chunk{box, (int)s});
+}
+
+// Fine cell set on the face (d, side) of box b: the ghost layer inside the
+// domain minus every box of the level (CFIVS / CFStencil definitions,
+// AMRTools/CFIVS.cpp:330-390, AMRTools/CFStencil.cpp:240-326).
+bool faceCFSet(const LevelPlan& L, const Box& b, int d, int side, CellSet& out) {
+  Box edge = b.adjCell(d, side, 1) & L.domain;
+  if (edge.empty()) return false;
+  out.define(edge, true);
+  for (size_t k = 0; k < L.grids.size(); ++k)
+    if (L.grids[k].intersects(edge)) out.subtract(L.grids[k]);
+  return !out.empty();
+}
+
+}  // namespace
+
+void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse) {
+  L.grids = grids;
+  L.domain = domain;
+  L.dx = dx;
+  L.dxCrse = dxCrse;
+  L.boxes.clear();
+  int64_t off = 0;
+  for (size_t b = 0; b < grids.size(); ++b) {
+    const Box& bx = grids[b];
+    BoxDesc d;
+    for (int k = 0; k < 3; ++k) {
+      d.lo[k] = bx.lo[k];
+      d.hi[k] = bx.hi[k];
+    }
+    d.px = ((bx.size(0) + 2 + XOFF) + 3) / 4 * 4;
+    d.py = bx.size(1) + 2;
+    d.off = off;
+    off += (int64_t)d.px * d.py * (bx.size(2) + 2);
+    L.boxes.push_back(d);
+  }
+  L.nelem = off;
+
+  // Exchange items (Copier::exchangeDefine + trimEdges) and homogeneous
+  // Dirichlet faces (the driver's BC function: face ghosts outside the domain).
+  L.ghost.clear();
+  for (const Motion& m : exchangePlan(grids)) {
+    GhostTask t{G_COPY, m.to, m.from, 0, 0, {}, {}};
+    for (int k = 0; k < 3; ++k) {
+      t.lo[k] = m.toRegion.lo[k];
+      t.hi[k] = m.toRegion.hi[k];
+    }
+    L.ghost.push_back(t);
+  }
+  for (size_t b = 0; b < grids.size(); ++b) {
+    if (domain.contains(grids[b].grow(1))) continue;
+    for (int d = 0; d < 3; ++d)
+      for (int side = -1; side <= 1; side += 2) {
+        Box g = grids[b].adjCell(d, side, 1);
+        if (domain.contains(g)) continue;
+        GhostTask t{G_BC, (int)b, (int)b, d, side, {}, {}};
+        for (int k = 0; k < 3; ++k) {
+          t.lo[k] = g.lo[k];
+          t.hi[k] = g.hi[k];
+        }
+        L.ghost.push_back(t);
+      }
+  }
+  L.nExchBC = (int)L.ghost.size();
+  // Homogeneous coarse-fine faces (AMRPoissonOp::homogeneousCFInterp,
+  // AMRElliptic/AMRPoissonOp.cpp:1598-1671).  A packed face is one box; an
+  // unpacked face is emitted cell by cell with the same formula.
+  if (dxCrse > 0) {
+    for (size_t b = 0; b < grids.size(); ++b)
+      for (int d = 0; d < 3; ++d)
+        for (int side = -1; side <= 1; side += 2) {
+          CellSet s;
+          if (!faceCFSet(L, grids[b], d, side, s)) continue;
+          int kind = (grids[b].size(d) == 1) ? G_CFLIN : G_CFQUAD;
+          Box mb = s.minBox();
+          std::vector<Box> regions;
+          if (mb.numPts() == s.numPts())
+            regions.push_back(mb);
+          else
+            for (const IV& p : s.cells()) regions.push_back(Box(p, p));
+          for (const Box& r : regions) {
+            GhostTask t{kind, (int)b, (int)b, d, side, {}, {}};
+            for (int k = 0; k < 3; ++k) {
+              t.lo[k] = r.lo[k];
+              t.hi[k] = r.hi[k];
+            }
+            L.ghost.push_back(t);
+          }
+        }
+  }
+
+  L.chunksAll.clear();
+  L.chunksColor[0].clear();
+  L.chunksColor[1].clear();
+  for (size_t b = 0; b < grids.size(); ++b) {
+    const Box& bx = grids[b];
+    chunkCounts(L.chunksAll, (int)b, bx.numPts());
+    int64_t rows = (int64_t)bx.size(1) * bx.size(2);
+    int64_t half = (bx.size(0) + 1) / 2;
+    chunkCounts(L.chunksColor[0], (int)b, rows * half);
+    chunkCounts(L.chunksColor[1], (int)b, rows * half);
+  }
+}
+
+int ownerOf(const LevelPlan& L, const IV& p) {
+  for (size_t b = 0; b < L.grids.size(); ++b) {
+    const Box& bx = L.grids[b];
+    if (bx.lo[0] > p[0]) break;
+    if (bx.contains(p)) return (int)b;
+  }
+  return -1;
+}
+
+// Cell -> box lookup through a bucket grid whose bucket edge is the largest
+// power of two (<= 16) that every box corner is aligned to, so each bucket
+// lies in at most one box.
+struct OwnerIndex {
+  const LevelPlan* L;
+  int B = 1;
+  IV org, n;
+  std::vector<int> own;
+  explicit OwnerIndex(const LevelPlan& lp) : L(&lp) {
+    B = 16;
+    for (const Box& b : lp.grids.boxes)
+      for (int d = 0; d < 3; ++d)
+        while (B > 1 && ((b.lo[d] % B) != 0 || ((b.hi[d] + 1) % B) != 0)) B /= 2;
+    Box dom = lp.domain;
+    for (int d = 0; d < 3; ++d) {
+      org[d] = floordiv(dom.lo[d], B);
+      n[d] = floordiv(dom.hi[d], B) - org[d] + 1;
+    }
+    own.assign((size_t)n[0] * n[1] * n[2], -1);
+    for (size_t k = 0; k < lp.grids.size(); ++k) {
+      Box c = lp.grids[k].coarsen(B);
+      for (int z = c.lo[2]; z <= c.hi[2]; ++z)
+        for (int y = c.lo[1]; y <= c.hi[1]; ++y)
+          for (int x = c.lo[0]; x <= c.hi[0]; ++x) own[slot(IV(x, y, z))] = (int)k;
+    }
+  }
+  size_t slot(const IV& q) const {
+    return (size_t)(q[0] - org[0]) + (size_t)n[0] * ((size_t)(q[1] - org[1]) + (size_t)n[1] * (q[2] - org[2]));
+  }
+  int find(const IV& p) const {
+    IV q(floordiv(p[0], B), floordiv(p[1], B), floordiv(p[2], B));
+    for (int d = 0; d < 3; ++d)
+      if (q[d] < org[d] || q[d] >= org[d] + n[d]) return -1;
+    return own[slot(q)];
+  }
+  int64_t cell(const IV& p) const {
+    int b = find(p);
+    if (b < 0) throw std::runtime_error("cmg: coarse cell outside the coarse level");
+    return cellOf(*L, b, p);
+  }
+};
+
+}  // namespace cmg
+
+namespace cmg {
+
+namespace {
+
+// Merged (cell, weight) list with the reference's accumulate semantics
+// (AMRTools/DerivStencil.cpp:79-105: equal cells add their weights).
+struct Sten {
+  bool defined = false;
+  std::vector<IV> iv;
+  std::vector<double> w;
+  void acc(const IV& p, double wt) {
+    defined = true;
+    for (size_t i = 0; i < iv.size(); ++i)
+      if (iv[i] == p) {
+        w[i] += wt;
+        return;
+      }
+    iv.push_back(p);
+    w.push_back(wt);
+  }
+};
+
+struct CoarseStencils {
+  bool drop = false;
+  Sten mixed, first[2], second[2];
+};
+
+// QuadCFStencil::buildStencils (AMRTools/QuadCFStencil.cpp:662-920) for one
+// irregular coarse cell.  t[0] < t[1] are the tangential directions.
+void buildIrregular(const IV& iv, const int t[2], const CellSet& good, CoarseStencils& cs) {
+  // Mixed derivative: average of the one-sided 2x2 quadrant stencils that lie
+  // in the good set, tested in the reference's order.  Each quadrant with low
+  // corner L carries -1 at L and L+e1+e2, +1 at L+e1 and L+e2.
+  const IV e1 = IV::basis(t[0]), e2 = IV::basis(t[1]);
+  const IV los[4] = {iv - e1, iv, iv - e2, iv - e1 - e2};
+  int nmixed = 0;
+  for (int q = 0; q < 4; ++q) {
+    Box qb(los[q], los[q] + e1 + e2);
+    if (!good.containsBox(qb)) continue;
+    ++nmixed;
+    for (int a2 = 0; a2 < 2; ++a2)
+      for (int a1 = 0; a1 < 2; ++a1) {
+        IV p = los[q];
+        p[t[0]] += a1;
+        p[t[1]] += a2;
+        cs.mixed.acc(p, (a1 == a2) ? -1.0 : 1.0);
+      }
+  }
+  if (nmixed > 0) {
+    double rn = nmixed;
+    for (double& w : cs.mixed.w) w /= rn;
+  }
+  cs.drop = (nmixed == 0);
+}
+
+void buildIrregularDir(const IV& iv, int ivec, int dir, const CellSet& good, CoarseStencils& cs) {
+  if (cs.drop) return;
+  const IV e = IV::basis(dir);
+  Box bsten = Box(iv, iv).grow(dir, 1);
+  Sten& s2 = cs.second[ivec];
+  Sten& s1 = cs.first[ivec];
+  if (good.containsBox(bsten)) {
+    s2.acc(iv - e, 1.0);
+    s2.acc(iv, -2.0);
+    s2.acc(iv + e, 1.0);
+    s1.acc(iv - e, -0.5);
+    s1.acc(iv, 0.0);
+    s1.acc(iv + e, 0.5);
+    return;
+  }
+  Box bshift = bsten.shift(dir, 1);
+  if (good.containsBox(bshift)) {
+    s2.acc(iv, 1.0);
+    s2.acc(iv + e, -2.0);
+    s2.acc(iv + e + e, 1.0);
+    s1.acc(iv, -3.0 / 2.0);
+    s1.acc(iv + e, 4.0 / 2.0);
+    s1.acc(iv + e + e, -1.0 / 2.0);
+    return;
+  }
+  bshift = bshift.shift(dir, -2);
+  if (good.containsBox(bshift)) {
+    s2.acc(iv - e - e, 1.0);
+    s2.acc(iv - e, -2.0);
+    s2.acc(iv, 1.0);
+    s1.acc(iv - e - e, 1.0 / 2.0);
+    s1.acc(iv - e, -4.0 / 2.0);
+    s1.acc(iv, 3.0 / 2.0);
+    return;
+  }
+  cs.drop = true;
+  if (good.contains(iv + e)) {
+    s1.acc(iv, -1.0);
+    s1.acc(iv + e, 1.0);
+  } else if (good.contains(iv - e)) {
+    s1.acc(iv - e, -1.0);
+    s1.acc(iv, 1.0);
+  } else {
+    s1.acc(iv, 0.0);
+  }
+}
+
+}  // namespace
+
+void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
+  F.cfCoarse.clear();
+  F.cfFine.clear();
+  F.cfW.clear();
+  F.cfOff.clear();
+  OwnerIndex owner(C);
+  Layout cfine = F.grids.coarsen(2);
+  const double dxf = F.dx;
+  const double dxc = 2 * dxf;
+  auto pushPool = [&](const std::vector<IV>& cells, const std::vector<double>* w) {
+    int start = (int)F.cfOff.size();
+    for (size_t i = 0; i < cells.size(); ++i) {
+      F.cfOff.push_back(owner.cell(cells[i]));
+      F.cfW.push_back(w ? (*w)[i] : 0.0);
+    }
+    return start;
+  };
+  for (size_t fb = 0; fb < F.grids.size(); ++fb) {
+    const Box& fbox = F.grids[fb];
+    for (int d = 0; d < 3; ++d) {
+      int t[2], it = 0;
+      for (int k = 0; k < 3; ++k)
+        if (k != d) t[it++] = k;
+      for (int side = -1; side <= 1; side += 2) {
+        CellSet fineIVS;
+        if (!faceCFSet(F, fbox, d, side, fineIVS)) continue;
+        Box packedBox = fineIVS.minBox();
+        bool packed = (packedBox.numPts() == fineIVS.numPts());
+        CellSet base = fineIVS.coarsen(2);
+        base.intersect(C.domain);
+        // Good set: coarse cells of the widened face slab that are valid on
+        // the coarse level and not under the fine level
+        // (QuadCFStencil::define, AMRTools/QuadCFStencil.cpp:500-660).
+        Box cgrid = fbox.coarsen(2);
+        Box g2 = cgrid.adjCell(d, side, 1), g1 = g2;
+        for (int k = 0; k < 2; ++k) {
+          g2 = g2.grow(t[k], 2);
+          g1 = g1.grow(t[k], 1);
+        }
+        g2 = g2 & C.domain;
+        g1 = g1 & C.domain;
+        CellSet good(g2, false);
+        for (const Box& cb : C.grids.boxes)
+          if (cb.intersects(g2)) good.set(cb, true);
+        for (const Box& fc : cfine.boxes)
+          if (fc.intersects(g2)) good.subtract(fc);
+        CellSet standard = good;
+        standard.intersect(g1);
+        standard = standard.erode(t[0]).erode(t[1]);
+        // Irregular stencils for base cells outside the standard set.
+        std::map<std::vector<int>, int> coarseIndex;
+        std::vector<IV> baseCells = base.cells();
+        std::vector<CoarseStencils> irr(baseCells.size());
+        for (size_t i = 0; i < baseCells.size(); ++i)
+          if (!standard.contains(baseCells[i])) buildIrregular(baseCells[i], t, good, irr[i]);
+        for (int ivec = 0; ivec < 2; ++ivec)
+          for (size_t i = 0; i < baseCells.size(); ++i)
+            if (!standard.contains(baseCells[i])) buildIrregularDir(baseCells[i], ivec, t[ivec], good, irr[i]);
+        for (size_t i = 0; i < baseCells.size(); ++i) {
+          const IV& c = baseCells[i];
+          CFCoarse e;
+          e.cc = owner.cell(c);
+          if (standard.contains(c)) {
+            for (int k = 0; k < 2; ++k) {
+              IV ek = IV::basis(t[k]);
+              e.d1[k] = CFDeriv{1, 2, pushPool({c - ek, c + ek}, nullptr)};
+              e.d2[k] = CFDeriv{1, 3, pushPool({c - ek, c + ek, c}, nullptr)};
+            }
+            // computeMixedDerivative: basex = e(t[0]), basey = e(t[1]).
+            IV bx = IV::basis(t[0]), by = IV::basis(t[1]);
+            e.mx = CFDeriv{1, 4, pushPool({c + bx + by, c - bx + by, c + bx - by, c - bx - by}, nullptr)};
+          } else {
+            const CoarseStencils& cs = irr[i];
+            for (int k = 0; k < 2; ++k) {
+              e.d1[k] = CFDeriv{2, (int)cs.first[k].iv.size(), pushPool(cs.first[k].iv, &cs.first[k].w)};
+              if (cs.drop)
+                e.d2[k] = CFDeriv{0, 0, 0};
+              else
+                e.d2[k] = CFDeriv{2, (int)cs.second[k].iv.size(), pushPool(cs.second[k].iv, &cs.second[k].w)};
+            }
+            if (cs.drop)
+              e.mx = CFDeriv{0, 0, 0};
+            else
+              e.mx = CFDeriv{2, (int)cs.mixed.iv.size(), pushPool(cs.mixed.iv, &cs.mixed.w)};
+          }
+          coarseIndex[{c[0], c[1], c[2]}] = (int)F.cfCoarse.size();
+          F.cfCoarse.push_back(e);
+        }
+        // Fine ghost cells.  Packed faces follow the Fortran PHISTAR index
+        // shift (QuadCFInterp.cpp:680-712, QuadCFInterpF.ChF:50-126).
+        IV shift = packedBox.lo;
+        shift[d] += side;
+        for (const IV& f : fineIVS.cells()) {
+          IV c(floordiv(f[0], 2), floordiv(f[1], 2), floordiv(f[2], 2));
+          CFFine ff;
+          ff.g = cellOf(F, (int)fb, f);
+          ff.pb = cellOf(F, (int)fb, f - IV::basis(d, side));
+          ff.pa = cellOf(F, (int)fb, f - IV::basis(d, 2 * side));
+          ff.coarse = coarseIndex.at({c[0], c[1], c[2]});
+          ff.packed = packed ? 1 : 0;
+          double xs[2];
+          for (int k = 0; k < 2; ++k) {
+            int you = t[k];
+            if (packed) {
+              int ir = f[you] - shift[you];
+              int ic = ir / 2;
+              double xf = (ir + 0.5) * dxf;
+              double xc = (ic + 0.5) * dxc;
+              xs[k] = xf - xc;
+            } else {
+              double xf = (f[you] + 0.5) * dxf;
+              double xc = (c[you] + 0.5) * dxc;
+              xs[k] = xf - xc;
+            }
+          }
+          ff.x1 = xs[0];
+          ff.x2 = xs[1];
+          F.cfFine.push_back(ff);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace cmg
+
+namespace cmg {
+
+void buildCoarseFine(LevelPlan& F, LevelPlan& C) {
+  // Copier from the coarsened fine layout to the coarse layout
+  // (AMRPoissonOp::buildCopier, AMRElliptic/AMRPoissonOp.cpp:474-483); the
+  // same items drive restriction, prolongation and zeroCovered.
+  Layout cfine = F.grids.coarsen(2);
+  F.toCoarse.clear();
+  F.toCoarseChunksC.clear();
+  F.toCoarseChunksF.clear();
+  C.zeroCovered.clear();
+  for (const Motion& m : copyPlan(cfine, C.grids)) {
+    CoarseFineItem it;
+    it.cbox = m.to;
+    it.fbox = m.from;
+    for (int k = 0; k < 3; ++k) {
+      it.lo[k] = m.toRegion.lo[k];
+      it.hi[k] = m.toRegion.hi[k];
+    }
+    int idx = (int)F.toCoarse.size();
+    F.toCoarse.push_back(it);
+    chunkCounts(F.toCoarseChunksC, idx, m.toRegion.numPts());
+    chunkCounts(F.toCoarseChunksF, idx, 8 * m.toRegion.numPts());
+    GhostTask z{G_ZERO, m.to, m.to, 0, 0, {}, {}};
+    for (int k = 0; k < 3; ++k) {
+      z.lo[k] = m.toRegion.lo[k];
+      z.hi[k] = m.toRegion.hi[k];
+    }
+    C.zeroCovered.push_back(z);
+  }
+}
+
+void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
+  // LevelFluxRegister::define / incrementCoarse / incrementFine / reflux
+  // (AMRTools/LevelFluxRegister.cpp:101-262, 372-586, 649-670) reduced to the
+  // uncovered coarse cells they change, with every addition kept in the
+  // reference's order.
+  C.rfCells.clear();
+  C.rfCoarse.clear();
+  C.rfFine.clear();
+  Layout cfine = F.grids.coarsen(2);
+  OwnerIndex fineOwner(F);
+  (void)fineOwner;
+  auto covered = [&](const IV& c) {
+    for (const Box& b : cfine.boxes)
+      if (b.contains(c)) return true;
+    return false;
+  };
+  for (size_t cb = 0; cb < C.grids.size(); ++cb) {
+    const Box& cbox = C.grids[cb];
+    // Per coarse cell of this box: its coarse terms and fine groups.
+    std::map<std::vector<int>, std::pair<std::vector<RefluxCoarseTerm>, std::vector<RefluxFineGroup>>> acc;
+    std::vector<std::vector<int>> order;
+    auto slot = [&](const IV& c) -> std::pair<std::vector<RefluxCoarseTerm>, std::vector<RefluxFineGroup>>& {
+      std::vector<int> key{c[0], c[1], c[2]};
+      auto it = acc.find(key);
+      if (it == acc.end()) {
+        order.push_back(key);
+        return acc[key];
+      }
+      return it->second;
+    };
+    // Coarse terms, in incrementCoarse order: direction, then low/high side.
+    for (int d = 0; d < 3; ++d)
+      for (int side = -1; side <= 1; side += 2)
+        for (size_t f = 0; f < cfine.size(); ++f) {
+          Box loc = cfine[f].adjCell(d, side, 1) & cbox;
+          if (loc.empty()) continue;
+          for (int k = loc.lo[2]; k <= loc.hi[2]; ++k)
+            for (int j = loc.lo[1]; j <= loc.hi[1]; ++j)
+              for (int i = loc.lo[0]; i <= loc.hi[0]; ++i) {
+                IV c(i, j, k);
+                if (covered(c)) continue;
+                RefluxCoarseTerm t;
+                IV e = IV::basis(d);
+                IV hi = (side < 0) ? c + e : c;
+                IV lo = (side < 0) ? c : c - e;
+                t.hi = cellOf(C, (int)cb, hi);
+                t.lo = cellOf(C, (int)cb, lo);
+                t.bface = vc ? t.hi : -1;
+                t.dir = d;
+                t.sgn = (side < 0) ? 1.0 : -1.0;
+                slot(c).first.push_back(t);
+              }
+        }
+    // Fine groups, in copyTo order: fine box index.
+    for (size_t f = 0; f < cfine.size(); ++f) {
+      const Box& fbox = F.grids[f];
+      for (int d = 0; d < 3; ++d)
+        for (int side = -1; side <= 1; side += 2) {
+          Box loc = cfine[f].adjCell(d, side, 1) & cbox;
+          if (loc.empty()) continue;
+          for (int k = loc.lo[2]; k <= loc.hi[2]; ++k)
+            for (int j = loc.lo[1]; j <= loc.hi[1]; ++j)
+              for (int i = loc.lo[0]; i <= loc.hi[0]; ++i) {
+                IV c(i, j, k);
+                if (covered(c)) continue;
+                RefluxFineGroup g;
+                g.dir = d;
+                g.scale = ((side < 0) ? -1.0 : 1.0) * 1.0 / 4.0;
+                Box ghosts = Box(c, c).refine(2) & fbox.adjCell(d, side, 1);
+                int n = 0;
+                IV e = IV::basis(d);
+                for (int z = ghosts.lo[2]; z <= ghosts.hi[2]; ++z)
+                  for (int y = ghosts.lo[1]; y <= ghosts.hi[1]; ++y)
+                    for (int x = ghosts.lo[0]; x <= ghosts.hi[0]; ++x) {
+                      IV gcell(x, y, z);
+                      IV v = gcell - IV::basis(d, side);
+                      IV hi = (side < 0) ? v : gcell;
+                      IV lo = (side < 0) ? gcell : v;
+                      (void)e;
+                      g.hi[n] = cellOf(F, (int)f, hi);
+                      g.lo[n] = cellOf(F, (int)f, lo);
+                      g.bface[n] = vc ? g.hi[n] : -1;
+                      ++n;
+                    }
+                if (n != 4) throw std::runtime_error("cmg: fine face group is not 2x2");
+                slot(c).second.push_back(g);
+              }
+        }
+    }
+    for (const auto& key : order) {
+      auto& pr = acc[key];
+      RefluxCell rc;
+      rc.c = cellOf(C, (int)cb, IV(key[0], key[1], key[2]));
+      rc.nco = (int)pr.first.size();
+      rc.nfi = (int)pr.second.size();
+      rc.start = (int)C.rfCoarse.size();
+      rc.fstart = (int)C.rfFine.size();
+      for (auto& t : pr.first) C.rfCoarse.push_back(t);
+      for (auto& g : pr.second) C.rfFine.push_back(g);
+      C.rfCells.push_back(rc);
+    }
+  }
+}
+
+}  // namespace cmg

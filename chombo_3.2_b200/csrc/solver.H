@@ -1,0 +1,154 @@
+// GPU AMR multigrid solver: the control flow of AMRMultiGrid::solve
+// (AMRElliptic/AMRMultiGrid.H:894-1124, 1341-1419) and MultiGrid::cycle
+// (AMRElliptic/MultiGrid.H:600-696) driving the device kernels, with all
+// hierarchy state resident in device memory.
+#ifndef CMG_SOLVER_H
+#define CMG_SOLVER_H
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "kernels.H"
+#include "plan.H"
+
+namespace cmg {
+
+struct HierarchyDesc {
+  Box domain;                            // level-0 domain
+  double dx0 = 1.0;                      // level-0 cell size
+  std::vector<std::vector<Box>> boxes;   // per AMR level, refinement ratio 2
+  int vc = 0;                            // 0: AMRPoissonOp, 1: VCAMRPoissonOp2
+  double alpha = 0.0, beta = 1.0;
+};
+
+struct SolveParams {
+  int pre = 4, post = 4, bottom = 4, numMG = 1, iterMax = 100, imin = 5;
+  double eps = 1e-10, hang = 1e-10, normThresh = 1e-30;
+};
+
+struct SolveResult {
+  int exitStatus = 0, iterations = 0;
+  std::vector<double> history;  // composite max-norm residual, start of each iteration, then final
+};
+
+// Device allocation owned by the solver.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() {}
+  explicit DevBuf(size_t n);
+  ~DevBuf();
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+
+class Solver {
+ public:
+  Solver(const HierarchyDesc& d, cudaStream_t stream);
+  ~Solver();
+  int numLevels() const { return (int)amr_.size(); }
+  const LevelPlan& level(int l) const { return amr_[l]; }
+  int numMGDepths() const { return (int)mg_.size(); }
+  const LevelPlan& mgLevel(int d) const { return mg_[d]; }
+  int64_t numValidCells(int l) const { return amr_[l].grids.numCells(); }
+  int64_t numFaces(int l, int dir) const;
+  // Valid-cell data in layout order, x fastest (host or device pointer).
+  void setRHS(int l, const double* src, bool onDevice);
+  void setACoef(int l, const double* src, bool onDevice);
+  void setBCoef(int l, int dir, const double* src, bool onDevice);
+  void getPhi(int l, double* dst, bool onDevice);
+  void getRHS(int l, double* dst, bool onDevice);
+  void setPhi(int l, const double* src, bool onDevice);
+  // Builds lambda and the coarsened multigrid coefficients (VC operator).
+  void finalizeCoefficients();
+  SolveResult solve(const SolveParams& p, bool zeroPhi = true);
+  // One composite residual evaluation (AMRMultiGrid::computeAMRResidual).
+  double residualNorm();
+  cudaStream_t stream() const { return s_; }
+  // Bytes moved per V-cycle by the algorithmic count (each array read once,
+  // each output written once per pass), for the roofline.
+  double vcycleBytes(const SolveParams& p) const;
+  double* devPhi(int l) { return lev_[l].phi; }
+  double* devRHS(int l) { return lev_[l].rhs; }
+
+  // Per-kernel-class device timing (CUDA events around each launch of the
+  // class, on the solver's stream) with the algorithmic bytes of each launch.
+  enum ProfClass { P_GSRB = 0, P_RESID = 1, P_OTHER = 2, P_NCLASS = 3 };
+  void profileEnable(bool on);
+  void profileRead(int cls, int64_t* launches, double* ms, double* bytes);
+
+  struct LevelFields {
+    double *phi = nullptr, *rhs = nullptr, *ures = nullptr, *ucorr = nullptr, *corr = nullptr, *res = nullptr;
+    double *a = nullptr, *b[3] = {nullptr, nullptr, nullptr}, *lambda = nullptr;
+  };
+
+ private:
+  void uploadLevel(const LevelPlan& p, LevelDev& d);
+  double* alloc(size_t n);
+  Coef<double> coefAMR(int l) const;
+  Coef<double> coefMG(int d) const;
+  void relaxAMR(int l, double* phi, const double* rhs, int n);
+  void relaxMG(int d, double* phi, const double* rhs, int n);
+  void amrResidualLevel(int ilev, int lmax, std::vector<double*>& res, std::vector<double*>& phi,
+                        std::vector<double*>& rhs);
+  double computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);
+  void amrVCycle(int ilev, int lmax);
+  void mgCycle(int depth, double* corr, double* res);
+  void zeroField(const LevelDev& L, double* f);
+  void copyField(const LevelDev& L, double* dst, const double* src);
+  void scatterValid(const LevelPlan& p, const LevelDev& d, double* dev, const double* src, bool onDevice,
+                    int faceDir);
+  void gatherValid(const LevelPlan& p, const LevelDev& d, const double* dev, double* dst, bool onDevice);
+  struct RegionPlan {
+    int n = 0;
+    int64_t total = 0;
+    const void* dev = nullptr;
+  };
+  std::map<std::pair<const void*, int>, RegionPlan> regionCache_;
+  const void* regionPlan(const LevelPlan& p, int faceDir, int* nreg, int64_t* total);
+  std::unique_ptr<DevBuf> stage_;
+  double* staging(int64_t n);
+
+  cudaStream_t s_;
+  HierarchyDesc desc_;
+  std::vector<LevelPlan> amr_;
+  std::vector<LevelPlan> mg_;        // multigrid depths below level 0; mg_[0] is depth 1
+  std::vector<LevelDev> amrDev_, mgDev_;
+  std::vector<LevelFields> lev_;
+  std::vector<LevelFields> mgf_;     // corr, res and coefficients per depth
+  std::vector<std::unique_ptr<DevBuf>> bufs_;
+  BottomWork bottom_;
+  double* dNorm_ = nullptr;
+  int64_t bottomCells_ = 0;
+  SolveParams sp_;
+  double bottomMetric_ = 0;
+  std::vector<std::vector<double>> hostA_, hostB_[3];
+
+  struct ProfRec {
+    cudaEvent_t a, b;
+    int cls;
+    double bytes;
+  };
+  bool profOn_ = false;
+  std::vector<ProfRec> prof_;
+  std::vector<cudaEvent_t> evPool_;
+  cudaEvent_t takeEvent();
+  template <class F>
+  void timed(int cls, double bytes, F f) {
+    if (!profOn_) return f();
+    ProfRec r{takeEvent(), takeEvent(), cls, bytes};
+    cudaEventRecord(r.a, s_);
+    f();
+    cudaEventRecord(r.b, s_);
+    prof_.push_back(r);
+  }
+  double profAcc_[P_NCLASS][3] = {};
+  void profileDrain();
+};
+
+}  // namespace cmg
+
+#endif

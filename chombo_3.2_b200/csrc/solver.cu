@@ -1,0 +1,696 @@
+// GPU AMR multigrid solver.  The V-cycle control flow restates
+// AMRMultiGrid::solveNoInitResid / AMRVCycle / computeAMRResidual
+// (AMRElliptic/AMRMultiGrid.H:682-1124, 1341-1419) and MultiGrid::cycle
+// (AMRElliptic/MultiGrid.H:629-696); every step below names the operator
+// method it performs.
+#include "solver.H"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+
+namespace cmg {
+
+namespace {
+
+inline void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "cmg: %s: %s", what, cudaGetErrorString(e));
+    throw std::runtime_error(buf);
+  }
+}
+
+// Valid (or face) region of box b for the user data layout.
+Box userRegion(const Box& b, int faceDir) {
+  Box r = b;
+  if (faceDir >= 0) r.hi[faceDir] += 1;
+  return r;
+}
+
+struct RegionCopy {
+  int box;
+  int lo[3], hi[3];
+  int64_t srcOff;
+};
+
+__global__ void k_scatter(const BoxDesc* boxes, const RegionCopy* rc, double* dev, const double* src, int toDev) {
+  const RegionCopy r = rc[blockIdx.x];
+  const BoxDesc b = boxes[r.box];
+  int nx = r.hi[0] - r.lo[0] + 1, ny = r.hi[1] - r.lo[1] + 1, nz = r.hi[2] - r.lo[2] + 1;
+  for (int q = threadIdx.x; q < nx * ny * nz; q += blockDim.x) {
+    int i = r.lo[0] + q % nx, t = q / nx, j = r.lo[1] + t % ny, k = r.lo[2] + t / ny;
+    int64_t c = cellIndex(b, i, j, k);
+    if (toDev)
+      dev[c] = src[r.srcOff + q];
+    else
+      const_cast<double*>(src)[r.srcOff + q] = dev[c];
+  }
+}
+
+}  // namespace
+
+DevBuf::DevBuf(size_t n) : bytes(n) { ck(cudaMalloc(&p, n ? n : 1), "cudaMalloc"); }
+DevBuf::~DevBuf() {
+  if (p) cudaFree(p);
+}
+
+double* Solver::alloc(size_t n) {
+  bufs_.emplace_back(new DevBuf(n * sizeof(double)));
+  double* p = (double*)bufs_.back()->p;
+  ck(cudaMemsetAsync(p, 0, n * sizeof(double), s_), "memset");
+  return p;
+}
+
+template <class V>
+static const typename V::value_type* upload(std::vector<std::unique_ptr<DevBuf>>& bufs, const V& v, cudaStream_t s) {
+  if (v.empty()) return nullptr;
+  size_t n = v.size() * sizeof(typename V::value_type);
+  bufs.emplace_back(new DevBuf(n));
+  ck(cudaMemcpyAsync(bufs.back()->p, v.data(), n, cudaMemcpyHostToDevice, s), "upload");
+  return (const typename V::value_type*)bufs.back()->p;
+}
+
+void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
+  d.boxes = upload(bufs_, p.boxes, s_);
+  d.nbox = (int)p.boxes.size();
+  d.nelem = p.nelem;
+  d.ghost = upload(bufs_, p.ghost, s_);
+  d.nExchBC = p.nExchBC;
+  d.nGhost = (int)p.ghost.size();
+  d.zero = upload(bufs_, p.zeroCovered, s_);
+  d.nZero = (int)p.zeroCovered.size();
+  d.chAll = upload(bufs_, p.chunksAll, s_);
+  d.nAll = (int)p.chunksAll.size();
+  for (int c = 0; c < 2; ++c) {
+    d.chColor[c] = upload(bufs_, p.chunksColor[c], s_);
+    d.nColor[c] = (int)p.chunksColor[c].size();
+  }
+  d.cfC = upload(bufs_, p.cfCoarse, s_);
+  d.cfF = upload(bufs_, p.cfFine, s_);
+  d.nCfF = (int)p.cfFine.size();
+  d.cfW = upload(bufs_, p.cfW, s_);
+  d.cfOff = upload(bufs_, p.cfOff, s_);
+  d.items = upload(bufs_, p.toCoarse, s_);
+  d.itemChC = upload(bufs_, p.toCoarseChunksC, s_);
+  d.nItemChC = (int)p.toCoarseChunksC.size();
+  d.itemChF = upload(bufs_, p.toCoarseChunksF, s_);
+  d.nItemChF = (int)p.toCoarseChunksF.size();
+  d.rfCells = upload(bufs_, p.rfCells, s_);
+  d.nRf = (int)p.rfCells.size();
+  d.rfC = upload(bufs_, p.rfCoarse, s_);
+  d.rfF = upload(bufs_, p.rfFine, s_);
+  d.dx = p.dx;
+  d.dxCrse = p.dxCrse;
+}
+
+Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), desc_(desc) {
+  const int nlev = (int)desc.boxes.size();
+  if (nlev < 1) throw std::runtime_error("cmg: hierarchy needs at least one level");
+  amr_.resize(nlev);
+  Box dom = desc.domain;
+  double dx = desc.dx0;
+  for (int l = 0; l < nlev; ++l) {
+    if (l > 0) {
+      dom = dom.refine(2);
+      dx = dx / 2;  // m_dx[i] = m_dx[i-1] / refRatio (VCAMRPoissonOp2.cpp:905-912)
+    }
+    Layout g(desc.boxes[l]);
+    buildLevel(amr_[l], g, dom, dx, l > 0 ? amr_[l - 1].dx : 0.0);
+  }
+  for (int l = 1; l < nlev; ++l) {
+    buildQuadCF(amr_[l], amr_[l - 1]);
+    buildCoarseFine(amr_[l], amr_[l - 1]);
+    buildReflux(amr_[l - 1], amr_[l], desc.vc != 0);
+  }
+  // Multigrid depths of level 0 (AMRPoissonOpFactory::MGnewOp,
+  // AMRElliptic/AMRPoissonOp.cpp:1923-1989: exists while the boxes are
+  // coarsenable by coarsening * s_maxCoarse(2)).
+  const Layout& g0 = amr_[0].grids;
+  for (int c = 2; g0.coarsenable(c * 2); c *= 2) {
+    LevelPlan L;
+    buildLevel(L, g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0);
+    mg_.push_back(L);
+  }
+  bottomCells_ = desc.domain.numPts();
+  for (size_t d = 0; d < mg_.size(); ++d) bottomCells_ /= 8;
+
+  amrDev_.resize(nlev);
+  lev_.resize(nlev);
+  for (int l = 0; l < nlev; ++l) {
+    uploadLevel(amr_[l], amrDev_[l]);
+    size_t n = amr_[l].nelem;
+    LevelFields& f = lev_[l];
+    f.phi = alloc(n);
+    f.rhs = alloc(n);
+    f.ures = alloc(n);
+    f.ucorr = alloc(n);
+    f.corr = alloc(n);
+    f.res = alloc(n);
+    if (desc.vc) {
+      f.a = alloc(n);
+      for (int d = 0; d < 3; ++d) f.b[d] = alloc(n);
+      f.lambda = alloc(n);
+    }
+  }
+  mgDev_.resize(mg_.size());
+  mgf_.resize(mg_.size());
+  for (size_t d = 0; d < mg_.size(); ++d) {
+    uploadLevel(mg_[d], mgDev_[d]);
+    size_t n = mg_[d].nelem;
+    mgf_[d].corr = alloc(n);
+    mgf_[d].res = alloc(n);
+    if (desc.vc) {
+      mgf_[d].a = alloc(n);
+      for (int k = 0; k < 3; ++k) mgf_[d].b[k] = alloc(n);
+      mgf_[d].lambda = alloc(n);
+    }
+  }
+  const LevelPlan& bl = mg_.empty() ? amr_[0] : mg_.back();
+  for (int k = 0; k < 8; ++k) bottom_.v[k] = alloc(bl.nelem);
+  bottom_.part = alloc(bl.boxes.size() + 1);
+  bufs_.emplace_back(new DevBuf(4 * sizeof(int)));
+  bottom_.status = (int*)bufs_.back()->p;
+  dNorm_ = alloc(1);
+  if (desc.vc) {
+    hostA_.resize(nlev);
+    for (int d = 0; d < 3; ++d) hostB_[d].resize(nlev);
+  }
+  ck(cudaStreamSynchronize(s_), "setup");
+}
+
+Solver::~Solver() { cudaStreamSynchronize(s_); }
+
+int64_t Solver::numFaces(int l, int dir) const {
+  int64_t n = 0;
+  for (const Box& b : amr_[l].grids.boxes) n += userRegion(b, dir).numPts();
+  return n;
+}
+
+const void* Solver::regionPlan(const LevelPlan& p, int faceDir, int* nreg, int64_t* total) {
+  auto key = std::make_pair((const void*)&p, faceDir);
+  auto it = regionCache_.find(key);
+  if (it == regionCache_.end()) {
+    std::vector<RegionCopy> rc;
+    int64_t off = 0;
+    for (size_t b = 0; b < p.grids.size(); ++b) {
+      Box r = userRegion(p.grids[b], faceDir);
+      RegionCopy c;
+      c.box = (int)b;
+      for (int k = 0; k < 3; ++k) {
+        c.lo[k] = r.lo[k];
+        c.hi[k] = r.hi[k];
+      }
+      c.srcOff = off;
+      off += r.numPts();
+      rc.push_back(c);
+    }
+    RegionPlan rp;
+    rp.n = (int)rc.size();
+    rp.total = off;
+    rp.dev = upload(bufs_, rc, s_);
+    it = regionCache_.emplace(key, rp).first;
+  }
+  *nreg = it->second.n;
+  *total = it->second.total;
+  return it->second.dev;
+}
+
+double* Solver::staging(int64_t n) {
+  if (!stage_ || stage_->bytes < (size_t)n * sizeof(double)) stage_.reset(new DevBuf(n * sizeof(double)));
+  return (double*)stage_->p;
+}
+
+void Solver::scatterValid(const LevelPlan& p, const LevelDev& d, double* dev, const double* src, bool onDevice,
+                          int faceDir) {
+  int nreg;
+  int64_t total;
+  const RegionCopy* rc = (const RegionCopy*)regionPlan(p, faceDir, &nreg, &total);
+  if (nreg == 0) return;
+  const double* dsrc = src;
+  if (!onDevice) {
+    double* st = staging(total);
+    ck(cudaMemcpyAsync(st, src, total * sizeof(double), cudaMemcpyHostToDevice, s_), "scatter h2d");
+    dsrc = st;
+  }
+  k_scatter<<<nreg, 256, 0, s_>>>(d.boxes, rc, dev, dsrc, 1);
+  ck(cudaGetLastError(), "scatter");
+  ck(cudaStreamSynchronize(s_), "scatter sync");
+}
+
+void Solver::gatherValid(const LevelPlan& p, const LevelDev& d, const double* dev, double* dst, bool onDevice) {
+  int nreg;
+  int64_t total;
+  const RegionCopy* rc = (const RegionCopy*)regionPlan(p, -1, &nreg, &total);
+  if (nreg == 0) return;
+  double* ddst = onDevice ? dst : staging(total);
+  k_scatter<<<nreg, 256, 0, s_>>>(d.boxes, rc, const_cast<double*>(dev), ddst, 0);
+  ck(cudaGetLastError(), "gather");
+  if (!onDevice) ck(cudaMemcpyAsync(dst, ddst, total * sizeof(double), cudaMemcpyDeviceToHost, s_), "gather d2h");
+  ck(cudaStreamSynchronize(s_), "gather sync");
+}
+
+void Solver::setRHS(int l, const double* src, bool onDevice) { scatterValid(amr_[l], amrDev_[l], lev_[l].rhs, src, onDevice, -1); }
+void Solver::setPhi(int l, const double* src, bool onDevice) { scatterValid(amr_[l], amrDev_[l], lev_[l].phi, src, onDevice, -1); }
+void Solver::getPhi(int l, double* dst, bool onDevice) { gatherValid(amr_[l], amrDev_[l], lev_[l].phi, dst, onDevice); }
+void Solver::getRHS(int l, double* dst, bool onDevice) { gatherValid(amr_[l], amrDev_[l], lev_[l].rhs, dst, onDevice); }
+
+void Solver::setACoef(int l, const double* src, bool onDevice) {
+  if (!desc_.vc) throw std::runtime_error("cmg: a coefficient on a constant-coefficient operator");
+  int64_t n = numValidCells(l);
+  hostA_[l].resize(n);
+  if (onDevice)
+    ck(cudaMemcpy(hostA_[l].data(), src, n * sizeof(double), cudaMemcpyDeviceToHost), "a d2h");
+  else
+    std::memcpy(hostA_[l].data(), src, n * sizeof(double));
+  scatterValid(amr_[l], amrDev_[l], lev_[l].a, hostA_[l].data(), false, -1);
+}
+
+void Solver::setBCoef(int l, int dir, const double* src, bool onDevice) {
+  if (!desc_.vc) throw std::runtime_error("cmg: b coefficient on a constant-coefficient operator");
+  int64_t n = numFaces(l, dir);
+  hostB_[dir][l].resize(n);
+  if (onDevice)
+    ck(cudaMemcpy(hostB_[dir][l].data(), src, n * sizeof(double), cudaMemcpyDeviceToHost), "b d2h");
+  else
+    std::memcpy(hostB_[dir][l].data(), src, n * sizeof(double));
+  scatterValid(amr_[l], amrDev_[l], lev_[l].b[dir], hostB_[dir][l].data(), false, dir);
+}
+
+}  // namespace cmg
+
+namespace cmg {
+
+namespace {
+
+// Offsets of each box's block in the user-order arrays.
+std::vector<int64_t> userOffsets(const Layout& g, int faceDir) {
+  std::vector<int64_t> off(g.size() + 1, 0);
+  for (size_t b = 0; b < g.size(); ++b) off[b + 1] = off[b] + userRegion(g[b], faceDir).numPts();
+  return off;
+}
+inline int64_t userIdx(const Box& r, int i, int j, int k) {
+  return (int64_t)(i - r.lo[0]) + (int64_t)r.size(0) * ((int64_t)(j - r.lo[1]) + (int64_t)r.size(1) * (k - r.lo[2]));
+}
+
+// lambda = 1 / (alpha a + sum_d scale beta (b_hi + b_lo)), VCAMRPoissonOp2::resetLambda
+// (AMRElliptic/VCAMRPoissonOp2.cpp:283-318) with SUMFACES (VCAMRPoissonOpF.ChF:498-525).
+std::vector<double> computeLambda(const Layout& g, const std::vector<double>& a, const std::vector<double>* b,
+                                  double alpha, double beta, double dx) {
+  std::vector<double> lam(a.size());
+  auto ao = userOffsets(g, -1);
+  std::vector<int64_t> bo[3];
+  for (int d = 0; d < 3; ++d) bo[d] = userOffsets(g, d);
+  const double scale = 1.0 / (dx * dx);
+  for (size_t bx = 0; bx < g.size(); ++bx) {
+    const Box& B = g[bx];
+    for (int k = B.lo[2]; k <= B.hi[2]; ++k)
+      for (int j = B.lo[1]; j <= B.hi[1]; ++j)
+        for (int i = B.lo[0]; i <= B.hi[0]; ++i) {
+          int64_t c = ao[bx] + userIdx(B, i, j, k);
+          double l = a[c] * alpha;
+          for (int d = 0; d < 3; ++d) {
+            Box fr = userRegion(B, d);
+            int hi[3] = {i, j, k};
+            hi[d] += 1;
+            double sumVal = b[d][bo[d][bx] + userIdx(fr, hi[0], hi[1], hi[2])] + b[d][bo[d][bx] + userIdx(fr, i, j, k)];
+            l = l + scale * beta * sumVal;
+          }
+          lam[c] = 1.0 / l;
+        }
+  }
+  return lam;
+}
+
+// CoarseAverage (AverageF.ChF:9-163) of cell data by ratio r, box b -> box b.
+std::vector<double> averageCells(const Layout& fine, const Layout& coarse, const std::vector<double>& f, int r) {
+  auto fo = userOffsets(fine, -1), co = userOffsets(coarse, -1);
+  std::vector<double> out(co.back());
+  const double refScale = 1.0 / (double)(r * r * r);
+  for (size_t bx = 0; bx < coarse.size(); ++bx) {
+    const Box& C = coarse[bx];
+    const Box& F = fine[bx];
+    for (int k = C.lo[2]; k <= C.hi[2]; ++k)
+      for (int j = C.lo[1]; j <= C.hi[1]; ++j)
+        for (int i = C.lo[0]; i <= C.hi[0]; ++i) {
+          double s = 0.0;
+          bool first = true;
+          for (int c = 0; c < r; ++c)
+            for (int b = 0; b < r; ++b)
+              for (int a = 0; a < r; ++a) {
+                double v = f[fo[bx] + userIdx(F, i * r + a, j * r + b, k * r + c)];
+                s = first ? v : s + v;
+                first = false;
+              }
+          out[co[bx] + userIdx(C, i, j, k)] = (r == 2 || r == 4) ? refScale * s : s * refScale;
+        }
+  }
+  return out;
+}
+
+// CoarseAverageFace arithmetic (AverageFaceF.ChF:22-66) by ratio r.
+std::vector<double> averageFaces(const Layout& fine, const Layout& coarse, const std::vector<double>& f, int r, int dir) {
+  auto fo = userOffsets(fine, dir), co = userOffsets(coarse, dir);
+  std::vector<double> out(co.back());
+  const double base = 1.0 / (double)r;
+  const double refScale = base * base;
+  int ext[3] = {r, r, r};
+  ext[dir] = 1;
+  for (size_t bx = 0; bx < coarse.size(); ++bx) {
+    Box C = userRegion(coarse[bx], dir);
+    Box F = userRegion(fine[bx], dir);
+    for (int k = C.lo[2]; k <= C.hi[2]; ++k)
+      for (int j = C.lo[1]; j <= C.hi[1]; ++j)
+        for (int i = C.lo[0]; i <= C.hi[0]; ++i) {
+          double s = 0;
+          for (int c = 0; c < ext[2]; ++c)
+            for (int b = 0; b < ext[1]; ++b)
+              for (int a = 0; a < ext[0]; ++a) s = s + f[fo[bx] + userIdx(F, i * r + a, j * r + b, k * r + c)];
+          out[co[bx] + userIdx(C, i, j, k)] = refScale * s;
+        }
+  }
+  return out;
+}
+
+}  // namespace
+
+void Solver::finalizeCoefficients() {
+  if (!desc_.vc) return;
+  for (int l = 0; l < numLevels(); ++l) {
+    if (hostA_[l].empty() || hostB_[0][l].empty() || hostB_[1][l].empty() || hostB_[2][l].empty())
+      throw std::runtime_error("cmg: coefficients missing on a level");
+    std::vector<double> b[3] = {hostB_[0][l], hostB_[1][l], hostB_[2][l]};
+    auto lam = computeLambda(amr_[l].grids, hostA_[l], b, desc_.alpha, desc_.beta, amr_[l].dx);
+    scatterValid(amr_[l], amrDev_[l], lev_[l].lambda, lam.data(), false, -1);
+  }
+  // Multigrid depths average the level-0 coefficients directly by 2^depth
+  // (VCAMRPoissonOp2Factory::MGnewOp, AMRElliptic/VCAMRPoissonOp2.cpp:1019-1058).
+  for (size_t d = 0; d < mg_.size(); ++d) {
+    int r = 2 << d;
+    auto a = averageCells(amr_[0].grids, mg_[d].grids, hostA_[0], r);
+    std::vector<double> b[3];
+    for (int k = 0; k < 3; ++k) b[k] = averageFaces(amr_[0].grids, mg_[d].grids, hostB_[k][0], r, k);
+    scatterValid(mg_[d], mgDev_[d], mgf_[d].a, a.data(), false, -1);
+    for (int k = 0; k < 3; ++k) scatterValid(mg_[d], mgDev_[d], mgf_[d].b[k], b[k].data(), false, k);
+    auto lam = computeLambda(mg_[d].grids, a, b, desc_.alpha, desc_.beta, mg_[d].dx);
+    scatterValid(mg_[d], mgDev_[d], mgf_[d].lambda, lam.data(), false, -1);
+  }
+}
+
+Coef<double> Solver::coefAMR(int l) const {
+  Coef<double> c;
+  c.vc = desc_.vc;
+  c.alpha = desc_.alpha;
+  c.beta = desc_.beta;
+  c.a = lev_[l].a;
+  for (int d = 0; d < 3; ++d) c.b[d] = lev_[l].b[d];
+  c.lambda = lev_[l].lambda;
+  return c;
+}
+
+Coef<double> Solver::coefMG(int d) const {
+  if (d == 0) return coefAMR(0);
+  Coef<double> c;
+  c.vc = desc_.vc;
+  c.alpha = desc_.alpha;
+  c.beta = desc_.beta;
+  const LevelFields& f = mgf_[d - 1];
+  c.a = f.a;
+  for (int k = 0; k < 3; ++k) c.b[k] = f.b[k];
+  c.lambda = f.lambda;
+  return c;
+}
+
+}  // namespace cmg
+
+namespace cmg {
+
+void Solver::zeroField(const LevelDev& L, double* f) {
+  ck(cudaMemsetAsync(f, 0, L.nelem * sizeof(double), s_), "zero");
+}
+void Solver::copyField(const LevelDev& L, double* dst, const double* src) {
+  ck(cudaMemcpyAsync(dst, src, L.nelem * sizeof(double), cudaMemcpyDeviceToDevice, s_), "copy");
+}
+
+// AMRPoissonOp::levelGSRB / VCAMRPoissonOp2::levelGSRB: per colour,
+// homogeneous CF interpolation + exchange + BC, then the colour update.
+void Solver::relaxAMR(int l, double* phi, const double* rhs, int n) {
+  Coef<double> c = coefAMR(l);
+  const double bytes = amr_[l].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0);
+  for (int it = 0; it < n; ++it)
+    for (int color = 0; color <= 1; ++color) {
+      ghostFill(amrDev_[l], phi, true, s_);
+      timed(P_GSRB, bytes, [&]() { gsrb(amrDev_[l], phi, rhs, c, color, s_); });
+    }
+}
+
+void Solver::relaxMG(int d, double* phi, const double* rhs, int n) {
+  if (d == 0) return relaxAMR(0, phi, rhs, n);
+  const LevelDev& L = mgDev_[d - 1];
+  Coef<double> c = coefMG(d);
+  const double bytes = mg_[d - 1].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0);
+  for (int it = 0; it < n; ++it)
+    for (int color = 0; color <= 1; ++color) {
+      ghostFill(L, phi, true, s_);
+      timed(P_GSRB, bytes, [&]() { gsrb(L, phi, rhs, c, color, s_); });
+    }
+}
+
+// AMRMultiGrid::computeAMRResidualLevel (AMRMultiGrid.H:836-892).
+void Solver::amrResidualLevel(int ilev, int lmax, std::vector<double*>& res, std::vector<double*>& phi,
+                              std::vector<double*>& rhs) {
+  const LevelDev& L = amrDev_[ilev];
+  Coef<double> c = coefAMR(ilev);
+  if (lmax == 0) {
+    // residual(): homogeneous CF (none on level 0), then residualI.
+    ghostFill(L, phi[0], true, s_);
+    timed(P_RESID, amr_[0].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[0], phi[0], rhs[0], c, s_); });
+    return;
+  }
+  if (ilev == lmax) {
+    // AMRResidualNF: coarse-fine interpolation, then residualI.
+    quadCF(L, phi[ilev], phi[ilev - 1], s_);
+    ghostFill(L, phi[ilev], false, s_);
+    timed(P_RESID, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[ilev], phi[ilev], rhs[ilev], c, s_); });
+    return;
+  }
+  // AMRResidual(NC): [CF interpolation], applyOpI, reflux, axby(-1, 1).
+  if (ilev > 0) quadCF(L, phi[ilev], phi[ilev - 1], s_);
+  ghostFill(L, phi[ilev], false, s_);
+  timed(P_RESID, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0), [&]() { applyOp(L, res[ilev], phi[ilev], c, s_); });
+  quadCF(amrDev_[ilev + 1], phi[ilev + 1], phi[ilev], s_);
+  reflux(L, res[ilev], phi[ilev], phi[ilev + 1], c, coefAMR(ilev + 1), s_);
+  negAdd(L, res[ilev], res[ilev], rhs[ilev], s_);
+}
+
+// AMRMultiGrid::computeAMRResidual (AMRMultiGrid.H:682-736).
+double Solver::computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs,
+                                  int lmax) {
+  ck(cudaMemsetAsync(dNorm_, 0, sizeof(double), s_), "norm reset");
+  for (int ilev = 0; ilev <= lmax; ++ilev) {
+    amrResidualLevel(ilev, lmax, res, phi, rhs);
+    if (ilev != lmax) zeroCovered(amrDev_[ilev], res[ilev], s_);
+    maxNorm(amrDev_[ilev], res[ilev], dNorm_, s_);
+  }
+  double h = 0;
+  ck(cudaMemcpyAsync(&h, dNorm_, sizeof(double), cudaMemcpyDeviceToHost, s_), "norm d2h");
+  ck(cudaStreamSynchronize(s_), "norm sync");
+  return h;
+}
+
+// MultiGrid::cycle (MultiGrid.H:629-696), V-cycle (m_cycle = 1).
+void Solver::mgCycle(int depth, double* corr, double* res) {
+  const int D = 1 + (int)mg_.size();
+  if (depth == D - 1) {
+    if (bottomCells_ == 1) {
+      relaxMG(depth, corr, res, 1);
+    } else {
+      relaxMG(depth, corr, res, sp_.bottom);
+      const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
+      bottomSolve(L, corr, res, coefMG(depth), bottom_, sp_.eps, bottomMetric_, s_);
+    }
+    return;
+  }
+  const LevelDev& F = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
+  const LevelDev& C = mgDev_[depth];
+  double* corrC = mgf_[depth].corr;
+  double* resC = mgf_[depth].res;
+  relaxMG(depth, corr, res, sp_.pre);
+  // restrictResidual: homogeneous CF (none) + exchange + BC, RESTRICTRES.
+  ghostFill(F, corr, true, s_);
+  restrictMG(F, C, resC, corr, res, coefMG(depth), s_);
+  zeroField(C, corrC);
+  for (int img = 0; img < sp_.numMG; ++img) mgCycle(depth + 1, corrC, resC);
+  prolongMG(F, C, corr, corrC, s_);
+  relaxMG(depth, corr, res, sp_.post);
+}
+
+// AMRMultiGrid::AMRVCycle (AMRMultiGrid.H:1341-1419), l_base = 0.
+void Solver::amrVCycle(int ilev, int lmax) {
+  if (ilev == lmax)
+    for (int l = 0; l <= lmax; ++l) {
+      copyField(amrDev_[l], lev_[l].res, lev_[l].ures);
+      zeroField(amrDev_[l], lev_[l].corr);
+    }
+  if (lmax == 0) {
+    mgCycle(0, lev_[0].ucorr, lev_[0].ures);
+    return;
+  }
+  if (ilev == 0) {
+    mgCycle(0, lev_[0].corr, lev_[0].res);
+    incr(amrDev_[0], lev_[0].ucorr, lev_[0].corr, 1.0, s_);
+    return;
+  }
+  const LevelDev& L = amrDev_[ilev];
+  const LevelDev& Lc = amrDev_[ilev - 1];
+  LevelFields& f = lev_[ilev];
+  LevelFields& fc = lev_[ilev - 1];
+  relaxAMR(ilev, f.corr, f.res, sp_.pre);
+  incr(L, f.ucorr, f.corr, 1.0, s_);
+  zeroField(Lc, fc.corr);
+  std::vector<double*> res(lmax + 1), ucorr(lmax + 1), ures(lmax + 1);
+  for (int l = 0; l <= lmax; ++l) {
+    res[l] = lev_[l].res;
+    ucorr[l] = lev_[l].ucorr;
+    ures[l] = lev_[l].ures;
+  }
+  amrResidualLevel(ilev - 1, lmax, res, ucorr, ures);
+  // AMRRestrictS: residual of the correction into the scratch (uberCorrection),
+  // averaged straight onto the coarse residual (assignCopier).
+  quadCF(L, f.corr, fc.corr, s_);
+  ghostFill(L, f.corr, false, s_);
+  timed(P_RESID, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.ucorr, f.corr, f.res, coefAMR(ilev), s_); });
+  averageAMR(L, Lc, fc.res, f.ucorr, s_);
+  for (int img = 0; img < sp_.numMG; ++img) amrVCycle(ilev - 1, lmax);
+  // AMRProlongS, AMRUpdateResidual, post-smoothing of the correction's correction.
+  prolongAMR(L, Lc, f.corr, fc.corr, s_);
+  quadCF(L, f.corr, fc.corr, s_);
+  ghostFill(L, f.corr, false, s_);
+  timed(P_RESID, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.res, f.corr, f.res, coefAMR(ilev), s_); });
+  zeroField(L, f.ucorr);
+  relaxAMR(ilev, f.ucorr, f.res, sp_.post);
+  incr(L, f.corr, f.ucorr, 1.0, s_);
+  copyField(L, f.ucorr, f.corr);
+}
+
+double Solver::residualNorm() {
+  int lmax = numLevels() - 1;
+  std::vector<double*> res(lmax + 1), phi(lmax + 1), rhs(lmax + 1);
+  for (int l = 0; l <= lmax; ++l) {
+    res[l] = lev_[l].res;
+    phi[l] = lev_[l].phi;
+    rhs[l] = lev_[l].rhs;
+  }
+  return computeAMRResidual(res, phi, rhs, lmax);
+}
+
+// AMRMultiGrid::solve -> solveNoInitResid (AMRMultiGrid.H:894-1124).
+SolveResult Solver::solve(const SolveParams& p, bool zeroPhi) {
+  sp_ = p;
+  const int lmax = numLevels() - 1;
+  SolveResult out;
+  std::vector<double*> ures(lmax + 1), phi(lmax + 1), rhs(lmax + 1);
+  for (int l = 0; l <= lmax; ++l) {
+    zeroField(amrDev_[l], lev_[l].ucorr);
+    zeroField(amrDev_[l], lev_[l].ures);
+    if (zeroPhi) zeroField(amrDev_[l], lev_[l].phi);
+    ures[l] = lev_[l].ures;
+    phi[l] = lev_[l].phi;
+    rhs[l] = lev_[l].rhs;
+  }
+  const double r0 = computeAMRResidual(ures, phi, rhs, lmax);
+  double rnorm = r0, normLast = 2 * r0;
+  bottomMetric_ = r0;  // setConvergenceMetrics(m_initial_rnorm, cushion * m_eps)
+  out.history.push_back(rnorm);
+  int iter = 0;
+  bool goNorm = rnorm > p.normThresh;
+  bool goRedu = rnorm > p.eps * r0;
+  bool goIter = iter < p.iterMax;
+  bool goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
+  while (goIter && goRedu && goHang && goNorm) {
+    normLast = rnorm;
+    amrVCycle(lmax, lmax);
+    for (int l = 0; l <= lmax; ++l) {
+      incr(amrDev_[l], lev_[l].phi, lev_[l].ucorr, 1.0, s_);
+      zeroField(amrDev_[l], lev_[l].ucorr);
+    }
+    rnorm = computeAMRResidual(ures, phi, rhs, lmax);
+    iter++;
+    out.history.push_back(rnorm);
+    goNorm = rnorm > p.normThresh;
+    goRedu = rnorm > p.eps * r0;
+    goIter = iter < p.iterMax;
+    goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
+  }
+  out.exitStatus = int(!goRedu) + int(!goIter) * 2 + int(!goHang) * 4 + int(!goNorm) * 8;
+  out.iterations = iter;
+  return out;
+}
+
+double Solver::vcycleBytes(const SolveParams& p) const {
+  // Per valid cell, in FP64 words: one GSRB colour pass reads phi and half of
+  // rhs and writes half of phi (VC adds half a, half lambda, all b faces);
+  // residual/operator passes read phi, rhs and write one array.
+  const double s = 8.0;
+  const double vc = desc_.vc ? 1.0 : 0.0;
+  const double colour = 2.0 + vc * 4.0;
+  const double resid = 3.0 + vc * 4.0;
+  double total = 0;
+  for (int l = 0; l < numLevels(); ++l) {
+    double n = (double)amr_[l].grids.numCells();
+    double sweeps = l == 0 && numLevels() == 1 ? p.pre + p.post : p.pre + p.post;
+    total += n * s * (2 * sweeps * colour + 3 * resid);
+  }
+  for (size_t d = 0; d < mg_.size(); ++d) {
+    double n = (double)mg_[d].grids.numCells();
+    total += n * s * (2 * (p.pre + p.post) * colour + resid);
+  }
+  return total;
+}
+
+}  // namespace cmg
+
+namespace cmg {
+
+cudaEvent_t Solver::takeEvent() {
+  if (!evPool_.empty()) {
+    cudaEvent_t e = evPool_.back();
+    evPool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  ck(cudaEventCreate(&e), "event");
+  return e;
+}
+
+void Solver::profileDrain() {
+  if (prof_.empty()) return;
+  ck(cudaStreamSynchronize(s_), "profile sync");
+  for (const ProfRec& r : prof_) {
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, r.a, r.b), "event elapsed");
+    profAcc_[r.cls][0] += 1;
+    profAcc_[r.cls][1] += ms;
+    profAcc_[r.cls][2] += r.bytes;
+    evPool_.push_back(r.a);
+    evPool_.push_back(r.b);
+  }
+  prof_.clear();
+}
+
+void Solver::profileEnable(bool on) {
+  profileDrain();
+  profOn_ = on;
+  for (auto& c : profAcc_) c[0] = c[1] = c[2] = 0;
+}
+
+void Solver::profileRead(int cls, int64_t* launches, double* ms, double* bytes) {
+  if (cls < 0 || cls >= P_NCLASS) throw std::invalid_argument("cmg: profile class out of range");
+  profileDrain();
+  *launches = (int64_t)profAcc_[cls][0];
+  *ms = profAcc_[cls][1];
+  *bytes = profAcc_[cls][2];
+}
+
+}  // namespace cmg

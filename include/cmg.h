@@ -1,0 +1,141 @@
+/*
+ * cmg.h -- C ABI of the B200 AMR multigrid solve (libcmg.so).
+ *
+ * This is the boundary a host program binds to replace the reference's
+ * AMRMultiGrid<LevelData<FArrayBox>>::solve over AMRPoissonOp /
+ * VCAMRPoissonOp2 (Chombo lib/src/AMRElliptic).  Plain pointers and sizes
+ * only; every call returns an int status (CMG_OK on success) and never aborts.
+ * Field data cross the boundary as the valid cells of every box of a level,
+ * boxes in DisjointBoxLayout order (sorted, BoxTools/BoxLayout.cpp:89-119),
+ * cells x-fastest inside a box (BaseFab order, BoxTools/BaseFabImplem.H:291-312).
+ * Face coefficients in direction d use the face box of each cell box
+ * (surroundingNodes, hi[d] + 1).
+ */
+#ifndef CMG_H
+#define CMG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CMG_OK = 0,
+  CMG_EINVAL = 1,    /* bad argument (level, direction, sizes, null pointer) */
+  CMG_ENOMEM = 2,    /* device allocation failed */
+  CMG_ECUDA = 3,     /* CUDA runtime error */
+  CMG_EINTERNAL = 4  /* anything else; see cmg_last_error() */
+};
+
+typedef struct cmg_box {
+  int lo[3];
+  int hi[3];
+} cmg_box;
+
+typedef struct cmg_hierarchy cmg_hierarchy;
+
+/* Solver parameters: AMRMultiGrid::setSolverParameters
+ * (AMRElliptic/AMRMultiGrid.H:527-553) plus m_imin (AMRMultiGrid.H:599-622). */
+typedef struct cmg_solve_params {
+  int pre, post, bottom, num_mg, iter_max, imin;
+  double eps, hang, norm_thresh;
+} cmg_solve_params;
+
+/* Message of the last failed call on this thread. */
+const char* cmg_last_error(void);
+
+/* Builds a hierarchy: level-0 domain box, level-0 cell size, per-level box
+ * counts and the concatenated boxes (refinement ratio 2 between levels), and
+ * the operator.  op = 0: AMRPoissonOp, L = alpha phi + beta Lap(phi)
+ * (AMRPoissonOpFactory::define, AMRElliptic/AMRPoissonOp.cpp:1857-1903);
+ * op = 1: VCAMRPoissonOp2, L = alpha a phi - beta div(b grad phi)
+ * (VCAMRPoissonOp2Factory::define, AMRElliptic/VCAMRPoissonOp2.cpp:873-924).
+ * Boundary conditions are homogeneous Dirichlet on every domain face
+ * (the examples' ParseBC, releasedExamples/AMRPoisson/execCell/poissonSolve.cpp:76-119).
+ * Builds every plan (exchange copiers, coarse-fine stencils, flux registers,
+ * multigrid levels: AMRMultiGrid::define, AMRMultiGrid.H:1292-1328) and
+ * allocates all device state. */
+int cmg_hierarchy_create(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
+                         const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta,
+                         cmg_hierarchy** out);
+int cmg_hierarchy_destroy(cmg_hierarchy* h);
+
+/* Sizes of the per-level data arrays. */
+int cmg_num_levels(const cmg_hierarchy* h, int* out);
+int cmg_num_boxes(const cmg_hierarchy* h, int level, int* out);
+int cmg_get_boxes(const cmg_hierarchy* h, int level, cmg_box* out, int cap);
+int cmg_num_cells(const cmg_hierarchy* h, int level, int64_t* out);
+int cmg_num_faces(const cmg_hierarchy* h, int level, int dir, int64_t* out);
+
+/* Right-hand side, coefficients and solution.  on_device != 0: the pointer is
+ * device memory of the current device.  Replaces filling the LevelData
+ * arguments of AMRMultiGrid::solve (AMRMultiGrid.H:894-904) and the
+ * coefficient LevelData of VCAMRPoissonOp2Factory::define. */
+int cmg_set_rhs(cmg_hierarchy* h, int level, const double* data, int on_device);
+int cmg_set_acoef(cmg_hierarchy* h, int level, const double* data, int on_device);
+int cmg_set_bcoef(cmg_hierarchy* h, int level, int dir, const double* data, int on_device);
+/* Computes the relaxation coefficient (VCAMRPoissonOp2::resetLambda,
+ * VCAMRPoissonOp2.cpp:283-318) and the multigrid coefficient averages
+ * (VCAMRPoissonOp2Factory::MGnewOp, VCAMRPoissonOp2.cpp:1019-1058).  Call
+ * after the coefficients are set and before cmg_solve (op = 1 only). */
+int cmg_finalize_coefficients(cmg_hierarchy* h);
+int cmg_get_phi(cmg_hierarchy* h, int level, double* data, int on_device);
+int cmg_get_rhs(cmg_hierarchy* h, int level, double* data, int on_device);
+int cmg_set_phi(cmg_hierarchy* h, int level, const double* data, int on_device);
+
+/* AMRMultiGrid::solve(phi, rhs, lmax, 0, zeroPhi) (AMRMultiGrid.H:894-1124).
+ * history receives the composite max-norm residual at the start of every
+ * iteration followed by the final one (up to history_cap values). */
+int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
+              double* history, int history_cap, int* history_len);
+
+/* AMRMultiGrid::computeAMRResidual(phi, rhs, lmax, 0) (AMRMultiGrid.H:738-750). */
+int cmg_residual_norm(cmg_hierarchy* h, double* out);
+
+/* Fills rhs (all levels) and, for op = 1, a and b from the seeded synthetic
+ * workload recipe (Gaussian bumps; exp of a random Fourier series), then
+ * finalizes the coefficients. */
+int cmg_fill_synthetic(cmg_hierarchy* h, uint64_t seed);
+
+/* domainSplit (BoxTools/BRMeshRefine.cpp:983-1092), all directions. Boxes are
+ * returned in layout order. */
+int cmg_domain_split(const int domain_lo[3], const int domain_hi[3], int max_box, int block_factor, cmg_box* out,
+                     int cap, int* n);
+
+/* Local motion items of a level's exchange copier (Copier::exchangeDefine +
+ * trimEdges, BoxTools/Copier.cpp:1464-1516, 142-177): per item
+ * from, to, fromRegion(6), toRegion(6).  Returns the item count in *n. */
+int cmg_exchange_plan(const cmg_hierarchy* h, int level, int* items14, int cap, int* n);
+/* Local motion items of the coarsened-fine to coarse copier of level >= 1
+ * (AMRPoissonOp::buildCopier, AMRElliptic/AMRPoissonOp.cpp:474-483). */
+int cmg_coarse_fine_plan(const cmg_hierarchy* h, int level, int* items14, int cap, int* n);
+
+/* Host-only variants (no device state): the same plans for a box list given
+ * directly, in layout order after sorting. */
+int cmg_layout_exchange_plan(const cmg_box* boxes, int nbox, int* items14, int cap, int* n);
+int cmg_layout_coarse_fine_plan(const cmg_box* fine, int nfine, const cmg_box* coarse, int ncoarse, int* items14,
+                                int cap, int* n);
+
+/* Algorithmic bytes moved per V-cycle (roofline numerator). */
+int cmg_vcycle_bytes(const cmg_hierarchy* h, const cmg_solve_params* p, double* out);
+
+/* The CUDA stream every call of this hierarchy runs on (cudaStream_t). */
+int cmg_get_stream(const cmg_hierarchy* h, void** stream);
+
+/* Kernel-class device timing, the counterpart of the reference's CH_TIMER
+ * trace timers (BaseTools/CH_Timer.H:44-163): while enabled, every launch of a
+ * class is bracketed by CUDA events on the hierarchy's stream.  Classes:
+ * 0 = red-black relaxation, 1 = residual / operator application, 2 = other.
+ * cmg_profile_read returns launches, total device milliseconds and the
+ * algorithmic bytes of those launches since the last enable. */
+int cmg_profile_enable(cmg_hierarchy* h, int on);
+/* Total kernel launches issued by this library in this process. */
+int cmg_launch_count(int64_t* out);
+int cmg_profile_read(cmg_hierarchy* h, int kernel_class, int64_t* launches, double* ms, double* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -96,7 +96,9 @@ static void dirichletBC(FArrayBox& a_state, const Box& a_valid, const ProblemDom
 class ResidualRecorder : public AMRMultiGridInspector<LDF> {
  public:
   std::vector<double> norms;
+  std::vector<double> stamps;  // wall time at the start of each iteration
   void recordResiduals(const Vector<LDF*>& r, int lmin, int lmax, int) override {
+    stamps.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count());
     double m = 0;
     for (int l = lmin; l <= lmax; ++l)
       for (DataIterator dit = r[l]->dataIterator(); dit.ok(); ++dit)
@@ -193,9 +195,35 @@ int main(int argc, char** argv) {
     LoadBalance(procs, oldBoxes[0]);
     grids[0].define(oldBoxes[0], procs, domains[0]);
   }
-  // Finer levels: VClocalFuncs.cpp:398-480.
+  // Finer levels: VClocalFuncs.cpp:398-480, or a given layout (boxfile=:
+  // "nlev" then per level "nbox" and nbox lines "lo0 lo1 lo2 hi0 hi1 hi2").
   int topLevel = 0;
-  if (numLevels > 1) {
+  const std::string boxfile = args("boxfile", "");
+  if (!boxfile.empty()) {
+    FILE* bf = std::fopen(boxfile.c_str(), "r");
+    if (!bf) {
+      std::fprintf(stderr, "oracle: cannot open %s\n", boxfile.c_str());
+      return 2;
+    }
+    int nl = 0;
+    if (std::fscanf(bf, "%d", &nl) != 1 || nl < 1 || nl > numLevels) return 2;
+    for (int l = 0; l < nl; ++l) {
+      int nb = 0;
+      if (std::fscanf(bf, "%d", &nb) != 1) return 2;
+      Vector<Box> bl;
+      for (int b = 0; b < nb; ++b) {
+        int v[6];
+        for (int k = 0; k < 6; ++k)
+          if (std::fscanf(bf, "%d", &v[k]) != 1) return 2;
+        bl.push_back(Box(IntVect(v[0], v[1], v[2]), IntVect(v[3], v[4], v[5])));
+      }
+      Vector<int> procs(bl.size(), 0);
+      LoadBalance(procs, bl);
+      grids[l] = DisjointBoxLayout(bl, procs, domains[l]);
+    }
+    std::fclose(bf);
+    topLevel = nl - 1;
+  } else if (numLevels > 1) {
     BRMeshRefine meshrefine(domains[0], refRatios, fillRatio, blockFactor, 2, maxBox);
     bool more = true;
     while (more) {
@@ -287,14 +315,27 @@ int main(int argc, char** argv) {
   RefCountedPtr<AMRMultiGridInspector<LDF> > insp(new ResidualRecorder);
   ResidualRecorder* rec = static_cast<ResidualRecorder*>(&(*insp));
 
-  double seconds = 0;
+  double seconds = 0, tstart = 0, tend = 0;
   for (int rep = 0; rep < repeat; ++rep) {
     rec->norms.clear();
+    rec->stamps.clear();
     if (rep == 0) solver->addInspector(insp);
     auto t0 = std::chrono::steady_clock::now();
     solver->solve(phi, rhs, finest, 0, true);
     auto t1 = std::chrono::steady_clock::now();
+    tstart = std::chrono::duration<double>(t0.time_since_epoch()).count();
+    tend = std::chrono::duration<double>(t1.time_since_epoch()).count();
     seconds += std::chrono::duration<double>(t1 - t0).count();
+    // Per-repeat record for the CPU timing runs: total, set-up part and
+    // per-iteration parts of this solve.
+    std::vector<double> its;
+    for (size_t i = 0; i < rec->stamps.size(); ++i)
+      its.push_back((i + 1 < rec->stamps.size() ? rec->stamps[i + 1] : tend) - rec->stamps[i]);
+    std::printf("repeat %d seconds %.9g setup %.9g iterations", rep, std::chrono::duration<double>(t1 - t0).count(),
+                rec->stamps.empty() ? 0.0 : rec->stamps[0] - tstart);
+    for (double t : its) std::printf(" %.9g", t);
+    std::printf("\n");
+    std::fflush(stdout);
   }
   int exitStatus = solver->m_exitStatus;
   double finalNorm = solver->computeAMRResidual(phi, rhs, finest, 0);
@@ -309,6 +350,14 @@ int main(int argc, char** argv) {
   std::fprintf(js, "\"pre\": %d, \"post\": %d, \"bottom\": %d, \"iters\": %d, \"eps\": %.17g, \"hang\": %.17g,\n",
                pre, post, bottom, iterMax, eps, hang);
   std::fprintf(js, "\"exit_status\": %d, \"seconds_per_solve\": %.9g,\n", exitStatus, seconds / repeat);
+  // Wall time of the last solve split into: start -> first iteration (set-up
+  // and initial residual), each V-cycle iteration, and the tail.
+  std::fprintf(js, "\"iteration_seconds\": [");
+  for (size_t i = 0; i < rec->stamps.size(); ++i) {
+    double t = (i + 1 < rec->stamps.size() ? rec->stamps[i + 1] : tend) - rec->stamps[i];
+    std::fprintf(js, "%s%.9g", i ? "," : "", t);
+  }
+  std::fprintf(js, "],\n\"setup_seconds\": %.9g,\n", rec->stamps.empty() ? 0.0 : rec->stamps[0] - tstart);
   std::fprintf(js, "\"residual_history\": [");
   for (size_t i = 0; i < rec->norms.size(); ++i) std::fprintf(js, "%s%.17g", i ? "," : "", rec->norms[i]);
   std::fprintf(js, "],\n\"boxes\": [");

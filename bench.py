@@ -28,6 +28,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 ORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle")
+PROFILE_CLASSES = ["relax_finest", "residual_op", "ghost_fill", "bottom", "relax_other"]
 METRIC = "Poisson solves/s & p50/p99 latency at 1e-10 rel. residual; V-cycle HBM GB/s"
 WORKLOADS = {
     "config1": {
@@ -237,7 +238,6 @@ def main():
     # exceeds L2, so no flush is needed between steps.
     sampler = ClockSampler(local)
     sampler.start()
-    h.profile_enable(True)
     barrier()
     launches0 = cmg.launch_count()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
@@ -251,8 +251,20 @@ def main():
     clocks = sampler.stop()
     step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[-1])
-    gsrb = h.profile_read(0)
-    resid = h.profile_read(1)
+
+    # Per-class breakdown from separate solves with CUDA events around every
+    # kernel class (events add a little time, so these solves are not the
+    # timed ones above).
+    n_prof = min(args.steps, 3)
+    h.profile_enable(True)
+    pe = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    pe[0].record(stream)
+    for _ in range(n_prof):
+        h.solve(params)
+    pe[1].record(stream)
+    barrier()
+    prof_ms = pe[0].elapsed_time(pe[1])
+    classes = {name: h.profile_read(i) for i, name in enumerate(PROFILE_CLASSES)}
     h.profile_enable(False)
     if dist:
         t = torch.tensor([total_ms], device="cuda")
@@ -290,21 +302,23 @@ def main():
            "d2h_bytes_per_step": d2h}
 
     peak, peak_kind = measured_peaks()
-    n_gsrb, ms_gsrb, bytes_gsrb = gsrb
-    achieved = (bytes_gsrb / 1e9) / (ms_gsrb / 1e3) if ms_gsrb > 0 else 0.0
+    n_fine, ms_fine, bytes_fine = classes["relax_finest"]
+    achieved = (bytes_fine / 1e9) / (ms_fine / 1e3) if ms_fine > 0 else 0.0
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(args.workload)
+    sweeps = n_fine / 2
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": "k_gsrb (red-black relaxation, one colour, every level)",
-                "peak_kind": peak_kind, "launches": n_gsrb,
-                "avg_launch_us": 1000.0 * ms_gsrb / max(n_gsrb, 1),
-                "bytes_per_launch": bytes_gsrb / max(n_gsrb, 1),
-                "residual_kernels_gbs": (resid[2] / 1e9) / (resid[1] / 1e3) if resid[1] > 0 else 0.0,
-                "gsrb_share_of_step": ms_gsrb / total_ms if total_ms > 0 else 0.0}
-
+                "kernel": "red-black sweep of the finest AMR level (k_relax_a + k_relax_b, one launch each per sweep)",
+                "peak_kind": peak_kind, "sweeps": sweeps,
+                "avg_sweep_us": 1000.0 * ms_fine / max(sweeps, 1),
+                "algorithmic_bytes_per_sweep": bytes_fine / max(sweeps, 1)}
+    breakdown = {name: {"launches": int(v[0]) // n_prof, "ms_per_solve": v[1] / n_prof,
+                        "share": v[1] / prof_ms if prof_ms > 0 else 0.0,
+                        "gbs": (v[2] / 1e9) / (v[1] / 1e3) if v[1] > 0 and v[2] > 0 else None}
+                 for name, v in classes.items()}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res = cpu_reference(meta, 1, 1)
@@ -322,7 +336,7 @@ def main():
                        "vcycles_per_solve": n_iter, "l2": "working set > L2 (no flush)",
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-            "vcycle_gbs": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "roofline": roofline, "breakdown": breakdown, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)

@@ -1,9 +1,12 @@
 // Plain-old-data tables that the host plan builder writes and the CUDA
 // kernels read.  One level's fields all share one ghosted layout:
-//   every box owns a FAB of (nx+2) x (ny+2) x (nz+2) cells (one ghost layer),
-//   stored x-fastest with the x pitch padded to a multiple of 4 elements and
-//   the first valid cell at column XOFF+1 = 4, so every valid row starts on
-//   a 32-byte boundary for FP64 (16-byte for FP32).
+//   every box owns a FAB of px x (ny+2) x (nz+2) cells (one ghost layer;
+//   px = nx+2 rounded up to even), stored red-black ordered: the cells of
+//   colour 0 ((i+j+k) even) first, then those of colour 1, each half in
+//   x-fastest order of the FAB with two x-neighbours sharing one slot.  A
+//   red-black pass therefore touches only its own colour's half of every
+//   cell-centred array (plus the other colour's phi), with contiguous,
+//   coalesced rows, and never moves bytes of the colour it does not update.
 // Face-centred data (the b coefficient in direction d) uses the same layout:
 // the face on the low side of cell i in direction d is stored at cell i, so
 // faces lo..hi+1 fit in the valid region plus the high ghost layer.
@@ -14,12 +17,11 @@
 
 namespace cmg {
 
-enum { XOFF = 3 };
-
 struct BoxDesc {
   int lo[3], hi[3];
-  int px, py;       // x pitch and y extent (ny + 2) of the ghosted FAB
-  int64_t off;      // element offset of ghost cell (lo0-1, lo1-1, lo2-1)
+  int px, py;       // x pitch (even) and y extent (ny + 2) of the ghosted FAB
+  int64_t off;      // element offset of the box's FAB
+  int64_t half;     // elements per colour (px * py * (nz + 2) / 2)
 };
 
 #if defined(__CUDACC__)
@@ -28,9 +30,35 @@ struct BoxDesc {
 #define CMG_HD inline
 #endif
 
+// Slot of cell (i,j,k) within its colour half (x-neighbour pairs share it).
+CMG_HD int64_t colourSlot(const BoxDesc& b, int i, int j, int k) {
+  return ((int64_t)(i - b.lo[0] + 1) + (int64_t)b.px * ((int64_t)(j - b.lo[1] + 1) + (int64_t)b.py * (k - b.lo[2] + 1))) >> 1;
+}
+
 CMG_HD int64_t cellIndex(const BoxDesc& b, int i, int j, int k) {
-  return b.off + (int64_t)(i - b.lo[0] + 1 + XOFF) +
-         (int64_t)b.px * ((int64_t)(j - b.lo[1] + 1) + (int64_t)b.py * (k - b.lo[2] + 1));
+  return b.off + ((i + j + k) & 1) * b.half + colourSlot(b, i, j, k);
+}
+
+// Element indices of a cell and of its six face neighbours.
+struct Stencil {
+  int64_t c, xp, xm, yp, ym, zp, zm;
+};
+
+CMG_HD Stencil stencil(const BoxDesc& b, int i, int j, int k) {
+  Stencil s;
+  const int col = (i + j + k) & 1;
+  const int64_t m = colourSlot(b, i, j, k);
+  const int64_t own = b.off + col * b.half, oth = b.off + (1 - col) * b.half + m;
+  const int xo = (i - b.lo[0] + 1) & 1;  // x parity inside the FAB
+  const int64_t sy = b.px >> 1, sz = (int64_t)(b.px >> 1) * b.py;
+  s.c = own + m;
+  s.xp = oth + xo;
+  s.xm = oth + xo - 1;
+  s.yp = oth + sy;
+  s.ym = oth - sy;
+  s.zp = oth + sz;
+  s.zm = oth - sz;
+  return s;
 }
 
 // Ghost-layer work items executed by one kernel per fill (exchange copies,
@@ -42,6 +70,9 @@ enum GhostKind {
   G_CFLIN = 3,     // one-cell-wide box: g = f*phi(1 in)
   G_ZERO = 4       // dst(cell) = 0 (covered cells before a norm)
 };
+
+// Ghost cells handled by one thread block of the ghost kernel.
+enum { GHOST_THREADS = 256 };
 
 struct GhostTask {
   int kind, dst, src, dir, side;  // side = -1 (low) or +1 (high)

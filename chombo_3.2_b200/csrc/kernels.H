@@ -18,8 +18,14 @@ struct LevelDev {
   int64_t nelem = 0;
   const GhostTask* ghost = nullptr;
   int nExchBC = 0, nGhost = 0;
+  const int* ghostStart = nullptr;       // cumulative cell counts (nGhost + 1)
+  const int* ghostBlock = nullptr;       // first task of each GHOST_THREADS cells
+  int nCellsExchBC = 0, nCellsGhost = 0;
   const GhostTask* zero = nullptr;
   int nZero = 0;
+  const int* zeroStart = nullptr;
+  const int* zeroBlock = nullptr;
+  int nCellsZero = 0;
   const Chunk* chAll = nullptr;
   int nAll = 0;
   const Chunk* chColor[2] = {nullptr, nullptr};

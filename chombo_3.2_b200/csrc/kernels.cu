@@ -23,16 +23,6 @@ inline void check(cudaError_t e, const char* what) {
 std::atomic<long long> g_launches{0};
 #define CMG_LAUNCHED(name) (g_launches.fetch_add(1, std::memory_order_relaxed), check(cudaGetLastError(), name))
 
-struct Strides {
-  int64_t sy, sz;
-};
-__device__ __forceinline__ Strides strides(const BoxDesc& b) {
-  Strides s;
-  s.sy = b.px;
-  s.sz = (int64_t)b.px * b.py;
-  return s;
-}
-
 // Cell q of box b in x-fastest order.
 __device__ __forceinline__ bool allCell(const BoxDesc& b, int q, int& i, int& j, int& k) {
   int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
@@ -62,13 +52,27 @@ __device__ __forceinline__ bool colorCell(const BoxDesc& b, int q, int color, in
 // Exchange copies (BoxLayoutData local copy), homogeneous Dirichlet faces
 // (BCFunc.cpp:25-32,294-354: ghost = 2*0 - near), homogeneous quadratic and
 // linear coarse-fine ghosts (InterpF.ChF:435-494) and zeroing.
+// One thread per ghost cell across all tasks; the task of cell g is found by
+// binary search in the cumulative cell counts, between the tasks holding the
+// first cells of this block and of the next (blockTask).
 template <class T>
-__global__ void k_ghost(const BoxDesc* boxes, const GhostTask* tasks, T* f, T c1, T c2, T flin) {
-  const GhostTask t = tasks[blockIdx.x];
+__global__ void k_ghost(const BoxDesc* boxes, const GhostTask* tasks, const int* start, const int* blockTask,
+                        int ntask, int ncell, T* f, T c1, T c2, T flin) {
+  int g0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g0 >= ncell) return;
+  int lo = blockTask[blockIdx.x], hi = min(blockTask[blockIdx.x + 1], ntask - 1);
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= g0)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const GhostTask t = tasks[lo];
   const BoxDesc db = boxes[t.dst];
-  int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1, nz = t.hi[2] - t.lo[2] + 1;
-  int n = nx * ny * nz;
-  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+  int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1;
+  {
+    int q = g0 - start[lo];
     int i = t.lo[0] + q % nx, r = q / nx;
     int j = t.lo[1] + r % ny, k = t.lo[2] + r / ny;
     int64_t g = cellIndex(db, i, j, k);
@@ -96,16 +100,17 @@ __global__ void k_ghost(const BoxDesc* boxes, const GhostTask* tasks, T* f, T c1
 // ---------------------------------------------------------------- stencils
 // Sum of the six neighbours in the ChF order (+x, -x, +y, -y, +z, -z).
 template <class T>
-__device__ __forceinline__ T nbrSum(const T* p, int64_t c, const Strides& s) {
-  return p[c + 1] + p[c - 1] + p[c + s.sy] + p[c - s.sy] + p[c + s.sz] + p[c - s.sz];
+__device__ __forceinline__ T nbrSum(const T* p, const Stencil& st) {
+  return p[st.xp] + p[st.xm] + p[st.yp] + p[st.ym] + p[st.zp] + p[st.zm];
 }
 
-// Variable-coefficient divergence term of VCAMRPoissonOpF.ChF:93-111.
+// Variable-coefficient divergence term of VCAMRPoissonOpF.ChF:93-111 (the
+// face above the cell in direction d is stored at the neighbour's index).
 template <class T>
-__device__ __forceinline__ T vcDiv(const T* p, const T* b0, const T* b1, const T* b2, int64_t c, const Strides& s) {
-  T pc = p[c];
-  return b0[c + 1] * (p[c + 1] - pc) - b0[c] * (pc - p[c - 1]) + b1[c + s.sy] * (p[c + s.sy] - pc) -
-         b1[c] * (pc - p[c - s.sy]) + b2[c + s.sz] * (p[c + s.sz] - pc) - b2[c] * (pc - p[c - s.sz]);
+__device__ __forceinline__ T vcDiv(const T* p, const T* b0, const T* b1, const T* b2, const Stencil& st) {
+  T pc = p[st.c];
+  return b0[st.xp] * (p[st.xp] - pc) - b0[st.c] * (pc - p[st.xm]) + b1[st.yp] * (p[st.yp] - pc) -
+         b1[st.c] * (pc - p[st.ym]) + b2[st.zp] * (p[st.zp] - pc) - b2[st.c] * (pc - p[st.zm]);
 }
 
 struct Scal {
@@ -122,19 +127,19 @@ __global__ void k_gsrb(const BoxDesc* boxes, const Chunk* chunks, T* phi, const 
   const BoxDesc bd = boxes[ch.box];
   int i, j, k;
   if (!colorCell(bd, ch.start + threadIdx.x, color, i, j, k)) return;
-  Strides s = strides(bd);
-  int64_t c = cellIndex(bd, i, j, k);
+  const Stencil st = stencil(bd, i, j, k);
+  const int64_t c = st.c;
   const T dxinv = T(sc.dxinv);
   if (VC) {
     T pc = phi[c];
-    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, c, s) * dxinv;
+    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, st) * dxinv;
     phi[c] = pc - lam[c] * (lofphi - rhs[c]);
   } else if (sc.laplacian) {
-    T lphi = nbrSum(phi, c, s) * dxinv;
+    T lphi = nbrSum(phi, st) * dxinv;
     phi[c] = T(sc.lambda) * (rhs[c] - lphi);
   } else {
     T pc = phi[c];
-    T lphi = (nbrSum(phi, c, s) - T(2.0) * T(3) * pc) * dxinv;
+    T lphi = (nbrSum(phi, st) - T(2.0) * T(3) * pc) * dxinv;
     T helmop = T(sc.alpha) * pc + T(sc.beta) * lphi;
     phi[c] = pc + T(sc.lambda) * (helmop - rhs[c]);
   }
@@ -150,15 +155,15 @@ __global__ void k_op(const BoxDesc* boxes, const Chunk* chunks, T* r, const T* p
   const BoxDesc bd = boxes[ch.box];
   int i, j, k;
   if (!allCell(bd, ch.start + threadIdx.x, i, j, k)) return;
-  Strides s = strides(bd);
-  int64_t c = cellIndex(bd, i, j, k);
+  const Stencil st = stencil(bd, i, j, k);
+  const int64_t c = st.c;
   const T dxinv = T(sc.dxinv);
   T pc = phi[c];
   if (VC) {
-    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, c, s) * dxinv;
+    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, st) * dxinv;
     r[c] = MODE == 0 ? rhs[c] - lofphi : lofphi;
   } else {
-    T lap = (nbrSum(phi, c, s) - T(6) * pc) * dxinv;
+    T lap = (nbrSum(phi, st) - T(6) * pc) * dxinv;
     if (MODE == 0)
       r[c] = -(T(sc.alpha) * pc) - T(sc.beta) * lap + rhs[c];
     else
@@ -222,20 +227,20 @@ __global__ void k_restrictmg(const BoxDesc* fboxes, const BoxDesc* cboxes, const
   int I, J, K;
   if (!allCell(cb, ch.start + threadIdx.x, I, J, K)) return;
   const BoxDesc fb = fboxes[ch.box];
-  Strides s = strides(fb);
   const T dxinv = T(sc.dxinv);
   const T denom = T(8);
   T acc = T(0);
   for (int kk = 0; kk < 2; ++kk)
     for (int jj = 0; jj < 2; ++jj)
       for (int ii = 0; ii < 2; ++ii) {
-        int64_t c = cellIndex(fb, 2 * I + ii, 2 * J + jj, 2 * K + kk);
+        const Stencil st = stencil(fb, 2 * I + ii, 2 * J + jj, 2 * K + kk);
+        const int64_t c = st.c;
         T pc = phi[c];
         T lofphi;
         if (VC)
-          lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, c, s) * dxinv;
+          lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, st) * dxinv;
         else
-          lofphi = T(sc.alpha) * pc + T(sc.beta) * (nbrSum(phi, c, s) - pc * T(2) * T(3)) * dxinv;
+          lofphi = T(sc.alpha) * pc + T(sc.beta) * (nbrSum(phi, st) - pc * T(2) * T(3)) * dxinv;
         acc = acc + (rhs[c] - lofphi) / denom;
       }
   resC[cellIndex(cb, I, J, K)] = acc;
@@ -265,10 +270,11 @@ __global__ void k_average(const BoxDesc* fboxes, const BoxDesc* cboxes, const Co
   if (q >= nx * ny * nz) return;
   int I = it.lo[0] + q % nx, r = q / nx, J = it.lo[1] + r % ny, K = it.lo[2] + r / ny;
   const BoxDesc fb = fboxes[it.fbox];
-  Strides s = strides(fb);
-  int64_t f = cellIndex(fb, 2 * I, 2 * J, 2 * K);
-  T sum = fine[f] + fine[f + 1] + fine[f + s.sy] + fine[f + s.sy + 1] + fine[f + s.sz] + fine[f + s.sz + 1] +
-          fine[f + s.sz + s.sy] + fine[f + s.sz + s.sy + 1];
+  const int i = 2 * I, j = 2 * J, k = 2 * K;
+  T sum = fine[cellIndex(fb, i, j, k)] + fine[cellIndex(fb, i + 1, j, k)] + fine[cellIndex(fb, i, j + 1, k)] +
+          fine[cellIndex(fb, i + 1, j + 1, k)] + fine[cellIndex(fb, i, j, k + 1)] +
+          fine[cellIndex(fb, i + 1, j, k + 1)] + fine[cellIndex(fb, i, j + 1, k + 1)] +
+          fine[cellIndex(fb, i + 1, j + 1, k + 1)];
   coarse[cellIndex(cboxes[it.cbox], I, J, K)] = T(0.125) * sum;
 }
 
@@ -448,7 +454,7 @@ __device__ void blkCells(const LevelDev& L, F fn) {
     Chunk ch = L.chAll[idx / CHUNK];
     const BoxDesc bd = L.boxes[ch.box];
     int i, j, k;
-    if (allCell(bd, ch.start + idx % CHUNK, i, j, k)) fn(bd, cellIndex(bd, i, j, k));
+    if (allCell(bd, ch.start + idx % CHUNK, i, j, k)) fn(bd, cellIndex(bd, i, j, k), i, j, k);
   }
   __syncthreads();
 }
@@ -461,19 +467,19 @@ __device__ void blkGsrb(const BottomArgs& A, double* phi, const double* rhs, int
     const BoxDesc bd = L.boxes[ch.box];
     int i, j, k;
     if (!colorCell(bd, ch.start + idx % CHUNK, color, i, j, k)) continue;
-    Strides s = strides(bd);
-    int64_t c = cellIndex(bd, i, j, k);
+    const Stencil st = stencil(bd, i, j, k);
+    const int64_t c = st.c;
     const double dxinv = A.sc.dxinv;
     if (A.vc) {
       double pc = phi[c];
-      double lofphi = A.sc.alpha * A.a[c] * pc - A.sc.beta * vcDiv(phi, A.b0, A.b1, A.b2, c, s) * dxinv;
+      double lofphi = A.sc.alpha * A.a[c] * pc - A.sc.beta * vcDiv(phi, A.b0, A.b1, A.b2, st) * dxinv;
       phi[c] = pc - A.lam[c] * (lofphi - rhs[c]);
     } else if (A.sc.laplacian) {
-      double lphi = nbrSum(phi, c, s) * dxinv;
+      double lphi = nbrSum(phi, st) * dxinv;
       phi[c] = A.sc.lambda * (rhs[c] - lphi);
     } else {
       double pc = phi[c];
-      double lphi = (nbrSum(phi, c, s) - 2.0 * 3 * pc) * dxinv;
+      double lphi = (nbrSum(phi, st) - 2.0 * 3 * pc) * dxinv;
       double helmop = A.sc.alpha * pc + A.sc.beta * lphi;
       phi[c] = pc + A.sc.lambda * (helmop - rhs[c]);
     }
@@ -494,21 +500,21 @@ __device__ void blkRelax(const BottomArgs& A, double* phi, const double* rhs, in
 __device__ void blkOp(const BottomArgs& A, double* r, double* phi, const double* rhs, int mode) {
   blkGhost(A, phi);
   const double dxinv = A.sc.dxinv;
-  blkCells(A.L, [&](const BoxDesc& bd, int64_t c) {
-    Strides s = strides(bd);
+  blkCells(A.L, [&](const BoxDesc& bd, int64_t c, int i, int j, int k) {
+    const Stencil st = stencil(bd, i, j, k);
     double pc = phi[c];
     if (A.vc) {
-      double lofphi = A.sc.alpha * A.a[c] * pc - A.sc.beta * vcDiv(phi, A.b0, A.b1, A.b2, c, s) * dxinv;
+      double lofphi = A.sc.alpha * A.a[c] * pc - A.sc.beta * vcDiv(phi, A.b0, A.b1, A.b2, st) * dxinv;
       r[c] = mode == 0 ? rhs[c] - lofphi : lofphi;
     } else {
-      double lap = (nbrSum(phi, c, s) - 6.0 * pc) * dxinv;
+      double lap = (nbrSum(phi, st) - 6.0 * pc) * dxinv;
       r[c] = mode == 0 ? -(A.sc.alpha * pc) - A.sc.beta * lap + rhs[c] : A.sc.alpha * pc + A.sc.beta * lap;
     }
   });
 }
 
 __device__ void blkPrecond(const BottomArgs& A, double* out, const double* in) {
-  blkCells(A.L, [&](const BoxDesc&, int64_t c) { out[c] = A.vc ? in[c] * A.lam[c] : in[c] * A.mult; });
+  blkCells(A.L, [&](const BoxDesc&, int64_t c, int, int, int) { out[c] = A.vc ? in[c] * A.lam[c] : in[c] * A.mult; });
   blkRelax(A, out, in, 2);
 }
 
@@ -561,9 +567,9 @@ __global__ void k_bottom(BottomArgs A) {
     for (int64_t q = threadIdx.x; q < L.nelem; q += blockDim.x) x[q] = 0.0;
     __syncthreads();
   };
-  auto copyValid = [&](double* d, const double* s) { blkCells(L, [&](const BoxDesc&, int64_t c) { d[c] = s[c]; }); };
+  auto copyValid = [&](double* d, const double* s) { blkCells(L, [&](const BoxDesc&, int64_t c, int, int, int) { d[c] = s[c]; }); };
   auto incrV = [&](double* y, const double* x, double sc) {
-    blkCells(L, [&](const BoxDesc&, int64_t c) { y[c] = y[c] + x[c] * sc; });
+    blkCells(L, [&](const BoxDesc&, int64_t c, int, int, int) { y[c] = y[c] + x[c] * sc; });
   };
   zeroAll(A.r);
   blkOp(A, A.r, A.phi, A.rhs, 0);
@@ -600,7 +606,7 @@ __global__ void k_bottom(BottomArgs A) {
       init = false;
     } else {
       beta[1] = (rho[1] / rho[2]) * (alpha[1] / omega[1]);
-      blkCells(L, [&](const BoxDesc&, int64_t c) { A.p[c] = A.p[c] * beta[1]; });
+      blkCells(L, [&](const BoxDesc&, int64_t c, int, int, int) { A.p[c] = A.p[c] * beta[1]; });
       incrV(A.p, A.v, -beta[1] * omega[1]);
       incrV(A.p, A.r, 1.0);
     }
@@ -686,19 +692,22 @@ Scal scalars(double dx, double alpha, double beta, int vc) {
 template <class T>
 void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s) {
   int n = withCF ? L.nGhost : L.nExchBC;
+  int ncell = withCF ? L.nCellsGhost : L.nCellsExchBC;
   if (n == 0) return;
   const double dx = L.dx, dxc = L.dxCrse;
   T c1 = T(2 * (dxc - dx) / (dxc + dx));
   T c2 = T(-(dxc - dx) / (dxc + 3 * dx));
   T flin = T(1 - 2 * dx / (dx + dxc));
-  k_ghost<T><<<n, 128, 0, s>>>(L.boxes, L.ghost, f, c1, c2, flin);
+  k_ghost<T><<<(ncell + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(L.boxes, L.ghost, L.ghostStart,
+                                                                                L.ghostBlock, n, ncell, f, c1, c2, flin);
   CMG_LAUNCHED("ghostFill");
 }
 
 template <class T>
 void zeroCovered(const LevelDev& L, T* f, cudaStream_t s) {
   if (L.nZero == 0) return;
-  k_ghost<T><<<L.nZero, 128, 0, s>>>(L.boxes, L.zero, f, T(0), T(0), T(0));
+  k_ghost<T><<<(L.nCellsZero + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(
+      L.boxes, L.zero, L.zeroStart, L.zeroBlock, L.nZero, L.nCellsZero, f, T(0), T(0), T(0));
   CMG_LAUNCHED("zeroCovered");
 }
 

@@ -23,7 +23,13 @@ struct LevelPlan {
   // Ghost work: [0, nExchBC) exchange + physical BC, then homogeneous CF.
   std::vector<GhostTask> ghost;
   int nExchBC = 0;
+  // Cumulative cell counts of the ghost tasks (ghostStart[t] = first cell of
+  // task t), so one ghost kernel can spread cells evenly over thread blocks.
+  std::vector<int> ghostStart;
+  std::vector<int> ghostBlock;         // task holding cell b*GHOST_THREADS
   std::vector<GhostTask> zeroCovered;  // covered by the next finer level
+  std::vector<int> zeroStart;          // cumulative cell counts of zeroCovered
+  std::vector<int> zeroBlock;
   std::vector<Chunk> chunksAll, chunksColor[2];
   // Coarse-fine interpolation from the next coarser level (levels >= 1).
   std::vector<CFCoarse> cfCoarse;
@@ -55,6 +61,10 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc);
 inline int64_t cellOf(const LevelPlan& L, int b, const IV& p) {
   return cellIndex(L.boxes[b], p[0], p[1], p[2]);
 }
+
+// blockTask[b] = task holding cell b*GHOST_THREADS for cumulative cell
+// counts `start` (one entry per block plus a last one = last task).
+std::vector<int> blockTasks(const std::vector<int>& start);
 
 // Finds the box of L containing p, or -1.
 int ownerOf(const LevelPlan& L, const IV& p);

@@ -25,7 +25,51 @@ bool faceCFSet(const LevelPlan& L, const Box& b, int d, int side, CellSet& out) 
   return !out.empty();
 }
 
+// Greedy cover of a cell set by disjoint boxes: from the first remaining cell
+// (x-fastest order) extend along x, then y, then z while every cell is in the
+// set.  Used for coarse-fine faces that are not a single box; the per-cell
+// formula does not depend on the grouping.
+std::vector<Box> coverByBoxes(const CellSet& s) {
+  CellSet left = s;
+  std::vector<Box> out;
+  for (const IV& p : s.cells()) {
+    if (!left.contains(p)) continue;
+    Box b(p, p);
+    while (left.contains(IV(b.hi[0] + 1, p[1], p[2]))) b.hi[0]++;
+    for (;;) {
+      Box nb = b;
+      nb.hi[1]++;
+      Box row(IV(b.lo[0], nb.hi[1], b.lo[2]), IV(b.hi[0], nb.hi[1], b.hi[2]));
+      if (!left.containsBox(row)) break;
+      b = nb;
+    }
+    for (;;) {
+      Box nb = b;
+      nb.hi[2]++;
+      Box slab(IV(b.lo[0], b.lo[1], nb.hi[2]), IV(b.hi[0], b.hi[1], nb.hi[2]));
+      if (!left.containsBox(slab)) break;
+      b = nb;
+    }
+    left.subtract(b);
+    out.push_back(b);
+  }
+  return out;
+}
+
 }  // namespace
+
+std::vector<int> blockTasks(const std::vector<int>& start) {
+  std::vector<int> bt;
+  if (start.size() < 2) return bt;
+  const int ntask = (int)start.size() - 1, ncell = start.back();
+  int t = 0;
+  for (int64_t c = 0; c < ncell; c += GHOST_THREADS) {
+    while (start[t + 1] <= c) ++t;
+    bt.push_back(t);
+  }
+  bt.push_back(ntask - 1);
+  return bt;
+}
 
 void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse) {
   L.grids = grids;
@@ -41,10 +85,11 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
       d.lo[k] = bx.lo[k];
       d.hi[k] = bx.hi[k];
     }
-    d.px = ((bx.size(0) + 2 + XOFF) + 3) / 4 * 4;
+    d.px = (bx.size(0) + 3) & ~1;  // nx + 2 rounded up to even
     d.py = bx.size(1) + 2;
     d.off = off;
-    off += (int64_t)d.px * d.py * (bx.size(2) + 2);
+    d.half = (int64_t)d.px * d.py * (bx.size(2) + 2) / 2;
+    off += 2 * d.half;
     L.boxes.push_back(d);
   }
   L.nelem = off;
@@ -90,7 +135,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
           if (mb.numPts() == s.numPts())
             regions.push_back(mb);
           else
-            for (const IV& p : s.cells()) regions.push_back(Box(p, p));
+            regions = coverByBoxes(s);
           for (const Box& r : regions) {
             GhostTask t{kind, (int)b, (int)b, d, side, {}, {}};
             for (int k = 0; k < 3; ++k) {
@@ -101,6 +146,13 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
           }
         }
   }
+
+  L.ghostStart.assign(1, 0);
+  for (const GhostTask& t : L.ghost) {
+    int64_t c = (int64_t)(t.hi[0] - t.lo[0] + 1) * (t.hi[1] - t.lo[1] + 1) * (t.hi[2] - t.lo[2] + 1);
+    L.ghostStart.push_back(L.ghostStart.back() + (int)c);
+  }
+  L.ghostBlock = blockTasks(L.ghostStart);
 
   L.chunksAll.clear();
   L.chunksColor[0].clear();
@@ -428,6 +480,11 @@ void buildCoarseFine(LevelPlan& F, LevelPlan& C) {
     }
     C.zeroCovered.push_back(z);
   }
+  C.zeroStart.assign(1, 0);
+  for (const GhostTask& t : C.zeroCovered)
+    C.zeroStart.push_back(C.zeroStart.back() +
+                          (t.hi[0] - t.lo[0] + 1) * (t.hi[1] - t.lo[1] + 1) * (t.hi[2] - t.lo[2] + 1));
+  C.zeroBlock = blockTasks(C.zeroStart);
 }
 
 void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {

@@ -76,7 +76,9 @@ class Solver {
 
   // Per-kernel-class device timing (CUDA events around each launch of the
   // class, on the solver's stream) with the algorithmic bytes of each launch.
-  enum ProfClass { P_GSRB = 0, P_RESID = 1, P_OTHER = 2, P_NCLASS = 3 };
+  // Profile classes: relaxation on the finest AMR level, residual/operator
+  // kernels, ghost fills, bottom solves, relaxation on every other level.
+  enum ProfClass { P_RELAX_FINE = 0, P_OP = 1, P_GHOST = 2, P_BOTTOM = 3, P_RELAX = 4, P_NCLASS = 5 };
   void profileEnable(bool on);
   void profileRead(int cls, int64_t* launches, double* ms, double* bytes);
 
@@ -92,6 +94,9 @@ class Solver {
   Coef<double> coefMG(int d) const;
   void relaxAMR(int l, double* phi, const double* rhs, int n);
   void relaxMG(int d, double* phi, const double* rhs, int n);
+  void relaxLevel(const LevelDev& L, double cells, const Coef<double>& c, double* phi, const double* rhs, int n,
+                  int cls);
+  void fill(const LevelDev& L, double* f, bool withCF);
   void amrResidualLevel(int ilev, int lmax, std::vector<double*>& res, std::vector<double*>& phi,
                         std::vector<double*>& rhs);
   double computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);

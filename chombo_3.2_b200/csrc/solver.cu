@@ -79,8 +79,15 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
   d.ghost = upload(bufs_, p.ghost, s_);
   d.nExchBC = p.nExchBC;
   d.nGhost = (int)p.ghost.size();
+  d.ghostStart = upload(bufs_, p.ghostStart, s_);
+  d.ghostBlock = upload(bufs_, p.ghostBlock, s_);
+  d.nCellsExchBC = p.ghostStart.empty() ? 0 : p.ghostStart[p.nExchBC];
+  d.nCellsGhost = p.ghostStart.empty() ? 0 : p.ghostStart.back();
   d.zero = upload(bufs_, p.zeroCovered, s_);
   d.nZero = (int)p.zeroCovered.size();
+  d.zeroStart = upload(bufs_, p.zeroStart, s_);
+  d.zeroBlock = upload(bufs_, p.zeroBlock, s_);
+  d.nCellsZero = p.zeroStart.empty() ? 0 : p.zeroStart.back();
   d.chAll = upload(bufs_, p.chunksAll, s_);
   d.nAll = (int)p.chunksAll.size();
   for (int c = 0; c < 2; ++c) {
@@ -435,26 +442,38 @@ void Solver::copyField(const LevelDev& L, double* dst, const double* src) {
 
 // AMRPoissonOp::levelGSRB / VCAMRPoissonOp2::levelGSRB: per colour,
 // homogeneous CF interpolation + exchange + BC, then the colour update.
-void Solver::relaxAMR(int l, double* phi, const double* rhs, int n) {
-  Coef<double> c = coefAMR(l);
-  const double bytes = amr_[l].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0);
+// Algorithmic bytes of one colour pass over the red-black ordered layout,
+// per cell of the level: half a word each for the updated colour's phi read,
+// phi write and rhs, and the other colour's phi read (constant
+// coefficients, 2 words); variable coefficients add half a word each for
+// a and lambda and a full word for each of the three face arrays, since
+// every face borders one cell of each colour (6 words).
+void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<double>& c, double* phi, const double* rhs,
+                        int n, int cls) {
+  const double bytes = cells * 8.0 * (c.vc ? 6.0 : 2.0);
   for (int it = 0; it < n; ++it)
     for (int color = 0; color <= 1; ++color) {
-      ghostFill(amrDev_[l], phi, true, s_);
-      timed(P_GSRB, bytes, [&]() { gsrb(amrDev_[l], phi, rhs, c, color, s_); });
+      fill(L, phi, true);
+      timed(cls, bytes, [&]() { gsrb(L, phi, rhs, c, color, s_); });
     }
+}
+
+void Solver::relaxAMR(int l, double* phi, const double* rhs, int n) {
+  const int finest = (int)amr_.size() - 1;
+  relaxLevel(amrDev_[l], (double)amr_[l].grids.numCells(), coefAMR(l), phi, rhs, n,
+             l == finest ? P_RELAX_FINE : P_RELAX);
 }
 
 void Solver::relaxMG(int d, double* phi, const double* rhs, int n) {
   if (d == 0) return relaxAMR(0, phi, rhs, n);
-  const LevelDev& L = mgDev_[d - 1];
-  Coef<double> c = coefMG(d);
-  const double bytes = mg_[d - 1].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0);
-  for (int it = 0; it < n; ++it)
-    for (int color = 0; color <= 1; ++color) {
-      ghostFill(L, phi, true, s_);
-      timed(P_GSRB, bytes, [&]() { gsrb(L, phi, rhs, c, color, s_); });
-    }
+  relaxLevel(mgDev_[d - 1], (double)mg_[d - 1].grids.numCells(), coefMG(d), phi, rhs, n, P_RELAX);
+}
+
+// Ghost fill, timed as its own class: every ghost cell written once and
+// its source read once (16 bytes per cell).
+void Solver::fill(const LevelDev& L, double* f, bool withCF) {
+  const double bytes = 16.0 * (withCF ? L.nCellsGhost : L.nCellsExchBC);
+  timed(P_GHOST, bytes, [&]() { ghostFill(L, f, withCF, s_); });
 }
 
 // AMRMultiGrid::computeAMRResidualLevel (AMRMultiGrid.H:836-892).
@@ -464,21 +483,21 @@ void Solver::amrResidualLevel(int ilev, int lmax, std::vector<double*>& res, std
   Coef<double> c = coefAMR(ilev);
   if (lmax == 0) {
     // residual(): homogeneous CF (none on level 0), then residualI.
-    ghostFill(L, phi[0], true, s_);
-    timed(P_RESID, amr_[0].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[0], phi[0], rhs[0], c, s_); });
+    fill(L, phi[0], true);
+    timed(P_OP, amr_[0].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[0], phi[0], rhs[0], c, s_); });
     return;
   }
   if (ilev == lmax) {
     // AMRResidualNF: coarse-fine interpolation, then residualI.
     quadCF(L, phi[ilev], phi[ilev - 1], s_);
-    ghostFill(L, phi[ilev], false, s_);
-    timed(P_RESID, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[ilev], phi[ilev], rhs[ilev], c, s_); });
+    fill(L, phi[ilev], false);
+    timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[ilev], phi[ilev], rhs[ilev], c, s_); });
     return;
   }
   // AMRResidual(NC): [CF interpolation], applyOpI, reflux, axby(-1, 1).
   if (ilev > 0) quadCF(L, phi[ilev], phi[ilev - 1], s_);
-  ghostFill(L, phi[ilev], false, s_);
-  timed(P_RESID, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0), [&]() { applyOp(L, res[ilev], phi[ilev], c, s_); });
+  fill(L, phi[ilev], false);
+  timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0), [&]() { applyOp(L, res[ilev], phi[ilev], c, s_); });
   quadCF(amrDev_[ilev + 1], phi[ilev + 1], phi[ilev], s_);
   reflux(L, res[ilev], phi[ilev], phi[ilev + 1], c, coefAMR(ilev + 1), s_);
   negAdd(L, res[ilev], res[ilev], rhs[ilev], s_);
@@ -508,7 +527,7 @@ void Solver::mgCycle(int depth, double* corr, double* res) {
     } else {
       relaxMG(depth, corr, res, sp_.bottom);
       const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
-      bottomSolve(L, corr, res, coefMG(depth), bottom_, sp_.eps, bottomMetric_, s_);
+      timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr, res, coefMG(depth), bottom_, sp_.eps, bottomMetric_, s_); });
     }
     return;
   }
@@ -518,7 +537,7 @@ void Solver::mgCycle(int depth, double* corr, double* res) {
   double* resC = mgf_[depth].res;
   relaxMG(depth, corr, res, sp_.pre);
   // restrictResidual: homogeneous CF (none) + exchange + BC, RESTRICTRES.
-  ghostFill(F, corr, true, s_);
+  fill(F, corr, true);
   restrictMG(F, C, resC, corr, res, coefMG(depth), s_);
   zeroField(C, corrC);
   for (int img = 0; img < sp_.numMG; ++img) mgCycle(depth + 1, corrC, resC);
@@ -559,15 +578,15 @@ void Solver::amrVCycle(int ilev, int lmax) {
   // AMRRestrictS: residual of the correction into the scratch (uberCorrection),
   // averaged straight onto the coarse residual (assignCopier).
   quadCF(L, f.corr, fc.corr, s_);
-  ghostFill(L, f.corr, false, s_);
-  timed(P_RESID, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.ucorr, f.corr, f.res, coefAMR(ilev), s_); });
+  fill(L, f.corr, false);
+  timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.ucorr, f.corr, f.res, coefAMR(ilev), s_); });
   averageAMR(L, Lc, fc.res, f.ucorr, s_);
   for (int img = 0; img < sp_.numMG; ++img) amrVCycle(ilev - 1, lmax);
   // AMRProlongS, AMRUpdateResidual, post-smoothing of the correction's correction.
   prolongAMR(L, Lc, f.corr, fc.corr, s_);
   quadCF(L, f.corr, fc.corr, s_);
-  ghostFill(L, f.corr, false, s_);
-  timed(P_RESID, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.res, f.corr, f.res, coefAMR(ilev), s_); });
+  fill(L, f.corr, false);
+  timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.res, f.corr, f.res, coefAMR(ilev), s_); });
   zeroField(L, f.ucorr);
   relaxAMR(ilev, f.ucorr, f.res, sp_.post);
   incr(L, f.corr, f.ucorr, 1.0, s_);

@@ -126,7 +126,9 @@ int cmg_get_stream(const cmg_hierarchy* h, void** stream);
 /* Kernel-class device timing, the counterpart of the reference's CH_TIMER
  * trace timers (BaseTools/CH_Timer.H:44-163): while enabled, every launch of a
  * class is bracketed by CUDA events on the hierarchy's stream.  Classes:
- * 0 = red-black relaxation, 1 = residual / operator application, 2 = other.
+ * 0 = red-black relaxation on the finest AMR level, 1 = residual / operator
+ * application, 2 = ghost fills (exchange, boundary and homogeneous coarse-fine
+ * values), 3 = bottom solves, 4 = red-black relaxation on every other level.
  * cmg_profile_read returns launches, total device milliseconds and the
  * algorithmic bytes of those launches since the last enable. */
 int cmg_profile_enable(cmg_hierarchy* h, int on);

@@ -188,6 +188,11 @@ class Hierarchy:
         _check(lib().cmg_residual_norm(self.h, ctypes.byref(r)))
         return r.value
 
+    def residual_norm_noalloc(self):
+        r = ctypes.c_double()
+        _check(lib().cmg_residual_norm_noalloc(self.h, ctypes.byref(r)))
+        return r.value
+
     def stream(self):
         s = ctypes.c_void_p()
         _check(lib().cmg_get_stream(self.h, ctypes.byref(s)))

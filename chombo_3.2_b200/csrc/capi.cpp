@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/cmg.h"
+#include "noalloc.H"
 #include "solver.H"
 #include "synthetic.H"
 
@@ -275,6 +276,16 @@ int cmg_residual_norm(cmg_hierarchy* h, double* out) {
   return guard([&]() {
     needLevel(h, 0);
     *out = h->solver->residualNorm();
+  });
+}
+
+static_assert(CMG_NOALLOC_MAX_BOXES == cmg::NOALLOC_MAX_BOXES, "header limit matches the scratch size");
+
+int cmg_residual_norm_noalloc(cmg_hierarchy* h, double* out) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (!out) throw std::invalid_argument("cmg: null output pointer");
+    *out = cmg::residualNormNoAlloc(*h->solver);
   });
 }
 

@@ -67,6 +67,10 @@ class Solver {
   SolveResult solve(const SolveParams& p, bool zeroPhi = true);
   // One composite residual evaluation (AMRMultiGrid::computeAMRResidual).
   double residualNorm();
+  // The same evaluation with the max-norm reduced through `scratch`, a
+  // device array of NOALLOC_MAX_BOXES + 1 doubles (noalloc.cu); allocates
+  // nothing on success.
+  double residualNormStatic(double* scratch);
   cudaStream_t stream() const { return s_; }
   // Bytes moved per V-cycle by the algorithmic count (each array read once,
   // each output written once per pass), for the roofline.

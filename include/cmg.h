@@ -93,6 +93,22 @@ int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* ex
 /* AMRMultiGrid::computeAMRResidual(phi, rhs, lmax, 0) (AMRMultiGrid.H:738-750). */
 int cmg_residual_norm(cmg_hierarchy* h, double* out);
 
+/* Same value as cmg_residual_norm, allocating no memory on success (no
+ * counterpart in the reference, which has no such constraint).  For callers
+ * that cannot let the library allocate at call time: a process whose memory
+ * pool holds all free device memory, or a loop that must not synchronise the
+ * device through cudaMalloc/cudaFree.  The reduction scratch is a fixed
+ * device array of 4097 doubles per device (CMG_NOALLOC_MAX_BOXES per-box
+ * partials plus one running maximum); hierarchies with a level of more than
+ * CMG_NOALLOC_MAX_BOXES boxes, or with more than 16 levels, are rejected with
+ * CMG_EINVAL.  The first call on a device looks the scratch up with
+ * cudaGetSymbolAddress (that device made current); make it before any stream
+ * capture begins on the device.  Every call zeroes the running maximum
+ * itself.  Calls that overlap in time on one device share the scratch and
+ * race: serialise them. */
+#define CMG_NOALLOC_MAX_BOXES 4096
+int cmg_residual_norm_noalloc(cmg_hierarchy* h, double* out);
+
 /* Fills rhs (all levels) and, for op = 1, a and b from the seeded synthetic
  * workload recipe (Gaussian bumps; exp of a random Fourier series), then
  * finalizes the coefficients. */

@@ -20,6 +20,9 @@ struct LevelDev {
   int nExchBC = 0, nGhost = 0;
   const int* ghostStart = nullptr;       // cumulative cell counts (nGhost + 1)
   const int* ghostBlock = nullptr;       // first task of each GHOST_THREADS cells
+  const int* slotStart = nullptr;        // the same over one-colour slots
+  const int* slotBlock = nullptr;
+  int nSlotsExchBC = 0, nSlotsGhost = 0;
   int nCellsExchBC = 0, nCellsGhost = 0;
   const GhostTask* zero = nullptr;
   int nZero = 0;
@@ -61,7 +64,10 @@ struct Coef {
   const T* lambda = nullptr;
 };
 
-template <class T> void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s);
+// Ghost fill: exchange copies and physical BC values, plus the homogeneous
+// coarse-fine values when withCF; par >= 0 restricts it to ghost cells of
+// colour par (the only ones a pass over colour 1 - par reads).
+template <class T> void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par = -1);
 template <class T> void zeroCovered(const LevelDev& L, T* f, cudaStream_t s);
 template <class T> void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s);
 // residualI form: r = rhs - L(phi) in the operator's own expression order.
@@ -89,18 +95,26 @@ template <class T> void incr(const LevelDev& L, T* lhs, const T* x, double scale
 // Max |f| over valid cells, folded into *out (device scalar) with max().
 template <class T> void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s);
 
-// Work vectors of the bottom BiCGStab: r, r~, e, p, p~, s~, t, v (each one
-// level-sized array), per-box partial sums and a 2-int status (exit, iters).
+// Bottom BiCGStab state in the compact slot space of the bottom level
+// (BottomPlan): slot tables, vectors r, r~, e, p, p~, s~, t, v, phi, rhs
+// (nv + ng doubles each), the compact coefficients of a variable-coefficient
+// operator, and a 2-int status (exit, iterations).
 struct BottomWork {
-  double* v[8];
-  double* part;
-  int* status;
+  int nv = 0, ng = 0, nbox = 0, ncol[2] = {0, 0};
+  const int *fab = nullptr, *nb = nullptr, *col[2] = {nullptr, nullptr}, *boxStart = nullptr;
+  const int *gsrc = nullptr, *gkind = nullptr;
+  double* v[10] = {};
+  double *a = nullptr, *b[3] = {nullptr, nullptr, nullptr}, *lam = nullptr;
+  int* status = nullptr;
 };
 // BiCGStab bottom solve of L(phi) = rhs (homogeneous boundary conditions) on
 // one level, one thread block, reference summation order.  eps and metric are
 // the tolerance and convergence metric AMRMultiGrid hands its bottom solver.
+// phi and rhs are level fields; the coefficients come from w.
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
                  double eps, double metric, cudaStream_t s);
+// dst[slot] = fab[w.fab[slot]] for every slot of the bottom level.
+void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream_t s);
 
 // Number of kernel launches issued by the launchers above since load.
 long long launchCount();

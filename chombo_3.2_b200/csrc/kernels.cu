@@ -54,10 +54,13 @@ __device__ __forceinline__ bool colorCell(const BoxDesc& b, int q, int color, in
 // linear coarse-fine ghosts (InterpF.ChF:435-494) and zeroing.
 // One thread per ghost cell across all tasks; the task of cell g is found by
 // binary search in the cumulative cell counts, between the tasks holding the
-// first cells of this block and of the next (blockTask).
+// first cells of this block and of the next (blockTask).  par >= 0 fills only
+// the ghost cells of colour par ((i+j+k) & 1 == par): a colour pass reads no
+// ghost of its own colour, so the fill before it needs only the other one.
+// Then each task row offers ceil(nx/2) slots and `start` counts slots.
 template <class T>
 __global__ void k_ghost(const BoxDesc* boxes, const GhostTask* tasks, const int* start, const int* blockTask,
-                        int ntask, int ncell, T* f, T c1, T c2, T flin) {
+                        int ntask, int ncell, int par, T* f, T c1, T c2, T flin) {
   int g0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (g0 >= ncell) return;
   int lo = blockTask[blockIdx.x], hi = min(blockTask[blockIdx.x + 1], ntask - 1);
@@ -71,28 +74,37 @@ __global__ void k_ghost(const BoxDesc* boxes, const GhostTask* tasks, const int*
   const GhostTask t = tasks[lo];
   const BoxDesc db = boxes[t.dst];
   int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1;
-  {
-    int q = g0 - start[lo];
-    int i = t.lo[0] + q % nx, r = q / nx;
-    int j = t.lo[1] + r % ny, k = t.lo[2] + r / ny;
-    int64_t g = cellIndex(db, i, j, k);
-    if (t.kind == G_COPY) {
-      f[g] = f[cellIndex(boxes[t.src], i, j, k)];
-    } else if (t.kind == G_ZERO) {
-      f[g] = T(0);
+  int q = g0 - start[lo], i, j, k;
+  if (par < 0) {
+    i = t.lo[0] + q % nx;
+    int r = q / nx;
+    j = t.lo[1] + r % ny;
+    k = t.lo[2] + r / ny;
+  } else {
+    const int hx = (nx + 1) >> 1;
+    int r = q / hx;
+    j = t.lo[1] + r % ny;
+    k = t.lo[2] + r / ny;
+    i = t.lo[0] + ((par - t.lo[0] - j - k) & 1) + 2 * (q % hx);
+    if (i > t.hi[0]) return;
+  }
+  int64_t g = cellIndex(db, i, j, k);
+  if (t.kind == G_COPY) {
+    f[g] = f[cellIndex(boxes[t.src], i, j, k)];
+  } else if (t.kind == G_ZERO) {
+    f[g] = T(0);
+  } else {
+    int e[3] = {0, 0, 0};
+    e[t.dir] = -t.side;  // one cell inward
+    int64_t in1 = cellIndex(db, i + e[0], j + e[1], k + e[2]);
+    if (t.kind == G_BC) {
+      T zero = T(0);
+      f[g] = T(2) * zero - f[in1];
+    } else if (t.kind == G_CFLIN) {
+      f[g] = flin * f[in1];
     } else {
-      int e[3] = {0, 0, 0};
-      e[t.dir] = -t.side;  // one cell inward
-      int64_t in1 = cellIndex(db, i + e[0], j + e[1], k + e[2]);
-      if (t.kind == G_BC) {
-        T zero = T(0);
-        f[g] = T(2) * zero - f[in1];
-      } else if (t.kind == G_CFLIN) {
-        f[g] = flin * f[in1];
-      } else {
-        int64_t in2 = cellIndex(db, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
-        f[g] = c1 * f[in1] + c2 * f[in2];
-      }
+      int64_t in2 = cellIndex(db, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
+      f[g] = c1 * f[in1] + c2 * f[in2];
     }
   }
 }
@@ -410,70 +422,67 @@ __global__ void k_reflux(const RefluxCell* cells, int n, const RefluxCoarseTerm*
 // deepest multigrid level, run by one thread block so that every dot product
 // and norm is summed in the reference's order: per box in x-fastest order
 // (FArrayBox::dotProduct, FArrayBox.cpp:260-280; FArrayBox::sumPow pencil
-// order, FArrayBox.cpp:168-209), then box by box.
+// order, FArrayBox.cpp:168-209), then box by box.  All vectors live in the
+// bottom level's compact slot space (valid cells, then the face ghosts the
+// stencil reads; BottomPlan), a few tens of KB that stay in L1, and every
+// pass is one flat loop over a precomputed slot list.
 struct BottomArgs {
-  LevelDev L;
+  BottomWork W;
+  const BoxDesc* boxes;
   Scal sc;
   int vc;
-  const double *a, *b0, *b1, *b2, *lam;
-  double *phi;
-  const double* rhs;
-  double *r, *rt, *e, *p, *pt, *st, *t, *v, *part;
+  double* phiFab;
+  const double* rhsFab;
+  double *phi, *rhs, *r, *rt, *e, *p, *pt, *st, *t, *v;
   double eps, metric, reps, hang, small, mult;
-  int imax, numRestarts, nsmooth;
-  int* status;
+  int imax, numRestarts;
 };
 
+// Exchange copies and homogeneous Dirichlet values of every ghost slot.
 __device__ void blkGhost(const BottomArgs& A, double* f) {
-  const LevelDev& L = A.L;
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int ti = warp; ti < L.nGhost; ti += nw) {
-    const GhostTask t = L.ghost[ti];
-    const BoxDesc db = L.boxes[t.dst];
-    int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1, nz = t.hi[2] - t.lo[2] + 1;
-    for (int q = lane; q < nx * ny * nz; q += 32) {
-      int i = t.lo[0] + q % nx, r = q / nx, j = t.lo[1] + r % ny, k = t.lo[2] + r / ny;
-      int64_t g = cellIndex(db, i, j, k);
-      if (t.kind == G_COPY) {
-        f[g] = f[cellIndex(L.boxes[t.src], i, j, k)];
-      } else if (t.kind == G_BC) {
-        int e[3] = {0, 0, 0};
-        e[t.dir] = -t.side;
-        double zero = 0.0;
-        f[g] = 2.0 * zero - f[cellIndex(db, i + e[0], j + e[1], k + e[2])];
-      }
+  const BottomWork& W = A.W;
+  for (int g = threadIdx.x; g < W.ng; g += blockDim.x) {
+    const int kind = W.gkind[g];
+    if (kind == 0) {
+      f[W.nv + g] = f[W.gsrc[g]];
+    } else if (kind == 1) {
+      double zero = 0.0;
+      f[W.nv + g] = 2.0 * zero - f[W.gsrc[g]];
     }
   }
   __syncthreads();
 }
 
 template <class F>
-__device__ void blkCells(const LevelDev& L, F fn) {
-  int n = L.nAll * CHUNK;
-  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-    Chunk ch = L.chAll[idx / CHUNK];
-    const BoxDesc bd = L.boxes[ch.box];
-    int i, j, k;
-    if (allCell(bd, ch.start + idx % CHUNK, i, j, k)) fn(bd, cellIndex(bd, i, j, k), i, j, k);
-  }
+__device__ void blkCells(const BottomArgs& A, F fn) {
+  for (int q = threadIdx.x; q < A.W.nv; q += blockDim.x) fn(q);
   __syncthreads();
 }
 
+__device__ __forceinline__ Stencil slotStencil(const BottomWork& W, int q) {
+  const int* n = W.nb + 6 * q;
+  Stencil st;
+  st.c = q;
+  st.xp = n[0];
+  st.xm = n[1];
+  st.yp = n[2];
+  st.ym = n[3];
+  st.zp = n[4];
+  st.zm = n[5];
+  return st;
+}
+
 __device__ void blkGsrb(const BottomArgs& A, double* phi, const double* rhs, int color) {
-  const LevelDev& L = A.L;
-  int n = L.nColor[color] * CHUNK;
-  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-    Chunk ch = L.chColor[color][idx / CHUNK];
-    const BoxDesc bd = L.boxes[ch.box];
-    int i, j, k;
-    if (!colorCell(bd, ch.start + idx % CHUNK, color, i, j, k)) continue;
-    const Stencil st = stencil(bd, i, j, k);
+  const BottomWork& W = A.W;
+  const int* list = W.col[color];
+  for (int idx = threadIdx.x; idx < W.ncol[color]; idx += blockDim.x) {
+    const Stencil st = slotStencil(W, list[idx]);
     const int64_t c = st.c;
     const double dxinv = A.sc.dxinv;
     if (A.vc) {
       double pc = phi[c];
-      double lofphi = A.sc.alpha * A.a[c] * pc - A.sc.beta * vcDiv(phi, A.b0, A.b1, A.b2, st) * dxinv;
-      phi[c] = pc - A.lam[c] * (lofphi - rhs[c]);
+      double lofphi = A.sc.alpha * W.a[c] * pc - A.sc.beta * vcDiv(phi, W.b[0], W.b[1], W.b[2], st) * dxinv;
+      phi[c] = pc - W.lam[c] * (lofphi - rhs[c]);
     } else if (A.sc.laplacian) {
       double lphi = nbrSum(phi, st) * dxinv;
       phi[c] = A.sc.lambda * (rhs[c] - lphi);
@@ -500,57 +509,56 @@ __device__ void blkRelax(const BottomArgs& A, double* phi, const double* rhs, in
 __device__ void blkOp(const BottomArgs& A, double* r, double* phi, const double* rhs, int mode) {
   blkGhost(A, phi);
   const double dxinv = A.sc.dxinv;
-  blkCells(A.L, [&](const BoxDesc& bd, int64_t c, int i, int j, int k) {
-    const Stencil st = stencil(bd, i, j, k);
-    double pc = phi[c];
+  const BottomWork& W = A.W;
+  blkCells(A, [&](int q) {
+    const Stencil st = slotStencil(W, q);
+    double pc = phi[q];
     if (A.vc) {
-      double lofphi = A.sc.alpha * A.a[c] * pc - A.sc.beta * vcDiv(phi, A.b0, A.b1, A.b2, st) * dxinv;
-      r[c] = mode == 0 ? rhs[c] - lofphi : lofphi;
+      double lofphi = A.sc.alpha * W.a[q] * pc - A.sc.beta * vcDiv(phi, W.b[0], W.b[1], W.b[2], st) * dxinv;
+      r[q] = mode == 0 ? rhs[q] - lofphi : lofphi;
     } else {
       double lap = (nbrSum(phi, st) - 6.0 * pc) * dxinv;
-      r[c] = mode == 0 ? -(A.sc.alpha * pc) - A.sc.beta * lap + rhs[c] : A.sc.alpha * pc + A.sc.beta * lap;
+      r[q] = mode == 0 ? -(A.sc.alpha * pc) - A.sc.beta * lap + rhs[q] : A.sc.alpha * pc + A.sc.beta * lap;
     }
   });
 }
 
 __device__ void blkPrecond(const BottomArgs& A, double* out, const double* in) {
-  blkCells(A.L, [&](const BoxDesc&, int64_t c, int, int, int) { out[c] = A.vc ? in[c] * A.lam[c] : in[c] * A.mult; });
+  blkCells(A, [&](int q) { out[q] = A.vc ? in[q] * A.W.lam[q] : in[q] * A.mult; });
   blkRelax(A, out, in, 2);
 }
 
 __device__ double blkDot(const BottomArgs& A, const double* x, const double* y, bool pencil) {
-  const LevelDev& L = A.L;
-  for (int b = threadIdx.x; b < L.nbox; b += blockDim.x) {
-    const BoxDesc bd = L.boxes[b];
+  extern __shared__ double spart[];
+  const BottomWork& W = A.W;
+  for (int b = threadIdx.x; b < W.nbox; b += blockDim.x) {
+    const BoxDesc bd = A.boxes[b];
+    const int nx = bd.hi[0] - bd.lo[0] + 1, ny = bd.hi[1] - bd.lo[1] + 1, nz = bd.hi[2] - bd.lo[2] + 1;
+    const int s0 = W.boxStart[b];
     double s = 0.0;
     if (!pencil) {
-      for (int k = bd.lo[2]; k <= bd.hi[2]; ++k)
-        for (int j = bd.lo[1]; j <= bd.hi[1]; ++j)
-          for (int i = bd.lo[0]; i <= bd.hi[0]; ++i) {
-            int64_t c = cellIndex(bd, i, j, k);
-            s += x[c] * y[c];
-          }
+      for (int q = s0; q < s0 + nx * ny * nz; ++q) s += x[q] * y[q];
     } else {
       // sumPow(p=2): per-x accumulation over pencils, then across x.
-      for (int i = bd.lo[0]; i <= bd.hi[0]; ++i) {
+      for (int i = 0; i < nx; ++i) {
         double acc = 0.0;
         bool first = true;
-        for (int k = bd.lo[2]; k <= bd.hi[2]; ++k)
-          for (int j = bd.lo[1]; j <= bd.hi[1]; ++j) {
-            double v = x[cellIndex(bd, i, j, k)];
+        for (int k = 0; k < nz; ++k)
+          for (int j = 0; j < ny; ++j) {
+            double v = x[s0 + i + nx * (j + ny * k)];
             acc = first ? v * v : acc + v * v;
             first = false;
           }
-        s = (i == bd.lo[0]) ? acc : s + acc;
+        s = (i == 0) ? acc : s + acc;
       }
     }
-    A.part[b] = s;
+    spart[b] = s;
   }
   __syncthreads();
   __shared__ double tot;
   if (threadIdx.x == 0) {
     double v = 0.0;
-    for (int b = 0; b < L.nbox; ++b) v += A.part[b];
+    for (int b = 0; b < W.nbox; ++b) v += spart[b];
     tot = v;
   }
   __syncthreads();
@@ -561,16 +569,15 @@ __device__ double blkDot(const BottomArgs& A, const double* x, const double* y, 
 
 __device__ double blkNorm(const BottomArgs& A, const double* x) { return sqrt(blkDot(A, x, x, true)); }
 
-__global__ void k_bottom(BottomArgs A) {
-  const LevelDev& L = A.L;
+__device__ void bicgstab(const BottomArgs& A) {
+  const BottomWork& W = A.W;
+  const int nc = W.nv + W.ng;
   auto zeroAll = [&](double* x) {
-    for (int64_t q = threadIdx.x; q < L.nelem; q += blockDim.x) x[q] = 0.0;
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) x[q] = 0.0;
     __syncthreads();
   };
-  auto copyValid = [&](double* d, const double* s) { blkCells(L, [&](const BoxDesc&, int64_t c, int, int, int) { d[c] = s[c]; }); };
-  auto incrV = [&](double* y, const double* x, double sc) {
-    blkCells(L, [&](const BoxDesc&, int64_t c, int, int, int) { y[c] = y[c] + x[c] * sc; });
-  };
+  auto copyValid = [&](double* d, const double* s) { blkCells(A, [&](int q) { d[q] = s[q]; }); };
+  auto incrV = [&](double* y, const double* x, double sc) { blkCells(A, [&](int q) { y[q] = y[q] + x[q] * sc; }); };
   zeroAll(A.r);
   blkOp(A, A.r, A.phi, A.rhs, 0);
   copyValid(A.rt, A.r);
@@ -598,7 +605,7 @@ __global__ void k_bottom(BottomArgs A) {
     rho[1] = blkDot(A, A.rt, A.r, false);
     if (rho[1] == 0.0) {
       incrV(A.phi, A.e, 1.0);
-      if (threadIdx.x == 0) A.status[0] = 2, A.status[1] = iter;
+      if (threadIdx.x == 0) W.status[0] = 2, W.status[1] = iter;
       return;
     }
     if (init) {
@@ -606,7 +613,7 @@ __global__ void k_bottom(BottomArgs A) {
       init = false;
     } else {
       beta[1] = (rho[1] / rho[2]) * (alpha[1] / omega[1]);
-      blkCells(L, [&](const BoxDesc&, int64_t c, int, int, int) { A.p[c] = A.p[c] * beta[1]; });
+      blkCells(A, [&](int q) { A.p[q] = A.p[q] * beta[1]; });
       incrV(A.p, A.v, -beta[1] * omega[1]);
       incrV(A.p, A.r, 1.0);
     }
@@ -645,7 +652,7 @@ __global__ void k_bottom(BottomArgs A) {
         recount = 0;
         incrV(A.phi, A.e, 1.0);
         if (restarts == A.numRestarts) {
-          if (threadIdx.x == 0) A.status[0] = 3, A.status[1] = iter;
+          if (threadIdx.x == 0) W.status[0] = 3, W.status[1] = iter;
           return;
         }
         blkOp(A, A.r, A.phi, A.rhs, 0);
@@ -664,7 +671,25 @@ __global__ void k_bottom(BottomArgs A) {
     }
   }
   incrV(A.phi, A.e, 1.0);
-  if (threadIdx.x == 0) A.status[0] = status, A.status[1] = iter;
+  if (threadIdx.x == 0) W.status[0] = status, W.status[1] = iter;
+}
+
+__global__ void __launch_bounds__(1024) k_bottom(BottomArgs A) {
+  const BottomWork& W = A.W;
+  const int nc = W.nv + W.ng;
+  for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+    A.phi[q] = A.phiFab[W.fab[q]];
+    A.rhs[q] = A.rhsFab[W.fab[q]];
+  }
+  __syncthreads();
+  bicgstab(A);
+  __syncthreads();
+  for (int q = threadIdx.x; q < W.nv; q += blockDim.x) A.phiFab[W.fab[q]] = A.phi[q];
+}
+
+__global__ void k_gather_slots(const int* fab, int n, const double* src, double* dst) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) dst[q] = src[fab[q]];
 }
 
 }  // namespace
@@ -690,16 +715,18 @@ Scal scalars(double dx, double alpha, double beta, int vc) {
 }  // namespace
 
 template <class T>
-void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s) {
-  int n = withCF ? L.nGhost : L.nExchBC;
-  int ncell = withCF ? L.nCellsGhost : L.nCellsExchBC;
+void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par) {
+  const int n = withCF ? L.nGhost : L.nExchBC;
   if (n == 0) return;
+  const bool half = par >= 0;
+  const int ncell = half ? (withCF ? L.nSlotsGhost : L.nSlotsExchBC) : (withCF ? L.nCellsGhost : L.nCellsExchBC);
   const double dx = L.dx, dxc = L.dxCrse;
   T c1 = T(2 * (dxc - dx) / (dxc + dx));
   T c2 = T(-(dxc - dx) / (dxc + 3 * dx));
   T flin = T(1 - 2 * dx / (dx + dxc));
-  k_ghost<T><<<(ncell + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(L.boxes, L.ghost, L.ghostStart,
-                                                                                L.ghostBlock, n, ncell, f, c1, c2, flin);
+  k_ghost<T><<<(ncell + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(
+      L.boxes, L.ghost, half ? L.slotStart : L.ghostStart, half ? L.slotBlock : L.ghostBlock, n, ncell,
+      half ? par : -1, f, c1, c2, flin);
   CMG_LAUNCHED("ghostFill");
 }
 
@@ -707,7 +734,7 @@ template <class T>
 void zeroCovered(const LevelDev& L, T* f, cudaStream_t s) {
   if (L.nZero == 0) return;
   k_ghost<T><<<(L.nCellsZero + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(
-      L.boxes, L.zero, L.zeroStart, L.zeroBlock, L.nZero, L.nCellsZero, f, T(0), T(0), T(0));
+      L.boxes, L.zero, L.zeroStart, L.zeroBlock, L.nZero, L.nCellsZero, -1, f, T(0), T(0), T(0));
   CMG_LAUNCHED("zeroCovered");
 }
 
@@ -836,16 +863,12 @@ long long launchCount() { return g_launches.load(std::memory_order_relaxed); }
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
                  double eps, double metric, cudaStream_t s) {
   BottomArgs A;
-  A.L = L;
+  A.W = w;
+  A.boxes = L.boxes;
   A.sc = scalars(L.dx, c.alpha, c.beta, c.vc);
   A.vc = c.vc;
-  A.a = c.a;
-  A.b0 = c.b[0];
-  A.b1 = c.b[1];
-  A.b2 = c.b[2];
-  A.lam = c.lambda;
-  A.phi = phi;
-  A.rhs = rhs;
+  A.phiFab = phi;
+  A.rhsFab = rhs;
   A.r = w.v[0];
   A.rt = w.v[1];
   A.e = w.v[2];
@@ -854,7 +877,8 @@ void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<d
   A.st = w.v[5];
   A.t = w.v[6];
   A.v = w.v[7];
-  A.part = w.part;
+  A.phi = w.v[8];
+  A.rhs = w.v[9];
   A.eps = eps;
   A.metric = metric;
   A.reps = 1.0e-12;
@@ -864,13 +888,19 @@ void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<d
   A.numRestarts = 5;
   // AMRPoissonOp::preCond multiplier (AMRPoissonOp.cpp:304-329).
   A.mult = 1.0 / (c.alpha - 2.0 * 3 * c.beta / (L.dx * L.dx));
-  A.status = w.status;
-  k_bottom<<<1, 1024, 0, s>>>(A);
+  k_bottom<<<1, 1024, w.nbox * sizeof(double), s>>>(A);
   CMG_LAUNCHED("bottomSolve");
 }
 
+void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream_t s) {
+  const int n = w.nv + w.ng;
+  if (n == 0) return;
+  k_gather_slots<<<(n + 255) / 256, 256, 0, s>>>(w.fab, n, fab, dst);
+  CMG_LAUNCHED("gatherSlots");
+}
+
 #define CMG_INST(T)                                                                                       \
-  template void ghostFill<T>(const LevelDev&, T*, bool, cudaStream_t);                                     \
+  template void ghostFill<T>(const LevelDev&, T*, bool, cudaStream_t, int);                                \
   template void zeroCovered<T>(const LevelDev&, T*, cudaStream_t);                                         \
   template void gsrb<T>(const LevelDev&, T*, const T*, const Coef<T>&, int, cudaStream_t);                 \
   template void residual<T>(const LevelDev&, T*, const T*, const T*, const Coef<T>&, cudaStream_t);        \

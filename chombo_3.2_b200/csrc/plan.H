@@ -27,6 +27,8 @@ struct LevelPlan {
   // task t), so one ghost kernel can spread cells evenly over thread blocks.
   std::vector<int> ghostStart;
   std::vector<int> ghostBlock;         // task holding cell b*GHOST_THREADS
+  // The same over one-colour slots: ceil(nx/2) per task row.
+  std::vector<int> slotStart, slotBlock;
   std::vector<GhostTask> zeroCovered;  // covered by the next finer level
   std::vector<int> zeroStart;          // cumulative cell counts of zeroCovered
   std::vector<int> zeroBlock;
@@ -45,6 +47,20 @@ struct LevelPlan {
   std::vector<RefluxCoarseTerm> rfCoarse;
   std::vector<RefluxFineGroup> rfFine;
 };
+
+// Compact indexing of the bottom level for the one-block BiCGStab: valid
+// cells first (box by box, x fastest, the reference's summation order), then
+// the face-ghost slots the 7-point stencil reads.  Every vector of the bottom
+// solve lives in this compact space, small enough to stay in L1.
+struct BottomPlan {
+  int nv = 0, ng = 0;            // valid cells, ghost slots
+  std::vector<int> fab;          // FAB element index of every slot (nv + ng)
+  std::vector<int> nb;           // 6 neighbour slots per valid cell (+x,-x,+y,-y,+z,-z)
+  std::vector<int> color[2];     // valid slots of each colour
+  std::vector<int> boxStart;     // first valid slot of each box (nbox + 1)
+  std::vector<int> gsrc, gkind;  // per ghost slot: source slot, 0 copy / 1 Dirichlet / 2 untouched
+};
+void buildBottom(const LevelPlan& L, BottomPlan& B);
 
 // Layout and ghost/chunk plans of one level (AMR level or multigrid depth).
 // dxCrse > 0 enables homogeneous coarse-fine ghost tasks on CF faces.

@@ -4,6 +4,7 @@
 
 #include <map>
 #include <stdexcept>
+#include <unordered_map>
 
 namespace cmg {
 
@@ -153,6 +154,12 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     L.ghostStart.push_back(L.ghostStart.back() + (int)c);
   }
   L.ghostBlock = blockTasks(L.ghostStart);
+  L.slotStart.assign(1, 0);
+  for (const GhostTask& t : L.ghost) {
+    int64_t c = (int64_t)((t.hi[0] - t.lo[0] + 2) / 2) * (t.hi[1] - t.lo[1] + 1) * (t.hi[2] - t.lo[2] + 1);
+    L.slotStart.push_back(L.slotStart.back() + (int)c);
+  }
+  L.slotBlock = blockTasks(L.slotStart);
 
   L.chunksAll.clear();
   L.chunksColor[0].clear();
@@ -588,6 +595,76 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
       for (auto& g : pr.second) C.rfFine.push_back(g);
       C.rfCells.push_back(rc);
     }
+  }
+}
+
+void buildBottom(const LevelPlan& L, BottomPlan& B) {
+  B = BottomPlan();
+  std::unordered_map<int64_t, int> slot;  // FAB element -> slot
+  const size_t nbox = L.boxes.size();
+  B.boxStart.assign(nbox + 1, 0);
+  for (size_t b = 0; b < nbox; ++b) {
+    const Box& bx = L.grids[b];
+    B.boxStart[b] = (int)B.fab.size();
+    for (int k = bx.lo[2]; k <= bx.hi[2]; ++k)
+      for (int j = bx.lo[1]; j <= bx.hi[1]; ++j)
+        for (int i = bx.lo[0]; i <= bx.hi[0]; ++i) {
+          int64_t e = cellIndex(L.boxes[b], i, j, k);
+          slot[e] = (int)B.fab.size();
+          B.fab.push_back((int)e);
+        }
+  }
+  B.boxStart[nbox] = (int)B.fab.size();
+  B.nv = (int)B.fab.size();
+  B.nb.resize(6 * (size_t)B.nv);
+  static const int dirs[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  for (size_t b = 0; b < nbox; ++b) {
+    const Box& bx = L.grids[b];
+    for (int k = bx.lo[2]; k <= bx.hi[2]; ++k)
+      for (int j = bx.lo[1]; j <= bx.hi[1]; ++j)
+        for (int i = bx.lo[0]; i <= bx.hi[0]; ++i) {
+          int q = slot[cellIndex(L.boxes[b], i, j, k)];
+          B.color[((i + j + k) & 1)].push_back(q);
+          for (int d = 0; d < 6; ++d) {
+            int64_t e = cellIndex(L.boxes[b], i + dirs[d][0], j + dirs[d][1], k + dirs[d][2]);
+            auto it = slot.find(e);
+            if (it == slot.end()) {
+              it = slot.emplace(e, (int)B.fab.size()).first;
+              B.fab.push_back((int)e);
+            }
+            B.nb[6 * (size_t)q + d] = it->second;
+          }
+        }
+  }
+  B.ng = (int)B.fab.size() - B.nv;
+  B.gsrc.assign(B.ng, 0);
+  B.gkind.assign(B.ng, 2);
+  // Ghost tasks of the level (exchange copies, then Dirichlet faces), in
+  // task order so that a slot written twice keeps the last writer.
+  for (const GhostTask& t : L.ghost) {
+    const BoxDesc& db = L.boxes[t.dst];
+    for (int k = t.lo[2]; k <= t.hi[2]; ++k)
+      for (int j = t.lo[1]; j <= t.hi[1]; ++j)
+        for (int i = t.lo[0]; i <= t.hi[0]; ++i) {
+          auto it = slot.find(cellIndex(db, i, j, k));
+          if (it == slot.end() || it->second < B.nv) continue;
+          const int g = it->second - B.nv;
+          int64_t src;
+          if (t.kind == G_COPY) {
+            src = cellIndex(L.boxes[t.src], i, j, k);
+            B.gkind[g] = 0;
+          } else if (t.kind == G_BC) {
+            int e[3] = {0, 0, 0};
+            e[t.dir] = -t.side;
+            src = cellIndex(db, i + e[0], j + e[1], k + e[2]);
+            B.gkind[g] = 1;
+          } else {
+            throw std::runtime_error("cmg: coarse-fine ghost task on the bottom level");
+          }
+          auto s2 = slot.find(src);
+          if (s2 == slot.end() || s2->second >= B.nv) throw std::runtime_error("cmg: bottom ghost source not valid");
+          B.gsrc[g] = s2->second;
+        }
   }
 }
 

@@ -100,7 +100,7 @@ class Solver {
   void relaxMG(int d, double* phi, const double* rhs, int n);
   void relaxLevel(const LevelDev& L, double cells, const Coef<double>& c, double* phi, const double* rhs, int n,
                   int cls);
-  void fill(const LevelDev& L, double* f, bool withCF);
+  void fill(const LevelDev& L, double* f, bool withCF, int par = -1);
   void amrResidualLevel(int ilev, int lmax, std::vector<double*>& res, std::vector<double*>& phi,
                         std::vector<double*>& rhs);
   double computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);

@@ -81,6 +81,10 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
   d.nGhost = (int)p.ghost.size();
   d.ghostStart = upload(bufs_, p.ghostStart, s_);
   d.ghostBlock = upload(bufs_, p.ghostBlock, s_);
+  d.slotStart = upload(bufs_, p.slotStart, s_);
+  d.slotBlock = upload(bufs_, p.slotBlock, s_);
+  d.nSlotsExchBC = p.slotStart.empty() ? 0 : p.slotStart[p.nExchBC];
+  d.nSlotsGhost = p.slotStart.empty() ? 0 : p.slotStart.back();
   d.nCellsExchBC = p.ghostStart.empty() ? 0 : p.ghostStart[p.nExchBC];
   d.nCellsGhost = p.ghostStart.empty() ? 0 : p.ghostStart.back();
   d.zero = upload(bufs_, p.zeroCovered, s_);
@@ -174,9 +178,29 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), des
       mgf_[d].lambda = alloc(n);
     }
   }
+  // Bottom solve in the compact slot space of the deepest level.
   const LevelPlan& bl = mg_.empty() ? amr_[0] : mg_.back();
-  for (int k = 0; k < 8; ++k) bottom_.v[k] = alloc(bl.nelem);
-  bottom_.part = alloc(bl.boxes.size() + 1);
+  BottomPlan bp;
+  buildBottom(bl, bp);
+  const size_t nc = (size_t)bp.nv + bp.ng;
+  bottom_.nv = bp.nv;
+  bottom_.ng = bp.ng;
+  bottom_.nbox = (int)bl.boxes.size();
+  bottom_.fab = upload(bufs_, bp.fab, s_);
+  bottom_.nb = upload(bufs_, bp.nb, s_);
+  for (int c = 0; c < 2; ++c) {
+    bottom_.col[c] = upload(bufs_, bp.color[c], s_);
+    bottom_.ncol[c] = (int)bp.color[c].size();
+  }
+  bottom_.boxStart = upload(bufs_, bp.boxStart, s_);
+  bottom_.gsrc = upload(bufs_, bp.gsrc, s_);
+  bottom_.gkind = upload(bufs_, bp.gkind, s_);
+  for (int k = 0; k < 10; ++k) bottom_.v[k] = alloc(nc);
+  if (desc.vc) {
+    bottom_.a = alloc(nc);
+    for (int d = 0; d < 3; ++d) bottom_.b[d] = alloc(nc);
+    bottom_.lam = alloc(nc);
+  }
   bufs_.emplace_back(new DevBuf(4 * sizeof(int)));
   bottom_.status = (int*)bufs_.back()->p;
   dNorm_ = alloc(1);
@@ -403,6 +427,12 @@ void Solver::finalizeCoefficients() {
     auto lam = computeLambda(mg_[d].grids, a, b, desc_.alpha, desc_.beta, mg_[d].dx);
     scatterValid(mg_[d], mgDev_[d], mgf_[d].lambda, lam.data(), false, -1);
   }
+  // Compact copies of the bottom level's coefficients for the bottom solve.
+  Coef<double> cb = coefMG((int)mg_.size());
+  gatherSlots(bottom_, cb.a, bottom_.a, s_);
+  for (int k = 0; k < 3; ++k) gatherSlots(bottom_, cb.b[k], bottom_.b[k], s_);
+  gatherSlots(bottom_, cb.lambda, bottom_.lam, s_);
+  ck(cudaStreamSynchronize(s_), "bottom coefficients");
 }
 
 Coef<double> Solver::coefAMR(int l) const {
@@ -453,7 +483,7 @@ void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<double>& c, 
   const double bytes = cells * 8.0 * (c.vc ? 6.0 : 2.0);
   for (int it = 0; it < n; ++it)
     for (int color = 0; color <= 1; ++color) {
-      fill(L, phi, true);
+      fill(L, phi, true, 1 - color);
       timed(cls, bytes, [&]() { gsrb(L, phi, rhs, c, color, s_); });
     }
 }
@@ -469,11 +499,12 @@ void Solver::relaxMG(int d, double* phi, const double* rhs, int n) {
   relaxLevel(mgDev_[d - 1], (double)mg_[d - 1].grids.numCells(), coefMG(d), phi, rhs, n, P_RELAX);
 }
 
-// Ghost fill, timed as its own class: every ghost cell written once and
-// its source read once (16 bytes per cell).
-void Solver::fill(const LevelDev& L, double* f, bool withCF) {
-  const double bytes = 16.0 * (withCF ? L.nCellsGhost : L.nCellsExchBC);
-  timed(P_GHOST, bytes, [&]() { ghostFill(L, f, withCF, s_); });
+// Ghost fill, timed as its own class: every ghost cell filled written once
+// and its source read once (16 bytes per cell; half the cells for a
+// one-colour fill).
+void Solver::fill(const LevelDev& L, double* f, bool withCF, int par) {
+  const double bytes = (par >= 0 ? 8.0 : 16.0) * (withCF ? L.nCellsGhost : L.nCellsExchBC);
+  timed(P_GHOST, bytes, [&]() { ghostFill(L, f, withCF, s_, par); });
 }
 
 // AMRMultiGrid::computeAMRResidualLevel (AMRMultiGrid.H:836-892).

@@ -71,13 +71,42 @@ enum GhostKind {
   G_ZERO = 4       // dst(cell) = 0 (covered cells before a norm)
 };
 
-// Ghost cells handled by one thread block of the ghost kernel.
-enum { GHOST_THREADS = 256 };
+// Ghost cells handled by one thread block of the ghost kernel (each thread
+// takes GHOST_PER_THREAD of them, GHOST_THREADS apart).
+enum { GHOST_THREADS = 256, GHOST_PER_THREAD = 1, GHOST_PER_BLOCK = GHOST_THREADS * GHOST_PER_THREAD };
 
 struct GhostTask {
   int kind, dst, src, dir, side;  // side = -1 (low) or +1 (high)
   int lo[3], hi[3];
 };
+
+// One ghost cell of a level's ghost fill, as element indices: dst = src1
+// (s2 == -1, exchange copy), dst = 2*0 - src1 (s2 == -2, homogeneous
+// Dirichlet face), dst = flin*src1 (s2 == -3, linear coarse-fine ghost of a
+// one-cell-wide box), dst = c1*src1 + c2*s2 (s2 >= 0, quadratic coarse-fine).
+struct GhostCell {
+  int dst, s1, s2;
+};
+
+// Device form of a ghost task: the task plus copies of its destination and
+// source box descriptors, so that a thread reaches its data after a single
+// table load.
+struct GhostTaskDev {
+  BoxDesc dst, src;
+  int kind, dir, side;
+  int lo[3], hi[3];
+  int ax;  // one-colour enumeration steps by 2 along this axis (first with extent > 1)
+};
+
+// Slots of a task in a one-colour fill: ceil(n_ax / 2) per line along ax.
+CMG_HD int64_t colourSlots(const int lo[3], const int hi[3], int ax) {
+  int64_t n = 1;
+  for (int d = 0; d < 3; ++d) n *= d == ax ? (hi[d] - lo[d] + 2) / 2 : (hi[d] - lo[d] + 1);
+  return n;
+}
+CMG_HD int parityAxis(const int lo[3], const int hi[3]) {
+  return hi[0] > lo[0] ? 0 : hi[1] > lo[1] ? 1 : hi[2] > lo[2] ? 2 : 0;
+}
 
 // Work decomposition of a box list into fixed-size chunks of cells (or of
 // one colour's cells for red-black sweeps): chunk c covers cells

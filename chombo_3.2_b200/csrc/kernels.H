@@ -16,15 +16,17 @@ struct LevelDev {
   const BoxDesc* boxes = nullptr;
   int nbox = 0;
   int64_t nelem = 0;
-  const GhostTask* ghost = nullptr;
+  const GhostTaskDev* ghost = nullptr;
   int nExchBC = 0, nGhost = 0;
   const int* ghostStart = nullptr;       // cumulative cell counts (nGhost + 1)
-  const int* ghostBlock = nullptr;       // first task of each GHOST_THREADS cells
+  const int* ghostBlock = nullptr;       // first task of each GHOST_PER_BLOCK cells
   const int* slotStart = nullptr;        // the same over one-colour slots
   const int* slotBlock = nullptr;
   int nSlotsExchBC = 0, nSlotsGhost = 0;
   int nCellsExchBC = 0, nCellsGhost = 0;
-  const GhostTask* zero = nullptr;
+  const GhostCell* gcells = nullptr;     // flat ghost-cell lists (LevelPlan::gcells)
+  int gcStart[2] = {0, 0}, gcExch[2] = {0, 0}, gcCF[2] = {0, 0};
+  const GhostTaskDev* zero = nullptr;
   int nZero = 0;
   const int* zeroStart = nullptr;
   const int* zeroBlock = nullptr;

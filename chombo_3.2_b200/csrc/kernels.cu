@@ -52,61 +52,117 @@ __device__ __forceinline__ bool colorCell(const BoxDesc& b, int q, int color, in
 // Exchange copies (BoxLayoutData local copy), homogeneous Dirichlet faces
 // (BCFunc.cpp:25-32,294-354: ghost = 2*0 - near), homogeneous quadratic and
 // linear coarse-fine ghosts (InterpF.ChF:435-494) and zeroing.
-// One thread per ghost cell across all tasks; the task of cell g is found by
-// binary search in the cumulative cell counts, between the tasks holding the
-// first cells of this block and of the next (blockTask).  par >= 0 fills only
-// the ghost cells of colour par ((i+j+k) & 1 == par): a colour pass reads no
-// ghost of its own colour, so the fill before it needs only the other one.
-// Then each task row offers ceil(nx/2) slots and `start` counts slots.
+// Each thread takes GHOST_PER_THREAD ghost cells of its block's range; the
+// task of cell g is found by binary search in the cumulative cell counts,
+// between the tasks holding the first cells of this block and of the next
+// (blockTask).  The cells' target and source indices are resolved first and
+// their loads issued together.  par >= 0 fills only the ghost cells of colour
+// par ((i+j+k) & 1 == par): a colour pass reads no ghost of its own colour,
+// so the fill before it needs only the other one; then a task offers
+// colourSlots() slots, stepping by two along its parity axis.
 template <class T>
-__global__ void k_ghost(const BoxDesc* boxes, const GhostTask* tasks, const int* start, const int* blockTask,
-                        int ntask, int ncell, int par, T* f, T c1, T c2, T flin) {
-  int g0 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g0 >= ncell) return;
-  int lo = blockTask[blockIdx.x], hi = min(blockTask[blockIdx.x + 1], ntask - 1);
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (start[mid] <= g0)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  const GhostTask t = tasks[lo];
-  const BoxDesc db = boxes[t.dst];
-  int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1;
-  int q = g0 - start[lo], i, j, k;
-  if (par < 0) {
-    i = t.lo[0] + q % nx;
-    int r = q / nx;
-    j = t.lo[1] + r % ny;
-    k = t.lo[2] + r / ny;
-  } else {
-    const int hx = (nx + 1) >> 1;
-    int r = q / hx;
-    j = t.lo[1] + r % ny;
-    k = t.lo[2] + r / ny;
-    i = t.lo[0] + ((par - t.lo[0] - j - k) & 1) + 2 * (q % hx);
-    if (i > t.hi[0]) return;
-  }
-  int64_t g = cellIndex(db, i, j, k);
-  if (t.kind == G_COPY) {
-    f[g] = f[cellIndex(boxes[t.src], i, j, k)];
-  } else if (t.kind == G_ZERO) {
-    f[g] = T(0);
-  } else {
-    int e[3] = {0, 0, 0};
-    e[t.dir] = -t.side;  // one cell inward
-    int64_t in1 = cellIndex(db, i + e[0], j + e[1], k + e[2]);
-    if (t.kind == G_BC) {
-      T zero = T(0);
-      f[g] = T(2) * zero - f[in1];
-    } else if (t.kind == G_CFLIN) {
-      f[g] = flin * f[in1];
+__global__ void __launch_bounds__(GHOST_THREADS) k_ghost(const GhostTaskDev* tasks, const int* start,
+                                                         const int* blockTask, int ntask, int ncell, int par, T* f,
+                                                         T c1, T c2, T flin) {
+  const int b0 = blockTask[blockIdx.x], b1 = min(blockTask[blockIdx.x + 1], ntask - 1);
+  int64_t dst[GHOST_PER_THREAD], s1[GHOST_PER_THREAD], s2[GHOST_PER_THREAD];
+  int kind[GHOST_PER_THREAD];
+#pragma unroll
+  for (int u = 0; u < GHOST_PER_THREAD; ++u) {
+    kind[u] = -1;
+    dst[u] = s1[u] = s2[u] = 0;
+    const int g0 = blockIdx.x * GHOST_PER_BLOCK + u * GHOST_THREADS + threadIdx.x;
+    if (g0 >= ncell) continue;
+    int lo = b0, hi = b1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (start[mid] <= g0)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const GhostTaskDev& t = tasks[lo];
+    int q = g0 - start[lo], c[3];
+    if (par < 0) {
+      const int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1;
+      c[0] = t.lo[0] + q % nx;
+      int r = q / nx;
+      c[1] = t.lo[1] + r % ny;
+      c[2] = t.lo[2] + r / ny;
     } else {
-      int64_t in2 = cellIndex(db, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
-      f[g] = c1 * f[in1] + c2 * f[in2];
+      const int a = t.ax, d1 = a == 0 ? 1 : 0, d2 = a == 2 ? 1 : 2;
+      const int ha = (t.hi[a] - t.lo[a] + 2) >> 1, n1 = t.hi[d1] - t.lo[d1] + 1;
+      int r = q / ha;
+      c[d1] = t.lo[d1] + r % n1;
+      c[d2] = t.lo[d2] + r / n1;
+      c[a] = t.lo[a] + ((par - t.lo[a] - c[d1] - c[d2]) & 1) + 2 * (q % ha);
+      if (c[a] > t.hi[a]) continue;
+    }
+    kind[u] = t.kind;
+    dst[u] = cellIndex(t.dst, c[0], c[1], c[2]);
+    if (t.kind == G_COPY) {
+      s1[u] = cellIndex(t.src, c[0], c[1], c[2]);
+    } else if (t.kind != G_ZERO) {
+      int e[3] = {0, 0, 0};
+      e[t.dir] = -t.side;  // one cell inward
+      s1[u] = cellIndex(t.dst, c[0] + e[0], c[1] + e[1], c[2] + e[2]);
+      s2[u] = t.kind == G_CFQUAD ? cellIndex(t.dst, c[0] + 2 * e[0], c[1] + 2 * e[1], c[2] + 2 * e[2]) : s1[u];
     }
   }
+  T v1[GHOST_PER_THREAD], v2[GHOST_PER_THREAD];
+#pragma unroll
+  for (int u = 0; u < GHOST_PER_THREAD; ++u) {
+    if (kind[u] > 0 && kind[u] != G_ZERO) v2[u] = f[s2[u]];
+    if (kind[u] >= 0 && kind[u] != G_ZERO) v1[u] = f[s1[u]];
+  }
+#pragma unroll
+  for (int u = 0; u < GHOST_PER_THREAD; ++u) {
+    const int k = kind[u];
+    if (k < 0) continue;
+    T out;
+    if (k == G_COPY) {
+      out = v1[u];
+    } else if (k == G_ZERO) {
+      out = T(0);
+    } else if (k == G_BC) {
+      T zero = T(0);
+      out = T(2) * zero - v1[u];
+    } else if (k == G_CFLIN) {
+      out = flin * v1[u];
+    } else {
+      out = c1 * v1[u] + c2 * v2[u];
+    }
+    f[dst[u]] = out;
+  }
+}
+
+// Ghost fill from the flat per-cell lists: entries [a0, a1) then [b0, b1),
+// one thread each, no table walk between a thread and its data.
+template <class T>
+__global__ void __launch_bounds__(GHOST_THREADS) k_ghostcells(const GhostCell* __restrict__ e, int a0, int a1,
+                                                              int b0, int b1, T* f, T c1, T c2, T flin) {
+  int q = blockIdx.x * GHOST_THREADS + threadIdx.x;
+  const int na = a1 - a0;
+  if (q < na)
+    q += a0;
+  else if (q - na < b1 - b0)
+    q = q - na + b0;
+  else
+    return;
+  const GhostCell g = e[q];
+  const T v1 = f[g.s1];
+  T out;
+  if (g.s2 == -1) {
+    out = v1;
+  } else if (g.s2 == -2) {
+    T zero = T(0);
+    out = T(2) * zero - v1;
+  } else if (g.s2 == -3) {
+    out = flin * v1;
+  } else {
+    out = c1 * v1 + c2 * f[g.s2];
+  }
+  f[g.dst] = out;
 }
 
 // ---------------------------------------------------------------- stencils
@@ -716,25 +772,29 @@ Scal scalars(double dx, double alpha, double beta, int vc) {
 
 template <class T>
 void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par) {
-  const int n = withCF ? L.nGhost : L.nExchBC;
+  auto range = [&](int p, int& r0, int& r1) {
+    r0 = L.gcStart[p];
+    r1 = r0 + L.gcExch[p] + (withCF ? L.gcCF[p] : 0);
+  };
+  int a0, a1, b0 = 0, b1 = 0;
+  range(par >= 0 ? par : 0, a0, a1);
+  if (par < 0) range(1, b0, b1);
+  const int n = (a1 - a0) + (b1 - b0);
   if (n == 0) return;
-  const bool half = par >= 0;
-  const int ncell = half ? (withCF ? L.nSlotsGhost : L.nSlotsExchBC) : (withCF ? L.nCellsGhost : L.nCellsExchBC);
   const double dx = L.dx, dxc = L.dxCrse;
   T c1 = T(2 * (dxc - dx) / (dxc + dx));
   T c2 = T(-(dxc - dx) / (dxc + 3 * dx));
   T flin = T(1 - 2 * dx / (dx + dxc));
-  k_ghost<T><<<(ncell + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(
-      L.boxes, L.ghost, half ? L.slotStart : L.ghostStart, half ? L.slotBlock : L.ghostBlock, n, ncell,
-      half ? par : -1, f, c1, c2, flin);
+  k_ghostcells<T><<<(n + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(L.gcells, a0, a1, b0, b1, f, c1,
+                                                                                    c2, flin);
   CMG_LAUNCHED("ghostFill");
 }
 
 template <class T>
 void zeroCovered(const LevelDev& L, T* f, cudaStream_t s) {
   if (L.nZero == 0) return;
-  k_ghost<T><<<(L.nCellsZero + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(
-      L.boxes, L.zero, L.zeroStart, L.zeroBlock, L.nZero, L.nCellsZero, -1, f, T(0), T(0), T(0));
+  k_ghost<T><<<(L.nCellsZero + GHOST_PER_BLOCK - 1) / GHOST_PER_BLOCK, GHOST_THREADS, 0, s>>>(
+      L.zero, L.zeroStart, L.zeroBlock, L.nZero, L.nCellsZero, -1, f, T(0), T(0), T(0));
   CMG_LAUNCHED("zeroCovered");
 }
 

@@ -26,9 +26,13 @@ struct LevelPlan {
   // Cumulative cell counts of the ghost tasks (ghostStart[t] = first cell of
   // task t), so one ghost kernel can spread cells evenly over thread blocks.
   std::vector<int> ghostStart;
-  std::vector<int> ghostBlock;         // task holding cell b*GHOST_THREADS
-  // The same over one-colour slots: ceil(nx/2) per task row.
+  std::vector<int> ghostBlock;         // task holding cell b*GHOST_PER_BLOCK
+  // The same over one-colour slots (colourSlots per task).
   std::vector<int> slotStart, slotBlock;
+  // The ghost fill cell by cell: [colour 0 exchange+BC | colour 0 CF |
+  // colour 1 exchange+BC | colour 1 CF], each group in task order.
+  std::vector<GhostCell> gcells;
+  int gcStart[2] = {0, 0}, gcExch[2] = {0, 0}, gcCF[2] = {0, 0};
   std::vector<GhostTask> zeroCovered;  // covered by the next finer level
   std::vector<int> zeroStart;          // cumulative cell counts of zeroCovered
   std::vector<int> zeroBlock;
@@ -78,7 +82,7 @@ inline int64_t cellOf(const LevelPlan& L, int b, const IV& p) {
   return cellIndex(L.boxes[b], p[0], p[1], p[2]);
 }
 
-// blockTask[b] = task holding cell b*GHOST_THREADS for cumulative cell
+// blockTask[b] = task holding cell b*GHOST_PER_BLOCK for cumulative cell
 // counts `start` (one entry per block plus a last one = last task).
 std::vector<int> blockTasks(const std::vector<int>& start);
 

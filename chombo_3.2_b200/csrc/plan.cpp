@@ -64,7 +64,7 @@ std::vector<int> blockTasks(const std::vector<int>& start) {
   if (start.size() < 2) return bt;
   const int ntask = (int)start.size() - 1, ncell = start.back();
   int t = 0;
-  for (int64_t c = 0; c < ncell; c += GHOST_THREADS) {
+  for (int64_t c = 0; c < ncell; c += GHOST_PER_BLOCK) {
     while (start[t + 1] <= c) ++t;
     bt.push_back(t);
   }
@@ -154,11 +154,39 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     L.ghostStart.push_back(L.ghostStart.back() + (int)c);
   }
   L.ghostBlock = blockTasks(L.ghostStart);
-  L.slotStart.assign(1, 0);
-  for (const GhostTask& t : L.ghost) {
-    int64_t c = (int64_t)((t.hi[0] - t.lo[0] + 2) / 2) * (t.hi[1] - t.lo[1] + 1) * (t.hi[2] - t.lo[2] + 1);
-    L.slotStart.push_back(L.slotStart.back() + (int)c);
+  if (L.nelem >= ((int64_t)1 << 31)) throw std::runtime_error("cmg: level too large for 32-bit ghost indices");
+  L.gcells.clear();
+  auto emit = [&](const GhostTask& t, int par) {
+    const BoxDesc& db = L.boxes[t.dst];
+    for (int k = t.lo[2]; k <= t.hi[2]; ++k)
+      for (int j = t.lo[1]; j <= t.hi[1]; ++j)
+        for (int i = t.lo[0]; i <= t.hi[0]; ++i) {
+          if (((i + j + k) & 1) != par) continue;
+          GhostCell g;
+          g.dst = (int)cellIndex(db, i, j, k);
+          if (t.kind == G_COPY) {
+            g.s1 = (int)cellIndex(L.boxes[t.src], i, j, k);
+            g.s2 = -1;
+          } else {
+            int e[3] = {0, 0, 0};
+            e[t.dir] = -t.side;
+            g.s1 = (int)cellIndex(db, i + e[0], j + e[1], k + e[2]);
+            g.s2 = t.kind == G_BC ? -2 : t.kind == G_CFLIN ? -3
+                                   : (int)cellIndex(db, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
+          }
+          L.gcells.push_back(g);
+        }
+  };
+  for (int par = 0; par < 2; ++par) {
+    L.gcStart[par] = (int)L.gcells.size();
+    for (int t = 0; t < L.nExchBC; ++t) emit(L.ghost[t], par);
+    L.gcExch[par] = (int)L.gcells.size() - L.gcStart[par];
+    for (size_t t = L.nExchBC; t < L.ghost.size(); ++t) emit(L.ghost[t], par);
+    L.gcCF[par] = (int)L.gcells.size() - L.gcStart[par] - L.gcExch[par];
   }
+  L.slotStart.assign(1, 0);
+  for (const GhostTask& t : L.ghost)
+    L.slotStart.push_back(L.slotStart.back() + (int)colourSlots(t.lo, t.hi, parityAxis(t.lo, t.hi)));
   L.slotBlock = blockTasks(L.slotStart);
 
   L.chunksAll.clear();

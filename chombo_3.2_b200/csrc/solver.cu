@@ -76,7 +76,25 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
   d.boxes = upload(bufs_, p.boxes, s_);
   d.nbox = (int)p.boxes.size();
   d.nelem = p.nelem;
-  d.ghost = upload(bufs_, p.ghost, s_);
+  auto devTasks = [&](const std::vector<GhostTask>& v) {
+    std::vector<GhostTaskDev> out(v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+      const GhostTask& t = v[i];
+      GhostTaskDev& o = out[i];
+      o.dst = p.boxes[t.dst];
+      o.src = p.boxes[t.src];
+      o.kind = t.kind;
+      o.dir = t.dir;
+      o.side = t.side;
+      for (int k = 0; k < 3; ++k) {
+        o.lo[k] = t.lo[k];
+        o.hi[k] = t.hi[k];
+      }
+      o.ax = parityAxis(t.lo, t.hi);
+    }
+    return out;
+  };
+  d.ghost = upload(bufs_, devTasks(p.ghost), s_);
   d.nExchBC = p.nExchBC;
   d.nGhost = (int)p.ghost.size();
   d.ghostStart = upload(bufs_, p.ghostStart, s_);
@@ -87,7 +105,13 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
   d.nSlotsGhost = p.slotStart.empty() ? 0 : p.slotStart.back();
   d.nCellsExchBC = p.ghostStart.empty() ? 0 : p.ghostStart[p.nExchBC];
   d.nCellsGhost = p.ghostStart.empty() ? 0 : p.ghostStart.back();
-  d.zero = upload(bufs_, p.zeroCovered, s_);
+  d.zero = upload(bufs_, devTasks(p.zeroCovered), s_);
+  d.gcells = upload(bufs_, p.gcells, s_);
+  for (int c = 0; c < 2; ++c) {
+    d.gcStart[c] = p.gcStart[c];
+    d.gcExch[c] = p.gcExch[c];
+    d.gcCF[c] = p.gcCF[c];
+  }
   d.nZero = (int)p.zeroCovered.size();
   d.zeroStart = upload(bufs_, p.zeroStart, s_);
   d.zeroBlock = upload(bufs_, p.zeroBlock, s_);

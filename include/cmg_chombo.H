@@ -1,0 +1,308 @@
+// Chombo-side drop-in for the GPU solve: the API of AMRMultiGrid<LevelData<
+// FArrayBox>> with AMRPoissonOpFactory / VCAMRPoissonOp2Factory, implemented
+// over the C ABI of cmg.h (libcmg.so).  A Chombo 3.2 program switches
+//
+//     AMRPoissonOpFactory f;     f.define(domain, grids, refRatios, dx, bc, alpha, beta);
+//     AMRMultiGrid<LevelData<FArrayBox> > s;
+//     s.define(domain, f, &bottomSolver, numLevels);
+//     s.setSolverParameters(pre, post, bottom, numMG, iterMax, eps, hang, normThresh);
+//     s.solve(phi, rhs, numLevels - 1, 0);
+//
+// to the same calls on cmg_chombo::GpuAMRPoissonOpFactory and
+// cmg_chombo::GpuAMRMultiGrid (or GpuVCAMRPoissonOp2Factory), with the same
+// arguments, and gets the same valid-cell phi (FP64, identical operation
+// order; see the parity tests), the same m_exitStatus and the same residual
+// history.  The header needs the Chombo headers (serial, 3D, double) and is
+// compiled inside the Chombo program; link with -lcmg.
+//
+// Scope, each checked with MayDay::Error like the reference's own checks:
+//   - refinement ratio 2 between all levels, non-periodic domain, serial
+//     (every box local), one component;
+//   - homogeneous Dirichlet boundary conditions on the domain faces (the
+//     examples' ParseBC with value 0, order 1): the BCHolder argument is kept
+//     for signature compatibility and is not called;
+//   - the bottom solver must be a BiCGStabSolver (its device restatement runs
+//     with the reference's default parameters);
+//   - solve over all levels: l_base = 0 and l_max = numLevels - 1.
+// Only valid cells of phi are written; ghost cells are left as they were.
+#ifndef CMG_CHOMBO_H
+#define CMG_CHOMBO_H
+
+#include <vector>
+
+#include "BCFunc.H"
+#include "BiCGStabSolver.H"
+#include "DisjointBoxLayout.H"
+#include "FArrayBox.H"
+#include "FluxBox.H"
+#include "LevelData.H"
+#include "LinearSolver.H"
+#include "MayDay.H"
+#include "ProblemDomain.H"
+#include "RefCountedPtr.H"
+#include "cmg.h"
+
+namespace cmg_chombo {
+
+typedef LevelData<FArrayBox> LDF;
+
+// What an operator factory conveys to the solver.
+struct GpuOpDescription {
+  ProblemDomain coarseDomain;
+  Vector<DisjointBoxLayout> grids;
+  Vector<int> refRatios;
+  Real coarsedx = 0, alpha = 0, beta = 1;
+  int vc = 0;
+  Vector<RefCountedPtr<LDF> > aCoef;
+  Vector<RefCountedPtr<LevelData<FluxBox> > > bCoef;
+  bool defined = false;
+};
+
+// AMRPoissonOpFactory::define (AMRElliptic/AMRPoissonOp.H:535-541).
+class GpuAMRPoissonOpFactory {
+ public:
+  void define(const ProblemDomain& a_coarseDomain, const Vector<DisjointBoxLayout>& a_grids,
+              const Vector<int>& a_refRatios, const Real& a_coarsedx, BCHolder /*a_bc*/, Real a_alpha = 0.0,
+              Real a_beta = 1.0) {
+    m_d = GpuOpDescription();
+    m_d.coarseDomain = a_coarseDomain;
+    m_d.grids = a_grids;
+    m_d.refRatios = a_refRatios;
+    m_d.coarsedx = a_coarsedx;
+    m_d.alpha = a_alpha;
+    m_d.beta = a_beta;
+    m_d.vc = 0;
+    m_d.defined = true;
+  }
+  const GpuOpDescription& description() const { return m_d; }
+
+ private:
+  GpuOpDescription m_d;
+};
+
+// VCAMRPoissonOp2Factory::define (AMRElliptic/VCAMRPoissonOp2.H:278-286).
+// The coefficients are read when GpuAMRMultiGrid::define runs (the reference
+// computes its relaxation coefficient from them at the same point).
+class GpuVCAMRPoissonOp2Factory {
+ public:
+  void define(const ProblemDomain& a_coarseDomain, const Vector<DisjointBoxLayout>& a_grids,
+              const Vector<int>& a_refRatios, const Real& a_coarsedx, BCHolder /*a_bc*/, const Real& a_alpha,
+              Vector<RefCountedPtr<LDF> >& a_aCoef, const Real& a_beta,
+              Vector<RefCountedPtr<LevelData<FluxBox> > >& a_bCoef) {
+    m_d = GpuOpDescription();
+    m_d.coarseDomain = a_coarseDomain;
+    m_d.grids = a_grids;
+    m_d.refRatios = a_refRatios;
+    m_d.coarsedx = a_coarsedx;
+    m_d.alpha = a_alpha;
+    m_d.beta = a_beta;
+    m_d.vc = 1;
+    m_d.aCoef = a_aCoef;
+    m_d.bCoef = a_bCoef;
+    m_d.defined = true;
+  }
+  const GpuOpDescription& description() const { return m_d; }
+
+ private:
+  GpuOpDescription m_d;
+};
+
+// AMRMultiGrid<LevelData<FArrayBox>> (AMRElliptic/AMRMultiGrid.H:301-470):
+// define, setSolverParameters, solve, computeAMRResidual, m_exitStatus.
+class GpuAMRMultiGrid {
+ public:
+  int m_exitStatus = 0;
+  int m_verbosity = 0;
+
+  GpuAMRMultiGrid() {}
+  ~GpuAMRMultiGrid() { clear(); }
+  GpuAMRMultiGrid(const GpuAMRMultiGrid&) = delete;
+  GpuAMRMultiGrid& operator=(const GpuAMRMultiGrid&) = delete;
+
+  void define(const ProblemDomain& a_coarseDomain, GpuAMRPoissonOpFactory& a_factory, LinearSolver<LDF>* a_bottom,
+              int a_numLevels) {
+    defineFrom(a_coarseDomain, a_factory.description(), a_bottom, a_numLevels);
+  }
+  void define(const ProblemDomain& a_coarseDomain, GpuVCAMRPoissonOp2Factory& a_factory, LinearSolver<LDF>* a_bottom,
+              int a_numLevels) {
+    defineFrom(a_coarseDomain, a_factory.description(), a_bottom, a_numLevels);
+  }
+
+  // AMRMultiGrid::setSolverParameters (AMRMultiGrid.H:451-458, 527-546).
+  void setSolverParameters(const int& a_pre, const int& a_post, const int& a_bottom, const int& a_numMG,
+                           const int& a_iterMax, const Real& a_eps, const Real& a_hang, const Real& a_normThresh) {
+    m_p.pre = a_pre;
+    m_p.post = a_post;
+    m_p.bottom = a_bottom;
+    m_p.num_mg = a_numMG;
+    m_p.iter_max = a_iterMax;
+    m_p.eps = a_eps;
+    m_p.hang = a_hang;
+    m_p.norm_thresh = a_normThresh;
+  }
+
+  // AMRMultiGrid::solve (AMRMultiGrid.H:894-1124) on the device.
+  void solve(Vector<LDF*>& a_phi, const Vector<LDF*>& a_rhs, int l_max, int l_base, bool a_zeroPhi = true,
+             bool /*forceHomogeneous*/ = false) {
+    checkRange(l_max, l_base);
+    std::vector<double> buf;
+    for (int l = 0; l < m_nlev; ++l) {
+      pack(*a_rhs[l], l, buf);
+      check(cmg_set_rhs(m_h, l, buf.data(), 0));
+      if (!a_zeroPhi) {
+        pack(*a_phi[l], l, buf);
+        check(cmg_set_phi(m_h, l, buf.data(), 0));
+      }
+    }
+    m_history.assign(m_p.iter_max + 2, 0.0);
+    int st = 0, it = 0, hl = 0;
+    check(cmg_solve(m_h, &m_p, a_zeroPhi ? 1 : 0, &st, &it, m_history.data(), (int)m_history.size(), &hl));
+    m_history.resize(hl);
+    m_exitStatus = st;
+    m_iterations = it;
+    for (int l = 0; l < m_nlev; ++l) {
+      buf.resize(cells(l));
+      check(cmg_get_phi(m_h, l, buf.data(), 0));
+      unpack(buf, l, *a_phi[l]);
+    }
+  }
+
+  // AMRMultiGrid::computeAMRResidual(phi, rhs, l_max, l_base) (AMRMultiGrid.H:738-750):
+  // the composite max-norm residual of the given phi and rhs.
+  Real computeAMRResidual(Vector<LDF*>& a_phi, const Vector<LDF*>& a_rhs, int l_max, int l_base) {
+    checkRange(l_max, l_base);
+    std::vector<double> buf;
+    for (int l = 0; l < m_nlev; ++l) {
+      pack(*a_rhs[l], l, buf);
+      check(cmg_set_rhs(m_h, l, buf.data(), 0));
+      pack(*a_phi[l], l, buf);
+      check(cmg_set_phi(m_h, l, buf.data(), 0));
+    }
+    double r = 0;
+    check(cmg_residual_norm(m_h, &r));
+    return r;
+  }
+
+  // Composite max-norm residual at the start of every iteration of the last
+  // solve, then the final one (what an AMRMultiGridInspector would record).
+  const std::vector<double>& residualHistory() const { return m_history; }
+  int iterations() const { return m_iterations; }
+
+  void clear() {
+    if (m_h) cmg_hierarchy_destroy(m_h);
+    m_h = nullptr;
+    m_nlev = 0;
+  }
+
+ private:
+  cmg_hierarchy* m_h = nullptr;
+  int m_nlev = 0;
+  GpuOpDescription m_d;
+  cmg_solve_params m_p = {4, 4, 4, 1, 100, 5, 1e-10, 1e-10, 1e-30};
+  std::vector<double> m_history;
+  int m_iterations = 0;
+
+  static void check(int rc) {
+    if (rc != CMG_OK) MayDay::Error(cmg_last_error());
+  }
+
+  void checkRange(int l_max, int l_base) const {
+    if (!m_h) MayDay::Error("GpuAMRMultiGrid: solve before define");
+    if (l_base != 0 || l_max != m_nlev - 1)
+      MayDay::Error("GpuAMRMultiGrid: only l_base = 0, l_max = numLevels - 1 is supported");
+  }
+
+  int64_t cells(int l) const {
+    int64_t n = 0;
+    check(cmg_num_cells(m_h, l, &n));
+    return n;
+  }
+
+  // Valid cells of every box in layout order, x fastest (the C ABI's order).
+  void pack(const LDF& a_ld, int l, std::vector<double>& out) const {
+    out.clear();
+    const DisjointBoxLayout& dbl = m_d.grids[l];
+    for (DataIterator dit = a_ld.dataIterator(); dit.ok(); ++dit) {
+      const Box& b = dbl[dit()];
+      const FArrayBox& f = a_ld[dit];
+      for (int k = b.smallEnd(2); k <= b.bigEnd(2); ++k)
+        for (int j = b.smallEnd(1); j <= b.bigEnd(1); ++j)
+          for (int i = b.smallEnd(0); i <= b.bigEnd(0); ++i) out.push_back(f(IntVect(i, j, k), 0));
+    }
+  }
+
+  void unpack(const std::vector<double>& in, int l, LDF& a_ld) const {
+    size_t p = 0;
+    const DisjointBoxLayout& dbl = m_d.grids[l];
+    for (DataIterator dit = a_ld.dataIterator(); dit.ok(); ++dit) {
+      const Box& b = dbl[dit()];
+      FArrayBox& f = a_ld[dit];
+      for (int k = b.smallEnd(2); k <= b.bigEnd(2); ++k)
+        for (int j = b.smallEnd(1); j <= b.bigEnd(1); ++j)
+          for (int i = b.smallEnd(0); i <= b.bigEnd(0); ++i) f(IntVect(i, j, k), 0) = in[p++];
+    }
+  }
+
+  void defineFrom(const ProblemDomain& a_coarseDomain, const GpuOpDescription& d, LinearSolver<LDF>* a_bottom,
+                  int a_numLevels) {
+    clear();
+    if (!d.defined) MayDay::Error("GpuAMRMultiGrid: factory not defined");
+    if (a_bottom && !dynamic_cast<BiCGStabSolver<LDF>*>(a_bottom))
+      MayDay::Error("GpuAMRMultiGrid: the device solve uses BiCGStab as its bottom solver");
+    if (a_numLevels < 1 || a_numLevels > d.grids.size()) MayDay::Error("GpuAMRMultiGrid: bad number of levels");
+    for (int l = 0; l + 1 < a_numLevels; ++l)
+      if (d.refRatios[l] != 2) MayDay::Error("GpuAMRMultiGrid: refinement ratio 2 only");
+    for (int dir = 0; dir < SpaceDim; ++dir)
+      if (a_coarseDomain.isPeriodic(dir)) MayDay::Error("GpuAMRMultiGrid: periodic domains are not supported");
+    m_d = d;
+    m_nlev = a_numLevels;
+    std::vector<int> counts;
+    std::vector<cmg_box> boxes;
+    for (int l = 0; l < m_nlev; ++l) {
+      const DisjointBoxLayout& dbl = d.grids[l];
+      int n = 0;
+      for (LayoutIterator lit = dbl.layoutIterator(); lit.ok(); ++lit, ++n) {
+        const Box& b = dbl[lit()];
+        cmg_box c;
+        for (int dir = 0; dir < 3; ++dir) {
+          c.lo[dir] = b.smallEnd(dir);
+          c.hi[dir] = b.bigEnd(dir);
+        }
+        boxes.push_back(c);
+      }
+      counts.push_back(n);
+    }
+    const Box& db = a_coarseDomain.domainBox();
+    int lo[3], hi[3];
+    for (int dir = 0; dir < 3; ++dir) {
+      lo[dir] = db.smallEnd(dir);
+      hi[dir] = db.bigEnd(dir);
+    }
+    check(cmg_hierarchy_create(lo, hi, d.coarsedx, m_nlev, counts.data(), boxes.data(), d.vc, d.alpha, d.beta,
+                               &m_h));
+    if (d.vc) {
+      std::vector<double> buf;
+      for (int l = 0; l < m_nlev; ++l) {
+        pack(*d.aCoef[l], l, buf);
+        check(cmg_set_acoef(m_h, l, buf.data(), 0));
+        for (int dir = 0; dir < 3; ++dir) {
+          buf.clear();
+          const LevelData<FluxBox>& bc = *d.bCoef[l];
+          for (DataIterator dit = bc.dataIterator(); dit.ok(); ++dit) {
+            const Box fb = surroundingNodes(d.grids[l][dit()], dir);
+            const FArrayBox& f = bc[dit][dir];
+            for (int k = fb.smallEnd(2); k <= fb.bigEnd(2); ++k)
+              for (int j = fb.smallEnd(1); j <= fb.bigEnd(1); ++j)
+                for (int i = fb.smallEnd(0); i <= fb.bigEnd(0); ++i) buf.push_back(f(IntVect(i, j, k), 0));
+          }
+          check(cmg_set_bcoef(m_h, l, dir, buf.data(), 0));
+        }
+      }
+      check(cmg_finalize_coefficients(m_h));
+    }
+  }
+};
+
+}  // namespace cmg_chombo
+
+#endif

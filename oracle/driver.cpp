@@ -53,9 +53,8 @@
 #include "CH_Timer.H"
 #include "parstream.H"
 
+#include "problem.H"
 #include "synthetic.H"
-
-typedef LevelData<FArrayBox> LDF;
 
 static std::map<std::string, std::string> g_args;
 
@@ -70,53 +69,6 @@ static int argi(const char* k, int d) {
 static std::string args(const char* k, const char* d) {
   auto it = g_args.find(k);
   return it == g_args.end() ? std::string(d) : it->second;
-}
-
-// Homogeneous Dirichlet on domain faces, first order (ghost = -interior), as
-// the reference driver's ParseBC (execCell/poissonSolve.cpp:76-119).
-static void zeroValue(Real*, int*, Side::LoHiSide*, Real* a_values) { a_values[0] = 0.; }
-
-static void dirichletBC(FArrayBox& a_state, const Box& a_valid, const ProblemDomain& a_domain,
-                        Real a_dx, bool a_homogeneous) {
-  if (!a_domain.domainBox().contains(a_state.box())) {
-    for (int i = 0; i < CH_SPACEDIM; ++i) {
-      if (!a_domain.isPeriodic(i)) {
-        Box lo = adjCellBox(a_valid, i, Side::Lo, 1);
-        Box hi = adjCellBox(a_valid, i, Side::Hi, 1);
-        if (!a_domain.domainBox().contains(lo))
-          DiriBC(a_state, a_valid, a_dx, true, zeroValue, i, Side::Lo, 1);
-        if (!a_domain.domainBox().contains(hi))
-          DiriBC(a_state, a_valid, a_dx, true, zeroValue, i, Side::Hi, 1);
-      }
-    }
-  }
-}
-
-// Records max-norm of the composite residual at the start of every iteration.
-class ResidualRecorder : public AMRMultiGridInspector<LDF> {
- public:
-  std::vector<double> norms;
-  std::vector<double> stamps;  // wall time at the start of each iteration
-  void recordResiduals(const Vector<LDF*>& r, int lmin, int lmax, int) override {
-    stamps.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count());
-    double m = 0;
-    for (int l = lmin; l <= lmax; ++l)
-      for (DataIterator dit = r[l]->dataIterator(); dit.ok(); ++dit)
-        m = std::max(m, (*r[l])[dit].norm(r[l]->box(dit()), 0, 0, 1));
-    norms.push_back(m);
-  }
-  void recordCorrections(const Vector<LDF*>&, int, int, int) override {}
-};
-
-static void fillRHS(LDF& rhs, Real dx, const cmg_synth::Bumps& bumps) {
-  for (DataIterator dit = rhs.dataIterator(); dit.ok(); ++dit) {
-    FArrayBox& f = rhs[dit];
-    const Box& b = rhs.box(dit());
-    for (BoxIterator bit(b); bit.ok(); ++bit) {
-      IntVect iv = bit();
-      f(iv, 0) = bumps.eval((iv[0] + 0.5) * dx, (iv[1] + 0.5) * dx, (iv[2] + 0.5) * dx);
-    }
-  }
 }
 
 static void writeBox(FILE* f, const Box& b) {
@@ -171,124 +123,27 @@ int main(int argc, char** argv) {
   const int repeat = argi("repeat", 1);
   const std::string out = args("out", "oracle_out");
 
-  cmg_synth::Problem prob(seed);
-
-  // Domains and dx per level (ratio 2).
-  Vector<int> refRatios(std::max(numLevels, 2), 2);
-  Vector<ProblemDomain> domains(numLevels);
-  Vector<Real> dxs(numLevels);
-  bool periodic[CH_SPACEDIM] = {false, false, false};
-  domains[0] = ProblemDomain(IntVect::Zero, (n0 - 1) * IntVect::Unit, periodic);
-  dxs[0] = 1.0 / n0;
-  for (int l = 1; l < numLevels; ++l) {
-    domains[l] = domains[l - 1];
-    domains[l].refine(2);
-    dxs[l] = dxs[l - 1] / 2;
-  }
-
-  // Base level.
-  Vector<DisjointBoxLayout> grids(numLevels);
-  Vector<Vector<Box> > oldBoxes(numLevels), newBoxes(numLevels);
-  domainSplit(domains[0], oldBoxes[0], maxBox, blockFactor);
-  {
-    Vector<int> procs(oldBoxes[0].size(), 0);
-    LoadBalance(procs, oldBoxes[0]);
-    grids[0].define(oldBoxes[0], procs, domains[0]);
-  }
-  // Finer levels: VClocalFuncs.cpp:398-480, or a given layout (boxfile=:
-  // "nlev" then per level "nbox" and nbox lines "lo0 lo1 lo2 hi0 hi1 hi2").
-  int topLevel = 0;
-  const std::string boxfile = args("boxfile", "");
-  if (!boxfile.empty()) {
-    FILE* bf = std::fopen(boxfile.c_str(), "r");
-    if (!bf) {
-      std::fprintf(stderr, "oracle: cannot open %s\n", boxfile.c_str());
-      return 2;
-    }
-    int nl = 0;
-    if (std::fscanf(bf, "%d", &nl) != 1 || nl < 1 || nl > numLevels) return 2;
-    for (int l = 0; l < nl; ++l) {
-      int nb = 0;
-      if (std::fscanf(bf, "%d", &nb) != 1) return 2;
-      Vector<Box> bl;
-      for (int b = 0; b < nb; ++b) {
-        int v[6];
-        for (int k = 0; k < 6; ++k)
-          if (std::fscanf(bf, "%d", &v[k]) != 1) return 2;
-        bl.push_back(Box(IntVect(v[0], v[1], v[2]), IntVect(v[3], v[4], v[5])));
-      }
-      Vector<int> procs(bl.size(), 0);
-      LoadBalance(procs, bl);
-      grids[l] = DisjointBoxLayout(bl, procs, domains[l]);
-    }
-    std::fclose(bf);
-    topLevel = nl - 1;
-  } else if (numLevels > 1) {
-    BRMeshRefine meshrefine(domains[0], refRatios, fillRatio, blockFactor, 2, maxBox);
-    bool more = true;
-    while (more) {
-      more = false;
-      int oldTop = topLevel;
-      Vector<IntVectSet> tags(topLevel + 1);
-      for (int l = 0; l <= topLevel; ++l) {
-        LDF rhs(grids[l], 1, IntVect::Zero);
-        fillRHS(rhs, dxs[l], prob.bumps);
-        Real maxRHS = norm(rhs, rhs.interval(), 0);
-        Real tagVal = maxRHS * thresh;
-        IntVectSet local;
-        for (DataIterator dit = rhs.dataIterator(); dit.ok(); ++dit) {
-          const Box b = grids[l].get(dit());
-          for (BoxIterator bit(b); bit.ok(); ++bit)
-            if (std::fabs(rhs[dit](bit(), 0)) > tagVal) local |= bit();
-        }
-        local.grow(1);
-        local &= domains[l].domainBox();
-        tags[l] = local;
-      }
-      int newFinest = meshrefine.regrid(newBoxes, tags, 0, topLevel, oldBoxes);
-      if (newFinest > topLevel) topLevel++;
-      oldBoxes = newBoxes;
-      for (int l = 1; l <= topLevel; ++l) {
-        Vector<int> procs(newBoxes[l].size(), 0);
-        LoadBalance(procs, newBoxes[l]);
-        grids[l] = DisjointBoxLayout(newBoxes[l], procs, domains[l]);
-      }
-      if (topLevel < numLevels - 1 && topLevel > oldTop) more = true;
-    }
-  }
-  const int finest = topLevel;
-  const int nlev = finest + 1;
-
-  // Data.
-  Vector<LDF*> phi(nlev, NULL), rhs(nlev, NULL);
-  Vector<RefCountedPtr<LDF> > aCoef(nlev);
-  Vector<RefCountedPtr<LevelData<FluxBox> > > bCoef(nlev);
-  for (int l = 0; l < nlev; ++l) {
-    phi[l] = new LDF(grids[l], 1, IntVect::Unit);
-    rhs[l] = new LDF(grids[l], 1, IntVect::Zero);
-    fillRHS(*rhs[l], dxs[l], prob.bumps);
-    if (opType == 1) {
-      aCoef[l] = RefCountedPtr<LDF>(new LDF(grids[l], 1, IntVect::Zero));
-      bCoef[l] = RefCountedPtr<LevelData<FluxBox> >(new LevelData<FluxBox>(grids[l], 1, IntVect::Zero));
-      Real dx = dxs[l];
-      for (DataIterator dit = grids[l].dataIterator(); dit.ok(); ++dit) {
-        FArrayBox& a = (*aCoef[l])[dit];
-        for (BoxIterator bit(a.box()); bit.ok(); ++bit) {
-          IntVect iv = bit();
-          a(iv, 0) = prob.acoef.eval((iv[0] + 0.5) * dx, (iv[1] + 0.5) * dx, (iv[2] + 0.5) * dx);
-        }
-        for (int d = 0; d < 3; ++d) {
-          FArrayBox& b = (*bCoef[l])[dit][d];
-          for (BoxIterator bit(b.box()); bit.ok(); ++bit) {
-            IntVect iv = bit();
-            double x[3];
-            for (int e = 0; e < 3; ++e) x[e] = (e == d) ? iv[e] * dx : (iv[e] + 0.5) * dx;
-            b(iv, 0) = prob.bcoef.eval(x[0], x[1], x[2]);
-          }
-        }
-      }
-    }
-  }
+  OracleProblem P;
+  P.n0 = n0;
+  P.numLevels = numLevels;
+  P.maxBox = maxBox;
+  P.blockFactor = blockFactor;
+  P.fillRatio = fillRatio;
+  P.opType = opType;
+  P.alpha = alpha;
+  P.beta = beta;
+  P.seed = seed;
+  P.thresh = thresh;
+  P.boxfile = args("boxfile", "");
+  if (buildProblem(P) != 0) return 2;
+  const int finest = P.finest, nlev = P.nlev;
+  Vector<ProblemDomain>& domains = P.domains;
+  Vector<Real>& dxs = P.dxs;
+  Vector<DisjointBoxLayout>& grids = P.grids;
+  Vector<LDF*>& phi = P.phi;
+  Vector<LDF*>& rhs = P.rhs;
+  Vector<RefCountedPtr<LDF> >& aCoef = P.aCoef;
+  Vector<RefCountedPtr<LevelData<FluxBox> > >& bCoef = P.bCoef;
 
   // Solver.
   Vector<DisjointBoxLayout> fgrids(nlev);

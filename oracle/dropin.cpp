@@ -1,0 +1,122 @@
+// ORACLE — test infrastructure only.
+//
+// The drop-in check: a Chombo program solves the same seeded hierarchy twice
+// through the same API, once with the reference's AMRMultiGrid over
+// AMRPoissonOp / VCAMRPoissonOp2 on the CPU and once with
+// cmg_chombo::GpuAMRMultiGrid over the GPU factories (include/cmg_chombo.H,
+// libcmg.so), and prints one JSON line comparing the two: exit status,
+// iteration count, residual histories and phi on every level.
+//
+// Usage: dropin key=value ...   (n0 levels maxbox block op alpha beta seed
+// pre post bottom iters eps hang, as for cmg_oracle)
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+
+#include "AMRMultiGrid.H"
+#include "AMRPoissonOp.H"
+#include "BiCGStabSolver.H"
+#include "VCAMRPoissonOp2.H"
+#include "cmg_chombo.H"
+#include "problem.H"
+
+static std::map<std::string, std::string> g_args;
+static double argd(const char* k, double d) {
+  auto it = g_args.find(k);
+  return it == g_args.end() ? d : std::atof(it->second.c_str());
+}
+
+int main(int argc, char** argv) {
+  for (int a = 1; a < argc; ++a) {
+    const char* eq = std::strchr(argv[a], '=');
+    if (eq) g_args[std::string(argv[a], eq - argv[a])] = std::string(eq + 1);
+  }
+  OracleProblem P;
+  P.n0 = (int)argd("n0", 16);
+  P.numLevels = (int)argd("levels", 3);
+  P.maxBox = (int)argd("maxbox", 8);
+  P.blockFactor = (int)argd("block", 4);
+  P.opType = (int)argd("op", 1);
+  P.alpha = argd("alpha", 1.0);
+  P.beta = argd("beta", -1.0);
+  P.seed = (unsigned long long)argd("seed", 20261203.0);
+  if (buildProblem(P) != 0) return 2;
+  const int pre = (int)argd("pre", 4), post = (int)argd("post", 4), bottom = (int)argd("bottom", 4);
+  const int iters = (int)argd("iters", 100);
+  const Real eps = argd("eps", 1e-10), hang = argd("hang", 1e-10);
+  const int nlev = P.nlev, lmax = P.finest;
+
+  Vector<LDF*> phiGpu(nlev);
+  for (int l = 0; l < nlev; ++l) phiGpu[l] = new LDF(P.grids[l], 1, IntVect::Unit);
+  Vector<int> rr(nlev, 2);
+
+  // Reference: CPU AMRMultiGrid.
+  RefCountedPtr<AMRLevelOpFactory<LDF> > factory;
+  if (P.opType == 0) {
+    AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
+  } else {
+    VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
+  }
+  BiCGStabSolver<LDF> bottomSolver;
+  bottomSolver.m_verbosity = 0;
+  AMRMultiGrid<LDF> cpu;
+  cpu.define(P.domains[0], *factory, &bottomSolver, nlev);
+  cpu.setSolverParameters(pre, post, bottom, 1, iters, eps, hang, 1e-30);
+  cpu.m_verbosity = 0;
+  RefCountedPtr<AMRMultiGridInspector<LDF> > insp(new ResidualRecorder);
+  cpu.addInspector(insp);
+  cpu.solve(P.phi, P.rhs, lmax, 0, true);
+  ResidualRecorder* rec = static_cast<ResidualRecorder*>(&(*insp));
+  rec->norms.push_back(cpu.computeAMRResidual(P.phi, P.rhs, lmax, 0));
+
+  // The same calls on the GPU drop-in.
+  cmg_chombo::GpuAMRMultiGrid gpu;
+  BiCGStabSolver<LDF> gpuBottom;
+  if (P.opType == 0) {
+    cmg_chombo::GpuAMRPoissonOpFactory f;
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    gpu.define(P.domains[0], f, &gpuBottom, nlev);
+  } else {
+    cmg_chombo::GpuVCAMRPoissonOp2Factory f;
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    gpu.define(P.domains[0], f, &gpuBottom, nlev);
+  }
+  gpu.setSolverParameters(pre, post, bottom, 1, iters, eps, hang, 1e-30);
+  gpu.solve(phiGpu, P.rhs, lmax, 0, true);
+  const Real gpuFinal = gpu.computeAMRResidual(phiGpu, P.rhs, lmax, 0);
+
+  double maxRel = 0, maxHist = 0;
+  for (int l = 0; l < nlev; ++l) {
+    double scale = 0, diff = 0;
+    for (DataIterator dit = P.grids[l].dataIterator(); dit.ok(); ++dit) {
+      const Box& b = P.grids[l][dit()];
+      for (BoxIterator bit(b); bit.ok(); ++bit) {
+        scale = std::max(scale, std::fabs((*P.phi[l])[dit](bit(), 0)));
+        diff = std::max(diff, std::fabs((*P.phi[l])[dit](bit(), 0) - (*phiGpu[l])[dit](bit(), 0)));
+      }
+    }
+    maxRel = std::max(maxRel, scale > 0 ? diff / scale : diff);
+  }
+  const std::vector<double>& gh = gpu.residualHistory();
+  const bool sameLen = gh.size() == rec->norms.size();
+  if (sameLen)
+    for (size_t i = 0; i < gh.size(); ++i) maxHist = std::max(maxHist, std::fabs(gh[i] - rec->norms[i]) / rec->norms[0]);
+  std::printf("{\"levels\": %d, \"cpu_exit\": %d, \"gpu_exit\": %d, \"cpu_iters\": %d, \"gpu_iters\": %d, "
+              "\"same_history_length\": %s, \"history_dev\": %.3e, \"phi_rel_dev\": %.3e, "
+              "\"gpu_final_residual\": %.17g, \"gpu_history_last\": %.17g}\n",
+              nlev, cpu.m_exitStatus, gpu.m_exitStatus, (int)rec->norms.size() - 1, gpu.iterations(),
+              sameLen ? "true" : "false", maxHist, maxRel, gpuFinal, gh.empty() ? -1.0 : gh.back());
+  for (int l = 0; l < nlev; ++l) {
+    delete phiGpu[l];
+    delete P.phi[l];
+    delete P.rhs[l];
+  }
+  return 0;
+}

@@ -36,6 +36,19 @@ WORKLOADS = {
         "name": "3-level VC Helmholtz (VCAMRPoissonOp2 alpha=1 beta=-1), base 128^3, ratio 2, block 8, "
                 "max box 32, fill 0.75, Dirichlet, GSRB 4+4, BiCGStab bottom, rel. residual 1e-10",
     },
+    "config2": {
+        "golden": "config2_vc_3lev_256",
+        "mixed": True,
+        "name": "3-level VC Helmholtz (VCAMRPoissonOp2 alpha=1 beta=-1), base 256^3, ratio 2, block 8, "
+                "max box 32, fill 0.75, Dirichlet, GSRB 4+4, BiCGStab bottom, rel. residual 1e-10; FP32 "
+                "V-cycles inside FP64 iterative refinement (residual, reflux, bottom, norms FP64)",
+    },
+    "config1-mixed": {
+        "golden": "config1_vc_3lev_128",
+        "mixed": True,
+        "name": "3-level VC Helmholtz, base 128^3 (as config1); FP32 V-cycles inside FP64 iterative "
+                "refinement (residual, reflux, bottom, norms FP64)",
+    },
     "config0": {
         "golden": "config0_poisson_64",
         "name": "single-level Poisson (AMRPoissonOp alpha=0 beta=1), 64^3, max box 32, Dirichlet, "
@@ -54,6 +67,22 @@ def load_cmg():
 
 def golden_meta(name):
     return json.load(open(os.path.join(GOLDEN, name + ".json")))
+
+
+def covered_cells(boxes, finer_boxes):
+    """Valid cells of a level (boxes in layout order, x fastest) under the next finer level (ratio 2)."""
+    masks = []
+    fine = [(np.array(b[:3]) // 2, np.array(b[3:]) // 2) for b in finer_boxes]
+    for b in boxes:
+        lo, hi = np.array(b[:3]), np.array(b[3:])
+        n = hi - lo + 1
+        m = np.zeros((n[2], n[1], n[0]), bool)
+        for flo, fhi in fine:
+            a, c = np.maximum(lo, flo), np.minimum(hi, fhi)
+            if np.all(a <= c):
+                m[a[2] - lo[2]:c[2] - lo[2] + 1, a[1] - lo[1]:c[1] - lo[1] + 1, a[0] - lo[0]:c[0] - lo[0] + 1] = True
+        masks.append(m.ravel())
+    return np.concatenate(masks)
 
 
 def measured_peaks():
@@ -221,6 +250,7 @@ def main():
     h.fill_synthetic(meta["seed"])
     params = cmg.solve_params(pre=meta["pre"], post=meta["post"], bottom=meta["bottom"], iter_max=meta["iters"],
                               eps=meta["eps"], hang=meta["hang"])
+    mixed = bool(wl.get("mixed", False))
     stream = torch.cuda.ExternalStream(h.stream())
     ncells = [h.num_cells(l) for l in range(len(meta["boxes"]))]
 
@@ -230,7 +260,7 @@ def main():
             dist.barrier()
 
     for _ in range(args.warmup):
-        out = h.solve(params)
+        out = h.solve(params, mixed=mixed)
     assert out["exit_status"] == meta["exit_status"], out
     n_iter = out["iterations"]
 
@@ -244,7 +274,7 @@ def main():
     with torch.cuda.stream(stream):
         ev[0].record(stream)
         for k in range(args.steps):
-            h.solve(params)
+            h.solve(params, mixed=mixed)
             ev[k + 1].record(stream)
     barrier()
     launches = cmg.launch_count() - launches0
@@ -260,7 +290,7 @@ def main():
     pe = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     pe[0].record(stream)
     for _ in range(n_prof):
-        h.solve(params)
+        h.solve(params, mixed=mixed)
     pe[1].record(stream)
     barrier()
     prof_ms = pe[0].elapsed_time(pe[1])
@@ -287,7 +317,7 @@ def main():
     for k in range(args.steps):
         for l in range(len(ncells)):
             h.set_rhs_ptr(l, host_rhs[l].data_ptr(), 0)
-        out = h.solve(params)
+        out = h.solve(params, mixed=mixed)
         for l in range(len(ncells)):
             h.get_phi_ptr(l, host_phi[l].data_ptr(), 0)
     e2e_ev[1].record(stream)
@@ -320,6 +350,31 @@ def main():
                         "share": v[1] / prof_ms if prof_ms > 0 else 0.0,
                         "gbs": (v[2] / 1e9) / (v[1] / 1e3) if v[1] > 0 and v[2] > 0 else None}
                  for name, v in classes.items()}
+    accuracy = None
+    if mixed:
+        # L-infinity deviation of the mixed-precision phi from the FP64
+        # reference solve's phi (golden samples), relative to max|phi| per
+        # level: over the composite solution (cells not covered by a finer
+        # level) and over the covered coarse cells, which the composite
+        # residual does not constrain.
+        gold = np.load(os.path.join(GOLDEN, wl["golden"] + ".npz"))
+        nlev, stride = len(meta["boxes"]), meta["sample_stride"]
+        comp, covd = 0.0, 0.0
+        for lev in range(nlev):
+            phi = h.phi(lev)
+            cov = covered_cells(meta["boxes"][lev], meta["boxes"][lev + 1]) if lev + 1 < nlev else \
+                np.zeros(phi.size, bool)
+            full = meta["full"]
+            ref = gold[f"phi{lev}"] if full else gold[f"phi{lev}_sample"]
+            if not full:
+                phi, cov = phi[::stride], cov[::stride]
+            dev = np.abs(phi - ref) / meta["phi_absmax"][lev]
+            comp = max(comp, float(dev[~cov].max()) if (~cov).any() else 0.0)
+            covd = max(covd, float(dev[cov].max()) if cov.any() else 0.0)
+        accuracy = {"linf_rel_vs_fp64_reference_composite": comp, "linf_rel_vs_fp64_reference_covered": covd,
+                    "fp64_refinement_steps": n_iter,
+                    "fp64_reference_vcycles": len(meta["residual_history"]) - 1,
+                    "sampled": not meta["full"]}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res = cpu_reference(meta, 1, 1)
@@ -331,7 +386,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
             "config": {"workload": wl["name"], "global_batch": world, "cells": sum(ncells),
                        "levels": len(ncells), "boxes": [len(b) for b in meta["boxes"]],
                        "vcycles_per_solve": n_iter, "l2": "working set > L2 (no flush)",
@@ -340,6 +395,8 @@ def main():
             "roofline": roofline, "breakdown": breakdown, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches,
         }
+        if accuracy:
+            line["accuracy"] = accuracy
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

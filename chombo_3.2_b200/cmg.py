@@ -175,12 +175,15 @@ class Hierarchy:
         a = np.ascontiguousarray(data, dtype=np.float64)
         _check(lib().cmg_set_phi(self.h, level, _ptr(a), 0))
 
-    def solve(self, params=None, zero_phi=True):
+    def solve(self, params=None, zero_phi=True, mixed=False):
+        """AMRMultiGrid::solve on the device; mixed=True runs the FP32
+        V-cycles inside FP64 iterative refinement (cmg_solve_mixed)."""
         p = params or solve_params()
         hist = np.zeros(p.iter_max + 2, dtype=np.float64)
         st, it, hl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        _check(lib().cmg_solve(self.h, ctypes.byref(p), int(zero_phi), ctypes.byref(st), ctypes.byref(it),
-                               _ptr(hist), len(hist), ctypes.byref(hl)))
+        fn = lib().cmg_solve_mixed if mixed else lib().cmg_solve
+        _check(fn(self.h, ctypes.byref(p), int(zero_phi), ctypes.byref(st), ctypes.byref(it),
+                  _ptr(hist), len(hist), ctypes.byref(hl)))
         return {"exit_status": st.value, "iterations": it.value, "history": hist[:hl.value].copy()}
 
     def residual_norm(self):

@@ -245,8 +245,9 @@ int cmg_set_phi(cmg_hierarchy* h, int level, const double* data, int on_device) 
   });
 }
 
-int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
-              double* history, int history_cap, int* history_len) {
+namespace {
+int solveWith(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
+              double* history, int history_cap, int* history_len, bool mixed) {
   return guard([&]() {
     needLevel(h, 0);
     if (!p) throw std::invalid_argument("cmg: null parameters");
@@ -262,7 +263,7 @@ int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* ex
     sp.normThresh = p->norm_thresh;
     if (sp.pre < 0 || sp.post < 0 || sp.bottom < 0 || sp.numMG < 1 || sp.iterMax < 0)
       throw std::invalid_argument("cmg: invalid solver parameters");
-    cmg::SolveResult r = h->solver->solve(sp, zero_phi != 0);
+    cmg::SolveResult r = mixed ? h->solver->solveMixed(sp, zero_phi != 0) : h->solver->solve(sp, zero_phi != 0);
     if (exit_status) *exit_status = r.exitStatus;
     if (iterations) *iterations = r.iterations;
     int n = (int)r.history.size();
@@ -270,6 +271,17 @@ int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* ex
     if (history)
       for (int i = 0; i < n && i < history_cap; ++i) history[i] = r.history[i];
   });
+}
+}  // namespace
+
+int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
+              double* history, int history_cap, int* history_len) {
+  return solveWith(h, p, zero_phi, exit_status, iterations, history, history_cap, history_len, false);
+}
+
+int cmg_solve_mixed(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
+                    double* history, int history_cap, int* history_len) {
+  return solveWith(h, p, zero_phi, exit_status, iterations, history, history_cap, history_len, true);
 }
 
 int cmg_residual_norm(cmg_hierarchy* h, double* out) {

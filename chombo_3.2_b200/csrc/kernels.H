@@ -94,6 +94,10 @@ template <class T> void reflux(const LevelDev& C, T* lofphiC, const T* phiC, con
                                const Coef<T>& cf, cudaStream_t s);
 // lhs += scale * x over valid cells.
 template <class T> void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s);
+// lhs += x over valid cells, an FP32 correction added to an FP64 field.
+void incrMixed(const LevelDev& L, double* lhs, const float* x, cudaStream_t s);
+// dst[q] = src[q] for every element of a level array (valid and ghost cells).
+template <class D, class S> void convert(D* dst, const S* src, int64_t n, cudaStream_t s);
 // Max |f| over valid cells, folded into *out (device scalar) with max().
 template <class T> void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s);
 

@@ -2,6 +2,7 @@
 // reference operation (ChF kernel or C++ routine, paths relative to the
 // Chombo lib/src tree) whose arithmetic it reproduces term for term, so the
 // FP64 build (compiled with --fmad=false) rounds exactly like the reference.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <stdexcept>
@@ -249,14 +250,21 @@ __global__ void k_negadd(const BoxDesc* boxes, const Chunk* chunks, T* r, const 
   r[c] = lofphi[c] * T(-1) + rhs[c] * T(1);
 }
 
-template <class T>
-__global__ void k_incr(const BoxDesc* boxes, const Chunk* chunks, T* lhs, const T* x, T scale) {
+template <class T, class X>
+__global__ void k_incr(const BoxDesc* boxes, const Chunk* chunks, T* lhs, const X* x, T scale) {
   Chunk ch = chunks[blockIdx.x];
   const BoxDesc bd = boxes[ch.box];
   int i, j, k;
   if (!allCell(bd, ch.start + threadIdx.x, i, j, k)) return;
   int64_t c = cellIndex(bd, i, j, k);
-  lhs[c] = lhs[c] + x[c] * scale;
+  lhs[c] = lhs[c] + T(x[c]) * scale;
+}
+
+// dst = src over whole arrays (ghosts included), converting the type.
+template <class D, class S>
+__global__ void k_convert(D* dst, const S* src, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    dst[q] = D(src[q]);
 }
 
 __device__ __forceinline__ void atomicMaxPos(double* addr, double v) {
@@ -906,7 +914,7 @@ void reflux(const LevelDev& C, T* lofphiC, const T* phiC, const T* phiF, const C
 template <class T>
 void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s) {
   if (L.nAll == 0) return;
-  k_incr<T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lhs, x, T(scale));
+  k_incr<T, T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lhs, x, T(scale));
   CMG_LAUNCHED("incr");
 }
 
@@ -958,6 +966,22 @@ void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream
   k_gather_slots<<<(n + 255) / 256, 256, 0, s>>>(w.fab, n, fab, dst);
   CMG_LAUNCHED("gatherSlots");
 }
+
+void incrMixed(const LevelDev& L, double* lhs, const float* x, cudaStream_t s) {
+  if (L.nAll == 0) return;
+  k_incr<double, float><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lhs, x, 1.0);
+  CMG_LAUNCHED("incrMixed");
+}
+
+template <class D, class S>
+void convert(D* dst, const S* src, int64_t n, cudaStream_t s) {
+  if (n == 0) return;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_convert<D, S><<<blocks, 256, 0, s>>>(dst, src, n);
+  CMG_LAUNCHED("convert");
+}
+template void convert<float, double>(float*, const double*, int64_t, cudaStream_t);
+template void convert<double, float>(double*, const float*, int64_t, cudaStream_t);
 
 #define CMG_INST(T)                                                                                       \
   template void ghostFill<T>(const LevelDev&, T*, bool, cudaStream_t, int);                                \

@@ -86,28 +86,44 @@ class Solver {
   void profileEnable(bool on);
   void profileRead(int cls, int64_t* launches, double* ms, double* bytes);
 
-  struct LevelFields {
-    double *phi = nullptr, *rhs = nullptr, *ures = nullptr, *ucorr = nullptr, *corr = nullptr, *res = nullptr;
-    double *a = nullptr, *b[3] = {nullptr, nullptr, nullptr}, *lambda = nullptr;
+  template <class T>
+  struct FieldsT {
+    T *phi = nullptr, *rhs = nullptr, *ures = nullptr, *ucorr = nullptr, *corr = nullptr, *res = nullptr;
+    T *a = nullptr, *b[3] = {nullptr, nullptr, nullptr}, *lambda = nullptr;
   };
+  using LevelFields = FieldsT<double>;
+
+  // FP32 V-cycles inside FP64 iterative refinement: the composite residual
+  // with its flux-register correction, the bottom solve and the norms stay
+  // FP64 (no counterpart in the reference, which is FP64 throughout).
+  SolveResult solveMixed(const SolveParams& p, bool zeroPhi = true);
 
  private:
   void uploadLevel(const LevelPlan& p, LevelDev& d);
   double* alloc(size_t n);
   Coef<double> coefAMR(int l) const;
   Coef<double> coefMG(int d) const;
-  void relaxAMR(int l, double* phi, const double* rhs, int n);
-  void relaxMG(int d, double* phi, const double* rhs, int n);
-  void relaxLevel(const LevelDev& L, double cells, const Coef<double>& c, double* phi, const double* rhs, int n,
-                  int cls);
-  void fill(const LevelDev& L, double* f, bool withCF, int par = -1);
-  void amrResidualLevel(int ilev, int lmax, std::vector<double*>& res, std::vector<double*>& phi,
-                        std::vector<double*>& rhs);
+  // The V-cycle in precision T (double: the drop-in; float: the inner
+  // cycles of solveMixed).
+  template <class T> std::vector<FieldsT<T>>& levF();
+  template <class T> std::vector<FieldsT<T>>& mgF();
+  template <class T> Coef<T> coefA(int l);
+  template <class T> Coef<T> coefM(int d);
+  template <class T> void relaxAMR(int l, T* phi, const T* rhs, int n);
+  template <class T> void relaxMG(int d, T* phi, const T* rhs, int n);
+  template <class T>
+  void relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls);
+  template <class T> void fill(const LevelDev& L, T* f, bool withCF, int par = -1);
+  template <class T>
+  void amrResidualLevel(int ilev, int lmax, std::vector<T*>& res, std::vector<T*>& phi, std::vector<T*>& rhs);
   double computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);
-  void amrVCycle(int ilev, int lmax);
-  void mgCycle(int depth, double* corr, double* res);
-  void zeroField(const LevelDev& L, double* f);
-  void copyField(const LevelDev& L, double* dst, const double* src);
+  template <class T> void amrVCycle(int ilev, int lmax);
+  template <class T> void mgCycle(int depth, T* corr, T* res);
+  template <class T> void bottom(int depth, T* corr, T* res);
+  template <class T> void zeroField(const LevelDev& L, T* f);
+  template <class T> void copyField(const LevelDev& L, T* dst, const T* src);
+  void ensure32();
+  float* allocF(size_t n);
   void scatterValid(const LevelPlan& p, const LevelDev& d, double* dev, const double* src, bool onDevice,
                     int faceDir);
   void gatherValid(const LevelPlan& p, const LevelDev& d, const double* dev, double* dst, bool onDevice);
@@ -128,6 +144,8 @@ class Solver {
   std::vector<LevelDev> amrDev_, mgDev_;
   std::vector<LevelFields> lev_;
   std::vector<LevelFields> mgf_;     // corr, res and coefficients per depth
+  std::vector<FieldsT<float>> lev32_, mgf32_;  // FP32 V-cycle fields (allocated on first solveMixed)
+  bool have32_ = false, coef32Stale_ = true;
   std::vector<std::unique_ptr<DevBuf>> bufs_;
   BottomWork bottom_;
   double* dNorm_ = nullptr;

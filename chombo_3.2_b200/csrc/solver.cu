@@ -451,6 +451,7 @@ void Solver::finalizeCoefficients() {
     auto lam = computeLambda(mg_[d].grids, a, b, desc_.alpha, desc_.beta, mg_[d].dx);
     scatterValid(mg_[d], mgDev_[d], mgf_[d].lambda, lam.data(), false, -1);
   }
+  coef32Stale_ = true;
   // Compact copies of the bottom level's coefficients for the bottom solve.
   Coef<double> cb = coefMG((int)mg_.size());
   gatherSlots(bottom_, cb.a, bottom_.a, s_);
@@ -487,11 +488,49 @@ Coef<double> Solver::coefMG(int d) const {
 
 namespace cmg {
 
-void Solver::zeroField(const LevelDev& L, double* f) {
-  ck(cudaMemsetAsync(f, 0, L.nelem * sizeof(double), s_), "zero");
+template <>
+std::vector<Solver::FieldsT<double>>& Solver::levF<double>() { return lev_; }
+template <>
+std::vector<Solver::FieldsT<float>>& Solver::levF<float>() { return lev32_; }
+template <>
+std::vector<Solver::FieldsT<double>>& Solver::mgF<double>() { return mgf_; }
+template <>
+std::vector<Solver::FieldsT<float>>& Solver::mgF<float>() { return mgf32_; }
+
+template <class T>
+Coef<T> Solver::coefA(int l) {
+  Coef<T> c;
+  c.vc = desc_.vc;
+  c.alpha = desc_.alpha;
+  c.beta = desc_.beta;
+  const FieldsT<T>& f = levF<T>()[l];
+  c.a = f.a;
+  for (int d = 0; d < 3; ++d) c.b[d] = f.b[d];
+  c.lambda = f.lambda;
+  return c;
 }
-void Solver::copyField(const LevelDev& L, double* dst, const double* src) {
-  ck(cudaMemcpyAsync(dst, src, L.nelem * sizeof(double), cudaMemcpyDeviceToDevice, s_), "copy");
+
+template <class T>
+Coef<T> Solver::coefM(int d) {
+  if (d == 0) return coefA<T>(0);
+  Coef<T> c;
+  c.vc = desc_.vc;
+  c.alpha = desc_.alpha;
+  c.beta = desc_.beta;
+  const FieldsT<T>& f = mgF<T>()[d - 1];
+  c.a = f.a;
+  for (int k = 0; k < 3; ++k) c.b[k] = f.b[k];
+  c.lambda = f.lambda;
+  return c;
+}
+
+template <class T>
+void Solver::zeroField(const LevelDev& L, T* f) {
+  ck(cudaMemsetAsync(f, 0, L.nelem * sizeof(T), s_), "zero");
+}
+template <class T>
+void Solver::copyField(const LevelDev& L, T* dst, const T* src) {
+  ck(cudaMemcpyAsync(dst, src, L.nelem * sizeof(T), cudaMemcpyDeviceToDevice, s_), "copy");
 }
 
 // AMRPoissonOp::levelGSRB / VCAMRPoissonOp2::levelGSRB: per colour,
@@ -502,9 +541,9 @@ void Solver::copyField(const LevelDev& L, double* dst, const double* src) {
 // coefficients, 2 words); variable coefficients add half a word each for
 // a and lambda and a full word for each of the three face arrays, since
 // every face borders one cell of each colour (6 words).
-void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<double>& c, double* phi, const double* rhs,
-                        int n, int cls) {
-  const double bytes = cells * 8.0 * (c.vc ? 6.0 : 2.0);
+template <class T>
+void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls) {
+  const double bytes = cells * sizeof(T) * (c.vc ? 6.0 : 2.0);
   for (int it = 0; it < n; ++it)
     for (int color = 0; color <= 1; ++color) {
       fill(L, phi, true, 1 - color);
@@ -512,49 +551,54 @@ void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<double>& c, 
     }
 }
 
-void Solver::relaxAMR(int l, double* phi, const double* rhs, int n) {
+template <class T>
+void Solver::relaxAMR(int l, T* phi, const T* rhs, int n) {
   const int finest = (int)amr_.size() - 1;
-  relaxLevel(amrDev_[l], (double)amr_[l].grids.numCells(), coefAMR(l), phi, rhs, n,
+  relaxLevel(amrDev_[l], (double)amr_[l].grids.numCells(), coefA<T>(l), phi, rhs, n,
              l == finest ? P_RELAX_FINE : P_RELAX);
 }
 
-void Solver::relaxMG(int d, double* phi, const double* rhs, int n) {
+template <class T>
+void Solver::relaxMG(int d, T* phi, const T* rhs, int n) {
   if (d == 0) return relaxAMR(0, phi, rhs, n);
-  relaxLevel(mgDev_[d - 1], (double)mg_[d - 1].grids.numCells(), coefMG(d), phi, rhs, n, P_RELAX);
+  relaxLevel(mgDev_[d - 1], (double)mg_[d - 1].grids.numCells(), coefM<T>(d), phi, rhs, n, P_RELAX);
 }
 
 // Ghost fill, timed as its own class: every ghost cell filled written once
-// and its source read once (16 bytes per cell; half the cells for a
+// and its source read once (two words per cell; half the cells for a
 // one-colour fill).
-void Solver::fill(const LevelDev& L, double* f, bool withCF, int par) {
-  const double bytes = (par >= 0 ? 8.0 : 16.0) * (withCF ? L.nCellsGhost : L.nCellsExchBC);
+template <class T>
+void Solver::fill(const LevelDev& L, T* f, bool withCF, int par) {
+  const double bytes = (par >= 0 ? 1.0 : 2.0) * sizeof(T) * (withCF ? L.nCellsGhost : L.nCellsExchBC);
   timed(P_GHOST, bytes, [&]() { ghostFill(L, f, withCF, s_, par); });
 }
 
 // AMRMultiGrid::computeAMRResidualLevel (AMRMultiGrid.H:836-892).
-void Solver::amrResidualLevel(int ilev, int lmax, std::vector<double*>& res, std::vector<double*>& phi,
-                              std::vector<double*>& rhs) {
+template <class T>
+void Solver::amrResidualLevel(int ilev, int lmax, std::vector<T*>& res, std::vector<T*>& phi,
+                              std::vector<T*>& rhs) {
   const LevelDev& L = amrDev_[ilev];
-  Coef<double> c = coefAMR(ilev);
+  Coef<T> c = coefA<T>(ilev);
+  const double w = sizeof(T);
   if (lmax == 0) {
     // residual(): homogeneous CF (none on level 0), then residualI.
     fill(L, phi[0], true);
-    timed(P_OP, amr_[0].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[0], phi[0], rhs[0], c, s_); });
+    timed(P_OP, amr_[0].grids.numCells() * w * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[0], phi[0], rhs[0], c, s_); });
     return;
   }
   if (ilev == lmax) {
     // AMRResidualNF: coarse-fine interpolation, then residualI.
     quadCF(L, phi[ilev], phi[ilev - 1], s_);
     fill(L, phi[ilev], false);
-    timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[ilev], phi[ilev], rhs[ilev], c, s_); });
+    timed(P_OP, amr_[ilev].grids.numCells() * w * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, res[ilev], phi[ilev], rhs[ilev], c, s_); });
     return;
   }
   // AMRResidual(NC): [CF interpolation], applyOpI, reflux, axby(-1, 1).
   if (ilev > 0) quadCF(L, phi[ilev], phi[ilev - 1], s_);
   fill(L, phi[ilev], false);
-  timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0), [&]() { applyOp(L, res[ilev], phi[ilev], c, s_); });
+  timed(P_OP, amr_[ilev].grids.numCells() * w * (desc_.vc ? 6.0 : 2.0), [&]() { applyOp(L, res[ilev], phi[ilev], c, s_); });
   quadCF(amrDev_[ilev + 1], phi[ilev + 1], phi[ilev], s_);
-  reflux(L, res[ilev], phi[ilev], phi[ilev + 1], c, coefAMR(ilev + 1), s_);
+  reflux(L, res[ilev], phi[ilev], phi[ilev + 1], c, coefA<T>(ilev + 1), s_);
   negAdd(L, res[ilev], res[ilev], rhs[ilev], s_);
 }
 
@@ -573,27 +617,46 @@ double Solver::computeAMRResidual(std::vector<double*>& res, std::vector<double*
   return h;
 }
 
+// BiCGStab bottom solve in FP64 whatever the V-cycle's precision: an FP32
+// V-cycle hands its correction and residual over through the FP64 fields of
+// the bottom level (free during the FP32 cycle) and takes the result back.
+template <>
+void Solver::bottom<double>(int depth, double* corr, double* res) {
+  const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
+  timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr, res, coefMG(depth), bottom_, sp_.eps, bottomMetric_, s_); });
+}
+template <>
+void Solver::bottom<float>(int depth, float* corr, float* res) {
+  const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
+  double* corr64 = depth == 0 ? lev_[0].corr : mgf_[depth - 1].corr;
+  double* res64 = depth == 0 ? lev_[0].res : mgf_[depth - 1].res;
+  convert(corr64, corr, L.nelem, s_);
+  convert(res64, res, L.nelem, s_);
+  timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr64, res64, coefMG(depth), bottom_, sp_.eps, bottomMetric_, s_); });
+  convert(corr, corr64, L.nelem, s_);
+}
+
 // MultiGrid::cycle (MultiGrid.H:629-696), V-cycle (m_cycle = 1).
-void Solver::mgCycle(int depth, double* corr, double* res) {
+template <class T>
+void Solver::mgCycle(int depth, T* corr, T* res) {
   const int D = 1 + (int)mg_.size();
   if (depth == D - 1) {
     if (bottomCells_ == 1) {
       relaxMG(depth, corr, res, 1);
     } else {
       relaxMG(depth, corr, res, sp_.bottom);
-      const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
-      timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr, res, coefMG(depth), bottom_, sp_.eps, bottomMetric_, s_); });
+      bottom<T>(depth, corr, res);
     }
     return;
   }
   const LevelDev& F = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
   const LevelDev& C = mgDev_[depth];
-  double* corrC = mgf_[depth].corr;
-  double* resC = mgf_[depth].res;
+  T* corrC = mgF<T>()[depth].corr;
+  T* resC = mgF<T>()[depth].res;
   relaxMG(depth, corr, res, sp_.pre);
   // restrictResidual: homogeneous CF (none) + exchange + BC, RESTRICTRES.
   fill(F, corr, true);
-  restrictMG(F, C, resC, corr, res, coefMG(depth), s_);
+  restrictMG(F, C, resC, corr, res, coefM<T>(depth), s_);
   zeroField(C, corrC);
   for (int img = 0; img < sp_.numMG; ++img) mgCycle(depth + 1, corrC, resC);
   prolongMG(F, C, corr, corrC, s_);
@@ -601,52 +664,58 @@ void Solver::mgCycle(int depth, double* corr, double* res) {
 }
 
 // AMRMultiGrid::AMRVCycle (AMRMultiGrid.H:1341-1419), l_base = 0.
+template <class T>
 void Solver::amrVCycle(int ilev, int lmax) {
+  std::vector<FieldsT<T>>& lev = levF<T>();
   if (ilev == lmax)
     for (int l = 0; l <= lmax; ++l) {
-      copyField(amrDev_[l], lev_[l].res, lev_[l].ures);
-      zeroField(amrDev_[l], lev_[l].corr);
+      copyField(amrDev_[l], lev[l].res, lev[l].ures);
+      zeroField(amrDev_[l], lev[l].corr);
     }
   if (lmax == 0) {
-    mgCycle(0, lev_[0].ucorr, lev_[0].ures);
+    mgCycle(0, lev[0].ucorr, lev[0].ures);
     return;
   }
   if (ilev == 0) {
-    mgCycle(0, lev_[0].corr, lev_[0].res);
-    incr(amrDev_[0], lev_[0].ucorr, lev_[0].corr, 1.0, s_);
+    mgCycle(0, lev[0].corr, lev[0].res);
+    incr(amrDev_[0], lev[0].ucorr, lev[0].corr, 1.0, s_);
     return;
   }
   const LevelDev& L = amrDev_[ilev];
   const LevelDev& Lc = amrDev_[ilev - 1];
-  LevelFields& f = lev_[ilev];
-  LevelFields& fc = lev_[ilev - 1];
+  FieldsT<T>& f = lev[ilev];
+  FieldsT<T>& fc = lev[ilev - 1];
+  const double w = sizeof(T);
   relaxAMR(ilev, f.corr, f.res, sp_.pre);
   incr(L, f.ucorr, f.corr, 1.0, s_);
   zeroField(Lc, fc.corr);
-  std::vector<double*> res(lmax + 1), ucorr(lmax + 1), ures(lmax + 1);
+  std::vector<T*> res(lmax + 1), ucorr(lmax + 1), ures(lmax + 1);
   for (int l = 0; l <= lmax; ++l) {
-    res[l] = lev_[l].res;
-    ucorr[l] = lev_[l].ucorr;
-    ures[l] = lev_[l].ures;
+    res[l] = lev[l].res;
+    ucorr[l] = lev[l].ucorr;
+    ures[l] = lev[l].ures;
   }
   amrResidualLevel(ilev - 1, lmax, res, ucorr, ures);
   // AMRRestrictS: residual of the correction into the scratch (uberCorrection),
   // averaged straight onto the coarse residual (assignCopier).
   quadCF(L, f.corr, fc.corr, s_);
   fill(L, f.corr, false);
-  timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.ucorr, f.corr, f.res, coefAMR(ilev), s_); });
+  timed(P_OP, amr_[ilev].grids.numCells() * w * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.ucorr, f.corr, f.res, coefA<T>(ilev), s_); });
   averageAMR(L, Lc, fc.res, f.ucorr, s_);
-  for (int img = 0; img < sp_.numMG; ++img) amrVCycle(ilev - 1, lmax);
+  for (int img = 0; img < sp_.numMG; ++img) amrVCycle<T>(ilev - 1, lmax);
   // AMRProlongS, AMRUpdateResidual, post-smoothing of the correction's correction.
   prolongAMR(L, Lc, f.corr, fc.corr, s_);
   quadCF(L, f.corr, fc.corr, s_);
   fill(L, f.corr, false);
-  timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.res, f.corr, f.res, coefAMR(ilev), s_); });
+  timed(P_OP, amr_[ilev].grids.numCells() * w * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.res, f.corr, f.res, coefA<T>(ilev), s_); });
   zeroField(L, f.ucorr);
   relaxAMR(ilev, f.ucorr, f.res, sp_.post);
   incr(L, f.corr, f.ucorr, 1.0, s_);
   copyField(L, f.ucorr, f.corr);
 }
+
+template void Solver::amrVCycle<double>(int, int);
+template void Solver::amrVCycle<float>(int, int);
 
 double Solver::residualNorm() {
   int lmax = numLevels() - 1;
@@ -684,11 +753,115 @@ SolveResult Solver::solve(const SolveParams& p, bool zeroPhi) {
   bool goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
   while (goIter && goRedu && goHang && goNorm) {
     normLast = rnorm;
-    amrVCycle(lmax, lmax);
+    amrVCycle<double>(lmax, lmax);
     for (int l = 0; l <= lmax; ++l) {
       incr(amrDev_[l], lev_[l].phi, lev_[l].ucorr, 1.0, s_);
       zeroField(amrDev_[l], lev_[l].ucorr);
     }
+    rnorm = computeAMRResidual(ures, phi, rhs, lmax);
+    iter++;
+    out.history.push_back(rnorm);
+    goNorm = rnorm > p.normThresh;
+    goRedu = rnorm > p.eps * r0;
+    goIter = iter < p.iterMax;
+    goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
+  }
+  out.exitStatus = int(!goRedu) + int(!goIter) * 2 + int(!goHang) * 4 + int(!goNorm) * 8;
+  out.iterations = iter;
+  return out;
+}
+
+float* Solver::allocF(size_t n) {
+  bufs_.emplace_back(new DevBuf(n * sizeof(float)));
+  float* p = (float*)bufs_.back()->p;
+  ck(cudaMemsetAsync(p, 0, n * sizeof(float), s_), "memset");
+  return p;
+}
+
+void Solver::ensure32() {
+  if (!have32_) {
+    lev32_.resize(amr_.size());
+    for (size_t l = 0; l < amr_.size(); ++l) {
+      const size_t n = amr_[l].nelem;
+      FieldsT<float>& f = lev32_[l];
+      f.ures = allocF(n);
+      f.ucorr = allocF(n);
+      f.corr = allocF(n);
+      f.res = allocF(n);
+      if (desc_.vc) {
+        f.a = allocF(n);
+        for (int d = 0; d < 3; ++d) f.b[d] = allocF(n);
+        f.lambda = allocF(n);
+      }
+    }
+    mgf32_.resize(mg_.size());
+    for (size_t d = 0; d < mg_.size(); ++d) {
+      const size_t n = mg_[d].nelem;
+      FieldsT<float>& f = mgf32_[d];
+      f.corr = allocF(n);
+      f.res = allocF(n);
+      if (desc_.vc) {
+        f.a = allocF(n);
+        for (int k = 0; k < 3; ++k) f.b[k] = allocF(n);
+        f.lambda = allocF(n);
+      }
+    }
+    have32_ = true;
+    coef32Stale_ = true;
+  }
+  if (desc_.vc && coef32Stale_) {
+    // The FP32 operators use the FP64 coefficients (and relaxation
+    // coefficient) rounded to FP32.
+    for (size_t l = 0; l < amr_.size(); ++l) {
+      const int64_t n = amr_[l].nelem;
+      convert(lev32_[l].a, lev_[l].a, n, s_);
+      for (int d = 0; d < 3; ++d) convert(lev32_[l].b[d], lev_[l].b[d], n, s_);
+      convert(lev32_[l].lambda, lev_[l].lambda, n, s_);
+    }
+    for (size_t d = 0; d < mg_.size(); ++d) {
+      const int64_t n = mg_[d].nelem;
+      convert(mgf32_[d].a, mgf_[d].a, n, s_);
+      for (int k = 0; k < 3; ++k) convert(mgf32_[d].b[k], mgf_[d].b[k], n, s_);
+      convert(mgf32_[d].lambda, mgf_[d].lambda, n, s_);
+    }
+    coef32Stale_ = false;
+  }
+}
+
+// Iterative refinement: the FP64 residual of the FP64 phi drives one FP32
+// AMR V-cycle per iteration (its input rounded to FP32), whose correction is
+// added to phi in FP64; the stopping rules, norms and residual history are
+// those of solve().
+SolveResult Solver::solveMixed(const SolveParams& p, bool zeroPhi) {
+  ensure32();
+  sp_ = p;
+  const int lmax = numLevels() - 1;
+  SolveResult out;
+  std::vector<double*> ures(lmax + 1), phi(lmax + 1), rhs(lmax + 1);
+  for (int l = 0; l <= lmax; ++l) {
+    zeroField(amrDev_[l], lev_[l].ures);
+    if (zeroPhi) zeroField(amrDev_[l], lev_[l].phi);
+    ures[l] = lev_[l].ures;
+    phi[l] = lev_[l].phi;
+    rhs[l] = lev_[l].rhs;
+  }
+  const double r0 = computeAMRResidual(ures, phi, rhs, lmax);
+  double rnorm = r0, normLast = 2 * r0;
+  bottomMetric_ = r0;
+  out.history.push_back(rnorm);
+  int iter = 0;
+  bool goNorm = rnorm > p.normThresh;
+  bool goRedu = rnorm > p.eps * r0;
+  bool goIter = iter < p.iterMax;
+  bool goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
+  while (goIter && goRedu && goHang && goNorm) {
+    normLast = rnorm;
+    for (int l = 0; l <= lmax; ++l) {
+      convert(lev32_[l].ures, lev_[l].ures, amrDev_[l].nelem, s_);
+      zeroField(amrDev_[l], lev32_[l].ucorr);
+    }
+    amrVCycle<float>(lmax, lmax);
+    for (int l = 0; l <= lmax; ++l) incrMixed(amrDev_[l], lev_[l].phi, lev32_[l].ucorr, s_);
     rnorm = computeAMRResidual(ures, phi, rhs, lmax);
     iter++;
     out.history.push_back(rnorm);

@@ -90,6 +90,16 @@ int cmg_set_phi(cmg_hierarchy* h, int level, const double* data, int on_device);
 int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
               double* history, int history_cap, int* history_len);
 
+/* Mixed precision (no counterpart in the reference, which runs FP64
+ * throughout): the loop of AMRMultiGrid::solve with each AMR V-cycle run in
+ * FP32 (smoothing, restriction, prolongation, the cycle's own residual
+ * updates) on the FP64 residual rounded to FP32, its correction added to the
+ * FP64 phi; the composite residual with its flux-register correction, the
+ * BiCGStab bottom solve and the norms stay FP64.  Same stopping rules and
+ * history as cmg_solve; iterations counts the FP64 refinement steps. */
+int cmg_solve_mixed(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
+                    double* history, int history_cap, int* history_len);
+
 /* AMRMultiGrid::computeAMRResidual(phi, rhs, lmax, 0) (AMRMultiGrid.H:738-750). */
 int cmg_residual_norm(cmg_hierarchy* h, double* out);
 

@@ -36,3 +36,20 @@ def golden(name):
 
 def golden_names():
     return sorted(f[:-5] for f in os.listdir(GOLDEN) if f.endswith(".json"))
+
+
+def covered_mask(boxes, finer_boxes):
+    """Valid cells of a level (boxes in layout order, x fastest) covered by the
+    next finer level (ratio 2): the cells outside the composite solution."""
+    masks = []
+    fine = [(np.array(b[:3]) // 2, np.array(b[3:]) // 2) for b in finer_boxes]
+    for b in boxes:
+        lo, hi = np.array(b[:3]), np.array(b[3:])
+        n = hi - lo + 1
+        m = np.zeros((n[2], n[1], n[0]), bool)
+        for flo, fhi in fine:
+            a, c = np.maximum(lo, flo), np.minimum(hi, fhi)
+            if np.all(a <= c):
+                m[a[2] - lo[2]:c[2] - lo[2] + 1, a[1] - lo[1]:c[1] - lo[1] + 1, a[0] - lo[0]:c[0] - lo[0] + 1] = True
+        masks.append(m.ravel())
+    return np.concatenate(masks) if masks else np.zeros(0, bool)

@@ -8,7 +8,9 @@ coarsened-fine copier plans, the per-iteration composite residual history,
 the exit status, checksums of the right-hand side, and phi (all cells for
 small cases, a strided sample for the benchmark-size cases).
 
-    python tests/golden/make_golden.py [case ...]
+    python tests/golden/make_golden.py [--from=<prefix>] [case ...]
+
+(--from reuses an oracle run already written with out=<prefix>.)
 """
 import json
 import os
@@ -34,14 +36,18 @@ CASES = {
     "vc_2lev_64": ("n0=64 levels=2 maxbox=32 op=1 alpha=1 beta=-1", False),
     "config0_poisson_64": ("n0=64 levels=1 maxbox=32 op=0 alpha=0 beta=1", False),
     "config1_vc_3lev_128": ("n0=128 levels=3 maxbox=32 op=1 alpha=1 beta=-1", False),
+    # the ~40M-cell mixed-precision workload: sparser samples keep the fixture small
+    "config2_vc_3lev_256": ("n0=256 levels=3 maxbox=32 op=1 alpha=1 beta=-1", False, 1009),
 }
 SAMPLE_STRIDE = 97
 
 
-def run_case(name, args, full):
-    tmp = os.path.join("/tmp", "cmg_golden_" + name)
-    cmd = [ORACLE] + args.split() + ["out=" + tmp]
-    subprocess.run(cmd, check=True)
+def run_case(name, args, full, stride=SAMPLE_STRIDE, prefix=None):
+    """prefix: reuse an oracle run already written to <prefix>.json/.bin."""
+    tmp = prefix or os.path.join("/tmp", "cmg_golden_" + name)
+    if not prefix:
+        cmd = [ORACLE] + args.split() + ["out=" + tmp]
+        subprocess.run(cmd, check=True)
     meta = json.load(open(tmp + ".json"))
     raw = np.fromfile(tmp + ".bin", dtype=np.float64)
     pos = 0
@@ -63,14 +69,14 @@ def run_case(name, args, full):
     meta["args"] = args
     meta["rhs_sum"] = [float(np.sum(r)) for r, _ in levels]
     meta["phi_absmax"] = [float(np.max(np.abs(p))) for _, p in levels]
-    meta["sample_stride"] = SAMPLE_STRIDE
+    meta["sample_stride"] = stride
     arrays = {}
     for lev, (rhs, phi) in enumerate(levels):
         if full:
             arrays[f"phi{lev}"] = phi
         else:
-            arrays[f"phi{lev}_sample"] = phi[::SAMPLE_STRIDE].copy()
-        arrays[f"rhs{lev}_sample"] = rhs[::SAMPLE_STRIDE].copy()
+            arrays[f"phi{lev}_sample"] = phi[::stride].copy()
+        arrays[f"rhs{lev}_sample"] = rhs[::stride].copy()
     meta["full"] = full
     if len(json.dumps(meta.get("exchange_plans", []))) > 400000:
         # plans of the big cases are checked through their sizes only
@@ -83,9 +89,13 @@ def run_case(name, args, full):
 
 
 def main():
-    names = sys.argv[1:] or list(CASES)
+    args = sys.argv[1:]
+    prefix = None
+    if args and args[0].startswith("--from="):
+        prefix = args.pop(0)[len("--from="):]
+    names = args or list(CASES)
     for n in names:
-        run_case(n, *CASES[n])
+        run_case(n, *CASES[n], prefix=prefix)
 
 
 if __name__ == "__main__":

@@ -227,6 +227,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     meta = golden_meta(wl["golden"])
@@ -251,6 +252,7 @@ def main():
     params = cmg.solve_params(pre=meta["pre"], post=meta["post"], bottom=meta["bottom"], iter_max=meta["iters"],
                               eps=meta["eps"], hang=meta["hang"])
     mixed = bool(wl.get("mixed", False))
+    h.use_graphs(not args.no_graphs)
     stream = torch.cuda.ExternalStream(h.stream())
     ncells = [h.num_cells(l) for l in range(len(meta["boxes"]))]
 
@@ -390,7 +392,8 @@ def main():
             "config": {"workload": wl["name"], "global_batch": world, "cells": sum(ncells),
                        "levels": len(ncells), "boxes": [len(b) for b in meta["boxes"]],
                        "vcycles_per_solve": n_iter, "l2": "working set > L2 (no flush)",
-                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
+                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+                       "cuda_graphs": not args.no_graphs},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
             "roofline": roofline, "breakdown": breakdown, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches,

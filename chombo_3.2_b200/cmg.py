@@ -186,6 +186,9 @@ class Hierarchy:
                   _ptr(hist), len(hist), ctypes.byref(hl)))
         return {"exit_status": st.value, "iterations": it.value, "history": hist[:hl.value].copy()}
 
+    def use_graphs(self, on=True):
+        _check(lib().cmg_use_graphs(self.h, int(on)))
+
     def residual_norm(self):
         r = ctypes.c_double()
         _check(lib().cmg_residual_norm(self.h, ctypes.byref(r)))

@@ -274,6 +274,13 @@ int solveWith(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* ex
 }
 }  // namespace
 
+int cmg_use_graphs(cmg_hierarchy* h, int on) {
+  return guard([&]() {
+    needLevel(h, 0);
+    h->solver->setUseGraphs(on != 0);
+  });
+}
+
 int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
               double* history, int history_cap, int* history_len) {
   return solveWith(h, p, zero_phi, exit_status, iterations, history, history_cap, history_len, false);

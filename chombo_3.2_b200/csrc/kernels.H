@@ -115,10 +115,12 @@ struct BottomWork {
 };
 // BiCGStab bottom solve of L(phi) = rhs (homogeneous boundary conditions) on
 // one level, one thread block, reference summation order.  eps and metric are
-// the tolerance and convergence metric AMRMultiGrid hands its bottom solver.
-// phi and rhs are level fields; the coefficients come from w.
+// the tolerance and convergence metric AMRMultiGrid hands its bottom solver
+// (the metric read from device memory when the kernel runs, so a captured
+// launch serves every solve).  phi and rhs are level fields; the
+// coefficients come from w.
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
-                 double eps, double metric, cudaStream_t s);
+                 double eps, const double* metric, cudaStream_t s);
 // dst[slot] = fab[w.fab[slot]] for every slot of the bottom level.
 void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream_t s);
 

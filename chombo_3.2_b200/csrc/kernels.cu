@@ -498,7 +498,8 @@ struct BottomArgs {
   double* phiFab;
   const double* rhsFab;
   double *phi, *rhs, *r, *rt, *e, *p, *pt, *st, *t, *v;
-  double eps, metric, reps, hang, small, mult;
+  double eps, reps, hang, small, mult;
+  const double* metric;  // device scalar: the solve's initial residual norm
   int imax, numRestarts;
 };
 
@@ -657,7 +658,8 @@ __device__ void bicgstab(const BottomArgs& A) {
   norm[1] = norm[0];
   double alpha[2] = {0, 0}, beta[2] = {0, 0}, omega[2] = {0, 0};
   bool init = true;
-  if (A.metric > 0) initial_norm = A.metric;
+  const double metric = *A.metric;
+  if (metric > 0) initial_norm = metric;
   while ((iter < A.imax && norm[0] > A.eps * norm[1]) && (norm[1] > 0)) {
     iter++;
     norm[1] = norm[0];
@@ -929,7 +931,7 @@ void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s) {
 long long launchCount() { return g_launches.load(std::memory_order_relaxed); }
 
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
-                 double eps, double metric, cudaStream_t s) {
+                 double eps, const double* metric, cudaStream_t s) {
   BottomArgs A;
   A.W = w;
   A.boxes = L.boxes;

@@ -97,6 +97,10 @@ class Solver {
   // with its flux-register correction, the bottom solve and the norms stay
   // FP64 (no counterpart in the reference, which is FP64 throughout).
   SolveResult solveMixed(const SolveParams& p, bool zeroPhi = true);
+  // Replay each solver iteration from a CUDA graph captured on first use
+  // (per precision and smoothing parameters); off by default.  Profiling
+  // (profileEnable) runs the uncaptured path.
+  void setUseGraphs(bool on);
 
  private:
   void uploadLevel(const LevelPlan& p, LevelDev& d);
@@ -117,6 +121,28 @@ class Solver {
   template <class T>
   void amrResidualLevel(int ilev, int lmax, std::vector<T*>& res, std::vector<T*>& phi, std::vector<T*>& rhs);
   double computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);
+  void launchAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);
+  double readNorm();
+  SolveResult solveImpl(const SolveParams& p, bool zeroPhi, bool mixed);
+  void iterationBody(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi, std::vector<double*>& rhs);
+  cudaGraphExec_t iterationGraph(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi,
+                                 std::vector<double*>& rhs);
+  struct GraphKey {
+    bool mixed;
+    int pre, post, bottom, numMG;
+    double eps;
+    bool operator<(const GraphKey& o) const {
+      if (mixed != o.mixed) return mixed < o.mixed;
+      if (pre != o.pre) return pre < o.pre;
+      if (post != o.post) return post < o.post;
+      if (bottom != o.bottom) return bottom < o.bottom;
+      if (numMG != o.numMG) return numMG < o.numMG;
+      return eps < o.eps;
+    }
+  };
+  std::map<GraphKey, cudaGraphExec_t> graphs_;
+  bool useGraphs_ = false;
+  double hostMetric_ = 0;
   template <class T> void amrVCycle(int ilev, int lmax);
   template <class T> void mgCycle(int depth, T* corr, T* res);
   template <class T> void bottom(int depth, T* corr, T* res);
@@ -151,7 +177,7 @@ class Solver {
   double* dNorm_ = nullptr;
   int64_t bottomCells_ = 0;
   SolveParams sp_;
-  double bottomMetric_ = 0;
+  double* dMetric_ = nullptr;  // bottom solver's convergence metric (device)
   std::vector<std::vector<double>> hostA_, hostB_[3];
 
   struct ProfRec {

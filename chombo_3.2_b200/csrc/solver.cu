@@ -228,6 +228,7 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), des
   bufs_.emplace_back(new DevBuf(4 * sizeof(int)));
   bottom_.status = (int*)bufs_.back()->p;
   dNorm_ = alloc(1);
+  dMetric_ = alloc(1);
   if (desc.vc) {
     hostA_.resize(nlev);
     for (int d = 0; d < 3; ++d) hostB_[d].resize(nlev);
@@ -235,7 +236,10 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), des
   ck(cudaStreamSynchronize(s_), "setup");
 }
 
-Solver::~Solver() { cudaStreamSynchronize(s_); }
+Solver::~Solver() {
+  cudaStreamSynchronize(s_);
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+}
 
 int64_t Solver::numFaces(int l, int dir) const {
   int64_t n = 0;
@@ -605,12 +609,23 @@ void Solver::amrResidualLevel(int ilev, int lmax, std::vector<T*>& res, std::vec
 // AMRMultiGrid::computeAMRResidual (AMRMultiGrid.H:682-736).
 double Solver::computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs,
                                   int lmax) {
+  launchAMRResidual(res, phi, rhs, lmax);
+  return readNorm();
+}
+
+// The device work of computeAMRResidual: residuals, zeroCovered, max-norm
+// into dNorm_ (no host synchronisation, so it can be captured).
+void Solver::launchAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs,
+                               int lmax) {
   ck(cudaMemsetAsync(dNorm_, 0, sizeof(double), s_), "norm reset");
   for (int ilev = 0; ilev <= lmax; ++ilev) {
     amrResidualLevel(ilev, lmax, res, phi, rhs);
     if (ilev != lmax) zeroCovered(amrDev_[ilev], res[ilev], s_);
     maxNorm(amrDev_[ilev], res[ilev], dNorm_, s_);
   }
+}
+
+double Solver::readNorm() {
   double h = 0;
   ck(cudaMemcpyAsync(&h, dNorm_, sizeof(double), cudaMemcpyDeviceToHost, s_), "norm d2h");
   ck(cudaStreamSynchronize(s_), "norm sync");
@@ -623,7 +638,7 @@ double Solver::computeAMRResidual(std::vector<double*>& res, std::vector<double*
 template <>
 void Solver::bottom<double>(int depth, double* corr, double* res) {
   const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
-  timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr, res, coefMG(depth), bottom_, sp_.eps, bottomMetric_, s_); });
+  timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr, res, coefMG(depth), bottom_, sp_.eps, dMetric_, s_); });
 }
 template <>
 void Solver::bottom<float>(int depth, float* corr, float* res) {
@@ -632,7 +647,7 @@ void Solver::bottom<float>(int depth, float* corr, float* res) {
   double* res64 = depth == 0 ? lev_[0].res : mgf_[depth - 1].res;
   convert(corr64, corr, L.nelem, s_);
   convert(res64, res, L.nelem, s_);
-  timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr64, res64, coefMG(depth), bottom_, sp_.eps, bottomMetric_, s_); });
+  timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr64, res64, coefMG(depth), bottom_, sp_.eps, dMetric_, s_); });
   convert(corr, corr64, L.nelem, s_);
 }
 
@@ -729,7 +744,38 @@ double Solver::residualNorm() {
 }
 
 // AMRMultiGrid::solve -> solveNoInitResid (AMRMultiGrid.H:894-1124).
-SolveResult Solver::solve(const SolveParams& p, bool zeroPhi) {
+SolveResult Solver::solve(const SolveParams& p, bool zeroPhi) { return solveImpl(p, zeroPhi, false); }
+
+// Iterative refinement: the FP64 residual of the FP64 phi drives one FP32
+// AMR V-cycle per iteration (its input rounded to FP32), whose correction is
+// added to phi in FP64; the stopping rules, norms and residual history are
+// those of solve().
+SolveResult Solver::solveMixed(const SolveParams& p, bool zeroPhi) { return solveImpl(p, zeroPhi, true); }
+
+// One iteration's device work after the norm check: the V-cycle, the update
+// of phi and the composite residual with its max-norm (into dNorm_).
+void Solver::iterationBody(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi,
+                           std::vector<double*>& rhs) {
+  const int lmax = numLevels() - 1;
+  if (!mixed) {
+    amrVCycle<double>(lmax, lmax);
+    for (int l = 0; l <= lmax; ++l) {
+      incr(amrDev_[l], lev_[l].phi, lev_[l].ucorr, 1.0, s_);
+      zeroField(amrDev_[l], lev_[l].ucorr);
+    }
+  } else {
+    for (int l = 0; l <= lmax; ++l) {
+      convert(lev32_[l].ures, lev_[l].ures, amrDev_[l].nelem, s_);
+      zeroField(amrDev_[l], lev32_[l].ucorr);
+    }
+    amrVCycle<float>(lmax, lmax);
+    for (int l = 0; l <= lmax; ++l) incrMixed(amrDev_[l], lev_[l].phi, lev32_[l].ucorr, s_);
+  }
+  launchAMRResidual(ures, phi, rhs, lmax);
+}
+
+SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
+  if (mixed) ensure32();
   sp_ = p;
   const int lmax = numLevels() - 1;
   SolveResult out;
@@ -744,21 +790,25 @@ SolveResult Solver::solve(const SolveParams& p, bool zeroPhi) {
   }
   const double r0 = computeAMRResidual(ures, phi, rhs, lmax);
   double rnorm = r0, normLast = 2 * r0;
-  bottomMetric_ = r0;  // setConvergenceMetrics(m_initial_rnorm, cushion * m_eps)
+  // setConvergenceMetrics(m_initial_rnorm, cushion * m_eps) of the bottom solver
+  hostMetric_ = r0;
+  ck(cudaMemcpyAsync(dMetric_, &hostMetric_, sizeof(double), cudaMemcpyHostToDevice, s_), "metric");
   out.history.push_back(rnorm);
   int iter = 0;
   bool goNorm = rnorm > p.normThresh;
   bool goRedu = rnorm > p.eps * r0;
   bool goIter = iter < p.iterMax;
   bool goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
+  const bool graph = useGraphs_ && !profOn_;
   while (goIter && goRedu && goHang && goNorm) {
     normLast = rnorm;
-    amrVCycle<double>(lmax, lmax);
-    for (int l = 0; l <= lmax; ++l) {
-      incr(amrDev_[l], lev_[l].phi, lev_[l].ucorr, 1.0, s_);
-      zeroField(amrDev_[l], lev_[l].ucorr);
+    if (graph) {
+      cudaGraphExec_t exec = iterationGraph(mixed, ures, phi, rhs);
+      ck(cudaGraphLaunch(exec, s_), "graph launch");
+    } else {
+      iterationBody(mixed, ures, phi, rhs);
     }
-    rnorm = computeAMRResidual(ures, phi, rhs, lmax);
+    rnorm = readNorm();
     iter++;
     out.history.push_back(rnorm);
     goNorm = rnorm > p.normThresh;
@@ -770,6 +820,35 @@ SolveResult Solver::solve(const SolveParams& p, bool zeroPhi) {
   out.iterations = iter;
   return out;
 }
+
+// The iteration body captured once per (precision, smoothing parameters)
+// into a CUDA graph and replayed: every pointer and launch argument of the
+// body is fixed for the hierarchy; the bottom solver's metric is read from
+// device memory at run time.
+cudaGraphExec_t Solver::iterationGraph(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi,
+                                       std::vector<double*>& rhs) {
+  GraphKey key{mixed, sp_.pre, sp_.post, sp_.bottom, sp_.numMG, sp_.eps};
+  auto it = graphs_.find(key);
+  if (it != graphs_.end()) return it->second;
+  cudaGraph_t g = nullptr;
+  ck(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal), "begin capture");
+  try {
+    iterationBody(mixed, ures, phi, rhs);
+  } catch (...) {
+    cudaStreamEndCapture(s_, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  ck(cudaStreamEndCapture(s_, &g), "end capture");
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  ck(e, "graph instantiate");
+  graphs_[key] = exec;
+  return exec;
+}
+
+void Solver::setUseGraphs(bool on) { useGraphs_ = on; }
 
 float* Solver::allocF(size_t n) {
   bufs_.emplace_back(new DevBuf(n * sizeof(float)));
@@ -826,53 +905,6 @@ void Solver::ensure32() {
     }
     coef32Stale_ = false;
   }
-}
-
-// Iterative refinement: the FP64 residual of the FP64 phi drives one FP32
-// AMR V-cycle per iteration (its input rounded to FP32), whose correction is
-// added to phi in FP64; the stopping rules, norms and residual history are
-// those of solve().
-SolveResult Solver::solveMixed(const SolveParams& p, bool zeroPhi) {
-  ensure32();
-  sp_ = p;
-  const int lmax = numLevels() - 1;
-  SolveResult out;
-  std::vector<double*> ures(lmax + 1), phi(lmax + 1), rhs(lmax + 1);
-  for (int l = 0; l <= lmax; ++l) {
-    zeroField(amrDev_[l], lev_[l].ures);
-    if (zeroPhi) zeroField(amrDev_[l], lev_[l].phi);
-    ures[l] = lev_[l].ures;
-    phi[l] = lev_[l].phi;
-    rhs[l] = lev_[l].rhs;
-  }
-  const double r0 = computeAMRResidual(ures, phi, rhs, lmax);
-  double rnorm = r0, normLast = 2 * r0;
-  bottomMetric_ = r0;
-  out.history.push_back(rnorm);
-  int iter = 0;
-  bool goNorm = rnorm > p.normThresh;
-  bool goRedu = rnorm > p.eps * r0;
-  bool goIter = iter < p.iterMax;
-  bool goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
-  while (goIter && goRedu && goHang && goNorm) {
-    normLast = rnorm;
-    for (int l = 0; l <= lmax; ++l) {
-      convert(lev32_[l].ures, lev_[l].ures, amrDev_[l].nelem, s_);
-      zeroField(amrDev_[l], lev32_[l].ucorr);
-    }
-    amrVCycle<float>(lmax, lmax);
-    for (int l = 0; l <= lmax; ++l) incrMixed(amrDev_[l], lev_[l].phi, lev32_[l].ucorr, s_);
-    rnorm = computeAMRResidual(ures, phi, rhs, lmax);
-    iter++;
-    out.history.push_back(rnorm);
-    goNorm = rnorm > p.normThresh;
-    goRedu = rnorm > p.eps * r0;
-    goIter = iter < p.iterMax;
-    goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
-  }
-  out.exitStatus = int(!goRedu) + int(!goIter) * 2 + int(!goHang) * 4 + int(!goNorm) * 8;
-  out.iterations = iter;
-  return out;
 }
 
 double Solver::vcycleBytes(const SolveParams& p) const {

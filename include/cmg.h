@@ -90,6 +90,13 @@ int cmg_set_phi(cmg_hierarchy* h, int level, const double* data, int on_device);
 int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
               double* history, int history_cap, int* history_len);
 
+/* Replays every solver iteration (V-cycle, phi update, composite residual)
+ * from a CUDA graph captured on its first use for the given precision and
+ * smoothing parameters (no counterpart in the reference).  Same kernels in
+ * the same order, so the same results; saves the per-launch host cost.
+ * Off by default; profiling (cmg_profile_enable) runs uncaptured. */
+int cmg_use_graphs(cmg_hierarchy* h, int on);
+
 /* Mixed precision (no counterpart in the reference, which runs FP64
  * throughout): the loop of AMRMultiGrid::solve with each AMR V-cycle run in
  * FP32 (smoothing, restriction, prolongation, the cycle's own residual

@@ -43,6 +43,11 @@ WORKLOADS = {
                 "max box 32, fill 0.75, Dirichlet, GSRB 4+4, BiCGStab bottom, rel. residual 1e-10; FP32 "
                 "V-cycles inside FP64 iterative refinement (residual, reflux, bottom, norms FP64)",
     },
+    "config2-fp64": {
+        "golden": "config2_vc_3lev_256",
+        "name": "3-level VC Helmholtz (VCAMRPoissonOp2 alpha=1 beta=-1), base 256^3, ratio 2, block 8, "
+                "max box 32, fill 0.75, Dirichlet, GSRB 4+4, BiCGStab bottom, rel. residual 1e-10; plain FP64",
+    },
     "config1-mixed": {
         "golden": "config1_vc_3lev_128",
         "mixed": True,

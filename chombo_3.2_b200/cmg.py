@@ -68,6 +68,23 @@ def boxes_array(boxes):
     return arr
 
 
+def synthetic_hierarchy(n0, levels, max_box=32, block_factor=8, fill_ratio=0.75, seed=20261203, thresh=0.1):
+    """Box lists (lo0, lo1, lo2, hi0, hi1, hi2) per level of the seeded example hierarchy."""
+    L = lib()
+    nl, tot = ctypes.c_int(), ctypes.c_int()
+    counts = (ctypes.c_int * levels)()
+    args = (int(n0), int(levels), int(max_box), int(block_factor), ctypes.c_double(fill_ratio),
+            ctypes.c_uint64(seed), ctypes.c_double(thresh), ctypes.byref(nl), counts)
+    _check(L.cmg_synthetic_hierarchy(*args, None, 0, ctypes.byref(tot)))
+    out = (Box * max(tot.value, 1))()
+    _check(L.cmg_synthetic_hierarchy(*args, out, tot.value, ctypes.byref(tot)))
+    res, k = [], 0
+    for l in range(nl.value):
+        res.append([tuple(out[k + i].lo) + tuple(out[k + i].hi) for i in range(counts[l])])
+        k += counts[l]
+    return res
+
+
 def domain_split(lo, hi, max_box, block_factor):
     L = lib()
     n = ctypes.c_int()

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/cmg.h"
+#include "meshrefine.H"
 #include "noalloc.H"
 #include "solver.H"
 #include "synthetic.H"
@@ -305,6 +306,27 @@ int cmg_residual_norm_noalloc(cmg_hierarchy* h, double* out) {
     needLevel(h, 0);
     if (!out) throw std::invalid_argument("cmg: null output pointer");
     *out = cmg::residualNormNoAlloc(*h->solver);
+  });
+}
+
+int cmg_synthetic_hierarchy(int n0, int nlevels, int max_box, int block_factor, double fill_ratio, uint64_t seed,
+                            double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes, int cap, int* ntotal) {
+  return guard([&]() {
+    if (!nlevels_out || !nboxes || !ntotal) throw std::invalid_argument("cmg: null output pointer");
+    if (max_box < 0 || block_factor < 1 || !(fill_ratio > 0.0 && fill_ratio <= 1.0))
+      throw std::invalid_argument("cmg: invalid grid generation parameters");
+    std::vector<std::vector<cmg::Box>> g =
+        cmg::syntheticHierarchy(n0, nlevels, max_box, block_factor, fill_ratio, seed, thresh);
+    *nlevels_out = (int)g.size();
+    int total = 0;
+    for (size_t l = 0; l < g.size(); ++l) {
+      nboxes[l] = (int)g[l].size();
+      for (const cmg::Box& b : g[l]) {
+        if (boxes && total < cap) fromBox(b, boxes[total]);
+        ++total;
+      }
+    }
+    *ntotal = total;
   });
 }
 

@@ -150,6 +150,20 @@ int cmg_layout_exchange_plan(const cmg_box* boxes, int nbox, int* items14, int c
 int cmg_layout_coarse_fine_plan(const cmg_box* fine, int nfine, const cmg_box* coarse, int ncoarse, int* items14,
                                 int cap, int* n);
 
+/* Grid generation (host only): the box lists of the examples' hierarchy
+ * for the seeded synthetic right-hand side.  Level 0 is domainSplit of
+ * [0, n0-1]^3 (BRMeshRefine.cpp:983-1092); each pass tags cells with
+ * |rhs| > thresh * max|rhs| on every level, grows the tags by one cell and
+ * calls MeshRefine::regrid (MeshRefine.cpp:438-729) with Berger-Rigoutsos
+ * clustering (BRMeshRefine::makeBoxes, BRMeshRefine.cpp:213-308), buffer 2,
+ * refinement ratio 2, adding one level per pass (as
+ * releasedExamples/AMRPoisson/execVariableCoefficient/VClocalFuncs.cpp:398-480).
+ * nboxes (capacity nlevels) receives the box count per level, boxes (capacity
+ * cap, may be NULL to query) the sorted boxes of every level in turn, ntotal
+ * their total. */
+int cmg_synthetic_hierarchy(int n0, int nlevels, int max_box, int block_factor, double fill_ratio, uint64_t seed,
+                            double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes, int cap, int* ntotal);
+
 /* Algorithmic bytes moved per V-cycle (roofline numerator). */
 int cmg_vcycle_bytes(const cmg_hierarchy* h, const cmg_solve_params* p, double* out);
 

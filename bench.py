@@ -224,16 +224,168 @@ def run_reference_arm(args, meta, wl):
     print(json.dumps(line))
 
 
+def round16(x):
+    return int(max(32, 16 * round(x / 16.0)))
+
+
+def batch_specs(n, seed):
+    """512 independent 2-level problems: base n0 log-uniform in [32, 128]
+    rounded to a multiple of 16, max box from {16, 24, 32}, Poisson
+    (AMRPoissonOp alpha=0 beta=1) or variable-coefficient Helmholtz
+    (VCAMRPoissonOp2 alpha=1 beta=-1, coefficients in [0.1, 10]) with p=1/2,
+    each with its own seed."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n):
+        n0 = min(128, round16(math.exp(rng.uniform(math.log(32), math.log(128)))))
+        vc = bool(rng.random() < 0.5)
+        specs.append(dict(n0=n0, levels=2, max_box=int(rng.choice([16, 24, 32])), block_factor=8, fill_ratio=0.75,
+                          thresh=0.1, seed=1000 + i, op=1 if vc else 0, alpha=1.0 if vc else 0.0,
+                          beta=-1.0 if vc else 1.0))
+    return specs
+
+
+def run_batch(args):
+    """Batching: N independent hierarchies resident on the GPU, solved
+    concurrently (one stream each, every iteration a CUDA-graph replay,
+    FP32 V-cycles inside FP64 refinement), against the plain FP64 drop-in
+    solving the same hierarchies one at a time."""
+    import concurrent.futures as cf
+    import torch
+    torch.cuda.set_device(0)
+    cmg = load_cmg()
+    specs = batch_specs(args.batch, 20261203)
+    params = cmg.solve_params(eps=1e-10)
+    wave = args.wave
+    t_batch = t_seq = 0.0
+    cells = 0
+    iters_mixed, iters_fp64, not_converged = [], [], 0
+    pool = cf.ThreadPoolExecutor(max_workers=args.inflight)
+
+    def build(sp):
+        boxes = cmg.synthetic_hierarchy(sp["n0"], sp["levels"], sp["max_box"], sp["block_factor"],
+                                        sp["fill_ratio"], sp["seed"], sp["thresh"])
+        h = cmg.Hierarchy(sp["n0"], boxes, op=sp["op"], alpha=sp["alpha"], beta=sp["beta"])
+        h.fill_synthetic(sp["seed"])
+        return h
+
+    for w0 in range(0, len(specs), wave):
+        hs = list(pool.map(build, specs[w0:w0 + wave]))
+        cells += sum(sum(h.num_cells(l) for l in range(h.nlev)) for h in hs)
+        for h in hs:
+            h.use_graphs(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        outs = list(pool.map(lambda h: h.solve(params, mixed=True), hs))
+        torch.cuda.synchronize()
+        t_batch += time.perf_counter() - t0
+        iters_mixed += [o["iterations"] for o in outs]
+        not_converged += sum(1 for o in outs if not (o["exit_status"] & 1))
+        for h in hs:
+            h.use_graphs(False)
+        t0 = time.perf_counter()
+        for h in hs:
+            o = h.solve(params)
+            iters_fp64.append(o["iterations"])
+        torch.cuda.synchronize()
+        t_seq += time.perf_counter() - t0
+        for h in hs:
+            h.close()
+    value = len(specs) / t_batch
+    base = len(specs) / t_seq
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": 1000.0 * t_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"{len(specs)} independent 2-level hierarchies, base 32^3-128^3 log-uniform (x16), "
+                               "max box 16/24/32, Poisson or VC Helmholtz, rel. residual 1e-10",
+                   "resident_per_wave": wave, "concurrent_streams": args.inflight, "cells": cells,
+                   "timing": "wall clock around the concurrent solves of each resident wave (host "
+                             "set-up of the hierarchies not timed)"},
+        "plain_fp64_one_at_a_time": {"value": base, "unit": "solves/s", "ratio": value / base},
+        "vcycles_mixed_mean": float(np.mean(iters_mixed)), "vcycles_fp64_mean": float(np.mean(iters_fp64)),
+        "not_converged": not_converged,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """Serving: open-loop Poisson arrivals at each rate; each request a 1-3
+    level hierarchy, base 32^3-256^3 log-uniform (x16), seeded inputs,
+    tolerance 1e-8 or 1e-10, admitted against a 120 GB device-memory budget
+    (cmg_serve); reports p50/p99 latency (arrival to solution on the host) and
+    completed solves/s per rate, beside the plain FP64 solve one request at a
+    time."""
+    import torch
+    torch.cuda.set_device(0)
+    cmg = load_cmg()
+    rates = [float(r) for r in args.rates.split(",")]
+
+    def stream(rate, n, seed):
+        rng = np.random.default_rng(seed)
+        t, reqs = 0.0, []
+        for i in range(n):
+            t += rng.exponential(1.0 / rate)
+            n0 = min(256, round16(math.exp(rng.uniform(math.log(32), math.log(256)))))
+            vc = bool(rng.random() < 0.5)
+            eps = 1e-8 if rng.random() < 0.5 else 1e-10
+            reqs.append(dict(arrival=t, n0=n0, levels=int(rng.integers(1, 4)), max_box=32, block_factor=8,
+                             seed=5000 + i, op=1 if vc else 0, alpha=1.0 if vc else 0.0,
+                             beta=-1.0 if vc else 1.0, params=cmg.solve_params(eps=eps), mixed=True,
+                             graphs=True))
+        return reqs
+
+    def stats(res, wall):
+        lat = np.array([r["finished"] - q for r, q in res])
+        ok = sum(1 for r, _ in res if r["error"] == 0 and r["exit_status"] & 1)
+        return {"p50_ms": 1000.0 * float(np.percentile(lat, 50)), "p99_ms": 1000.0 * float(np.percentile(lat, 99)),
+                "solves_per_s": len(res) / wall, "converged": ok, "requests": len(res),
+                "mean_setup_ms": 1000.0 * float(np.mean([r["setup_seconds"] for r, _ in res])),
+                "mean_solve_ms": 1000.0 * float(np.mean([r["solve_seconds"] for r, _ in res]))}
+
+    per_rate = {}
+    for rate in rates:
+        reqs = stream(rate, args.requests, int(rate))
+        res, wall = cmg.serve(reqs, hbm_budget=120e9, max_inflight=args.inflight, open_loop=True)
+        per_rate[str(int(rate))] = stats(list(zip(res, [q["arrival"] for q in reqs])), wall)
+    # The plain FP64 GPU solve, one request at a time, on the first rate's stream.
+    reqs = stream(rates[0], args.requests, int(rates[0]))
+    for q in reqs:
+        q["mixed"], q["graphs"] = False, False
+    res, wall = cmg.serve(reqs, hbm_budget=120e9, max_inflight=1, open_loop=True)
+    base = stats(list(zip(res, [q["arrival"] for q in reqs])), wall)
+    top = per_rate[str(int(rates[-1]))]
+    line = {
+        "metric": METRIC, "value": top["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": 1,
+        "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "open-loop Poisson arrivals, 1-3 level hierarchies, base 32^3-256^3 log-uniform "
+                               "(x16), Poisson or VC Helmholtz, tolerance 1e-8 or 1e-10, 120 GB budget",
+                   "requests_per_rate": args.requests, "workers": args.inflight,
+                   "latency": "arrival to phi on the host, including grid generation and set-up"},
+        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "per_rate": per_rate,
+        "plain_fp64_one_at_a_time": base,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS) + ["config3", "config4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
+    ap.add_argument("--batch", type=int, default=512, help="config3: number of hierarchies")
+    ap.add_argument("--wave", type=int, default=128, help="config3: hierarchies resident at once")
+    ap.add_argument("--inflight", type=int, default=16, help="config3/4: concurrent solves")
+    ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="config4: arrival rates (req/s)")
+    ap.add_argument("--requests", type=int, default=48, help="config4: requests per rate")
     args = ap.parse_args()
+    if args.impl != "reference" and args.workload in ("config3", "config4"):
+        return run_batch(args) if args.workload == "config3" else run_serving(args)
     wl = WORKLOADS[args.workload]
     meta = golden_meta(wl["golden"])
     if args.impl == "reference":

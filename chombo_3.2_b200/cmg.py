@@ -36,6 +36,44 @@ def solve_params(pre=4, post=4, bottom=4, num_mg=1, iter_max=100, imin=5, eps=1e
     return SolveParams(pre, post, bottom, num_mg, iter_max, imin, eps, hang, norm_thresh)
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("arrival", ctypes.c_double), ("n0", ctypes.c_int), ("levels", ctypes.c_int),
+                ("max_box", ctypes.c_int), ("block_factor", ctypes.c_int), ("fill_ratio", ctypes.c_double),
+                ("thresh", ctypes.c_double), ("seed", ctypes.c_uint64), ("op", ctypes.c_int),
+                ("alpha", ctypes.c_double), ("beta", ctypes.c_double), ("params", SolveParams),
+                ("mixed", ctypes.c_int), ("graphs", ctypes.c_int)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("exit_status", ctypes.c_int), ("iterations", ctypes.c_int), ("error", ctypes.c_int),
+                ("admitted", ctypes.c_double), ("started", ctypes.c_double), ("solved", ctypes.c_double),
+                ("finished", ctypes.c_double), ("setup_seconds", ctypes.c_double),
+                ("solve_seconds", ctypes.c_double), ("r0", ctypes.c_double), ("rfinal", ctypes.c_double),
+                ("cells", ctypes.c_int64), ("device_bytes", ctypes.c_uint64), ("phi_hash", ctypes.c_uint64)]
+
+
+def serve(requests, hbm_budget=120e9, max_inflight=16, open_loop=True):
+    """Runs cmg_serve over a list of dicts with Request fields; returns (results, wall seconds)."""
+    n = len(requests)
+    arr = (Request * max(n, 1))()
+    for i, r in enumerate(requests):
+        q = arr[i]
+        q.arrival = r.get("arrival", 0.0)
+        q.n0, q.levels = r["n0"], r.get("levels", 1)
+        q.max_box, q.block_factor = r.get("max_box", 32), r.get("block_factor", 8)
+        q.fill_ratio, q.thresh = r.get("fill_ratio", 0.75), r.get("thresh", 0.1)
+        q.seed, q.op = r.get("seed", 20261203), r.get("op", 0)
+        q.alpha, q.beta = r.get("alpha", 0.0), r.get("beta", 1.0)
+        q.params = r.get("params") or solve_params(eps=r.get("eps", 1e-10))
+        q.mixed, q.graphs = int(r.get("mixed", True)), int(r.get("graphs", True))
+    out = (RequestResult * max(n, 1))()
+    wall = ctypes.c_double()
+    _check(lib().cmg_serve(arr, n, ctypes.c_double(hbm_budget), int(max_inflight), int(open_loop), out,
+                           ctypes.byref(wall)))
+    keys = [f[0] for f in RequestResult._fields_]
+    return [{k: getattr(out[i], k) for k in keys} for i in range(n)], wall.value
+
+
 _lib = None
 
 

@@ -13,8 +13,9 @@
 #include "../../include/cmg.h"
 #include "meshrefine.H"
 #include "noalloc.H"
+#include "serve.H"
 #include "solver.H"
-#include "synthetic.H"
+#include "synthfill.H"
 
 struct cmg_hierarchy {
   cudaStream_t stream = nullptr;
@@ -330,57 +331,72 @@ int cmg_synthetic_hierarchy(int n0, int nlevels, int max_box, int block_factor, 
   });
 }
 
+int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_inflight, int open_loop,
+              cmg_request_result* out, double* wall_seconds) {
+  return guard([&]() {
+    if ((!reqs && n > 0) || (!out && n > 0) || n < 0 || max_inflight < 1 || !(hbm_budget > 0))
+      throw std::invalid_argument("cmg: invalid serve arguments");
+    std::vector<cmg::Request> rq(n);
+    for (int i = 0; i < n; ++i) {
+      const cmg_request& a = reqs[i];
+      cmg::Request& r = rq[i];
+      if (a.n0 < 8 || a.levels < 1 || (a.op != 0 && a.op != 1) || a.block_factor < 1 || a.max_box < 0)
+        throw std::invalid_argument("cmg: invalid request");
+      r.arrival = a.arrival;
+      r.n0 = a.n0;
+      r.levels = a.levels;
+      r.maxBox = a.max_box;
+      r.blockFactor = a.block_factor;
+      r.fillRatio = a.fill_ratio;
+      r.thresh = a.thresh;
+      r.seed = a.seed;
+      r.op = a.op;
+      r.alpha = a.alpha;
+      r.beta = a.beta;
+      r.params.pre = a.params.pre;
+      r.params.post = a.params.post;
+      r.params.bottom = a.params.bottom;
+      r.params.numMG = a.params.num_mg;
+      r.params.iterMax = a.params.iter_max;
+      r.params.imin = a.params.imin;
+      r.params.eps = a.params.eps;
+      r.params.hang = a.params.hang;
+      r.params.normThresh = a.params.norm_thresh;
+      r.mixed = a.mixed != 0;
+      r.graphs = a.graphs != 0;
+    }
+    cmg::ServeOptions opt;
+    opt.hbmBudget = hbm_budget;
+    opt.maxInflight = max_inflight;
+    opt.openLoop = open_loop != 0;
+    std::vector<cmg::RequestResult> res;
+    double wall = cmg::serve(rq, opt, res);
+    if (wall_seconds) *wall_seconds = wall;
+    for (int i = 0; i < n; ++i) {
+      const cmg::RequestResult& a = res[i];
+      cmg_request_result& o = out[i];
+      o.exit_status = a.exitStatus;
+      o.iterations = a.iterations;
+      o.error = a.error;
+      o.admitted = a.admitted;
+      o.started = a.started;
+      o.solved = a.solved;
+      o.finished = a.finished;
+      o.setup_seconds = a.setupSeconds;
+      o.solve_seconds = a.solveSeconds;
+      o.r0 = a.r0;
+      o.rfinal = a.rfinal;
+      o.cells = a.cells;
+      o.device_bytes = a.deviceBytes;
+      o.phi_hash = a.phiHash;
+    }
+  });
+}
+
 int cmg_fill_synthetic(cmg_hierarchy* h, uint64_t seed) {
   return guard([&]() {
     needLevel(h, 0);
-    cmg_synth::Problem prob(seed);
-    cmg::Solver& S = *h->solver;
-    for (int l = 0; l < S.numLevels(); ++l) {
-      const cmg::LevelPlan& L = S.level(l);
-      const double dx = L.dx;
-      std::vector<int64_t> off(L.grids.size() + 1, 0);
-      for (size_t b = 0; b < L.grids.size(); ++b) off[b + 1] = off[b] + L.grids[b].numPts();
-      std::vector<double> rhs(off.back()), a;
-      if (h->desc.vc) a.resize(off.back());
-      parallelBoxes(L.grids.size(), [&](size_t b) {
-        const cmg::Box& B = L.grids[b];
-        int64_t q = off[b];
-        for (int k = B.lo[2]; k <= B.hi[2]; ++k)
-          for (int j = B.lo[1]; j <= B.hi[1]; ++j)
-            for (int i = B.lo[0]; i <= B.hi[0]; ++i, ++q) {
-              double x = (i + 0.5) * dx, y = (j + 0.5) * dx, z = (k + 0.5) * dx;
-              rhs[q] = prob.bumps.eval(x, y, z);
-              if (!a.empty()) a[q] = prob.acoef.eval(x, y, z);
-            }
-      });
-      S.setRHS(l, rhs.data(), false);
-      if (!h->desc.vc) continue;
-      S.setACoef(l, a.data(), false);
-      for (int d = 0; d < 3; ++d) {
-        std::vector<int64_t> fo(L.grids.size() + 1, 0);
-        for (size_t b = 0; b < L.grids.size(); ++b) {
-          cmg::Box fb = L.grids[b];
-          fb.hi[d] += 1;
-          fo[b + 1] = fo[b] + fb.numPts();
-        }
-        std::vector<double> bc(fo.back());
-        parallelBoxes(L.grids.size(), [&](size_t b) {
-          cmg::Box fb = L.grids[b];
-          fb.hi[d] += 1;
-          int64_t q = fo[b];
-          for (int k = fb.lo[2]; k <= fb.hi[2]; ++k)
-            for (int j = fb.lo[1]; j <= fb.hi[1]; ++j)
-              for (int i = fb.lo[0]; i <= fb.hi[0]; ++i, ++q) {
-                int iv[3] = {i, j, k};
-                double x[3];
-                for (int e = 0; e < 3; ++e) x[e] = (e == d) ? iv[e] * dx : (iv[e] + 0.5) * dx;
-                bc[q] = prob.bcoef.eval(x[0], x[1], x[2]);
-              }
-        });
-        S.setBCoef(l, d, bc.data(), false);
-      }
-    }
-    if (h->desc.vc) S.finalizeCoefficients();
+    cmg::fillSynthetic(*h->solver, h->desc.vc != 0, seed);
   });
 }
 

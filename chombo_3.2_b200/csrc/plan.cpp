@@ -531,38 +531,44 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
   C.rfCoarse.clear();
   C.rfFine.clear();
   Layout cfine = F.grids.coarsen(2);
-  OwnerIndex fineOwner(F);
-  (void)fineOwner;
-  auto covered = [&](const IV& c) {
-    for (const Box& b : cfine.boxes)
-      if (b.contains(c)) return true;
-    return false;
-  };
+  CellSet covered(C.domain, false);
+  for (const Box& b : cfine.boxes) covered.set(b, true);
   for (size_t cb = 0; cb < C.grids.size(); ++cb) {
     const Box& cbox = C.grids[cb];
-    // Per coarse cell of this box: its coarse terms and fine groups.
-    std::map<std::vector<int>, std::pair<std::vector<RefluxCoarseTerm>, std::vector<RefluxFineGroup>>> acc;
-    std::vector<std::vector<int>> order;
-    auto slot = [&](const IV& c) -> std::pair<std::vector<RefluxCoarseTerm>, std::vector<RefluxFineGroup>>& {
-      std::vector<int> key{c[0], c[1], c[2]};
-      auto it = acc.find(key);
-      if (it == acc.end()) {
-        order.push_back(key);
-        return acc[key];
+    // coarsened fine boxes next to this coarse box, in fine box order
+    std::vector<size_t> near;
+    const Box grown = cbox.grow(1);
+    for (size_t f = 0; f < cfine.size(); ++f)
+      if (cfine[f].intersects(grown)) near.push_back(f);
+    if (near.empty()) continue;
+    // Per coarse cell of this box (first-touch order): its coarse terms and
+    // fine groups.
+    std::vector<int> slotOf((size_t)cbox.numPts(), -1);
+    std::vector<IV> order;
+    std::vector<std::vector<RefluxCoarseTerm>> terms;
+    std::vector<std::vector<RefluxFineGroup>> groups;
+    auto slot = [&](const IV& c) -> int {
+      size_t q = (size_t)(c[0] - cbox.lo[0]) +
+                 (size_t)cbox.size(0) * ((size_t)(c[1] - cbox.lo[1]) + (size_t)cbox.size(1) * (c[2] - cbox.lo[2]));
+      if (slotOf[q] < 0) {
+        slotOf[q] = (int)order.size();
+        order.push_back(c);
+        terms.emplace_back();
+        groups.emplace_back();
       }
-      return it->second;
+      return slotOf[q];
     };
     // Coarse terms, in incrementCoarse order: direction, then low/high side.
     for (int d = 0; d < 3; ++d)
       for (int side = -1; side <= 1; side += 2)
-        for (size_t f = 0; f < cfine.size(); ++f) {
+        for (size_t f : near) {
           Box loc = cfine[f].adjCell(d, side, 1) & cbox;
           if (loc.empty()) continue;
           for (int k = loc.lo[2]; k <= loc.hi[2]; ++k)
             for (int j = loc.lo[1]; j <= loc.hi[1]; ++j)
               for (int i = loc.lo[0]; i <= loc.hi[0]; ++i) {
                 IV c(i, j, k);
-                if (covered(c)) continue;
+                if (covered.contains(c)) continue;
                 RefluxCoarseTerm t;
                 IV e = IV::basis(d);
                 IV hi = (side < 0) ? c + e : c;
@@ -572,11 +578,11 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
                 t.bface = vc ? t.hi : -1;
                 t.dir = d;
                 t.sgn = (side < 0) ? 1.0 : -1.0;
-                slot(c).first.push_back(t);
+                terms[slot(c)].push_back(t);
               }
         }
     // Fine groups, in copyTo order: fine box index.
-    for (size_t f = 0; f < cfine.size(); ++f) {
+    for (size_t f : near) {
       const Box& fbox = F.grids[f];
       for (int d = 0; d < 3; ++d)
         for (int side = -1; side <= 1; side += 2) {
@@ -586,13 +592,12 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
             for (int j = loc.lo[1]; j <= loc.hi[1]; ++j)
               for (int i = loc.lo[0]; i <= loc.hi[0]; ++i) {
                 IV c(i, j, k);
-                if (covered(c)) continue;
+                if (covered.contains(c)) continue;
                 RefluxFineGroup g;
                 g.dir = d;
                 g.scale = ((side < 0) ? -1.0 : 1.0) * 1.0 / 4.0;
                 Box ghosts = Box(c, c).refine(2) & fbox.adjCell(d, side, 1);
                 int n = 0;
-                IV e = IV::basis(d);
                 for (int z = ghosts.lo[2]; z <= ghosts.hi[2]; ++z)
                   for (int y = ghosts.lo[1]; y <= ghosts.hi[1]; ++y)
                     for (int x = ghosts.lo[0]; x <= ghosts.hi[0]; ++x) {
@@ -600,27 +605,25 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
                       IV v = gcell - IV::basis(d, side);
                       IV hi = (side < 0) ? v : gcell;
                       IV lo = (side < 0) ? gcell : v;
-                      (void)e;
                       g.hi[n] = cellOf(F, (int)f, hi);
                       g.lo[n] = cellOf(F, (int)f, lo);
                       g.bface[n] = vc ? g.hi[n] : -1;
                       ++n;
                     }
                 if (n != 4) throw std::runtime_error("cmg: fine face group is not 2x2");
-                slot(c).second.push_back(g);
+                groups[slot(c)].push_back(g);
               }
         }
     }
-    for (const auto& key : order) {
-      auto& pr = acc[key];
+    for (size_t q = 0; q < order.size(); ++q) {
       RefluxCell rc;
-      rc.c = cellOf(C, (int)cb, IV(key[0], key[1], key[2]));
-      rc.nco = (int)pr.first.size();
-      rc.nfi = (int)pr.second.size();
+      rc.c = cellOf(C, (int)cb, order[q]);
+      rc.nco = (int)terms[q].size();
+      rc.nfi = (int)groups[q].size();
       rc.start = (int)C.rfCoarse.size();
       rc.fstart = (int)C.rfFine.size();
-      for (auto& t : pr.first) C.rfCoarse.push_back(t);
-      for (auto& g : pr.second) C.rfFine.push_back(g);
+      for (auto& t : terms[q]) C.rfCoarse.push_back(t);
+      for (auto& g : groups[q]) C.rfFine.push_back(g);
       C.rfCells.push_back(rc);
     }
   }

@@ -1,0 +1,59 @@
+// Request loop for many independent solves on one GPU (batching and
+// serving; no counterpart in the reference, which solves one hierarchy per
+// call).  Each request describes a seeded synthetic problem: the example
+// hierarchy (grid generation of meshrefine.H), Poisson/Helmholtz or the
+// variable-coefficient operator, a tolerance and the precision.  Workers
+// admit requests in arrival order as long as the device memory held by the
+// admitted hierarchies stays within a budget, build each hierarchy (plans,
+// device state, inputs) on its own CUDA stream, solve it (CUDA-graph replay
+// of each iteration), read phi back and release the memory, so that the
+// solves of all in-flight requests overlap on the device.  Requests never
+// share device data, so each result is the same alone and in the mix.
+#ifndef CMG_SERVE_H
+#define CMG_SERVE_H
+
+#include <cstdint>
+#include <vector>
+
+#include "solver.H"
+
+namespace cmg {
+
+struct Request {
+  double arrival = 0;  // seconds after the start of the run (open loop)
+  int n0 = 32, levels = 1, maxBox = 32, blockFactor = 8;
+  double fillRatio = 0.75, thresh = 0.1;
+  uint64_t seed = 20261203;
+  int op = 0;  // 0: AMRPoissonOp, 1: VCAMRPoissonOp2
+  double alpha = 0.0, beta = 1.0;
+  SolveParams params;
+  bool mixed = true, graphs = true;
+};
+
+struct RequestResult {
+  int exitStatus = -1, iterations = 0;
+  double admitted = 0, started = 0, solved = 0, finished = 0;  // seconds after the start
+  double setupSeconds = 0, solveSeconds = 0;
+  double r0 = 0, rfinal = 0;
+  int64_t cells = 0;
+  size_t deviceBytes = 0;
+  uint64_t phiHash = 0;  // FNV-1a of the bits of phi on every level (valid cells)
+  int error = 0;
+};
+
+struct ServeOptions {
+  double hbmBudget = 120e9;  // bytes of device memory the admitted hierarchies may hold
+  int maxInflight = 16;      // worker threads, each owning one hierarchy at a time
+  bool openLoop = true;      // release requests at their arrival times
+};
+
+// Runs every request; returns the wall time of the run in seconds.
+double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vector<RequestResult>& out);
+
+// Device bytes a request's hierarchy will hold, from its box lists (the
+// admission estimate; the real figure is recorded after creation).
+size_t estimateDeviceBytes(const std::vector<std::vector<Box>>& boxes, bool vc, bool mixed);
+
+}  // namespace cmg
+
+#endif

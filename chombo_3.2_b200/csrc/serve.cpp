@@ -1,0 +1,157 @@
+// Request loop (see serve.H).
+#include "serve.H"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <thread>
+
+#include "meshrefine.H"
+#include "synthfill.H"
+
+namespace cmg {
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+uint64_t fnv1a(const double* v, size_t n, uint64_t h) {
+  const unsigned char* p = reinterpret_cast<const unsigned char*>(v);
+  for (size_t i = 0; i < n * sizeof(double); ++i) {
+    h ^= p[i];
+    h *= 1099511628211ULL;
+  }
+  return h;
+}
+
+int64_t fabElements(const Box& b) {
+  const int64_t px = (b.size(0) + 3) & ~1;
+  return px * (b.size(1) + 2) * (b.size(2) + 2);
+}
+
+}  // namespace
+
+size_t estimateDeviceBytes(const std::vector<std::vector<Box>>& boxes, bool vc, bool mixed) {
+  // Per AMR level: 6 FP64 fields (+5 coefficient arrays), FP32 copies of 4
+  // fields (+5) for mixed precision; multigrid depths below level 0 add at
+  // most 1/7 of level 0; plans and ghost lists about 30% more.
+  const double f64 = 6 + (vc ? 5 : 0), f32 = mixed ? 4 + (vc ? 5 : 0) : 0;
+  double bytes = 0;
+  for (size_t l = 0; l < boxes.size(); ++l) {
+    int64_t n = 0;
+    for (const Box& b : boxes[l]) n += fabElements(b);
+    double lev = n * (8.0 * f64 + 4.0 * f32);
+    bytes += l == 0 ? lev * (1.0 + 1.0 / 7.0) : lev;
+  }
+  return (size_t)(bytes * 1.3) + (64u << 20);
+}
+
+double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vector<RequestResult>& out) {
+  const size_t n = reqs.size();
+  out.assign(n, RequestResult());
+  std::vector<size_t> order(n);
+  for (size_t i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return reqs[a].arrival < reqs[b].arrival; });
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cmg: no CUDA device");
+
+  std::mutex m;
+  std::condition_variable cv;
+  size_t next = 0;
+  double used = 0;
+  const Clock::time_point t0 = Clock::now();
+  auto since = [&](Clock::time_point t) { return std::chrono::duration<double>(t - t0).count(); };
+
+  auto work = [&]() {
+    cudaSetDevice(dev);
+    for (;;) {
+      size_t idx;
+      {
+        std::lock_guard<std::mutex> lk(m);
+        if (next >= n) return;
+        idx = order[next++];
+      }
+      const Request& q = reqs[idx];
+      RequestResult& r = out[idx];
+      if (opt.openLoop) std::this_thread::sleep_until(t0 + std::chrono::duration_cast<Clock::duration>(
+                                                                 std::chrono::duration<double>(q.arrival)));
+      double est = 0;
+      bool reserved = false;
+      cudaStream_t s = nullptr;
+      try {
+        const Clock::time_point ts = Clock::now();
+        std::vector<std::vector<Box>> boxes =
+            syntheticHierarchy(q.n0, q.levels, q.maxBox, q.blockFactor, q.fillRatio, q.seed, q.thresh);
+        est = (double)estimateDeviceBytes(boxes, q.op == 1, q.mixed);
+        {
+          std::unique_lock<std::mutex> lk(m);
+          cv.wait(lk, [&]() { return used + est <= opt.hbmBudget || used == 0; });
+          used += est;
+          reserved = true;
+        }
+        r.admitted = since(Clock::now());
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+          throw std::runtime_error("cmg: stream");
+        HierarchyDesc d;
+        d.domain = Box(IV(0, 0, 0), IV(q.n0 - 1, q.n0 - 1, q.n0 - 1));
+        d.dx0 = 1.0 / q.n0;
+        d.boxes = boxes;
+        d.vc = q.op;
+        d.alpha = q.alpha;
+        d.beta = q.beta;
+        {
+          std::unique_ptr<Solver> S(new Solver(d, s));
+          fillSynthetic(*S, q.op == 1, q.seed);
+          S->setUseGraphs(q.graphs);
+          const Clock::time_point tsolve = Clock::now();
+          r.setupSeconds = std::chrono::duration<double>(tsolve - ts).count();
+          r.started = since(tsolve);
+          SolveResult res = q.mixed ? S->solveMixed(q.params) : S->solve(q.params);
+          const Clock::time_point tsolved = Clock::now();
+          r.solveSeconds = std::chrono::duration<double>(tsolved - tsolve).count();
+          r.solved = since(tsolved);
+          r.exitStatus = res.exitStatus;
+          r.iterations = res.iterations;
+          r.r0 = res.history.front();
+          r.rfinal = res.history.back();
+          uint64_t h = 1469598103934665603ULL;
+          std::vector<double> phi;
+          for (int l = 0; l < S->numLevels(); ++l) {
+            phi.resize(S->numValidCells(l));
+            S->getPhi(l, phi.data(), false);
+            h = fnv1a(phi.data(), phi.size(), h);
+            r.cells += S->numValidCells(l);
+          }
+          r.phiHash = h;
+          r.deviceBytes = S->deviceBytes();
+        }
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        s = nullptr;
+      } catch (...) {
+        r.error = 1;
+        if (s) {
+          cudaStreamSynchronize(s);
+          cudaStreamDestroy(s);
+        }
+      }
+      r.finished = since(Clock::now());
+      if (reserved) {
+        std::lock_guard<std::mutex> lk(m);
+        used -= est;
+      }
+      cv.notify_all();
+    }
+  };
+  const int nw = std::max(1, std::min<int>(opt.maxInflight, (int)std::max<size_t>(n, 1)));
+  std::vector<std::thread> th;
+  for (int w = 0; w < nw; ++w) th.emplace_back(work);
+  for (auto& t : th) t.join();
+  return since(Clock::now());
+}
+
+}  // namespace cmg

@@ -34,12 +34,16 @@ struct SolveResult {
   std::vector<double> history;  // composite max-norm residual, start of each iteration, then final
 };
 
-// Device allocation owned by the solver.
+// Device allocation owned by the solver, stream-ordered (cudaMallocAsync /
+// cudaFreeAsync on the solver's stream), so that hierarchies created and
+// destroyed while others solve on their own streams never synchronise the
+// device.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  cudaStream_t s = nullptr;
   DevBuf() {}
-  explicit DevBuf(size_t n);
+  DevBuf(size_t n, cudaStream_t stream);
   ~DevBuf();
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
@@ -72,6 +76,8 @@ class Solver {
   // nothing on success.
   double residualNormStatic(double* scratch);
   cudaStream_t stream() const { return s_; }
+  // Device bytes held by this hierarchy.
+  size_t deviceBytes() const;
   // Bytes moved per V-cycle by the algorithmic count (each array read once,
   // each output written once per pass), for the roofline.
   double vcycleBytes(const SolveParams& p) const;
@@ -142,7 +148,7 @@ class Solver {
   };
   std::map<GraphKey, cudaGraphExec_t> graphs_;
   bool useGraphs_ = false;
-  double hostMetric_ = 0;
+  double* hostScalars_ = nullptr;  // pinned: [0] norm read back, [1] bottom metric
   template <class T> void amrVCycle(int ilev, int lmax);
   template <class T> void mgCycle(int depth, T* corr, T* res);
   template <class T> void bottom(int depth, T* corr, T* res);

@@ -5,6 +5,9 @@
 // method it performs.
 #include "solver.H"
 
+#include <cstdint>
+#include <mutex>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -51,13 +54,39 @@ __global__ void k_scatter(const BoxDesc* boxes, const RegionCopy* rc, double* de
 
 }  // namespace
 
-DevBuf::DevBuf(size_t n) : bytes(n) { ck(cudaMalloc(&p, n ? n : 1), "cudaMalloc"); }
+namespace {
+// Keep freed blocks in the stream-ordered pool of each device for reuse by
+// the next hierarchy instead of returning them to the driver.
+void keepPoolMemory() {
+  static std::once_flag once[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::call_once(once[dev], [dev]() {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  });
+}
+}  // namespace
+
+DevBuf::DevBuf(size_t n, cudaStream_t stream) : bytes(n), s(stream) {
+  keepPoolMemory();
+  ck(cudaMallocAsync(&p, n ? n : 1, s), "cudaMalloc");
+}
 DevBuf::~DevBuf() {
-  if (p) cudaFree(p);
+  if (p) cudaFreeAsync(p, s);
+}
+
+size_t Solver::deviceBytes() const {
+  size_t n = stage_ ? stage_->bytes : 0;
+  for (const auto& b : bufs_) n += b->bytes;
+  return n;
 }
 
 double* Solver::alloc(size_t n) {
-  bufs_.emplace_back(new DevBuf(n * sizeof(double)));
+  bufs_.emplace_back(new DevBuf(n * sizeof(double), s_));
   double* p = (double*)bufs_.back()->p;
   ck(cudaMemsetAsync(p, 0, n * sizeof(double), s_), "memset");
   return p;
@@ -67,7 +96,7 @@ template <class V>
 static const typename V::value_type* upload(std::vector<std::unique_ptr<DevBuf>>& bufs, const V& v, cudaStream_t s) {
   if (v.empty()) return nullptr;
   size_t n = v.size() * sizeof(typename V::value_type);
-  bufs.emplace_back(new DevBuf(n));
+  bufs.emplace_back(new DevBuf(n, s));
   ck(cudaMemcpyAsync(bufs.back()->p, v.data(), n, cudaMemcpyHostToDevice, s), "upload");
   return (const typename V::value_type*)bufs.back()->p;
 }
@@ -225,10 +254,11 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), des
     for (int d = 0; d < 3; ++d) bottom_.b[d] = alloc(nc);
     bottom_.lam = alloc(nc);
   }
-  bufs_.emplace_back(new DevBuf(4 * sizeof(int)));
+  bufs_.emplace_back(new DevBuf(4 * sizeof(int), s_));
   bottom_.status = (int*)bufs_.back()->p;
   dNorm_ = alloc(1);
   dMetric_ = alloc(1);
+  ck(cudaMallocHost((void**)&hostScalars_, 2 * sizeof(double)), "pinned scalars");
   if (desc.vc) {
     hostA_.resize(nlev);
     for (int d = 0; d < 3; ++d) hostB_[d].resize(nlev);
@@ -239,6 +269,7 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), des
 Solver::~Solver() {
   cudaStreamSynchronize(s_);
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  if (hostScalars_) cudaFreeHost(hostScalars_);
 }
 
 int64_t Solver::numFaces(int l, int dir) const {
@@ -277,7 +308,7 @@ const void* Solver::regionPlan(const LevelPlan& p, int faceDir, int* nreg, int64
 }
 
 double* Solver::staging(int64_t n) {
-  if (!stage_ || stage_->bytes < (size_t)n * sizeof(double)) stage_.reset(new DevBuf(n * sizeof(double)));
+  if (!stage_ || stage_->bytes < (size_t)n * sizeof(double)) stage_.reset(new DevBuf(n * sizeof(double), s_));
   return (double*)stage_->p;
 }
 
@@ -625,11 +656,12 @@ void Solver::launchAMRResidual(std::vector<double*>& res, std::vector<double*>& 
   }
 }
 
+// Through pinned host memory, so that the copy is a plain stream operation
+// and concurrent solves on other streams are not serialised behind it.
 double Solver::readNorm() {
-  double h = 0;
-  ck(cudaMemcpyAsync(&h, dNorm_, sizeof(double), cudaMemcpyDeviceToHost, s_), "norm d2h");
+  ck(cudaMemcpyAsync(&hostScalars_[0], dNorm_, sizeof(double), cudaMemcpyDeviceToHost, s_), "norm d2h");
   ck(cudaStreamSynchronize(s_), "norm sync");
-  return h;
+  return hostScalars_[0];
 }
 
 // BiCGStab bottom solve in FP64 whatever the V-cycle's precision: an FP32
@@ -791,8 +823,8 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
   const double r0 = computeAMRResidual(ures, phi, rhs, lmax);
   double rnorm = r0, normLast = 2 * r0;
   // setConvergenceMetrics(m_initial_rnorm, cushion * m_eps) of the bottom solver
-  hostMetric_ = r0;
-  ck(cudaMemcpyAsync(dMetric_, &hostMetric_, sizeof(double), cudaMemcpyHostToDevice, s_), "metric");
+  hostScalars_[1] = r0;
+  ck(cudaMemcpyAsync(dMetric_, &hostScalars_[1], sizeof(double), cudaMemcpyHostToDevice, s_), "metric");
   out.history.push_back(rnorm);
   int iter = 0;
   bool goNorm = rnorm > p.normThresh;
@@ -851,7 +883,7 @@ cudaGraphExec_t Solver::iterationGraph(bool mixed, std::vector<double*>& ures, s
 void Solver::setUseGraphs(bool on) { useGraphs_ = on; }
 
 float* Solver::allocF(size_t n) {
-  bufs_.emplace_back(new DevBuf(n * sizeof(float)));
+  bufs_.emplace_back(new DevBuf(n * sizeof(float), s_));
   float* p = (float*)bufs_.back()->p;
   ck(cudaMemsetAsync(p, 0, n * sizeof(float), s_), "memset");
   return p;

@@ -164,6 +164,40 @@ int cmg_layout_coarse_fine_plan(const cmg_box* fine, int nfine, const cmg_box* c
 int cmg_synthetic_hierarchy(int n0, int nlevels, int max_box, int block_factor, double fill_ratio, uint64_t seed,
                             double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes, int cap, int* ntotal);
 
+/* Batching and serving (no counterpart in the reference, which solves one
+ * hierarchy per call).  A request is a seeded synthetic problem: the
+ * example hierarchy of cmg_synthetic_hierarchy, operator (op as in
+ * cmg_hierarchy_create), solver parameters, precision (mixed != 0:
+ * cmg_solve_mixed) and CUDA-graph replay.  cmg_serve runs max_inflight
+ * workers; each takes the next request in arrival order (released at its
+ * arrival time when open_loop != 0, all at once otherwise), generates its
+ * grids, waits until the device memory of the admitted hierarchies plus its
+ * own estimate fits in hbm_budget bytes, builds the hierarchy on its own
+ * stream, solves, reads phi back (hashed into phi_hash) and frees it.  The
+ * solves of all admitted requests overlap on the device; requests share no
+ * device data, so every result is the same alone and in the mix.  Times are
+ * seconds after the start of the run. */
+typedef struct cmg_request {
+  double arrival;
+  int n0, levels, max_box, block_factor;
+  double fill_ratio, thresh;
+  uint64_t seed;
+  int op;
+  double alpha, beta;
+  cmg_solve_params params;
+  int mixed, graphs;
+} cmg_request;
+
+typedef struct cmg_request_result {
+  int exit_status, iterations, error;
+  double admitted, started, solved, finished, setup_seconds, solve_seconds, r0, rfinal;
+  int64_t cells;
+  uint64_t device_bytes, phi_hash;
+} cmg_request_result;
+
+int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_inflight, int open_loop,
+              cmg_request_result* out, double* wall_seconds);
+
 /* Algorithmic bytes moved per V-cycle (roofline numerator). */
 int cmg_vcycle_bytes(const cmg_hierarchy* h, const cmg_solve_params* p, double* out);
 

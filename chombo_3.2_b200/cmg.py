@@ -241,6 +241,9 @@ class Hierarchy:
                   _ptr(hist), len(hist), ctypes.byref(hl)))
         return {"exit_status": st.value, "iterations": it.value, "history": hist[:hl.value].copy()}
 
+    def set_relax_mode(self, mode):
+        _check(lib().cmg_set_relax_mode(self.h, int(mode)))
+
     def use_graphs(self, on=True):
         _check(lib().cmg_use_graphs(self.h, int(on)))
 

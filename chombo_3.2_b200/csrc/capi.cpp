@@ -276,6 +276,13 @@ int solveWith(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* ex
 }
 }  // namespace
 
+int cmg_set_relax_mode(cmg_hierarchy* h, int mode) {
+  return guard([&]() {
+    needLevel(h, 0);
+    h->solver->setRelaxMode(mode);
+  });
+}
+
 int cmg_use_graphs(cmg_hierarchy* h, int on) {
   return guard([&]() {
     needLevel(h, 0);

@@ -88,6 +88,23 @@ struct GhostCell {
   int dst, s1, s2;
 };
 
+// How a relaxation pass obtains the value of one face-ghost cell of a box
+// without a ghost fill: the rule the fill before the pass would apply,
+// evaluated at the moment the adjacent valid cell (the only cell whose
+// stencil reads this ghost) is updated.  Every value the rule reads belongs to
+// the other colour or is the updated cell's own old value, so it is the value
+// the fill would have written.
+enum FaceRuleKind {
+  FR_COPY = 0,    // exchange: src = element of the source box's valid cell
+  FR_BC = 1,      // homogeneous Dirichlet: 2*0 - (the adjacent cell)
+  FR_CFQUAD = 2,  // homogeneous quadratic CF: c1*(adjacent) + c2*f[src], src two cells inward
+  FR_CFLIN = 3,   // linear CF of a one-cell-wide box: flin*(adjacent)
+  FR_FAB = 4      // no fill rule: the FAB ghost element src as it is
+};
+struct FaceRule {
+  int src, kind;
+};
+
 // Device form of a ghost task: the task plus copies of its destination and
 // source box descriptors, so that a thread reaches its data after a single
 // table load.

@@ -26,6 +26,8 @@ struct LevelDev {
   int nCellsExchBC = 0, nCellsGhost = 0;
   const GhostCell* gcells = nullptr;     // flat ghost-cell lists (LevelPlan::gcells)
   int gcStart[2] = {0, 0}, gcExch[2] = {0, 0}, gcCF[2] = {0, 0};
+  const FaceRule* faceRules = nullptr;    // LevelPlan::faceRules / faceOff
+  const int* faceOff = nullptr;
   const GhostTaskDev* zero = nullptr;
   int nZero = 0;
   const int* zeroStart = nullptr;
@@ -71,7 +73,13 @@ struct Coef {
 // colour par (the only ones a pass over colour 1 - par reads).
 template <class T> void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par = -1);
 template <class T> void zeroCovered(const LevelDev& L, T* f, cudaStream_t s);
-template <class T> void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s);
+// One colour pass of levelGSRB.  inlineGhosts: the neighbours beyond each
+// box come from the level's face-ghost rules, so no ghost fill is needed
+// before the pass; otherwise they are read from ghost cells filled by
+// ghostFill(withCF) just before.
+template <class T>
+void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s,
+          bool inlineGhosts = false);
 // residualI form: r = rhs - L(phi) in the operator's own expression order.
 template <class T> void residual(const LevelDev& L, T* r, const T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s);
 // applyOpI form: lofphi = L(phi).

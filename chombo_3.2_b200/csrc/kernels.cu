@@ -187,28 +187,71 @@ struct Scal {
   int laplacian;
 };
 
+// Value of the face ghost of box b beyond cell (i,j,k) in direction d on
+// side s, from its fill rule (FaceRule); pc is the cell's current value.
+struct GhostCoef {
+  double c1, c2, flin;
+};
+template <class T>
+__device__ __forceinline__ T ghostValue(const FaceRule* __restrict__ rules, const int* __restrict__ faceOff,
+                                        const BoxDesc& bd, int b, int d, int s, int i, int j, int k, T pc,
+                                        const T* phi, const GhostCoef& gc) {
+  const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+  const int p[3] = {i, j, k};
+  const FaceRule r = rules[faceOff[6 * b + 2 * d + (s > 0)] + (p[t0] - bd.lo[t0]) +
+                           (bd.hi[t0] - bd.lo[t0] + 1) * (p[t1] - bd.lo[t1])];
+  if (r.kind == FR_COPY || r.kind == FR_FAB) return phi[r.src];
+  if (r.kind == FR_BC) {
+    T zero = T(0);
+    return T(2) * zero - pc;
+  }
+  if (r.kind == FR_CFLIN) return T(gc.flin) * pc;
+  return T(gc.c1) * pc + T(gc.c2) * phi[r.src];
+}
+
 // GSRBLAPLACIAN / GSRBHELMHOLTZ (AMRPoissonOpF.ChF:51-198) and
-// GSRBHELMHOLTZVC3D (VCAMRPoissonOpF.ChF:57-125), one colour.
-template <class T, int VC>
+// GSRBHELMHOLTZVC3D (VCAMRPoissonOpF.ChF:57-125), one colour.  With face
+// rules, the neighbours beyond the box are evaluated from the rules instead
+// of read from ghost cells filled before the pass (same values, no fill).
+template <class T, int VC, bool INL>
 __global__ void k_gsrb(const BoxDesc* boxes, const Chunk* chunks, T* phi, const T* rhs, int color, Scal sc,
-                       const T* a, const T* b0, const T* b1, const T* b2, const T* lam) {
+                       const T* a, const T* b0, const T* b1, const T* b2, const T* lam,
+                       const FaceRule* __restrict__ rules, const int* __restrict__ faceOff, GhostCoef gc) {
   Chunk ch = chunks[blockIdx.x];
   const BoxDesc bd = boxes[ch.box];
   int i, j, k;
   if (!colorCell(bd, ch.start + threadIdx.x, color, i, j, k)) return;
   const Stencil st = stencil(bd, i, j, k);
   const int64_t c = st.c;
+  const T pc = phi[c];
+  T v[6];
+  if (INL) {
+    const int b = ch.box;
+    v[0] = i == bd.hi[0] ? ghostValue(rules, faceOff, bd, b, 0, 1, i, j, k, pc, phi, gc) : phi[st.xp];
+    v[1] = i == bd.lo[0] ? ghostValue(rules, faceOff, bd, b, 0, -1, i, j, k, pc, phi, gc) : phi[st.xm];
+    v[2] = j == bd.hi[1] ? ghostValue(rules, faceOff, bd, b, 1, 1, i, j, k, pc, phi, gc) : phi[st.yp];
+    v[3] = j == bd.lo[1] ? ghostValue(rules, faceOff, bd, b, 1, -1, i, j, k, pc, phi, gc) : phi[st.ym];
+    v[4] = k == bd.hi[2] ? ghostValue(rules, faceOff, bd, b, 2, 1, i, j, k, pc, phi, gc) : phi[st.zp];
+    v[5] = k == bd.lo[2] ? ghostValue(rules, faceOff, bd, b, 2, -1, i, j, k, pc, phi, gc) : phi[st.zm];
+  } else {
+    v[0] = phi[st.xp];
+    v[1] = phi[st.xm];
+    v[2] = phi[st.yp];
+    v[3] = phi[st.ym];
+    v[4] = phi[st.zp];
+    v[5] = phi[st.zm];
+  }
   const T dxinv = T(sc.dxinv);
   if (VC) {
-    T pc = phi[c];
-    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, st) * dxinv;
+    T div = b0[st.xp] * (v[0] - pc) - b0[c] * (pc - v[1]) + b1[st.yp] * (v[2] - pc) - b1[c] * (pc - v[3]) +
+            b2[st.zp] * (v[4] - pc) - b2[c] * (pc - v[5]);
+    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * div * dxinv;
     phi[c] = pc - lam[c] * (lofphi - rhs[c]);
   } else if (sc.laplacian) {
-    T lphi = nbrSum(phi, st) * dxinv;
+    T lphi = (v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) * dxinv;
     phi[c] = T(sc.lambda) * (rhs[c] - lphi);
   } else {
-    T pc = phi[c];
-    T lphi = (nbrSum(phi, st) - T(2.0) * T(3) * pc) * dxinv;
+    T lphi = ((v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) - T(2.0) * T(3) * pc) * dxinv;
     T helmop = T(sc.alpha) * pc + T(sc.beta) * lphi;
     phi[c] = pc + T(sc.lambda) * (helmop - rhs[c]);
   }
@@ -809,16 +852,28 @@ void zeroCovered(const LevelDev& L, T* f, cudaStream_t s) {
 }
 
 template <class T>
-void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s) {
+void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s, bool inlineGhosts) {
   int n = L.nColor[color];
   if (n == 0) return;
   Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
-  if (c.vc)
-    k_gsrb<T, 1><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, c.a, c.b[0], c.b[1], c.b[2],
-                                     c.lambda);
-  else
-    k_gsrb<T, 0><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, nullptr, nullptr, nullptr,
-                                     nullptr, nullptr);
+  const double dx = L.dx, dxc = L.dxCrse;
+  GhostCoef gc{2 * (dxc - dx) / (dxc + dx), -(dxc - dx) / (dxc + 3 * dx), 1 - 2 * dx / (dx + dxc)};
+  const FaceRule* rules = L.faceRules;
+  auto launch = [&](auto kern, const T* a, const T* b0, const T* b1, const T* b2, const T* lam) {
+    kern<<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, a, b0, b1, b2, lam, rules, L.faceOff,
+                             gc);
+  };
+  if (c.vc) {
+    if (inlineGhosts)
+      launch(k_gsrb<T, 1, true>, c.a, c.b[0], c.b[1], c.b[2], c.lambda);
+    else
+      launch(k_gsrb<T, 1, false>, c.a, c.b[0], c.b[1], c.b[2], c.lambda);
+  } else {
+    if (inlineGhosts)
+      launch(k_gsrb<T, 0, true>, nullptr, nullptr, nullptr, nullptr, nullptr);
+    else
+      launch(k_gsrb<T, 0, false>, nullptr, nullptr, nullptr, nullptr, nullptr);
+  }
   CMG_LAUNCHED("gsrb");
 }
 
@@ -988,7 +1043,7 @@ template void convert<double, float>(double*, const float*, int64_t, cudaStream_
 #define CMG_INST(T)                                                                                       \
   template void ghostFill<T>(const LevelDev&, T*, bool, cudaStream_t, int);                                \
   template void zeroCovered<T>(const LevelDev&, T*, cudaStream_t);                                         \
-  template void gsrb<T>(const LevelDev&, T*, const T*, const Coef<T>&, int, cudaStream_t);                 \
+  template void gsrb<T>(const LevelDev&, T*, const T*, const Coef<T>&, int, cudaStream_t, bool);           \
   template void residual<T>(const LevelDev&, T*, const T*, const T*, const Coef<T>&, cudaStream_t);        \
   template void applyOp<T>(const LevelDev&, T*, const T*, const Coef<T>&, cudaStream_t);                   \
   template void negAdd<T>(const LevelDev&, T*, const T*, const T*, cudaStream_t);                          \

@@ -33,6 +33,11 @@ struct LevelPlan {
   // colour 1 exchange+BC | colour 1 CF], each group in task order.
   std::vector<GhostCell> gcells;
   int gcStart[2] = {0, 0}, gcExch[2] = {0, 0}, gcCF[2] = {0, 0};
+  // Face-ghost rules for relaxation without ghost fills: per box, six faces
+  // (direction-major, low side first), each over its two tangential
+  // directions in increasing order; faceOff[6*b + 2*d + (side > 0)].
+  std::vector<FaceRule> faceRules;
+  std::vector<int> faceOff;
   std::vector<GhostTask> zeroCovered;  // covered by the next finer level
   std::vector<int> zeroStart;          // cumulative cell counts of zeroCovered
   std::vector<int> zeroBlock;
@@ -65,6 +70,9 @@ struct BottomPlan {
   std::vector<int> gsrc, gkind;  // per ghost slot: source slot, 0 copy / 1 Dirichlet / 2 untouched
 };
 void buildBottom(const LevelPlan& L, BottomPlan& B);
+
+// Face-ghost rules of a level from its ghost tasks (LevelPlan::faceRules).
+void buildFaceRules(LevelPlan& L);
 
 // Layout and ghost/chunk plans of one level (AMR level or multigrid depth).
 // dxCrse > 0 enables homogeneous coarse-fine ghost tasks on CF faces.

@@ -59,6 +59,78 @@ std::vector<Box> coverByBoxes(const CellSet& s) {
 
 }  // namespace
 
+// Index of a face-ghost cell g of box b in its face table, or -1 when g is
+// not a face ghost (inside the box, or outside in more than one direction).
+static int64_t faceSlot(const LevelPlan& L, size_t b, const IV& g, int& dir, int& side) {
+  const Box& bx = L.grids[b];
+  int n = 0;
+  for (int d = 0; d < 3; ++d) {
+    if (g[d] < bx.lo[d]) dir = d, side = -1, ++n;
+    else if (g[d] > bx.hi[d]) dir = d, side = 1, ++n;
+  }
+  if (n != 1 || g[dir] != (side < 0 ? bx.lo[dir] - 1 : bx.hi[dir] + 1)) return -1;
+  const int t0 = dir == 0 ? 1 : 0, t1 = dir == 2 ? 1 : 2;
+  return L.faceOff[6 * b + 2 * dir + (side > 0)] + (g[t0] - bx.lo[t0]) +
+         (int64_t)bx.size(t0) * (g[t1] - bx.lo[t1]);
+}
+
+// Rules of every face-ghost cell from the level's ghost tasks (the fill with
+// coarse-fine values that precedes each relaxation pass).
+void buildFaceRules(LevelPlan& L) {
+  L.faceOff.assign(6 * L.grids.size() + 1, 0);
+  int64_t off = 0;
+  for (size_t b = 0; b < L.grids.size(); ++b) {
+    const Box& bx = L.grids[b];
+    for (int d = 0; d < 3; ++d) {
+      const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+      for (int s = 0; s < 2; ++s) {
+        L.faceOff[6 * b + 2 * d + s] = (int)off;
+        off += (int64_t)bx.size(t0) * bx.size(t1);
+      }
+    }
+  }
+  L.faceOff[6 * L.grids.size()] = (int)off;
+  L.faceRules.assign((size_t)off, FaceRule{0, FR_FAB});
+  for (size_t b = 0; b < L.grids.size(); ++b) {
+    const Box& bx = L.grids[b];
+    for (int d = 0; d < 3; ++d) {
+      const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+      for (int s = 0; s < 2; ++s)
+        for (int v = bx.lo[t1]; v <= bx.hi[t1]; ++v)
+          for (int u = bx.lo[t0]; u <= bx.hi[t0]; ++u) {
+            IV g;
+            g[d] = s ? bx.hi[d] + 1 : bx.lo[d] - 1;
+            g[t0] = u;
+            g[t1] = v;
+            int dd, ss;
+            L.faceRules[faceSlot(L, b, g, dd, ss)].src = (int)cellOf(L, (int)b, g);
+          }
+    }
+  }
+  for (const GhostTask& t : L.ghost) {
+    for (int k = t.lo[2]; k <= t.hi[2]; ++k)
+      for (int j = t.lo[1]; j <= t.hi[1]; ++j)
+        for (int i = t.lo[0]; i <= t.hi[0]; ++i) {
+          IV g(i, j, k);
+          int d = 0, side = 0;
+          int64_t q = faceSlot(L, t.dst, g, d, side);
+          if (q < 0) continue;
+          FaceRule& r = L.faceRules[q];
+          if (t.kind == G_COPY) {
+            r = FaceRule{(int)cellOf(L, t.src, g), FR_COPY};
+          } else if (t.kind == G_BC) {
+            r = FaceRule{0, FR_BC};
+          } else if (t.kind == G_CFLIN) {
+            r = FaceRule{0, FR_CFLIN};
+          } else if (t.kind == G_CFQUAD) {
+            int e[3] = {0, 0, 0};
+            e[t.dir] = -2 * t.side;
+            r = FaceRule{(int)cellOf(L, t.dst, IV(i + e[0], j + e[1], k + e[2])), FR_CFQUAD};
+          }
+        }
+  }
+}
+
 std::vector<int> blockTasks(const std::vector<int>& start) {
   std::vector<int> bt;
   if (start.size() < 2) return bt;
@@ -154,6 +226,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     L.ghostStart.push_back(L.ghostStart.back() + (int)c);
   }
   L.ghostBlock = blockTasks(L.ghostStart);
+  buildFaceRules(L);
   if (L.nelem >= ((int64_t)1 << 31)) throw std::runtime_error("cmg: level too large for 32-bit ghost indices");
   L.gcells.clear();
   auto emit = [&](const GhostTask& t, int par) {

@@ -107,6 +107,10 @@ class Solver {
   // (per precision and smoothing parameters); off by default.  Profiling
   // (profileEnable) runs the uncaptured path.
   void setUseGraphs(bool on);
+  // Relaxation variant: 0 autotuned per level at the first solve (default),
+  // 1 ghost fill before every colour pass, 2 face ghosts evaluated inside the
+  // pass.  All three give identical results.
+  void setRelaxMode(int mode);
 
  private:
   void uploadLevel(const LevelPlan& p, LevelDev& d);
@@ -122,7 +126,7 @@ class Solver {
   template <class T> void relaxAMR(int l, T* phi, const T* rhs, int n);
   template <class T> void relaxMG(int d, T* phi, const T* rhs, int n);
   template <class T>
-  void relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls);
+  void relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls, bool inl);
   template <class T> void fill(const LevelDev& L, T* f, bool withCF, int par = -1);
   template <class T>
   void amrResidualLevel(int ilev, int lmax, std::vector<T*>& res, std::vector<T*>& phi, std::vector<T*>& rhs);
@@ -148,6 +152,12 @@ class Solver {
   };
   std::map<GraphKey, cudaGraphExec_t> graphs_;
   bool useGraphs_ = false;
+  // Relaxation variant per AMR level / MG depth: ghost fill before each
+  // colour pass (0) or face ghosts evaluated inside the pass (1).
+  std::vector<char> inlineA_, inlineM_;
+  bool tuned_ = false;
+  int relaxMode_ = 0;  // 0: autotuned, 1: always fills, 2: always inline
+  void tuneRelaxation();
   double* hostScalars_ = nullptr;  // pinned: [0] norm read back, [1] bottom metric
   template <class T> void amrVCycle(int ilev, int lmax);
   template <class T> void mgCycle(int depth, T* corr, T* res);

@@ -136,6 +136,8 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
   d.nCellsGhost = p.ghostStart.empty() ? 0 : p.ghostStart.back();
   d.zero = upload(bufs_, devTasks(p.zeroCovered), s_);
   d.gcells = upload(bufs_, p.gcells, s_);
+  d.faceRules = upload(bufs_, p.faceRules, s_);
+  d.faceOff = upload(bufs_, p.faceOff, s_);
   for (int c = 0; c < 2; ++c) {
     d.gcStart[c] = p.gcStart[c];
     d.gcExch[c] = p.gcExch[c];
@@ -577,12 +579,13 @@ void Solver::copyField(const LevelDev& L, T* dst, const T* src) {
 // a and lambda and a full word for each of the three face arrays, since
 // every face borders one cell of each colour (6 words).
 template <class T>
-void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls) {
+void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls,
+                        bool inl) {
   const double bytes = cells * sizeof(T) * (c.vc ? 6.0 : 2.0);
   for (int it = 0; it < n; ++it)
     for (int color = 0; color <= 1; ++color) {
-      fill(L, phi, true, 1 - color);
-      timed(cls, bytes, [&]() { gsrb(L, phi, rhs, c, color, s_); });
+      if (!inl) fill(L, phi, true, 1 - color);
+      timed(cls, bytes, [&]() { gsrb(L, phi, rhs, c, color, s_, inl); });
     }
 }
 
@@ -590,13 +593,70 @@ template <class T>
 void Solver::relaxAMR(int l, T* phi, const T* rhs, int n) {
   const int finest = (int)amr_.size() - 1;
   relaxLevel(amrDev_[l], (double)amr_[l].grids.numCells(), coefA<T>(l), phi, rhs, n,
-             l == finest ? P_RELAX_FINE : P_RELAX);
+             l == finest ? P_RELAX_FINE : P_RELAX, inlineA_[l] != 0);
 }
 
 template <class T>
 void Solver::relaxMG(int d, T* phi, const T* rhs, int n) {
   if (d == 0) return relaxAMR(0, phi, rhs, n);
-  relaxLevel(mgDev_[d - 1], (double)mg_[d - 1].grids.numCells(), coefM<T>(d), phi, rhs, n, P_RELAX);
+  relaxLevel(mgDev_[d - 1], (double)mg_[d - 1].grids.numCells(), coefM<T>(d), phi, rhs, n, P_RELAX,
+             inlineM_[d - 1] != 0);
+}
+
+// Relaxation autotuner: per AMR level and multigrid depth, time one red-black
+// sweep with a ghost fill before each colour pass and one with the face
+// ghosts evaluated inside the pass (identical results), on the level's
+// scratch fields, and keep the faster.  Runs once per hierarchy, before its
+// first solve, unless a mode is forced.
+void Solver::tuneRelaxation() {
+  tuned_ = true;
+  inlineA_.assign(amr_.size(), relaxMode_ == 2);
+  inlineM_.assign(mg_.size(), relaxMode_ == 2);
+  if (relaxMode_ != 0) return;
+  cudaEvent_t e[3];
+  for (auto& x : e) ck(cudaEventCreate(&x), "event");
+  const bool prof = profOn_;
+  profOn_ = false;
+  auto timeOne = [&](const LevelDev& L, double cells, const Coef<double>& c, double* phi, const double* rhs,
+                     bool inl) {
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      ck(cudaEventRecord(e[0], s_), "event");
+      relaxLevel(L, cells, c, phi, rhs, 1, P_RELAX, inl);
+      ck(cudaEventRecord(e[1], s_), "event");
+      ck(cudaEventSynchronize(e[1]), "event sync");
+      float ms = 0;
+      ck(cudaEventElapsedTime(&ms, e[0], e[1]), "event time");
+      best = std::min(best, ms);
+    }
+    return best;
+  };
+  for (size_t l = 0; l < amr_.size(); ++l) {
+    const double cells = (double)amr_[l].grids.numCells();
+    Coef<double> c = coefAMR((int)l);
+    float tf = timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, false);
+    float ti = timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, true);
+    inlineA_[l] = ti < tf;
+    zeroField(amrDev_[l], lev_[l].corr);
+  }
+  for (size_t d = 0; d < mg_.size(); ++d) {
+    const double cells = (double)mg_[d].grids.numCells();
+    Coef<double> c = coefMG((int)d + 1);
+    float tf = timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, false);
+    float ti = timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, true);
+    inlineM_[d] = ti < tf;
+    zeroField(mgDev_[d], mgf_[d].corr);
+  }
+  profOn_ = prof;
+  for (auto& x : e) cudaEventDestroy(x);
+}
+
+void Solver::setRelaxMode(int mode) {
+  if (mode < 0 || mode > 2) throw std::invalid_argument("cmg: relaxation mode is 0 (tuned), 1 (fills) or 2 (inline)");
+  relaxMode_ = mode;
+  tuned_ = false;
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  graphs_.clear();
 }
 
 // Ghost fill, timed as its own class: every ghost cell filled written once
@@ -807,6 +867,7 @@ void Solver::iterationBody(bool mixed, std::vector<double*>& ures, std::vector<d
 }
 
 SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
+  if (!tuned_) tuneRelaxation();
   if (mixed) ensure32();
   sp_ = p;
   const int lmax = numLevels() - 1;

@@ -97,6 +97,13 @@ int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* ex
  * Off by default; profiling (cmg_profile_enable) runs uncaptured. */
 int cmg_use_graphs(cmg_hierarchy* h, int on);
 
+/* Relaxation variant (no counterpart in the reference): 0 = chosen per level
+ * by a timing autotuner before the first solve (default); 1 = ghost fill
+ * (exchange, boundary and coarse-fine values) before each colour pass, as the
+ * reference's levelGSRB; 2 = the neighbours beyond each box evaluated inside
+ * the pass from the same fill rules, no fill.  Identical results. */
+int cmg_set_relax_mode(cmg_hierarchy* h, int mode);
+
 /* Mixed precision (no counterpart in the reference, which runs FP64
  * throughout): the loop of AMRMultiGrid::solve with each AMR V-cycle run in
  * FP32 (smoothing, restriction, prolongation, the cycle's own residual

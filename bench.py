@@ -378,6 +378,8 @@ def main():
     ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS) + ["config3", "config4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
+    ap.add_argument("--relax-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="relaxation variant: 0 autotuned per level, 1 ghost fills, 2 in-pass ghosts")
     ap.add_argument("--batch", type=int, default=512, help="config3: number of hierarchies")
     ap.add_argument("--wave", type=int, default=128, help="config3: hierarchies resident at once")
     ap.add_argument("--inflight", type=int, default=16, help="config3/4: concurrent solves")
@@ -410,6 +412,7 @@ def main():
                               eps=meta["eps"], hang=meta["hang"])
     mixed = bool(wl.get("mixed", False))
     h.use_graphs(not args.no_graphs)
+    h.set_relax_mode(args.relax_mode)
     stream = torch.cuda.ExternalStream(h.stream())
     ncells = [h.num_cells(l) for l in range(len(meta["boxes"]))]
 
@@ -553,7 +556,8 @@ def main():
                        "cuda_graphs": not args.no_graphs},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
             "roofline": roofline, "breakdown": breakdown, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": launches,
+            "gpu_launches": launches, "launch_index_at_timed_start": launches0,
+            "relax_variants": h.relax_variants(),
         }
         if accuracy:
             line["accuracy"] = accuracy

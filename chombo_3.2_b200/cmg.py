@@ -244,6 +244,15 @@ class Hierarchy:
     def set_relax_mode(self, mode):
         _check(lib().cmg_set_relax_mode(self.h, int(mode)))
 
+    def relax_variants(self):
+        n = ctypes.c_int()
+        _check(lib().cmg_relax_variants(self.h, None, None, None, 0, ctypes.byref(n)))
+        v = (ctypes.c_int * max(n.value, 1))()
+        a = (ctypes.c_float * max(n.value, 1))()
+        b = (ctypes.c_float * max(n.value, 1))()
+        _check(lib().cmg_relax_variants(self.h, v, a, b, n.value, ctypes.byref(n)))
+        return [{"inline": bool(v[i]), "ms_fill": a[i], "ms_inline": b[i]} for i in range(n.value)]
+
     def use_graphs(self, on=True):
         _check(lib().cmg_use_graphs(self.h, int(on)))
 

@@ -283,6 +283,22 @@ int cmg_set_relax_mode(cmg_hierarchy* h, int mode) {
   });
 }
 
+int cmg_relax_variants(cmg_hierarchy* h, int* inline_out, float* ms_fill, float* ms_inline, int cap, int* n) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (!n) throw std::invalid_argument("cmg: null output pointer");
+    std::vector<int> v;
+    std::vector<float> a, b;
+    h->solver->relaxVariants(v, a, b);
+    *n = (int)v.size();
+    for (int i = 0; i < (int)v.size() && i < cap; ++i) {
+      if (inline_out) inline_out[i] = v[i];
+      if (ms_fill) ms_fill[i] = i < (int)a.size() ? a[i] : -1.0f;
+      if (ms_inline) ms_inline[i] = i < (int)b.size() ? b[i] : -1.0f;
+    }
+  });
+}
+
 int cmg_use_graphs(cmg_hierarchy* h, int on) {
   return guard([&]() {
     needLevel(h, 0);

@@ -134,6 +134,9 @@ void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream
 
 // Number of kernel launches issued by the launchers above since load.
 long long launchCount();
+// Counts n launches that ran without passing through the launchers (the
+// kernel nodes of a replayed CUDA graph).
+void addLaunches(long long n);
 
 }  // namespace cmg
 

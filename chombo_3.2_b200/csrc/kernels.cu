@@ -984,6 +984,7 @@ void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s) {
 
 
 long long launchCount() { return g_launches.load(std::memory_order_relaxed); }
+void addLaunches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
                  double eps, const double* metric, cudaStream_t s) {

@@ -111,6 +111,9 @@ class Solver {
   // 1 ghost fill before every colour pass, 2 face ghosts evaluated inside the
   // pass.  All three give identical results.
   void setRelaxMode(int mode);
+  // The variant of every AMR level then every multigrid depth (1: inline),
+  // and the tuner's sweep times (ms; empty when a mode was forced).
+  void relaxVariants(std::vector<int>& inl, std::vector<float>& msFill, std::vector<float>& msInline);
 
  private:
   void uploadLevel(const LevelPlan& p, LevelDev& d);
@@ -151,12 +154,14 @@ class Solver {
     }
   };
   std::map<GraphKey, cudaGraphExec_t> graphs_;
+  std::map<cudaGraphExec_t, long long> graphLaunches_;  // kernel launches per replay
   bool useGraphs_ = false;
   // Relaxation variant per AMR level / MG depth: ghost fill before each
   // colour pass (0) or face ghosts evaluated inside the pass (1).
   std::vector<char> inlineA_, inlineM_;
   bool tuned_ = false;
   int relaxMode_ = 0;  // 0: autotuned, 1: always fills, 2: always inline
+  std::vector<std::pair<float, float>> tuneMs_;
   void tuneRelaxation();
   double* hostScalars_ = nullptr;  // pinned: [0] norm read back, [1] bottom metric
   template <class T> void amrVCycle(int ilev, int lmax);

@@ -610,6 +610,7 @@ void Solver::relaxMG(int d, T* phi, const T* rhs, int n) {
 // first solve, unless a mode is forced.
 void Solver::tuneRelaxation() {
   tuned_ = true;
+  tuneMs_.clear();
   inlineA_.assign(amr_.size(), relaxMode_ == 2);
   inlineM_.assign(mg_.size(), relaxMode_ == 2);
   if (relaxMode_ != 0) return;
@@ -637,6 +638,7 @@ void Solver::tuneRelaxation() {
     float tf = timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, false);
     float ti = timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, true);
     inlineA_[l] = ti < tf;
+    tuneMs_.push_back({tf, ti});
     zeroField(amrDev_[l], lev_[l].corr);
   }
   for (size_t d = 0; d < mg_.size(); ++d) {
@@ -645,10 +647,24 @@ void Solver::tuneRelaxation() {
     float tf = timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, false);
     float ti = timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, true);
     inlineM_[d] = ti < tf;
+    tuneMs_.push_back({tf, ti});
     zeroField(mgDev_[d], mgf_[d].corr);
   }
   profOn_ = prof;
   for (auto& x : e) cudaEventDestroy(x);
+}
+
+void Solver::relaxVariants(std::vector<int>& inl, std::vector<float>& msFill, std::vector<float>& msInline) {
+  if (!tuned_) tuneRelaxation();
+  inl.clear();
+  msFill.clear();
+  msInline.clear();
+  for (char c : inlineA_) inl.push_back(c);
+  for (char c : inlineM_) inl.push_back(c);
+  for (auto& t : tuneMs_) {
+    msFill.push_back(t.first);
+    msInline.push_back(t.second);
+  }
 }
 
 void Solver::setRelaxMode(int mode) {
@@ -898,6 +914,7 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
     if (graph) {
       cudaGraphExec_t exec = iterationGraph(mixed, ures, phi, rhs);
       ck(cudaGraphLaunch(exec, s_), "graph launch");
+      addLaunches(graphLaunches_[exec]);
     } else {
       iterationBody(mixed, ures, phi, rhs);
     }
@@ -924,6 +941,7 @@ cudaGraphExec_t Solver::iterationGraph(bool mixed, std::vector<double*>& ures, s
   auto it = graphs_.find(key);
   if (it != graphs_.end()) return it->second;
   cudaGraph_t g = nullptr;
+  const long long before = launchCount();
   ck(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal), "begin capture");
   try {
     iterationBody(mixed, ures, phi, rhs);
@@ -938,6 +956,9 @@ cudaGraphExec_t Solver::iterationGraph(bool mixed, std::vector<double*>& ures, s
   cudaGraphDestroy(g);
   ck(e, "graph instantiate");
   graphs_[key] = exec;
+  // the captured launches did not run; each replay adds them
+  graphLaunches_[exec] = launchCount() - before;
+  addLaunches(-(launchCount() - before));
   return exec;
 }
 

@@ -103,6 +103,10 @@ int cmg_use_graphs(cmg_hierarchy* h, int on);
  * reference's levelGSRB; 2 = the neighbours beyond each box evaluated inside
  * the pass from the same fill rules, no fill.  Identical results. */
 int cmg_set_relax_mode(cmg_hierarchy* h, int mode);
+/* The relaxation variant of every AMR level, then every multigrid depth
+ * (1 = in-pass ghosts), with the autotuner's sweep times in ms (-1 when a
+ * mode was forced); runs the tuner if it has not run.  n: entries. */
+int cmg_relax_variants(cmg_hierarchy* h, int* inline_out, float* ms_fill, float* ms_inline, int cap, int* n);
 
 /* Mixed precision (no counterpart in the reference, which runs FP64
  * throughout): the loop of AMRMultiGrid::solve with each AMR V-cycle run in

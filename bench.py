@@ -266,7 +266,7 @@ def run_batch(args):
         boxes = cmg.synthetic_hierarchy(sp["n0"], sp["levels"], sp["max_box"], sp["block_factor"],
                                         sp["fill_ratio"], sp["seed"], sp["thresh"])
         h = cmg.Hierarchy(sp["n0"], boxes, op=sp["op"], alpha=sp["alpha"], beta=sp["beta"])
-        h.fill_synthetic(sp["seed"])
+        h.fill_synthetic(sp["seed"], device=True)
         return h
 
     for w0 in range(0, len(specs), wave):

@@ -49,6 +49,8 @@ class RequestResult(ctypes.Structure):
                 ("admitted", ctypes.c_double), ("started", ctypes.c_double), ("solved", ctypes.c_double),
                 ("finished", ctypes.c_double), ("setup_seconds", ctypes.c_double),
                 ("solve_seconds", ctypes.c_double), ("r0", ctypes.c_double), ("rfinal", ctypes.c_double),
+                ("grid_seconds", ctypes.c_double), ("build_seconds", ctypes.c_double),
+                ("fill_seconds", ctypes.c_double),
                 ("cells", ctypes.c_int64), ("device_bytes", ctypes.c_uint64), ("phi_hash", ctypes.c_uint64)]
 
 
@@ -203,8 +205,9 @@ class Hierarchy:
         _check(lib().cmg_get_boxes(self.h, level, out, n.value))
         return [tuple(b.lo) + tuple(b.hi) for b in out]
 
-    def fill_synthetic(self, seed):
-        _check(lib().cmg_fill_synthetic(self.h, ctypes.c_uint64(seed)))
+    def fill_synthetic(self, seed, device=False):
+        fn = lib().cmg_fill_synthetic_device if device else lib().cmg_fill_synthetic
+        _check(fn(self.h, ctypes.c_uint64(seed)))
 
     def set_rhs(self, level, data):
         a = np.ascontiguousarray(data, dtype=np.float64)
@@ -224,6 +227,11 @@ class Hierarchy:
     def phi(self, level):
         out = np.empty(self.num_cells(level), dtype=np.float64)
         _check(lib().cmg_get_phi(self.h, level, _ptr(out), 0))
+        return out
+
+    def get_rhs(self, level):
+        out = np.empty(self.num_cells(level), dtype=np.float64)
+        _check(lib().cmg_get_rhs(self.h, level, _ptr(out), 0))
         return out
 
     def set_phi(self, level, data):

@@ -409,10 +409,20 @@ int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_infligh
       o.solve_seconds = a.solveSeconds;
       o.r0 = a.r0;
       o.rfinal = a.rfinal;
+      o.grid_seconds = a.gridSeconds;
+      o.build_seconds = a.buildSeconds;
+      o.fill_seconds = a.fillSeconds;
       o.cells = a.cells;
       o.device_bytes = a.deviceBytes;
       o.phi_hash = a.phiHash;
     }
+  });
+}
+
+int cmg_fill_synthetic_device(cmg_hierarchy* h, uint64_t seed) {
+  return guard([&]() {
+    needLevel(h, 0);
+    h->solver->fillSyntheticDevice(seed);
   });
 }
 

@@ -132,6 +132,19 @@ void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<d
 // dst[slot] = fab[w.fab[slot]] for every slot of the bottom level.
 void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream_t s);
 
+// Seeded synthetic inputs of one level on the device (rhs; a and the three
+// face arrays b when not null), the same formulas as synthetic.H.
+void fillSyntheticLevel(const LevelDev& L, uint64_t seed, double* rhs, double* a, double* const b[3],
+                        cudaStream_t s);
+// lambda of the variable-coefficient relaxation on one level
+// (VCAMRPoissonOp2::resetLambda with SUMFACES).
+void lambdaLevel(const LevelDev& L, const double* a, const double* const b[3], double alpha, double beta,
+                 double* lam, cudaStream_t s);
+// a and b of multigrid level C averaged from level F by ratio r, box b <- box b
+// (CoarseAverage / CoarseAverageFace arithmetic).
+void averageCoefficients(const LevelDev& F, const LevelDev& C, int r, const double* fa, const double* const fb[3],
+                         double* ca, double* const cb[3], cudaStream_t s);
+
 // Number of kernel launches issued by the launchers above since load.
 long long launchCount();
 // Counts n launches that ran without passing through the launchers (the

@@ -9,6 +9,7 @@
 
 #include "kernels.H"
 #include "plan.H"
+#include "synthetic.H"
 
 namespace cmg {
 
@@ -317,12 +318,16 @@ __device__ __forceinline__ void atomicMaxPos(double* addr, double v) {
 }
 
 template <class T>
-__global__ void k_maxnorm(const BoxDesc* boxes, const Chunk* chunks, const T* f, double* out) {
-  Chunk ch = chunks[blockIdx.x];
-  const BoxDesc bd = boxes[ch.box];
-  int i, j, k;
+__global__ void k_maxnorm(const BoxDesc* boxes, const Chunk* chunks, int nchunks, const T* f, double* out) {
+  // Grid-stride over the chunks, so that only one atomic per block (not per
+  // chunk) reaches the single output word.
   double v = 0.0;
-  if (allCell(bd, ch.start + threadIdx.x, i, j, k)) v = fabs((double)f[cellIndex(bd, i, j, k)]);
+  for (int cix = blockIdx.x; cix < nchunks; cix += gridDim.x) {
+    Chunk ch = chunks[cix];
+    const BoxDesc bd = boxes[ch.box];
+    int i, j, k;
+    if (allCell(bd, ch.start + threadIdx.x, i, j, k)) v = fmax(v, fabs((double)f[cellIndex(bd, i, j, k)]));
+  }
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   __shared__ double red[CHUNK / 32];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
@@ -978,7 +983,8 @@ void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s) {
 template <class T>
 void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s) {
   if (L.nAll == 0) return;
-  k_maxnorm<T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, f, out);
+  const int blocks = std::min(L.nAll, 148 * 8);
+  k_maxnorm<T><<<blocks, CHUNK, 0, s>>>(L.boxes, L.chAll, L.nAll, f, out);
   CMG_LAUNCHED("maxNorm");
 }
 
@@ -1040,6 +1046,149 @@ void convert(D* dst, const S* src, int64_t n, cudaStream_t s) {
 }
 template void convert<float, double>(float*, const double*, int64_t, cudaStream_t);
 template void convert<double, float>(double*, const float*, int64_t, cudaStream_t);
+
+// ------------------------------------------------ synthetic inputs, device
+// The seeded fields of synthetic.H evaluated on the device (same formulas and
+// operation order; exp and cos of the CUDA math library, so values agree with
+// the host generator to within their last bits), and the coefficient set-up
+// of finalizeCoefficients (resetLambda with SUMFACES, MG coefficient
+// averages) with the host code's operation order.
+namespace {
+
+__device__ double devBumps(const cmg_synth::Bumps& B, double x, double y, double z) {
+  double v = 0.0;
+  for (int i = 0; i < 16; ++i) {
+    double dx = x - B.cx[i], dy = y - B.cy[i], dz = z - B.cz[i];
+    double r2 = dx * dx + dy * dy + dz * dz;
+    v += B.amp[i] * exp(-r2 / B.w2x2[i]);
+  }
+  return v;
+}
+
+__device__ double devModes(const cmg_synth::Modes& M, double x, double y, double z) {
+  double g = 0.0;
+  for (int m = 0; m < 8; ++m)
+    g += M.c[m] * cos(6.283185307179586 * (M.kx[m] * x + M.ky[m] * y + M.kz[m] * z) + M.ph[m]);
+  g = g / M.norm;
+  return exp(2.302585092994046 * g);
+}
+
+__global__ void k_fill_cells(const BoxDesc* boxes, const Chunk* chunks, double dx, cmg_synth::Bumps bumps,
+                             cmg_synth::Modes am, double* rhs, double* a) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  int i, j, k;
+  if (!allCell(bd, ch.start + threadIdx.x, i, j, k)) return;
+  const double x = (i + 0.5) * dx, y = (j + 0.5) * dx, z = (k + 0.5) * dx;
+  const int64_t c = cellIndex(bd, i, j, k);
+  rhs[c] = devBumps(bumps, x, y, z);
+  if (a) a[c] = devModes(am, x, y, z);
+}
+
+// One block per box: faces lo..hi+1 in direction d.
+__global__ void k_fill_faces(const BoxDesc* boxes, double dx, int d, cmg_synth::Modes bm, double* b) {
+  const BoxDesc bd = boxes[blockIdx.x];
+  int n[3];
+  for (int e = 0; e < 3; ++e) n[e] = bd.hi[e] - bd.lo[e] + 1 + (e == d);
+  const int total = n[0] * n[1] * n[2];
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    int iv[3] = {bd.lo[0] + q % n[0], bd.lo[1] + (q / n[0]) % n[1], bd.lo[2] + q / (n[0] * n[1])};
+    double x[3];
+    for (int e = 0; e < 3; ++e) x[e] = (e == d) ? iv[e] * dx : (iv[e] + 0.5) * dx;
+    b[cellIndex(bd, iv[0], iv[1], iv[2])] = devModes(bm, x[0], x[1], x[2]);
+  }
+}
+
+// lambda = 1 / (alpha a + sum_d scale beta (b_hi + b_lo)) (computeLambda).
+__global__ void k_lambda(const BoxDesc* boxes, const Chunk* chunks, const double* a, const double* b0,
+                         const double* b1, const double* b2, double alpha, double beta, double dx, double* lam) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  int i, j, k;
+  if (!allCell(bd, ch.start + threadIdx.x, i, j, k)) return;
+  const Stencil st = stencil(bd, i, j, k);
+  const double scale = 1.0 / (dx * dx);
+  double l = a[st.c] * alpha;
+  l = l + scale * beta * (b0[st.xp] + b0[st.c]);
+  l = l + scale * beta * (b1[st.yp] + b1[st.c]);
+  l = l + scale * beta * (b2[st.zp] + b2[st.c]);
+  lam[st.c] = 1.0 / l;
+}
+
+// averageCells: coarse(i) = refScale * sum of its r^3 fine values in k-j-i order.
+__global__ void k_avg_cells(const BoxDesc* fboxes, const BoxDesc* cboxes, const Chunk* chunks, int r,
+                            const double* f, double* out) {
+  Chunk ch = chunks[blockIdx.x];
+  const BoxDesc cb = cboxes[ch.box];
+  int i, j, k;
+  if (!allCell(cb, ch.start + threadIdx.x, i, j, k)) return;
+  const BoxDesc fb = fboxes[ch.box];
+  const double refScale = 1.0 / (double)(r * r * r);
+  double s = 0.0;
+  bool first = true;
+  for (int c = 0; c < r; ++c)
+    for (int bb = 0; bb < r; ++bb)
+      for (int aa = 0; aa < r; ++aa) {
+        double v = f[cellIndex(fb, i * r + aa, j * r + bb, k * r + c)];
+        s = first ? v : s + v;
+        first = false;
+      }
+  out[cellIndex(cb, i, j, k)] = refScale * s;
+}
+
+// averageFaces: coarse face = refScale * sum over the r^2 fine faces.
+__global__ void k_avg_faces(const BoxDesc* fboxes, const BoxDesc* cboxes, int r, int d, const double* f,
+                            double* out) {
+  const BoxDesc cb = cboxes[blockIdx.x];
+  const BoxDesc fb = fboxes[blockIdx.x];
+  int n[3], ext[3] = {r, r, r};
+  ext[d] = 1;
+  for (int e = 0; e < 3; ++e) n[e] = cb.hi[e] - cb.lo[e] + 1 + (e == d);
+  const double base = 1.0 / (double)r;
+  const double refScale = base * base;
+  const int total = n[0] * n[1] * n[2];
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    int i = cb.lo[0] + q % n[0], j = cb.lo[1] + (q / n[0]) % n[1], k = cb.lo[2] + q / (n[0] * n[1]);
+    double s = 0;
+    for (int c = 0; c < ext[2]; ++c)
+      for (int bb = 0; bb < ext[1]; ++bb)
+        for (int aa = 0; aa < ext[0]; ++aa) s = s + f[cellIndex(fb, i * r + aa, j * r + bb, k * r + c)];
+    out[cellIndex(cb, i, j, k)] = refScale * s;
+  }
+}
+
+}  // namespace
+
+void fillSyntheticLevel(const LevelDev& L, uint64_t seed, double* rhs, double* a, double* const b[3],
+                        cudaStream_t s) {
+  cmg_synth::Problem prob(seed);
+  if (L.nAll == 0) return;
+  k_fill_cells<<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, L.dx, prob.bumps, prob.acoef, rhs, a);
+  CMG_LAUNCHED("fillCells");
+  if (!b) return;
+  for (int d = 0; d < 3; ++d) {
+    k_fill_faces<<<L.nbox, 256, 0, s>>>(L.boxes, L.dx, d, prob.bcoef, b[d]);
+    CMG_LAUNCHED("fillFaces");
+  }
+}
+
+void lambdaLevel(const LevelDev& L, const double* a, const double* const b[3], double alpha, double beta,
+                 double* lam, cudaStream_t s) {
+  if (L.nAll == 0) return;
+  k_lambda<<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, a, b[0], b[1], b[2], alpha, beta, L.dx, lam);
+  CMG_LAUNCHED("lambda");
+}
+
+void averageCoefficients(const LevelDev& F, const LevelDev& C, int r, const double* fa, const double* const fb[3],
+                         double* ca, double* const cbf[3], cudaStream_t s) {
+  if (C.nAll == 0) return;
+  k_avg_cells<<<C.nAll, CHUNK, 0, s>>>(F.boxes, C.boxes, C.chAll, r, fa, ca);
+  CMG_LAUNCHED("averageCells");
+  for (int d = 0; d < 3; ++d) {
+    k_avg_faces<<<C.nbox, 256, 0, s>>>(F.boxes, C.boxes, r, d, fb[d], cbf[d]);
+    CMG_LAUNCHED("averageFaces");
+  }
+}
 
 #define CMG_INST(T)                                                                                       \
   template void ghostFill<T>(const LevelDev&, T*, bool, cudaStream_t, int);                                \

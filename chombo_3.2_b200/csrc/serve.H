@@ -34,6 +34,7 @@ struct RequestResult {
   int exitStatus = -1, iterations = 0;
   double admitted = 0, started = 0, solved = 0, finished = 0;  // seconds after the start
   double setupSeconds = 0, solveSeconds = 0;
+  double gridSeconds = 0, buildSeconds = 0, fillSeconds = 0;  // parts of setupSeconds
   double r0 = 0, rfinal = 0;
   int64_t cells = 0;
   size_t deviceBytes = 0;

@@ -86,6 +86,7 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
         const Clock::time_point ts = Clock::now();
         std::vector<std::vector<Box>> boxes =
             syntheticHierarchy(q.n0, q.levels, q.maxBox, q.blockFactor, q.fillRatio, q.seed, q.thresh);
+        r.gridSeconds = std::chrono::duration<double>(Clock::now() - ts).count();
         est = (double)estimateDeviceBytes(boxes, q.op == 1, q.mixed);
         {
           std::unique_lock<std::mutex> lk(m);
@@ -104,8 +105,12 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
         d.alpha = q.alpha;
         d.beta = q.beta;
         {
+          const Clock::time_point tb = Clock::now();
           std::unique_ptr<Solver> S(new Solver(d, s));
-          fillSynthetic(*S, q.op == 1, q.seed);
+          const Clock::time_point tf = Clock::now();
+          r.buildSeconds = std::chrono::duration<double>(tf - tb).count();
+          S->fillSyntheticDevice(q.seed);
+          r.fillSeconds = std::chrono::duration<double>(Clock::now() - tf).count();
           S->setUseGraphs(q.graphs);
           const Clock::time_point tsolve = Clock::now();
           r.setupSeconds = std::chrono::duration<double>(tsolve - ts).count();

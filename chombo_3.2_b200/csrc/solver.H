@@ -68,6 +68,10 @@ class Solver {
   void setPhi(int l, const double* src, bool onDevice);
   // Builds lambda and the coarsened multigrid coefficients (VC operator).
   void finalizeCoefficients();
+  // The seeded synthetic inputs generated on the device, coefficients
+  // finalised there too (values within the last bits of the host
+  // generator's, which the oracle reproduces bit for bit).
+  void fillSyntheticDevice(uint64_t seed);
   SolveResult solve(const SolveParams& p, bool zeroPhi = true);
   // One composite residual evaluation (AMRMultiGrid::computeAMRResidual).
   double residualNorm();

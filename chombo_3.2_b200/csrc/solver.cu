@@ -497,6 +497,26 @@ void Solver::finalizeCoefficients() {
   ck(cudaStreamSynchronize(s_), "bottom coefficients");
 }
 
+void Solver::fillSyntheticDevice(uint64_t seed) {
+  for (int l = 0; l < numLevels(); ++l)
+    fillSyntheticLevel(amrDev_[l], seed, lev_[l].rhs, desc_.vc ? lev_[l].a : nullptr, desc_.vc ? lev_[l].b : nullptr,
+                       s_);
+  if (desc_.vc) {
+    for (int l = 0; l < numLevels(); ++l)
+      lambdaLevel(amrDev_[l], lev_[l].a, lev_[l].b, desc_.alpha, desc_.beta, lev_[l].lambda, s_);
+    for (size_t d = 0; d < mg_.size(); ++d) {
+      averageCoefficients(amrDev_[0], mgDev_[d], 2 << d, lev_[0].a, lev_[0].b, mgf_[d].a, mgf_[d].b, s_);
+      lambdaLevel(mgDev_[d], mgf_[d].a, mgf_[d].b, desc_.alpha, desc_.beta, mgf_[d].lambda, s_);
+    }
+    coef32Stale_ = true;
+    Coef<double> cb = coefMG((int)mg_.size());
+    gatherSlots(bottom_, cb.a, bottom_.a, s_);
+    for (int k = 0; k < 3; ++k) gatherSlots(bottom_, cb.b[k], bottom_.b[k], s_);
+    gatherSlots(bottom_, cb.lambda, bottom_.lam, s_);
+  }
+  ck(cudaStreamSynchronize(s_), "device inputs");
+}
+
 Coef<double> Solver::coefAMR(int l) const {
   Coef<double> c;
   c.vc = desc_.vc;

@@ -141,6 +141,11 @@ int cmg_residual_norm_noalloc(cmg_hierarchy* h, double* out);
  * workload recipe (Gaussian bumps; exp of a random Fourier series), then
  * finalizes the coefficients. */
 int cmg_fill_synthetic(cmg_hierarchy* h, uint64_t seed);
+/* The same seeded inputs generated on the device, with the coefficient
+ * set-up of cmg_finalize_coefficients done there too (no counterpart in the
+ * reference): fast set-up for served requests.  Values agree with
+ * cmg_fill_synthetic to within the last bits of exp and cos. */
+int cmg_fill_synthetic_device(cmg_hierarchy* h, uint64_t seed);
 
 /* domainSplit (BoxTools/BRMeshRefine.cpp:983-1092), all directions. Boxes are
  * returned in layout order. */
@@ -202,6 +207,7 @@ typedef struct cmg_request {
 typedef struct cmg_request_result {
   int exit_status, iterations, error;
   double admitted, started, solved, finished, setup_seconds, solve_seconds, r0, rfinal;
+  double grid_seconds, build_seconds, fill_seconds; /* parts of setup_seconds */
   int64_t cells;
   uint64_t device_bytes, phi_hash;
 } cmg_request_result;

@@ -241,6 +241,66 @@ struct Motion {
 std::vector<Motion> exchangePlan(const Layout& g);
 // Copier::define(src, dest, ghost=0) local plan (BoxTools/Copier.cpp:903-1110).
 std::vector<Motion> copyPlan(const Layout& src, const Layout& dst);
+// Spatial index of a box list: the boxes overlapping each block of B^3
+// cells, so that "every box meeting region r" costs the blocks of r instead
+// of the whole list.  query() returns box indices in increasing order.
+struct BoxIndex {
+  int B = 8;
+  IV org, n;
+  std::vector<int> start, ids;  // CSR: blocks -> box indices
+  void build(const std::vector<Box>& boxes, int blockSize = 8) {
+    B = blockSize;
+    start.clear();
+    ids.clear();
+    if (boxes.empty()) {
+      n = IV(0, 0, 0);
+      return;
+    }
+    Box all = boxes[0];
+    for (const Box& b : boxes)
+      for (int d = 0; d < 3; ++d) {
+        all.lo[d] = std::min(all.lo[d], b.lo[d]);
+        all.hi[d] = std::max(all.hi[d], b.hi[d]);
+      }
+    Box c = all.coarsen(B);
+    org = c.lo;
+    n = IV(c.size(0), c.size(1), c.size(2));
+    const size_t nb = (size_t)n[0] * n[1] * n[2];
+    std::vector<int> count(nb + 1, 0);
+    auto each = [&](const Box& b, auto fn) {
+      Box q = b.coarsen(B);
+      for (int z = q.lo[2]; z <= q.hi[2]; ++z)
+        for (int y = q.lo[1]; y <= q.hi[1]; ++y)
+          for (int x = q.lo[0]; x <= q.hi[0]; ++x) fn(slot(IV(x, y, z)));
+    };
+    for (const Box& b : boxes) each(b, [&](size_t s) { count[s + 1]++; });
+    for (size_t i = 0; i < nb; ++i) count[i + 1] += count[i];
+    start = count;
+    ids.assign(count[nb], 0);
+    std::vector<int> fillp(count.begin(), count.end() - 1);
+    for (size_t k = 0; k < boxes.size(); ++k) each(boxes[k], [&](size_t s) { ids[fillp[s]++] = (int)k; });
+  }
+  size_t slot(const IV& q) const {
+    return (size_t)(q[0] - org[0]) + (size_t)n[0] * ((size_t)(q[1] - org[1]) + (size_t)n[1] * (q[2] - org[2]));
+  }
+  // Indices of the boxes of `boxes` that intersect r (increasing order).
+  // Read-only, so concurrent queries are safe.
+  void query(const std::vector<Box>& boxes, const Box& r, std::vector<int>& out) const {
+    out.clear();
+    if (r.empty() || n[0] == 0) return;
+    Box q = r.coarsen(B);
+    for (int z = std::max(q.lo[2], org[2]); z <= std::min(q.hi[2], org[2] + n[2] - 1); ++z)
+      for (int y = std::max(q.lo[1], org[1]); y <= std::min(q.hi[1], org[1] + n[1] - 1); ++y)
+        for (int x = std::max(q.lo[0], org[0]); x <= std::min(q.hi[0], org[0] + n[0] - 1); ++x) {
+          size_t s = slot(IV(x, y, z));
+          for (int i = start[s]; i < start[s + 1]; ++i)
+            if (boxes[ids[i]].intersects(r)) out.push_back(ids[i]);
+        }
+    std::sort(out.begin(), out.end());
+    out.erase(std::unique(out.begin(), out.end()), out.end());
+  }
+};
+
 // domainSplit (BoxTools/BRMeshRefine.cpp:983-1092) with all directions refined.
 std::vector<Box> domainSplit(const Box& domain, int maxBoxSize, int blockFactor);
 

@@ -16,6 +16,7 @@ enum { CHUNK = 256 };
 
 struct LevelPlan {
   Layout grids;
+  BoxIndex index;  // spatial index of grids
   Box domain;
   double dx = 0, dxCrse = 0;   // dxCrse: spacing of the coarser AMR level (2 dx)
   std::vector<BoxDesc> boxes;

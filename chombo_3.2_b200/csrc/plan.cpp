@@ -21,8 +21,9 @@ bool faceCFSet(const LevelPlan& L, const Box& b, int d, int side, CellSet& out) 
   Box edge = b.adjCell(d, side, 1) & L.domain;
   if (edge.empty()) return false;
   out.define(edge, true);
-  for (size_t k = 0; k < L.grids.size(); ++k)
-    if (L.grids[k].intersects(edge)) out.subtract(L.grids[k]);
+  std::vector<int> hits;
+  L.index.query(L.grids.boxes, edge, hits);
+  for (int k : hits) out.subtract(L.grids[k]);
   return !out.empty();
 }
 
@@ -146,6 +147,7 @@ std::vector<int> blockTasks(const std::vector<int>& start) {
 
 void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse) {
   L.grids = grids;
+  L.index.build(L.grids.boxes);
   L.domain = domain;
   L.dx = dx;
   L.dxCrse = dxCrse;
@@ -439,6 +441,9 @@ void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
   F.cfOff.clear();
   OwnerIndex owner(C);
   Layout cfine = F.grids.coarsen(2);
+  BoxIndex cfineIndex;
+  cfineIndex.build(cfine.boxes);
+  std::vector<int> hits;
   const double dxf = F.dx;
   const double dxc = 2 * dxf;
   auto pushPool = [&](const std::vector<IV>& cells, const std::vector<double>* w) {
@@ -474,15 +479,16 @@ void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
         g2 = g2 & C.domain;
         g1 = g1 & C.domain;
         CellSet good(g2, false);
-        for (const Box& cb : C.grids.boxes)
-          if (cb.intersects(g2)) good.set(cb, true);
-        for (const Box& fc : cfine.boxes)
-          if (fc.intersects(g2)) good.subtract(fc);
+        C.index.query(C.grids.boxes, g2, hits);
+        for (int k : hits) good.set(C.grids[k], true);
+        cfineIndex.query(cfine.boxes, g2, hits);
+        for (int k : hits) good.subtract(cfine[k]);
         CellSet standard = good;
         standard.intersect(g1);
         standard = standard.erode(t[0]).erode(t[1]);
         // Irregular stencils for base cells outside the standard set.
-        std::map<std::vector<int>, int> coarseIndex;
+        // CFCoarse entry of each base cell (dense over the base set's box)
+        std::vector<int> coarseIndex((size_t)base.dom.numPts(), -1);
         std::vector<IV> baseCells = base.cells();
         std::vector<CoarseStencils> irr(baseCells.size());
         for (size_t i = 0; i < baseCells.size(); ++i)
@@ -517,7 +523,7 @@ void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
             else
               e.mx = CFDeriv{2, (int)cs.mixed.iv.size(), pushPool(cs.mixed.iv, &cs.mixed.w)};
           }
-          coarseIndex[{c[0], c[1], c[2]}] = (int)F.cfCoarse.size();
+          coarseIndex[base.at(c)] = (int)F.cfCoarse.size();
           F.cfCoarse.push_back(e);
         }
         // Fine ghost cells.  Packed faces follow the Fortran PHISTAR index
@@ -530,7 +536,8 @@ void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
           ff.g = cellOf(F, (int)fb, f);
           ff.pb = cellOf(F, (int)fb, f - IV::basis(d, side));
           ff.pa = cellOf(F, (int)fb, f - IV::basis(d, 2 * side));
-          ff.coarse = coarseIndex.at({c[0], c[1], c[2]});
+          ff.coarse = coarseIndex[base.at(c)];
+          if (ff.coarse < 0) throw std::runtime_error("cmg: fine ghost without coarse stencil");
           ff.packed = packed ? 1 : 0;
           double xs[2];
           for (int k = 0; k < 2; ++k) {

@@ -38,7 +38,7 @@ struct RequestResult {
   double r0 = 0, rfinal = 0;
   int64_t cells = 0;
   size_t deviceBytes = 0;
-  uint64_t phiHash = 0;  // FNV-1a of the bits of phi on every level (valid cells)
+  uint64_t phiHash = 0;  // FNV-1a over the 64-bit words of phi on every level (valid cells)
   int error = 0;
 };
 

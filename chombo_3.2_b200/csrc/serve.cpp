@@ -19,10 +19,12 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// FNV-1a over the 64-bit words of the values.
 uint64_t fnv1a(const double* v, size_t n, uint64_t h) {
-  const unsigned char* p = reinterpret_cast<const unsigned char*>(v);
-  for (size_t i = 0; i < n * sizeof(double); ++i) {
-    h ^= p[i];
+  for (size_t i = 0; i < n; ++i) {
+    uint64_t w;
+    std::memcpy(&w, &v[i], sizeof(w));
+    h ^= w;
     h *= 1099511628211ULL;
   }
   return h;

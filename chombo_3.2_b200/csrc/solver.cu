@@ -7,6 +7,8 @@
 
 #include <cstdint>
 #include <mutex>
+#include <exception>
+#include <thread>
 
 #include <cmath>
 #include <cstdio>
@@ -175,29 +177,63 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), des
   const int nlev = (int)desc.boxes.size();
   if (nlev < 1) throw std::runtime_error("cmg: hierarchy needs at least one level");
   amr_.resize(nlev);
-  Box dom = desc.domain;
-  double dx = desc.dx0;
-  for (int l = 0; l < nlev; ++l) {
-    if (l > 0) {
-      dom = dom.refine(2);
-      dx = dx / 2;  // m_dx[i] = m_dx[i-1] / refRatio (VCAMRPoissonOp2.cpp:905-912)
-    }
-    Layout g(desc.boxes[l]);
-    buildLevel(amr_[l], g, dom, dx, l > 0 ? amr_[l - 1].dx : 0.0);
-  }
+  // Host plans, one thread per level and then one per level pair (each pair
+  // writes distinct members of its two levels).
+  std::vector<Box> doms(nlev);
+  std::vector<double> dxs(nlev);
+  doms[0] = desc.domain;
+  dxs[0] = desc.dx0;
   for (int l = 1; l < nlev; ++l) {
-    buildQuadCF(amr_[l], amr_[l - 1]);
-    buildCoarseFine(amr_[l], amr_[l - 1]);
-    buildReflux(amr_[l - 1], amr_[l], desc.vc != 0);
+    doms[l] = doms[l - 1].refine(2);
+    dxs[l] = dxs[l - 1] / 2;  // m_dx[i] = m_dx[i-1] / refRatio (VCAMRPoissonOp2.cpp:905-912)
   }
   // Multigrid depths of level 0 (AMRPoissonOpFactory::MGnewOp,
   // AMRElliptic/AMRPoissonOp.cpp:1923-1989: exists while the boxes are
   // coarsenable by coarsening * s_maxCoarse(2)).
-  const Layout& g0 = amr_[0].grids;
-  for (int c = 2; g0.coarsenable(c * 2); c *= 2) {
-    LevelPlan L;
-    buildLevel(L, g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0);
-    mg_.push_back(L);
+  const Layout g0(desc.boxes[0]);
+  std::vector<int> mgc;
+  for (int c = 2; g0.coarsenable(c * 2); c *= 2) mgc.push_back(c);
+  mg_.resize(mgc.size());
+  {
+    std::vector<std::exception_ptr> err(nlev + mgc.size());
+    std::vector<std::thread> th;
+    for (int l = 0; l < nlev; ++l)
+      th.emplace_back([&, l]() {
+        try {
+          buildLevel(amr_[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0);
+        } catch (...) {
+          err[l] = std::current_exception();
+        }
+      });
+    for (size_t d = 0; d < mgc.size(); ++d)
+      th.emplace_back([&, d]() {
+        try {
+          const int c = mgc[d];
+          buildLevel(mg_[d], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0);
+        } catch (...) {
+          err[nlev + d] = std::current_exception();
+        }
+      });
+    for (auto& t : th) t.join();
+    for (auto& e : err)
+      if (e) std::rethrow_exception(e);
+  }
+  {
+    std::vector<std::exception_ptr> err(nlev);
+    std::vector<std::thread> th;
+    for (int l = 1; l < nlev; ++l)
+      th.emplace_back([&, l]() {
+        try {
+          buildQuadCF(amr_[l], amr_[l - 1]);
+          buildCoarseFine(amr_[l], amr_[l - 1]);
+          buildReflux(amr_[l - 1], amr_[l], desc.vc != 0);
+        } catch (...) {
+          err[l] = std::current_exception();
+        }
+      });
+    for (auto& t : th) t.join();
+    for (auto& e : err)
+      if (e) std::rethrow_exception(e);
   }
   bottomCells_ = desc.domain.numPts();
   for (size_t d = 0; d < mg_.size(); ++d) bottomCells_ /= 8;

@@ -266,7 +266,7 @@ def run_batch(args):
         boxes = cmg.synthetic_hierarchy(sp["n0"], sp["levels"], sp["max_box"], sp["block_factor"],
                                         sp["fill_ratio"], sp["seed"], sp["thresh"])
         h = cmg.Hierarchy(sp["n0"], boxes, op=sp["op"], alpha=sp["alpha"], beta=sp["beta"])
-        h.fill_synthetic(sp["seed"], device=True)
+        h.fill_synthetic(sp["seed"], device=not args.host_fill)
         return h
 
     for w0 in range(0, len(specs), wave):
@@ -274,6 +274,7 @@ def run_batch(args):
         cells += sum(sum(h.num_cells(l) for l in range(h.nlev)) for h in hs)
         for h in hs:
             h.use_graphs(True)
+            h.set_relax_mode(args.relax_mode)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         outs = list(pool.map(lambda h: h.solve(params, mixed=True), hs))
@@ -300,6 +301,7 @@ def run_batch(args):
         "config": {"workload": f"{len(specs)} independent 2-level hierarchies, base 32^3-128^3 log-uniform (x16), "
                                "max box 16/24/32, Poisson or VC Helmholtz, rel. residual 1e-10",
                    "resident_per_wave": wave, "concurrent_streams": args.inflight, "cells": cells,
+                   "relax_mode": args.relax_mode,
                    "timing": "wall clock around the concurrent solves of each resident wave (host "
                              "set-up of the hierarchies not timed)"},
         "plain_fp64_one_at_a_time": {"value": base, "unit": "solves/s", "ratio": value / base},
@@ -381,6 +383,7 @@ def main():
     ap.add_argument("--relax-mode", type=int, default=0, choices=[0, 1, 2],
                     help="relaxation variant: 0 autotuned per level, 1 ghost fills, 2 in-pass ghosts")
     ap.add_argument("--batch", type=int, default=512, help="config3: number of hierarchies")
+    ap.add_argument("--host-fill", action="store_true", help="config3: generate the inputs on the host")
     ap.add_argument("--wave", type=int, default=128, help="config3: hierarchies resident at once")
     ap.add_argument("--inflight", type=int, default=16, help="config3/4: concurrent solves")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="config4: arrival rates (req/s)")

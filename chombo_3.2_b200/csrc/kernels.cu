@@ -319,8 +319,8 @@ __device__ __forceinline__ void atomicMaxPos(double* addr, double v) {
 
 template <class T>
 __global__ void k_maxnorm(const BoxDesc* boxes, const Chunk* chunks, int nchunks, const T* f, double* out) {
-  // Grid-stride over the chunks, so that only one atomic per block (not per
-  // chunk) reaches the single output word.
+  // Blocks stride over the chunks (one chunk each when the grid covers
+  // them), so a large level sends one atomic per block, not per chunk.
   double v = 0.0;
   for (int cix = blockIdx.x; cix < nchunks; cix += gridDim.x) {
     Chunk ch = chunks[cix];
@@ -983,7 +983,9 @@ void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s) {
 template <class T>
 void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s) {
   if (L.nAll == 0) return;
-  const int blocks = std::min(L.nAll, 148 * 8);
+  // One chunk per block (lowest latency) up to 4096 chunks; beyond, a
+  // grid of 4096 blocks striding over them.
+  const int blocks = std::min(L.nAll, 4096);
   k_maxnorm<T><<<blocks, CHUNK, 0, s>>>(L.boxes, L.chAll, L.nAll, f, out);
   CMG_LAUNCHED("maxNorm");
 }

@@ -80,6 +80,10 @@ template <class T> void zeroCovered(const LevelDev& L, T* f, cudaStream_t s);
 template <class T>
 void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s,
           bool inlineGhosts = false);
+// nsweeps red-black sweeps of a small level in a single one-block launch
+// (in-pass ghosts, block barriers between colour passes); same results.
+template <class T>
+void relaxBlock(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int nsweeps, cudaStream_t s);
 // residualI form: r = rhs - L(phi) in the operator's own expression order.
 template <class T> void residual(const LevelDev& L, T* r, const T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s);
 // applyOpI form: lofphi = L(phi).

@@ -258,6 +258,55 @@ __global__ void k_gsrb(const BoxDesc* boxes, const Chunk* chunks, T* phi, const 
   }
 }
 
+// n red-black sweeps of a small level in one launch: one block walks every
+// cell of a colour (ghosts from their rules), synchronises, and goes on to
+// the next colour and sweep -- the launches of 2n colour passes replaced by
+// block barriers.  Same cell updates in the same colour order.
+template <class T, int VC>
+__global__ void __launch_bounds__(1024) k_relax_block(const BoxDesc* boxes, const Chunk* ch0, int n0,
+                                                      const Chunk* ch1, int n1, T* phi, const T* rhs, Scal sc,
+                                                      const T* a, const T* b0, const T* b1, const T* b2,
+                                                      const T* lam, const FaceRule* __restrict__ rules,
+                                                      const int* __restrict__ faceOff, GhostCoef gc, int nsweeps) {
+  const T dxinv = T(sc.dxinv);
+  for (int it = 0; it < nsweeps; ++it)
+    for (int color = 0; color <= 1; ++color) {
+      const Chunk* chunks = color ? ch1 : ch0;
+      const int total = (color ? n1 : n0) * CHUNK;
+      for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const Chunk ch = chunks[idx / CHUNK];
+        const BoxDesc bd = boxes[ch.box];
+        int i, j, k;
+        if (!colorCell(bd, ch.start + idx % CHUNK, color, i, j, k)) continue;
+        const Stencil st = stencil(bd, i, j, k);
+        const int64_t c = st.c;
+        const T pc = phi[c];
+        const int b = ch.box;
+        T v[6];
+        v[0] = i == bd.hi[0] ? ghostValue(rules, faceOff, bd, b, 0, 1, i, j, k, pc, phi, gc) : phi[st.xp];
+        v[1] = i == bd.lo[0] ? ghostValue(rules, faceOff, bd, b, 0, -1, i, j, k, pc, phi, gc) : phi[st.xm];
+        v[2] = j == bd.hi[1] ? ghostValue(rules, faceOff, bd, b, 1, 1, i, j, k, pc, phi, gc) : phi[st.yp];
+        v[3] = j == bd.lo[1] ? ghostValue(rules, faceOff, bd, b, 1, -1, i, j, k, pc, phi, gc) : phi[st.ym];
+        v[4] = k == bd.hi[2] ? ghostValue(rules, faceOff, bd, b, 2, 1, i, j, k, pc, phi, gc) : phi[st.zp];
+        v[5] = k == bd.lo[2] ? ghostValue(rules, faceOff, bd, b, 2, -1, i, j, k, pc, phi, gc) : phi[st.zm];
+        if (VC) {
+          T div = b0[st.xp] * (v[0] - pc) - b0[c] * (pc - v[1]) + b1[st.yp] * (v[2] - pc) - b1[c] * (pc - v[3]) +
+                  b2[st.zp] * (v[4] - pc) - b2[c] * (pc - v[5]);
+          T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * div * dxinv;
+          phi[c] = pc - lam[c] * (lofphi - rhs[c]);
+        } else if (sc.laplacian) {
+          T lphi = (v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) * dxinv;
+          phi[c] = T(sc.lambda) * (rhs[c] - lphi);
+        } else {
+          T lphi = ((v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) - T(2.0) * T(3) * pc) * dxinv;
+          T helmop = T(sc.alpha) * pc + T(sc.beta) * lphi;
+          phi[c] = pc + T(sc.lambda) * (helmop - rhs[c]);
+        }
+      }
+      __syncthreads();
+    }
+}
+
 // OPERATORLAPRES / OPERATORLAP (AMRPoissonOpF.ChF:287-377) and
 // VCCOMPUTERES3D / VCCOMPUTEOP3D (VCAMRPoissonOpF.ChF:148-312).
 // mode 0: r = rhs - L(phi) (residual form), mode 1: r = L(phi).
@@ -857,6 +906,23 @@ void zeroCovered(const LevelDev& L, T* f, cudaStream_t s) {
 }
 
 template <class T>
+void relaxBlock(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int nsweeps, cudaStream_t s) {
+  if (L.nColor[0] + L.nColor[1] == 0 || nsweeps <= 0) return;
+  Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
+  const double dx = L.dx, dxc = L.dxCrse;
+  GhostCoef gc{2 * (dxc - dx) / (dxc + dx), -(dxc - dx) / (dxc + 3 * dx), 1 - 2 * dx / (dx + dxc)};
+  if (c.vc)
+    k_relax_block<T, 1><<<1, 1024, 0, s>>>(L.boxes, L.chColor[0], L.nColor[0], L.chColor[1], L.nColor[1], phi, rhs,
+                                           sc, c.a, c.b[0], c.b[1], c.b[2], c.lambda, L.faceRules, L.faceOff, gc,
+                                           nsweeps);
+  else
+    k_relax_block<T, 0><<<1, 1024, 0, s>>>(L.boxes, L.chColor[0], L.nColor[0], L.chColor[1], L.nColor[1], phi, rhs,
+                                           sc, nullptr, nullptr, nullptr, nullptr, nullptr, L.faceRules, L.faceOff,
+                                           gc, nsweeps);
+  CMG_LAUNCHED("relaxBlock");
+}
+
+template <class T>
 void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s, bool inlineGhosts) {
   int n = L.nColor[color];
   if (n == 0) return;
@@ -1196,6 +1262,7 @@ void averageCoefficients(const LevelDev& F, const LevelDev& C, int r, const doub
   template void ghostFill<T>(const LevelDev&, T*, bool, cudaStream_t, int);                                \
   template void zeroCovered<T>(const LevelDev&, T*, cudaStream_t);                                         \
   template void gsrb<T>(const LevelDev&, T*, const T*, const Coef<T>&, int, cudaStream_t, bool);           \
+  template void relaxBlock<T>(const LevelDev&, T*, const T*, const Coef<T>&, int, cudaStream_t);              \
   template void residual<T>(const LevelDev&, T*, const T*, const T*, const Coef<T>&, cudaStream_t);        \
   template void applyOp<T>(const LevelDev&, T*, const T*, const Coef<T>&, cudaStream_t);                   \
   template void negAdd<T>(const LevelDev&, T*, const T*, const T*, cudaStream_t);                          \

@@ -133,7 +133,10 @@ class Solver {
   template <class T> void relaxAMR(int l, T* phi, const T* rhs, int n);
   template <class T> void relaxMG(int d, T* phi, const T* rhs, int n);
   template <class T>
-  void relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls, bool inl);
+  void relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls,
+                  int variant);
+  // Levels up to this many cells may relax all sweeps in one one-block launch.
+  static constexpr double kBlockRelaxMaxCells = 32768;
   template <class T> void fill(const LevelDev& L, T* f, bool withCF, int par = -1);
   template <class T>
   void amrResidualLevel(int ilev, int lmax, std::vector<T*>& res, std::vector<T*>& phi, std::vector<T*>& rhs);
@@ -161,7 +164,8 @@ class Solver {
   std::map<cudaGraphExec_t, long long> graphLaunches_;  // kernel launches per replay
   bool useGraphs_ = false;
   // Relaxation variant per AMR level / MG depth: ghost fill before each
-  // colour pass (0) or face ghosts evaluated inside the pass (1).
+  // colour pass (0), face ghosts evaluated inside the pass (1), or every
+  // sweep in one one-block launch with in-pass ghosts (2).
   std::vector<char> inlineA_, inlineM_;
   bool tuned_ = false;
   int relaxMode_ = 0;  // 0: autotuned, 1: always fills, 2: always inline

@@ -6,6 +6,7 @@
 #include "solver.H"
 
 #include <cstdint>
+#include <algorithm>
 #include <mutex>
 #include <exception>
 #include <thread>
@@ -636,8 +637,13 @@ void Solver::copyField(const LevelDev& L, T* dst, const T* src) {
 // every face borders one cell of each colour (6 words).
 template <class T>
 void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* phi, const T* rhs, int n, int cls,
-                        bool inl) {
+                        int variant) {
   const double bytes = cells * sizeof(T) * (c.vc ? 6.0 : 2.0);
+  if (variant == 2) {
+    timed(cls, bytes * 2 * n, [&]() { relaxBlock(L, phi, rhs, c, n, s_); });
+    return;
+  }
+  const bool inl = variant == 1;
   for (int it = 0; it < n; ++it)
     for (int color = 0; color <= 1; ++color) {
       if (!inl) fill(L, phi, true, 1 - color);
@@ -649,14 +655,14 @@ template <class T>
 void Solver::relaxAMR(int l, T* phi, const T* rhs, int n) {
   const int finest = (int)amr_.size() - 1;
   relaxLevel(amrDev_[l], (double)amr_[l].grids.numCells(), coefA<T>(l), phi, rhs, n,
-             l == finest ? P_RELAX_FINE : P_RELAX, inlineA_[l] != 0);
+             l == finest ? P_RELAX_FINE : P_RELAX, inlineA_[l]);
 }
 
 template <class T>
 void Solver::relaxMG(int d, T* phi, const T* rhs, int n) {
   if (d == 0) return relaxAMR(0, phi, rhs, n);
   relaxLevel(mgDev_[d - 1], (double)mg_[d - 1].grids.numCells(), coefM<T>(d), phi, rhs, n, P_RELAX,
-             inlineM_[d - 1] != 0);
+             inlineM_[d - 1]);
 }
 
 // Relaxation autotuner: per AMR level and multigrid depth, time one red-black
@@ -667,19 +673,19 @@ void Solver::relaxMG(int d, T* phi, const T* rhs, int n) {
 void Solver::tuneRelaxation() {
   tuned_ = true;
   tuneMs_.clear();
-  inlineA_.assign(amr_.size(), relaxMode_ == 2);
-  inlineM_.assign(mg_.size(), relaxMode_ == 2);
+  inlineA_.assign(amr_.size(), relaxMode_ == 2 ? 1 : 0);
+  inlineM_.assign(mg_.size(), relaxMode_ == 2 ? 1 : 0);
   if (relaxMode_ != 0) return;
   cudaEvent_t e[3];
   for (auto& x : e) ck(cudaEventCreate(&x), "event");
   const bool prof = profOn_;
   profOn_ = false;
   auto timeOne = [&](const LevelDev& L, double cells, const Coef<double>& c, double* phi, const double* rhs,
-                     bool inl) {
+                     int variant) {
     float best = 1e30f;
     for (int rep = 0; rep < 3; ++rep) {
       ck(cudaEventRecord(e[0], s_), "event");
-      relaxLevel(L, cells, c, phi, rhs, 1, P_RELAX, inl);
+      relaxLevel(L, cells, c, phi, rhs, 4, P_RELAX, variant);
       ck(cudaEventRecord(e[1], s_), "event");
       ck(cudaEventSynchronize(e[1]), "event sync");
       float ms = 0;
@@ -691,19 +697,23 @@ void Solver::tuneRelaxation() {
   for (size_t l = 0; l < amr_.size(); ++l) {
     const double cells = (double)amr_[l].grids.numCells();
     Coef<double> c = coefAMR((int)l);
-    float tf = timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, false);
-    float ti = timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, true);
-    inlineA_[l] = ti < tf;
-    tuneMs_.push_back({tf, ti});
+    float t[3];
+    for (int v = 0; v < 3; ++v)
+      t[v] = (v == 2 && cells > kBlockRelaxMaxCells) ? 1e30f
+                                                     : timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, v);
+    inlineA_[l] = (char)(std::min_element(t, t + 3) - t);
+    tuneMs_.push_back({t[0], std::min(t[1], t[2])});
     zeroField(amrDev_[l], lev_[l].corr);
   }
   for (size_t d = 0; d < mg_.size(); ++d) {
     const double cells = (double)mg_[d].grids.numCells();
     Coef<double> c = coefMG((int)d + 1);
-    float tf = timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, false);
-    float ti = timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, true);
-    inlineM_[d] = ti < tf;
-    tuneMs_.push_back({tf, ti});
+    float t[3];
+    for (int v = 0; v < 3; ++v)
+      t[v] = (v == 2 && cells > kBlockRelaxMaxCells) ? 1e30f
+                                                     : timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, v);
+    inlineM_[d] = (char)(std::min_element(t, t + 3) - t);
+    tuneMs_.push_back({t[0], std::min(t[1], t[2])});
     zeroField(mgDev_[d], mgf_[d].corr);
   }
   profOn_ = prof;
@@ -716,7 +726,7 @@ void Solver::relaxVariants(std::vector<int>& inl, std::vector<float>& msFill, st
   msFill.clear();
   msInline.clear();
   for (char c : inlineA_) inl.push_back(c);
-  for (char c : inlineM_) inl.push_back(c);
+  for (char c : inlineM_) inl.push_back(c);  // 0 fills, 1 in-pass ghosts, 2 one-block sweeps
   for (auto& t : tuneMs_) {
     msFill.push_back(t.first);
     msInline.push_back(t.second);

@@ -104,7 +104,9 @@ int cmg_use_graphs(cmg_hierarchy* h, int on);
  * the pass from the same fill rules, no fill.  Identical results. */
 int cmg_set_relax_mode(cmg_hierarchy* h, int mode);
 /* The relaxation variant of every AMR level, then every multigrid depth
- * (1 = in-pass ghosts), with the autotuner's sweep times in ms (-1 when a
+ * (0 = ghost fills, 1 = in-pass ghosts, 2 = all sweeps in one one-block
+ * launch, for levels of at most 32768 cells), with the autotuner's times in
+ * ms for four sweeps with fills and with the best other variant (-1 when a
  * mode was forced); runs the tuner if it has not run.  n: entries. */
 int cmg_relax_variants(cmg_hierarchy* h, int* inline_out, float* ms_fill, float* ms_inline, int cap, int* n);
 

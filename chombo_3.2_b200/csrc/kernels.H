@@ -88,7 +88,8 @@ void relaxBlock(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int n
 template <class T> void residual(const LevelDev& L, T* r, const T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s);
 // applyOpI form: lofphi = L(phi).
 template <class T> void applyOp(const LevelDev& L, T* lofphi, const T* phi, const Coef<T>& c, cudaStream_t s);
-// r = -lofphi + rhs over valid cells (LevelDataOps::axby(r, r, rhs, -1, 1)).
+// r = -lofphi + rhs (LevelDataOps::axby(r, r, rhs, -1, 1)); valid cells as the
+// reference, ghost slots overwritten too (they are refilled before any read).
 template <class T> void negAdd(const LevelDev& L, T* r, const T* lofphi, const T* rhs, cudaStream_t s);
 // Multigrid restriction of the residual (RESTRICTRES), box b -> coarsened box b.
 template <class T> void restrictMG(const LevelDev& F, const LevelDev& C, T* resC, const T* phi, const T* rhs,
@@ -104,7 +105,8 @@ template <class T> void quadCF(const LevelDev& F, T* phiF, const T* phiC, cudaSt
 // Flux-register correction of lofphiC from phiC and phiF (finer level).
 template <class T> void reflux(const LevelDev& C, T* lofphiC, const T* phiC, const T* phiF, const Coef<T>& cc,
                                const Coef<T>& cf, cudaStream_t s);
-// lhs += scale * x over valid cells.
+// lhs += scale * x (LevelDataOps::incr); valid cells as the reference, ghost
+// slots too (refilled before any read).
 template <class T> void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s);
 // lhs += x over valid cells, an FP32 correction added to an FP64 field.
 void incrMixed(const LevelDev& L, double* lhs, const float* x, cudaStream_t s);

@@ -353,6 +353,23 @@ __global__ void k_incr(const BoxDesc* boxes, const Chunk* chunks, T* lhs, const 
   lhs[c] = lhs[c] + T(x[c]) * scale;
 }
 
+// lhs += x * scale and r = -lofphi + rhs over whole level arrays, ghost and
+// padding slots included: the valid cells get exactly the reference's
+// values, the ghost slots of these fields are rewritten by a ghost fill or
+// coarse-fine interpolation before anything reads them, and one flat,
+// perfectly coalesced loop beats walking the valid cells box by box.
+template <class T, class X>
+__global__ void k_incr_flat(T* lhs, const X* x, T scale, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    lhs[q] = lhs[q] + T(x[q]) * scale;
+}
+template <class T>
+__global__ void k_negadd_flat(T* r, const T* lofphi, const T* rhs, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    r[q] = lofphi[q] * T(-1) + rhs[q] * T(1);
+}
+inline int flatBlocks(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 16); }
+
 // dst = src over whole arrays (ghosts included), converting the type.
 template <class D, class S>
 __global__ void k_convert(D* dst, const S* src, int64_t n) {
@@ -973,8 +990,8 @@ void applyOp(const LevelDev& L, T* lofphi, const T* phi, const Coef<T>& c, cudaS
 
 template <class T>
 void negAdd(const LevelDev& L, T* r, const T* lofphi, const T* rhs, cudaStream_t s) {
-  if (L.nAll == 0) return;
-  k_negadd<T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, r, lofphi, rhs);
+  if (L.nelem == 0) return;
+  k_negadd_flat<T><<<flatBlocks(L.nelem), 256, 0, s>>>(r, lofphi, rhs, L.nelem);
   CMG_LAUNCHED("negAdd");
 }
 
@@ -1041,8 +1058,8 @@ void reflux(const LevelDev& C, T* lofphiC, const T* phiC, const T* phiF, const C
 
 template <class T>
 void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s) {
-  if (L.nAll == 0) return;
-  k_incr<T, T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lhs, x, T(scale));
+  if (L.nelem == 0) return;
+  k_incr_flat<T, T><<<flatBlocks(L.nelem), 256, 0, s>>>(lhs, x, T(scale), L.nelem);
   CMG_LAUNCHED("incr");
 }
 
@@ -1100,8 +1117,8 @@ void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream
 }
 
 void incrMixed(const LevelDev& L, double* lhs, const float* x, cudaStream_t s) {
-  if (L.nAll == 0) return;
-  k_incr<double, float><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lhs, x, 1.0);
+  if (L.nelem == 0) return;
+  k_incr_flat<double, float><<<flatBlocks(L.nelem), 256, 0, s>>>(lhs, x, 1.0, L.nelem);
   CMG_LAUNCHED("incrMixed");
 }
 

@@ -139,32 +139,44 @@ __global__ void __launch_bounds__(GHOST_THREADS) k_ghost(const GhostTaskDev* tas
 }
 
 // Ghost fill from the flat per-cell lists: entries [a0, a1) then [b0, b1),
-// one thread each, no table walk between a thread and its data.
-template <class T>
+// U per thread (GHOST_THREADS apart, so each batch of loads is coalesced),
+// no table walk between a thread and its data.  A fill's sources are valid
+// cells and its destinations ghost cells, so all loads of a thread are
+// issued before its stores: the list and source latencies of its U entries
+// overlap instead of adding up.
+template <class T, int U>
 __global__ void __launch_bounds__(GHOST_THREADS) k_ghostcells(const GhostCell* __restrict__ e, int a0, int a1,
                                                               int b0, int b1, T* f, T c1, T c2, T flin) {
-  int q = blockIdx.x * GHOST_THREADS + threadIdx.x;
-  const int na = a1 - a0;
-  if (q < na)
-    q += a0;
-  else if (q - na < b1 - b0)
-    q = q - na + b0;
-  else
-    return;
-  const GhostCell g = e[q];
-  const T v1 = f[g.s1];
-  T out;
-  if (g.s2 == -1) {
-    out = v1;
-  } else if (g.s2 == -2) {
-    T zero = T(0);
-    out = T(2) * zero - v1;
-  } else if (g.s2 == -3) {
-    out = flin * v1;
-  } else {
-    out = c1 * v1 + c2 * f[g.s2];
+  const int na = a1 - a0, n = na + (b1 - b0);
+  const int base = blockIdx.x * (GHOST_THREADS * U) + threadIdx.x;
+  GhostCell g[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int q = base + u * GHOST_THREADS;
+    g[u] = q < n ? e[q < na ? a0 + q : b0 + (q - na)] : GhostCell{-1, 0, -1};
   }
-  f[g.dst] = out;
+  T v1[U], v2[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    v1[u] = g[u].dst >= 0 ? f[g[u].s1] : T(0);
+    v2[u] = g[u].dst >= 0 && g[u].s2 >= 0 ? f[g[u].s2] : T(0);
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (g[u].dst < 0) continue;
+    T out;
+    if (g[u].s2 == -1) {
+      out = v1[u];
+    } else if (g[u].s2 == -2) {
+      T zero = T(0);
+      out = T(2) * zero - v1[u];
+    } else if (g[u].s2 == -3) {
+      out = flin * v1[u];
+    } else {
+      out = c1 * v1[u] + c2 * v2[u];
+    }
+    f[g[u].dst] = out;
+  }
 }
 
 // ---------------------------------------------------------------- stencils
@@ -909,8 +921,16 @@ void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par) {
   T c1 = T(2 * (dxc - dx) / (dxc + dx));
   T c2 = T(-(dxc - dx) / (dxc + 3 * dx));
   T flin = T(1 - 2 * dx / (dx + dxc));
-  k_ghostcells<T><<<(n + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(L.gcells, a0, a1, b0, b1, f, c1,
-                                                                                    c2, flin);
+  // Four entries per thread once the fill exceeds one wave of resident
+  // threads (148 SMs x 2048), one per thread below that.
+  if (n > 148 * 2048) {
+    constexpr int U = 4;
+    k_ghostcells<T, U><<<(n + GHOST_THREADS * U - 1) / (GHOST_THREADS * U), GHOST_THREADS, 0, s>>>(
+        L.gcells, a0, a1, b0, b1, f, c1, c2, flin);
+  } else {
+    k_ghostcells<T, 1><<<(n + GHOST_THREADS - 1) / GHOST_THREADS, GHOST_THREADS, 0, s>>>(L.gcells, a0, a1, b0, b1, f,
+                                                                                       c1, c2, flin);
+  }
   CMG_LAUNCHED("ghostFill");
 }
 

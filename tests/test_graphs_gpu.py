@@ -48,11 +48,14 @@ def test_graph_replay_is_bit_identical(cmg, name, mixed):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["vc_3lev_16", "poisson_3lev_32", "helmholtz_2lev_16"])
-def test_relaxation_variants_are_bit_identical(cmg, name):
+@pytest.mark.parametrize("name,num_mg", [("vc_3lev_16", 1), ("poisson_3lev_32", 1), ("helmholtz_2lev_16", 1),
+                                         ("vc_3lev_16", 2), ("poisson_1lev_32", 1), ("vc_1lev_32", 2)])
+def test_relaxation_variants_are_bit_identical(cmg, name, num_mg):
     """Ghost fill before each colour pass (mode 1), face ghosts evaluated in
-    the pass (mode 2) and the autotuned mix (mode 0) give the same bits."""
+    the pass (mode 2) and the autotuned mix (mode 0) give the same bits, with
+    V-cycles and with W-cycles (num_mg=2), on one and on several levels."""
     h, p, meta = make(cmg, name)
+    p.num_mg = num_mg
     nlev = len(meta["boxes"])
     ref = None
     for mode in (1, 2, 0):

@@ -334,7 +334,7 @@ def run_serving(args):
             reqs.append(dict(arrival=t, n0=n0, levels=int(rng.integers(1, 4)), max_box=32, block_factor=8,
                              seed=5000 + i, op=1 if vc else 0, alpha=1.0 if vc else 0.0,
                              beta=-1.0 if vc else 1.0, params=cmg.solve_params(eps=eps), mixed=True,
-                             graphs=True))
+                             graphs=True, device_tags=not args.host_tags))
         return reqs
 
     def stats(res, wall):
@@ -343,7 +343,9 @@ def run_serving(args):
         return {"p50_ms": 1000.0 * float(np.percentile(lat, 50)), "p99_ms": 1000.0 * float(np.percentile(lat, 99)),
                 "solves_per_s": len(res) / wall, "converged": ok, "requests": len(res),
                 "mean_setup_ms": 1000.0 * float(np.mean([r["setup_seconds"] for r, _ in res])),
-                "mean_solve_ms": 1000.0 * float(np.mean([r["solve_seconds"] for r, _ in res]))}
+                "mean_solve_ms": 1000.0 * float(np.mean([r["solve_seconds"] for r, _ in res])),
+                "mean_grid_ms": 1000.0 * float(np.mean([r["grid_seconds"] for r, _ in res])),
+                "mean_build_ms": 1000.0 * float(np.mean([r["build_seconds"] for r, _ in res]))}
 
     per_rate = {}
     for rate in rates:
@@ -364,7 +366,8 @@ def run_serving(args):
         "config": {"workload": "open-loop Poisson arrivals, 1-3 level hierarchies, base 32^3-256^3 log-uniform "
                                "(x16), Poisson or VC Helmholtz, tolerance 1e-8 or 1e-10, 120 GB budget",
                    "requests_per_rate": args.requests, "workers": args.inflight,
-                   "latency": "arrival to phi on the host, including grid generation and set-up"},
+                   "latency": "arrival to phi on the host, including grid generation and set-up",
+                   "tagging": "host" if args.host_tags else "device"},
         "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "per_rate": per_rate,
         "plain_fp64_one_at_a_time": base,
     }
@@ -387,6 +390,7 @@ def main():
     ap.add_argument("--wave", type=int, default=128, help="config3: hierarchies resident at once")
     ap.add_argument("--inflight", type=int, default=16, help="config3/4: concurrent solves")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="config4: arrival rates (req/s)")
+    ap.add_argument("--host-tags", action="store_true", help="config4: tag for grid generation on the host")
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per rate")
     args = ap.parse_args()
     if args.impl != "reference" and args.workload in ("config3", "config4"):

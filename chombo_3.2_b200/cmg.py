@@ -41,7 +41,7 @@ class Request(ctypes.Structure):
                 ("max_box", ctypes.c_int), ("block_factor", ctypes.c_int), ("fill_ratio", ctypes.c_double),
                 ("thresh", ctypes.c_double), ("seed", ctypes.c_uint64), ("op", ctypes.c_int),
                 ("alpha", ctypes.c_double), ("beta", ctypes.c_double), ("params", SolveParams),
-                ("mixed", ctypes.c_int), ("graphs", ctypes.c_int)]
+                ("mixed", ctypes.c_int), ("graphs", ctypes.c_int), ("device_tags", ctypes.c_int)]
 
 
 class RequestResult(ctypes.Structure):
@@ -68,6 +68,7 @@ def serve(requests, hbm_budget=120e9, max_inflight=16, open_loop=True):
         q.alpha, q.beta = r.get("alpha", 0.0), r.get("beta", 1.0)
         q.params = r.get("params") or solve_params(eps=r.get("eps", 1e-10))
         q.mixed, q.graphs = int(r.get("mixed", True)), int(r.get("graphs", True))
+        q.device_tags = int(r.get("device_tags", False))
     out = (RequestResult * max(n, 1))()
     wall = ctypes.c_double()
     _check(lib().cmg_serve(arr, n, ctypes.c_double(hbm_budget), int(max_inflight), int(open_loop), out,
@@ -108,16 +109,22 @@ def boxes_array(boxes):
     return arr
 
 
-def synthetic_hierarchy(n0, levels, max_box=32, block_factor=8, fill_ratio=0.75, seed=20261203, thresh=0.1):
-    """Box lists (lo0, lo1, lo2, hi0, hi1, hi2) per level of the seeded example hierarchy."""
+def synthetic_hierarchy(n0, levels, max_box=32, block_factor=8, fill_ratio=0.75, seed=20261203, thresh=0.1,
+                        device_tags=False):
+    """Box lists (lo0, lo1, lo2, hi0, hi1, hi2) per level of the seeded example hierarchy; device_tags runs the
+    tagging passes on the current CUDA device (cmg_synthetic_hierarchy_device)."""
     L = lib()
+    fn = L.cmg_synthetic_hierarchy_device if device_tags else L.cmg_synthetic_hierarchy
     nl, tot = ctypes.c_int(), ctypes.c_int()
     counts = (ctypes.c_int * levels)()
     args = (int(n0), int(levels), int(max_box), int(block_factor), ctypes.c_double(fill_ratio),
             ctypes.c_uint64(seed), ctypes.c_double(thresh), ctypes.byref(nl), counts)
-    _check(L.cmg_synthetic_hierarchy(*args, None, 0, ctypes.byref(tot)))
-    out = (Box * max(tot.value, 1))()
-    _check(L.cmg_synthetic_hierarchy(*args, out, tot.value, ctypes.byref(tot)))
+    cap = 1 << 16
+    out = (Box * cap)()
+    _check(fn(*args, out, cap, ctypes.byref(tot)))
+    if tot.value > cap:
+        out = (Box * tot.value)()
+        _check(fn(*args, out, tot.value, ctypes.byref(tot)))
     res, k = [], 0
     for l in range(nl.value):
         res.append([tuple(out[k + i].lo) + tuple(out[k + i].hi) for i in range(counts[l])])

@@ -16,6 +16,7 @@
 #include "serve.H"
 #include "solver.H"
 #include "synthfill.H"
+#include "tagging.H"
 
 struct cmg_hierarchy {
   cudaStream_t stream = nullptr;
@@ -333,14 +334,29 @@ int cmg_residual_norm_noalloc(cmg_hierarchy* h, double* out) {
   });
 }
 
-int cmg_synthetic_hierarchy(int n0, int nlevels, int max_box, int block_factor, double fill_ratio, uint64_t seed,
-                            double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes, int cap, int* ntotal) {
+static int syntheticHierarchyImpl(int n0, int nlevels, int max_box, int block_factor, double fill_ratio,
+                                  uint64_t seed, double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes,
+                                  int cap, int* ntotal, bool device) {
   return guard([&]() {
     if (!nlevels_out || !nboxes || !ntotal) throw std::invalid_argument("cmg: null output pointer");
     if (max_box < 0 || block_factor < 1 || !(fill_ratio > 0.0 && fill_ratio <= 1.0))
       throw std::invalid_argument("cmg: invalid grid generation parameters");
-    std::vector<std::vector<cmg::Box>> g =
-        cmg::syntheticHierarchy(n0, nlevels, max_box, block_factor, fill_ratio, seed, thresh);
+    std::vector<std::vector<cmg::Box>> g;
+    if (device) {
+      cudaStream_t s = nullptr;
+      if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+        throw std::runtime_error("cmg: no CUDA device for tagging");
+      try {
+        cmg::DeviceTagger tagger(s);
+        g = cmg::syntheticHierarchy(n0, nlevels, max_box, block_factor, fill_ratio, seed, thresh, &tagger);
+      } catch (...) {
+        cudaStreamDestroy(s);
+        throw;
+      }
+      cudaStreamDestroy(s);
+    } else {
+      g = cmg::syntheticHierarchy(n0, nlevels, max_box, block_factor, fill_ratio, seed, thresh);
+    }
     *nlevels_out = (int)g.size();
     int total = 0;
     for (size_t l = 0; l < g.size(); ++l) {
@@ -352,6 +368,19 @@ int cmg_synthetic_hierarchy(int n0, int nlevels, int max_box, int block_factor, 
     }
     *ntotal = total;
   });
+}
+
+int cmg_synthetic_hierarchy(int n0, int nlevels, int max_box, int block_factor, double fill_ratio, uint64_t seed,
+                            double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes, int cap, int* ntotal) {
+  return syntheticHierarchyImpl(n0, nlevels, max_box, block_factor, fill_ratio, seed, thresh, nlevels_out, nboxes,
+                                boxes, cap, ntotal, false);
+}
+
+int cmg_synthetic_hierarchy_device(int n0, int nlevels, int max_box, int block_factor, double fill_ratio,
+                                   uint64_t seed, double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes,
+                                   int cap, int* ntotal) {
+  return syntheticHierarchyImpl(n0, nlevels, max_box, block_factor, fill_ratio, seed, thresh, nlevels_out, nboxes,
+                                boxes, cap, ntotal, true);
 }
 
 int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_inflight, int open_loop,
@@ -387,6 +416,7 @@ int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_infligh
       r.params.normThresh = a.params.norm_thresh;
       r.mixed = a.mixed != 0;
       r.graphs = a.graphs != 0;
+      r.deviceTags = a.device_tags != 0;
     }
     cmg::ServeOptions opt;
     opt.hbmBudget = hbm_budget;

@@ -151,6 +151,7 @@ struct CellSet {
   }
   void subtract(const Box& b) { set(b, false); }
   void intersect(const Box& b) {
+    if (dom.empty() || (b.contains(dom.lo) && b.contains(dom.hi))) return;
     for (int k = dom.lo[2]; k <= dom.hi[2]; ++k)
       for (int j = dom.lo[1]; j <= dom.hi[1]; ++j)
         for (int i = dom.lo[0]; i <= dom.hi[0]; ++i)
@@ -161,7 +162,7 @@ struct CellSet {
     for (uint8_t b : bits) n += b;
     return n;
   }
-  bool empty() const { return numPts() == 0; }
+  bool empty() const { return std::find(bits.begin(), bits.end(), (uint8_t)1) == bits.end(); }
   Box minBox() const {
     Box r;
     bool first = true;

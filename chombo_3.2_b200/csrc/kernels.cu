@@ -8,6 +8,7 @@
 #include <stdexcept>
 
 #include "kernels.H"
+#include "synthdev.H"
 #include "plan.H"
 #include "synthetic.H"
 
@@ -1159,24 +1160,6 @@ template void convert<double, float>(double*, const float*, int64_t, cudaStream_
 // of finalizeCoefficients (resetLambda with SUMFACES, MG coefficient
 // averages) with the host code's operation order.
 namespace {
-
-__device__ double devBumps(const cmg_synth::Bumps& B, double x, double y, double z) {
-  double v = 0.0;
-  for (int i = 0; i < 16; ++i) {
-    double dx = x - B.cx[i], dy = y - B.cy[i], dz = z - B.cz[i];
-    double r2 = dx * dx + dy * dy + dz * dz;
-    v += B.amp[i] * exp(-r2 / B.w2x2[i]);
-  }
-  return v;
-}
-
-__device__ double devModes(const cmg_synth::Modes& M, double x, double y, double z) {
-  double g = 0.0;
-  for (int m = 0; m < 8; ++m)
-    g += M.c[m] * cos(6.283185307179586 * (M.kx[m] * x + M.ky[m] * y + M.kz[m] * z) + M.ph[m]);
-  g = g / M.norm;
-  return exp(2.302585092994046 * g);
-}
 
 __global__ void k_fill_cells(const BoxDesc* boxes, const Chunk* chunks, double dx, cmg_synth::Bumps bumps,
                              cmg_synth::Modes am, double* rhs, double* a) {

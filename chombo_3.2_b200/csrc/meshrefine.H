@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "geom.H"
+#include "synthetic.H"
 
 namespace cmg {
 
@@ -47,15 +48,25 @@ class MeshRefiner {
                     int maxBoxSize, int totalBufferSize) const;
 };
 
+// Computes the grown, domain-clipped tags of one level that levelTags in
+// meshrefine.cpp computes on the host (used to move that pass to a device).
+struct LevelTagger {
+  virtual ~LevelTagger() {}
+  virtual void tags(const std::vector<Box>& grids, const Box& domain, double dx, const cmg_synth::Bumps& bumps,
+                    double thresh, CellSet& out) = 0;
+};
+
 // The example drivers' hierarchy (oracle/driver.cpp, after
 // releasedExamples/AMRPoisson/execCell/poissonSolve.cpp:296-317 and
 // execVariableCoefficient/VClocalFuncs.cpp:398-480): base level by
 // domainSplit of [0, n0-1]^3, then passes that tag |rhs| > thresh*max|rhs|
 // (seeded Gaussian bumps) on every level, grow the tags by one cell and
 // regrid with buffer 2, one new level per pass, up to numLevels levels.
-// Returns the sorted box list of every level.
+// Returns the sorted box list of every level.  The tags of a level whose
+// grids did not change since the previous pass are reused.  tagger, when
+// given, computes the tags instead of the host.
 std::vector<std::vector<Box>> syntheticHierarchy(int n0, int numLevels, int maxBox, int blockFactor, double fillRatio,
-                                                 uint64_t seed, double thresh);
+                                                 uint64_t seed, double thresh, LevelTagger* tagger = nullptr);
 
 }  // namespace cmg
 

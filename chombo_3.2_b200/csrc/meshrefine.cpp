@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <stdexcept>
 #include <thread>
 
@@ -115,16 +116,49 @@ Box minBoxOf(const IV* begin, const IV* end) {
   return r;
 }
 
+template <class F>
+void parallelFor(size_t n, F fn) {
+  unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; ++t)
+    th.emplace_back([&, t]() {
+      for (size_t i = t; i < n; i += nt) fn(i);
+    });
+  for (auto& x : th) x.join();
+}
+
+// Coarse cells of cdom that contain a member of s.  Planes of coarse cells
+// are independent (each takes r fine planes), so they run on host threads;
+// rows of fine cells are skipped eight bytes at a time while they are empty.
 CellSet coarsenSet(const CellSet& s, int r, const Box& cdom) {
   CellSet c(cdom, false);
   const Box& d = s.dom;
-  for (int k = d.lo[2]; k <= d.hi[2]; ++k)
-    for (int j = d.lo[1]; j <= d.hi[1]; ++j)
-      for (int i = d.lo[0]; i <= d.hi[0]; ++i)
-        if (s.bits[s.at(IV(i, j, k))]) {
-          IV q(floordiv(i, r), floordiv(j, r), floordiv(k, r));
-          if (cdom.contains(q)) c.bits[c.at(q)] = 1;
+  if (d.empty() || cdom.empty()) return c;
+  const int kc0 = floordiv(d.lo[2], r), kc1 = floordiv(d.hi[2], r);
+  const int nx = d.size(0);
+  parallelFor((size_t)(kc1 - kc0 + 1), [&](size_t t) {
+    const int kc = kc0 + (int)t;
+    for (int k = std::max(d.lo[2], kc * r); k <= std::min(d.hi[2], kc * r + r - 1); ++k)
+      for (int j = d.lo[1]; j <= d.hi[1]; ++j) {
+        const uint8_t* row = &s.bits[s.at(IV(d.lo[0], j, k))];
+        int i = 0;
+        while (i < nx) {
+          if (i + 8 <= nx) {
+            uint64_t w;
+            std::memcpy(&w, row + i, 8);
+            if (w == 0) {
+              i += 8;
+              continue;
+            }
+          }
+          if (row[i]) {
+            IV q(floordiv(d.lo[0] + i, r), floordiv(j, r), kc);
+            if (cdom.contains(q)) c.bits[c.at(q)] = 1;
+          }
+          ++i;
         }
+      }
+  });
   return c;
 }
 
@@ -300,16 +334,6 @@ int MeshRefiner::regrid(std::vector<std::vector<Box>>& newMeshes, std::vector<Ce
 
 namespace {
 
-template <class F>
-void parallelFor(size_t n, F fn) {
-  unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> th;
-  for (unsigned t = 0; t < nt; ++t)
-    th.emplace_back([&, t]() {
-      for (size_t i = t; i < n; i += nt) fn(i);
-    });
-  for (auto& x : th) x.join();
-}
 
 // Tags of one level, grown by one cell and clipped to the level's domain:
 // cells of `grids` with |rhs| > thresh * max|rhs| (oracle/driver.cpp, after
@@ -350,7 +374,7 @@ CellSet levelTags(const std::vector<Box>& grids, const Box& domain, double dx, c
 }  // namespace
 
 std::vector<std::vector<Box>> syntheticHierarchy(int n0, int numLevels, int maxBox, int blockFactor, double fillRatio,
-                                                 uint64_t seed, double thresh) {
+                                                 uint64_t seed, double thresh, LevelTagger* tagger) {
   if (n0 < 1 || numLevels < 1) throw std::invalid_argument("cmg: invalid hierarchy parameters");
   cmg_synth::Problem prob(seed);
   std::vector<Box> domains(numLevels);
@@ -368,12 +392,26 @@ std::vector<std::vector<Box>> syntheticHierarchy(int n0, int numLevels, int maxB
   if (numLevels > 1) {
     MeshRefiner refiner(domains[0], std::vector<int>(std::max(numLevels, 2), 2), fillRatio, blockFactor, 2, maxBox);
     bool more = true;
+    std::vector<CellSet> cached(numLevels);
+    std::vector<std::vector<Box>> cachedGrids(numLevels);
+    std::vector<char> haveCache(numLevels, 0);
     while (more) {
       more = false;
       const int oldTop = topLevel;
-      std::vector<CellSet> tags(topLevel + 1);
-      for (int l = 0; l <= topLevel; ++l) tags[l] = levelTags(grids[l], domains[l], dxs[l], prob.bumps, thresh);
-      int newFinest = refiner.regrid(newBoxes, tags, 0, topLevel, oldBoxes);
+      for (int l = 0; l <= topLevel; ++l) {
+        if (!haveCache[l] || !(cachedGrids[l] == grids[l])) {
+          if (tagger)
+            tagger->tags(grids[l], domains[l], dxs[l], prob.bumps, thresh, cached[l]);
+          else
+            cached[l] = levelTags(grids[l], domains[l], dxs[l], prob.bumps, thresh);
+          cachedGrids[l] = grids[l];
+          haveCache[l] = 1;
+        }
+      }
+      // regrid reads levels 0..topLevel and only clips each tag set to its
+      // level's domain, which these sets already are: the cache is passed
+      // as it is.
+      int newFinest = refiner.regrid(newBoxes, cached, 0, topLevel, oldBoxes);
       if (newFinest > topLevel) topLevel++;
       oldBoxes = newBoxes;
       oldBoxes.resize(std::max<size_t>(oldBoxes.size(), numLevels));

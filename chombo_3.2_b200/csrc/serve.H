@@ -28,6 +28,7 @@ struct Request {
   double alpha = 0.0, beta = 1.0;
   SolveParams params;
   bool mixed = true, graphs = true;
+  bool deviceTags = false;  // tagging pass of the grid generation on the device (tagging.H)
 };
 
 struct RequestResult {

@@ -12,6 +12,7 @@
 
 #include "meshrefine.H"
 #include "synthfill.H"
+#include "tagging.H"
 
 namespace cmg {
 
@@ -86,8 +87,15 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
       cudaStream_t s = nullptr;
       try {
         const Clock::time_point ts = Clock::now();
-        std::vector<std::vector<Box>> boxes =
-            syntheticHierarchy(q.n0, q.levels, q.maxBox, q.blockFactor, q.fillRatio, q.seed, q.thresh);
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+          throw std::runtime_error("cmg: stream");
+        std::vector<std::vector<Box>> boxes;
+        if (q.deviceTags) {
+          DeviceTagger tagger(s);
+          boxes = syntheticHierarchy(q.n0, q.levels, q.maxBox, q.blockFactor, q.fillRatio, q.seed, q.thresh, &tagger);
+        } else {
+          boxes = syntheticHierarchy(q.n0, q.levels, q.maxBox, q.blockFactor, q.fillRatio, q.seed, q.thresh);
+        }
         r.gridSeconds = std::chrono::duration<double>(Clock::now() - ts).count();
         est = (double)estimateDeviceBytes(boxes, q.op == 1, q.mixed);
         {
@@ -97,8 +105,6 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
           reserved = true;
         }
         r.admitted = since(Clock::now());
-        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
-          throw std::runtime_error("cmg: stream");
         HierarchyDesc d;
         d.domain = Box(IV(0, 0, 0), IV(q.n0 - 1, q.n0 - 1, q.n0 - 1));
         d.dx0 = 1.0 / q.n0;

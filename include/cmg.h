@@ -181,6 +181,15 @@ int cmg_layout_coarse_fine_plan(const cmg_box* fine, int nfine, const cmg_box* c
  * their total. */
 int cmg_synthetic_hierarchy(int n0, int nlevels, int max_box, int block_factor, double fill_ratio, uint64_t seed,
                             double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes, int cap, int* ntotal);
+/* The same hierarchy with the tagging pass of every level (|rhs| at every
+ * cell, max-reduction, threshold, one-cell growth; VClocalFuncs.cpp:586-624)
+ * run on the current CUDA device; Berger-Rigoutsos stays on the host.  The
+ * right-hand side is evaluated with the CUDA math library, whose exp differs
+ * from the host's in the last bit at most, so a cell within a few ulps of the
+ * threshold could be tagged differently from cmg_synthetic_hierarchy. */
+int cmg_synthetic_hierarchy_device(int n0, int nlevels, int max_box, int block_factor, double fill_ratio,
+                                   uint64_t seed, double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes,
+                                   int cap, int* ntotal);
 
 /* Batching and serving (no counterpart in the reference, which solves one
  * hierarchy per call).  A request is a seeded synthetic problem: the
@@ -204,6 +213,7 @@ typedef struct cmg_request {
   double alpha, beta;
   cmg_solve_params params;
   int mixed, graphs;
+  int device_tags; /* != 0: tag on the device (cmg_synthetic_hierarchy_device) */
 } cmg_request;
 
 typedef struct cmg_request_result {

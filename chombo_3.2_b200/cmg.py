@@ -31,6 +31,18 @@ class SolveParams(ctypes.Structure):
                 ("eps", ctypes.c_double), ("hang", ctypes.c_double), ("norm_thresh", ctypes.c_double)]
 
 
+class MLSolveParams(ctypes.Structure):
+    _fields_ = [("mg_iters", ctypes.c_int), ("mg_smooth", ctypes.c_int), ("imax", ctypes.c_int),
+                ("num_restarts", ctypes.c_int), ("eps", ctypes.c_double), ("reps", ctypes.c_double),
+                ("hang", ctypes.c_double), ("small", ctypes.c_double)]
+
+
+def mlsolve_params(mg_iters=1, mg_smooth=4, imax=80, num_restarts=5, eps=1e-6, reps=1e-12, hang=1e-8, small=1e-30):
+    """Parameters of cmg_solve_multilevel_bicgstab; defaults are the reference's MultilevelLinearOp and
+    BiCGStabSolver defaults."""
+    return MLSolveParams(mg_iters, mg_smooth, imax, num_restarts, eps, reps, hang, small)
+
+
 def solve_params(pre=4, post=4, bottom=4, num_mg=1, iter_max=100, imin=5, eps=1e-10, hang=1e-10,
                  norm_thresh=1e-30):
     return SolveParams(pre, post, bottom, num_mg, iter_max, imin, eps, hang, norm_thresh)
@@ -255,6 +267,18 @@ class Hierarchy:
         _check(fn(self.h, ctypes.byref(p), int(zero_phi), ctypes.byref(st), ctypes.byref(it),
                   _ptr(hist), len(hist), ctypes.byref(hl)))
         return {"exit_status": st.value, "iterations": it.value, "history": hist[:hl.value].copy()}
+
+    def solve_bicgstab(self, params=None, zero_phi=True):
+        """BiCGStab over MultilevelLinearOp preconditioned by AMR multigrid (cmg_solve_multilevel_bicgstab)."""
+        p = params or mlsolve_params()
+        hist = np.zeros(p.imax + 1, dtype=np.float64)
+        st, it, hl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        r0, rf = ctypes.c_double(), ctypes.c_double()
+        _check(lib().cmg_solve_multilevel_bicgstab(self.h, ctypes.byref(p), int(zero_phi), ctypes.byref(st),
+                                                   ctypes.byref(it), ctypes.byref(r0), ctypes.byref(rf), _ptr(hist),
+                                                   len(hist), ctypes.byref(hl)))
+        return {"exit_status": st.value, "iterations": it.value, "initial_residual": r0.value,
+                "final_residual": rf.value, "history": hist[:hl.value].copy()}
 
     def set_relax_mode(self, mode):
         _check(lib().cmg_set_relax_mode(self.h, int(mode)))

@@ -317,6 +317,33 @@ int cmg_solve_mixed(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, i
   return solveWith(h, p, zero_phi, exit_status, iterations, history, history_cap, history_len, true);
 }
 
+int cmg_solve_multilevel_bicgstab(cmg_hierarchy* h, const cmg_mlsolve_params* p, int zero_phi, int* exit_status,
+                                  int* iterations, double* initial_residual, double* final_residual, double* history,
+                                  int history_cap, int* history_len) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (!p) throw std::invalid_argument("cmg: null parameters");
+    cmg::MLSolveParams mp;
+    mp.mgIters = p->mg_iters;
+    mp.mgSmooth = p->mg_smooth;
+    mp.imax = p->imax;
+    mp.numRestarts = p->num_restarts;
+    mp.eps = p->eps;
+    mp.reps = p->reps;
+    mp.hang = p->hang;
+    mp.small = p->small;
+    cmg::MLSolveResult r = h->solver->solveMultilevelBiCGStab(mp, zero_phi != 0);
+    if (exit_status) *exit_status = r.exitStatus;
+    if (iterations) *iterations = r.iterations;
+    if (initial_residual) *initial_residual = r.initialResidual;
+    if (final_residual) *final_residual = r.finalResidual;
+    const int n = (int)r.history.size();
+    if (history_len) *history_len = n;
+    if (history)
+      for (int i = 0; i < n && i < history_cap; ++i) history[i] = r.history[i];
+  });
+}
+
 int cmg_residual_norm(cmg_hierarchy* h, double* out) {
   return guard([&]() {
     needLevel(h, 0);

@@ -73,6 +73,11 @@ struct Coef {
 // colour par (the only ones a pass over colour 1 - par reads).
 template <class T> void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par = -1);
 template <class T> void zeroCovered(const LevelDev& L, T* f, cudaStream_t s);
+// x *= scale over a whole level array.
+void scaleField(double* x, double scale, int64_t n, cudaStream_t s);
+// out[b] = sum of x*y over the valid cells of box b, accumulated in the
+// reference's order (FArrayBox::dotProduct: k, j, i with i fastest).
+void boxDots(const LevelDev& L, const double* x, const double* y, double* out, cudaStream_t s);
 // One colour pass of levelGSRB.  inlineGhosts: the neighbours beyond each
 // box come from the level's face-ghost rules, so no ghost fill is needed
 // before the pass; otherwise they are read from ghost cells filled by

@@ -383,6 +383,34 @@ __global__ void k_negadd_flat(T* r, const T* lofphi, const T* rhs, int64_t n) {
 }
 inline int flatBlocks(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 16); }
 
+// x *= s over a whole level array (LevelDataOps::scale -> FArrayBox::mult).
+__global__ void k_scale_flat(double* x, double s, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    x[q] = x[q] * s;
+}
+
+// Per-box dot products in the reference's order: FArrayBox::dotProduct
+// (BoxTools/FArrayBox.cpp:260-280) accumulates x*y over the valid box k, j, i
+// with i fastest into one running sum, so one thread walks each box; the sum
+// over boxes and levels is left to the caller (LevelDataOps::dotProduct,
+// MultilevelLinearOp::dotProduct).
+__global__ void k_box_dot(const BoxDesc* boxes, int nbox, const double* __restrict__ x,
+                          const double* __restrict__ y, double* out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbox) return;
+  const BoxDesc bd = boxes[b];
+  double s = 0.0;
+  for (int k = bd.lo[2]; k <= bd.hi[2]; ++k)
+    for (int j = bd.lo[1]; j <= bd.hi[1]; ++j) {
+#pragma unroll 4
+      for (int i = bd.lo[0]; i <= bd.hi[0]; ++i) {
+        const int64_t c = cellIndex(bd, i, j, k);
+        s += x[c] * y[c];
+      }
+    }
+  out[b] = s;
+}
+
 // dst = src over whole arrays (ghosts included), converting the type.
 template <class D, class S>
 __global__ void k_convert(D* dst, const S* src, int64_t n) {
@@ -933,6 +961,18 @@ void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par) {
                                                                                        c1, c2, flin);
   }
   CMG_LAUNCHED("ghostFill");
+}
+
+void scaleField(double* x, double scale, int64_t n, cudaStream_t s) {
+  if (n == 0) return;
+  k_scale_flat<<<flatBlocks(n), 256, 0, s>>>(x, scale, n);
+  CMG_LAUNCHED("scale");
+}
+
+void boxDots(const LevelDev& L, const double* x, const double* y, double* out, cudaStream_t s) {
+  if (L.nbox == 0) return;
+  k_box_dot<<<(L.nbox + 63) / 64, 64, 0, s>>>(L.boxes, L.nbox, x, y, out);
+  CMG_LAUNCHED("boxDots");
 }
 
 template <class T>

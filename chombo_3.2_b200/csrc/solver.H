@@ -34,6 +34,22 @@ struct SolveResult {
   std::vector<double> history;  // composite max-norm residual, start of each iteration, then final
 };
 
+// BiCGStab over the whole hierarchy preconditioned by AMR multigrid, as the
+// variable-coefficient example solves (BiCGStabSolver<Vector<LevelData*>>
+// over MultilevelLinearOp, VCPoissonSolve.cpp:146-183).  Defaults are the
+// reference's: MultilevelLinearOp (mgIters 1, mgSmooth 4), BiCGStabSolver
+// (imax 80, eps 1e-6, reps 1e-12, hang 1e-8, small 1e-30, 5 restarts) with
+// the example's max norm.
+struct MLSolveParams {
+  int mgIters = 1, mgSmooth = 4, imax = 80, numRestarts = 5;
+  double eps = 1e-6, reps = 1e-12, hang = 1e-8, small = 1e-30;
+};
+struct MLSolveResult {
+  int exitStatus = 0, iterations = 0;  // BiCGStabSolver::m_exitStatus (1 converged, 2 rho = 0, 3 stalled), m_iter
+  double initialResidual = 0, finalResidual = 0;
+  std::vector<double> history;  // residual norm after each iteration
+};
+
 // Device allocation owned by the solver, stream-ordered (cudaMallocAsync /
 // cudaFreeAsync on the solver's stream), so that hierarchies created and
 // destroyed while others solve on their own streams never synchronise the
@@ -73,6 +89,9 @@ class Solver {
   // generator's, which the oracle reproduces bit for bit).
   void fillSyntheticDevice(uint64_t seed);
   SolveResult solve(const SolveParams& p, bool zeroPhi = true);
+  // BiCGStab over MultilevelLinearOp (see MLSolveParams) from the current
+  // phi, or from zero (ghost cells included) when zeroPhi.
+  MLSolveResult solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroPhi = true);
   // One composite residual evaluation (AMRMultiGrid::computeAMRResidual).
   double residualNorm();
   // The same evaluation with the max-norm reduced through `scratch`, a
@@ -179,6 +198,22 @@ class Solver {
   template <class T> void copyField(const LevelDev& L, T* dst, const T* src);
   void ensure32();
   float* allocF(size_t n);
+  // MultilevelLinearOp on device vectors (one array per AMR level).
+  using MLVec = std::vector<double*>;
+  std::vector<MLVec> mlVecs_;    // r, r_tilde, e, p, p_tilde, s_tilde, t, v, and two scratch vectors
+  double* dBoxSums_ = nullptr;   // one per box of every level
+  double* hostBoxSums_ = nullptr;
+  MLVec mlVec(int i);
+  void mlZero(MLVec& x);
+  void mlAssign(MLVec& dst, const MLVec& src);
+  void mlIncr(MLVec& y, const MLVec& x, double scale);
+  void mlScale(MLVec& x, double scale);
+  void mlResidual(MLVec& lhs, MLVec& phi, MLVec& rhs);
+  void mlApplyOp(MLVec& lhs, MLVec& phi);
+  double mlNorm(const MLVec& x);
+  double mlDot(const MLVec& x, const MLVec& y);
+  void mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p);
+  void amrOperatorLevel(int ilev, int lmax, MLVec& lhs, MLVec& phi);
   void scatterValid(const LevelPlan& p, const LevelDev& d, double* dev, const double* src, bool onDevice,
                     int faceDir);
   void gatherValid(const LevelPlan& p, const LevelDev& d, const double* dev, double* dst, bool onDevice);

@@ -309,6 +309,7 @@ Solver::~Solver() {
   cudaStreamSynchronize(s_);
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
   if (hostScalars_) cudaFreeHost(hostScalars_);
+  if (hostBoxSums_) cudaFreeHost(hostBoxSums_);
 }
 
 int64_t Solver::numFaces(int l, int dir) const {
@@ -905,6 +906,286 @@ void Solver::amrVCycle(int ilev, int lmax) {
 
 template void Solver::amrVCycle<double>(int, int);
 template void Solver::amrVCycle<float>(int, int);
+
+// ------------------------------------------------ BiCGStab over MultilevelLinearOp
+// BiCGStabSolver<Vector<LevelData<FArrayBox>*>>::solve (BiCGStabSolver.H:199-515)
+// over MultilevelLinearOp<FArrayBox> (MultilevelLinearOpI.H), the solve path of
+// the variable-coefficient example.  Vectors are one device array per AMR
+// level in the level's ghosted layout; the scalars (rho, alpha, beta, omega,
+// norms) live on the host as in the reference, each dot product and norm read
+// back once.
+
+Solver::MLVec Solver::mlVec(int i) {
+  if (mlVecs_.empty()) {
+    const int nlev = numLevels();
+    mlVecs_.assign(10, MLVec(nlev, nullptr));
+    for (auto& v : mlVecs_)
+      for (int l = 0; l < nlev; ++l) v[l] = alloc(amr_[l].nelem);
+    size_t nb = 0;
+    for (const LevelDev& L : amrDev_) nb += (size_t)L.nbox;
+    dBoxSums_ = alloc(std::max<size_t>(nb, 1));
+    ck(cudaMallocHost((void**)&hostBoxSums_, std::max<size_t>(nb, 1) * sizeof(double)), "pinned box sums");
+  }
+  return mlVecs_[i];
+}
+
+void Solver::mlZero(MLVec& x) {
+  for (int l = 0; l < numLevels(); ++l) zeroField(amrDev_[l], x[l]);
+}
+void Solver::mlAssign(MLVec& dst, const MLVec& src) {
+  for (int l = 0; l < numLevels(); ++l) copyField(amrDev_[l], dst[l], src[l]);
+}
+void Solver::mlIncr(MLVec& y, const MLVec& x, double scale) {
+  for (int l = 0; l < numLevels(); ++l) incr(amrDev_[l], y[l], x[l], scale, s_);
+}
+void Solver::mlScale(MLVec& x, double scale) {
+  for (int l = 0; l < numLevels(); ++l) scaleField(x[l], scale, amrDev_[l].nelem, s_);
+}
+
+// MultilevelLinearOp::residual: AMRResidual(NC/NF) or residual per level, in
+// level order.  The homogeneous and inhomogeneous physical boundary
+// conditions coincide for these zero-value Dirichlet faces.
+void Solver::mlResidual(MLVec& lhs, MLVec& phi, MLVec& rhs) {
+  const int lmax = numLevels() - 1;
+  for (int l = 0; l <= lmax; ++l) amrResidualLevel<double>(l, lmax, lhs, phi, rhs);
+}
+
+// AMROperator / AMROperatorNC / AMROperatorNF / applyOp of one level
+// (AMRPoissonOp.cpp:332-340, 790-858): coarse-fine interpolation from the
+// coarser level, exchange and boundary values, the operator, and the
+// flux-register correction from the finer level.
+void Solver::amrOperatorLevel(int ilev, int lmax, MLVec& lhs, MLVec& phi) {
+  const LevelDev& L = amrDev_[ilev];
+  Coef<double> c = coefA<double>(ilev);
+  if (ilev > 0) quadCF(L, phi[ilev], phi[ilev - 1], s_);
+  fill(L, phi[ilev], false);
+  timed(P_OP, amr_[ilev].grids.numCells() * 8.0 * (desc_.vc ? 6.0 : 2.0), [&]() { applyOp(L, lhs[ilev], phi[ilev], c, s_); });
+  if (ilev < lmax) {
+    quadCF(amrDev_[ilev + 1], phi[ilev + 1], phi[ilev], s_);
+    reflux(L, lhs[ilev], phi[ilev], phi[ilev + 1], c, coefA<double>(ilev + 1), s_);
+  }
+}
+
+void Solver::mlApplyOp(MLVec& lhs, MLVec& phi) {
+  const int lmax = numLevels() - 1;
+  for (int l = 0; l <= lmax; ++l) amrOperatorLevel(l, lmax, lhs, phi);
+}
+
+// MultilevelLinearOp::norm with order 0: the largest AMRNorm over the
+// levels, each the max-norm of the level with the cells under the next finer
+// level zeroed.
+double Solver::mlNorm(const MLVec& x) {
+  const int lmax = numLevels() - 1;
+  MLVec tmp = mlVec(8);
+  ck(cudaMemsetAsync(dNorm_, 0, sizeof(double), s_), "norm reset");
+  for (int l = 0; l <= lmax; ++l) {
+    const double* src = x[l];
+    if (l < lmax) {
+      copyField(amrDev_[l], tmp[l], x[l]);
+      zeroCovered(amrDev_[l], tmp[l], s_);
+      src = tmp[l];
+    }
+    maxNorm(amrDev_[l], src, dNorm_, s_);
+  }
+  return readNorm();
+}
+
+// MultilevelLinearOp::dotProduct: copies with the covered cells zeroed, per
+// level LevelDataOps::dotProduct (box dot products summed in box order), each
+// level scaled by dx^3 and summed coarse to fine.
+double Solver::mlDot(const MLVec& x, const MLVec& y) {
+  const int lmax = numLevels() - 1;
+  MLVec ta = mlVec(8), tb = mlVec(9);
+  int off = 0;
+  for (int l = 0; l <= lmax; ++l) {
+    const LevelDev& L = amrDev_[l];
+    const double* a = x[l];
+    const double* b = y[l];
+    if (l < lmax) {
+      copyField(L, ta[l], x[l]);
+      zeroCovered(L, ta[l], s_);
+      a = ta[l];
+      if (y[l] == x[l]) {
+        b = a;
+      } else {
+        copyField(L, tb[l], y[l]);
+        zeroCovered(L, tb[l], s_);
+        b = tb[l];
+      }
+    }
+    boxDots(L, a, b, dBoxSums_ + off, s_);
+    off += L.nbox;
+  }
+  ck(cudaMemcpyAsync(hostBoxSums_, dBoxSums_, std::max(off, 1) * sizeof(double), cudaMemcpyDeviceToHost, s_),
+     "box sums d2h");
+  ck(cudaStreamSynchronize(s_), "box sums sync");
+  double prod = 0.0;
+  off = 0;
+  for (int l = 0; l <= lmax; ++l) {
+    double val = 0.0;
+    for (int b = 0; b < amrDev_[l].nbox; ++b) val += hostBoxSums_[off + b];
+    off += amrDev_[l].nbox;
+    const double dx = amr_[l].dx;
+    const double scale = dx * dx * dx;
+    val *= scale;
+    prod += val;
+  }
+  return prod;
+}
+
+// MultilevelLinearOp::preCond with the multigrid preconditioner: mgIters
+// times, the homogeneous residual of the current correction, one AMR
+// V-cycle from a zero correction (AMRMultiGrid::AMRVCycle on the
+// preconditioner's own scratch), and the increment.
+void Solver::mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p) {
+  const int lmax = numLevels() - 1;
+  MLVec ures(lmax + 1), ucorr(lmax + 1);
+  for (int l = 0; l <= lmax; ++l) {
+    ures[l] = lev_[l].ures;
+    ucorr[l] = lev_[l].ucorr;
+  }
+  for (int it = 0; it < p.mgIters; ++it) {
+    mlResidual(ures, cor, res);
+    mlZero(ucorr);
+    amrVCycle<double>(lmax, lmax);
+    mlIncr(cor, ucorr, 1.0);
+  }
+}
+
+MLSolveResult Solver::solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroPhi) {
+  if (p.mgIters < 0 || p.mgSmooth < 0 || p.imax < 0 || p.numRestarts < 0)
+    throw std::invalid_argument("cmg: invalid BiCGStab parameters");
+  if (!tuned_) tuneRelaxation();
+  const int lmax = numLevels() - 1;
+  // The preconditioner's AMRMultiGrid (MultilevelLinearOp::define): pre,
+  // post and bottom smoothings m_num_mg_smooth, one V-cycle per call, and a
+  // default BiCGStabSolver at the bottom (eps 1e-6, no convergence metric:
+  // AMRVCycle is called directly, so setConvergenceMetrics never runs).
+  const SolveParams saved = sp_;
+  sp_ = SolveParams();
+  sp_.pre = sp_.post = sp_.bottom = p.mgSmooth;
+  sp_.numMG = 1;
+  sp_.eps = 1e-6;
+  hostScalars_[1] = -1.0;
+  ck(cudaMemcpyAsync(dMetric_, &hostScalars_[1], sizeof(double), cudaMemcpyHostToDevice, s_), "metric");
+  MLVec phi(lmax + 1), rhs(lmax + 1);
+  for (int l = 0; l <= lmax; ++l) {
+    phi[l] = lev_[l].phi;
+    rhs[l] = lev_[l].rhs;
+  }
+  if (zeroPhi) mlZero(phi);
+  MLVec r = mlVec(0), rt = mlVec(1), e = mlVec(2), pv = mlVec(3), pt = mlVec(4), st = mlVec(5), t = mlVec(6),
+        v = mlVec(7);
+  MLSolveResult out;
+  out.exitStatus = -1;
+  int recount = 0;
+  mlZero(r);
+  mlResidual(r, phi, rhs);
+  mlAssign(rt, r);
+  mlZero(e);
+  mlZero(pt);
+  mlZero(st);
+  int iter = 0;
+  double rho[4] = {0, 0, 0, 0};
+  double norm[2];
+  norm[0] = mlNorm(r);
+  const double initial_norm = norm[0];
+  out.initialResidual = norm[0];
+  out.finalResidual = norm[0];
+  norm[1] = norm[0];
+  double alpha[2] = {0, 0}, beta[2] = {0, 0}, omega[2] = {0, 0};
+  bool init = true;
+  int restarts = 0;
+  while ((iter < p.imax && norm[0] > p.eps * norm[1]) && (norm[1] > 0)) {
+    iter++;
+    norm[1] = norm[0];
+    alpha[1] = alpha[0];
+    beta[1] = beta[0];
+    omega[1] = omega[0];
+    rho[3] = rho[2];
+    rho[2] = rho[1];
+    rho[1] = mlDot(rt, r);
+    if (rho[1] == 0.0) {
+      mlIncr(phi, e, 1.0);
+      out.finalResidual = norm[0];
+      out.exitStatus = 2;
+      out.iterations = iter;
+      sp_ = saved;
+      return out;
+    }
+    if (init) {
+      mlAssign(pv, r);
+      init = false;
+    } else {
+      beta[1] = (rho[1] / rho[2]) * (alpha[1] / omega[1]);
+      mlScale(pv, beta[1]);
+      mlIncr(pv, v, -beta[1] * omega[1]);
+      mlIncr(pv, r, 1.0);
+    }
+    mlPreCond(pt, pv, p);
+    mlZero(v);
+    mlApplyOp(v, pt);
+    const double m = mlDot(rt, v);
+    alpha[0] = rho[1] / m;
+    if (std::fabs(m) > p.small * std::fabs(rho[1])) {
+      mlIncr(r, v, -alpha[0]);
+      norm[0] = mlNorm(r);
+      mlIncr(e, pt, alpha[0]);
+    } else {
+      mlZero(r);
+      norm[0] = 0.0;
+    }
+    out.finalResidual = norm[0];
+    if (norm[0] > p.eps * initial_norm && norm[0] > p.reps * out.initialResidual) {
+      mlPreCond(st, r, p);
+      mlZero(t);
+      mlApplyOp(t, st);
+      const double tr = mlDot(t, r);
+      const double tt = mlDot(t, t);
+      omega[0] = tr / tt;
+      mlIncr(e, st, omega[0]);
+      mlIncr(r, t, -omega[0]);
+      norm[0] = mlNorm(r);
+    }
+    out.finalResidual = norm[0];
+    out.history.push_back(norm[0]);
+    if (norm[0] <= p.eps * initial_norm || norm[0] <= p.reps * out.initialResidual) {
+      out.exitStatus = 1;
+      break;
+    }
+    if (omega[0] == 0.0 || norm[0] > (1 - p.hang) * norm[1]) {
+      if (recount == 0) {
+        recount = 1;
+      } else {
+        recount = 0;
+        mlIncr(phi, e, 1.0);
+        if (restarts == p.numRestarts) {
+          out.exitStatus = 3;
+          out.iterations = iter;
+          sp_ = saved;
+          return out;
+        }
+        mlResidual(r, phi, rhs);
+        norm[0] = mlNorm(r);
+        rho[1] = 0.0;
+        rho[2] = 0.0;
+        rho[3] = 0.0;
+        alpha[0] = 0;
+        beta[0] = 0;
+        omega[0] = 0;
+        mlAssign(rt, r);
+        mlZero(e);
+        restarts++;
+        init = true;
+      }
+    }
+  }
+  out.iterations = iter;
+  mlIncr(phi, e, 1.0);
+  ck(cudaStreamSynchronize(s_), "bicgstab sync");
+  sp_ = saved;
+  return out;
+}
 
 double Solver::residualNorm() {
   int lmax = numLevels() - 1;

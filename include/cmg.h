@@ -123,6 +123,27 @@ int cmg_solve_mixed(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, i
 /* AMRMultiGrid::computeAMRResidual(phi, rhs, lmax, 0) (AMRMultiGrid.H:738-750). */
 int cmg_residual_norm(cmg_hierarchy* h, double* out);
 
+/* BiCGStab over the whole hierarchy, preconditioned by AMR multigrid: the
+ * solve path of the reference's variable-coefficient example
+ * (BiCGStabSolver<Vector<LevelData<FArrayBox>*>>::solve, BiCGStabSolver.H:
+ * 199-515, over MultilevelLinearOp<FArrayBox>, MultilevelLinearOpI.H, set up
+ * as VCPoissonSolve.cpp:146-183 with the max norm).  Each preconditioner call
+ * runs mg_iters rounds of (homogeneous residual, one AMR V-cycle with
+ * mg_smooth pre, post and bottom smoothings from a zero correction,
+ * increment); dot products follow the reference's summation order (each box
+ * in k, j, i order, boxes in layout order, levels scaled by dx^3 and summed
+ * coarse to fine).  exit_status is the solver's m_exitStatus (1 converged,
+ * 2 rho = 0, 3 stalled after num_restarts restarts, -1 iteration limit),
+ * iterations its m_iter; history receives the residual norm after every
+ * iteration.  Starts from phi as it is, or from zero when zero_phi != 0. */
+typedef struct cmg_mlsolve_params {
+  int mg_iters, mg_smooth, imax, num_restarts;
+  double eps, reps, hang, small;
+} cmg_mlsolve_params;
+int cmg_solve_multilevel_bicgstab(cmg_hierarchy* h, const cmg_mlsolve_params* p, int zero_phi, int* exit_status,
+                                  int* iterations, double* initial_residual, double* final_residual, double* history,
+                                  int history_cap, int* history_len);
+
 /* Same value as cmg_residual_norm, allocating no memory on success (no
  * counterpart in the reference, which has no such constraint).  For callers
  * that cannot let the library allocate at call time: a process whose memory

@@ -60,3 +60,26 @@ def test_reference_amrtools_test_passes(test):
         pytest.skip("reference tests not built (make -C oracle reftests)")
     r = subprocess.run([exe], capture_output=True, timeout=600, cwd=REFTESTS)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+
+
+MLORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle_mlbicgstab")
+
+
+@pytest.mark.skipif(not os.path.exists(MLORACLE), reason="oracle not built (needs the reference tree)")
+@pytest.mark.parametrize("name", ["bicgstab_poisson_1lev_32", "bicgstab_vc_3lev_16"])
+def test_bicgstab_oracle_reproduces_golden(tmp_path, name):
+    """The reference's BiCGStab over MultilevelLinearOp reproduces its fixture bit for bit."""
+    meta, arrays = golden(name)
+    base, _ = golden(meta["base"])
+    out = str(tmp_path / name)
+    subprocess.run([MLORACLE] + base["args"].split() + meta["solver_args"].split() + ["out=" + out], check=True,
+                   capture_output=True, timeout=300)
+    got = json.load(open(out + ".json"))
+    for k in ("exit_status", "iterations", "initial_residual", "final_residual"):
+        assert got[k] == meta[k], k
+    raw = np.fromfile(out + ".bin", dtype=np.float64)
+    pos = 0
+    for lev, boxes in enumerate(base["boxes"]):
+        n = sum((b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1) for b in boxes)
+        assert np.array_equal(raw[pos:pos + n][::meta["sample_stride"]], arrays[f"phi{lev}"])
+        pos += n

@@ -28,6 +28,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 ORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle")
+MLORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle_mlbicgstab")
 PROFILE_CLASSES = ["relax_finest", "residual_op", "ghost_fill", "bottom", "relax_other"]
 METRIC = "Poisson solves/s & p50/p99 latency at 1e-10 rel. residual; V-cycle HBM GB/s"
 WORKLOADS = {
@@ -47,6 +48,14 @@ WORKLOADS = {
         "golden": "config2_vc_3lev_256",
         "name": "3-level VC Helmholtz (VCAMRPoissonOp2 alpha=1 beta=-1), base 256^3, ratio 2, block 8, "
                 "max box 32, fill 0.75, Dirichlet, GSRB 4+4, BiCGStab bottom, rel. residual 1e-10; plain FP64",
+    },
+    "config1-bicgstab": {
+        "golden": "config1_vc_3lev_128",
+        "solver": "bicgstab",
+        "bicgstab": {"mg_iters": 2, "mg_smooth": 4, "eps": 1e-10, "imax": 100},
+        "name": "3-level VC Helmholtz, base 128^3 (as config1), solved as the variable-coefficient example solves: "
+                "BiCGStab over MultilevelLinearOp preconditioned by 2 AMR V-cycles (GSRB 4+4+4), max norm, "
+                "rel. residual 1e-10",
     },
     "config1-mixed": {
         "golden": "config1_vc_3lev_128",
@@ -197,6 +206,28 @@ def cpu_reference(meta, processes, repeats):
             "wall_step": [max(o[k]["seconds"] for o in outs if len(o) > k) for k in range(repeats)]}
 
 
+def cpu_reference_bicgstab(meta, wl, processes):
+    """The reference's BiCGStab over MultilevelLinearOp (oracle/_ref/cmg_oracle_mlbicgstab) on host cores:
+    `processes` concurrent single-thread solves of the workload capped at 1 and at 2 BiCGStab iterations; the
+    full solve is extrapolated as t(1) + (n - 1) (t(2) - t(1)) with n the GPU solve's iteration count."""
+    if not os.path.exists(MLORACLE):
+        return None
+    boxfile = write_boxfile(meta)
+    b = wl["bicgstab"]
+    base = [MLORACLE, f"n0={meta['n0']}", f"levels={len(meta['boxes'])}", f"maxbox={meta['maxbox']}",
+            f"block={meta['block']}", f"op={meta['op']}", f"alpha={meta['alpha']}", f"beta={meta['beta']}",
+            f"seed={meta['seed']}", f"mgiters={b['mg_iters']}", f"mgsmooth={b['mg_smooth']}", f"eps={b['eps']}",
+            f"boxfile={boxfile}"]
+    times = {}
+    for imax in (1, 2):
+        procs = [subprocess.Popen(base + [f"imax={imax}", f"out={boxfile}.{imax}.{k}"], stdout=subprocess.PIPE,
+                                  stderr=subprocess.DEVNULL, text=True) for k in range(processes)]
+        outs = [p.communicate()[0] for p in procs]
+        ts = [float(o.split("seconds=")[1].split()[0]) for o in outs if "seconds=" in o]
+        times[imax] = max(ts) if ts else float("nan")
+    return times
+
+
 def run_reference_arm(args, meta, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -208,6 +239,24 @@ def run_reference_arm(args, meta, wl):
     cores = os.cpu_count() or 1
     # each process holds ~3 GB for this workload; bound the concurrency
     procs = max(1, min(cores, 8))
+    if wl.get("solver") == "bicgstab":
+        n_iter = wl.get("reference_iterations", 8)
+        t = cpu_reference_bicgstab(meta, wl, procs)
+        if t is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cmg_oracle_mlbicgstab not built"}))
+            return
+        solve_s = t[1] + (n_iter - 1) * (t[2] - t[1])
+        value = procs / solve_s
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": 1, "warmup": 0, "ms_per_step": 1000.0 * solve_s, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["name"], "global_batch": 1, "parallelism": f"{procs} concurrent host processes"},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "reference",
+                             "sample": f"{procs} concurrent single-thread reference BiCGStab solves capped at 1 and 2 "
+                                       f"iterations, extrapolated to {n_iter} iterations"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
     res = cpu_reference(meta, procs, args.warmup + args.steps)
     timed = res["per_step"][args.warmup:]
     value = float(np.mean(timed))
@@ -418,6 +467,12 @@ def main():
     params = cmg.solve_params(pre=meta["pre"], post=meta["post"], bottom=meta["bottom"], iter_max=meta["iters"],
                               eps=meta["eps"], hang=meta["hang"])
     mixed = bool(wl.get("mixed", False))
+    bicg = wl.get("solver") == "bicgstab"
+    mlp = cmg.mlsolve_params(**wl["bicgstab"]) if bicg else None
+
+    def solve_once():
+        return h.solve_bicgstab(mlp) if bicg else h.solve(params, mixed=mixed)
+
     h.use_graphs(not args.no_graphs)
     h.set_relax_mode(args.relax_mode)
     stream = torch.cuda.ExternalStream(h.stream())
@@ -429,7 +484,7 @@ def main():
             dist.barrier()
 
     for _ in range(args.warmup):
-        out = h.solve(params, mixed=mixed)
+        out = solve_once()
     assert out["exit_status"] == meta["exit_status"], out
     n_iter = out["iterations"]
 
@@ -443,7 +498,7 @@ def main():
     with torch.cuda.stream(stream):
         ev[0].record(stream)
         for k in range(args.steps):
-            h.solve(params, mixed=mixed)
+            solve_once()
             ev[k + 1].record(stream)
     barrier()
     launches = cmg.launch_count() - launches0
@@ -459,7 +514,7 @@ def main():
     pe = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     pe[0].record(stream)
     for _ in range(n_prof):
-        h.solve(params, mixed=mixed)
+        solve_once()
     pe[1].record(stream)
     barrier()
     prof_ms = pe[0].elapsed_time(pe[1])
@@ -486,7 +541,7 @@ def main():
     for k in range(args.steps):
         for l in range(len(ncells)):
             h.set_rhs_ptr(l, host_rhs[l].data_ptr(), 0)
-        out = h.solve(params, mixed=mixed)
+        out = solve_once()
         for l in range(len(ncells)):
             h.get_phi_ptr(l, host_phi[l].data_ptr(), 0)
     e2e_ev[1].record(stream)
@@ -510,8 +565,9 @@ def main():
         traffic = t["dram_bytes_per_launch"] if t else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": "k_gsrb<double,1>: one red-black colour pass over the finest AMR level (two launches per "
-                          "sweep; the one-colour ghost fill between them is timed separately)",
+                "kernel": f"k_gsrb<{'float' if mixed else 'double'},{meta['op']}>: one red-black colour pass over "
+                          "the finest AMR level (two launches per sweep; the one-colour ghost fill between them is "
+                          "timed separately)",
                 "peak_kind": peak_kind, "launches": int(n_fine),
                 "avg_launch_us": 1000.0 * ms_fine / max(n_fine, 1),
                 "algorithmic_bytes_per_launch": bytes_fine / max(n_fine, 1)}
@@ -545,7 +601,14 @@ def main():
                     "fp64_reference_vcycles": len(meta["residual_history"]) - 1,
                     "sampled": not meta["full"]}
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and bicg:
+        t = cpu_reference_bicgstab(meta, wl, 1)
+        if t:
+            solve_s = t[1] + (n_iter - 1) * (t[2] - t[1])
+            cpu = {"value": 1.0 / solve_s, "unit": "solves/s", "cores": 1, "kind": "reference",
+                   "sample": f"one single-thread reference BiCGStab solve capped at 1 and at 2 iterations, "
+                             f"extrapolated to {n_iter} iterations"}
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         res = cpu_reference(meta, 1, 1)
         if res:
             cpu = {"value": res["per_step"][0], "unit": "solves/s", "cores": 1, "kind": "reference",
@@ -558,7 +621,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
             "config": {"workload": wl["name"], "global_batch": world, "cells": sum(ncells),
                        "levels": len(ncells), "boxes": [len(b) for b in meta["boxes"]],
-                       "vcycles_per_solve": n_iter, "l2": "working set > L2 (no flush)",
+                       ("bicgstab_iterations_per_solve" if bicg else "vcycles_per_solve"): n_iter,
+                       "l2": "working set > L2 (no flush)",
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                        "cuda_graphs": not args.no_graphs},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),

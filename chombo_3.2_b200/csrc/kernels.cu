@@ -391,24 +391,58 @@ __global__ void k_scale_flat(double* x, double s, int64_t n) {
 
 // Per-box dot products in the reference's order: FArrayBox::dotProduct
 // (BoxTools/FArrayBox.cpp:260-280) accumulates x*y over the valid box k, j, i
-// with i fastest into one running sum, so one thread walks each box; the sum
-// over boxes and levels is left to the caller (LevelDataOps::dotProduct,
+// with i fastest into one running sum.  One warp per box: the lanes load and
+// multiply a chunk of DOT_CHUNK consecutive cells (the products round the same
+// whatever computes them) into shared memory, then lane 0 adds the chunk in
+// order, so the sum is the reference's bit for bit; the sum over boxes and
+// levels is left to the caller (LevelDataOps::dotProduct,
 // MultilevelLinearOp::dotProduct).
-__global__ void k_box_dot(const BoxDesc* boxes, int nbox, const double* __restrict__ x,
-                          const double* __restrict__ y, double* out) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nbox) return;
-  const BoxDesc bd = boxes[b];
-  double s = 0.0;
-  for (int k = bd.lo[2]; k <= bd.hi[2]; ++k)
-    for (int j = bd.lo[1]; j <= bd.hi[1]; ++j) {
-#pragma unroll 4
-      for (int i = bd.lo[0]; i <= bd.hi[0]; ++i) {
+enum { DOT_CHUNK = 512, DOT_PER_LANE = DOT_CHUNK / 32 };
+__global__ void __launch_bounds__(32) k_box_dot(const BoxDesc* boxes, const double* __restrict__ x,
+                                                const double* __restrict__ y, double* out) {
+  __shared__ double prod[2][DOT_CHUNK];
+  const BoxDesc bd = boxes[blockIdx.x];
+  const int nx = bd.hi[0] - bd.lo[0] + 1, ny = bd.hi[1] - bd.lo[1] + 1, nz = bd.hi[2] - bd.lo[2] + 1;
+  const int n = nx * ny * nz;
+  const int lane = threadIdx.x;
+  double xr[DOT_PER_LANE], yr[DOT_PER_LANE];
+  // Loads of one chunk into registers (issued, not waited for).
+  auto issue = [&](int base) {
+#pragma unroll
+    for (int u = 0; u < DOT_PER_LANE; ++u) {
+      const int q = base + lane + 32 * u;
+      xr[u] = 0.0;
+      yr[u] = 0.0;
+      if (q < n) {
+        const int i = bd.lo[0] + q % nx, j = bd.lo[1] + (q / nx) % ny, k = bd.lo[2] + q / (nx * ny);
         const int64_t c = cellIndex(bd, i, j, k);
-        s += x[c] * y[c];
+        xr[u] = x[c];
+        yr[u] = y[c];
       }
     }
-  out[b] = s;
+  };
+  auto store = [&](double* dst) {
+#pragma unroll
+    for (int u = 0; u < DOT_PER_LANE; ++u) dst[lane + 32 * u] = xr[u] * yr[u];
+  };
+  double s = 0.0;
+  issue(0);
+  store(prod[0]);
+  __syncwarp();
+  for (int base = 0, buf = 0; base < n; base += DOT_CHUNK, buf ^= 1) {
+    // the next chunk's loads are in flight while lane 0 adds this one
+    const bool more = base + DOT_CHUNK < n;
+    if (more) issue(base + DOT_CHUNK);
+    if (lane == 0) {
+      const int m = min(DOT_CHUNK, n - base);
+      const double* p = prod[buf];
+      for (int u = 0; u < m; ++u) s += p[u];
+    }
+    __syncwarp();
+    if (more) store(prod[buf ^ 1]);
+    __syncwarp();
+  }
+  if (lane == 0) out[blockIdx.x] = s;
 }
 
 // dst = src over whole arrays (ghosts included), converting the type.
@@ -971,7 +1005,7 @@ void scaleField(double* x, double scale, int64_t n, cudaStream_t s) {
 
 void boxDots(const LevelDev& L, const double* x, const double* y, double* out, cudaStream_t s) {
   if (L.nbox == 0) return;
-  k_box_dot<<<(L.nbox + 63) / 64, 64, 0, s>>>(L.boxes, L.nbox, x, y, out);
+  k_box_dot<<<L.nbox, 32, 0, s>>>(L.boxes, x, y, out);
   CMG_LAUNCHED("boxDots");
 }
 

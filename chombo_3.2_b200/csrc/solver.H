@@ -9,6 +9,7 @@
 
 #include <map>
 #include <memory>
+#include <tuple>
 #include <vector>
 
 #include "kernels.H"
@@ -213,6 +214,10 @@ class Solver {
   double mlNorm(const MLVec& x);
   double mlDot(const MLVec& x, const MLVec& y);
   void mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p);
+  void mlPreCondBody(MLVec& cor, MLVec& res, const MLSolveParams& p);
+  // Captured preconditioner calls, per (correction, residual) vector pair and
+  // smoothing parameters.
+  std::map<std::tuple<const void*, const void*, int, int>, cudaGraphExec_t> precondGraphs_;
   void amrOperatorLevel(int ilev, int lmax, MLVec& lhs, MLVec& phi);
   void scatterValid(const LevelPlan& p, const LevelDev& d, double* dev, const double* src, bool onDevice,
                     int faceDir);

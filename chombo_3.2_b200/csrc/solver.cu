@@ -308,6 +308,7 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), des
 Solver::~Solver() {
   cudaStreamSynchronize(s_);
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
   if (hostScalars_) cudaFreeHost(hostScalars_);
   if (hostBoxSums_) cudaFreeHost(hostBoxSums_);
 }
@@ -740,6 +741,8 @@ void Solver::setRelaxMode(int mode) {
   tuned_ = false;
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
   graphs_.clear();
+  for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
+  precondGraphs_.clear();
 }
 
 // Ghost fill, timed as its own class: every ghost cell filled written once
@@ -1037,7 +1040,7 @@ double Solver::mlDot(const MLVec& x, const MLVec& y) {
 // times, the homogeneous residual of the current correction, one AMR
 // V-cycle from a zero correction (AMRMultiGrid::AMRVCycle on the
 // preconditioner's own scratch), and the increment.
-void Solver::mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p) {
+void Solver::mlPreCondBody(MLVec& cor, MLVec& res, const MLSolveParams& p) {
   const int lmax = numLevels() - 1;
   MLVec ures(lmax + 1), ucorr(lmax + 1);
   for (int l = 0; l <= lmax; ++l) {
@@ -1050,6 +1053,42 @@ void Solver::mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p) {
     amrVCycle<double>(lmax, lmax);
     mlIncr(cor, ucorr, 1.0);
   }
+}
+
+// The preconditioner call is one CUDA-graph replay when graphs are on (no
+// host decision inside it; the bottom solve reads its metric from device
+// memory).
+void Solver::mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p) {
+  if (!useGraphs_ || profOn_) {
+    mlPreCondBody(cor, res, p);
+    return;
+  }
+  const auto key = std::make_tuple((const void*)cor[0], (const void*)res[0], p.mgIters, p.mgSmooth);
+  auto it = precondGraphs_.find(key);
+  cudaGraphExec_t exec = nullptr;
+  if (it != precondGraphs_.end()) {
+    exec = it->second;
+  } else {
+    cudaGraph_t g = nullptr;
+    const long long before = launchCount();
+    ck(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      mlPreCondBody(cor, res, p);
+    } catch (...) {
+      cudaStreamEndCapture(s_, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    ck(cudaStreamEndCapture(s_, &g), "end capture");
+    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    ck(e, "graph instantiate");
+    precondGraphs_[key] = exec;
+    graphLaunches_[exec] = launchCount() - before;
+    addLaunches(-(launchCount() - before));
+  }
+  ck(cudaGraphLaunch(exec, s_), "graph launch");
+  addLaunches(graphLaunches_[exec]);
 }
 
 MLSolveResult Solver::solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroPhi) {

@@ -13,7 +13,7 @@
 //
 // Usage: cmg_oracle_mlbicgstab key=value ... out=<prefix>
 //   n0 levels maxbox block fill op alpha beta seed thresh (as cmg_oracle)
-//   mgiters=1 mgsmooth=4 eps=1e-9 imax=100
+//   mgiters=1 mgsmooth=4 eps=1e-9 imax=100 [boxfile=<file> as cmg_oracle]
 // Writes <prefix>.json and <prefix>.bin (per level, per box in layout order,
 // valid cells x-fastest: phi).
 
@@ -58,6 +58,7 @@ int main(int argc, char** argv) {
   P.beta = argd("beta", 1.0);
   P.seed = (unsigned long long)argd("seed", 20261203.0);
   P.thresh = argd("thresh", 0.1);
+  if (g_args.count("boxfile")) P.boxfile = g_args["boxfile"];
   const int mgIters = argi("mgiters", 1), mgSmooth = argi("mgsmooth", 4), imax = argi("imax", 100);
   const Real eps = argd("eps", 1e-9);
   const std::string out = g_args.count("out") ? g_args["out"] : std::string("mlbicgstab_out");

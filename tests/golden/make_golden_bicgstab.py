@@ -28,6 +28,8 @@ CASES = {
     "bicgstab_helmholtz_2lev_16": ("helmholtz_2lev_16", "mgiters=1 mgsmooth=2 eps=1e-10 imax=100", 1),
     "bicgstab_vc_3lev_16": ("vc_3lev_16", "mgiters=2 mgsmooth=4 eps=1e-9 imax=100", 1),
     "bicgstab_poisson_3lev_32": ("poisson_3lev_32", "mgiters=1 mgsmooth=4 eps=1e-9 imax=100", 97),
+    # the config-1 hierarchy as the bench's config1-bicgstab workload solves it (about 3 minutes)
+    "bicgstab_config1_vc_3lev_128": ("config1_vc_3lev_128", "mgiters=2 mgsmooth=4 eps=1e-10 imax=100", 997),
 }
 
 

@@ -14,7 +14,7 @@ from conftest import golden
 
 TOL = 1e-12
 CASES = ["bicgstab_poisson_1lev_32", "bicgstab_vc_1lev_32", "bicgstab_helmholtz_2lev_16", "bicgstab_vc_3lev_16",
-         "bicgstab_poisson_3lev_32"]
+         "bicgstab_poisson_3lev_32", "bicgstab_config1_vc_3lev_128"]
 
 
 def params(cmg, meta):
@@ -62,4 +62,24 @@ def test_bicgstab_from_current_phi(cmg):
     first = h.solve_bicgstab(p)
     again = h.solve_bicgstab(p, zero_phi=False)
     assert again["initial_residual"] <= 2 * first["final_residual"]
+    h.close()
+
+
+@pytest.mark.gpu
+def test_bicgstab_graph_replay_is_bit_identical(cmg):
+    """Each preconditioner call replayed from a captured CUDA graph gives the same bits as launching it."""
+    meta, _ = golden("bicgstab_vc_3lev_16")
+    base, _ = golden(meta["base"])
+    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"])
+    h.fill_synthetic(base["seed"])
+    p = params(cmg, meta)
+    plain = h.solve_bicgstab(p)
+    phi = [h.phi(l) for l in range(len(base["boxes"]))]
+    h.use_graphs(True)
+    for _ in range(2):  # capture, then replay
+        g = h.solve_bicgstab(p)
+        assert g["iterations"] == plain["iterations"] and g["final_residual"] == plain["final_residual"]
+        assert np.array_equal(g["history"], plain["history"])
+        for l in range(len(phi)):
+            assert np.array_equal(h.phi(l), phi[l])
     h.close()

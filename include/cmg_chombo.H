@@ -25,6 +25,11 @@
 //     with the reference's default parameters);
 //   - solve over all levels: l_base = 0 and l_max = numLevels - 1.
 // Only valid cells of phi are written; ghost cells are left as they were.
+//
+// The variable-coefficient example's solve path has its drop-in too:
+// MultilevelLinearOp<FArrayBox> + BiCGStabSolver<Vector<LevelData<FArrayBox>*>>
+// become cmg_chombo::GpuMultilevelLinearOp + GpuMultilevelBiCGStabSolver with
+// the same members and calls (define with the GPU factory, solve(phi, rhs)).
 #ifndef CMG_CHOMBO_H
 #define CMG_CHOMBO_H
 
@@ -39,6 +44,7 @@
 #include "LinearSolver.H"
 #include "MayDay.H"
 #include "ProblemDomain.H"
+#include "RealVect.H"
 #include "RefCountedPtr.H"
 #include "cmg.h"
 
@@ -109,107 +115,24 @@ class GpuVCAMRPoissonOp2Factory {
 
 // AMRMultiGrid<LevelData<FArrayBox>> (AMRElliptic/AMRMultiGrid.H:301-470):
 // define, setSolverParameters, solve, computeAMRResidual, m_exitStatus.
-class GpuAMRMultiGrid {
+// The device hierarchy behind the drop-ins: the factory's description turned
+// into a cmg_hierarchy, and LevelData valid cells moved to and from it.
+class GpuHierarchy {
  public:
-  int m_exitStatus = 0;
-  int m_verbosity = 0;
-
-  GpuAMRMultiGrid() {}
-  ~GpuAMRMultiGrid() { clear(); }
-  GpuAMRMultiGrid(const GpuAMRMultiGrid&) = delete;
-  GpuAMRMultiGrid& operator=(const GpuAMRMultiGrid&) = delete;
-
-  void define(const ProblemDomain& a_coarseDomain, GpuAMRPoissonOpFactory& a_factory, LinearSolver<LDF>* a_bottom,
-              int a_numLevels) {
-    defineFrom(a_coarseDomain, a_factory.description(), a_bottom, a_numLevels);
-  }
-  void define(const ProblemDomain& a_coarseDomain, GpuVCAMRPoissonOp2Factory& a_factory, LinearSolver<LDF>* a_bottom,
-              int a_numLevels) {
-    defineFrom(a_coarseDomain, a_factory.description(), a_bottom, a_numLevels);
-  }
-
-  // AMRMultiGrid::setSolverParameters (AMRMultiGrid.H:451-458, 527-546).
-  void setSolverParameters(const int& a_pre, const int& a_post, const int& a_bottom, const int& a_numMG,
-                           const int& a_iterMax, const Real& a_eps, const Real& a_hang, const Real& a_normThresh) {
-    m_p.pre = a_pre;
-    m_p.post = a_post;
-    m_p.bottom = a_bottom;
-    m_p.num_mg = a_numMG;
-    m_p.iter_max = a_iterMax;
-    m_p.eps = a_eps;
-    m_p.hang = a_hang;
-    m_p.norm_thresh = a_normThresh;
-  }
-
-  // AMRMultiGrid::solve (AMRMultiGrid.H:894-1124) on the device.
-  void solve(Vector<LDF*>& a_phi, const Vector<LDF*>& a_rhs, int l_max, int l_base, bool a_zeroPhi = true,
-             bool /*forceHomogeneous*/ = false) {
-    checkRange(l_max, l_base);
-    std::vector<double> buf;
-    for (int l = 0; l < m_nlev; ++l) {
-      pack(*a_rhs[l], l, buf);
-      check(cmg_set_rhs(m_h, l, buf.data(), 0));
-      if (!a_zeroPhi) {
-        pack(*a_phi[l], l, buf);
-        check(cmg_set_phi(m_h, l, buf.data(), 0));
-      }
-    }
-    m_history.assign(m_p.iter_max + 2, 0.0);
-    int st = 0, it = 0, hl = 0;
-    check(cmg_solve(m_h, &m_p, a_zeroPhi ? 1 : 0, &st, &it, m_history.data(), (int)m_history.size(), &hl));
-    m_history.resize(hl);
-    m_exitStatus = st;
-    m_iterations = it;
-    for (int l = 0; l < m_nlev; ++l) {
-      buf.resize(cells(l));
-      check(cmg_get_phi(m_h, l, buf.data(), 0));
-      unpack(buf, l, *a_phi[l]);
-    }
-  }
-
-  // AMRMultiGrid::computeAMRResidual(phi, rhs, l_max, l_base) (AMRMultiGrid.H:738-750):
-  // the composite max-norm residual of the given phi and rhs.
-  Real computeAMRResidual(Vector<LDF*>& a_phi, const Vector<LDF*>& a_rhs, int l_max, int l_base) {
-    checkRange(l_max, l_base);
-    std::vector<double> buf;
-    for (int l = 0; l < m_nlev; ++l) {
-      pack(*a_rhs[l], l, buf);
-      check(cmg_set_rhs(m_h, l, buf.data(), 0));
-      pack(*a_phi[l], l, buf);
-      check(cmg_set_phi(m_h, l, buf.data(), 0));
-    }
-    double r = 0;
-    check(cmg_residual_norm(m_h, &r));
-    return r;
-  }
-
-  // Composite max-norm residual at the start of every iteration of the last
-  // solve, then the final one (what an AMRMultiGridInspector would record).
-  const std::vector<double>& residualHistory() const { return m_history; }
-  int iterations() const { return m_iterations; }
-
+  GpuHierarchy() {}
+  ~GpuHierarchy() { clear(); }
+  GpuHierarchy(const GpuHierarchy&) = delete;
+  GpuHierarchy& operator=(const GpuHierarchy&) = delete;
   void clear() {
     if (m_h) cmg_hierarchy_destroy(m_h);
     m_h = nullptr;
     m_nlev = 0;
   }
-
- private:
-  cmg_hierarchy* m_h = nullptr;
-  int m_nlev = 0;
-  GpuOpDescription m_d;
-  cmg_solve_params m_p = {4, 4, 4, 1, 100, 5, 1e-10, 1e-10, 1e-30};
-  std::vector<double> m_history;
-  int m_iterations = 0;
+  cmg_hierarchy* handle() const { return m_h; }
+  int numLevels() const { return m_nlev; }
 
   static void check(int rc) {
     if (rc != CMG_OK) MayDay::Error(cmg_last_error());
-  }
-
-  void checkRange(int l_max, int l_base) const {
-    if (!m_h) MayDay::Error("GpuAMRMultiGrid: solve before define");
-    if (l_base != 0 || l_max != m_nlev - 1)
-      MayDay::Error("GpuAMRMultiGrid: only l_base = 0, l_max = numLevels - 1 is supported");
   }
 
   int64_t cells(int l) const {
@@ -243,17 +166,31 @@ class GpuAMRMultiGrid {
     }
   }
 
-  void defineFrom(const ProblemDomain& a_coarseDomain, const GpuOpDescription& d, LinearSolver<LDF>* a_bottom,
-                  int a_numLevels) {
+  void setLevels(const Vector<LDF*>& a_data, bool phi) const {
+    std::vector<double> buf;
+    for (int l = 0; l < m_nlev; ++l) {
+      pack(*a_data[l], l, buf);
+      check(phi ? cmg_set_phi(m_h, l, buf.data(), 0) : cmg_set_rhs(m_h, l, buf.data(), 0));
+    }
+  }
+
+  void getPhi(Vector<LDF*>& a_phi) const {
+    std::vector<double> buf;
+    for (int l = 0; l < m_nlev; ++l) {
+      buf.resize(cells(l));
+      check(cmg_get_phi(m_h, l, buf.data(), 0));
+      unpack(buf, l, *a_phi[l]);
+    }
+  }
+
+  void defineFrom(const ProblemDomain& a_coarseDomain, const GpuOpDescription& d, int a_numLevels) {
     clear();
-    if (!d.defined) MayDay::Error("GpuAMRMultiGrid: factory not defined");
-    if (a_bottom && !dynamic_cast<BiCGStabSolver<LDF>*>(a_bottom))
-      MayDay::Error("GpuAMRMultiGrid: the device solve uses BiCGStab as its bottom solver");
-    if (a_numLevels < 1 || a_numLevels > d.grids.size()) MayDay::Error("GpuAMRMultiGrid: bad number of levels");
+    if (!d.defined) MayDay::Error("cmg_chombo: factory not defined");
+    if (a_numLevels < 1 || a_numLevels > d.grids.size()) MayDay::Error("cmg_chombo: bad number of levels");
     for (int l = 0; l + 1 < a_numLevels; ++l)
-      if (d.refRatios[l] != 2) MayDay::Error("GpuAMRMultiGrid: refinement ratio 2 only");
+      if (d.refRatios[l] != 2) MayDay::Error("cmg_chombo: refinement ratio 2 only");
     for (int dir = 0; dir < SpaceDim; ++dir)
-      if (a_coarseDomain.isPeriodic(dir)) MayDay::Error("GpuAMRMultiGrid: periodic domains are not supported");
+      if (a_coarseDomain.isPeriodic(dir)) MayDay::Error("cmg_chombo: periodic domains are not supported");
     m_d = d;
     m_nlev = a_numLevels;
     std::vector<int> counts;
@@ -301,6 +238,182 @@ class GpuAMRMultiGrid {
       check(cmg_finalize_coefficients(m_h));
     }
   }
+
+ protected:
+  cmg_hierarchy* m_h = nullptr;
+  int m_nlev = 0;
+  GpuOpDescription m_d;
+};
+
+class GpuAMRMultiGrid : private GpuHierarchy {
+ public:
+  int m_exitStatus = 0;
+  int m_verbosity = 0;
+
+  GpuAMRMultiGrid() {}
+
+  void define(const ProblemDomain& a_coarseDomain, GpuAMRPoissonOpFactory& a_factory, LinearSolver<LDF>* a_bottom,
+              int a_numLevels) {
+    defineWith(a_coarseDomain, a_factory.description(), a_bottom, a_numLevels);
+  }
+  void define(const ProblemDomain& a_coarseDomain, GpuVCAMRPoissonOp2Factory& a_factory, LinearSolver<LDF>* a_bottom,
+              int a_numLevels) {
+    defineWith(a_coarseDomain, a_factory.description(), a_bottom, a_numLevels);
+  }
+
+  // AMRMultiGrid::setSolverParameters (AMRMultiGrid.H:451-458, 527-546).
+  void setSolverParameters(const int& a_pre, const int& a_post, const int& a_bottom, const int& a_numMG,
+                           const int& a_iterMax, const Real& a_eps, const Real& a_hang, const Real& a_normThresh) {
+    m_p.pre = a_pre;
+    m_p.post = a_post;
+    m_p.bottom = a_bottom;
+    m_p.num_mg = a_numMG;
+    m_p.iter_max = a_iterMax;
+    m_p.eps = a_eps;
+    m_p.hang = a_hang;
+    m_p.norm_thresh = a_normThresh;
+  }
+
+  // AMRMultiGrid::solve (AMRMultiGrid.H:894-1124) on the device.
+  void solve(Vector<LDF*>& a_phi, const Vector<LDF*>& a_rhs, int l_max, int l_base, bool a_zeroPhi = true,
+             bool /*forceHomogeneous*/ = false) {
+    checkRange(l_max, l_base);
+    setLevels(a_rhs, false);
+    if (!a_zeroPhi) setLevels(a_phi, true);
+    m_history.assign(m_p.iter_max + 2, 0.0);
+    int st = 0, it = 0, hl = 0;
+    check(cmg_solve(m_h, &m_p, a_zeroPhi ? 1 : 0, &st, &it, m_history.data(), (int)m_history.size(), &hl));
+    m_history.resize(hl);
+    m_exitStatus = st;
+    m_iterations = it;
+    getPhi(a_phi);
+  }
+
+  // AMRMultiGrid::computeAMRResidual(phi, rhs, l_max, l_base) (AMRMultiGrid.H:738-750):
+  // the composite max-norm residual of the given phi and rhs.
+  Real computeAMRResidual(Vector<LDF*>& a_phi, const Vector<LDF*>& a_rhs, int l_max, int l_base) {
+    checkRange(l_max, l_base);
+    setLevels(a_rhs, false);
+    setLevels(a_phi, true);
+    double r = 0;
+    check(cmg_residual_norm(m_h, &r));
+    return r;
+  }
+
+  // Composite max-norm residual at the start of every iteration of the last
+  // solve, then the final one (what an AMRMultiGridInspector would record).
+  const std::vector<double>& residualHistory() const { return m_history; }
+  int iterations() const { return m_iterations; }
+
+  void clear() { GpuHierarchy::clear(); }
+
+ private:
+  cmg_solve_params m_p = {4, 4, 4, 1, 100, 5, 1e-10, 1e-10, 1e-30};
+  std::vector<double> m_history;
+  int m_iterations = 0;
+
+  void checkRange(int l_max, int l_base) const {
+    if (!m_h) MayDay::Error("GpuAMRMultiGrid: solve before define");
+    if (l_base != 0 || l_max != m_nlev - 1)
+      MayDay::Error("GpuAMRMultiGrid: only l_base = 0, l_max = numLevels - 1 is supported");
+  }
+
+  void defineWith(const ProblemDomain& a_coarseDomain, const GpuOpDescription& d, LinearSolver<LDF>* a_bottom,
+                  int a_numLevels) {
+    if (a_bottom && !dynamic_cast<BiCGStabSolver<LDF>*>(a_bottom))
+      MayDay::Error("GpuAMRMultiGrid: the device solve uses BiCGStab as its bottom solver");
+    defineFrom(a_coarseDomain, d, a_numLevels);
+  }
+};
+
+// MultilevelLinearOp<FArrayBox> (AMRElliptic/MultilevelLinearOp.H) for the
+// GPU factories: the multilevel operator with the AMR multigrid
+// preconditioner, as the variable-coefficient example defines it
+// (VCPoissonSolve.cpp:148-167).  Supported: lBase 0, the multigrid
+// preconditioner at full depth (m_preCondSolverDepth -1).
+class GpuMultilevelLinearOp : public GpuHierarchy {
+ public:
+  bool m_use_multigrid_preconditioner = true;
+  int m_num_mg_iterations = 1;
+  int m_num_mg_smooth = 4;
+  int m_preCondSolverDepth = -1;
+
+  void define(const Vector<DisjointBoxLayout>& a_vectGrids, const Vector<int>& /*a_refRatios*/,
+              const Vector<ProblemDomain>& a_domains, const Vector<RealVect>& /*a_vectDx*/,
+              GpuAMRPoissonOpFactory& a_factory, int a_lBase) {
+    defineWith(a_vectGrids, a_domains, a_factory.description(), a_lBase);
+  }
+  void define(const Vector<DisjointBoxLayout>& a_vectGrids, const Vector<int>& /*a_refRatios*/,
+              const Vector<ProblemDomain>& a_domains, const Vector<RealVect>& /*a_vectDx*/,
+              GpuVCAMRPoissonOp2Factory& a_factory, int a_lBase) {
+    defineWith(a_vectGrids, a_domains, a_factory.description(), a_lBase);
+  }
+
+ private:
+  void defineWith(const Vector<DisjointBoxLayout>& a_vectGrids, const Vector<ProblemDomain>& a_domains,
+                  const GpuOpDescription& d, int a_lBase) {
+    if (a_lBase != 0) MayDay::Error("GpuMultilevelLinearOp: only lBase = 0 is supported");
+    if (a_domains.size() < 1) MayDay::Error("GpuMultilevelLinearOp: no domains");
+    defineFrom(a_domains[0], d, a_vectGrids.size());
+  }
+};
+
+// BiCGStabSolver<Vector<LevelData<FArrayBox>*>> over GpuMultilevelLinearOp
+// (BiCGStabSolver.H:199-515 with MultilevelLinearOp's vector operations):
+// the same members and solve(phi, rhs), phi being the initial guess.  The
+// max norm (m_normType 0, what the example sets) is supported; no
+// convergence metric (m_convergenceMetric <= 0).
+class GpuMultilevelBiCGStabSolver {
+ public:
+  bool m_homogeneous = false;
+  int m_imax = 80;
+  int m_verbosity = 3;
+  Real m_eps = 1.0E-6;
+  Real m_reps = 1.0E-12;
+  Real m_convergenceMetric = -1.0;
+  Real m_hang = 1E-8;
+  int m_exitStatus = -1;
+  int m_iter = -1;
+  Real m_residual = -1e300;
+  Real m_initial_residual = -1e300;
+  Real m_small = 1.0E-30;
+  int m_numRestarts = 5;
+  int m_normType = 2;
+
+  void define(GpuMultilevelLinearOp* a_operator, bool a_homogeneous) {
+    m_op = a_operator;
+    m_homogeneous = a_homogeneous;
+  }
+
+  void solve(Vector<LDF*>& a_phi, const Vector<LDF*>& a_rhs) {
+    if (!m_op || !m_op->handle()) MayDay::Error("GpuMultilevelBiCGStabSolver: solve before define");
+    if (m_normType != 0) MayDay::Error("GpuMultilevelBiCGStabSolver: only the max norm (m_normType 0) is supported");
+    if (m_convergenceMetric > 0) MayDay::Error("GpuMultilevelBiCGStabSolver: convergence metrics are not supported");
+    if (!m_op->m_use_multigrid_preconditioner || m_op->m_preCondSolverDepth >= 0)
+      MayDay::Error("GpuMultilevelBiCGStabSolver: only the full-depth multigrid preconditioner is supported");
+    if (a_phi.size() != m_op->numLevels() || a_rhs.size() != m_op->numLevels())
+      MayDay::Error("GpuMultilevelBiCGStabSolver: level count differs from the operator's");
+    m_op->setLevels(a_rhs, false);
+    m_op->setLevels(a_phi, true);
+    cmg_mlsolve_params p = {m_op->m_num_mg_iterations, m_op->m_num_mg_smooth, m_imax, m_numRestarts,
+                            m_eps, m_reps, m_hang, m_small};
+    m_history.assign(m_imax + 1, 0.0);
+    int hl = 0;
+    double r0 = 0, rf = 0;
+    GpuHierarchy::check(cmg_solve_multilevel_bicgstab(m_op->handle(), &p, 0, &m_exitStatus, &m_iter, &r0, &rf,
+                                                      m_history.data(), (int)m_history.size(), &hl));
+    m_history.resize(hl);
+    m_initial_residual = r0;
+    m_residual = rf;
+    m_op->getPhi(a_phi);
+  }
+
+  // Residual norm after every iteration of the last solve.
+  const std::vector<double>& residualHistory() const { return m_history; }
+
+ private:
+  GpuMultilevelLinearOp* m_op = nullptr;
+  std::vector<double> m_history;
 };
 
 }  // namespace cmg_chombo

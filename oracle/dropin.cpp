@@ -8,7 +8,8 @@
 // iteration count, residual histories and phi on every level.
 //
 // Usage: dropin key=value ...   (n0 levels maxbox block op alpha beta seed
-// pre post bottom iters eps hang, as for cmg_oracle)
+// pre post bottom iters eps hang, as for cmg_oracle; bicgstab=1 mgiters
+// mgsmooth imax eps for the BiCGStab over MultilevelLinearOp path)
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -19,6 +20,7 @@
 #include "AMRMultiGrid.H"
 #include "AMRPoissonOp.H"
 #include "BiCGStabSolver.H"
+#include "MultilevelLinearOp.H"
 #include "VCAMRPoissonOp2.H"
 #include "cmg_chombo.H"
 #include "problem.H"
@@ -27,6 +29,90 @@ static std::map<std::string, std::string> g_args;
 static double argd(const char* k, double d) {
   auto it = g_args.find(k);
   return it == g_args.end() ? d : std::atof(it->second.c_str());
+}
+
+static double phiDeviation(const OracleProblem& P, const Vector<LDF*>& phiGpu) {
+  double maxRel = 0;
+  for (int l = 0; l < P.nlev; ++l) {
+    double scale = 0, diff = 0;
+    for (DataIterator dit = P.grids[l].dataIterator(); dit.ok(); ++dit) {
+      const Box& b = P.grids[l][dit()];
+      for (BoxIterator bit(b); bit.ok(); ++bit) {
+        scale = std::max(scale, std::fabs((*P.phi[l])[dit](bit(), 0)));
+        diff = std::max(diff, std::fabs((*P.phi[l])[dit](bit(), 0) - (*phiGpu[l])[dit](bit(), 0)));
+      }
+    }
+    maxRel = std::max(maxRel, scale > 0 ? diff / scale : diff);
+  }
+  return maxRel;
+}
+
+// The variable-coefficient example's solve path (VCPoissonSolve.cpp:146-183):
+// the reference's BiCGStabSolver over MultilevelLinearOp on the CPU, then the
+// same calls on cmg_chombo::GpuMultilevelLinearOp + GpuMultilevelBiCGStabSolver.
+static int bicgstabCheck(OracleProblem& P, Vector<LDF*>& phiGpu, Vector<int>& rr) {
+  const int nlev = P.nlev;
+  const int mgIters = (int)argd("mgiters", 2), mgSmooth = (int)argd("mgsmooth", 4), imax = (int)argd("imax", 100);
+  const Real eps = argd("eps", 1e-9);
+  Vector<RealVect> dxv(nlev);
+  for (int l = 0; l < nlev; ++l) dxv[l] = RealVect::Unit * P.dxs[l];
+  RefCountedPtr<AMRLevelOpFactory<LDF> > factory;
+  if (P.opType == 0) {
+    AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
+  } else {
+    VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
+  }
+  for (int l = 0; l < nlev; ++l)
+    for (DataIterator dit = P.grids[l].dataIterator(); dit.ok(); ++dit) {
+      (*P.phi[l])[dit()].setVal(0.0);
+      (*phiGpu[l])[dit()].setVal(0.0);
+    }
+  MultilevelLinearOp<FArrayBox> mlOp;
+  mlOp.m_num_mg_iterations = mgIters;
+  mlOp.m_num_mg_smooth = mgSmooth;
+  mlOp.define(P.grids, rr, P.domains, dxv, factory, 0);
+  BiCGStabSolver<Vector<LDF*> > cpu;
+  cpu.define(&mlOp, false);
+  cpu.m_verbosity = 0;
+  cpu.m_normType = 0;
+  cpu.m_eps = eps;
+  cpu.m_imax = imax;
+  cpu.solve(P.phi, P.rhs);
+
+  cmg_chombo::GpuMultilevelLinearOp gop;
+  gop.m_num_mg_iterations = mgIters;
+  gop.m_num_mg_smooth = mgSmooth;
+  if (P.opType == 0) {
+    cmg_chombo::GpuAMRPoissonOpFactory f;
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    gop.define(P.grids, rr, P.domains, dxv, f, 0);
+  } else {
+    cmg_chombo::GpuVCAMRPoissonOp2Factory f;
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    gop.define(P.grids, rr, P.domains, dxv, f, 0);
+  }
+  cmg_chombo::GpuMultilevelBiCGStabSolver gpu;
+  gpu.define(&gop, false);
+  gpu.m_verbosity = 0;
+  gpu.m_normType = 0;
+  gpu.m_eps = eps;
+  gpu.m_imax = imax;
+  gpu.solve(phiGpu, P.rhs);
+  std::printf("{\"levels\": %d, \"cpu_exit\": %d, \"gpu_exit\": %d, \"cpu_iters\": %d, \"gpu_iters\": %d, "
+              "\"cpu_r0\": %.17g, \"gpu_r0\": %.17g, \"cpu_rfinal\": %.17g, \"gpu_rfinal\": %.17g, "
+              "\"phi_rel_dev\": %.3e}\n",
+              nlev, cpu.m_exitStatus, gpu.m_exitStatus, cpu.m_iter, gpu.m_iter, cpu.m_initial_residual,
+              gpu.m_initial_residual, cpu.m_residual, gpu.m_residual, phiDeviation(P, phiGpu));
+  for (int l = 0; l < nlev; ++l) {
+    delete phiGpu[l];
+    delete P.phi[l];
+    delete P.rhs[l];
+  }
+  return 0;
 }
 
 int main(int argc, char** argv) {
@@ -52,6 +138,7 @@ int main(int argc, char** argv) {
   Vector<LDF*> phiGpu(nlev);
   for (int l = 0; l < nlev; ++l) phiGpu[l] = new LDF(P.grids[l], 1, IntVect::Unit);
   Vector<int> rr(nlev, 2);
+  if (argd("bicgstab", 0) != 0) return bicgstabCheck(P, phiGpu, rr);
 
   // Reference: CPU AMRMultiGrid.
   RefCountedPtr<AMRLevelOpFactory<LDF> > factory;

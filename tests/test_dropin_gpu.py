@@ -39,3 +39,26 @@ def test_dropin_matches_reference_solver(name):
     assert out["phi_rel_dev"] <= TOL, out
     # computeAMRResidual through the drop-in reproduces the solve's last entry.
     assert out["gpu_final_residual"] == out["gpu_history_last"], out
+
+
+BICG_CASES = {
+    "vc_3lev_16": "n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=-1 bicgstab=1 mgiters=2 mgsmooth=4 eps=1e-9",
+    "poisson_1lev_32": "n0=32 levels=1 maxbox=16 op=0 alpha=0 beta=1 bicgstab=1 mgiters=1 mgsmooth=4 eps=1e-9",
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(BICG_CASES))
+def test_dropin_bicgstab_matches_reference_solver(name):
+    """MultilevelLinearOp + BiCGStabSolver<Vector<LevelData*>> (the variable-coefficient example's solve path)
+    against cmg_chombo::GpuMultilevelLinearOp + GpuMultilevelBiCGStabSolver with the same calls."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in check not built (make -C oracle dropin, needs the reference tree)")
+    r = subprocess.run([DROPIN] + BICG_CASES[name].split(), capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["gpu_exit"] == out["cpu_exit"] == 1, out
+    assert out["gpu_iters"] == out["cpu_iters"], out
+    assert abs(out["gpu_r0"] - out["cpu_r0"]) <= TOL * out["cpu_r0"], out
+    assert abs(out["gpu_rfinal"] - out["cpu_rfinal"]) <= TOL * out["cpu_r0"], out
+    assert out["phi_rel_dev"] <= TOL, out

@@ -268,6 +268,19 @@ class Hierarchy:
                   _ptr(hist), len(hist), ctypes.byref(hl)))
         return {"exit_status": st.value, "iterations": it.value, "history": hist[:hl.value].copy()}
 
+    def set_alpha_beta(self, alpha, beta):
+        """TGAHelmOp::setAlphaAndBeta on every operator of the hierarchy (cmg_set_alpha_beta)."""
+        _check(lib().cmg_set_alpha_beta(self.h, ctypes.c_double(alpha), ctypes.c_double(beta)))
+
+    def backward_euler(self, params, dt, nsteps, zero_phi=False):
+        """nsteps BackwardEuler::oneStep steps on phi with the right-hand side as the source
+        (cmg_backward_euler); returns each step's exit status and iteration count."""
+        st = (ctypes.c_int * max(nsteps, 1))()
+        it = (ctypes.c_int * max(nsteps, 1))()
+        _check(lib().cmg_backward_euler(self.h, ctypes.byref(params), ctypes.c_double(dt), int(nsteps),
+                                        int(zero_phi), st, it))
+        return [{"exit_status": st[n], "iterations": it[n]} for n in range(nsteps)]
+
     def solve_bicgstab(self, params=None, zero_phi=True):
         """BiCGStab over MultilevelLinearOp preconditioned by AMR multigrid (cmg_solve_multilevel_bicgstab)."""
         p = params or mlsolve_params()

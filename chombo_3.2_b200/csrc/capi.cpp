@@ -317,6 +317,39 @@ int cmg_solve_mixed(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, i
   return solveWith(h, p, zero_phi, exit_status, iterations, history, history_cap, history_len, true);
 }
 
+int cmg_set_alpha_beta(cmg_hierarchy* h, double alpha, double beta) {
+  return guard([&]() {
+    needLevel(h, 0);
+    h->solver->setAlphaAndBeta(alpha, beta);
+  });
+}
+
+int cmg_backward_euler(cmg_hierarchy* h, const cmg_solve_params* p, double dt, int nsteps, int zero_phi,
+                       int* exit_status, int* iterations) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (!p) throw std::invalid_argument("cmg: null parameters");
+    if (nsteps < 0 || !(dt > 0)) throw std::invalid_argument("cmg: invalid time step");
+    cmg::SolveParams sp;
+    sp.pre = p->pre;
+    sp.post = p->post;
+    sp.bottom = p->bottom;
+    sp.numMG = p->num_mg;
+    sp.iterMax = p->iter_max;
+    sp.imin = p->imin;
+    sp.eps = p->eps;
+    sp.hang = p->hang;
+    sp.normThresh = p->norm_thresh;
+    if (sp.pre < 0 || sp.post < 0 || sp.bottom < 0 || sp.numMG < 1 || sp.iterMax < 0)
+      throw std::invalid_argument("cmg: invalid solver parameters");
+    std::vector<cmg::SolveResult> r = h->solver->backwardEuler(sp, dt, nsteps, zero_phi != 0);
+    for (int n = 0; n < nsteps; ++n) {
+      if (exit_status) exit_status[n] = r[n].exitStatus;
+      if (iterations) iterations[n] = r[n].iterations;
+    }
+  });
+}
+
 int cmg_solve_multilevel_bicgstab(cmg_hierarchy* h, const cmg_mlsolve_params* p, int zero_phi, int* exit_status,
                                   int* iterations, double* initial_residual, double* final_residual, double* history,
                                   int history_cap, int* history_len) {

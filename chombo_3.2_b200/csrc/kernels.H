@@ -73,6 +73,10 @@ struct Coef {
 // colour par (the only ones a pass over colour 1 - par reads).
 template <class T> void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par = -1);
 template <class T> void zeroCovered(const LevelDev& L, T* f, cudaStream_t s);
+// Backward-Euler right-hand side over a whole level array:
+// rhs = ((0 + phi) * a) + ((0 + src) * dt), a == nullptr for no a-coefficient.
+void eulerRHS(double* rhs, const double* phi, const double* a, const double* src, double dt, int64_t n,
+              cudaStream_t s);
 // x *= scale over a whole level array.
 void scaleField(double* x, double scale, int64_t n, cudaStream_t s);
 // out[b] = sum of x*y over the valid cells of box b, accumulated in the

@@ -997,6 +997,27 @@ void ghostFill(const LevelDev& L, T* f, bool withCF, cudaStream_t s, int par) {
   CMG_LAUNCHED("ghostFill");
 }
 
+// BackwardEuler::createEulerRHS (BackwardEuler.cpp:190-226) over whole
+// arrays: rhs = ((0 + phi) * a) + ((0 + src) * dt), a omitted for the
+// constant-coefficient operator (its diagonalScale is a no-op).
+__global__ void k_euler_rhs(double* rhs, const double* phi, const double* a, const double* src, double dt,
+                            int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0 + phi[q];
+    if (a) v = v * a[q];
+    double w = 0.0 + src[q];
+    w = w * dt;
+    rhs[q] = v + w;
+  }
+}
+
+void eulerRHS(double* rhs, const double* phi, const double* a, const double* src, double dt, int64_t n,
+              cudaStream_t s) {
+  if (n == 0) return;
+  k_euler_rhs<<<flatBlocks(n), 256, 0, s>>>(rhs, phi, a, src, dt, n);
+  CMG_LAUNCHED("eulerRHS");
+}
+
 void scaleField(double* x, double scale, int64_t n, cudaStream_t s) {
   if (n == 0) return;
   k_scale_flat<<<flatBlocks(n), 256, 0, s>>>(x, scale, n);

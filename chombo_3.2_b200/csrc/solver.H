@@ -90,6 +90,18 @@ class Solver {
   // generator's, which the oracle reproduces bit for bit).
   void fillSyntheticDevice(uint64_t seed);
   SolveResult solve(const SolveParams& p, bool zeroPhi = true);
+  // TGAHelmOp::setAlphaAndBeta on every operator of the hierarchy (AMR
+  // levels and multigrid depths): AMRPoissonOp scales the factory's own
+  // coefficients (m_alpha = alpha * aCoef, AMRPoissonOp.cpp:1103-1108),
+  // VCAMRPoissonOp2 takes them as they are and recomputes lambda
+  // (VCAMRPoissonOp2.cpp:258-318).
+  void setAlphaAndBeta(double alpha, double beta);
+  // nsteps steps of BackwardEuler::oneStep (BackwardEuler.cpp:156-189,
+  // 228-245) with phi as the state and the right-hand side as the source:
+  // rhs_n = a phi_n + dt src, setAlphaAndBeta(1, -dt), solve for phi_{n+1}
+  // from phi_n (or from zero when zeroPhi).  The source is restored into the
+  // right-hand side afterwards.  Returns each step's solve.
+  std::vector<SolveResult> backwardEuler(const SolveParams& p, double dt, int nsteps, bool zeroPhi);
   // BiCGStab over MultilevelLinearOp (see MLSolveParams) from the current
   // phi, or from zero (ghost cells included) when zeroPhi.
   MLSolveResult solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroPhi = true);
@@ -201,6 +213,8 @@ class Solver {
   float* allocF(size_t n);
   // MultilevelLinearOp on device vectors (one array per AMR level).
   using MLVec = std::vector<double*>;
+  double alpha0_ = 0.0, beta0_ = 1.0;  // the factory's coefficients (AMRPoissonOp m_aCoef, m_bCoef)
+  std::vector<double*> src_;           // backward-Euler source per level
   std::vector<MLVec> mlVecs_;    // r, r_tilde, e, p, p_tilde, s_tilde, t, v, and two scratch vectors
   double* dBoxSums_ = nullptr;   // one per box of every level
   double* hostBoxSums_ = nullptr;

@@ -174,7 +174,8 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
   d.dxCrse = p.dxCrse;
 }
 
-Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream) : s_(stream), desc_(desc) {
+Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
+    : s_(stream), desc_(desc), alpha0_(desc.alpha), beta0_(desc.beta) {
   const int nlev = (int)desc.boxes.size();
   if (nlev < 1) throw std::runtime_error("cmg: hierarchy needs at least one level");
   amr_.resize(nlev);
@@ -733,6 +734,49 @@ void Solver::relaxVariants(std::vector<int>& inl, std::vector<float>& msFill, st
     msFill.push_back(t.first);
     msInline.push_back(t.second);
   }
+}
+
+void Solver::setAlphaAndBeta(double alpha, double beta) {
+  if (desc_.vc) {
+    desc_.alpha = alpha;
+    desc_.beta = beta;
+    for (int l = 0; l < numLevels(); ++l)
+      lambdaLevel(amrDev_[l], lev_[l].a, lev_[l].b, desc_.alpha, desc_.beta, lev_[l].lambda, s_);
+    for (size_t d = 0; d < mg_.size(); ++d)
+      lambdaLevel(mgDev_[d], mgf_[d].a, mgf_[d].b, desc_.alpha, desc_.beta, mgf_[d].lambda, s_);
+    gatherSlots(bottom_, coefMG((int)mg_.size()).lambda, bottom_.lam, s_);
+    coef32Stale_ = true;
+  } else {
+    desc_.alpha = alpha * alpha0_;
+    desc_.beta = beta * beta0_;
+  }
+  // captured iterations hold the old coefficients
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  graphs_.clear();
+  for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
+  precondGraphs_.clear();
+  ck(cudaStreamSynchronize(s_), "alpha and beta");
+}
+
+std::vector<SolveResult> Solver::backwardEuler(const SolveParams& p, double dt, int nsteps, bool zeroPhi) {
+  if (nsteps < 0) throw std::invalid_argument("cmg: negative step count");
+  const int nlev = numLevels();
+  if (src_.empty()) {
+    src_.resize(nlev);
+    for (int l = 0; l < nlev; ++l) src_[l] = alloc(amr_[l].nelem);
+  }
+  for (int l = 0; l < nlev; ++l) copyField(amrDev_[l], src_[l], lev_[l].rhs);
+  std::vector<SolveResult> out;
+  for (int n = 0; n < nsteps; ++n) {
+    // createEulerRHS, then phiNew = phiOld (in place), solveHelm.
+    for (int l = 0; l < nlev; ++l)
+      eulerRHS(lev_[l].rhs, lev_[l].phi, desc_.vc ? lev_[l].a : nullptr, src_[l], dt, amr_[l].nelem, s_);
+    setAlphaAndBeta(1.0, -dt);
+    out.push_back(solve(p, zeroPhi));
+  }
+  for (int l = 0; l < nlev; ++l) copyField(amrDev_[l], lev_[l].rhs, src_[l]);
+  ck(cudaStreamSynchronize(s_), "backward Euler");
+  return out;
 }
 
 void Solver::setRelaxMode(int mode) {

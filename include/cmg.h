@@ -123,6 +123,24 @@ int cmg_solve_mixed(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, i
 /* AMRMultiGrid::computeAMRResidual(phi, rhs, lmax, 0) (AMRMultiGrid.H:738-750). */
 int cmg_residual_norm(cmg_hierarchy* h, double* out);
 
+/* TGAHelmOp::setAlphaAndBeta on every operator of the hierarchy, as the
+ * reference's heat solvers call it (BackwardEuler::resetAlphaAndBeta,
+ * BackwardEuler.cpp:22-31): op 0 scales the coefficients given at creation
+ * (AMRPoissonOp.cpp:1103-1108: alpha = a_alpha * alpha0, beta = a_beta *
+ * beta0); op 1 takes them as given and recomputes the relaxation coefficient
+ * (VCAMRPoissonOp2.cpp:258-318) on every level and multigrid depth. */
+int cmg_set_alpha_beta(cmg_hierarchy* h, double alpha, double beta);
+/* nsteps backward-Euler steps of the heat equation (BackwardEuler::oneStep,
+ * BackwardEuler.cpp:156-189, createEulerRHS :190-226, solveHelm :228-245):
+ * phi is the state, the right-hand side set with cmg_set_rhs is the source.
+ * Each step forms rhs = a*phi + dt*src (a = 1 for op 0), calls
+ * setAlphaAndBeta(1, -dt) and solves (AMRMultiGrid::solve with p) for the new
+ * phi from the old one (zero_phi == 0, the heat solvers' choice) or from zero.
+ * exit_status and iterations (nsteps entries each, may be NULL) receive each
+ * step's solve; the source is left in the right-hand side afterwards. */
+int cmg_backward_euler(cmg_hierarchy* h, const cmg_solve_params* p, double dt, int nsteps, int zero_phi,
+                       int* exit_status, int* iterations);
+
 /* BiCGStab over the whole hierarchy, preconditioned by AMR multigrid: the
  * solve path of the reference's variable-coefficient example
  * (BiCGStabSolver<Vector<LevelData<FArrayBox>*>>::solve, BiCGStabSolver.H:

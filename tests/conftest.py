@@ -39,9 +39,14 @@ def golden(name):
 LARGE = {"config2_vc_3lev_256"}
 
 
+# Fixtures of the other solve paths (multilevel BiCGStab, backward Euler),
+# which reuse the hierarchies of the AMRMultiGrid fixtures.
+OTHER_PATHS = ("bicgstab_", "heat_")
+
+
 def golden_names():
-    """The AMRMultiGrid fixtures (the bicgstab_* ones are the multilevel BiCGStab solves)."""
-    names = sorted(f[:-5] for f in os.listdir(GOLDEN) if f.endswith(".json") and not f.startswith("bicgstab_"))
+    """The AMRMultiGrid fixtures."""
+    names = sorted(f[:-5] for f in os.listdir(GOLDEN) if f.endswith(".json") and not f.startswith(OTHER_PATHS))
     if os.environ.get("CMG_LARGE") != "1":
         names = [n for n in names if n not in LARGE]
     return names

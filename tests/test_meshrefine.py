@@ -11,10 +11,10 @@ import subprocess
 
 import pytest
 
-from conftest import GOLDEN, ROOT
+from conftest import GOLDEN, OTHER_PATHS, ROOT
 
 ORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle")
-FIXTURES = sorted(f[:-5] for f in os.listdir(GOLDEN) if f.endswith(".json") and not f.startswith("bicgstab_"))
+FIXTURES = sorted(f[:-5] for f in os.listdir(GOLDEN) if f.endswith(".json") and not f.startswith(OTHER_PATHS))
 
 
 @pytest.mark.parametrize("name", FIXTURES)

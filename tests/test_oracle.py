@@ -83,3 +83,26 @@ def test_bicgstab_oracle_reproduces_golden(tmp_path, name):
         n = sum((b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1) for b in boxes)
         assert np.array_equal(raw[pos:pos + n][::meta["sample_stride"]], arrays[f"phi{lev}"])
         pos += n
+
+
+HEATORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle_heat")
+
+
+@pytest.mark.skipif(not os.path.exists(HEATORACLE), reason="oracle not built (needs the reference tree)")
+@pytest.mark.parametrize("name", ["heat_poisson_1lev_32", "heat_vc_3lev_16"])
+def test_heat_oracle_reproduces_golden(tmp_path, name):
+    """The reference's BackwardEuler steps reproduce their fixture bit for bit."""
+    meta, arrays = golden(name)
+    base, _ = golden(meta["base"])
+    out = str(tmp_path / name)
+    grid = [a for a in base["args"].split() if a.split("=")[0] not in ("op", "alpha", "beta")]
+    subprocess.run([HEATORACLE] + grid + meta["heat_args"].split() + ["out=" + out], check=True,
+                   capture_output=True, timeout=300)
+    got = json.load(open(out + ".json"))
+    assert got["exit_status"] == meta["exit_status"] and got["iterations"] == meta["iterations"]
+    raw = np.fromfile(out + ".bin", dtype=np.float64)
+    pos = 0
+    for lev, boxes in enumerate(base["boxes"]):
+        n = sum((b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1) for b in boxes)
+        assert np.array_equal(raw[pos:pos + n], arrays[f"phi{lev}"])
+        pos += n

@@ -10,9 +10,9 @@ import os
 
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, OTHER_PATHS
 
-FIXTURES = sorted(f[:-5] for f in os.listdir(GOLDEN) if f.endswith(".json") and not f.startswith("bicgstab_"))
+FIXTURES = sorted(f[:-5] for f in os.listdir(GOLDEN) if f.endswith(".json") and not f.startswith(OTHER_PATHS))
 
 SWEEP = [
     dict(n0=48, levels=3, maxbox=16, block=8, fill=0.75, seed=7, thresh=0.1),

@@ -281,6 +281,15 @@ class Hierarchy:
                                         int(zero_phi), st, it))
         return [{"exit_status": st[n], "iterations": it[n]} for n in range(nsteps)]
 
+    def tga(self, params, dt, nsteps):
+        """nsteps AMRTGA::oneStep steps on phi with the right-hand side as the source (cmg_tga); returns the
+        2 * nsteps Helmholtz solves' exit status and iteration count."""
+        n = 2 * nsteps
+        st = (ctypes.c_int * max(n, 1))()
+        it = (ctypes.c_int * max(n, 1))()
+        _check(lib().cmg_tga(self.h, ctypes.byref(params), ctypes.c_double(dt), int(nsteps), st, it))
+        return [{"exit_status": st[k], "iterations": it[k]} for k in range(n)]
+
     def solve_bicgstab(self, params=None, zero_phi=True):
         """BiCGStab over MultilevelLinearOp preconditioned by AMR multigrid (cmg_solve_multilevel_bicgstab)."""
         p = params or mlsolve_params()

@@ -324,6 +324,38 @@ int cmg_set_alpha_beta(cmg_hierarchy* h, double alpha, double beta) {
   });
 }
 
+namespace {
+cmg::SolveParams solverParams(const cmg_solve_params* p) {
+  if (!p) throw std::invalid_argument("cmg: null parameters");
+  cmg::SolveParams sp;
+  sp.pre = p->pre;
+  sp.post = p->post;
+  sp.bottom = p->bottom;
+  sp.numMG = p->num_mg;
+  sp.iterMax = p->iter_max;
+  sp.imin = p->imin;
+  sp.eps = p->eps;
+  sp.hang = p->hang;
+  sp.normThresh = p->norm_thresh;
+  if (sp.pre < 0 || sp.post < 0 || sp.bottom < 0 || sp.numMG < 1 || sp.iterMax < 0)
+    throw std::invalid_argument("cmg: invalid solver parameters");
+  return sp;
+}
+}  // namespace
+
+int cmg_tga(cmg_hierarchy* h, const cmg_solve_params* p, double dt, int nsteps, int* exit_status,
+            int* iterations) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (nsteps < 0 || !(dt > 0)) throw std::invalid_argument("cmg: invalid time step");
+    std::vector<cmg::SolveResult> r = h->solver->tga(solverParams(p), dt, nsteps);
+    for (size_t n = 0; n < r.size(); ++n) {
+      if (exit_status) exit_status[n] = r[n].exitStatus;
+      if (iterations) iterations[n] = r[n].iterations;
+    }
+  });
+}
+
 int cmg_backward_euler(cmg_hierarchy* h, const cmg_solve_params* p, double dt, int nsteps, int zero_phi,
                        int* exit_status, int* iterations) {
   return guard([&]() {

@@ -77,6 +77,11 @@ template <class T> void zeroCovered(const LevelDev& L, T* f, cudaStream_t s);
 // rhs = ((0 + phi) * a) + ((0 + src) * dt), a == nullptr for no a-coefficient.
 void eulerRHS(double* rhs, const double* phi, const double* a, const double* src, double dt, int64_t n,
               cudaStream_t s);
+// TGA source term over a whole level array: out = (0 + src * 1) / a (no
+// division when a == nullptr).
+void tgaSource(double* out, const double* src, const double* a, int64_t n, cudaStream_t s);
+// x *= a elementwise over a whole level array.
+void multField(double* x, const double* a, int64_t n, cudaStream_t s);
 // x *= scale over a whole level array.
 void scaleField(double* x, double scale, int64_t n, cudaStream_t s);
 // out[b] = sum of x*y over the valid cells of box b, accumulated in the

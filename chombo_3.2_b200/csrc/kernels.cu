@@ -1011,6 +1011,34 @@ __global__ void k_euler_rhs(double* rhs, const double* phi, const double* a, con
   }
 }
 
+// AMRTGA::oneStep's source term: (0 + src * 1) / a (setToZero, incr,
+// divideByIdentityCoef; no division for the constant-coefficient operator).
+__global__ void k_tga_source(double* out, const double* src, const double* a, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0 + src[q] * 1.0;
+    if (a) v = v / a[q];
+    out[q] = v;
+  }
+}
+
+// x *= a (FArrayBox::mult by a FAB: the VC operator's diagonalScale).
+__global__ void k_mult_field(double* x, const double* a, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    x[q] = x[q] * a[q];
+}
+
+void tgaSource(double* out, const double* src, const double* a, int64_t n, cudaStream_t s) {
+  if (n == 0) return;
+  k_tga_source<<<flatBlocks(n), 256, 0, s>>>(out, src, a, n);
+  CMG_LAUNCHED("tgaSource");
+}
+
+void multField(double* x, const double* a, int64_t n, cudaStream_t s) {
+  if (n == 0) return;
+  k_mult_field<<<flatBlocks(n), 256, 0, s>>>(x, a, n);
+  CMG_LAUNCHED("multField");
+}
+
 void eulerRHS(double* rhs, const double* phi, const double* a, const double* src, double dt, int64_t n,
               cudaStream_t s) {
   if (n == 0) return;

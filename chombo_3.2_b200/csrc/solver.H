@@ -102,6 +102,11 @@ class Solver {
   // from phi_n (or from zero when zeroPhi).  The source is restored into the
   // right-hand side afterwards.  Returns each step's solve.
   std::vector<SolveResult> backwardEuler(const SolveParams& p, double dt, int nsteps, bool zeroPhi);
+  // nsteps steps of AMRTGA::oneStep (AMRTGA.H:420-560), the second-order
+  // Twizell-Gumel-Arigu scheme: two Helmholtz solves per step from the old
+  // phi, with phi the state and the right-hand side the source (restored
+  // afterwards).  Returns the 2 nsteps solves in order.
+  std::vector<SolveResult> tga(const SolveParams& p, double dt, int nsteps);
   // BiCGStab over MultilevelLinearOp (see MLSolveParams) from the current
   // phi, or from zero (ghost cells included) when zeroPhi.
   MLSolveResult solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroPhi = true);

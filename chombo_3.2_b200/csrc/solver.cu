@@ -779,6 +779,59 @@ std::vector<SolveResult> Solver::backwardEuler(const SolveParams& p, double dt, 
   return out;
 }
 
+std::vector<SolveResult> Solver::tga(const SolveParams& p, double dt, int nsteps) {
+  if (nsteps < 0) throw std::invalid_argument("cmg: negative step count");
+  const int nlev = numLevels();
+  // AMRTGA::setMu (AMRTGA.H:351-366).
+  const double tgaEpsilon = 1.e-12;
+  const double a = 2.0 - std::sqrt(2.0) - tgaEpsilon;
+  const double mu1 = (a - std::sqrt(a * a - 4.0 * a + 2.0)) / 2.0;
+  const double mu2 = (a + std::sqrt(a * a - 4.0 * a + 2.0)) / 2.0;
+  const double mu3 = (1.0 - a);
+  const double mu4 = 0.5 - a;
+  if (src_.empty()) {
+    src_.resize(nlev);
+    for (int l = 0; l < nlev; ++l) src_[l] = alloc(amr_[l].nelem);
+  }
+  for (int l = 0; l < nlev; ++l) copyField(amrDev_[l], src_[l], lev_[l].rhs);
+  MLVec phiOld = mlVec(0), srct = mlVec(1), rhst = mlVec(2);
+  MLVec phiNew(nlev), src(nlev);
+  for (int l = 0; l < nlev; ++l) {
+    phiNew[l] = lev_[l].phi;
+    src[l] = src_[l];
+  }
+  auto aCoef = [&](int l) -> const double* { return desc_.vc ? lev_[l].a : nullptr; };
+  std::vector<SolveResult> out;
+  for (int n = 0; n < nsteps; ++n) {
+    mlAssign(phiOld, phiNew);
+    for (int l = 0; l < nlev; ++l) tgaSource(srct[l], src[l], aCoef(l), amr_[l].nelem, s_);
+    // applyHelm(rhst, srct, mu4): (a I + mu4 dt L) S/a, then times dt.
+    setAlphaAndBeta(1.0, mu4 * dt);
+    mlApplyOp(rhst, srct);
+    mlScale(rhst, dt);
+    // applyHelm(phiNew, phiOld, mu3), added to rhst.
+    setAlphaAndBeta(1.0, mu3 * dt);
+    mlApplyOp(phiNew, phiOld);
+    mlIncr(rhst, phiNew, 1.0);
+    // solveHelm(phiNew, rhst, mu2) from phiOld.
+    mlAssign(phiNew, phiOld);
+    setAlphaAndBeta(1.0, -mu2 * dt);
+    for (int l = 0; l < nlev; ++l) copyField(amrDev_[l], lev_[l].rhs, rhst[l]);
+    out.push_back(solve(p, false));
+    // rhst = diagonalScale(phiNew); solveHelm(phiNew, rhst, mu1) from phiOld.
+    mlAssign(rhst, phiNew);
+    if (desc_.vc)
+      for (int l = 0; l < nlev; ++l) multField(rhst[l], lev_[l].a, amr_[l].nelem, s_);
+    mlAssign(phiNew, phiOld);
+    setAlphaAndBeta(1.0, -mu1 * dt);
+    for (int l = 0; l < nlev; ++l) copyField(amrDev_[l], lev_[l].rhs, rhst[l]);
+    out.push_back(solve(p, false));
+  }
+  for (int l = 0; l < nlev; ++l) copyField(amrDev_[l], lev_[l].rhs, src_[l]);
+  ck(cudaStreamSynchronize(s_), "TGA");
+  return out;
+}
+
 void Solver::setRelaxMode(int mode) {
   if (mode < 0 || mode > 2) throw std::invalid_argument("cmg: relaxation mode is 0 (tuned), 1 (fills) or 2 (inline)");
   relaxMode_ = mode;

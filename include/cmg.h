@@ -140,6 +140,16 @@ int cmg_set_alpha_beta(cmg_hierarchy* h, double alpha, double beta);
  * step's solve; the source is left in the right-hand side afterwards. */
 int cmg_backward_euler(cmg_hierarchy* h, const cmg_solve_params* p, double dt, int nsteps, int zero_phi,
                        int* exit_status, int* iterations);
+/* nsteps steps of the second-order TGA heat solver (AMRTGA<T>::oneStep,
+ * AMRTGA.H:420-560): per step the source term (a I + mu4 dt L) S/a and
+ * (a I + mu3 dt L) phi^n through the composite operator
+ * (AMRMultiGrid::computeAMROperator), then two Helmholtz solves
+ * (setAlphaAndBeta(1, -mu2 dt), then (1, -mu1 dt)) from the old phi, with
+ * the mu of AMRTGA::setMu.  phi is the state and the right-hand side the
+ * source, as for cmg_backward_euler; exit_status and iterations receive the
+ * 2 * nsteps solves in order. */
+int cmg_tga(cmg_hierarchy* h, const cmg_solve_params* p, double dt, int nsteps, int* exit_status,
+            int* iterations);
 
 /* BiCGStab over the whole hierarchy, preconditioned by AMR multigrid: the
  * solve path of the reference's variable-coefficient example

@@ -1,9 +1,9 @@
 """Regenerates the backward-Euler fixtures (heat_*.json|npz) from the reference oracle.
 
-oracle/_ref/cmg_oracle_heat runs the reference's BackwardEuler heat solver
-(lib/src/AMRElliptic/BackwardEuler.cpp over AMRMultiGrid), compiled from the
-reference's own sources (oracle/Makefile), for a few steps: the initial state
-and the source are the seeded right-hand side.  Each case uses the hierarchy
+oracle/_ref/cmg_oracle_heat runs the reference's BackwardEuler or AMRTGA heat
+solver (lib/src/AMRElliptic/BackwardEuler.cpp, AMRTGA.H, over AMRMultiGrid),
+compiled from the reference's own sources (oracle/Makefile), for a few steps:
+the initial state and the source are the seeded right-hand side.  Each case uses the hierarchy
 of an existing AMRMultiGrid fixture (same grid arguments and seed) with its
 own operator coefficients and time step, and records every step's exit
 status and V-cycle count and the final phi on every level.
@@ -26,6 +26,9 @@ CASES = {
     "heat_poisson_1lev_32": ("poisson_1lev_32", "op=0 alpha=1 beta=1 dt=1e-3 steps=3"),
     "heat_poisson_3lev_16": ("poisson_3lev_16", "op=0 alpha=1 beta=1 dt=1e-3 steps=3"),
     "heat_vc_3lev_16": ("vc_3lev_16", "op=1 alpha=1 beta=1 dt=1e-6 steps=3"),
+    "heat_tga_poisson_1lev_32": ("poisson_1lev_32", "op=0 alpha=1 beta=1 dt=1e-3 steps=2 scheme=tga"),
+    "heat_tga_poisson_3lev_16": ("poisson_3lev_16", "op=0 alpha=1 beta=1 dt=1e-3 steps=2 scheme=tga"),
+    "heat_tga_vc_3lev_16": ("vc_3lev_16", "op=1 alpha=1 beta=1 dt=1e-6 steps=2 scheme=tga"),
 }
 
 

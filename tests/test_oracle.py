@@ -89,7 +89,7 @@ HEATORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle_heat")
 
 
 @pytest.mark.skipif(not os.path.exists(HEATORACLE), reason="oracle not built (needs the reference tree)")
-@pytest.mark.parametrize("name", ["heat_poisson_1lev_32", "heat_vc_3lev_16"])
+@pytest.mark.parametrize("name", ["heat_poisson_1lev_32", "heat_vc_3lev_16", "heat_tga_vc_3lev_16"])
 def test_heat_oracle_reproduces_golden(tmp_path, name):
     """The reference's BackwardEuler steps reproduce their fixture bit for bit."""
     meta, arrays = golden(name)

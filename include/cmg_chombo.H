@@ -246,6 +246,9 @@ class GpuHierarchy {
 };
 
 class GpuAMRMultiGrid : private GpuHierarchy {
+  friend class GpuBackwardEuler;
+  friend class GpuAMRTGA;
+
  public:
   int m_exitStatus = 0;
   int m_verbosity = 0;
@@ -324,6 +327,63 @@ class GpuAMRMultiGrid : private GpuHierarchy {
       MayDay::Error("GpuAMRMultiGrid: the device solve uses BiCGStab as its bottom solver");
     defineFrom(a_coarseDomain, d, a_numLevels);
   }
+};
+
+// The reference's heat solvers over the GPU solve: BackwardEuler
+// (AMRElliptic/BackwardEuler.cpp) and AMRTGA<LevelData<FArrayBox>>
+// (AMRElliptic/AMRTGA.H), same constructor and oneStep arguments, built on a
+// GpuAMRMultiGrid (its solver parameters are the solves').  Each oneStep
+// moves phiOld and the source to the device, runs the step there
+// (cmg_backward_euler / cmg_tga) and returns phiNew; lbase 0 and
+// lmax = numLevels - 1 only.
+class GpuBackwardEuler {
+ public:
+  template <class Factory>
+  GpuBackwardEuler(const RefCountedPtr<GpuAMRMultiGrid>& a_solver, const Factory& /*a_opFact*/,
+                   const ProblemDomain& /*a_level0Domain*/, const Vector<int>& /*a_refRat*/, int /*a_numLevels*/ = -1,
+                   int /*a_verbosity*/ = 3)
+      : m_solver(a_solver) {}
+
+  void oneStep(Vector<LDF*>& a_phiNew, Vector<LDF*>& a_phiOld, Vector<LDF*>& a_source, const Real& a_dt,
+               int a_lbase, int a_lmax, bool a_zeroPhi = true) {
+    GpuAMRMultiGrid& s = *m_solver;
+    s.checkRange(a_lmax, a_lbase);
+    s.setLevels(a_phiOld, true);
+    s.setLevels(a_source, false);
+    int st = 0, it = 0;
+    GpuHierarchy::check(cmg_backward_euler(s.m_h, &s.m_p, a_dt, 1, a_zeroPhi ? 1 : 0, &st, &it));
+    s.m_exitStatus = st;
+    s.m_iterations = it;
+    s.getPhi(a_phiNew);
+  }
+
+ private:
+  RefCountedPtr<GpuAMRMultiGrid> m_solver;
+};
+
+class GpuAMRTGA {
+ public:
+  template <class Factory>
+  GpuAMRTGA(const RefCountedPtr<GpuAMRMultiGrid>& a_solver, const Factory& /*a_factory*/,
+            const ProblemDomain& /*a_level0Domain*/, const Vector<int>& /*a_refRat*/, int /*a_numLevels*/ = -1,
+            int /*a_verbosity*/ = 0)
+      : m_solver(a_solver) {}
+
+  void oneStep(Vector<LDF*>& a_phiNew, Vector<LDF*>& a_phiOld, Vector<LDF*>& a_source, const Real& a_dt,
+               int a_lbase, int a_lmax, Real /*a_timeOld*/ = 0) {
+    GpuAMRMultiGrid& s = *m_solver;
+    s.checkRange(a_lmax, a_lbase);
+    s.setLevels(a_phiOld, true);
+    s.setLevels(a_source, false);
+    int st[2] = {0, 0}, it[2] = {0, 0};
+    GpuHierarchy::check(cmg_tga(s.m_h, &s.m_p, a_dt, 1, st, it));
+    s.m_exitStatus = st[1];
+    s.m_iterations = it[1];
+    s.getPhi(a_phiNew);
+  }
+
+ private:
+  RefCountedPtr<GpuAMRMultiGrid> m_solver;
 };
 
 // MultilevelLinearOp<FArrayBox> (AMRElliptic/MultilevelLinearOp.H) for the

@@ -9,7 +9,8 @@
 //
 // Usage: dropin key=value ...   (n0 levels maxbox block op alpha beta seed
 // pre post bottom iters eps hang, as for cmg_oracle; bicgstab=1 mgiters
-// mgsmooth imax eps for the BiCGStab over MultilevelLinearOp path)
+// mgsmooth imax eps for the BiCGStab over MultilevelLinearOp path; heat=1
+// (backward Euler) or heat=2 (TGA) with dt steps for the heat solvers)
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -19,6 +20,8 @@
 
 #include "AMRMultiGrid.H"
 #include "AMRPoissonOp.H"
+#include "AMRTGA.H"
+#include "BackwardEuler.H"
 #include "BiCGStabSolver.H"
 #include "MultilevelLinearOp.H"
 #include "VCAMRPoissonOp2.H"
@@ -115,6 +118,94 @@ static int bicgstabCheck(OracleProblem& P, Vector<LDF*>& phiGpu, Vector<int>& rr
   return 0;
 }
 
+// The heat solvers (BackwardEuler, AMRTGA) on the CPU and through
+// cmg_chombo::GpuBackwardEuler / GpuAMRTGA with the same calls: the initial
+// state and the source are the seeded right-hand side (with one ghost layer).
+static int heatCheck(OracleProblem& P, Vector<LDF*>& phiGpu, Vector<int>& rr, bool tga) {
+  const int nlev = P.nlev, lmax = P.finest;
+  const int steps = (int)argd("steps", 2);
+  const Real dt = argd("dt", 1e-3);
+  const int pre = (int)argd("pre", 4), post = (int)argd("post", 4), bottom = (int)argd("bottom", 4);
+  const Real eps = argd("eps", 1e-10), hang = argd("hang", 1e-10);
+  Vector<LDF*> phiOld(nlev), phiNew(nlev), src(nlev), gOld(nlev);
+  for (int l = 0; l < nlev; ++l) {
+    phiOld[l] = new LDF(P.grids[l], 1, IntVect::Unit);
+    phiNew[l] = new LDF(P.grids[l], 1, IntVect::Unit);
+    src[l] = new LDF(P.grids[l], 1, IntVect::Unit);
+    gOld[l] = new LDF(P.grids[l], 1, IntVect::Unit);
+    for (DataIterator dit = P.grids[l].dataIterator(); dit.ok(); ++dit) {
+      for (LDF* f : {phiOld[l], phiNew[l], src[l], gOld[l], phiGpu[l]}) (*f)[dit()].setVal(0.0);
+      (*phiOld[l])[dit()].copy((*P.rhs[l])[dit()], P.grids[l][dit()]);
+      (*gOld[l])[dit()].copy((*P.rhs[l])[dit()], P.grids[l][dit()]);
+      (*src[l])[dit()].copy((*P.rhs[l])[dit()], P.grids[l][dit()]);
+    }
+  }
+  RefCountedPtr<AMRLevelOpFactory<LDF> > factory;
+  if (P.opType == 0) {
+    AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
+  } else {
+    VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
+  }
+  BiCGStabSolver<LDF> bottomSolver;
+  bottomSolver.m_verbosity = 0;
+  RefCountedPtr<AMRMultiGrid<LDF> > cpu(new AMRMultiGrid<LDF>());
+  cpu->define(P.domains[0], *factory, &bottomSolver, nlev);
+  cpu->setSolverParameters(pre, post, bottom, 1, 100, eps, hang, 1e-30);
+  cpu->m_verbosity = 0;
+  if (tga) {
+    cpu->init(phiNew, src, lmax, 0);
+    cpu->setBottomSolver(lmax, 0);
+    AMRTGA<LDF> t(cpu, *factory, P.domains[0], rr, nlev, 0);
+    for (int n = 0; n < steps; ++n) {
+      t.oneStep(phiNew, phiOld, src, dt, 0, lmax, 0.0);
+      std::swap(phiNew, phiOld);
+    }
+  } else {
+    BackwardEuler be(cpu, *factory, P.domains[0], rr, nlev, 0);
+    for (int n = 0; n < steps; ++n) {
+      be.oneStep(phiNew, phiOld, src, dt, 0, lmax, false);
+      std::swap(phiNew, phiOld);
+    }
+  }
+
+  RefCountedPtr<cmg_chombo::GpuAMRMultiGrid> gpu(new cmg_chombo::GpuAMRMultiGrid());
+  BiCGStabSolver<LDF> gpuBottom;
+  cmg_chombo::GpuAMRPoissonOpFactory pf;
+  cmg_chombo::GpuVCAMRPoissonOp2Factory vf;
+  if (P.opType == 0) {
+    pf.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    gpu->define(P.domains[0], pf, &gpuBottom, nlev);
+  } else {
+    vf.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    gpu->define(P.domains[0], vf, &gpuBottom, nlev);
+  }
+  gpu->setSolverParameters(pre, post, bottom, 1, 100, eps, hang, 1e-30);
+  if (tga) {
+    cmg_chombo::GpuAMRTGA t(gpu, pf, P.domains[0], rr, nlev, 0);
+    for (int n = 0; n < steps; ++n) {
+      t.oneStep(phiGpu, gOld, src, dt, 0, lmax, 0.0);
+      std::swap(phiGpu, gOld);
+    }
+  } else {
+    cmg_chombo::GpuBackwardEuler be(gpu, pf, P.domains[0], rr, nlev, 0);
+    for (int n = 0; n < steps; ++n) {
+      be.oneStep(phiGpu, gOld, src, dt, 0, lmax, false);
+      std::swap(phiGpu, gOld);
+    }
+  }
+  // the latest states are in phiOld (CPU) and gOld (GPU)
+  for (int l = 0; l < nlev; ++l) delete P.phi[l];
+  for (int l = 0; l < nlev; ++l) P.phi[l] = phiOld[l];
+  std::printf("{\"levels\": %d, \"scheme\": \"%s\", \"cpu_exit\": %d, \"gpu_exit\": %d, "
+              "\"phi_rel_dev\": %.3e}\n",
+              nlev, tga ? "tga" : "euler", cpu->m_exitStatus, gpu->m_exitStatus, phiDeviation(P, gOld));
+  return 0;
+}
+
 int main(int argc, char** argv) {
   for (int a = 1; a < argc; ++a) {
     const char* eq = std::strchr(argv[a], '=');
@@ -139,6 +230,7 @@ int main(int argc, char** argv) {
   for (int l = 0; l < nlev; ++l) phiGpu[l] = new LDF(P.grids[l], 1, IntVect::Unit);
   Vector<int> rr(nlev, 2);
   if (argd("bicgstab", 0) != 0) return bicgstabCheck(P, phiGpu, rr);
+  if (argd("heat", 0) != 0) return heatCheck(P, phiGpu, rr, argd("heat", 0) == 2);
 
   // Reference: CPU AMRMultiGrid.
   RefCountedPtr<AMRLevelOpFactory<LDF> > factory;

@@ -62,3 +62,24 @@ def test_dropin_bicgstab_matches_reference_solver(name):
     assert abs(out["gpu_r0"] - out["cpu_r0"]) <= TOL * out["cpu_r0"], out
     assert abs(out["gpu_rfinal"] - out["cpu_rfinal"]) <= TOL * out["cpu_r0"], out
     assert out["phi_rel_dev"] <= TOL, out
+
+
+HEAT_CASES = {
+    "euler_poisson_3lev_16": "n0=16 levels=3 maxbox=8 block=4 op=0 alpha=1 beta=1 heat=1 dt=1e-3 steps=2",
+    "tga_vc_3lev_16": "n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=1 heat=2 dt=1e-6 steps=2",
+    "tga_poisson_1lev_32": "n0=32 levels=1 maxbox=16 op=0 alpha=1 beta=1 heat=2 dt=1e-3 steps=2",
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(HEAT_CASES))
+def test_dropin_heat_matches_reference_solver(name):
+    """BackwardEuler / AMRTGA over AMRMultiGrid against cmg_chombo::GpuBackwardEuler / GpuAMRTGA over
+    GpuAMRMultiGrid with the same calls."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in check not built (make -C oracle dropin, needs the reference tree)")
+    r = subprocess.run([DROPIN] + HEAT_CASES[name].split(), capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["gpu_exit"] == out["cpu_exit"] == 1, out
+    assert out["phi_rel_dev"] <= TOL, out

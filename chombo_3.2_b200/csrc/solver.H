@@ -184,19 +184,25 @@ class Solver {
   void iterationBody(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi, std::vector<double*>& rhs);
   cudaGraphExec_t iterationGraph(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi,
                                  std::vector<double*>& rhs);
+  // Captured graphs hold the operator coefficients as kernel arguments, so
+  // alpha and beta are part of the key (setAlphaAndBeta switches between
+  // captured graphs instead of recapturing).
   struct GraphKey {
     bool mixed;
     int pre, post, bottom, numMG;
-    double eps;
+    double eps, alpha, beta;
     bool operator<(const GraphKey& o) const {
       if (mixed != o.mixed) return mixed < o.mixed;
       if (pre != o.pre) return pre < o.pre;
       if (post != o.post) return post < o.post;
       if (bottom != o.bottom) return bottom < o.bottom;
       if (numMG != o.numMG) return numMG < o.numMG;
-      return eps < o.eps;
+      if (eps != o.eps) return eps < o.eps;
+      if (alpha != o.alpha) return alpha < o.alpha;
+      return beta < o.beta;
     }
   };
+  static constexpr size_t kMaxGraphs = 16;  // cache bound (a new key past it drops the cache)
   std::map<GraphKey, cudaGraphExec_t> graphs_;
   std::map<cudaGraphExec_t, long long> graphLaunches_;  // kernel launches per replay
   bool useGraphs_ = false;
@@ -236,7 +242,7 @@ class Solver {
   void mlPreCondBody(MLVec& cor, MLVec& res, const MLSolveParams& p);
   // Captured preconditioner calls, per (correction, residual) vector pair and
   // smoothing parameters.
-  std::map<std::tuple<const void*, const void*, int, int>, cudaGraphExec_t> precondGraphs_;
+  std::map<std::tuple<const void*, const void*, int, int, double, double>, cudaGraphExec_t> precondGraphs_;
   void amrOperatorLevel(int ilev, int lmax, MLVec& lhs, MLVec& phi);
   void scatterValid(const LevelPlan& p, const LevelDev& d, double* dev, const double* src, bool onDevice,
                     int faceDir);

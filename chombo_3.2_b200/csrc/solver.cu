@@ -750,11 +750,6 @@ void Solver::setAlphaAndBeta(double alpha, double beta) {
     desc_.alpha = alpha * alpha0_;
     desc_.beta = beta * beta0_;
   }
-  // captured iterations hold the old coefficients
-  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
-  graphs_.clear();
-  for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
-  precondGraphs_.clear();
   ck(cudaStreamSynchronize(s_), "alpha and beta");
 }
 
@@ -1160,12 +1155,17 @@ void Solver::mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p) {
     mlPreCondBody(cor, res, p);
     return;
   }
-  const auto key = std::make_tuple((const void*)cor[0], (const void*)res[0], p.mgIters, p.mgSmooth);
+  const auto key = std::make_tuple((const void*)cor[0], (const void*)res[0], p.mgIters, p.mgSmooth, desc_.alpha,
+                                   desc_.beta);
   auto it = precondGraphs_.find(key);
   cudaGraphExec_t exec = nullptr;
   if (it != precondGraphs_.end()) {
     exec = it->second;
   } else {
+    if (precondGraphs_.size() >= kMaxGraphs) {
+      for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
+      precondGraphs_.clear();
+    }
     cudaGraph_t g = nullptr;
     const long long before = launchCount();
     ck(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -1420,9 +1420,13 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
 // device memory at run time.
 cudaGraphExec_t Solver::iterationGraph(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi,
                                        std::vector<double*>& rhs) {
-  GraphKey key{mixed, sp_.pre, sp_.post, sp_.bottom, sp_.numMG, sp_.eps};
+  GraphKey key{mixed, sp_.pre, sp_.post, sp_.bottom, sp_.numMG, sp_.eps, desc_.alpha, desc_.beta};
   auto it = graphs_.find(key);
   if (it != graphs_.end()) return it->second;
+  if (graphs_.size() >= kMaxGraphs) {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+  }
   cudaGraph_t g = nullptr;
   const long long before = launchCount();
   ck(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal), "begin capture");

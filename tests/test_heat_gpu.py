@@ -69,3 +69,19 @@ def test_set_alpha_beta_matches_a_fresh_hierarchy(cmg):
         assert np.array_equal(a.phi(lev), b.phi(lev))
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_tga_graph_replay_is_bit_identical(cmg):
+    """With CUDA graphs on, the TGA solves switch between graphs captured per (alpha, beta): same bits as launched."""
+    runs = []
+    for graphs in (False, True):
+        h, meta, arrays, base, dt, steps = setup(cmg, "heat_tga_vc_3lev_16")
+        h.use_graphs(graphs)
+        p = cmg.solve_params(pre=4, post=4, bottom=4, iter_max=100, eps=1e-10, hang=1e-10)
+        out = h.tga(p, dt, 3)
+        runs.append(([o["iterations"] for o in out], [h.phi(l) for l in range(len(base["boxes"]))]))
+        h.close()
+    assert runs[0][0] == runs[1][0]
+    for a, b in zip(runs[0][1], runs[1][1]):
+        assert np.array_equal(a, b)

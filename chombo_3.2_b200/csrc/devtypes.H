@@ -22,6 +22,10 @@ struct BoxDesc {
   int px, py;       // x pitch (even) and y extent (ny + 2) of the ghosted FAB
   int64_t off;      // element offset of the box's FAB
   int64_t half;     // elements per colour (px * py * (nz + 2) / 2)
+  // Division multipliers (divMagic) for the cell enumerations: by nx, by
+  // (nx + 1) / 2 and by ny; 0 where a box is too large for them (a plain
+  // division is used there).
+  uint64_t mNx, mHalf, mNy;
 };
 
 #if defined(__CUDACC__)
@@ -29,6 +33,19 @@ struct BoxDesc {
 #else
 #define CMG_HD inline
 #endif
+
+// ceil(2^32 / d): for 0 <= q < 2^32 / d, q / d == (q * divMagic(d)) >> 32
+// (the rounding error of the multiplier, below d, cannot carry into the
+// integer part for such q), which replaces the divide sequence of a runtime
+// divisor by one wide multiply.  qmax: the largest dividend; 0 (plain
+// division) when it is outside that range.
+CMG_HD uint64_t divMagic(int d, int64_t qmax) {
+  if (d < 1 || qmax < 0 || (uint64_t)qmax >= (uint64_t(1) << 32) / (uint64_t)d) return 0;
+  return ((uint64_t(1) << 32) + (uint64_t)d - 1) / (uint64_t)d;
+}
+CMG_HD int fastDiv(int q, int d, uint64_t m) {
+  return m ? (int)(((uint64_t)(unsigned)q * m) >> 32) : q / d;
+}
 
 // Slot of cell (i,j,k) within its colour half (x-neighbour pairs share it).
 CMG_HD int64_t colourSlot(const BoxDesc& b, int i, int j, int k) {
@@ -39,18 +56,20 @@ CMG_HD int64_t cellIndex(const BoxDesc& b, int i, int j, int k) {
   return b.off + ((i + j + k) & 1) * b.half + colourSlot(b, i, j, k);
 }
 
-// Element indices of a cell and of its six face neighbours.
+// Element indices of a cell and of its six face neighbours (a level holds
+// fewer than 2^31 elements, which the plan builder checks).
 struct Stencil {
-  int64_t c, xp, xm, yp, ym, zp, zm;
+  int c, xp, xm, yp, ym, zp, zm;
 };
 
 CMG_HD Stencil stencil(const BoxDesc& b, int i, int j, int k) {
   Stencil s;
   const int col = (i + j + k) & 1;
-  const int64_t m = colourSlot(b, i, j, k);
-  const int64_t own = b.off + col * b.half, oth = b.off + (1 - col) * b.half + m;
+  const int m = ((i - b.lo[0] + 1) + b.px * ((j - b.lo[1] + 1) + b.py * (k - b.lo[2] + 1))) >> 1;
+  const int off = (int)b.off, half = (int)b.half;
+  const int own = off + col * half, oth = off + (1 - col) * half + m;
   const int xo = (i - b.lo[0] + 1) & 1;  // x parity inside the FAB
-  const int64_t sy = b.px >> 1, sz = (int64_t)(b.px >> 1) * b.py;
+  const int sy = b.px >> 1, sz = (b.px >> 1) * b.py;
   s.c = own + m;
   s.xp = oth + xo;
   s.xm = oth + xo - 1;

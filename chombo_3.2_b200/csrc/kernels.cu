@@ -30,10 +30,11 @@ std::atomic<long long> g_launches{0};
 __device__ __forceinline__ bool allCell(const BoxDesc& b, int q, int& i, int& j, int& k) {
   int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
   if (q >= nx * ny * nz) return false;
-  i = b.lo[0] + q % nx;
-  int r = q / nx;
-  j = b.lo[1] + r % ny;
-  k = b.lo[2] + r / ny;
+  const int r = fastDiv(q, nx, b.mNx);
+  const int kk = fastDiv(r, ny, b.mNy);
+  i = b.lo[0] + (q - r * nx);
+  j = b.lo[1] + (r - kk * ny);
+  k = b.lo[2] + kk;
   return true;
 }
 
@@ -42,12 +43,13 @@ __device__ __forceinline__ bool allCell(const BoxDesc& b, int q, int& i, int& j,
 __device__ __forceinline__ bool colorCell(const BoxDesc& b, int q, int color, int& i, int& j, int& k) {
   int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
   int half = (nx + 1) / 2;
-  int r = q / half;
+  const int r = fastDiv(q, half, b.mHalf);
   if (r >= ny * nz) return false;
-  j = b.lo[1] + r % ny;
-  k = b.lo[2] + r / ny;
-  int par = ((b.lo[0] + j + k + color) % 2 + 2) % 2;
-  i = b.lo[0] + par + 2 * (q % half);
+  const int kk = fastDiv(r, ny, b.mNy);
+  j = b.lo[1] + (r - kk * ny);
+  k = b.lo[2] + kk;
+  const int par = (b.lo[0] + j + k + color) & 1;
+  i = b.lo[0] + par + 2 * (q - r * half);
   return i <= b.hi[0];
 }
 

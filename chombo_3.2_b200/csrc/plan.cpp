@@ -164,6 +164,15 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     d.py = bx.size(1) + 2;
     d.off = off;
     d.half = (int64_t)d.px * d.py * (bx.size(2) + 2) / 2;
+    {
+      // dividends: cell numbers of the box (plus the 256 threads of a
+      // chunk's tail) and row numbers (nx ... cells per row)
+      const int64_t nx = bx.size(0), ny = bx.size(1), nz = bx.size(2), half = (nx + 1) / 2;
+      const int64_t qmax = nx * ny * nz + CHUNK;
+      d.mNx = divMagic((int)nx, qmax);
+      d.mHalf = divMagic((int)half, qmax);
+      d.mNy = divMagic((int)ny, qmax);
+    }
     off += 2 * d.half;
     L.boxes.push_back(d);
   }

@@ -307,6 +307,80 @@ def batch_specs(n, seed):
     return specs
 
 
+def cpu_reference_sample(cmg, specs, processes):
+    """The reference solve (oracle/_ref/cmg_oracle, full solves to 1e-10) of a sample of independent problems on
+    the host cores, `processes` at a time, each from the product's grid generation (box lists identical to the
+    reference's BRMeshRefine).  Returns (solves/s over the wall time, wall seconds)."""
+    if not os.path.exists(ORACLE):
+        return None
+    jobs = []
+    for sp in specs:
+        boxes = cmg.synthetic_hierarchy(sp["n0"], sp["levels"], sp["max_box"], sp["block_factor"],
+                                        sp["fill_ratio"], sp["seed"], sp["thresh"])
+        bf = write_boxfile({"boxes": boxes})
+        jobs.append([ORACLE, f"n0={sp['n0']}", f"levels={len(boxes)}", f"maxbox={sp['max_box']}",
+                     f"block={sp['block_factor']}", f"op={sp['op']}", f"alpha={sp['alpha']}", f"beta={sp['beta']}",
+                     f"seed={sp['seed']}", f"eps={sp.get('eps', 1e-10)}", "dumpphi=0", f"boxfile={bf}",
+                     f"out={bf}.out"])
+    t0 = time.perf_counter()
+    running = []
+    for cmd in jobs:
+        running.append(subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+        if len(running) >= processes:
+            running.pop(0).wait()
+    for p in running:
+        p.wait()
+    wall = time.perf_counter() - t0
+    return len(jobs) / wall, wall
+
+
+def serving_stream(rate, n, seed):
+    """Open-loop request stream: exponential inter-arrival times at `rate`, levels U{1,2,3}, base n0
+    log-uniform in [32, 256] (x16), Poisson or VC Helmholtz and tolerance 1e-8 or 1e-10 with p = 1/2 each."""
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        n0 = min(256, round16(math.exp(rng.uniform(math.log(32), math.log(256)))))
+        vc = bool(rng.random() < 0.5)
+        eps = 1e-8 if rng.random() < 0.5 else 1e-10
+        reqs.append(dict(arrival=t, n0=n0, levels=int(rng.integers(1, 4)), max_box=32, block_factor=8,
+                         fill_ratio=0.75, thresh=0.1, seed=5000 + i, op=1 if vc else 0, alpha=1.0 if vc else 0.0,
+                         beta=-1.0 if vc else 1.0, eps=eps))
+    return reqs
+
+
+def run_reference_batch(args):
+    """Reference arm of the batch (config3) and serving (config4) workloads: the reference solve of a seeded
+    sample of their problems on the host cores (all cores for the batch, one at a time for serving, whose
+    reference baseline is sequential solves)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    if not os.path.exists(ORACLE):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cmg_oracle not built"}))
+        return
+    cmg = load_cmg()
+    if args.workload == "config3":
+        specs = batch_specs(args.batch, 20261203)[::16]
+        procs = max(1, min(os.cpu_count() or 1, 8))
+        name = f"{args.batch} independent 2-level hierarchies (sample of {len(specs)})"
+    else:
+        # the first requests of the lowest-rate stream, sized so the sample ends within minutes
+        specs = [q for q in serving_stream(50.0, args.requests, 50) if q["n0"] * q["levels"] <= 256][:6]
+        procs = 1
+        name = (f"open-loop serving requests (the first {len(specs)} of the 50 req/s stream with n0 x levels <= 256, "
+                "solved one at a time)")
+    rate, wall = cpu_reference_sample(cmg, specs, procs)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "solves/s", "n_gpus": args.gpus, "steps": 1,
+        "warmup": 0, "ms_per_step": 1000.0 * wall, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": name, "global_batch": len(specs), "parallelism": f"{procs} host processes"},
+        "cpu_baseline": {"value": rate, "unit": "solves/s", "cores": procs, "kind": "reference",
+                         "sample": f"{len(specs)} problems, full reference solves to 1e-10"},
+        "e2e": {"value": rate, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
 def run_batch(args):
     """Batching: N independent hierarchies resident on the GPU, solved
     concurrently (one stream each, every iteration a CUDA-graph replay,
@@ -356,6 +430,16 @@ def run_batch(args):
             h.close()
     value = len(specs) / t_batch
     base = len(specs) / t_seq
+    cpu = None
+    if not args.no_cpu_baseline:
+        procs = max(1, min(os.cpu_count() or 1, 8))
+        sample = specs[::16]
+        r = cpu_reference_sample(cmg, sample, procs)
+        if r:
+            cpu = {"value": r[0], "unit": "solves/s", "cores": procs, "kind": "reference",
+                   "sample": f"{len(sample)} of the {len(specs)} problems (every 16th), full reference solves to "
+                             f"1e-10, {procs} at a time on the host cores; rate = problems / wall time "
+                             f"({r[1]:.1f} s)"}
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": 0,
         "ms_per_step": 1000.0 * t_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -366,6 +450,7 @@ def run_batch(args):
                    "relax_mode": args.relax_mode,
                    "timing": "wall clock around the concurrent solves of each resident wave (host "
                              "set-up of the hierarchies not timed)"},
+        "cpu_baseline": cpu,
         "plain_fp64_one_at_a_time": {"value": base, "unit": "solves/s", "ratio": value / base},
         "vcycles_mixed_mean": float(np.mean(iters_mixed)), "vcycles_fp64_mean": float(np.mean(iters_fp64)),
         "not_converged": not_converged,
@@ -386,17 +471,9 @@ def run_serving(args):
     rates = [float(r) for r in args.rates.split(",")]
 
     def stream(rate, n, seed):
-        rng = np.random.default_rng(seed)
-        t, reqs = 0.0, []
-        for i in range(n):
-            t += rng.exponential(1.0 / rate)
-            n0 = min(256, round16(math.exp(rng.uniform(math.log(32), math.log(256)))))
-            vc = bool(rng.random() < 0.5)
-            eps = 1e-8 if rng.random() < 0.5 else 1e-10
-            reqs.append(dict(arrival=t, n0=n0, levels=int(rng.integers(1, 4)), max_box=32, block_factor=8,
-                             seed=5000 + i, op=1 if vc else 0, alpha=1.0 if vc else 0.0,
-                             beta=-1.0 if vc else 1.0, params=cmg.solve_params(eps=eps), mixed=True,
-                             graphs=True, device_tags=not args.host_tags))
+        reqs = serving_stream(rate, n, seed)
+        for q in reqs:
+            q.update(params=cmg.solve_params(eps=q["eps"]), mixed=True, graphs=True, device_tags=not args.host_tags)
         return reqs
 
     def stats(res, wall):
@@ -455,7 +532,9 @@ def main():
     ap.add_argument("--host-tags", action="store_true", help="config4: tag for grid generation on the host")
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per rate")
     args = ap.parse_args()
-    if args.impl != "reference" and args.workload in ("config3", "config4"):
+    if args.workload in ("config3", "config4"):
+        if args.impl == "reference":
+            return run_reference_batch(args)
         return run_batch(args) if args.workload == "config3" else run_serving(args)
     wl = WORKLOADS[args.workload]
     meta = golden_meta(wl["golden"])

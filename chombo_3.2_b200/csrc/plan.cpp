@@ -2,6 +2,10 @@
 // reproduces; the kernels then apply these tables without any geometry logic.
 #include "plan.H"
 
+#include <atomic>
+#include <exception>
+#include <thread>
+#include <algorithm>
 #include <map>
 #include <stdexcept>
 #include <unordered_map>
@@ -75,6 +79,31 @@ static int64_t faceSlot(const LevelPlan& L, size_t b, const IV& g, int& dir, int
          (int64_t)bx.size(t0) * (g[t1] - bx.lo[t1]);
 }
 
+// Runs fn(i) for every i in [0, n) on up to 16 host threads; the items must
+// write disjoint data.
+template <class F>
+void parallelItems(size_t n, F fn) {
+  const size_t nt = std::min<size_t>(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  if (nt <= 1) {
+    for (size_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::vector<std::exception_ptr> err(nt);
+  std::vector<std::thread> th;
+  for (size_t t = 0; t < nt; ++t)
+    th.emplace_back([&, t]() {
+      try {
+        for (size_t i = next++; i < n; i = next++) fn(i);
+      } catch (...) {
+        err[t] = std::current_exception();
+      }
+    });
+  for (auto& x : th) x.join();
+  for (auto& e : err)
+    if (e) std::rethrow_exception(e);
+}
+
 // Rules of every face-ghost cell from the level's ghost tasks (the fill with
 // coarse-fine values that precedes each relaxation pass).
 void buildFaceRules(LevelPlan& L) {
@@ -92,7 +121,9 @@ void buildFaceRules(LevelPlan& L) {
   }
   L.faceOff[6 * L.grids.size()] = (int)off;
   L.faceRules.assign((size_t)off, FaceRule{0, FR_FAB});
-  for (size_t b = 0; b < L.grids.size(); ++b) {
+  // Boxes write their own slots, and ghost tasks disjoint ghost regions, so
+  // both loops run on host threads.
+  parallelItems(L.grids.size(), [&](size_t b) {
     const Box& bx = L.grids[b];
     for (int d = 0; d < 3; ++d) {
       const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
@@ -107,8 +138,9 @@ void buildFaceRules(LevelPlan& L) {
             L.faceRules[faceSlot(L, b, g, dd, ss)].src = (int)cellOf(L, (int)b, g);
           }
     }
-  }
-  for (const GhostTask& t : L.ghost) {
+  });
+  parallelItems(L.ghost.size(), [&](size_t ti) {
+    const GhostTask& t = L.ghost[ti];
     for (int k = t.lo[2]; k <= t.hi[2]; ++k)
       for (int j = t.lo[1]; j <= t.hi[1]; ++j)
         for (int i = t.lo[0]; i <= t.hi[0]; ++i) {
@@ -129,7 +161,7 @@ void buildFaceRules(LevelPlan& L) {
             r = FaceRule{(int)cellOf(L, t.dst, IV(i + e[0], j + e[1], k + e[2])), FR_CFQUAD};
           }
         }
-  }
+  });
 }
 
 std::vector<int> blockTasks(const std::vector<int>& start) {
@@ -239,8 +271,37 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
   L.ghostBlock = blockTasks(L.ghostStart);
   buildFaceRules(L);
   if (L.nelem >= ((int64_t)1 << 31)) throw std::runtime_error("cmg: level too large for 32-bit ghost indices");
-  L.gcells.clear();
-  auto emit = [&](const GhostTask& t, int par) {
+  // Flat lists: per parity the exchange and boundary tasks, then the
+  // coarse-fine ones, each task's cells of that parity in k, j, i order.
+  // Counts first, then every task fills its own range on host threads.
+  const size_t ntask = L.ghost.size();
+  auto parityCount = [](const GhostTask& t, int par) {
+    int64_t n = 0;
+    const int nx = t.hi[0] - t.lo[0] + 1;
+    for (int k = t.lo[2]; k <= t.hi[2]; ++k)
+      for (int j = t.lo[1]; j <= t.hi[1]; ++j) {
+        const int first = ((t.lo[0] + j + k) & 1) == par ? 0 : 1;  // offset of the row's first cell of parity par
+        n += nx > first ? (nx - first + 1) / 2 : 0;
+      }
+    return n;
+  };
+  std::vector<int64_t> start(2 * ntask + 1, 0);
+  {
+    int64_t pos = 0;
+    for (int par = 0; par < 2; ++par) {
+      L.gcStart[par] = (int)pos;
+      for (size_t t = 0; t < ntask; ++t) {
+        if (t == (size_t)L.nExchBC) L.gcExch[par] = (int)(pos - L.gcStart[par]);
+        start[par * ntask + t] = pos;
+        pos += parityCount(L.ghost[t], par);
+      }
+      if (ntask <= (size_t)L.nExchBC) L.gcExch[par] = (int)(pos - L.gcStart[par]);
+      L.gcCF[par] = (int)(pos - L.gcStart[par] - L.gcExch[par]);
+    }
+    start[2 * ntask] = pos;
+    L.gcells.assign((size_t)pos, GhostCell{0, 0, 0});
+  }
+  auto emit = [&](const GhostTask& t, int par, int64_t at) {
     const BoxDesc& db = L.boxes[t.dst];
     for (int k = t.lo[2]; k <= t.hi[2]; ++k)
       for (int j = t.lo[1]; j <= t.hi[1]; ++j)
@@ -258,16 +319,16 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
             g.s2 = t.kind == G_BC ? -2 : t.kind == G_CFLIN ? -3
                                    : (int)cellIndex(db, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
           }
-          L.gcells.push_back(g);
+          L.gcells[at++] = g;
         }
+    if (at != start[par * ntask + (&t - L.ghost.data()) + 1] && (size_t)(&t - L.ghost.data()) + 1 < ntask)
+      throw std::logic_error("cmg: ghost-cell count mismatch");
   };
-  for (int par = 0; par < 2; ++par) {
-    L.gcStart[par] = (int)L.gcells.size();
-    for (int t = 0; t < L.nExchBC; ++t) emit(L.ghost[t], par);
-    L.gcExch[par] = (int)L.gcells.size() - L.gcStart[par];
-    for (size_t t = L.nExchBC; t < L.ghost.size(); ++t) emit(L.ghost[t], par);
-    L.gcCF[par] = (int)L.gcells.size() - L.gcStart[par] - L.gcExch[par];
-  }
+  parallelItems(2 * ntask, [&](size_t q) {
+    const int par = (int)(q / ntask);
+    const size_t t = q % ntask;
+    emit(L.ghost[t], par, start[q]);
+  });
   L.slotStart.assign(1, 0);
   for (const GhostTask& t : L.ghost)
     L.slotStart.push_back(L.slotStart.back() + (int)colourSlots(t.lo, t.hi, parityAxis(t.lo, t.hi)));
@@ -443,6 +504,138 @@ void buildIrregularDir(const IV& iv, int ivec, int dir, const CellSet& good, Coa
 
 }  // namespace
 
+// Tables of one fine box: CFCoarse pool starts relative to its own pool,
+// CFFine coarse indices relative to its own CFCoarse list.
+struct QuadCFPart {
+  std::vector<CFCoarse> coarse;
+  std::vector<CFFine> fine;
+  std::vector<double> w;
+  std::vector<int64_t> off;
+};
+
+void buildQuadCFBox(const LevelPlan& F, const LevelPlan& C, const OwnerIndex& owner, const Layout& cfine,
+                    const BoxIndex& cfineIndex, size_t fb, QuadCFPart& out) {
+  std::vector<int> hits;
+  const double dxf = F.dx;
+  const double dxc = 2 * dxf;
+  auto pushPool = [&](const std::vector<IV>& cells, const std::vector<double>* w) {
+    int start = (int)out.off.size();
+    for (size_t i = 0; i < cells.size(); ++i) {
+      out.off.push_back(owner.cell(cells[i]));
+      out.w.push_back(w ? (*w)[i] : 0.0);
+    }
+    return start;
+  };
+  const Box& fbox = F.grids[fb];
+  for (int d = 0; d < 3; ++d) {
+    int t[2], it = 0;
+    for (int k = 0; k < 3; ++k)
+      if (k != d) t[it++] = k;
+    for (int side = -1; side <= 1; side += 2) {
+      CellSet fineIVS;
+      if (!faceCFSet(F, fbox, d, side, fineIVS)) continue;
+      Box packedBox = fineIVS.minBox();
+      bool packed = (packedBox.numPts() == fineIVS.numPts());
+      CellSet base = fineIVS.coarsen(2);
+      base.intersect(C.domain);
+      // Good set: coarse cells of the widened face slab that are valid on
+      // the coarse level and not under the fine level
+      // (QuadCFStencil::define, AMRTools/QuadCFStencil.cpp:500-660).
+      Box cgrid = fbox.coarsen(2);
+      Box g2 = cgrid.adjCell(d, side, 1), g1 = g2;
+      for (int k = 0; k < 2; ++k) {
+        g2 = g2.grow(t[k], 2);
+        g1 = g1.grow(t[k], 1);
+      }
+      g2 = g2 & C.domain;
+      g1 = g1 & C.domain;
+      CellSet good(g2, false);
+      C.index.query(C.grids.boxes, g2, hits);
+      for (int k : hits) good.set(C.grids[k], true);
+      cfineIndex.query(cfine.boxes, g2, hits);
+      for (int k : hits) good.subtract(cfine[k]);
+      CellSet standard = good;
+      standard.intersect(g1);
+      standard = standard.erode(t[0]).erode(t[1]);
+      // Irregular stencils for base cells outside the standard set.
+      // CFCoarse entry of each base cell (dense over the base set's box)
+      std::vector<int> coarseIndex((size_t)base.dom.numPts(), -1);
+      std::vector<IV> baseCells = base.cells();
+      std::vector<CoarseStencils> irr(baseCells.size());
+      for (size_t i = 0; i < baseCells.size(); ++i)
+        if (!standard.contains(baseCells[i])) buildIrregular(baseCells[i], t, good, irr[i]);
+      for (int ivec = 0; ivec < 2; ++ivec)
+        for (size_t i = 0; i < baseCells.size(); ++i)
+          if (!standard.contains(baseCells[i])) buildIrregularDir(baseCells[i], ivec, t[ivec], good, irr[i]);
+      for (size_t i = 0; i < baseCells.size(); ++i) {
+        const IV& c = baseCells[i];
+        CFCoarse e;
+        e.cc = owner.cell(c);
+        if (standard.contains(c)) {
+          for (int k = 0; k < 2; ++k) {
+            IV ek = IV::basis(t[k]);
+            e.d1[k] = CFDeriv{1, 2, pushPool({c - ek, c + ek}, nullptr)};
+            e.d2[k] = CFDeriv{1, 3, pushPool({c - ek, c + ek, c}, nullptr)};
+          }
+          // computeMixedDerivative: basex = e(t[0]), basey = e(t[1]).
+          IV bx = IV::basis(t[0]), by = IV::basis(t[1]);
+          e.mx = CFDeriv{1, 4, pushPool({c + bx + by, c - bx + by, c + bx - by, c - bx - by}, nullptr)};
+        } else {
+          const CoarseStencils& cs = irr[i];
+          for (int k = 0; k < 2; ++k) {
+            e.d1[k] = CFDeriv{2, (int)cs.first[k].iv.size(), pushPool(cs.first[k].iv, &cs.first[k].w)};
+            if (cs.drop)
+              e.d2[k] = CFDeriv{0, 0, 0};
+            else
+              e.d2[k] = CFDeriv{2, (int)cs.second[k].iv.size(), pushPool(cs.second[k].iv, &cs.second[k].w)};
+          }
+          if (cs.drop)
+            e.mx = CFDeriv{0, 0, 0};
+          else
+            e.mx = CFDeriv{2, (int)cs.mixed.iv.size(), pushPool(cs.mixed.iv, &cs.mixed.w)};
+        }
+        coarseIndex[base.at(c)] = (int)out.coarse.size();
+        out.coarse.push_back(e);
+      }
+      // Fine ghost cells.  Packed faces follow the Fortran PHISTAR index
+      // shift (QuadCFInterp.cpp:680-712, QuadCFInterpF.ChF:50-126).
+      IV shift = packedBox.lo;
+      shift[d] += side;
+      for (const IV& f : fineIVS.cells()) {
+        IV c(floordiv(f[0], 2), floordiv(f[1], 2), floordiv(f[2], 2));
+        CFFine ff;
+        ff.g = cellOf(F, (int)fb, f);
+        ff.pb = cellOf(F, (int)fb, f - IV::basis(d, side));
+        ff.pa = cellOf(F, (int)fb, f - IV::basis(d, 2 * side));
+        ff.coarse = coarseIndex[base.at(c)];
+        if (ff.coarse < 0) throw std::runtime_error("cmg: fine ghost without coarse stencil");
+        ff.packed = packed ? 1 : 0;
+        double xs[2];
+        for (int k = 0; k < 2; ++k) {
+          int you = t[k];
+          if (packed) {
+            int ir = f[you] - shift[you];
+            int ic = ir / 2;
+            double xf = (ir + 0.5) * dxf;
+            double xc = (ic + 0.5) * dxc;
+            xs[k] = xf - xc;
+          } else {
+            double xf = (f[you] + 0.5) * dxf;
+            double xc = (c[you] + 0.5) * dxc;
+            xs[k] = xf - xc;
+          }
+        }
+        ff.x1 = xs[0];
+        ff.x2 = xs[1];
+        out.fine.push_back(ff);
+      }
+    }
+  }
+}
+
+// The fine boxes are independent: built on host threads, then concatenated in
+// box order with their pool and coarse-entry indices shifted (the same tables
+// as one pass over the boxes).
 void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
   F.cfCoarse.clear();
   F.cfFine.clear();
@@ -452,123 +645,52 @@ void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
   Layout cfine = F.grids.coarsen(2);
   BoxIndex cfineIndex;
   cfineIndex.build(cfine.boxes);
-  std::vector<int> hits;
-  const double dxf = F.dx;
-  const double dxc = 2 * dxf;
-  auto pushPool = [&](const std::vector<IV>& cells, const std::vector<double>* w) {
-    int start = (int)F.cfOff.size();
-    for (size_t i = 0; i < cells.size(); ++i) {
-      F.cfOff.push_back(owner.cell(cells[i]));
-      F.cfW.push_back(w ? (*w)[i] : 0.0);
-    }
-    return start;
-  };
-  for (size_t fb = 0; fb < F.grids.size(); ++fb) {
-    const Box& fbox = F.grids[fb];
-    for (int d = 0; d < 3; ++d) {
-      int t[2], it = 0;
-      for (int k = 0; k < 3; ++k)
-        if (k != d) t[it++] = k;
-      for (int side = -1; side <= 1; side += 2) {
-        CellSet fineIVS;
-        if (!faceCFSet(F, fbox, d, side, fineIVS)) continue;
-        Box packedBox = fineIVS.minBox();
-        bool packed = (packedBox.numPts() == fineIVS.numPts());
-        CellSet base = fineIVS.coarsen(2);
-        base.intersect(C.domain);
-        // Good set: coarse cells of the widened face slab that are valid on
-        // the coarse level and not under the fine level
-        // (QuadCFStencil::define, AMRTools/QuadCFStencil.cpp:500-660).
-        Box cgrid = fbox.coarsen(2);
-        Box g2 = cgrid.adjCell(d, side, 1), g1 = g2;
-        for (int k = 0; k < 2; ++k) {
-          g2 = g2.grow(t[k], 2);
-          g1 = g1.grow(t[k], 1);
-        }
-        g2 = g2 & C.domain;
-        g1 = g1 & C.domain;
-        CellSet good(g2, false);
-        C.index.query(C.grids.boxes, g2, hits);
-        for (int k : hits) good.set(C.grids[k], true);
-        cfineIndex.query(cfine.boxes, g2, hits);
-        for (int k : hits) good.subtract(cfine[k]);
-        CellSet standard = good;
-        standard.intersect(g1);
-        standard = standard.erode(t[0]).erode(t[1]);
-        // Irregular stencils for base cells outside the standard set.
-        // CFCoarse entry of each base cell (dense over the base set's box)
-        std::vector<int> coarseIndex((size_t)base.dom.numPts(), -1);
-        std::vector<IV> baseCells = base.cells();
-        std::vector<CoarseStencils> irr(baseCells.size());
-        for (size_t i = 0; i < baseCells.size(); ++i)
-          if (!standard.contains(baseCells[i])) buildIrregular(baseCells[i], t, good, irr[i]);
-        for (int ivec = 0; ivec < 2; ++ivec)
-          for (size_t i = 0; i < baseCells.size(); ++i)
-            if (!standard.contains(baseCells[i])) buildIrregularDir(baseCells[i], ivec, t[ivec], good, irr[i]);
-        for (size_t i = 0; i < baseCells.size(); ++i) {
-          const IV& c = baseCells[i];
-          CFCoarse e;
-          e.cc = owner.cell(c);
-          if (standard.contains(c)) {
-            for (int k = 0; k < 2; ++k) {
-              IV ek = IV::basis(t[k]);
-              e.d1[k] = CFDeriv{1, 2, pushPool({c - ek, c + ek}, nullptr)};
-              e.d2[k] = CFDeriv{1, 3, pushPool({c - ek, c + ek, c}, nullptr)};
-            }
-            // computeMixedDerivative: basex = e(t[0]), basey = e(t[1]).
-            IV bx = IV::basis(t[0]), by = IV::basis(t[1]);
-            e.mx = CFDeriv{1, 4, pushPool({c + bx + by, c - bx + by, c + bx - by, c - bx - by}, nullptr)};
-          } else {
-            const CoarseStencils& cs = irr[i];
-            for (int k = 0; k < 2; ++k) {
-              e.d1[k] = CFDeriv{2, (int)cs.first[k].iv.size(), pushPool(cs.first[k].iv, &cs.first[k].w)};
-              if (cs.drop)
-                e.d2[k] = CFDeriv{0, 0, 0};
-              else
-                e.d2[k] = CFDeriv{2, (int)cs.second[k].iv.size(), pushPool(cs.second[k].iv, &cs.second[k].w)};
-            }
-            if (cs.drop)
-              e.mx = CFDeriv{0, 0, 0};
-            else
-              e.mx = CFDeriv{2, (int)cs.mixed.iv.size(), pushPool(cs.mixed.iv, &cs.mixed.w)};
-          }
-          coarseIndex[base.at(c)] = (int)F.cfCoarse.size();
-          F.cfCoarse.push_back(e);
-        }
-        // Fine ghost cells.  Packed faces follow the Fortran PHISTAR index
-        // shift (QuadCFInterp.cpp:680-712, QuadCFInterpF.ChF:50-126).
-        IV shift = packedBox.lo;
-        shift[d] += side;
-        for (const IV& f : fineIVS.cells()) {
-          IV c(floordiv(f[0], 2), floordiv(f[1], 2), floordiv(f[2], 2));
-          CFFine ff;
-          ff.g = cellOf(F, (int)fb, f);
-          ff.pb = cellOf(F, (int)fb, f - IV::basis(d, side));
-          ff.pa = cellOf(F, (int)fb, f - IV::basis(d, 2 * side));
-          ff.coarse = coarseIndex[base.at(c)];
-          if (ff.coarse < 0) throw std::runtime_error("cmg: fine ghost without coarse stencil");
-          ff.packed = packed ? 1 : 0;
-          double xs[2];
-          for (int k = 0; k < 2; ++k) {
-            int you = t[k];
-            if (packed) {
-              int ir = f[you] - shift[you];
-              int ic = ir / 2;
-              double xf = (ir + 0.5) * dxf;
-              double xc = (ic + 0.5) * dxc;
-              xs[k] = xf - xc;
-            } else {
-              double xf = (f[you] + 0.5) * dxf;
-              double xc = (c[you] + 0.5) * dxc;
-              xs[k] = xf - xc;
-            }
-          }
-          ff.x1 = xs[0];
-          ff.x2 = xs[1];
-          F.cfFine.push_back(ff);
+  const size_t nb = F.grids.size();
+  std::vector<QuadCFPart> parts(nb);
+  std::vector<std::exception_ptr> err(nb);
+  const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  std::atomic<size_t> next{0};
+  for (unsigned t = 0; t < nt; ++t)
+    th.emplace_back([&]() {
+      for (size_t fb = next++; fb < nb; fb = next++) {
+        try {
+          buildQuadCFBox(F, C, owner, cfine, cfineIndex, fb, parts[fb]);
+        } catch (...) {
+          err[fb] = std::current_exception();
         }
       }
+    });
+  for (auto& x : th) x.join();
+  for (auto& e : err)
+    if (e) std::rethrow_exception(e);
+  size_t nc = 0, nf = 0, np = 0;
+  for (const QuadCFPart& p : parts) {
+    nc += p.coarse.size();
+    nf += p.fine.size();
+    np += p.off.size();
+  }
+  F.cfCoarse.reserve(nc);
+  F.cfFine.reserve(nf);
+  F.cfW.reserve(np);
+  F.cfOff.reserve(np);
+  for (size_t fb = 0; fb < nb; ++fb) {
+    QuadCFPart& p = parts[fb];
+    const int coarseBase = (int)F.cfCoarse.size(), poolBase = (int)F.cfOff.size();
+    for (CFCoarse e : p.coarse) {
+      for (int k = 0; k < 2; ++k) {
+        if (e.d1[k].kind) e.d1[k].start += poolBase;
+        if (e.d2[k].kind) e.d2[k].start += poolBase;
+      }
+      if (e.mx.kind) e.mx.start += poolBase;
+      F.cfCoarse.push_back(e);
     }
+    for (CFFine f : p.fine) {
+      f.coarse += coarseBase;
+      F.cfFine.push_back(f);
+    }
+    F.cfW.insert(F.cfW.end(), p.w.begin(), p.w.end());
+    F.cfOff.insert(F.cfOff.end(), p.off.begin(), p.off.end());
   }
 }
 

@@ -325,13 +325,20 @@ __global__ void __launch_bounds__(1024) k_relax_block(const BoxDesc* boxes, cons
 // OPERATORLAPRES / OPERATORLAP (AMRPoissonOpF.ChF:287-377) and
 // VCCOMPUTERES3D / VCCOMPUTEOP3D (VCAMRPoissonOpF.ChF:148-312).
 // mode 0: r = rhs - L(phi) (residual form), mode 1: r = L(phi).
+// Each block takes half a colour chunk of both colours: threads 0-127 the
+// colour-0 cells of 128 consecutive slots, threads 128-255 the colour-1 cells
+// of the same slots (the two colour chunk lists of a box have the same
+// boundaries).  Every warp reads one colour half of each array, and the
+// block's two halves read each other's cells as neighbours from L1.
 template <class T, int VC, int MODE>
-__global__ void k_op(const BoxDesc* boxes, const Chunk* chunks, T* r, const T* phi, const T* rhs, Scal sc,
-                     const T* a, const T* b0, const T* b1, const T* b2) {
-  Chunk ch = chunks[blockIdx.x];
+__global__ void k_op(const BoxDesc* boxes, const Chunk* ch0, const Chunk* ch1, T* r, const T* phi, const T* rhs,
+                     Scal sc, const T* a, const T* b0, const T* b1, const T* b2) {
+  const int color = threadIdx.x >= CHUNK / 2;
+  Chunk ch = (color ? ch1 : ch0)[blockIdx.x >> 1];
   const BoxDesc bd = boxes[ch.box];
   int i, j, k;
-  if (!allCell(bd, ch.start + threadIdx.x, i, j, k)) return;
+  if (!colorCell(bd, ch.start + (blockIdx.x & 1) * (CHUNK / 2) + (threadIdx.x & (CHUNK / 2 - 1)), color, i, j, k))
+    return;
   const Stencil st = stencil(bd, i, j, k);
   const int64_t c = st.c;
   const T dxinv = T(sc.dxinv);
@@ -1115,10 +1122,13 @@ template <class T>
 void residual(const LevelDev& L, T* r, const T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s) {
   if (L.nAll == 0) return;
   Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
+  const int n = 2 * L.nColor[0];
   if (c.vc)
-    k_op<T, 1, 0><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, r, phi, rhs, sc, c.a, c.b[0], c.b[1], c.b[2]);
+    k_op<T, 1, 0><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], r, phi, rhs, sc, c.a, c.b[0], c.b[1],
+                                      c.b[2]);
   else
-    k_op<T, 0, 0><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, r, phi, rhs, sc, nullptr, nullptr, nullptr, nullptr);
+    k_op<T, 0, 0><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], r, phi, rhs, sc, nullptr, nullptr,
+                                      nullptr, nullptr);
   CMG_LAUNCHED("residual");
 }
 
@@ -1126,11 +1136,13 @@ template <class T>
 void applyOp(const LevelDev& L, T* lofphi, const T* phi, const Coef<T>& c, cudaStream_t s) {
   if (L.nAll == 0) return;
   Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
+  const int n = 2 * L.nColor[0];
   if (c.vc)
-    k_op<T, 1, 1><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lofphi, phi, nullptr, sc, c.a, c.b[0], c.b[1], c.b[2]);
+    k_op<T, 1, 1><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], lofphi, phi, nullptr, sc, c.a, c.b[0],
+                                      c.b[1], c.b[2]);
   else
-    k_op<T, 0, 1><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, lofphi, phi, nullptr, sc, nullptr, nullptr, nullptr,
-                                           nullptr);
+    k_op<T, 0, 1><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], lofphi, phi, nullptr, sc, nullptr,
+                                      nullptr, nullptr, nullptr);
   CMG_LAUNCHED("applyOp");
 }
 

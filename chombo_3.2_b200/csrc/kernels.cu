@@ -558,12 +558,15 @@ __global__ void k_prolongamr(const BoxDesc* fboxes, const BoxDesc* cboxes, const
                              const Chunk* chunks, T* fine, const T* coarse) {
   Chunk ch = chunks[blockIdx.x];
   const CoarseFineItem it = items[ch.box];
-  int q = ch.start + threadIdx.x;
-  int nx = it.hi[0] - it.lo[0] + 1, ny = it.hi[1] - it.lo[1] + 1, nz = it.hi[2] - it.lo[2] + 1;
-  int cq = q >> 3, sub = q & 7;
-  if (cq >= nx * ny * nz) return;
-  int I = it.lo[0] + cq % nx, r = cq / nx, J = it.lo[1] + r % ny, K = it.lo[2] + r / ny;
-  int64_t f = cellIndex(fboxes[it.fbox], 2 * I + (sub & 1), 2 * J + ((sub >> 1) & 1), 2 * K + (sub >> 2));
+  const int q = ch.start + threadIdx.x;
+  // fine cells of the item's region in x-fastest order: a warp covers a fine
+  // row segment and the coarse row segment above it
+  const int fnx = 2 * (it.hi[0] - it.lo[0] + 1), fny = 2 * (it.hi[1] - it.lo[1] + 1);
+  const int fnz = 2 * (it.hi[2] - it.lo[2] + 1);
+  if (q >= fnx * fny * fnz) return;
+  const int r = q / fnx, fi = q - r * fnx, fk = r / fny, fj = r - fk * fny;
+  const int I = it.lo[0] + (fi >> 1), J = it.lo[1] + (fj >> 1), K = it.lo[2] + (fk >> 1);
+  int64_t f = cellIndex(fboxes[it.fbox], 2 * it.lo[0] + fi, 2 * it.lo[1] + fj, 2 * it.lo[2] + fk);
   fine[f] = fine[f] + coarse[cellIndex(cboxes[it.cbox], I, J, K)];
 }
 

@@ -744,14 +744,24 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
   Layout cfine = F.grids.coarsen(2);
   CellSet covered(C.domain, false);
   for (const Box& b : cfine.boxes) covered.set(b, true);
-  for (size_t cb = 0; cb < C.grids.size(); ++cb) {
+  // Coarse boxes are independent: each builds its cells with pool starts
+  // relative to its own pools on a host thread; the parts are concatenated
+  // in box order (the same tables as one pass over the boxes).
+  struct Part {
+    std::vector<RefluxCell> cells;
+    std::vector<RefluxCoarseTerm> co;
+    std::vector<RefluxFineGroup> fi;
+  };
+  std::vector<Part> parts(C.grids.size());
+  parallelItems(C.grids.size(), [&](size_t cb) {
+    Part& out = parts[cb];
     const Box& cbox = C.grids[cb];
     // coarsened fine boxes next to this coarse box, in fine box order
     std::vector<size_t> near;
     const Box grown = cbox.grow(1);
     for (size_t f = 0; f < cfine.size(); ++f)
       if (cfine[f].intersects(grown)) near.push_back(f);
-    if (near.empty()) continue;
+    if (near.empty()) return;
     // Per coarse cell of this box (first-touch order): its coarse terms and
     // fine groups.
     std::vector<int> slotOf((size_t)cbox.numPts(), -1);
@@ -831,12 +841,22 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
       rc.c = cellOf(C, (int)cb, order[q]);
       rc.nco = (int)terms[q].size();
       rc.nfi = (int)groups[q].size();
-      rc.start = (int)C.rfCoarse.size();
-      rc.fstart = (int)C.rfFine.size();
-      for (auto& t : terms[q]) C.rfCoarse.push_back(t);
-      for (auto& g : groups[q]) C.rfFine.push_back(g);
+      rc.start = (int)out.co.size();
+      rc.fstart = (int)out.fi.size();
+      for (auto& t : terms[q]) out.co.push_back(t);
+      for (auto& g : groups[q]) out.fi.push_back(g);
+      out.cells.push_back(rc);
+    }
+  });
+  for (Part& p : parts) {
+    const int cbase = (int)C.rfCoarse.size(), fbase = (int)C.rfFine.size();
+    for (RefluxCell rc : p.cells) {
+      rc.start += cbase;
+      rc.fstart += fbase;
       C.rfCells.push_back(rc);
     }
+    C.rfCoarse.insert(C.rfCoarse.end(), p.co.begin(), p.co.end());
+    C.rfFine.insert(C.rfFine.end(), p.fi.begin(), p.fi.end());
   }
 }
 

@@ -29,6 +29,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 ORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle")
 MLORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle_mlbicgstab")
+FIORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle_fineinterp")
 PROFILE_CLASSES = ["relax_finest", "residual_op", "ghost_fill", "bottom", "relax_other"]
 METRIC = "Poisson solves/s & p50/p99 latency at 1e-10 rel. residual; V-cycle HBM GB/s"
 WORKLOADS = {
@@ -458,6 +459,143 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def fineinterp_reference(meta, repeat):
+    """The reference's FineInterp (oracle/_ref/cmg_oracle_fineinterp, interpToFine with PCInterp limiting) on
+    one host core, for every level above 0 of the hierarchy: `repeat` timed interpolations per level; returns
+    (fine cells per second, seconds per step)."""
+    if not os.path.exists(FIORACLE):
+        return None
+    boxfile = write_boxfile(meta)
+    secs, cells = 0.0, 0
+    for lev in range(1, len(meta["boxes"])):
+        out = subprocess.run([FIORACLE, f"n0={meta['n0']}", f"levels={len(meta['boxes'])}",
+                              f"maxbox={meta['maxbox']}", f"block={meta['block']}", f"seed={meta['seed']}",
+                              f"level={lev}", f"repeat={repeat}", f"boxfile={boxfile}", f"out={boxfile}.fi"],
+                             capture_output=True, text=True, check=True).stdout
+        w = out.split("fine cells=")[1].split()
+        cells += int(w[0])
+        secs += float(w[1].split("=")[1])
+    return cells / secs, secs
+
+
+def run_fineinterp(args):
+    """FineInterp::interpToFine of every level above 0 of the config-1
+    hierarchy (what a regrid does to initialise new levels): device-resident
+    fine cells per second from CUDA events around each level's two kernels,
+    L2 flushed between steps; end to end through the standalone
+    cmg_fine_interp object with the coarse data sent from and the fine data
+    read back to host memory every step."""
+    meta = golden_meta("config1_vc_3lev_128")
+    nlev = len(meta["boxes"])
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        r = fineinterp_reference(meta, max(1, args.steps))
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cmg_oracle_fineinterp not built"}))
+            return
+        cpu = {"value": r[0], "unit": "cells/s", "cores": 1, "kind": "reference",
+               "sample": f"full workload, {max(1, args.steps)} interpolations per level (the reference's "
+                         "interpToFine loops over boxes on one thread)"}
+        print(json.dumps({"impl": "reference", "metric": "FineInterp fine cells/s", "value": r[0], "unit": "cells/s",
+                          "n_gpus": 1, "steps": args.steps, "warmup": 0, "ms_per_step": 1000.0 * r[1],
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": {"workload": "fineinterp-config1"}, "cpu_baseline": cpu,
+                          "e2e": {"value": r[0], "unit": "cells/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    torch.cuda.set_device(0)
+    cmg = load_cmg()
+    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+    h.fill_synthetic(meta["seed"])
+    rhs = [h.get_rhs(l) for l in range(nlev)]
+    for l in range(nlev - 1):
+        h.set_phi(l, rhs[l])
+    fine_cells = sum(h.num_cells(l) for l in range(1, nlev))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        for l in range(1, nlev):
+            h.interp_to_fine(l)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    launches0 = cmg.launch_count()
+    h.profile_enable(True)
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        step()
+    n_runs, ms, nbytes = h.profile_read(5)
+    h.profile_enable(False)
+    launches = cmg.launch_count() - launches0
+    clocks = sampler.stop()
+    value = fine_cells * args.steps / (ms / 1e3)
+
+    # the reference's output at level 2 from the level-1 right-hand side
+    ref = np.load(os.path.join(ROOT, "tests", "golden", "fineinterp_config1_vc_3lev_128_l2.npz"))["fine"]
+    h.set_phi(1, rhs[1])
+    h.interp_to_fine(2)
+    parity = bool(np.array_equal(h.phi(2)[::997], ref))
+    h.close()
+
+    # end to end: standalone objects, host data in and out every step
+    nf = meta["n0"]
+    fis, coarse = [], []
+    for l in range(1, nlev):
+        nf *= 2
+        fis.append(cmg.FineInterp((0, 0, 0, nf - 1, nf - 1, nf - 1), meta["boxes"][l], meta["boxes"][l - 1]))
+        coarse.append(rhs[l - 1])
+    for fi, c in zip(fis, coarse):
+        fi.interp_to_fine(c)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for fi, c in zip(fis, coarse):
+            fi.interp_to_fine(c)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    for fi in fis:
+        fi.close()
+    h2d = sum(c.size for c in coarse) * 8
+    d2h = fine_cells * 8
+    e2e = {"value": fine_cells * args.steps / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "timing": "wall clock, host arrays (pageable) in and out"}
+
+    peak, peak_kind = measured_peaks()
+    achieved = (nbytes / 1e9) / (ms / 1e3)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        t = json.load(open(tpath)).get("fineinterp")
+        traffic = t["dram_bytes_per_launch"] if t else None
+    cpu = None
+    if not args.no_cpu_baseline:
+        r = fineinterp_reference(meta, 1)
+        if r:
+            cpu = {"value": r[0], "unit": "cells/s", "cores": 1, "kind": "reference",
+                   "sample": "full workload, one interpolation per level"}
+    line = {"metric": "FineInterp fine cells/s", "value": value, "unit": "cells/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "fineinterp-config1: interpToFine of levels 1 and 2 of the 3-level 128^3 "
+                                   "hierarchy from the seeded right-hand side", "fine_cells_per_step": fine_cells,
+                       "l2": "flushed (256 MB write) before every step",
+                       "timing": "sum of CUDA-event device times around each level's gather + interpolation"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_fi_gather + k_fi_interp (one timed region per level; algorithmic bytes: "
+                                   "8 B written per fine cell + 8 B read per coarse parent)",
+                         "launches": int(n_runs) * 2, "algorithmic_bytes_per_step": nbytes / args.steps},
+            "parity_level2_vs_reference": parity, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": launches}
+    print(json.dumps(line), flush=True)
+
+
 def run_serving(args):
     """Serving: open-loop Poisson arrivals at each rate; each request a 1-3
     level hierarchy, base 32^3-256^3 log-uniform (x16), seeded inputs,
@@ -519,7 +657,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS) + ["config3", "config4"])
+    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS) + ["config3", "config4", "fineinterp"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
     ap.add_argument("--relax-mode", type=int, default=0, choices=[0, 1, 2],
@@ -532,6 +670,8 @@ def main():
     ap.add_argument("--host-tags", action="store_true", help="config4: tag for grid generation on the host")
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per rate")
     args = ap.parse_args()
+    if args.workload == "fineinterp":
+        return run_fineinterp(args)
     if args.workload in ("config3", "config4"):
         if args.impl == "reference":
             return run_reference_batch(args)

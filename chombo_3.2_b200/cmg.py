@@ -179,6 +179,43 @@ def layout_coarse_fine_plan(fine, coarse):
     return _plan(lib().cmg_layout_coarse_fine_plan, fa, len(fine), ca, len(coarse))
 
 
+class FineInterp:
+    """FineInterp (AMRTools/FineInterp.H) as a standalone object
+    (cmg_fine_interp_*): fine layout and fine problem domain, refinement ratio
+    2, and the coarse layout the data come on.  interp_to_fine takes the
+    coarse level's valid cells (per box in order, x fastest) and returns the
+    fine level's."""
+
+    def __init__(self, fine_domain, fine_boxes, coarse_boxes):
+        lo, hi = fine_domain[0:3], fine_domain[3:6]
+        h = ctypes.c_void_p()
+        _check(lib().cmg_fine_interp_create((ctypes.c_int * 3)(*lo), (ctypes.c_int * 3)(*hi), len(fine_boxes),
+                                            boxes_array(fine_boxes), len(coarse_boxes), boxes_array(coarse_boxes),
+                                            ctypes.byref(h)))
+        self.h = h
+        self.nfine = sum((b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1) for b in fine_boxes)
+        self.ncoarse = sum((b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1) for b in coarse_boxes)
+
+    def interp_to_fine(self, coarse, pwc=False):
+        a = np.ascontiguousarray(coarse, dtype=np.float64)
+        if a.size != self.ncoarse:
+            raise ValueError(f"coarse data has {a.size} cells, the coarse layout {self.ncoarse}")
+        out = np.empty(self.nfine, dtype=np.float64)
+        _check(lib().cmg_fine_interp_run(self.h, _ptr(a), _ptr(out), 0, int(pwc)))
+        return out
+
+    def close(self):
+        if self.h:
+            _check(lib().cmg_fine_interp_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Hierarchy:
     """One AMR hierarchy with device-resident state (cmg_hierarchy)."""
 
@@ -271,6 +308,11 @@ class Hierarchy:
     def set_alpha_beta(self, alpha, beta):
         """TGAHelmOp::setAlphaAndBeta on every operator of the hierarchy (cmg_set_alpha_beta)."""
         _check(lib().cmg_set_alpha_beta(self.h, ctypes.c_double(alpha), ctypes.c_double(beta)))
+
+    def interp_to_fine(self, level, pwc=False):
+        """FineInterp::interpToFine (pwc: pwcinterpToFine) of phi: every valid
+        cell of `level` from phi on level - 1 (cmg_interp_to_fine)."""
+        _check(lib().cmg_interp_to_fine(self.h, level, int(pwc)))
 
     def backward_euler(self, params, dt, nsteps, zero_phi=False):
         """nsteps BackwardEuler::oneStep steps on phi with the right-hand side as the source

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/cmg.h"
+#include "fineinterp.H"
 #include "meshrefine.H"
 #include "noalloc.H"
 #include "serve.H"
@@ -22,6 +23,17 @@ struct cmg_hierarchy {
   cudaStream_t stream = nullptr;
   cmg::Solver* solver = nullptr;
   cmg::HierarchyDesc desc;
+};
+
+struct cmg_fine_interp {
+  cudaStream_t stream = nullptr;
+  cmg::FineInterpOp* op = nullptr;
+  int64_t ncoarse = 0, nfine = 0;
+  void* mem = nullptr;  // FlatBox tables of both layouts, then coarse and fine staging for host data
+  const cmg::FlatBox* cflat = nullptr;
+  const cmg::FlatBox* fflat = nullptr;
+  double* dcoarse = nullptr;
+  double* dfine = nullptr;
 };
 
 namespace {
@@ -406,6 +418,106 @@ int cmg_solve_multilevel_bicgstab(cmg_hierarchy* h, const cmg_mlsolve_params* p,
     if (history_len) *history_len = n;
     if (history)
       for (int i = 0; i < n && i < history_cap; ++i) history[i] = r.history[i];
+  });
+}
+
+int cmg_interp_to_fine(cmg_hierarchy* h, int level, int piecewise_constant) {
+  return guard([&]() {
+    needLevel(h, level);
+    h->solver->interpToFine(level, piecewise_constant != 0);
+  });
+}
+
+int cmg_fine_interp_destroy(cmg_fine_interp* fi) {
+  return guard([&]() {
+    if (!fi) return;
+    delete fi->op;
+    if (fi->mem) cudaFreeAsync(fi->mem, fi->stream);
+    if (fi->stream) {
+      cudaStreamSynchronize(fi->stream);
+      cudaStreamDestroy(fi->stream);
+    }
+    delete fi;
+  });
+}
+
+int cmg_fine_interp_create(const int fine_domain_lo[3], const int fine_domain_hi[3], int nfine, const cmg_box* fine,
+                           int ncoarse, const cmg_box* coarse, cmg_fine_interp** out) {
+  return guard([&]() {
+    if (!fine_domain_lo || !fine_domain_hi || !fine || !coarse || !out || nfine < 1 || ncoarse < 1)
+      throw std::invalid_argument("cmg: invalid fine interpolation description");
+    *out = nullptr;
+    cmg::Box fdom(cmg::IV(fine_domain_lo[0], fine_domain_lo[1], fine_domain_lo[2]),
+                  cmg::IV(fine_domain_hi[0], fine_domain_hi[1], fine_domain_hi[2]));
+    if (fdom.empty() || !fdom.coarsenable(2)) throw std::invalid_argument("cmg: fine domain empty or not coarsenable by 2");
+    const cmg::Box cdom = fdom.coarsen(2);
+    std::vector<cmg::Box> fb, cb;
+    for (int b = 0; b < nfine; ++b) {
+      cmg::Box x = toBox(fine[b]);
+      if (x.empty() || !fdom.contains(x) || !x.coarsenable(2))
+        throw std::invalid_argument("cmg: fine box empty, outside the fine domain or not coarsenable by 2");
+      fb.push_back(x);
+    }
+    for (int b = 0; b < ncoarse; ++b) {
+      cmg::Box x = toBox(coarse[b]);
+      if (x.empty() || !cdom.contains(x)) throw std::invalid_argument("cmg: coarse box empty or outside the domain");
+      cb.push_back(x);
+    }
+    cmg::BoxIndex cindex;
+    cindex.build(cb);
+    std::vector<cmg::FlatBox> cf, ff;
+    cmg_fine_interp* fi = new cmg_fine_interp;
+    fi->ncoarse = cmg::flatBoxes(cb, cf);
+    fi->nfine = cmg::flatBoxes(fb, ff);
+    try {
+      cudaError_t e = cudaStreamCreateWithFlags(&fi->stream, cudaStreamNonBlocking);
+      if (e != cudaSuccess) throw std::runtime_error(std::string("cmg: stream: ") + cudaGetErrorString(e));
+      fi->op = new cmg::FineInterpOp(cb, cindex, cdom, fb, fi->stream);
+      auto up = [](size_t n) { return (n + 255) & ~(size_t)255; };
+      const size_t cB = up(cf.size() * sizeof(cmg::FlatBox)), fB = up(ff.size() * sizeof(cmg::FlatBox));
+      const size_t dC = up(fi->ncoarse * sizeof(double)), dF = up(fi->nfine * sizeof(double));
+      e = cudaMallocAsync(&fi->mem, cB + fB + dC + dF, fi->stream);
+      if (e != cudaSuccess) throw std::runtime_error(std::string("cmg: cudaMalloc fine interpolation: ") + cudaGetErrorString(e));
+      char* p = (char*)fi->mem;
+      std::vector<char> host(cB + fB);
+      std::memcpy(host.data(), cf.data(), cf.size() * sizeof(cmg::FlatBox));
+      std::memcpy(host.data() + cB, ff.data(), ff.size() * sizeof(cmg::FlatBox));
+      e = cudaMemcpyAsync(p, host.data(), host.size(), cudaMemcpyHostToDevice, fi->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(fi->stream);
+      if (e != cudaSuccess) throw std::runtime_error(std::string("cmg: fine interpolation tables: ") + cudaGetErrorString(e));
+      fi->cflat = (const cmg::FlatBox*)p;
+      fi->fflat = (const cmg::FlatBox*)(p + cB);
+      fi->dcoarse = (double*)(p + cB + fB);
+      fi->dfine = (double*)(p + cB + fB + dC);
+    } catch (...) {
+      cmg_fine_interp_destroy(fi);
+      throw;
+    }
+    *out = fi;
+  });
+}
+
+int cmg_fine_interp_run(cmg_fine_interp* fi, const double* coarse, double* fine, int on_device,
+                        int piecewise_constant) {
+  return guard([&]() {
+    if (!fi || !fi->op || !coarse || !fine) throw std::invalid_argument("cmg: null fine interpolation argument");
+    const bool pwc = piecewise_constant != 0;
+    auto ck = [](cudaError_t e, const char* what) {
+      if (e != cudaSuccess) throw std::runtime_error(std::string("cmg: ") + what + ": " + cudaGetErrorString(e));
+    };
+    const double* c = coarse;
+    double* f = fine;
+    if (!on_device) {
+      ck(cudaMemcpyAsync(fi->dcoarse, coarse, fi->ncoarse * sizeof(double), cudaMemcpyHostToDevice, fi->stream),
+         "fine interpolation h2d");
+      c = fi->dcoarse;
+      f = fi->dfine;
+    }
+    fi->op->runFlat(fi->cflat, c, fi->fflat, f, pwc);
+    if (!on_device)
+      ck(cudaMemcpyAsync(fine, fi->dfine, fi->nfine * sizeof(double), cudaMemcpyDeviceToHost, fi->stream),
+         "fine interpolation d2h");
+    ck(cudaStreamSynchronize(fi->stream), "fine interpolation sync");
   });
 }
 

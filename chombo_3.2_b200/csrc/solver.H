@@ -17,6 +17,8 @@
 
 namespace cmg {
 
+class FineInterpOp;
+
 struct HierarchyDesc {
   Box domain;                            // level-0 domain
   double dx0 = 1.0;                      // level-0 cell size
@@ -110,6 +112,9 @@ class Solver {
   // BiCGStab over MultilevelLinearOp (see MLSolveParams) from the current
   // phi, or from zero (ghost cells included) when zeroPhi.
   MLSolveResult solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroPhi = true);
+  // FineInterp::interpToFine (pwc: pwcinterpToFine) of phi: every valid cell
+  // of level l from phi on level l - 1 (AMRTools/FineInterp.cpp:106-160).
+  void interpToFine(int l, bool pwc);
   // One composite residual evaluation (AMRMultiGrid::computeAMRResidual).
   double residualNorm();
   // The same evaluation with the max-norm reduced through `scratch`, a
@@ -129,7 +134,7 @@ class Solver {
   // class, on the solver's stream) with the algorithmic bytes of each launch.
   // Profile classes: relaxation on the finest AMR level, residual/operator
   // kernels, ghost fills, bottom solves, relaxation on every other level.
-  enum ProfClass { P_RELAX_FINE = 0, P_OP = 1, P_GHOST = 2, P_BOTTOM = 3, P_RELAX = 4, P_NCLASS = 5 };
+  enum ProfClass { P_RELAX_FINE = 0, P_OP = 1, P_GHOST = 2, P_BOTTOM = 3, P_RELAX = 4, P_FINEINTERP = 5, P_NCLASS = 6 };
   void profileEnable(bool on);
   void profileRead(int cls, int64_t* launches, double* ms, double* bytes);
 
@@ -226,6 +231,7 @@ class Solver {
   using MLVec = std::vector<double*>;
   double alpha0_ = 0.0, beta0_ = 1.0;  // the factory's coefficients (AMRPoissonOp m_aCoef, m_bCoef)
   std::vector<double*> src_;           // backward-Euler source per level
+  std::vector<std::unique_ptr<FineInterpOp>> fineInterp_;  // per fine level, built on first use
   std::vector<MLVec> mlVecs_;    // r, r_tilde, e, p, p_tilde, s_tilde, t, v, and two scratch vectors
   double* dBoxSums_ = nullptr;   // one per box of every level
   double* hostBoxSums_ = nullptr;

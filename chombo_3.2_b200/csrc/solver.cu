@@ -4,6 +4,7 @@
 // (AMRElliptic/MultiGrid.H:629-696); every step below names the operator
 // method it performs.
 #include "solver.H"
+#include "fineinterp.H"
 
 #include <cstdint>
 #include <algorithm>
@@ -1186,6 +1187,19 @@ void Solver::mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p) {
   }
   ck(cudaGraphLaunch(exec, s_), "graph launch");
   addLaunches(graphLaunches_[exec]);
+}
+
+void Solver::interpToFine(int l, bool pwc) {
+  if (l < 1 || l >= numLevels()) throw std::invalid_argument("cmg: fine interpolation needs a level in 1..finest");
+  if (fineInterp_.size() < amr_.size()) fineInterp_.resize(amr_.size());
+  if (!fineInterp_[l])
+    fineInterp_[l].reset(
+        new FineInterpOp(amr_[l - 1].grids.boxes, amr_[l - 1].index, amr_[l - 1].domain, amr_[l].grids.boxes, s_));
+  // algorithmic bytes: every fine cell written once, every coarse parent read once
+  const double bytes = 9.0 * sizeof(double) / 8.0 * (double)fineInterp_[l]->fineCells();
+  timed(P_FINEINTERP, bytes,
+        [&]() { fineInterp_[l]->run(amrDev_[l - 1].boxes, lev_[l - 1].phi, amrDev_[l].boxes, lev_[l].phi, pwc); });
+  ck(cudaStreamSynchronize(s_), "fine interpolation sync");
 }
 
 MLSolveResult Solver::solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroPhi) {

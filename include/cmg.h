@@ -172,6 +172,28 @@ int cmg_solve_multilevel_bicgstab(cmg_hierarchy* h, const cmg_mlsolve_params* p,
                                   int* iterations, double* initial_residual, double* final_residual, double* history,
                                   int history_cap, int* history_len);
 
+/* Coarse-to-fine interpolation of a new level, FineInterp::interpToFine
+ * (AMRTools/FineInterp.cpp:106-160; FineInterp.H:158-162) with the default
+ * PCInterp boundary limiting, refinement ratio 2, one component: every valid
+ * cell of phi on `level` (1..finest) from phi on level - 1.  Coarse cells of
+ * the layer next to the domain boundary interpolate piecewise constant; the
+ * others add the limited central slopes.  piecewise_constant != 0 gives
+ * pwcinterpToFine (FineInterp.cpp:162-199; FineInterp.H:164-168).
+ * CMG_EINVAL when the level is not properly nested (the interpolation reads
+ * grow(coarsen(fine box), 1) & domain from the coarse level). */
+int cmg_interp_to_fine(cmg_hierarchy* h, int level, int piecewise_constant);
+
+/* FineInterp as a standalone object (FineInterp.H:59-121): define() with the
+ * fine layout and fine problem domain (ratio 2, one component), plus the
+ * coarse layout the data come on.  Data are valid cells per box in the given
+ * box order, x fastest; on_device selects device or host pointers. */
+typedef struct cmg_fine_interp cmg_fine_interp;
+int cmg_fine_interp_create(const int fine_domain_lo[3], const int fine_domain_hi[3], int nfine, const cmg_box* fine,
+                           int ncoarse, const cmg_box* coarse, cmg_fine_interp** out);
+int cmg_fine_interp_run(cmg_fine_interp* fi, const double* coarse, double* fine, int on_device,
+                        int piecewise_constant);
+int cmg_fine_interp_destroy(cmg_fine_interp* fi);
+
 /* Same value as cmg_residual_norm, allocating no memory on success (no
  * counterpart in the reference, which has no such constraint).  For callers
  * that cannot let the library allocate at call time: a process whose memory
@@ -287,7 +309,8 @@ int cmg_get_stream(const cmg_hierarchy* h, void** stream);
  * class is bracketed by CUDA events on the hierarchy's stream.  Classes:
  * 0 = red-black relaxation on the finest AMR level, 1 = residual / operator
  * application, 2 = ghost fills (exchange, boundary and homogeneous coarse-fine
- * values), 3 = bottom solves, 4 = red-black relaxation on every other level.
+ * values), 3 = bottom solves, 4 = red-black relaxation on every other level,
+ * 5 = fine interpolation (cmg_interp_to_fine).
  * cmg_profile_read returns launches, total device milliseconds and the
  * algorithmic bytes of those launches since the last enable. */
 int cmg_profile_enable(cmg_hierarchy* h, int on);

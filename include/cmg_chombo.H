@@ -476,6 +476,113 @@ class GpuMultilevelBiCGStabSolver {
   std::vector<double> m_history;
 };
 
+// FineInterp (AMRTools/FineInterp.H:35-245) on the device: define() with the
+// fine layout, one component, refinement ratio 2 and the fine problem domain;
+// interpToFine / pwcinterpToFine send the coarse data's valid cells, run
+// cmg_fine_interp_run and write every valid cell of the fine data, with the
+// reference's default PCInterp boundary limiting.  The device plan is built
+// on the first call for a coarse layout and kept while that layout is the
+// same object.  Only properly nested levels are accepted (the reference then
+// reads nothing but coarse data), so a_averageFromDest, whose averages the
+// coarse copy overwrites on such levels (FineInterp.cpp:124-148), changes
+// nothing.
+class GpuFineInterp {
+ public:
+  GpuFineInterp() {}
+  GpuFineInterp(const DisjointBoxLayout& a_fine_domain, const int& a_numcomps, const int& a_ref_ratio,
+                const ProblemDomain& a_fine_problem_domain) {
+    define(a_fine_domain, a_numcomps, a_ref_ratio, a_fine_problem_domain);
+  }
+  GpuFineInterp(const DisjointBoxLayout& a_fine_domain, const int& a_numcomps, const int& a_ref_ratio,
+                const Box& a_fine_problem_domain) {
+    define(a_fine_domain, a_numcomps, a_ref_ratio, ProblemDomain(a_fine_problem_domain));
+  }
+  ~GpuFineInterp() { clear(); }
+  GpuFineInterp(const GpuFineInterp&) = delete;
+  GpuFineInterp& operator=(const GpuFineInterp&) = delete;
+
+  void define(const DisjointBoxLayout& a_fine_domain, const int& a_numcomps, const int& a_ref_ratio,
+              const ProblemDomain& a_fine_problem_domain) {
+    if (a_numcomps != 1) MayDay::Error("cmg_chombo: GpuFineInterp takes one component");
+    if (a_ref_ratio != 2) MayDay::Error("cmg_chombo: refinement ratio 2 only");
+    for (int dir = 0; dir < SpaceDim; ++dir)
+      if (a_fine_problem_domain.isPeriodic(dir)) MayDay::Error("cmg_chombo: periodic domains are not supported");
+    clear();
+    m_fine = a_fine_domain;
+    m_domain = a_fine_problem_domain.domainBox();
+    m_defined = true;
+  }
+  void define(const DisjointBoxLayout& a_fine_domain, const int& a_numcomps, const int& a_ref_ratio,
+              const Box& a_fine_problem_domain) {
+    define(a_fine_domain, a_numcomps, a_ref_ratio, ProblemDomain(a_fine_problem_domain));
+  }
+  bool isDefined() const { return m_defined; }
+
+  void interpToFine(LevelData<FArrayBox>& a_fine_data, const LevelData<FArrayBox>& a_coarse_data,
+                    bool a_averageFromDest = false) {
+    run(a_fine_data, a_coarse_data, false);
+  }
+  void pwcinterpToFine(LevelData<FArrayBox>& a_fine_data, const LevelData<FArrayBox>& a_coarse_data,
+                       bool a_averageFromDest = false) {
+    run(a_fine_data, a_coarse_data, true);
+  }
+
+ private:
+  static void boxesOf(const DisjointBoxLayout& g, std::vector<cmg_box>& out) {
+    out.clear();
+    for (LayoutIterator lit = g.layoutIterator(); lit.ok(); ++lit) {
+      const Box& b = g[lit];
+      cmg_box c;
+      for (int d = 0; d < 3; ++d) {
+        c.lo[d] = b.smallEnd(d);
+        c.hi[d] = b.bigEnd(d);
+      }
+      out.push_back(c);
+    }
+  }
+  void clear() {
+    if (m_h) cmg_fine_interp_destroy(m_h);
+    m_h = nullptr;
+  }
+  void run(LevelData<FArrayBox>& a_fine, const LevelData<FArrayBox>& a_coarse, bool pwc) {
+    if (!m_defined) MayDay::Error("cmg_chombo: GpuFineInterp not defined");
+    if (a_coarse.nComp() != 1 || a_fine.nComp() != 1) MayDay::Error("cmg_chombo: GpuFineInterp takes one component");
+    const DisjointBoxLayout& cg = a_coarse.disjointBoxLayout();
+    if (!m_h || !(cg == m_coarse)) {
+      clear();
+      std::vector<cmg_box> fb, cb;
+      boxesOf(m_fine, fb);
+      boxesOf(cg, cb);
+      const int lo[3] = {m_domain.smallEnd(0), m_domain.smallEnd(1), m_domain.smallEnd(2)};
+      const int hi[3] = {m_domain.bigEnd(0), m_domain.bigEnd(1), m_domain.bigEnd(2)};
+      GpuHierarchy::check(cmg_fine_interp_create(lo, hi, (int)fb.size(), fb.data(), (int)cb.size(), cb.data(), &m_h));
+      m_coarse = cg;
+    }
+    std::vector<double> in, out;
+    for (DataIterator dit = a_coarse.dataIterator(); dit.ok(); ++dit) {
+      const Box& b = cg[dit()];
+      const FArrayBox& f = a_coarse[dit];
+      for (int k = b.smallEnd(2); k <= b.bigEnd(2); ++k)
+        for (int j = b.smallEnd(1); j <= b.bigEnd(1); ++j)
+          for (int i = b.smallEnd(0); i <= b.bigEnd(0); ++i) in.push_back(f(IntVect(i, j, k), 0));
+    }
+    out.resize(m_fine.numCells());
+    GpuHierarchy::check(cmg_fine_interp_run(m_h, in.data(), out.data(), 0, pwc ? 1 : 0));
+    size_t p = 0;
+    for (DataIterator dit = a_fine.dataIterator(); dit.ok(); ++dit) {
+      const Box& b = m_fine[dit()];
+      FArrayBox& f = a_fine[dit];
+      for (int k = b.smallEnd(2); k <= b.bigEnd(2); ++k)
+        for (int j = b.smallEnd(1); j <= b.bigEnd(1); ++j)
+          for (int i = b.smallEnd(0); i <= b.bigEnd(0); ++i) f(IntVect(i, j, k), 0) = out[p++];
+    }
+  }
+  bool m_defined = false;
+  DisjointBoxLayout m_fine, m_coarse;
+  Box m_domain;
+  cmg_fine_interp* m_h = nullptr;
+};
+
 }  // namespace cmg_chombo
 
 #endif

@@ -596,6 +596,127 @@ void interphomolinear_(FAB(phi), BOX(region), const Real* x1, const Real* dxCrse
         }
 }
 
+// InterpF.ChF:12-44 (interpconstant): every fine cell of the refined box of
+// each coarse cell of b takes the coarse value.
+void interpconstant_(FAB(fine), FAB(coarse), BOX(b), const int* refRatio, BOX(bref)) {
+  MKFAB(fine);
+  MKFAB(coarse);
+  const int r = *refRatio;
+  for (int var = 0; var < F_coarse.nc; ++var)
+    for (int k = BLO(b, 2); k <= BHI(b, 2); ++k)
+      for (int j = BLO(b, 1); j <= BHI(b, 1); ++j)
+        for (int i = BLO(b, 0); i <= BHI(b, 0); ++i)
+          for (int kk = BLO(bref, 2); kk <= BHI(bref, 2); ++kk)
+            for (int jj = BLO(bref, 1); jj <= BHI(bref, 1); ++jj)
+              for (int ii = BLO(bref, 0); ii <= BHI(bref, 0); ++ii)
+                F_fine(i * r + ii, j * r + jj, k * r + kk, var) = F_coarse(i, j, k, var);
+}
+
+// InterpF.ChF:48-71 (interpcentralslope): half * (state[+1] - state[-1]).
+void interpcentralslope_(FAB(slope), FAB(state), BOX(b), const int* dir) {
+  MKFAB(slope);
+  MKFAB(state);
+  const int d0 = *dir == 0, d1 = *dir == 1, d2 = *dir == 2;
+  for (int var = 0; var < F_state.nc; ++var)
+    for (int k = BLO(b, 2); k <= BHI(b, 2); ++k)
+      for (int j = BLO(b, 1); j <= BHI(b, 1); ++j)
+        for (int i = BLO(b, 0); i <= BHI(b, 0); ++i)
+          F_slope(i, j, k, var) = 0.5 * (F_state(i + d0, j + d1, k + d2, var) - F_state(i - d0, j - d1, k - d2, var));
+}
+
+// InterpF.ChF:76-100 (interphisideslope): state[+1] - state.
+void interphisideslope_(FAB(slope), FAB(state), BOX(b), const int* dir) {
+  MKFAB(slope);
+  MKFAB(state);
+  const int d0 = *dir == 0, d1 = *dir == 1, d2 = *dir == 2;
+  for (int var = 0; var < F_state.nc; ++var)
+    for (int k = BLO(b, 2); k <= BHI(b, 2); ++k)
+      for (int j = BLO(b, 1); j <= BHI(b, 1); ++j)
+        for (int i = BLO(b, 0); i <= BHI(b, 0); ++i)
+          F_slope(i, j, k, var) = F_state(i + d0, j + d1, k + d2, var) - F_state(i, j, k, var);
+}
+
+// InterpF.ChF:104-126 (interplosideslope): state - state[-1].
+void interplosideslope_(FAB(slope), FAB(state), BOX(b), const int* dir) {
+  MKFAB(slope);
+  MKFAB(state);
+  const int d0 = *dir == 0, d1 = *dir == 1, d2 = *dir == 2;
+  for (int var = 0; var < F_state.nc; ++var)
+    for (int k = BLO(b, 2); k <= BHI(b, 2); ++k)
+      for (int j = BLO(b, 1); j <= BHI(b, 1); ++j)
+        for (int i = BLO(b, 0); i <= BHI(b, 0); ++i)
+          F_slope(i, j, k, var) = F_state(i, j, k, var) - F_state(i - d0, j - d1, k - d2, var);
+}
+
+// InterpF.ChF:135-312 (interplimit): multidimensional limiter.  statemax /
+// statemin over the neighbours (bn) inside the state FAB; deltasum = half *
+// (|islope| + |jslope| + |kslope|); eta = min(statemax - state, state -
+// statemin), zero when eta <= 1.e-9 * |statemax|, else eta / deltasum when
+// deltasum > eta, else one; every slope scaled by eta.  The literal 1.e-9 is
+// a default-kind (single precision) Fortran constant in the reference's GNU
+// build (no real-8 promotion flag), so it enters as (double)1.0e-9f.
+void interplimit_(FAB(islope), FAB(jslope), FAB(kslope), FAB(state), BOX(bcoarse), BOX(bn), BOX(physdomain)) {
+  MKFAB(islope);
+  MKFAB(jslope);
+  MKFAB(kslope);
+  MKFAB(state);
+  (void)iphysdomainlo0; (void)iphysdomainlo1; (void)iphysdomainlo2;
+  (void)iphysdomainhi0; (void)iphysdomainhi1; (void)iphysdomainhi2;
+  const Real tiny = (Real)1.0e-9f;
+  for (int var = 0; var < F_islope.nc; ++var)
+    for (int k = BLO(bcoarse, 2); k <= BHI(bcoarse, 2); ++k)
+      for (int j = BLO(bcoarse, 1); j <= BHI(bcoarse, 1); ++j)
+        for (int i = BLO(bcoarse, 0); i <= BHI(bcoarse, 0); ++i) {
+          const Real s = F_state(i, j, k, var);
+          Real smax = s, smin = s;
+          for (int kk = BLO(bn, 2); kk <= BHI(bn, 2); ++kk)
+            for (int jj = BLO(bn, 1); jj <= BHI(bn, 1); ++jj)
+              for (int ii = BLO(bn, 0); ii <= BHI(bn, 0); ++ii) {
+                const int a = i + ii, b = j + jj, c = k + kk;
+                if (a >= F_state.lo0 && a <= F_state.hi0 && b >= F_state.lo1 && b <= F_state.hi1 &&
+                    c >= F_state.lo2 && c <= F_state.hi2) {
+                  const Real v = F_state(a, b, c, var);
+                  smax = std::fmax(smax, v);
+                  smin = std::fmin(smin, v);
+                }
+              }
+          const Real deltasum = 0.5 * (std::fabs(F_islope(i, j, k, var)) + std::fabs(F_jslope(i, j, k, var)) +
+                                       std::fabs(F_kslope(i, j, k, var)));
+          Real eta = std::fmin(smax - s, s - smin);
+          if (eta <= tiny * std::fabs(smax)) {
+            eta = 0.0;
+          } else if (deltasum > eta) {
+            eta = eta / deltasum;
+          } else {
+            eta = 1.0;
+          }
+          F_islope(i, j, k, var) = eta * F_islope(i, j, k, var);
+          F_jslope(i, j, k, var) = eta * F_jslope(i, j, k, var);
+          F_kslope(i, j, k, var) = eta * F_kslope(i, j, k, var);
+        }
+}
+
+// InterpF.ChF:318-369 (interplinear): fine += dxf * slope over the refined
+// box of each coarse cell, dxf = -half + (id + half) / ref_ratio with id the
+// fine offset in direction dir.
+void interplinear_(FAB(fine), FAB(slope), BOX(b), const int* dir, const int* refRatio, BOX(bref)) {
+  MKFAB(fine);
+  MKFAB(slope);
+  const int r = *refRatio, d = *dir;
+  for (int var = 0; var < F_fine.nc; ++var)
+    for (int k = BLO(b, 2); k <= BHI(b, 2); ++k)
+      for (int j = BLO(b, 1); j <= BHI(b, 1); ++j)
+        for (int i = BLO(b, 0); i <= BHI(b, 0); ++i)
+          for (int kk = BLO(bref, 2); kk <= BHI(bref, 2); ++kk)
+            for (int jj = BLO(bref, 1); jj <= BHI(bref, 1); ++jj)
+              for (int ii = BLO(bref, 0); ii <= BHI(bref, 0); ++ii) {
+                const int id = d == 0 ? ii : (d == 1 ? jj : kk);
+                const Real dxf = -0.5 + ((id + 0.5) / r);
+                Real& f = F_fine(i * r + ii, j * r + jj, k * r + kk, var);
+                f = f + dxf * F_slope(i, j, k, var);
+              }
+}
+
 // QuadCFInterpF.ChF:9-48 (quadinterp): quadratic through phistar and two
 // interior fine cells.
 void quadinterp_(FAB(phi), FAB(phistar), BOX(box), const int* ihilo, const Real* h,

@@ -10,7 +10,8 @@
 // Usage: dropin key=value ...   (n0 levels maxbox block op alpha beta seed
 // pre post bottom iters eps hang, as for cmg_oracle; bicgstab=1 mgiters
 // mgsmooth imax eps for the BiCGStab over MultilevelLinearOp path; heat=1
-// (backward Euler) or heat=2 (TGA) with dt steps for the heat solvers)
+// (backward Euler) or heat=2 (TGA) with dt steps for the heat solvers;
+// fineinterp=1 (interpToFine) or 2 (pwcinterpToFine) for FineInterp)
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -23,6 +24,7 @@
 #include "AMRTGA.H"
 #include "BackwardEuler.H"
 #include "BiCGStabSolver.H"
+#include "FineInterp.H"
 #include "MultilevelLinearOp.H"
 #include "VCAMRPoissonOp2.H"
 #include "cmg_chombo.H"
@@ -206,6 +208,42 @@ static int heatCheck(OracleProblem& P, Vector<LDF*>& phiGpu, Vector<int>& rr, bo
   return 0;
 }
 
+// FineInterp on the CPU and cmg_chombo::GpuFineInterp with the same calls:
+// every level above 0 is filled from the level below (interpToFine, or
+// pwcinterpToFine with fineinterp=2), the coarse data being the seeded
+// right-hand side; the fine data must agree bit for bit.
+static int fineInterpCheck(OracleProblem& P, bool pwc) {
+  double maxDiff = 0.0;
+  long cells = 0;
+  for (int l = 1; l < P.nlev; ++l) {
+    LDF cpuFine(P.grids[l], 1, IntVect::Unit), gpuFine(P.grids[l], 1, IntVect::Unit);
+    for (DataIterator dit = P.grids[l].dataIterator(); dit.ok(); ++dit) {
+      cpuFine[dit()].setVal(0.0);
+      gpuFine[dit()].setVal(0.0);
+    }
+    FineInterp cpu(P.grids[l], 1, 2, P.domains[l]);
+    cmg_chombo::GpuFineInterp gpu(P.grids[l], 1, 2, P.domains[l]);
+    if (pwc) {
+      cpu.pwcinterpToFine(cpuFine, *P.rhs[l - 1]);
+      gpu.pwcinterpToFine(gpuFine, *P.rhs[l - 1]);
+    } else {
+      cpu.interpToFine(cpuFine, *P.rhs[l - 1]);
+      gpu.interpToFine(gpuFine, *P.rhs[l - 1]);
+      gpu.interpToFine(gpuFine, *P.rhs[l - 1]);  // the kept device plan
+    }
+    for (DataIterator dit = P.grids[l].dataIterator(); dit.ok(); ++dit) {
+      const Box& b = P.grids[l][dit()];
+      for (BoxIterator bit(b); bit.ok(); ++bit) {
+        maxDiff = std::max(maxDiff, std::fabs(cpuFine[dit()](bit(), 0) - gpuFine[dit()](bit(), 0)));
+        ++cells;
+      }
+    }
+  }
+  std::printf("{\"fineinterp\": %d, \"levels\": %d, \"cells\": %ld, \"max_abs_diff\": %.17g}\n", pwc ? 2 : 1,
+              P.nlev, cells, maxDiff);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   for (int a = 1; a < argc; ++a) {
     const char* eq = std::strchr(argv[a], '=');
@@ -231,6 +269,7 @@ int main(int argc, char** argv) {
   Vector<int> rr(nlev, 2);
   if (argd("bicgstab", 0) != 0) return bicgstabCheck(P, phiGpu, rr);
   if (argd("heat", 0) != 0) return heatCheck(P, phiGpu, rr, argd("heat", 0) == 2);
+  if (argd("fineinterp", 0) != 0) return fineInterpCheck(P, argd("fineinterp", 0) == 2);
 
   // Reference: CPU AMRMultiGrid.
   RefCountedPtr<AMRLevelOpFactory<LDF> > factory;

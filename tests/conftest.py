@@ -39,9 +39,9 @@ def golden(name):
 LARGE = {"config2_vc_3lev_256"}
 
 
-# Fixtures of the other solve paths (multilevel BiCGStab, backward Euler),
+# Fixtures of the other paths (multilevel BiCGStab, heat solvers, FineInterp),
 # which reuse the hierarchies of the AMRMultiGrid fixtures.
-OTHER_PATHS = ("bicgstab_", "heat_")
+OTHER_PATHS = ("bicgstab_", "heat_", "fineinterp_")
 
 
 def golden_names():

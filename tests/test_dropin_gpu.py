@@ -83,3 +83,22 @@ def test_dropin_heat_matches_reference_solver(name):
     out = json.loads(r.stdout.strip().splitlines()[-1])
     assert out["gpu_exit"] == out["cpu_exit"] == 1, out
     assert out["phi_rel_dev"] <= TOL, out
+
+
+FINEINTERP_CASES = {
+    "fineinterp_vc_3lev_16": "n0=16 levels=3 maxbox=8 block=4 fineinterp=1",
+    "fineinterp_poisson_3lev_32": "n0=32 levels=3 maxbox=16 fineinterp=1",
+    "fineinterp_pwc_poisson_3lev_32": "n0=32 levels=3 maxbox=16 fineinterp=2",
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(FINEINTERP_CASES))
+def test_dropin_fineinterp_matches_reference(name):
+    """FineInterp against cmg_chombo::GpuFineInterp with the same calls: bit for bit."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in check not built (make -C oracle dropin, needs the reference tree)")
+    r = subprocess.run([DROPIN] + FINEINTERP_CASES[name].split(), capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["cells"] > 0 and out["max_abs_diff"] == 0.0, out

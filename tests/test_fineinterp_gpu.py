@@ -1,0 +1,109 @@
+"""FineInterp on the device (cmg_interp_to_fine on a hierarchy's phi, and the
+standalone cmg_fine_interp object) against the reference's FineInterp output
+recorded in the fixtures: bit for bit.  At the config-1 sizes, properties
+that hold exactly: a constant stays constant, scaling the coarse data by a
+power of two scales the fine data by it, and the two entry points agree."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from test_fineinterp import CASES, coarse_input
+
+
+def setup(cmg, name):
+    meta, arrays = golden(name)
+    base, _ = golden(meta["base"])
+    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"])
+    lev = meta["level"]
+    c = coarse_input(meta, base)
+    if c is None:
+        h.fill_synthetic(base["seed"])
+        c = h.get_rhs(lev - 1)
+    return meta, arrays, base, h, c
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_interp_to_fine_matches_reference(cmg, name):
+    meta, arrays, base, h, c = setup(cmg, name)
+    lev = meta["level"]
+    h.set_phi(lev - 1, c)
+    h.set_phi(lev, np.full(h.num_cells(lev), 7.0))
+    h.interp_to_fine(lev, pwc=bool(meta["pwc"]))
+    got = h.phi(lev)
+    assert got.size == meta["fine_cells"]
+    assert np.array_equal(got[::meta["sample_stride"]], arrays["fine"])
+    h.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_standalone_fine_interp_matches_reference(cmg, name):
+    meta, arrays, base, h, c = setup(cmg, name)
+    h.close()
+    lev = meta["level"]
+    nf = base["n0"] << lev
+    fi = cmg.FineInterp((0, 0, 0, nf - 1, nf - 1, nf - 1), base["boxes"][lev], base["boxes"][lev - 1])
+    got = fi.interp_to_fine(c, pwc=bool(meta["pwc"]))
+    assert np.array_equal(got[::meta["sample_stride"]], arrays["fine"])
+    fi.close()
+
+
+@pytest.mark.gpu
+def test_exact_properties_at_config1_size(cmg):
+    meta, arrays, base, h, c = setup(cmg, "fineinterp_config1_vc_3lev_128_l2")
+    h.set_phi(1, c)
+    h.interp_to_fine(2)
+    ref = h.phi(2)
+    h.set_phi(1, 4.0 * c)
+    h.interp_to_fine(2)
+    assert np.array_equal(h.phi(2), 4.0 * ref)
+    h.set_phi(1, np.full(c.size, -0.375))
+    h.interp_to_fine(2)
+    assert np.all(h.phi(2) == -0.375)
+    # piecewise constant: every fine cell holds its parent's value
+    h.set_phi(1, c)
+    h.interp_to_fine(2, pwc=True)
+    pwc = h.phi(2)
+    cb, fbox = base["boxes"][1], base["boxes"][2]
+    parent = {}
+    pos = 0
+    for b in cb:
+        n = (b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1)
+        parent[tuple(b)] = (pos, b)
+        pos += n
+    # check one fine box per 50 against its coarse parent cells
+    fpos = 0
+    for t, b in enumerate(fbox):
+        n = (b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1)
+        if t % 50 == 0:
+            k, j, i = np.meshgrid(np.arange(b[2], b[5] + 1), np.arange(b[1], b[4] + 1), np.arange(b[0], b[3] + 1),
+                                  indexing="ij")
+            I, J, K = i.ravel() // 2, j.ravel() // 2, k.ravel() // 2
+            want = np.empty(n)
+            for p0, q in parent.values():
+                m = (I >= q[0]) & (I <= q[3]) & (J >= q[1]) & (J <= q[4]) & (K >= q[2]) & (K <= q[5])
+                nx, ny = q[3] - q[0] + 1, q[4] - q[1] + 1
+                want[m] = c[p0 + (I[m] - q[0]) + nx * ((J[m] - q[1]) + ny * (K[m] - q[2]))]
+            assert np.array_equal(pwc[fpos:fpos + n], want)
+        fpos += n
+    h.close()
+
+
+@pytest.mark.gpu
+def test_improperly_nested_level_is_an_error(cmg):
+    # fine box away from the only coarse box
+    fi = cmg.FineInterp((0, 0, 0, 31, 31, 31), [(16, 16, 16, 23, 23, 23)], [(0, 0, 0, 7, 7, 7)])
+    with pytest.raises(cmg.CmgError) as e:
+        fi.interp_to_fine(np.zeros(512))
+    assert e.value.code == cmg.CMG_EINVAL and "nested" in str(e.value)
+    # piecewise constant needs only the coarsened fine box, not covered either
+    with pytest.raises(cmg.CmgError):
+        fi.interp_to_fine(np.zeros(512), pwc=True)
+    fi.close()
+    fi = cmg.FineInterp((0, 0, 0, 31, 31, 31), [(0, 0, 0, 7, 7, 7)], [(0, 0, 0, 3, 3, 3)])
+    with pytest.raises(cmg.CmgError):
+        fi.interp_to_fine(np.zeros(64))  # grow(b, 1) & domain reaches past the coarse box
+    out = fi.interp_to_fine(np.arange(64.0), pwc=True)
+    assert out.size == 512 and out[0] == 0.0 and out[-1] == 63.0
+    fi.close()

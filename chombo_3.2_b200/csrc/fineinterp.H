@@ -7,11 +7,12 @@
 // cell with its coarse parent (interpconstant) and, on b_mod = the coarsened
 // box trimmed one cell from the domain boundary (FineInterp.cpp:285-292),
 // adds the limited central slopes (interpcentralslope, interplimit,
-// interplinear; InterpF.ChF).  Here the same two steps are two kernels: a
-// gather of grow(coarsen(fine box), 1) & domain into a per-fine-box staging
-// block, and one thread per coarse cell that computes the three slopes and
-// the limiter from the staging block and writes the eight fine cells with the
-// reference's operations in its order.  Slopes on the domain-boundary layer
+// interplinear; InterpF.ChF).  Here a thread block per fine box loads
+// grow(coarsen(fine box), 1) & domain from the coarse level into shared
+// memory, and one thread per coarse cell computes the three slopes and the
+// limiter from it and writes the eight fine cells with the reference's
+// operations in its order (boxes whose staging block exceeds shared memory
+// take a gather kernel into device memory and a second kernel).  Slopes on the domain-boundary layer
 // (interphisideslope / interplosideslope) feed nothing: those cells stay
 // piecewise constant, as in the reference.
 #ifndef CMG_FINEINTERP_H
@@ -57,8 +58,9 @@ class FineInterpOp {
  public:
   // coarse: the coarse layout with its spatial index; coarseDomain: the
   // coarse problem domain; fine: the fine layout (boxes coarsenable by 2).
+  // allowFused = false keeps the two-kernel path whatever the box sizes.
   FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cindex, const Box& coarseDomain,
-               const std::vector<Box>& fine, cudaStream_t s);
+               const std::vector<Box>& fine, cudaStream_t s, bool allowFused = true);
   ~FineInterpOp();
   FineInterpOp(const FineInterpOp&) = delete;
   FineInterpOp& operator=(const FineInterpOp&) = delete;
@@ -72,19 +74,23 @@ class FineInterpOp {
   // Flat valid-cell arrays (FlatBox tables of the two levels, on the device).
   void runFlat(const FlatBox* cboxes, const double* coarse, const FlatBox* fboxes, double* fine, bool pwc);
   int64_t fineCells() const { return fineCells_; }
-  int kernelLaunches() const { return (nGatherCh_ > 0 ? 1 : 0) + (nBoxCh_ > 0 ? 1 : 0); }
+  // one kernel with the staging blocks in shared memory (every block fits)
+  bool fused() const { return fused_; }
 
  private:
   void check(bool pwc) const;
   cudaStream_t s_;
   bool nested_ = true, covered_ = true;
   int64_t fineCells_ = 0, stageCells_ = 0;
-  int nBoxCh_ = 0, nGatherCh_ = 0;
+  int nBoxCh_ = 0, nGatherCh_ = 0, nbox_ = 0;
+  bool fused_ = false;
+  size_t smem_ = 0;
   void* mem_ = nullptr;  // one allocation: boxes, chunks, gathers, staging
   const FiBox* boxes_ = nullptr;
   const Chunk* boxCh_ = nullptr;
   const FiGather* gathers_ = nullptr;
   const Chunk* gatherCh_ = nullptr;
+  const int* itemStart_ = nullptr;  // gather items of each fine box (nbox + 1)
   double* stage_ = nullptr;
 };
 

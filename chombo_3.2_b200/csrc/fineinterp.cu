@@ -2,6 +2,12 @@
 // compiled with --fmad=false, every slope, limiter and fine value is formed
 // with the reference's operations in its order (InterpF.ChF:48-71, 135-312,
 // 318-369).
+//
+// Two paths.  When every fine box's staging block (its coarsened box grown by
+// one) fits in shared memory, one kernel does everything: a thread block per
+// fine box loads the block from the coarse level, then computes and stores
+// the box's fine cells.  Otherwise a gather kernel fills per-box staging
+// blocks in device memory and a second kernel interpolates from them.
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -15,6 +21,8 @@ namespace cmg {
 namespace {
 
 constexpr int kChunk = 256;
+constexpr int kFusedThreads = 256;
+constexpr size_t kFusedSmemMax = 96 * 1024;  // staging bytes per block on the one-kernel path
 
 inline void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -45,40 +53,13 @@ struct FlatCells {
   }
 };
 
-// Coarse cells of grow(b, 1) & domain into the staging blocks
-// (LevelData::copyTo into the coarsened fine layout, FineInterp.cpp:148-160).
-template <class CI>
-__global__ void k_fi_gather(const FiGather* gathers, const FiBox* boxes, const Chunk* ch, CI cidx,
-                            const double* __restrict__ coarse, double* __restrict__ stage) {
-  const Chunk c = ch[blockIdx.x];
-  const FiGather g = gathers[c.box];
-  const int q = c.start + threadIdx.x;
-  const int nx = g.hi[0] - g.lo[0] + 1, ny = g.hi[1] - g.lo[1] + 1, nz = g.hi[2] - g.lo[2] + 1;
-  if (q >= nx * ny * nz) return;
-  const int r = q / nx, k = r / ny;
-  const int I = g.lo[0] + (q - r * nx), J = g.lo[1] + (r - k * ny), K = g.lo[2] + k;
-  const FiBox& b = boxes[g.fi];
-  stage[b.soff + (I - b.lo[0] + 1) + (int64_t)b.sx * ((J - b.lo[1] + 1) + (int64_t)b.sy * (K - b.lo[2] + 1))] =
-      coarse[cidx(g.cbox, I, J, K)];
-}
-
-// One thread per coarse cell of b: interpconstant, then on b_mod the central
-// slopes (interpcentralslope), the limiter (interplimit) and the three
-// linear corrections (interplinear, dir 0, 1, 2).  Threads of a warp take
-// consecutive x cells, so each of the eight fine stores covers contiguous
-// slots of one colour half.
+// Coarse cell (I, J, K) of b, its staging value at s (strides sy, sz): the
+// eight fine cells.  interpconstant, then on b_mod the central slopes
+// (interpcentralslope), the limiter (interplimit) and the three linear
+// corrections (interplinear, dir 0, 1, 2).
 template <class FI>
-__global__ void k_fi_interp(const FiBox* boxes, const Chunk* ch, const double* __restrict__ stage, FI fidx,
-                            double* __restrict__ fine, int pwc) {
-  const Chunk c = ch[blockIdx.x];
-  const FiBox b = boxes[c.box];
-  const int q = c.start + threadIdx.x;
-  const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
-  if (q >= nx * ny * nz) return;
-  const int r = q / nx, kk = r / ny;
-  const int I = b.lo[0] + (q - r * nx), J = b.lo[1] + (r - kk * ny), K = b.lo[2] + kk;
-  const int64_t sy = b.sx, sz = (int64_t)b.sx * b.sy;
-  const double* s = stage + b.soff + (I - b.lo[0] + 1) + sy * (J - b.lo[1] + 1) + sz * (K - b.lo[2] + 1);
+__device__ __forceinline__ void interpCell(const FiBox& b, int I, int J, int K, const double* s, int sy, int sz,
+                                           FI fidx, double* __restrict__ fine, int pwc) {
   const double v = s[0];
   const bool lin = !pwc && I >= b.mlo[0] && I <= b.mhi[0] && J >= b.mlo[1] && J <= b.mhi[1] && K >= b.mlo[2] &&
                    K <= b.mhi[2];
@@ -129,6 +110,102 @@ __global__ void k_fi_interp(const FiBox* boxes, const Chunk* ch, const double* _
       }
 }
 
+// One-kernel path: block = fine box.  Its gather items (grow(b, 1) & domain
+// split over the coarse boxes, LevelData::copyTo into the coarsened fine
+// layout, FineInterp.cpp:148-160) go to shared memory; then one thread per
+// coarse cell of b, consecutive x cells on consecutive threads, so each of
+// the eight fine stores of a warp covers contiguous slots.
+template <class CI, class FI>
+__global__ void __launch_bounds__(kFusedThreads) k_fi_fused(const FiBox* boxes, const int* itemStart,
+                                                            const FiGather* gathers, CI cidx,
+                                                            const double* __restrict__ coarse, FI fidx,
+                                                            double* __restrict__ fine, int pwc) {
+  extern __shared__ double st[];
+  const FiBox b = boxes[blockIdx.x];
+  const int sy = b.sx, sz = b.sx * b.sy;
+  const int i0 = itemStart[blockIdx.x], i1 = itemStart[blockIdx.x + 1];
+  for (int it = i0; it < i1; ++it) {
+    const FiGather g = gathers[it];
+    const int nx = g.hi[0] - g.lo[0] + 1, ny = g.hi[1] - g.lo[1] + 1, n = nx * ny * (g.hi[2] - g.lo[2] + 1);
+    for (int q = threadIdx.x; q < n; q += kFusedThreads) {
+      const int r = q / nx, k = r / ny;
+      const int I = g.lo[0] + (q - r * nx), J = g.lo[1] + (r - k * ny), K = g.lo[2] + k;
+      st[(I - b.lo[0] + 1) + sy * (J - b.lo[1] + 1) + sz * (K - b.lo[2] + 1)] = coarse[cidx(g.cbox, I, J, K)];
+    }
+  }
+  __syncthreads();
+  const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, n = nx * ny * (b.hi[2] - b.lo[2] + 1);
+  for (int q = threadIdx.x; q < n; q += kFusedThreads) {
+    const int r = q / nx, kk = r / ny;
+    const int i = q - r * nx, j = r - kk * ny;
+    interpCell(b, b.lo[0] + i, b.lo[1] + j, b.lo[2] + kk, st + (i + 1) + sy * (j + 1) + sz * (kk + 1), sy, sz,
+               fidx, fine, pwc);
+  }
+}
+
+// Two-kernel path, step 1: coarse cells of grow(b, 1) & domain into the
+// staging blocks in device memory.
+template <class CI>
+__global__ void k_fi_gather(const FiGather* gathers, const FiBox* boxes, const Chunk* ch, CI cidx,
+                            const double* __restrict__ coarse, double* __restrict__ stage) {
+  const Chunk c = ch[blockIdx.x];
+  const FiGather g = gathers[c.box];
+  const int q = c.start + threadIdx.x;
+  const int nx = g.hi[0] - g.lo[0] + 1, ny = g.hi[1] - g.lo[1] + 1, nz = g.hi[2] - g.lo[2] + 1;
+  if (q >= nx * ny * nz) return;
+  const int r = q / nx, k = r / ny;
+  const int I = g.lo[0] + (q - r * nx), J = g.lo[1] + (r - k * ny), K = g.lo[2] + k;
+  const FiBox& b = boxes[g.fi];
+  stage[b.soff + (I - b.lo[0] + 1) + (int64_t)b.sx * ((J - b.lo[1] + 1) + (int64_t)b.sy * (K - b.lo[2] + 1))] =
+      coarse[cidx(g.cbox, I, J, K)];
+}
+
+// Two-kernel path, step 2: one thread per coarse cell of b.
+template <class FI>
+__global__ void k_fi_interp(const FiBox* boxes, const Chunk* ch, const double* __restrict__ stage, FI fidx,
+                            double* __restrict__ fine, int pwc) {
+  const Chunk c = ch[blockIdx.x];
+  const FiBox b = boxes[c.box];
+  const int q = c.start + threadIdx.x;
+  const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
+  if (q >= nx * ny * nz) return;
+  const int r = q / nx, kk = r / ny;
+  const int i = q - r * nx, j = r - kk * ny;
+  const int sy = b.sx, sz = b.sx * b.sy;
+  interpCell(b, b.lo[0] + i, b.lo[1] + j, b.lo[2] + kk, stage + b.soff + (i + 1) + sy * (j + 1) + sz * (kk + 1),
+             sy, sz, fidx, fine, pwc);
+}
+
+template <class CI, class FI>
+void launch(cudaStream_t s, bool fused, int nbox, size_t smem, int nGatherCh, int nBoxCh, const FiBox* boxes,
+            const int* itemStart, const FiGather* gathers, const Chunk* gatherCh, const Chunk* boxCh, double* stage,
+            CI cidx, const double* coarse, FI fidx, double* fine, bool pwc) {
+  if (fused) {
+    if (nbox == 0) return;
+    static bool attr = false;  // once per instantiation
+    if (!attr) {
+      ck(cudaFuncSetAttribute(k_fi_fused<CI, FI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmemMax),
+         "fine interpolation smem attribute");
+      attr = true;
+    }
+    k_fi_fused<CI, FI><<<nbox, kFusedThreads, smem, s>>>(boxes, itemStart, gathers, cidx, coarse, fidx, fine,
+                                                         pwc ? 1 : 0);
+    ck(cudaGetLastError(), "fine interpolation");
+    addLaunches(1);
+    return;
+  }
+  if (nGatherCh) {
+    k_fi_gather<<<nGatherCh, kChunk, 0, s>>>(gathers, boxes, gatherCh, cidx, coarse, stage);
+    ck(cudaGetLastError(), "fine interpolation gather");
+    addLaunches(1);
+  }
+  if (nBoxCh) {
+    k_fi_interp<<<nBoxCh, kChunk, 0, s>>>(boxes, boxCh, stage, fidx, fine, pwc ? 1 : 0);
+    ck(cudaGetLastError(), "fine interpolation");
+    addLaunches(1);
+  }
+}
+
 }  // namespace
 
 int64_t flatBoxes(const std::vector<Box>& grids, std::vector<FlatBox>& out) {
@@ -147,13 +224,14 @@ int64_t flatBoxes(const std::vector<Box>& grids, std::vector<FlatBox>& out) {
 }
 
 FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cindex, const Box& coarseDomain,
-                           const std::vector<Box>& fine, cudaStream_t s)
+                           const std::vector<Box>& fine, cudaStream_t s, bool allowFused)
     : s_(s) {
   std::vector<FiBox> boxes;
   std::vector<FiGather> gathers;
   std::vector<Chunk> boxCh, gatherCh;
+  std::vector<int> itemStart(1, 0);
   std::vector<int> hits;
-  int64_t soff = 0;
+  int64_t soff = 0, maxStage = 0;
   for (size_t f = 0; f < fine.size(); ++f) {
     if (!fine[f].coarsenable(2)) throw std::invalid_argument("cmg: fine box not coarsenable by 2");
     const Box b = fine[f].coarsen(2);
@@ -171,7 +249,9 @@ FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cinde
     fb.sx = b.size(0) + 2;
     fb.sy = b.size(1) + 2;
     fb.soff = soff;
-    soff += (int64_t)fb.sx * fb.sy * (b.size(2) + 2);
+    const int64_t stageCells = (int64_t)fb.sx * fb.sy * (b.size(2) + 2);
+    soff += stageCells;
+    maxStage = std::max(maxStage, stageCells);
     const int item = (int)boxes.size();
     boxes.push_back(fb);
     chunks(boxCh, item, b.numPts());
@@ -193,10 +273,14 @@ FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cinde
       inG += r.numPts();
       inB += (b & coarse[cb]).numPts();
     }
+    itemStart.push_back((int)gathers.size());
     if (inG != g.numPts()) nested_ = false;
     if (inB != b.numPts()) covered_ = false;
   }
-  stageCells_ = soff;
+  nbox_ = (int)boxes.size();
+  fused_ = allowFused && (size_t)maxStage * sizeof(double) <= kFusedSmemMax;
+  smem_ = (size_t)maxStage * sizeof(double);
+  stageCells_ = fused_ ? 0 : soff;
   nBoxCh_ = (int)boxCh.size();
   nGatherCh_ = (int)gatherCh.size();
 
@@ -204,12 +288,13 @@ FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cinde
   auto up = [](size_t n) { return (n + 255) & ~(size_t)255; };
   const size_t bBytes = up(boxes.size() * sizeof(FiBox)), bcBytes = up(boxCh.size() * sizeof(Chunk));
   const size_t gBytes = up(gathers.size() * sizeof(FiGather)), gcBytes = up(gatherCh.size() * sizeof(Chunk));
+  const size_t iBytes = up(itemStart.size() * sizeof(int));
   const size_t sBytes = up((size_t)stageCells_ * sizeof(double));
-  const size_t total = bBytes + bcBytes + gBytes + gcBytes + sBytes;
-  if (total == 0) return;
-  ck(cudaMallocAsync(&mem_, total, s_), "cudaMalloc fine interpolation plan");
+  const size_t tables = bBytes + bcBytes + gBytes + gcBytes + iBytes;
+  if (tables + sBytes == 0) return;
+  ck(cudaMallocAsync(&mem_, tables + sBytes, s_), "cudaMalloc fine interpolation plan");
   char* p = (char*)mem_;
-  std::vector<char> host(bBytes + bcBytes + gBytes + gcBytes);
+  std::vector<char> host(tables);
   auto put = [&](size_t at, const void* src, size_t n) {
     if (n) std::memcpy(host.data() + at, src, n);
   };
@@ -217,12 +302,14 @@ FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cinde
   put(bBytes, boxCh.data(), boxCh.size() * sizeof(Chunk));
   put(bBytes + bcBytes, gathers.data(), gathers.size() * sizeof(FiGather));
   put(bBytes + bcBytes + gBytes, gatherCh.data(), gatherCh.size() * sizeof(Chunk));
-  if (!host.empty()) ck(cudaMemcpyAsync(p, host.data(), host.size(), cudaMemcpyHostToDevice, s_), "fine interpolation plan h2d");
+  put(bBytes + bcBytes + gBytes + gcBytes, itemStart.data(), itemStart.size() * sizeof(int));
+  ck(cudaMemcpyAsync(p, host.data(), host.size(), cudaMemcpyHostToDevice, s_), "fine interpolation plan h2d");
   boxes_ = (const FiBox*)p;
   boxCh_ = (const Chunk*)(p + bBytes);
   gathers_ = (const FiGather*)(p + bBytes + bcBytes);
   gatherCh_ = (const Chunk*)(p + bBytes + bcBytes + gBytes);
-  stage_ = (double*)(p + bBytes + bcBytes + gBytes + gcBytes);
+  itemStart_ = (const int*)(p + bBytes + bcBytes + gBytes + gcBytes);
+  stage_ = stageCells_ ? (double*)(p + tables) : nullptr;
   ck(cudaStreamSynchronize(s_), "fine interpolation plan sync");
 }
 
@@ -241,29 +328,15 @@ void FineInterpOp::check(bool pwc) const {
 
 void FineInterpOp::run(const BoxDesc* cboxes, const double* coarse, const BoxDesc* fboxes, double* fine, bool pwc) {
   check(pwc);
-  if (nGatherCh_) {
-    k_fi_gather<<<nGatherCh_, kChunk, 0, s_>>>(gathers_, boxes_, gatherCh_, RBCells{cboxes}, coarse, stage_);
-    ck(cudaGetLastError(), "fine interpolation gather");
-  }
-  if (nBoxCh_) {
-    k_fi_interp<<<nBoxCh_, kChunk, 0, s_>>>(boxes_, boxCh_, stage_, RBCells{fboxes}, fine, pwc ? 1 : 0);
-    ck(cudaGetLastError(), "fine interpolation");
-  }
-  addLaunches(kernelLaunches());
+  launch(s_, fused_, nbox_, smem_, nGatherCh_, nBoxCh_, boxes_, itemStart_, gathers_, gatherCh_, boxCh_, stage_,
+         RBCells{cboxes}, coarse, RBCells{fboxes}, fine, pwc);
 }
 
 void FineInterpOp::runFlat(const FlatBox* cboxes, const double* coarse, const FlatBox* fboxes, double* fine,
                            bool pwc) {
   check(pwc);
-  if (nGatherCh_) {
-    k_fi_gather<<<nGatherCh_, kChunk, 0, s_>>>(gathers_, boxes_, gatherCh_, FlatCells{cboxes}, coarse, stage_);
-    ck(cudaGetLastError(), "fine interpolation gather");
-  }
-  if (nBoxCh_) {
-    k_fi_interp<<<nBoxCh_, kChunk, 0, s_>>>(boxes_, boxCh_, stage_, FlatCells{fboxes}, fine, pwc ? 1 : 0);
-    ck(cudaGetLastError(), "fine interpolation");
-  }
-  addLaunches(kernelLaunches());
+  launch(s_, fused_, nbox_, smem_, nGatherCh_, nBoxCh_, boxes_, itemStart_, gathers_, gatherCh_, boxCh_, stage_,
+         FlatCells{cboxes}, coarse, FlatCells{fboxes}, fine, pwc);
 }
 
 }  // namespace cmg

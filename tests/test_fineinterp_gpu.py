@@ -2,7 +2,8 @@
 standalone cmg_fine_interp object) against the reference's FineInterp output
 recorded in the fixtures: bit for bit.  At the config-1 sizes, properties
 that hold exactly: a constant stays constant, scaling the coarse data by a
-power of two scales the fine data by it, and the two entry points agree."""
+power of two scales the fine data by it, and piecewise-constant
+interpolation copies every parent."""
 import numpy as np
 import pytest
 
@@ -106,4 +107,26 @@ def test_improperly_nested_level_is_an_error(cmg):
         fi.interp_to_fine(np.zeros(64))  # grow(b, 1) & domain reaches past the coarse box
     out = fi.interp_to_fine(np.arange(64.0), pwc=True)
     assert out.size == 512 and out[0] == 0.0 and out[-1] == 63.0
+    fi.close()
+
+
+@pytest.mark.gpu
+def test_large_boxes_take_the_two_kernel_path(cmg):
+    """A fine box whose staging block exceeds shared memory (48^3 fine, 26^3
+    coarse staging cells) sends the whole level through the gather kernel and
+    the interpolation kernel; both entry points still equal the numpy
+    restatement of the reference bit for bit."""
+    from test_fineinterp import fine_interp_numpy
+    import make_golden_fineinterp as mg
+    coarse_boxes = [(x, y, z, x + 15, y + 15, z + 15) for z in (0, 16) for y in (0, 16) for x in (0, 16)]
+    fine_boxes = [(8, 8, 8, 55, 55, 55), (56, 0, 0, 63, 7, 7)]
+    c = mg.seeded_field(coarse_boxes, 32, 77)
+    want = fine_interp_numpy(coarse_boxes, c, fine_boxes, 32, 0)
+    h = cmg.Hierarchy(32, [coarse_boxes, fine_boxes])
+    h.set_phi(0, c)
+    h.interp_to_fine(1)
+    assert np.array_equal(h.phi(1), want)
+    h.close()
+    fi = cmg.FineInterp((0, 0, 0, 63, 63, 63), fine_boxes, coarse_boxes)
+    assert np.array_equal(fi.interp_to_fine(c), want)
     fi.close()

@@ -118,11 +118,13 @@ def test_large_boxes_take_the_two_kernel_path(cmg):
     restatement of the reference bit for bit."""
     from test_fineinterp import fine_interp_numpy
     import make_golden_fineinterp as mg
-    coarse_boxes = [(x, y, z, x + 15, y + 15, z + 15) for z in (0, 16) for y in (0, 16) for x in (0, 16)]
+    # in the hierarchy's (sorted) box order, which its data follow
+    coarse_boxes = sorted((x, y, z, x + 15, y + 15, z + 15) for z in (0, 16) for y in (0, 16) for x in (0, 16))
     fine_boxes = [(8, 8, 8, 55, 55, 55), (56, 0, 0, 63, 7, 7)]
     c = mg.seeded_field(coarse_boxes, 32, 77)
     want = fine_interp_numpy(coarse_boxes, c, fine_boxes, 32, 0)
     h = cmg.Hierarchy(32, [coarse_boxes, fine_boxes])
+    assert h.boxes(0) == coarse_boxes and h.boxes(1) == fine_boxes
     h.set_phi(0, c)
     h.interp_to_fine(1)
     assert np.array_equal(h.phi(1), want)

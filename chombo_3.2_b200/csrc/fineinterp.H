@@ -35,6 +35,7 @@ struct FiBox {
   int lo[3], hi[3];
   int mlo[3], mhi[3];
   int sx, sy;
+  int gcells;    // cells of grow(b, 1) & domain that the coarse level holds
   int64_t soff;
 };
 
@@ -42,6 +43,7 @@ struct FiBox {
 struct FiGather {
   int fi, cbox;
   int lo[3], hi[3];
+  int cstart;    // cells of the box's earlier items
 };
 
 // A box of a flat valid-cell array: cells x fastest from off.

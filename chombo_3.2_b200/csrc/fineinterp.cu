@@ -22,6 +22,7 @@ namespace {
 
 constexpr int kChunk = 256;
 constexpr int kFusedThreads = 256;
+constexpr int kLoadILP = 8;
 constexpr size_t kFusedSmemMax = 96 * 1024;  // staging bytes per block on the one-kernel path
 
 inline void ck(cudaError_t e, const char* what) {
@@ -123,15 +124,30 @@ __global__ void __launch_bounds__(kFusedThreads) k_fi_fused(const FiBox* boxes, 
   extern __shared__ double st[];
   const FiBox b = boxes[blockIdx.x];
   const int sy = b.sx, sz = b.sx * b.sy;
-  const int i0 = itemStart[blockIdx.x], i1 = itemStart[blockIdx.x + 1];
-  for (int it = i0; it < i1; ++it) {
-    const FiGather g = gathers[it];
-    const int nx = g.hi[0] - g.lo[0] + 1, ny = g.hi[1] - g.lo[1] + 1, n = nx * ny * (g.hi[2] - g.lo[2] + 1);
-    for (int q = threadIdx.x; q < n; q += kFusedThreads) {
-      const int r = q / nx, k = r / ny;
-      const int I = g.lo[0] + (q - r * nx), J = g.lo[1] + (r - k * ny), K = g.lo[2] + k;
-      st[(I - b.lo[0] + 1) + sy * (J - b.lo[1] + 1) + sz * (K - b.lo[2] + 1)] = coarse[cidx(g.cbox, I, J, K)];
+  // The cells of all items in one enumeration, kLoadILP loads in flight per
+  // thread; each thread walks the items forward (its cells only increase).
+  const int i1 = itemStart[blockIdx.x + 1];
+  int it = itemStart[blockIdx.x];
+  for (int base = threadIdx.x; base < b.gcells; base += kLoadILP * kFusedThreads) {
+    double v[kLoadILP];
+    int at[kLoadILP];
+#pragma unroll
+    for (int u = 0; u < kLoadILP; ++u) {
+      const int q = base + u * kFusedThreads;
+      at[u] = -1;
+      if (q < b.gcells) {
+        while (it + 1 < i1 && gathers[it + 1].cstart <= q) ++it;
+        const FiGather& g = gathers[it];
+        const int nx = g.hi[0] - g.lo[0] + 1, ny = g.hi[1] - g.lo[1] + 1;
+        const int p = q - g.cstart, r = p / nx, k = r / ny;
+        const int I = g.lo[0] + (p - r * nx), J = g.lo[1] + (r - k * ny), K = g.lo[2] + k;
+        at[u] = (I - b.lo[0] + 1) + sy * (J - b.lo[1] + 1) + sz * (K - b.lo[2] + 1);
+        v[u] = coarse[cidx(g.cbox, I, J, K)];
+      }
     }
+#pragma unroll
+    for (int u = 0; u < kLoadILP; ++u)
+      if (at[u] >= 0) st[at[u]] = v[u];
   }
   __syncthreads();
   const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, n = nx * ny * (b.hi[2] - b.lo[2] + 1);
@@ -249,6 +265,7 @@ FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cinde
     fb.sx = b.size(0) + 2;
     fb.sy = b.size(1) + 2;
     fb.soff = soff;
+    fb.gcells = 0;
     const int64_t stageCells = (int64_t)fb.sx * fb.sy * (b.size(2) + 2);
     soff += stageCells;
     maxStage = std::max(maxStage, stageCells);
@@ -264,6 +281,7 @@ FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cinde
       FiGather gg;
       gg.fi = item;
       gg.cbox = cb;
+      gg.cstart = (int)inG;
       for (int d = 0; d < 3; ++d) {
         gg.lo[d] = r.lo[d];
         gg.hi[d] = r.hi[d];
@@ -273,6 +291,8 @@ FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cinde
       inG += r.numPts();
       inB += (b & coarse[cb]).numPts();
     }
+    // the cells the items hold (all of grow(b, 1) & domain when nested)
+    boxes[item].gcells = (int)inG;
     itemStart.push_back((int)gathers.size());
     if (inG != g.numPts()) nested_ = false;
     if (inB != b.numPts()) covered_ = false;

@@ -23,6 +23,7 @@ namespace {
 constexpr int kChunk = 256;
 constexpr int kFusedThreads = 256;
 constexpr int kLoadILP = 8;
+constexpr int kSeg = 8;  // planes per work item of the one-kernel path
 constexpr size_t kFusedSmemMax = 96 * 1024;  // staging bytes per block on the one-kernel path
 
 inline void ck(cudaError_t e, const char* what) {
@@ -37,11 +38,31 @@ void chunks(std::vector<Chunk>& out, int item, int64_t n) {
   for (int64_t s = 0; s < n; s += kChunk) out.push_back(Chunk{item, (int)s});
 }
 
+// The fine cells of one box addressed from a base: cell (2i + c0, 2j + c1,
+// 2k + c2), (i, j, k) local to the coarsened box, is at(lin(i, j, k) + c0 +
+// dy c1 + dz c2, (c0 + c1 + c2) & 1).
+struct FineRB {  // red-black level field (colourSlot / cellIndex)
+  int64_t off, half;
+  int dy, dz;
+  __device__ __forceinline__ int lin(int i, int j, int k) const { return (2 * i + 1) + dy * (2 * j + 1) + dz * (2 * k + 1); }
+  __device__ __forceinline__ int64_t at(int l, int colour) const { return off + colour * half + (l >> 1); }
+};
+struct FineFlat {  // flat valid-cell array
+  int64_t off;
+  int dy, dz;
+  __device__ __forceinline__ int lin(int i, int j, int k) const { return 2 * i + dy * 2 * j + dz * 2 * k; }
+  __device__ __forceinline__ int64_t at(int l, int) const { return off + l; }
+};
+
 // Element index of cell (i, j, k) of box `box` in a red-black level field.
 struct RBCells {
   const BoxDesc* b;
   __device__ __forceinline__ int64_t operator()(int box, int i, int j, int k) const {
     return cellIndex(b[box], i, j, k);
+  }
+  __device__ __forceinline__ FineRB rows(int box) const {
+    const BoxDesc x = b[box];
+    return FineRB{x.off, x.half, x.px, x.px * x.py};
   }
 };
 
@@ -52,7 +73,25 @@ struct FlatCells {
     const FlatBox& x = b[box];
     return x.off + (i - x.lo[0]) + (int64_t)x.nx * ((j - x.lo[1]) + (int64_t)x.ny * (k - x.lo[2]));
   }
+  __device__ __forceinline__ FineFlat rows(int box) const {
+    const FlatBox x = b[box];
+    return FineFlat{x.off, x.nx, x.nx * x.ny};
+  }
 };
+
+// Extrema of the 3 x 3 cells around p in its plane (row stride sy).
+__device__ __forceinline__ void planeExtrema(const double* p, int sy, double& mx, double& mn) {
+  mx = p[0];
+  mn = p[0];
+#pragma unroll
+  for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+    for (int di = -1; di <= 1; ++di) {
+      const double w = p[di + dj * sy];
+      mx = fmax(mx, w);
+      mn = fmin(mn, w);
+    }
+}
 
 // Coarse cell (I, J, K) of b, its staging value at s (strides sy, sz): the
 // eight fine cells.  interpconstant, then on b_mod the central slopes
@@ -150,12 +189,76 @@ __global__ void __launch_bounds__(kFusedThreads) k_fi_fused(const FiBox* boxes, 
       if (at[u] >= 0) st[at[u]] = v[u];
   }
   __syncthreads();
-  const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, n = nx * ny * (b.hi[2] - b.lo[2] + 1);
-  for (int q = threadIdx.x; q < n; q += kFusedThreads) {
-    const int r = q / nx, kk = r / ny;
-    const int i = q - r * nx, j = r - kk * ny;
-    interpCell(b, b.lo[0] + i, b.lo[1] + j, b.lo[2] + kk, st + (i + 1) + sy * (j + 1) + sz * (kk + 1), sy, sz,
-               fidx, fine, pwc);
+  // Work items: a column (i, j) of the coarsened box over up to kSeg planes,
+  // consecutive threads on consecutive i.  Down a column the 27-cell extrema
+  // come from three plane extrema, each plane's computed once.  Extrema over
+  // the same cells are the same numbers in any order; cells outside b_mod
+  // (whose neighbours may lie outside the domain) ignore them.
+  const auto fr = fidx.rows(b.fbox);
+  const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
+  const int ncol = nx * ny, nseg = (nz + kSeg - 1) / kSeg;
+  for (int w = threadIdx.x; w < ncol * nseg; w += kFusedThreads) {
+    const int seg = w / ncol, col = w - seg * ncol;
+    const int j = col / nx, i = col - j * nx;
+    const int k0 = seg * kSeg, k1 = min(k0 + kSeg, nz);
+    const int I = b.lo[0] + i, J = b.lo[1] + j;
+    const bool linIJ = !pwc && I >= b.mlo[0] && I <= b.mhi[0] && J >= b.mlo[1] && J <= b.mhi[1];
+    const double* c = st + (i + 1) + sy * (j + 1) + sz * (k0 + 1);
+    double mxm = 0.0, mnm = 0.0, mx0 = 0.0, mn0 = 0.0;
+    if (linIJ) {
+      planeExtrema(c - sz, sy, mxm, mnm);
+      planeExtrema(c, sy, mx0, mn0);
+    }
+    int l = fr.lin(i, j, k0);
+    for (int k = k0; k < k1; ++k, c += sz, l += 2 * fr.dz) {
+      const double v = c[0];
+      const int K = b.lo[2] + k;
+      const bool lin = linIJ && K >= b.mlo[2] && K <= b.mhi[2];
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      if (linIJ) {
+        double mxp, mnp;
+        planeExtrema(c + sz, sy, mxp, mnp);
+        if (lin) {
+          // interpcentralslope, interplimit
+          s0 = 0.5 * (c[1] - c[-1]);
+          s1 = 0.5 * (c[sy] - c[-sy]);
+          s2 = 0.5 * (c[sz] - c[-sz]);
+          const double smax = fmax(fmax(mxm, mx0), mxp), smin = fmin(fmin(mnm, mn0), mnp);
+          const double deltasum = 0.5 * (fabs(s0) + fabs(s1) + fabs(s2));
+          double eta = fmin(smax - v, v - smin);
+          // the reference's 1.e-9 is a single-precision Fortran literal
+          if (eta <= (double)1.0e-9f * fabs(smax)) {
+            eta = 0.0;
+          } else if (deltasum > eta) {
+            eta = eta / deltasum;
+          } else {
+            eta = 1.0;
+          }
+          s0 = eta * s0;
+          s1 = eta * s1;
+          s2 = eta * s2;
+        }
+        mxm = mx0;
+        mnm = mn0;
+        mx0 = mxp;
+        mn0 = mnp;
+      }
+      // interpconstant, then interplinear dir 0, 1, 2
+#pragma unroll
+      for (int c2 = 0; c2 < 2; ++c2)
+#pragma unroll
+        for (int c1 = 0; c1 < 2; ++c1)
+#pragma unroll
+          for (int c0 = 0; c0 < 2; ++c0) {
+            double f = v;
+            if (lin) {
+              f = f + (c0 ? 0.25 : -0.25) * s0;
+              f = f + (c1 ? 0.25 : -0.25) * s1;
+              f = f + (c2 ? 0.25 : -0.25) * s2;
+            }
+            fine[fr.at(l + c0 + fr.dy * c1 + fr.dz * c2, (c0 + c1 + c2) & 1)] = f;
+          }
+    }
   }
 }
 

@@ -572,7 +572,7 @@ def run_fineinterp(args):
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         t = json.load(open(tpath)).get("fineinterp")
-        traffic = t["dram_bytes_per_launch"] if t else None
+        traffic = t["dram_bytes_per_step"] if t else None
     cpu = None
     if not args.no_cpu_baseline:
         r = fineinterp_reference(meta, 1)
@@ -585,12 +585,14 @@ def run_fineinterp(args):
             "config": {"workload": "fineinterp-config1: interpToFine of levels 1 and 2 of the 3-level 128^3 "
                                    "hierarchy from the seeded right-hand side", "fine_cells_per_step": fine_cells,
                        "l2": "flushed (256 MB write) before every step",
-                       "timing": "sum of CUDA-event device times around each level's gather + interpolation"},
+                       "timing": "sum of CUDA-event device times around each level's interpolation launches"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_fi_gather + k_fi_interp (one timed region per level; algorithmic bytes: "
-                                   "8 B written per fine cell + 8 B read per coarse parent)",
-                         "launches": int(n_runs) * 2, "algorithmic_bytes_per_step": nbytes / args.steps},
+                         "traffic": traffic, "traffic_unit": "DRAM bytes per step (both levels)",
+                         "peak_kind": peak_kind,
+                         "kernel": "k_fi_fused: one launch per level, the coarse staging block of a fine box in "
+                                   "shared memory (algorithmic bytes: 8 B written per fine cell + 8 B read per "
+                                   "coarse parent)",
+                         "timed_regions": int(n_runs), "algorithmic_bytes_per_step": nbytes / args.steps},
             "parity_level2_vs_reference": parity, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches}
     print(json.dumps(line), flush=True)

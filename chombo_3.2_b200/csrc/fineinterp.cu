@@ -301,12 +301,11 @@ void launch(cudaStream_t s, bool fused, int nbox, size_t smem, int nGatherCh, in
             CI cidx, const double* coarse, FI fidx, double* fine, bool pwc) {
   if (fused) {
     if (nbox == 0) return;
-    static bool attr = false;  // once per instantiation
-    if (!attr) {
+    // above the default 48 KB the kernel needs the opt-in, which is per device
+    // (set on every such launch: a host call, no device work)
+    if (smem > 48 * 1024)
       ck(cudaFuncSetAttribute(k_fi_fused<CI, FI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmemMax),
          "fine interpolation smem attribute");
-      attr = true;
-    }
     k_fi_fused<CI, FI><<<nbox, kFusedThreads, smem, s>>>(boxes, itemStart, gathers, cidx, coarse, fidx, fine,
                                                          pwc ? 1 : 0);
     ck(cudaGetLastError(), "fine interpolation");

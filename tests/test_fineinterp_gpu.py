@@ -132,3 +132,20 @@ def test_large_boxes_take_the_two_kernel_path(cmg):
     fi = cmg.FineInterp((0, 0, 0, 63, 63, 63), fine_boxes, coarse_boxes)
     assert np.array_equal(fi.interp_to_fine(c), want)
     fi.close()
+
+
+@pytest.mark.gpu
+def test_staging_above_48kb_takes_the_shared_memory_opt_in(cmg):
+    """A 40^3 fine box (22^3 coarse staging cells, 85 KB) stays on the one-kernel path with the shared-memory
+    opt-in; the output equals the numpy restatement bit for bit."""
+    from test_fineinterp import fine_interp_numpy
+    import make_golden_fineinterp as mg
+    coarse_boxes = sorted((x, y, z, x + 15, y + 15, z + 15) for z in (0, 16) for y in (0, 16) for x in (0, 16))
+    fine_boxes = [(8, 8, 8, 47, 47, 47)]
+    c = mg.seeded_field(coarse_boxes, 32, 78)
+    want = fine_interp_numpy(coarse_boxes, c, fine_boxes, 32, 0)
+    h = cmg.Hierarchy(32, [coarse_boxes, fine_boxes])
+    h.set_phi(0, c)
+    h.interp_to_fine(1)
+    assert np.array_equal(h.phi(1), want)
+    h.close()

@@ -152,9 +152,9 @@ __device__ __forceinline__ void interpCell(const FiBox& b, int I, int J, int K, 
 
 // One-kernel path: block = fine box.  Its gather items (grow(b, 1) & domain
 // split over the coarse boxes, LevelData::copyTo into the coarsened fine
-// layout, FineInterp.cpp:148-160) go to shared memory; then one thread per
-// coarse cell of b, consecutive x cells on consecutive threads, so each of
-// the eight fine stores of a warp covers contiguous slots.
+// layout, FineInterp.cpp:148-160) go to shared memory; then each thread takes
+// a column segment of b's coarse cells, consecutive threads on consecutive x,
+// so each of the eight fine stores of a warp covers contiguous slots.
 template <class CI, class FI>
 __global__ void __launch_bounds__(kFusedThreads) k_fi_fused(const FiBox* boxes, const int* itemStart,
                                                             const FiGather* gathers, CI cidx,

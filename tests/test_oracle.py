@@ -53,7 +53,7 @@ def test_oracle_reproduces_golden(tmp_path, name):
         assert float(np.sum(rhs)) == meta["rhs_sum"][lev]
 
 
-@pytest.mark.parametrize("test", ["quadCFInterpTest", "testCoarseAverage"])
+@pytest.mark.parametrize("test", ["quadCFInterpTest", "testCoarseAverage", "testFineInterp"])
 def test_reference_amrtools_test_passes(test):
     exe = os.path.join(REFTESTS, test)
     if not os.path.exists(exe):

@@ -28,7 +28,8 @@ class Box(ctypes.Structure):
 class SolveParams(ctypes.Structure):
     _fields_ = [("pre", ctypes.c_int), ("post", ctypes.c_int), ("bottom", ctypes.c_int),
                 ("num_mg", ctypes.c_int), ("iter_max", ctypes.c_int), ("imin", ctypes.c_int),
-                ("eps", ctypes.c_double), ("hang", ctypes.c_double), ("norm_thresh", ctypes.c_double)]
+                ("eps", ctypes.c_double), ("hang", ctypes.c_double), ("norm_thresh", ctypes.c_double),
+                ("iter_min", ctypes.c_int)]
 
 
 class MLSolveParams(ctypes.Structure):
@@ -44,8 +45,8 @@ def mlsolve_params(mg_iters=1, mg_smooth=4, imax=80, num_restarts=5, eps=1e-6, r
 
 
 def solve_params(pre=4, post=4, bottom=4, num_mg=1, iter_max=100, imin=5, eps=1e-10, hang=1e-10,
-                 norm_thresh=1e-30):
-    return SolveParams(pre, post, bottom, num_mg, iter_max, imin, eps, hang, norm_thresh)
+                 norm_thresh=1e-30, iter_min=-1):
+    return SolveParams(pre, post, bottom, num_mg, iter_max, imin, eps, hang, norm_thresh, iter_min)
 
 
 class Request(ctypes.Structure):

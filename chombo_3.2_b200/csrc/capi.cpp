@@ -26,7 +26,8 @@ struct cmg_hierarchy {
 };
 
 struct cmg_fine_interp {
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // own stream: plan memory, and the work until cmg_fine_interp_set_stream
+  cudaStream_t work = nullptr;    // stream of the interpolation work
   cmg::FineInterpOp* op = nullptr;
   int64_t ncoarse = 0, nfine = 0;
   void* mem = nullptr;  // FlatBox tables of both layouts, then coarse and fine staging for host data
@@ -40,6 +41,13 @@ namespace {
 
 thread_local std::string g_err;
 
+// A solve whose residual norm became NaN or infinite: its outputs are
+// written, and the call returns CMG_EDIVERGED.
+struct Diverged : std::runtime_error {
+  explicit Diverged(int iter)
+      : std::runtime_error("cmg: residual norm is not finite after " + std::to_string(iter) + " iterations") {}
+};
+
 int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
@@ -50,6 +58,8 @@ int guard(F fn) {
   try {
     fn();
     return CMG_OK;
+  } catch (const Diverged& e) {
+    return fail(CMG_EDIVERGED, e.what());
   } catch (const std::bad_alloc& e) {
     return fail(CMG_ENOMEM, e.what());
   } catch (const std::invalid_argument& e) {
@@ -261,23 +271,31 @@ int cmg_set_phi(cmg_hierarchy* h, int level, const double* data, int on_device) 
 }
 
 namespace {
+cmg::SolveParams solverParams(const cmg_solve_params* p) {
+  if (!p) throw std::invalid_argument("cmg: null parameters");
+  cmg::SolveParams sp;
+  sp.pre = p->pre;
+  sp.post = p->post;
+  sp.bottom = p->bottom;
+  sp.numMG = p->num_mg;
+  sp.iterMax = p->iter_max;
+  sp.imin = p->imin;
+  sp.eps = p->eps;
+  sp.hang = p->hang;
+  sp.normThresh = p->norm_thresh;
+  sp.iterMin = p->iter_min;
+  if (sp.pre < 0 || sp.post < 0 || sp.bottom < 0 || sp.numMG < 1 || sp.iterMax < 0)
+    throw std::invalid_argument("cmg: invalid solver parameters");
+  return sp;
+}
+}  // namespace
+
+namespace {
 int solveWith(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
               double* history, int history_cap, int* history_len, bool mixed) {
   return guard([&]() {
     needLevel(h, 0);
-    if (!p) throw std::invalid_argument("cmg: null parameters");
-    cmg::SolveParams sp;
-    sp.pre = p->pre;
-    sp.post = p->post;
-    sp.bottom = p->bottom;
-    sp.numMG = p->num_mg;
-    sp.iterMax = p->iter_max;
-    sp.imin = p->imin;
-    sp.eps = p->eps;
-    sp.hang = p->hang;
-    sp.normThresh = p->norm_thresh;
-    if (sp.pre < 0 || sp.post < 0 || sp.bottom < 0 || sp.numMG < 1 || sp.iterMax < 0)
-      throw std::invalid_argument("cmg: invalid solver parameters");
+    const cmg::SolveParams sp = solverParams(p);
     cmg::SolveResult r = mixed ? h->solver->solveMixed(sp, zero_phi != 0) : h->solver->solve(sp, zero_phi != 0);
     if (exit_status) *exit_status = r.exitStatus;
     if (iterations) *iterations = r.iterations;
@@ -285,6 +303,7 @@ int solveWith(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* ex
     if (history_len) *history_len = n;
     if (history)
       for (int i = 0; i < n && i < history_cap; ++i) history[i] = r.history[i];
+    if (r.diverged) throw Diverged(r.iterations);
   });
 }
 }  // namespace
@@ -336,24 +355,6 @@ int cmg_set_alpha_beta(cmg_hierarchy* h, double alpha, double beta) {
   });
 }
 
-namespace {
-cmg::SolveParams solverParams(const cmg_solve_params* p) {
-  if (!p) throw std::invalid_argument("cmg: null parameters");
-  cmg::SolveParams sp;
-  sp.pre = p->pre;
-  sp.post = p->post;
-  sp.bottom = p->bottom;
-  sp.numMG = p->num_mg;
-  sp.iterMax = p->iter_max;
-  sp.imin = p->imin;
-  sp.eps = p->eps;
-  sp.hang = p->hang;
-  sp.normThresh = p->norm_thresh;
-  if (sp.pre < 0 || sp.post < 0 || sp.bottom < 0 || sp.numMG < 1 || sp.iterMax < 0)
-    throw std::invalid_argument("cmg: invalid solver parameters");
-  return sp;
-}
-}  // namespace
 
 int cmg_tga(cmg_hierarchy* h, const cmg_solve_params* p, double dt, int nsteps, int* exit_status,
             int* iterations) {
@@ -372,20 +373,8 @@ int cmg_backward_euler(cmg_hierarchy* h, const cmg_solve_params* p, double dt, i
                        int* exit_status, int* iterations) {
   return guard([&]() {
     needLevel(h, 0);
-    if (!p) throw std::invalid_argument("cmg: null parameters");
     if (nsteps < 0 || !(dt > 0)) throw std::invalid_argument("cmg: invalid time step");
-    cmg::SolveParams sp;
-    sp.pre = p->pre;
-    sp.post = p->post;
-    sp.bottom = p->bottom;
-    sp.numMG = p->num_mg;
-    sp.iterMax = p->iter_max;
-    sp.imin = p->imin;
-    sp.eps = p->eps;
-    sp.hang = p->hang;
-    sp.normThresh = p->norm_thresh;
-    if (sp.pre < 0 || sp.post < 0 || sp.bottom < 0 || sp.numMG < 1 || sp.iterMax < 0)
-      throw std::invalid_argument("cmg: invalid solver parameters");
+    const cmg::SolveParams sp = solverParams(p);
     std::vector<cmg::SolveResult> r = h->solver->backwardEuler(sp, dt, nsteps, zero_phi != 0);
     for (int n = 0; n < nsteps; ++n) {
       if (exit_status) exit_status[n] = r[n].exitStatus;
@@ -431,6 +420,7 @@ int cmg_interp_to_fine(cmg_hierarchy* h, int level, int piecewise_constant) {
 int cmg_fine_interp_destroy(cmg_fine_interp* fi) {
   return guard([&]() {
     if (!fi) return;
+    if (fi->work && fi->work != fi->stream) cudaStreamSynchronize(fi->work);
     delete fi->op;
     if (fi->mem) cudaFreeAsync(fi->mem, fi->stream);
     if (fi->stream) {
@@ -472,6 +462,7 @@ int cmg_fine_interp_create(const int fine_domain_lo[3], const int fine_domain_hi
     try {
       cudaError_t e = cudaStreamCreateWithFlags(&fi->stream, cudaStreamNonBlocking);
       if (e != cudaSuccess) throw std::runtime_error(std::string("cmg: stream: ") + cudaGetErrorString(e));
+      fi->work = fi->stream;
       fi->op = new cmg::FineInterpOp(cb, cindex, cdom, fb, fi->stream);
       auto up = [](size_t n) { return (n + 255) & ~(size_t)255; };
       const size_t cB = up(cf.size() * sizeof(cmg::FlatBox)), fB = up(ff.size() * sizeof(cmg::FlatBox));
@@ -508,16 +499,16 @@ int cmg_fine_interp_run(cmg_fine_interp* fi, const double* coarse, double* fine,
     const double* c = coarse;
     double* f = fine;
     if (!on_device) {
-      ck(cudaMemcpyAsync(fi->dcoarse, coarse, fi->ncoarse * sizeof(double), cudaMemcpyHostToDevice, fi->stream),
+      ck(cudaMemcpyAsync(fi->dcoarse, coarse, fi->ncoarse * sizeof(double), cudaMemcpyHostToDevice, fi->work),
          "fine interpolation h2d");
       c = fi->dcoarse;
       f = fi->dfine;
     }
     fi->op->runFlat(fi->cflat, c, fi->fflat, f, pwc);
     if (!on_device)
-      ck(cudaMemcpyAsync(fine, fi->dfine, fi->nfine * sizeof(double), cudaMemcpyDeviceToHost, fi->stream),
+      ck(cudaMemcpyAsync(fine, fi->dfine, fi->nfine * sizeof(double), cudaMemcpyDeviceToHost, fi->work),
          "fine interpolation d2h");
-    ck(cudaStreamSynchronize(fi->stream), "fine interpolation sync");
+    ck(cudaStreamSynchronize(fi->work), "fine interpolation sync");
   });
 }
 
@@ -618,6 +609,7 @@ int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_infligh
       r.params.eps = a.params.eps;
       r.params.hang = a.params.hang;
       r.params.normThresh = a.params.norm_thresh;
+      r.params.iterMin = a.params.iter_min;
       r.mixed = a.mixed != 0;
       r.graphs = a.graphs != 0;
       r.deviceTags = a.device_tags != 0;
@@ -717,7 +709,204 @@ int cmg_get_stream(const cmg_hierarchy* h, void** stream) {
   return guard([&]() {
     needLevel(h, 0);
     if (!stream) throw std::invalid_argument("cmg: null output");
-    *stream = (void*)h->stream;
+    *stream = (void*)h->solver->stream();
+  });
+}
+
+int cmg_set_stream(cmg_hierarchy* h, void* stream) {
+  return guard([&]() {
+    needLevel(h, 0);
+    h->solver->setStream((cudaStream_t)stream);
+  });
+}
+
+int cmg_fine_interp_set_stream(cmg_fine_interp* fi, void* stream) {
+  return guard([&]() {
+    if (!fi || !fi->op) throw std::invalid_argument("cmg: null fine interpolation");
+    cudaStream_t s = stream ? (cudaStream_t)stream : fi->stream;
+    if (s == fi->work) return;
+    cudaError_t e = cudaStreamSynchronize(fi->work);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("cmg: stream switch: ") + cudaGetErrorString(e));
+    fi->work = s;
+    fi->op->setStream(s);
+  });
+}
+
+int cmg_fine_interp_is_fused(const cmg_fine_interp* fi, int* out) {
+  return guard([&]() {
+    if (!fi || !fi->op || !out) throw std::invalid_argument("cmg: null fine interpolation argument");
+    *out = fi->op->fused() ? 1 : 0;
+  });
+}
+
+// ---------------------------------------------------------------- operator-level calls
+
+namespace {
+cmg::Solver& opSolver(cmg_hierarchy* h, int lev) {
+  needLevel(h, 0);
+  h->solver->opPlan(lev);  // range check
+  return *h->solver;
+}
+const cmg::Solver& opSolverC(const cmg_hierarchy* h, int lev) {
+  needLevel(h, 0);
+  h->solver->opPlan(lev);
+  return *h->solver;
+}
+void needPtr(const void* p) {
+  if (!p) throw std::invalid_argument("cmg: null operator argument");
+}
+}  // namespace
+
+int cmg_op_num_mg_depths(const cmg_hierarchy* h, int* out) {
+  return guard([&]() {
+    needLevel(h, 0);
+    needPtr(out);
+    *out = h->solver->numMGDepths();
+  });
+}
+
+int cmg_op_num_boxes(const cmg_hierarchy* h, int lev, int* out) {
+  return guard([&]() {
+    needPtr(out);
+    *out = (int)opSolverC(h, lev).opPlan(lev).grids.size();
+  });
+}
+
+int cmg_op_get_boxes(const cmg_hierarchy* h, int lev, cmg_box* out, int cap) {
+  return guard([&]() {
+    needPtr(out);
+    const cmg::Layout& g = opSolverC(h, lev).opPlan(lev).grids;
+    if (cap < (int)g.size()) throw std::invalid_argument("cmg: box buffer too small");
+    for (size_t b = 0; b < g.size(); ++b) fromBox(g[b], out[b]);
+  });
+}
+
+int cmg_op_size(const cmg_hierarchy* h, int lev, int64_t* out) {
+  return guard([&]() {
+    needPtr(out);
+    *out = opSolverC(h, lev).opSize(lev);
+  });
+}
+
+int cmg_op_coarsened_size(const cmg_hierarchy* h, int level, int64_t* out) {
+  return guard([&]() {
+    needPtr(out);
+    *out = opSolverC(h, level).opCoarsenedSize(level);
+  });
+}
+
+int cmg_op_residual(cmg_hierarchy* h, int lev, double* lhs, const double* phi, const double* rhs, int homogeneous) {
+  return guard([&]() {
+    needPtr(lhs);
+    opSolver(h, lev).opResidual(lev, lhs, phi, rhs, homogeneous != 0);
+  });
+}
+
+int cmg_op_apply(cmg_hierarchy* h, int lev, double* lhs, const double* phi, int homogeneous) {
+  return guard([&]() {
+    needPtr(lhs);
+    opSolver(h, lev).opApply(lev, lhs, phi, homogeneous != 0);
+  });
+}
+
+int cmg_op_relax(cmg_hierarchy* h, int lev, double* phi, const double* rhs, int iterations) {
+  return guard([&]() {
+    if (iterations < 0) throw std::invalid_argument("cmg: negative relaxation count");
+    opSolver(h, lev).opRelax(lev, phi, rhs, iterations);
+  });
+}
+
+int cmg_op_precond(cmg_hierarchy* h, int lev, double* cor, const double* res) {
+  return guard([&]() { opSolver(h, lev).opPreCond(lev, cor, res); });
+}
+
+int cmg_op_restrict_residual(cmg_hierarchy* h, int lev, double* res_coarse, const double* phi, const double* rhs) {
+  return guard([&]() { opSolver(h, lev).opRestrictResidual(lev, res_coarse, phi, rhs); });
+}
+
+int cmg_op_prolong_increment(cmg_hierarchy* h, int lev, double* phi, const double* corr_coarse) {
+  return guard([&]() { opSolver(h, lev).opProlongIncrement(lev, phi, corr_coarse); });
+}
+
+int cmg_op_amr_operator(cmg_hierarchy* h, int level, int form, double* out, const double* phi_fine,
+                        const double* phi, const double* phi_coarse, const double* rhs) {
+  return guard([&]() {
+    needPtr(out);
+    opSolver(h, level).opAMROperator(level, out, phi_fine, phi, phi_coarse, rhs, form);
+  });
+}
+
+int cmg_op_amr_restrict(cmg_hierarchy* h, int level, double* res_coarsened, const double* residual,
+                        const double* correction, const double* coarse_correction) {
+  return guard([&]() {
+    needPtr(res_coarsened);
+    if (correction) needPtr(coarse_correction);
+    opSolver(h, level).opAMRRestrict(level, res_coarsened, residual, correction, coarse_correction);
+  });
+}
+
+int cmg_op_assign_coarsened(cmg_hierarchy* h, int level, double* coarse, const double* coarsened) {
+  return guard([&]() {
+    needPtr(coarsened);
+    opSolver(h, level).opAssignCoarsened(level, coarse, coarsened);
+  });
+}
+
+int cmg_op_amr_prolong(cmg_hierarchy* h, int level, double* correction, const double* coarse_correction) {
+  return guard([&]() { opSolver(h, level).opAMRProlong(level, correction, coarse_correction); });
+}
+
+int cmg_op_amr_update_residual(cmg_hierarchy* h, int level, double* residual, const double* correction,
+                               const double* coarse_correction) {
+  return guard([&]() { opSolver(h, level).opAMRUpdateResidual(level, residual, correction, coarse_correction); });
+}
+
+int cmg_op_cf_interp(cmg_hierarchy* h, int level, double* phi, const double* phi_coarse) {
+  return guard([&]() {
+    needPtr(phi_coarse);
+    opSolver(h, level).opCFInterp(level, phi, phi_coarse);
+  });
+}
+
+int cmg_op_zero_covered(cmg_hierarchy* h, int level, double* data) {
+  return guard([&]() { opSolver(h, level).opZeroCovered(level, data); });
+}
+
+int cmg_op_axby(cmg_hierarchy* h, int lev, double* lhs, const double* x, const double* y, double a, double b) {
+  return guard([&]() {
+    needPtr(lhs);
+    needPtr(x);
+    needPtr(y);
+    opSolver(h, lev).opAxby(lev, lhs, x, y, a, b);
+  });
+}
+
+int cmg_op_incr(cmg_hierarchy* h, int lev, double* lhs, const double* x, double scale) {
+  return guard([&]() {
+    needPtr(lhs);
+    needPtr(x);
+    opSolver(h, lev).opIncr(lev, lhs, x, scale);
+  });
+}
+
+int cmg_op_scale(cmg_hierarchy* h, int lev, double* lhs, double scale) {
+  return guard([&]() {
+    needPtr(lhs);
+    opSolver(h, lev).opScale(lev, lhs, scale);
+  });
+}
+
+int cmg_op_dot(cmg_hierarchy* h, int lev, const double* x, const double* y, double* out) {
+  return guard([&]() {
+    needPtr(out);
+    *out = opSolver(h, lev).opDot(lev, x, y);
+  });
+}
+
+int cmg_op_norm(cmg_hierarchy* h, int lev, const double* x, int ord, double* out) {
+  return guard([&]() {
+    needPtr(out);
+    *out = opSolver(h, lev).opNorm(lev, x, ord);
   });
 }
 

@@ -78,10 +78,13 @@ class FineInterpOp {
   int64_t fineCells() const { return fineCells_; }
   // one kernel with the staging blocks in shared memory (every block fits)
   bool fused() const { return fused_; }
+  // Stream the interpolation kernels run on from now on (the plan's memory
+  // stays with the stream given at construction, which must outlive this).
+  void setStream(cudaStream_t s) { s_ = s; }
 
  private:
   void check(bool pwc) const;
-  cudaStream_t s_;
+  cudaStream_t s_, own_;
   bool nested_ = true, covered_ = true;
   int64_t fineCells_ = 0, stageCells_ = 0;
   int nBoxCh_ = 0, nGatherCh_ = 0, nbox_ = 0;

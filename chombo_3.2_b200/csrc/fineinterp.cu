@@ -343,7 +343,7 @@ int64_t flatBoxes(const std::vector<Box>& grids, std::vector<FlatBox>& out) {
 
 FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cindex, const Box& coarseDomain,
                            const std::vector<Box>& fine, cudaStream_t s, bool allowFused)
-    : s_(s) {
+    : s_(s), own_(s) {
   std::vector<FiBox> boxes;
   std::vector<FiGather> gathers;
   std::vector<Chunk> boxCh, gatherCh;
@@ -437,8 +437,9 @@ FineInterpOp::FineInterpOp(const std::vector<Box>& coarse, const BoxIndex& cinde
 
 FineInterpOp::~FineInterpOp() {
   if (mem_) {
-    cudaFreeAsync(mem_, s_);
     cudaStreamSynchronize(s_);
+    cudaFreeAsync(mem_, own_);
+    cudaStreamSynchronize(own_);
   }
 }
 

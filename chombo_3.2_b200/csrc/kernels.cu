@@ -462,10 +462,15 @@ __global__ void k_convert(D* dst, const S* src, int64_t n) {
 }
 
 __device__ __forceinline__ void atomicMaxPos(double* addr, double v) {
-  // v >= 0: the IEEE bit pattern of a non-negative double orders like an
-  // unsigned integer, so an integer max is a floating max.
+  // v >= 0 or a NaN without sign: the IEEE bit pattern of a non-negative
+  // double orders like an unsigned integer, so an integer max is a floating
+  // max, and such a NaN (exponent all ones, mantissa non-zero) is above
+  // every number, infinity included: a NaN anywhere wins.
   atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
 }
+
+// max(a, b) that keeps a NaN from either side (fmax drops it).
+__device__ __forceinline__ double nanMax(double a, double b) { return (b > a || b != b) ? b : a; }
 
 template <class T>
 __global__ void k_maxnorm(const BoxDesc* boxes, const Chunk* chunks, int nchunks, const T* f, double* out) {
@@ -476,16 +481,16 @@ __global__ void k_maxnorm(const BoxDesc* boxes, const Chunk* chunks, int nchunks
     Chunk ch = chunks[cix];
     const BoxDesc bd = boxes[ch.box];
     int i, j, k;
-    if (allCell(bd, ch.start + threadIdx.x, i, j, k)) v = fmax(v, fabs((double)f[cellIndex(bd, i, j, k)]));
+    if (allCell(bd, ch.start + threadIdx.x, i, j, k)) v = nanMax(v, fabs((double)f[cellIndex(bd, i, j, k)]));
   }
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
   __shared__ double red[CHUNK / 32];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
   if (threadIdx.x < 32) {
     v = threadIdx.x < CHUNK / 32 ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (threadIdx.x == 0) atomicMaxPos(out, v);
+    for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) atomicMaxPos(out, fabs(v));
   }
 }
 

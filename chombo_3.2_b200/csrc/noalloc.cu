@@ -69,14 +69,18 @@ double* scratchFor(int dev) {
 
 enum { NT = 256 };
 
+// max(a, b) that keeps a NaN from either side (fmax drops it), so that a
+// residual holding a NaN reduces to NaN.
+__device__ __forceinline__ double nanMax(double a, double b) { return (b > a || b != b) ? b : a; }
+
 __device__ __forceinline__ double blockMax(double v) {
   __shared__ double red[NT / 32];
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
   if (threadIdx.x < 32) {
     v = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
   }
   return v;
 }
@@ -90,7 +94,7 @@ __global__ void __launch_bounds__(NT) k_boxmax(const BoxDesc* boxes, const doubl
   double v = 0.0;
   for (int q = threadIdx.x; q < n; q += NT) {
     int i = bd.lo[0] + q % nx, r = q / nx, j = bd.lo[1] + r % ny, k = bd.lo[2] + r / ny;
-    v = fmax(v, fabs(f[cellIndex(bd, i, j, k)]));
+    v = nanMax(v, fabs(f[cellIndex(bd, i, j, k)]));
   }
   v = blockMax(v);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
@@ -99,9 +103,9 @@ __global__ void __launch_bounds__(NT) k_boxmax(const BoxDesc* boxes, const doubl
 // One block: fold the per-box maxima of a level into the running maximum.
 __global__ void __launch_bounds__(NT) k_foldmax(const double* part, int nbox, double* acc) {
   double v = 0.0;
-  for (int b = threadIdx.x; b < nbox; b += NT) v = fmax(v, part[b]);
+  for (int b = threadIdx.x; b < nbox; b += NT) v = nanMax(v, part[b]);
   v = blockMax(v);
-  if (threadIdx.x == 0) *acc = fmax(*acc, v);
+  if (threadIdx.x == 0) *acc = nanMax(*acc, v);
 }
 
 // Makes the stream's device current for the lifetime of the object.
@@ -142,22 +146,8 @@ double Solver::residualNormStatic(double* scratch) {
   ck(cudaMemsetAsync(acc, 0, sizeof(double), s_), "scratch reset");
   for (int ilev = 0; ilev <= lmax; ++ilev) {
     const LevelDev& L = amrDev_[ilev];
-    Coef<double> c = coefAMR(ilev);
-    if (lmax == 0) {
-      ghostFill(L, phi[0], true, s_);
-      residual(L, res[0], phi[0], rhs[0], c, s_);
-    } else if (ilev == lmax) {
-      quadCF(L, phi[ilev], phi[ilev - 1], s_);
-      ghostFill(L, phi[ilev], false, s_);
-      residual(L, res[ilev], phi[ilev], rhs[ilev], c, s_);
-    } else {
-      if (ilev > 0) quadCF(L, phi[ilev], phi[ilev - 1], s_);
-      ghostFill(L, phi[ilev], false, s_);
-      applyOp(L, res[ilev], phi[ilev], c, s_);
-      quadCF(amrDev_[ilev + 1], phi[ilev + 1], phi[ilev], s_);
-      reflux(L, res[ilev], phi[ilev], phi[ilev + 1], c, coefAMR(ilev + 1), s_);
-      negAdd(L, res[ilev], res[ilev], rhs[ilev], s_);
-    }
+    // The composite residual of the level, by the same code as every solve.
+    amrResidualLevel<double>(ilev, lmax, res, phi, rhs);
     if (ilev != lmax) zeroCovered(L, res[ilev], s_);
     if (L.nbox == 0) continue;
     k_boxmax<<<L.nbox, NT, 0, s_>>>(L.boxes, res[ilev], scratch);

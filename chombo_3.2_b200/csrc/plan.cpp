@@ -534,8 +534,16 @@ void buildQuadCFBox(const LevelPlan& F, const LevelPlan& C, const OwnerIndex& ow
     for (int side = -1; side <= 1; side += 2) {
       CellSet fineIVS;
       if (!faceCFSet(F, fbox, d, side, fineIVS)) continue;
-      Box packedBox = fineIVS.minBox();
-      bool packed = (packedBox.numPts() == fineIVS.numPts());
+      // CFStencil::define (AMRTools/CFStencil.cpp:240-326) starts from the
+      // face layer as a dense IntVectSet and removes the fine boxes cell by
+      // cell, which leaves the set's cached minBox at the whole face layer:
+      // the face is "packed" (Fortran PHISTAR / QUADINTERP arithmetic) only
+      // when no cell was removed, and its packed box is the face layer.
+      // A face partly covered by another fine box takes the C++ form even
+      // where its remaining cells form a box.
+      const Box faceLayer = fbox.adjCell(d, side, 1) & F.domain;
+      Box packedBox = faceLayer;
+      bool packed = (faceLayer.numPts() == fineIVS.numPts());
       CellSet base = fineIVS.coarsen(2);
       base.intersect(C.domain);
       // Good set: coarse cells of the widened face slab that are valid on

@@ -30,11 +30,13 @@ struct HierarchyDesc {
 struct SolveParams {
   int pre = 4, post = 4, bottom = 4, numMG = 1, iterMax = 100, imin = 5;
   double eps = 1e-10, hang = 1e-10, normThresh = 1e-30;
+  int iterMin = -1;  // m_iterMin: iterate at least this often whatever the norms
 };
 
 struct SolveResult {
   int exitStatus = 0, iterations = 0;
   std::vector<double> history;  // composite max-norm residual, start of each iteration, then final
+  bool diverged = false;        // a residual norm was NaN or infinite (the solve stopped there)
 };
 
 // BiCGStab over the whole hierarchy preconditioned by AMR multigrid, as the
@@ -122,6 +124,9 @@ class Solver {
   // nothing on success.
   double residualNormStatic(double* scratch);
   cudaStream_t stream() const { return s_; }
+  // Runs every later call's device work on stream s (nullptr: back to the
+  // hierarchy's own stream), after the work already queued has finished.
+  void setStream(cudaStream_t s);
   // Device bytes held by this hierarchy.
   size_t deviceBytes() const;
   // Bytes moved per V-cycle by the algorithmic count (each array read once,
@@ -161,7 +166,57 @@ class Solver {
   // and the tuner's sweep times (ms; empty when a mode was forced).
   void relaxVariants(std::vector<int>& inl, std::vector<float>& msFill, std::vector<float>& msInline);
 
+  // Operator-level calls (levelops.cu): one AMRLevelOp / MGLevelOp / LinearOp
+  // method of one level on host arrays in the ghosted box format (every
+  // box's FAB grown by one cell, x fastest, boxes in layout order).  lev >= 0
+  // is an AMR level, lev < 0 the multigrid depth -lev below level 0.  Inputs
+  // are read whole; outputs get their valid cells written (ghost positions
+  // unspecified).  Each call synchronises the solver's stream.
+  const LevelPlan& opPlan(int lev) const;
+  int64_t opSize(int lev) const;          // doubles in one ghosted array of lev
+  int64_t opCoarsenedSize(int l) const;   // doubles in one ghosted array of coarsen(level l, 2)
+  void opResidual(int lev, double* lhs, const double* phi, const double* rhs, bool homogeneous);
+  void opApply(int lev, double* lhs, const double* phi, bool homogeneous);
+  void opRelax(int lev, double* phi, const double* rhs, int iterations);
+  void opPreCond(int lev, double* cor, const double* res);
+  void opRestrictResidual(int lev, double* resCoarse, const double* phi, const double* rhs);
+  void opProlongIncrement(int lev, double* phi, const double* corrCoarse);
+  void opAMROperator(int l, double* out, const double* phiFine, const double* phi, const double* phiCoarse,
+                     const double* rhs, int form);
+  void opAMRRestrict(int l, double* resCoarsened, const double* residual, const double* corr,
+                     const double* corrCoarse);
+  void opAssignCoarsened(int l, double* coarse, const double* coarsened);
+  void opAMRProlong(int l, double* corr, const double* corrCoarse);
+  void opAMRUpdateResidual(int l, double* res, const double* corr, const double* corrCoarse);
+  void opZeroCovered(int l, double* data);
+  void opCFInterp(int l, double* phi, const double* phiCoarse);
+  void opAxby(int lev, double* lhs, const double* x, const double* y, double a, double b);
+  void opIncr(int lev, double* lhs, const double* x, double scale);
+  void opScale(int lev, double* lhs, double scale);
+  double opDot(int lev, const double* x, const double* y);
+  double opNorm(int lev, const double* x, int p);
+
  private:
+  // Device state of the operator-level calls of one level.
+  struct OpState {
+    static constexpr int kFields = 5;
+    int64_t size = 0, csize = 0;                // ghosted and coarsened-fine ghosted doubles
+    const int64_t* off = nullptr;               // per box: first element in the ghosted format
+    const int64_t* coff = nullptr;              // the same in the coarsened-fine format
+    double *packed = nullptr, *packed2 = nullptr, *packed3 = nullptr;  // host-format staging
+    double* field[kFields] = {};                // level-sized device fields
+  };
+  std::map<int, std::unique_ptr<OpState>> opStates_;
+  OpState& opState(int lev);
+  double* opField(int lev, int k);
+  void* uploadRaw(const void* src, size_t bytes);
+  double* opLoad(int lev, int k, const double* host);
+  void opStore(int lev, const double* f, double* host);
+  void opEnsureTuned();
+  std::vector<double> opBoxValues(int lev, int nbox);
+  const LevelDev& opDev(int lev) const;
+  Coef<double> opCoef(int lev) const;
+
   void uploadLevel(const LevelPlan& p, LevelDev& d);
   double* alloc(size_t n);
   Coef<double> coefAMR(int l) const;
@@ -181,7 +236,7 @@ class Solver {
   static constexpr double kBlockRelaxMaxCells = 32768;
   template <class T> void fill(const LevelDev& L, T* f, bool withCF, int par = -1);
   template <class T>
-  void amrResidualLevel(int ilev, int lmax, std::vector<T*>& res, std::vector<T*>& phi, std::vector<T*>& rhs);
+  void amrResidualLevel(int ilev, int lmax, T* const* res, T* const* phi, T* const* rhs);
   double computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);
   void launchAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);
   double readNorm();
@@ -263,7 +318,9 @@ class Solver {
   std::unique_ptr<DevBuf> stage_;
   double* staging(int64_t n);
 
-  cudaStream_t s_;
+  cudaStream_t s_;    // stream of the device work
+  cudaStream_t own_;  // the hierarchy's own stream: every allocation and free
+  void ownSync();     // completes pending allocations before s_ uses them
   HierarchyDesc desc_;
   std::vector<LevelPlan> amr_;
   std::vector<LevelPlan> mg_;        // multigrid depths below level 0; mg_[0] is depth 1

@@ -83,6 +83,20 @@ DevBuf::~DevBuf() {
   if (p) cudaFreeAsync(p, s);
 }
 
+// Work moves to the caller's stream; allocations stay on the hierarchy's own
+// stream (so they can be freed whatever becomes of the caller's), each one
+// completed before the work stream can use it.
+void Solver::setStream(cudaStream_t s) {
+  if (!s) s = own_;
+  if (s == s_) return;
+  ck(cudaStreamSynchronize(s_), "stream switch");
+  s_ = s;
+}
+
+void Solver::ownSync() {
+  if (s_ != own_) ck(cudaStreamSynchronize(own_), "allocation sync");
+}
+
 size_t Solver::deviceBytes() const {
   size_t n = stage_ ? stage_->bytes : 0;
   for (const auto& b : bufs_) n += b->bytes;
@@ -90,7 +104,8 @@ size_t Solver::deviceBytes() const {
 }
 
 double* Solver::alloc(size_t n) {
-  bufs_.emplace_back(new DevBuf(n * sizeof(double), s_));
+  bufs_.emplace_back(new DevBuf(n * sizeof(double), own_));
+  ownSync();
   double* p = (double*)bufs_.back()->p;
   ck(cudaMemsetAsync(p, 0, n * sizeof(double), s_), "memset");
   return p;
@@ -176,7 +191,7 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
 }
 
 Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
-    : s_(stream), desc_(desc), alpha0_(desc.alpha), beta0_(desc.beta) {
+    : s_(stream), own_(stream), desc_(desc), alpha0_(desc.alpha), beta0_(desc.beta) {
   const int nlev = (int)desc.boxes.size();
   if (nlev < 1) throw std::runtime_error("cmg: hierarchy needs at least one level");
   amr_.resize(nlev);
@@ -342,7 +357,8 @@ const void* Solver::regionPlan(const LevelPlan& p, int faceDir, int* nreg, int64
     RegionPlan rp;
     rp.n = (int)rc.size();
     rp.total = off;
-    rp.dev = upload(bufs_, rc, s_);
+    rp.dev = upload(bufs_, rc, own_);
+    ownSync();
     it = regionCache_.emplace(key, rp).first;
   }
   *nreg = it->second.n;
@@ -351,7 +367,11 @@ const void* Solver::regionPlan(const LevelPlan& p, int faceDir, int* nreg, int64
 }
 
 double* Solver::staging(int64_t n) {
-  if (!stage_ || stage_->bytes < (size_t)n * sizeof(double)) stage_.reset(new DevBuf(n * sizeof(double), s_));
+  if (!stage_ || stage_->bytes < (size_t)n * sizeof(double)) {
+    if (s_ != own_) ck(cudaStreamSynchronize(s_), "staging");
+    stage_.reset(new DevBuf(n * sizeof(double), own_));
+    ownSync();
+  }
   return (double*)stage_->p;
 }
 
@@ -849,8 +869,7 @@ void Solver::fill(const LevelDev& L, T* f, bool withCF, int par) {
 
 // AMRMultiGrid::computeAMRResidualLevel (AMRMultiGrid.H:836-892).
 template <class T>
-void Solver::amrResidualLevel(int ilev, int lmax, std::vector<T*>& res, std::vector<T*>& phi,
-                              std::vector<T*>& rhs) {
+void Solver::amrResidualLevel(int ilev, int lmax, T* const* res, T* const* phi, T* const* rhs) {
   const LevelDev& L = amrDev_[ilev];
   Coef<T> c = coefA<T>(ilev);
   const double w = sizeof(T);
@@ -889,7 +908,7 @@ void Solver::launchAMRResidual(std::vector<double*>& res, std::vector<double*>& 
                                int lmax) {
   ck(cudaMemsetAsync(dNorm_, 0, sizeof(double), s_), "norm reset");
   for (int ilev = 0; ilev <= lmax; ++ilev) {
-    amrResidualLevel(ilev, lmax, res, phi, rhs);
+    amrResidualLevel<double>(ilev, lmax, res.data(), phi.data(), rhs.data());
     if (ilev != lmax) zeroCovered(amrDev_[ilev], res[ilev], s_);
     maxNorm(amrDev_[ilev], res[ilev], dNorm_, s_);
   }
@@ -981,7 +1000,7 @@ void Solver::amrVCycle(int ilev, int lmax) {
     ucorr[l] = lev[l].ucorr;
     ures[l] = lev[l].ures;
   }
-  amrResidualLevel(ilev - 1, lmax, res, ucorr, ures);
+  amrResidualLevel<T>(ilev - 1, lmax, res.data(), ucorr.data(), ures.data());
   // AMRRestrictS: residual of the correction into the scratch (uberCorrection),
   // averaged straight onto the coarse residual (assignCopier).
   quadCF(L, f.corr, fc.corr, s_);
@@ -1002,6 +1021,11 @@ void Solver::amrVCycle(int ilev, int lmax) {
 
 template void Solver::amrVCycle<double>(int, int);
 template void Solver::amrVCycle<float>(int, int);
+// Used by the operator-level calls (levelops.cu) and the allocation-free
+// residual norm (noalloc.cu).
+template void Solver::amrResidualLevel<double>(int, int, double* const*, double* const*, double* const*);
+template void Solver::relaxAMR<double>(int, double*, const double*, int);
+template void Solver::relaxMG<double>(int, double*, const double*, int);
 
 // ------------------------------------------------ BiCGStab over MultilevelLinearOp
 // BiCGStabSolver<Vector<LevelData<FArrayBox>*>>::solve (BiCGStabSolver.H:199-515)
@@ -1043,7 +1067,7 @@ void Solver::mlScale(MLVec& x, double scale) {
 // conditions coincide for these zero-value Dirichlet faces.
 void Solver::mlResidual(MLVec& lhs, MLVec& phi, MLVec& rhs) {
   const int lmax = numLevels() - 1;
-  for (int l = 0; l <= lmax; ++l) amrResidualLevel<double>(l, lmax, lhs, phi, rhs);
+  for (int l = 0; l <= lmax; ++l) amrResidualLevel<double>(l, lmax, lhs.data(), phi.data(), rhs.data());
 }
 
 // AMROperator / AMROperatorNC / AMROperatorNF / applyOp of one level
@@ -1194,7 +1218,8 @@ void Solver::interpToFine(int l, bool pwc) {
   if (fineInterp_.size() < amr_.size()) fineInterp_.resize(amr_.size());
   if (!fineInterp_[l])
     fineInterp_[l].reset(
-        new FineInterpOp(amr_[l - 1].grids.boxes, amr_[l - 1].index, amr_[l - 1].domain, amr_[l].grids.boxes, s_));
+        new FineInterpOp(amr_[l - 1].grids.boxes, amr_[l - 1].index, amr_[l - 1].domain, amr_[l].grids.boxes, own_));
+  fineInterp_[l]->setStream(s_);
   // algorithmic bytes: every fine cell written once, every coarse parent read once
   const double bytes = 9.0 * sizeof(double) / 8.0 * (double)fineInterp_[l]->fineCells();
   timed(P_FINEINTERP, bytes,
@@ -1405,8 +1430,13 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
   bool goRedu = rnorm > p.eps * r0;
   bool goIter = iter < p.iterMax;
   bool goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
+  bool goMin = iter < p.iterMin;
+  // A NaN or infinite norm ends the solve (the reference's loop stops at a
+  // NaN too, since every comparison with it is false); the stopping flags
+  // and exit status are computed as for any other norm.
+  bool finite = std::isfinite(rnorm);
   const bool graph = useGraphs_ && !profOn_;
-  while (goIter && goRedu && goHang && goNorm) {
+  while (finite && (goMin || (goIter && goRedu && goHang && goNorm))) {
     normLast = rnorm;
     if (graph) {
       cudaGraphExec_t exec = iterationGraph(mixed, ures, phi, rhs);
@@ -1422,9 +1452,12 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
     goRedu = rnorm > p.eps * r0;
     goIter = iter < p.iterMax;
     goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
+    goMin = iter < p.iterMin;
+    finite = std::isfinite(rnorm);
   }
   out.exitStatus = int(!goRedu) + int(!goIter) * 2 + int(!goHang) * 4 + int(!goNorm) * 8;
   out.iterations = iter;
+  out.diverged = !finite;
   return out;
 }
 
@@ -1466,7 +1499,8 @@ cudaGraphExec_t Solver::iterationGraph(bool mixed, std::vector<double*>& ures, s
 void Solver::setUseGraphs(bool on) { useGraphs_ = on; }
 
 float* Solver::allocF(size_t n) {
-  bufs_.emplace_back(new DevBuf(n * sizeof(float), s_));
+  bufs_.emplace_back(new DevBuf(n * sizeof(float), own_));
+  ownSync();
   float* p = (float*)bufs_.back()->p;
   ck(cudaMemsetAsync(p, 0, n * sizeof(float), s_), "memset");
   return p;

@@ -25,7 +25,11 @@ enum {
   CMG_EINVAL = 1,    /* bad argument (level, direction, sizes, null pointer) */
   CMG_ENOMEM = 2,    /* device allocation failed */
   CMG_ECUDA = 3,     /* CUDA runtime error */
-  CMG_EINTERNAL = 4  /* anything else; see cmg_last_error() */
+  CMG_EINTERNAL = 4, /* anything else; see cmg_last_error() */
+  CMG_EDIVERGED = 5, /* a residual norm became NaN or infinite: the solve stopped there; its outputs
+                        (phi, exit status, history up to that norm) are written */
+  CMG_ETIMEOUT = 6,  /* a request's time limit passed before it finished (cmg_serve) */
+  CMG_ECANCELLED = 7 /* a request was cancelled (cmg_serve) */
 };
 
 typedef struct cmg_box {
@@ -36,10 +40,13 @@ typedef struct cmg_box {
 typedef struct cmg_hierarchy cmg_hierarchy;
 
 /* Solver parameters: AMRMultiGrid::setSolverParameters
- * (AMRElliptic/AMRMultiGrid.H:527-553) plus m_imin (AMRMultiGrid.H:599-622). */
+ * (AMRElliptic/AMRMultiGrid.H:527-553) plus m_imin and m_iterMin
+ * (AMRMultiGrid.H:599-622, 1003-1008).  The reference's defaults are
+ * {2, 2, 2, 1, 20, 5, 1e-6, 1e-15, 1e-30, -1}. */
 typedef struct cmg_solve_params {
   int pre, post, bottom, num_mg, iter_max, imin;
   double eps, hang, norm_thresh;
+  int iter_min; /* iterate while iteration < iter_min whatever the norms (-1: no minimum) */
 } cmg_solve_params;
 
 /* Message of the last failed call on this thread. */
@@ -86,7 +93,11 @@ int cmg_set_phi(cmg_hierarchy* h, int level, const double* data, int on_device);
 
 /* AMRMultiGrid::solve(phi, rhs, lmax, 0, zeroPhi) (AMRMultiGrid.H:894-1124).
  * history receives the composite max-norm residual at the start of every
- * iteration followed by the final one (up to history_cap values). */
+ * iteration followed by the final one (up to history_cap values).  A norm
+ * that is NaN or infinite (a NaN in the right-hand side, or a diverging
+ * iteration) ends the solve there and the call returns CMG_EDIVERGED with
+ * every output written; exit_status is the reference's bitmask for that
+ * norm (AMRMultiGrid.H:1099). */
 int cmg_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int* exit_status, int* iterations,
               double* history, int history_cap, int* history_len);
 
@@ -193,6 +204,14 @@ int cmg_fine_interp_create(const int fine_domain_lo[3], const int fine_domain_hi
 int cmg_fine_interp_run(cmg_fine_interp* fi, const double* coarse, double* fine, int on_device,
                         int piecewise_constant);
 int cmg_fine_interp_destroy(cmg_fine_interp* fi);
+/* Runs later cmg_fine_interp_run calls on `stream` (a cudaStream_t; NULL: the
+ * object's own stream), as cmg_set_stream does for a hierarchy.  With
+ * on_device != 0 the run reads `coarse` in stream order, so a caller that
+ * produced it on another stream must make this stream wait for it first. */
+int cmg_fine_interp_set_stream(cmg_fine_interp* fi, void* stream);
+/* 1 when the fused one-kernel path runs (every fine box's coarse staging
+ * block fits in shared memory), 0 for the gather + interpolate path. */
+int cmg_fine_interp_is_fused(const cmg_fine_interp* fi, int* out);
 
 /* Same value as cmg_residual_norm, allocating no memory on success (no
  * counterpart in the reference, which has no such constraint).  For callers
@@ -303,6 +322,119 @@ int cmg_vcycle_bytes(const cmg_hierarchy* h, const cmg_solve_params* p, double* 
 
 /* The CUDA stream every call of this hierarchy runs on (cudaStream_t). */
 int cmg_get_stream(const cmg_hierarchy* h, void** stream);
+/* Streams (no counterpart in the reference, whose calls are synchronous host
+ * code).  After cmg_set_stream every later call of this hierarchy issues its
+ * device work on `stream` (a cudaStream_t of the current device; NULL goes
+ * back to the hierarchy's own stream), in order with what the caller queued
+ * on that stream before the call: device-pointer inputs produced on that
+ * stream need no synchronisation.  Work already queued on the previous
+ * stream is finished first.  Device memory stays on the hierarchy's own
+ * stream, so the caller's stream may be destroyed after the hierarchy's last
+ * call that used it has returned.  Calls that return results to the host
+ * (norms, histories, host arrays) still synchronise the stream before they
+ * return. */
+int cmg_set_stream(cmg_hierarchy* h, void* stream);
+
+/* Operator-level calls: one virtual of the reference's operator interfaces
+ * (AMRLevelOp, AMRElliptic/AMRMultiGrid.H:39-225; MGLevelOp, MultiGrid.H:
+ * 116-160; LinearOp, LinearSolver.H:41-137), as AMRPoissonOp and
+ * VCAMRPoissonOp2 implement them, on one level of a hierarchy: what a
+ * Chombo program's own AMRMultiGrid / MultiGrid / BiCGStabSolver calls when
+ * it drives the GPU operators through include/cmg_chombo.H
+ * (GpuAMRPoissonOpFactory as an AMRLevelOpFactory).  Same kernels and
+ * operation order as cmg_solve.
+ *
+ * lev >= 0 names AMR level lev; lev < 0 names multigrid depth -lev below
+ * level 0 (AMRPoissonOpFactory::MGnewOp, AMRPoissonOp.cpp:1923-1989), for
+ * 1 <= -lev <= cmg_op_num_mg_depths.  Arrays are host memory in the ghosted
+ * format: every box's FAB grown by one cell, x fastest, boxes in layout
+ * order (the memory of a one-component LevelData<FArrayBox> with one ghost
+ * layer, box after box); cmg_op_size gives its length.  Inputs are read whole,
+ * ghost cells included (a ghost the operator does not refill is read as the
+ * caller left it, as in the reference).  Outputs receive their valid cells;
+ * their ghost positions are unspecified.  Boundary conditions are the
+ * hierarchy's homogeneous Dirichlet, so `homogeneous` changes nothing for
+ * them; on levels >= 1 it selects whether residual sets the homogeneous
+ * coarse-fine ghosts first (AMRPoissonOp::residual, AMRPoissonOp.cpp:227-238).
+ * Every call copies its arguments to the device and back and synchronises. */
+int cmg_op_num_mg_depths(const cmg_hierarchy* h, int* out);
+int cmg_op_num_boxes(const cmg_hierarchy* h, int lev, int* out);
+int cmg_op_get_boxes(const cmg_hierarchy* h, int lev, cmg_box* out, int cap);
+int cmg_op_size(const cmg_hierarchy* h, int lev, int64_t* out);
+/* Length of a ghosted array over coarsen(level's boxes, 2) (level >= 1): the
+ * layout of AMRMultiGrid's m_resC (createCoarsened, AMRPoissonOp.cpp:459-471). */
+int cmg_op_coarsened_size(const cmg_hierarchy* h, int level, int64_t* out);
+/* LinearOp::residual: lhs = rhs - L(phi) (OPERATORLAPRES / VCCOMPUTERES3D
+ * after exchange and boundary values; AMRPoissonOp.cpp:227-297). */
+int cmg_op_residual(cmg_hierarchy* h, int lev, double* lhs, const double* phi, const double* rhs, int homogeneous);
+/* LinearOp::applyOp: lhs = L(phi) with homogeneous coarse-fine ghosts
+ * (AMRPoissonOp.cpp:332-385). */
+int cmg_op_apply(cmg_hierarchy* h, int lev, double* lhs, const double* phi, int homogeneous);
+/* MGLevelOp::relax: iterations red-black Gauss-Seidel sweeps (levelGSRB,
+ * AMRPoissonOp.cpp:600-632, 1216-1281; VCAMRPoissonOp2.cpp:547-626). */
+int cmg_op_relax(cmg_hierarchy* h, int lev, double* phi, const double* rhs, int iterations);
+/* LinearOp::preCond: cor = res / diagonal, then two sweeps
+ * (AMRPoissonOp.cpp:304-329, VCAMRPoissonOp2.cpp:93-127). */
+int cmg_op_precond(cmg_hierarchy* h, int lev, double* cor, const double* res);
+/* MGLevelOp::restrictResidual: res_coarse (level lev - 1, i.e. the next
+ * multigrid depth) = average of rhs - L(phi) (RESTRICTRES(VC3D),
+ * AMRPoissonOp.cpp:651-703).  lev <= 0. */
+int cmg_op_restrict_residual(cmg_hierarchy* h, int lev, double* res_coarse, const double* phi, const double* rhs);
+/* MGLevelOp::prolongIncrement: phi += corr_coarse at the parent cell (PROLONG,
+ * AMRPoissonOp.cpp:706-733).  lev <= 0; corr_coarse on level lev - 1. */
+int cmg_op_prolong_increment(cmg_hierarchy* h, int lev, double* phi, const double* corr_coarse);
+/* The AMROperator / AMRResidual family (AMRPoissonOp.cpp:736-858) on AMR
+ * level `level`: inhomogeneous quadratic coarse-fine ghosts from phi_coarse
+ * (level - 1) when it is not NULL, exchange and boundary values, then
+ *   form 0: out = L(phi), with the flux-register correction from phi_fine
+ *           (level + 1) when it is not NULL (AMROperator, AMROperatorNC/NF);
+ *   form 1: the same followed by out = rhs - out as axby(out, out, rhs, -1, 1)
+ *           (AMRResidual, AMRResidualNC);
+ *   form 2: out = rhs - L(phi) in residualI's own expression, phi_fine NULL
+ *           (AMRResidualNF). */
+int cmg_op_amr_operator(cmg_hierarchy* h, int level, int form, double* out, const double* phi_fine,
+                        const double* phi, const double* phi_coarse, const double* rhs);
+/* AMRLevelOp::AMRRestrictS (AMRPoissonOp.cpp:877-919), level >= 1: the
+ * residual of `correction` against `residual` with coarse-fine ghosts from
+ * coarse_correction (level - 1), averaged onto the coarsened-fine layout
+ * (res_coarsened, cmg_op_coarsened_size doubles).  correction == NULL is
+ * a_skip_res: `residual` itself is averaged (the FAS restriction). */
+int cmg_op_amr_restrict(cmg_hierarchy* h, int level, double* res_coarsened, const double* residual,
+                        const double* correction, const double* coarse_correction);
+/* assignCopier(coarse, coarsened, m_resCopier) of AMRMultiGrid::AMRVCycle
+ * (AMRMultiGrid.H:1391): the valid cells of level - 1 under level take the
+ * coarsened-fine values; coarse (level - 1) is read and written. */
+int cmg_op_assign_coarsened(cmg_hierarchy* h, int level, double* coarse, const double* coarsened);
+/* AMRLevelOp::AMRProlongS / AMRProlong (AMRPoissonOp.cpp:926-990), level >= 1:
+ * correction += coarse_correction (level - 1) at the parent cell. */
+int cmg_op_amr_prolong(cmg_hierarchy* h, int level, double* correction, const double* coarse_correction);
+/* AMRLevelOp::AMRUpdateResidual (AMRPoissonOp.cpp:1045-1054), level >= 1:
+ * residual -= L(correction) with coarse-fine ghosts from coarse_correction. */
+int cmg_op_amr_update_residual(cmg_hierarchy* h, int level, double* residual, const double* correction,
+                               const double* coarse_correction);
+/* QuadCFInterp::coarseFineInterp (AMRTools/QuadCFInterp.cpp:845-889), level
+ * >= 1: the coarse-fine face ghosts of phi from phi_coarse (level - 1), by the
+ * tangential Taylor expansion of the coarse data (PHISTAR, QuadCFStencil) and
+ * the quadratic through it and two fine cells (QUADINTERP / interpOnIVS).
+ * phi is read whole and returned whole: valid cells unchanged, coarse-fine
+ * ghosts set, every other ghost as it was. */
+int cmg_op_cf_interp(cmg_hierarchy* h, int level, double* phi, const double* phi_coarse);
+/* AMRLevelOp::zeroCovered (AMRMultiGrid.H:197-201): zero the valid cells of
+ * `level` covered by level + 1. */
+int cmg_op_zero_covered(cmg_hierarchy* h, int level, double* data);
+/* LevelDataOps (AMRElliptic/LevelDataOps.H:179-281): lhs = a x + b y
+ * (x*a then + y*b), lhs += scale x, lhs *= scale. */
+int cmg_op_axby(cmg_hierarchy* h, int lev, double* lhs, const double* x, const double* y, double a, double b);
+int cmg_op_incr(cmg_hierarchy* h, int lev, double* lhs, const double* x, double scale);
+int cmg_op_scale(cmg_hierarchy* h, int lev, double* lhs, double scale);
+/* LevelDataOps::dotProduct (LevelDataOps.H:109-131): per box in k, j, i
+ * order, boxes summed in layout order. */
+int cmg_op_dot(cmg_hierarchy* h, int lev, const double* x, const double* y, double* out);
+/* norm(LevelData, ord) as AMRPoissonOp::norm computes it (BoxTools/
+ * BoxLayoutData.cpp:23-93, FArrayBox::norm/sumPow): ord 0 the max norm (a NaN
+ * anywhere gives NaN), 1 the sum of |x|, 2 the 2-norm, each box in pencil
+ * order. */
+int cmg_op_norm(cmg_hierarchy* h, int lev, const double* x, int ord, double* out);
 
 /* Kernel-class device timing, the counterpart of the reference's CH_TIMER
  * trace timers (BaseTools/CH_Timer.H:44-163): while enabled, every launch of a

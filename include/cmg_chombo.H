@@ -19,12 +19,23 @@
 //   - refinement ratio 2 between all levels, non-periodic domain, serial
 //     (every box local), one component;
 //   - homogeneous Dirichlet boundary conditions on the domain faces (the
-//     examples' ParseBC with value 0, order 1): the BCHolder argument is kept
-//     for signature compatibility and is not called;
+//     examples' ParseBC with value 0, order 1).  The factories' define()
+//     probes the BCHolder: on a two-cell slab along each of the six domain
+//     faces it calls the BC (inhomogeneous) and requires every face ghost to
+//     be minus the cell inside it; any other condition (Neumann, a non-zero
+//     Dirichlet value, a higher-order stencil) is rejected there;
 //   - the bottom solver must be a BiCGStabSolver (its device restatement runs
 //     with the reference's default parameters);
 //   - solve over all levels: l_base = 0 and l_max = numLevels - 1.
 // Only valid cells of phi are written; ghost cells are left as they were.
+//
+// The factories are also AMRLevelOpFactory<LevelData<FArrayBox>>s: the
+// reference's own, unmodified AMRMultiGrid (or MultiGrid, BiCGStabSolver or
+// any other caller of the operator interface) can be defined with them and
+// drives GpuAMRPoissonOp objects one virtual at a time.  Each call moves its
+// LevelData arguments to the device and back (the cmg_op_* entry points),
+// which is correct but slow; GpuAMRMultiGrid, whose hierarchy stays on the
+// device for the whole solve, is the fast path.
 //
 // The variable-coefficient example's solve path has its drop-in too:
 // MultilevelLinearOp<FArrayBox> + BiCGStabSolver<Vector<LevelData<FArrayBox>*>>
@@ -33,8 +44,12 @@
 #ifndef CMG_CHOMBO_H
 #define CMG_CHOMBO_H
 
+#include <algorithm>
+#include <cstring>
+#include <memory>
 #include <vector>
 
+#include "AMRMultiGrid.H"
 #include "BCFunc.H"
 #include "BiCGStabSolver.H"
 #include "DisjointBoxLayout.H"
@@ -64,53 +79,368 @@ struct GpuOpDescription {
   bool defined = false;
 };
 
-// AMRPoissonOpFactory::define (AMRElliptic/AMRPoissonOp.H:535-541).
-class GpuAMRPoissonOpFactory {
+// Rejects every boundary condition but the homogeneous Dirichlet one the
+// device solve applies (ghost = 2*0 - inside, BCFunc.cpp:294-354 with value
+// 0, order 1): on a slab two cells deep along each domain face the BC is
+// called inhomogeneous on distinct cell values, and every ghost across that
+// face must be minus the cell next to it.
+inline void requireHomogeneousDirichlet(BCHolder a_bc, const ProblemDomain& a_domain, Real a_dx) {
+  const Box& d = a_domain.domainBox();
+  for (int dir = 0; dir < SpaceDim; ++dir)
+    for (SideIterator sit; sit.ok(); ++sit) {
+      Box valid = d;
+      const int w = std::min(2, d.size(dir));
+      if (sit() == Side::Lo)
+        valid.setBig(dir, d.smallEnd(dir) + w - 1);
+      else
+        valid.setSmall(dir, d.bigEnd(dir) - w + 1);
+      FArrayBox fab(grow(valid, 1), 1);
+      fab.setVal(1.0e30);
+      for (BoxIterator bit(valid); bit.ok(); ++bit) {
+        const IntVect& iv = bit();
+        fab(iv, 0) = 1.0 + 0.25 * iv[0] + 7.0 * iv[1] + 53.0 * iv[2];
+      }
+      a_bc(fab, valid, a_domain, a_dx, false);
+      const Box ghost = adjCellBox(valid, dir, sit(), 1);
+      const IntVect in = (sit() == Side::Lo ? 1 : -1) * BASISV(dir);
+      for (BoxIterator bit(ghost); bit.ok(); ++bit)
+        if (fab(bit(), 0) != -fab(bit() + in, 0))
+          MayDay::Error("cmg_chombo: the device operators support homogeneous Dirichlet boundary conditions only "
+                        "(ghost = -inside on every domain face); this BCHolder sets something else");
+    }
+}
+
+inline bool sameBoxes(const DisjointBoxLayout& a, const DisjointBoxLayout& b) {
+  if (a.size() != b.size()) return false;
+  LayoutIterator ia = a.layoutIterator(), ib = b.layoutIterator();
+  for (; ia.ok() && ib.ok(); ++ia, ++ib)
+    if (a[ia()] != b[ib()]) return false;
+  return true;
+}
+
+class GpuHierarchy;
+
+// AMRPoissonOp / VCAMRPoissonOp2 (AMRElliptic/AMRPoissonOp.H:35-510,
+// VCAMRPoissonOp2.H:25-249) as an AMRLevelOp over the device hierarchy of
+// its factory: one AMR level (lev >= 0) or one multigrid depth below level 0
+// (lev = -depth).  Every operator method sends its LevelData arguments (in
+// the ghosted format of cmg.h: each FAB grown by one cell) to the matching
+// cmg_op_* call and writes the valid cells of its outputs back; ghost cells
+// of the caller's data are left as they were.  Container methods (create,
+// createCoarser, createCoarsened, assign, assignLocal, setToZero,
+// buildCopier) are the reference's LevelData operations.
+class GpuAMRPoissonOp : public AMRLevelOp<LDF> {
  public:
-  void define(const ProblemDomain& a_coarseDomain, const Vector<DisjointBoxLayout>& a_grids,
-              const Vector<int>& a_refRatios, const Real& a_coarsedx, BCHolder /*a_bc*/, Real a_alpha = 0.0,
-              Real a_beta = 1.0) {
-    m_d = GpuOpDescription();
-    m_d.coarseDomain = a_coarseDomain;
-    m_d.grids = a_grids;
-    m_d.refRatios = a_refRatios;
-    m_d.coarsedx = a_coarsedx;
-    m_d.alpha = a_alpha;
-    m_d.beta = a_beta;
-    m_d.vc = 0;
-    m_d.defined = true;
+  GpuAMRPoissonOp(std::shared_ptr<GpuHierarchy> a_h, int a_lev, const DisjointBoxLayout& a_grids, Real a_dx,
+                  const DisjointBoxLayout* a_finerCoarsened)
+      : m_sh(a_h), m_lev(a_lev), m_grids(a_grids), m_dx(a_dx) {
+    if (a_finerCoarsened) {
+      m_finerCoarsened = *a_finerCoarsened;
+      m_hasFiner = true;
+    }
   }
-  const GpuOpDescription& description() const { return m_d; }
+  virtual ~GpuAMRPoissonOp() {}
+
+  int level() const { return m_lev; }
+
+  // ---------------------------------------------------------------- LinearOp
+  virtual void residual(LDF& a_lhs, const LDF& a_phi, const LDF& a_rhs, bool a_homogeneous = false) {
+    in(a_phi, m_a);
+    in(a_rhs, m_b);
+    out0(m_o);
+    check(cmg_op_residual(h(), m_lev, m_o.data(), m_a.data(), m_b.data(), a_homogeneous ? 1 : 0));
+    outValid(m_o, a_lhs);
+  }
+  virtual void preCond(LDF& a_cor, const LDF& a_residual) {
+    in(a_cor, m_a);
+    in(a_residual, m_b);
+    check(cmg_op_precond(h(), m_lev, m_a.data(), m_b.data()));
+    outValid(m_a, a_cor);
+  }
+  virtual void applyOp(LDF& a_lhs, const LDF& a_phi, bool a_homogeneous = false) {
+    in(a_phi, m_a);
+    out0(m_o);
+    check(cmg_op_apply(h(), m_lev, m_o.data(), m_a.data(), a_homogeneous ? 1 : 0));
+    outValid(m_o, a_lhs);
+  }
+  // LevelDataOps::create / assign / assignLocal / setToZero (LevelDataOps.H).
+  virtual void create(LDF& a_lhs, const LDF& a_rhs) {
+    a_lhs.define(a_rhs.disjointBoxLayout(), a_rhs.nComp(), a_rhs.ghostVect());
+  }
+  virtual void assign(LDF& a_lhs, const LDF& a_rhs) { a_rhs.copyTo(a_rhs.interval(), a_lhs, a_lhs.interval()); }
+  virtual void assignLocal(LDF& a_lhs, const LDF& a_rhs) {
+    for (DataIterator dit = a_lhs.dataIterator(); dit.ok(); ++dit) a_lhs[dit].copy(a_rhs[dit]);
+  }
+  virtual Real dotProduct(const LDF& a_1, const LDF& a_2) {
+    in(a_1, m_a);
+    in(a_2, m_b);
+    double r = 0;
+    check(cmg_op_dot(h(), m_lev, m_a.data(), m_b.data(), &r));
+    return r;
+  }
+  virtual void incr(LDF& a_lhs, const LDF& a_x, Real a_scale) {
+    in(a_lhs, m_o);
+    in(a_x, m_a);
+    check(cmg_op_incr(h(), m_lev, m_o.data(), m_a.data(), a_scale));
+    outValid(m_o, a_lhs);
+  }
+  virtual void axby(LDF& a_lhs, const LDF& a_x, const LDF& a_y, Real a_a, Real a_b) {
+    in(a_x, m_a);
+    in(a_y, m_b);
+    out0(m_o);
+    check(cmg_op_axby(h(), m_lev, m_o.data(), m_a.data(), m_b.data(), a_a, a_b));
+    outValid(m_o, a_lhs);
+  }
+  virtual void scale(LDF& a_lhs, const Real& a_scale) {
+    in(a_lhs, m_o);
+    check(cmg_op_scale(h(), m_lev, m_o.data(), a_scale));
+    outValid(m_o, a_lhs);
+  }
+  virtual Real norm(const LDF& a_x, int a_ord) {
+    in(a_x, m_a);
+    double r = 0;
+    check(cmg_op_norm(h(), m_lev, m_a.data(), a_ord, &r));
+    return r;
+  }
+  virtual void setToZero(LDF& a_lhs) {
+    for (DataIterator dit = a_lhs.dataIterator(); dit.ok(); ++dit) a_lhs[dit].setVal(0.0);
+  }
+  virtual Real dx() const { return m_dx; }
+
+  // ---------------------------------------------------------------- MGLevelOp
+  virtual void createCoarser(LDF& a_coarse, const LDF& a_fine, bool /*a_ghosted*/) {
+    DisjointBoxLayout dbl;
+    coarsen(dbl, a_fine.disjointBoxLayout(), 2);
+    a_coarse.define(dbl, a_fine.nComp(), a_fine.ghostVect());
+  }
+  virtual void relax(LDF& a_correction, const LDF& a_residual, int a_iterations) {
+    in(a_correction, m_a);
+    in(a_residual, m_b);
+    check(cmg_op_relax(h(), m_lev, m_a.data(), m_b.data(), a_iterations));
+    outValid(m_a, a_correction);
+  }
+  virtual void restrictResidual(LDF& a_resCoarse, LDF& a_phiFine, const LDF& a_rhsFine) {
+    in(a_phiFine, m_a);
+    in(a_rhsFine, m_b);
+    packGhosted(a_resCoarse, m_o);
+    check(cmg_op_restrict_residual(h(), m_lev, m_o.data(), m_a.data(), m_b.data()));
+    unpackValid(m_o, a_resCoarse);
+  }
+  virtual void prolongIncrement(LDF& a_phiThisLevel, const LDF& a_correctCoarse) {
+    in(a_phiThisLevel, m_a);
+    packGhosted(a_correctCoarse, m_b);
+    check(cmg_op_prolong_increment(h(), m_lev, m_a.data(), m_b.data()));
+    outValid(m_a, a_phiThisLevel);
+  }
+
+  // ---------------------------------------------------------------- AMRLevelOp
+  virtual int refToCoarser() { return 2; }
+  virtual void AMRResidual(LDF& a_residual, const LDF& a_phiFine, const LDF& a_phi, const LDF& a_phiCoarse,
+                           const LDF& a_rhs, bool, AMRLevelOp<LDF>*) {
+    amrOp(1, a_residual, &a_phiFine, a_phi, &a_phiCoarse, &a_rhs);
+  }
+  virtual void AMRResidualNF(LDF& a_residual, const LDF& a_phi, const LDF& a_phiCoarse, const LDF& a_rhs, bool) {
+    amrOp(2, a_residual, nullptr, a_phi, &a_phiCoarse, &a_rhs);
+  }
+  virtual void AMRResidualNC(LDF& a_residual, const LDF& a_phiFine, const LDF& a_phi, const LDF& a_rhs, bool,
+                             AMRLevelOp<LDF>*) {
+    amrOp(1, a_residual, &a_phiFine, a_phi, nullptr, &a_rhs);
+  }
+  virtual void AMROperator(LDF& a_LofPhi, const LDF& a_phiFine, const LDF& a_phi, const LDF& a_phiCoarse, bool,
+                           AMRLevelOp<LDF>*) {
+    amrOp(0, a_LofPhi, &a_phiFine, a_phi, &a_phiCoarse, nullptr);
+  }
+  virtual void AMROperatorNF(LDF& a_LofPhi, const LDF& a_phi, const LDF& a_phiCoarse, bool) {
+    amrOp(0, a_LofPhi, nullptr, a_phi, &a_phiCoarse, nullptr);
+  }
+  virtual void AMROperatorNC(LDF& a_LofPhi, const LDF& a_phiFine, const LDF& a_phi, bool, AMRLevelOp<LDF>*) {
+    amrOp(0, a_LofPhi, &a_phiFine, a_phi, nullptr, nullptr);
+  }
+  virtual void AMRRestrict(LDF& a_resCoarse, const LDF& a_residual, const LDF& a_correction,
+                           const LDF& a_coarseCorrection, bool a_skip_res) {
+    LDF scratch;
+    AMRRestrictS(a_resCoarse, a_residual, a_correction, a_coarseCorrection, scratch, a_skip_res);
+  }
+  virtual void AMRRestrictS(LDF& a_resCoarse, const LDF& a_residual, const LDF& a_correction,
+                            const LDF& a_coarseCorrection, LDF& /*scratch*/, bool a_skip_res = false) {
+    in(a_residual, m_a);
+    if (!a_skip_res) {
+      in(a_correction, m_b);
+      packGhosted(a_coarseCorrection, m_c);
+    }
+    int64_t n = 0;
+    check(cmg_op_coarsened_size(h(), m_lev, &n));
+    m_o.resize(n);
+    check(cmg_op_amr_restrict(h(), m_lev, m_o.data(), m_a.data(), a_skip_res ? nullptr : m_b.data(),
+                              a_skip_res ? nullptr : m_c.data()));
+    unpackValid(m_o, a_resCoarse);
+  }
+  virtual void AMRProlong(LDF& a_correction, const LDF& a_coarseCorrection) {
+    in(a_correction, m_a);
+    packGhosted(a_coarseCorrection, m_b);
+    check(cmg_op_amr_prolong(h(), m_lev, m_a.data(), m_b.data()));
+    outValid(m_a, a_correction);
+  }
+  virtual void AMRProlongS(LDF& a_correction, const LDF& a_coarseCorrection, LDF& /*a_temp*/,
+                           const Copier& /*a_copier*/) {
+    AMRProlong(a_correction, a_coarseCorrection);
+  }
+  virtual void AMRUpdateResidual(LDF& a_residual, const LDF& a_correction, const LDF& a_coarseCorrection) {
+    in(a_residual, m_o);
+    in(a_correction, m_a);
+    packGhosted(a_coarseCorrection, m_b);
+    check(cmg_op_amr_update_residual(h(), m_lev, m_o.data(), m_a.data(), m_b.data()));
+    outValid(m_o, a_residual);
+  }
+  virtual void createCoarsened(LDF& a_lhs, const LDF& a_rhs, const int& a_refRat) {
+    DisjointBoxLayout dbl;
+    coarsen(dbl, a_rhs.disjointBoxLayout(), a_refRat);
+    a_lhs.define(dbl, a_rhs.nComp(), a_rhs.ghostVect());
+  }
+  // AMRPoissonOp::buildCopier (AMRPoissonOp.cpp:474-483).
+  virtual void buildCopier(Copier& a_copier, const LDF& a_lhs, const LDF& a_rhs) {
+    a_copier.define(a_rhs.disjointBoxLayout(), a_lhs.disjointBoxLayout(), a_lhs.ghostVect());
+  }
+  // The coarsened-fine residual of the next finer level onto this level
+  // (AMRMultiGrid::AMRVCycle) runs on the device; any other copy is the
+  // reference's copyTo with the given copier.
+  virtual void assignCopier(LDF& a_lhs, const LDF& a_rhs, const Copier& a_copier) {
+    if (m_hasFiner && sameBoxes(a_lhs.disjointBoxLayout(), m_grids) &&
+        sameBoxes(a_rhs.disjointBoxLayout(), m_finerCoarsened)) {
+      in(a_lhs, m_o);
+      packGhosted(a_rhs, m_a);
+      check(cmg_op_assign_coarsened(h(), m_lev + 1, m_o.data(), m_a.data()));
+      outValid(m_o, a_lhs);
+    } else {
+      a_rhs.copyTo(a_rhs.interval(), a_lhs, a_lhs.interval(), a_copier);
+    }
+  }
+  virtual void zeroCovered(LDF& a_lhs, LDF& a_rhs, const Copier& a_copier) {
+    setToZero(a_rhs);
+    if (m_hasFiner && sameBoxes(a_lhs.disjointBoxLayout(), m_grids) &&
+        sameBoxes(a_rhs.disjointBoxLayout(), m_finerCoarsened)) {
+      in(a_lhs, m_o);
+      check(cmg_op_zero_covered(h(), m_lev, m_o.data()));
+      outValid(m_o, a_lhs);
+    } else {
+      a_rhs.copyTo(a_rhs.interval(), a_lhs, a_lhs.interval(), a_copier);
+    }
+  }
+  virtual Real localMaxNorm(const LDF& a_phi) { return norm(a_phi, 0); }
+
+  // QuadCFInterp::coarseFineInterp of this level (AMRPoissonOp's
+  // m_interpWithCoarser): the coarse-fine ghosts of a_phi from a_phiCoarse.
+  void coarseFineInterp(LDF& a_phi, const LDF& a_phiCoarse) {
+    if (m_lev < 1) MayDay::Error("cmg_chombo: coarseFineInterp on a level without a coarser level");
+    in(a_phi, m_a);
+    packGhosted(a_phiCoarse, m_b);
+    check(cmg_op_cf_interp(h(), m_lev, m_a.data(), m_b.data()));
+    unpackGrown(m_a, a_phi);
+  }
 
  private:
-  GpuOpDescription m_d;
-};
+  std::shared_ptr<GpuHierarchy> m_sh;
+  int m_lev;
+  DisjointBoxLayout m_grids, m_finerCoarsened;
+  bool m_hasFiner = false;
+  Real m_dx;
+  std::vector<double> m_a, m_b, m_c, m_o;
 
-// VCAMRPoissonOp2Factory::define (AMRElliptic/VCAMRPoissonOp2.H:278-286).
-// The coefficients are read when GpuAMRMultiGrid::define runs (the reference
-// computes its relaxation coefficient from them at the same point).
-class GpuVCAMRPoissonOp2Factory {
- public:
-  void define(const ProblemDomain& a_coarseDomain, const Vector<DisjointBoxLayout>& a_grids,
-              const Vector<int>& a_refRatios, const Real& a_coarsedx, BCHolder /*a_bc*/, const Real& a_alpha,
-              Vector<RefCountedPtr<LDF> >& a_aCoef, const Real& a_beta,
-              Vector<RefCountedPtr<LevelData<FluxBox> > >& a_bCoef) {
-    m_d = GpuOpDescription();
-    m_d.coarseDomain = a_coarseDomain;
-    m_d.grids = a_grids;
-    m_d.refRatios = a_refRatios;
-    m_d.coarsedx = a_coarsedx;
-    m_d.alpha = a_alpha;
-    m_d.beta = a_beta;
-    m_d.vc = 1;
-    m_d.aCoef = a_aCoef;
-    m_d.bCoef = a_bCoef;
-    m_d.defined = true;
+  cmg_hierarchy* h() const;
+  static void check(int rc) {
+    if (rc != CMG_OK) MayDay::Error(cmg_last_error());
   }
-  const GpuOpDescription& description() const { return m_d; }
+
+ public:
+  // Every FAB of a_ld grown by one cell (zero where the FAB has no ghost
+  // layer), box after box in layout order: the cmg.h ghosted format.
+  static void packGhosted(const LDF& a_ld, std::vector<double>& a_out) {
+    a_out.clear();
+    const DisjointBoxLayout& dbl = a_ld.disjointBoxLayout();
+    for (DataIterator dit = a_ld.dataIterator(); dit.ok(); ++dit) {
+      const Box g = grow(dbl[dit()], 1);
+      const FArrayBox& f = a_ld[dit];
+      const size_t base = a_out.size();
+      a_out.resize(base + g.numPts());
+      double* o = a_out.data() + base;
+      if (f.box() == g) {
+        std::memcpy(o, f.dataPtr(0), g.numPts() * sizeof(double));
+        continue;
+      }
+      const Box fb = f.box();
+      size_t q = 0;
+      for (int k = g.smallEnd(2); k <= g.bigEnd(2); ++k)
+        for (int j = g.smallEnd(1); j <= g.bigEnd(1); ++j)
+          for (int i = g.smallEnd(0); i <= g.bigEnd(0); ++i, ++q) {
+            const IntVect iv(i, j, k);
+            o[q] = fb.contains(iv) ? f(iv, 0) : 0.0;
+          }
+    }
+  }
+  // Every cell of a ghosted array that a_ld's FABs hold (valid and ghost).
+  static void unpackGrown(const std::vector<double>& a_in, LDF& a_ld) {
+    const DisjointBoxLayout& dbl = a_ld.disjointBoxLayout();
+    size_t base = 0;
+    for (DataIterator dit = a_ld.dataIterator(); dit.ok(); ++dit) {
+      const Box g = grow(dbl[dit()], 1);
+      FArrayBox& f = a_ld[dit];
+      const Box r = g & f.box();
+      for (BoxIterator bit(r); bit.ok(); ++bit) {
+        const IntVect& iv = bit();
+        f(iv, 0) = a_in[base + (iv[0] - g.smallEnd(0)) +
+                        (size_t)g.size(0) * ((iv[1] - g.smallEnd(1)) + (size_t)g.size(1) * (iv[2] - g.smallEnd(2)))];
+      }
+      base += g.numPts();
+    }
+  }
+  // The valid cells of a ghosted array into a_ld.
+  static void unpackValid(const std::vector<double>& a_in, LDF& a_ld) {
+    const DisjointBoxLayout& dbl = a_ld.disjointBoxLayout();
+    size_t base = 0;
+    for (DataIterator dit = a_ld.dataIterator(); dit.ok(); ++dit) {
+      const Box& b = dbl[dit()];
+      const Box g = grow(b, 1);
+      const int gx = g.size(0), gy = g.size(1), nx = b.size(0);
+      FArrayBox& f = a_ld[dit];
+      for (int k = b.smallEnd(2); k <= b.bigEnd(2); ++k)
+        for (int j = b.smallEnd(1); j <= b.bigEnd(1); ++j) {
+          const double* src = a_in.data() + base + 1 + (size_t)gx * ((j - g.smallEnd(1)) + (size_t)gy * (k - g.smallEnd(2)));
+          std::memcpy(&f(IntVect(b.smallEnd(0), j, k), 0), src, nx * sizeof(double));
+        }
+      base += g.numPts();
+    }
+  }
 
  private:
-  GpuOpDescription m_d;
+  void in(const LDF& a_ld, std::vector<double>& a_buf) const {
+    if (!sameBoxes(a_ld.disjointBoxLayout(), m_grids))
+      MayDay::Error("cmg_chombo: LevelData on another layout than the operator's level");
+    packGhosted(a_ld, a_buf);
+  }
+  void out0(std::vector<double>& a_buf) const {
+    int64_t n = 0;
+    check(cmg_op_size(h(), m_lev, &n));
+    a_buf.assign(n, 0.0);
+  }
+  void outValid(const std::vector<double>& a_buf, LDF& a_ld) const {
+    if (!sameBoxes(a_ld.disjointBoxLayout(), m_grids))
+      MayDay::Error("cmg_chombo: LevelData on another layout than the operator's level");
+    unpackValid(a_buf, a_ld);
+  }
+  void amrOp(int a_form, LDF& a_out, const LDF* a_phiFine, const LDF& a_phi, const LDF* a_phiCoarse,
+             const LDF* a_rhs) {
+    const bool fine = a_phiFine && a_phiFine->isDefined();
+    const bool coarse = a_phiCoarse && a_phiCoarse->isDefined() && m_lev > 0;
+    in(a_phi, m_a);
+    if (a_rhs) in(*a_rhs, m_b);
+    if (fine) packGhosted(*a_phiFine, m_c);
+    if (coarse) packGhosted(*a_phiCoarse, m_d);
+    out0(m_o);
+    check(cmg_op_amr_operator(h(), m_lev, a_form, m_o.data(), fine ? m_c.data() : nullptr, m_a.data(),
+                              coarse ? m_d.data() : nullptr, a_rhs ? m_b.data() : nullptr));
+    outValid(m_o, a_out);
+  }
+  std::vector<double> m_d;
 };
 
 // AMRMultiGrid<LevelData<FArrayBox>> (AMRElliptic/AMRMultiGrid.H:301-470):
@@ -245,21 +575,157 @@ class GpuHierarchy {
   GpuOpDescription m_d;
 };
 
+inline cmg_hierarchy* GpuAMRPoissonOp::h() const { return m_sh->handle(); }
+
+// What AMRPoissonOpFactory and VCAMRPoissonOp2Factory share as
+// AMRLevelOpFactory<LevelData<FArrayBox>> (AMRElliptic/AMRMultiGrid.H:233-251,
+// MultiGrid.H:295-320): AMRnewOp for each AMR level's domain, MGnewOp for the
+// multigrid depths below level 0 (AMRPoissonOp.cpp:1923-1989: depth d exists
+// while level 0's boxes coarsen by 2^(d+1)), refToFiner.  The device
+// hierarchy behind the operators is built at the first AMRnewOp / MGnewOp
+// after define() (the VC coefficients are read then, as the reference's
+// factory computes its relaxation coefficient when it makes an operator) and
+// shared by every operator made from it.  MGnewOp below a refined level
+// returns NULL: with refinement ratio 2 between AMR levels the reference's
+// AMRMultiGrid never runs those depths (AMRMultiGrid::init sets their
+// MultiGrid depth to 0).
+class GpuOpFactoryBase : public AMRLevelOpFactory<LDF> {
+ public:
+  virtual ~GpuOpFactoryBase() {}
+  const GpuOpDescription& description() const { return m_d; }
+
+  virtual AMRLevelOp<LDF>* AMRnewOp(const ProblemDomain& a_indexSpace) {
+    const int l = levelOf(a_indexSpace);
+    std::shared_ptr<GpuHierarchy> sh = shared();
+    if (l >= sh->numLevels()) MayDay::Error("cmg_chombo: AMRnewOp for a level without boxes");
+    return newOp(sh, l);
+  }
+  virtual MGLevelOp<LDF>* MGnewOp(const ProblemDomain& a_fineIndexSpace, int a_depth, bool /*a_homoOnly*/ = true) {
+    const int l = levelOf(a_fineIndexSpace);
+    std::shared_ptr<GpuHierarchy> sh = shared();
+    if (l >= sh->numLevels()) MayDay::Error("cmg_chombo: MGnewOp for a level without boxes");
+    if (a_depth == 0) return newOp(sh, l);
+    int depths = 0;
+    GpuHierarchy::check(cmg_op_num_mg_depths(sh->handle(), &depths));
+    if (l > 0 || a_depth > depths) return nullptr;
+    return newOp(sh, -a_depth);
+  }
+  virtual int refToFiner(const ProblemDomain& a_indexSpace) const {
+    const int l = levelOf(a_indexSpace);
+    return l < m_d.refRatios.size() ? m_d.refRatios[l] : 2;
+  }
+
+ protected:
+  GpuOpDescription m_d;
+  BCHolder m_bc;
+  std::shared_ptr<GpuHierarchy> m_shared;
+
+  void redefine(const GpuOpDescription& a_d, BCHolder a_bc) {
+    m_d = a_d;
+    m_bc = a_bc;
+    m_shared.reset();
+    requireHomogeneousDirichlet(a_bc, a_d.coarseDomain, a_d.coarsedx);
+  }
+  int levelOf(const ProblemDomain& a_domain) const {
+    if (!m_d.defined) MayDay::Error("cmg_chombo: factory not defined");
+    ProblemDomain dom = m_d.coarseDomain;
+    for (int l = 0; l < m_d.grids.size(); ++l) {
+      if (dom.domainBox() == a_domain.domainBox()) return l;
+      if (l < m_d.refRatios.size()) dom.refine(m_d.refRatios[l]);
+    }
+    MayDay::Error("cmg_chombo: operator requested for a domain of no level");
+    return -1;
+  }
+  std::shared_ptr<GpuHierarchy> shared();
+  GpuAMRPoissonOp* newOp(const std::shared_ptr<GpuHierarchy>& a_sh, int a_lev) const;
+};
+
+// AMRPoissonOpFactory::define (AMRElliptic/AMRPoissonOp.H:535-541).
+class GpuAMRPoissonOpFactory : public GpuOpFactoryBase {
+ public:
+  void define(const ProblemDomain& a_coarseDomain, const Vector<DisjointBoxLayout>& a_grids,
+              const Vector<int>& a_refRatios, const Real& a_coarsedx, BCHolder a_bc, Real a_alpha = 0.0,
+              Real a_beta = 1.0) {
+    GpuOpDescription d;
+    d.coarseDomain = a_coarseDomain;
+    d.grids = a_grids;
+    d.refRatios = a_refRatios;
+    d.coarsedx = a_coarsedx;
+    d.alpha = a_alpha;
+    d.beta = a_beta;
+    d.vc = 0;
+    d.defined = true;
+    redefine(d, a_bc);
+  }
+};
+
+// VCAMRPoissonOp2Factory::define (AMRElliptic/VCAMRPoissonOp2.H:278-286).
+// The coefficients are read when the device hierarchy is built (the first
+// operator made, or GpuAMRMultiGrid::define).
+class GpuVCAMRPoissonOp2Factory : public GpuOpFactoryBase {
+ public:
+  void define(const ProblemDomain& a_coarseDomain, const Vector<DisjointBoxLayout>& a_grids,
+              const Vector<int>& a_refRatios, const Real& a_coarsedx, BCHolder a_bc, const Real& a_alpha,
+              Vector<RefCountedPtr<LDF> >& a_aCoef, const Real& a_beta,
+              Vector<RefCountedPtr<LevelData<FluxBox> > >& a_bCoef) {
+    GpuOpDescription d;
+    d.coarseDomain = a_coarseDomain;
+    d.grids = a_grids;
+    d.refRatios = a_refRatios;
+    d.coarsedx = a_coarsedx;
+    d.alpha = a_alpha;
+    d.beta = a_beta;
+    d.vc = 1;
+    d.aCoef = a_aCoef;
+    d.bCoef = a_bCoef;
+    d.defined = true;
+    redefine(d, a_bc);
+  }
+};
+
+inline std::shared_ptr<GpuHierarchy> GpuOpFactoryBase::shared() {
+  if (!m_shared) {
+    int nlev = 0;
+    while (nlev < m_d.grids.size() && m_d.grids[nlev].size() > 0) ++nlev;
+    std::shared_ptr<GpuHierarchy> sh(new GpuHierarchy);
+    sh->defineFrom(m_d.coarseDomain, m_d, nlev);
+    m_shared = sh;
+  }
+  return m_shared;
+}
+
+inline GpuAMRPoissonOp* GpuOpFactoryBase::newOp(const std::shared_ptr<GpuHierarchy>& a_sh, int a_lev) const {
+  if (a_lev >= 0) {
+    Real dx = m_d.coarsedx;
+    for (int l = 0; l < a_lev; ++l) dx /= m_d.refRatios[l];
+    DisjointBoxLayout finer;
+    const bool hasFiner = a_lev + 1 < a_sh->numLevels();
+    if (hasFiner) coarsen(finer, m_d.grids[a_lev + 1], 2);
+    return new GpuAMRPoissonOp(a_sh, a_lev, m_d.grids[a_lev], dx, hasFiner ? &finer : nullptr);
+  }
+  const int coarsening = 1 << (-a_lev);
+  DisjointBoxLayout g;
+  coarsen(g, m_d.grids[0], coarsening);
+  return new GpuAMRPoissonOp(a_sh, a_lev, g, m_d.coarsedx * coarsening, nullptr);
+}
+
+// AMRMultiGrid<LevelData<FArrayBox>> (AMRElliptic/AMRMultiGrid.H:301-470) on
+// the device: define, setSolverParameters, solve, computeAMRResidual, and the
+// reference's public solver members with its defaults (AMRMultiGrid.H:
+// 599-622): eps 1e-6, hang 1e-15, normThresh 1e-30, imin 5, iterMax 20,
+// iterMin -1, pre = post = bottom = 2, one V-cycle per level.
 class GpuAMRMultiGrid : private GpuHierarchy {
   friend class GpuBackwardEuler;
   friend class GpuAMRTGA;
 
  public:
-  int m_exitStatus = 0;
-  int m_verbosity = 0;
+  Real m_eps = 1e-6, m_hang = 1e-15, m_normThresh = 1e-30;
+  int m_imin = 5, m_iterMax = 20, m_iterMin = -1, m_verbosity = 3, m_exitStatus = -1;
+  int m_pre = 2, m_post = 2, m_bottom = 2, m_numMG = 1;
 
   GpuAMRMultiGrid() {}
 
-  void define(const ProblemDomain& a_coarseDomain, GpuAMRPoissonOpFactory& a_factory, LinearSolver<LDF>* a_bottom,
-              int a_numLevels) {
-    defineWith(a_coarseDomain, a_factory.description(), a_bottom, a_numLevels);
-  }
-  void define(const ProblemDomain& a_coarseDomain, GpuVCAMRPoissonOp2Factory& a_factory, LinearSolver<LDF>* a_bottom,
+  void define(const ProblemDomain& a_coarseDomain, GpuOpFactoryBase& a_factory, LinearSolver<LDF>* a_bottom,
               int a_numLevels) {
     defineWith(a_coarseDomain, a_factory.description(), a_bottom, a_numLevels);
   }
@@ -267,26 +733,35 @@ class GpuAMRMultiGrid : private GpuHierarchy {
   // AMRMultiGrid::setSolverParameters (AMRMultiGrid.H:451-458, 527-546).
   void setSolverParameters(const int& a_pre, const int& a_post, const int& a_bottom, const int& a_numMG,
                            const int& a_iterMax, const Real& a_eps, const Real& a_hang, const Real& a_normThresh) {
-    m_p.pre = a_pre;
-    m_p.post = a_post;
-    m_p.bottom = a_bottom;
-    m_p.num_mg = a_numMG;
-    m_p.iter_max = a_iterMax;
-    m_p.eps = a_eps;
-    m_p.hang = a_hang;
-    m_p.norm_thresh = a_normThresh;
+    m_pre = a_pre;
+    m_post = a_post;
+    m_bottom = a_bottom;
+    m_numMG = a_numMG;
+    m_iterMax = a_iterMax;
+    m_eps = a_eps;
+    m_hang = a_hang;
+    m_normThresh = a_normThresh;
   }
 
   // AMRMultiGrid::solve (AMRMultiGrid.H:894-1124) on the device.
+  // forceHomogeneous changes nothing: the boundary values are zero either way.
+  // A residual norm that turns NaN or infinite ends the solve (the C ABI's
+  // CMG_EDIVERGED); phi and m_exitStatus are set as for any other end, with a
+  // warning, as the reference's loop also stops on a NaN norm.
   void solve(Vector<LDF*>& a_phi, const Vector<LDF*>& a_rhs, int l_max, int l_base, bool a_zeroPhi = true,
              bool /*forceHomogeneous*/ = false) {
     checkRange(l_max, l_base);
     setLevels(a_rhs, false);
     if (!a_zeroPhi) setLevels(a_phi, true);
-    m_history.assign(m_p.iter_max + 2, 0.0);
+    const cmg_solve_params p = params();
+    m_history.assign(std::max(p.iter_max, p.iter_min) + 2, 0.0);
     int st = 0, it = 0, hl = 0;
-    check(cmg_solve(m_h, &m_p, a_zeroPhi ? 1 : 0, &st, &it, m_history.data(), (int)m_history.size(), &hl));
-    m_history.resize(hl);
+    const int rc = cmg_solve(m_h, &p, a_zeroPhi ? 1 : 0, &st, &it, m_history.data(), (int)m_history.size(), &hl);
+    if (rc == CMG_EDIVERGED)
+      MayDay::Warning(cmg_last_error());
+    else
+      check(rc);
+    m_history.resize(std::min<size_t>(hl, m_history.size()));
     m_exitStatus = st;
     m_iterations = it;
     getPhi(a_phi);
@@ -311,9 +786,23 @@ class GpuAMRMultiGrid : private GpuHierarchy {
   void clear() { GpuHierarchy::clear(); }
 
  private:
-  cmg_solve_params m_p = {4, 4, 4, 1, 100, 5, 1e-10, 1e-10, 1e-30};
   std::vector<double> m_history;
   int m_iterations = 0;
+
+  cmg_solve_params params() const {
+    cmg_solve_params p;
+    p.pre = m_pre;
+    p.post = m_post;
+    p.bottom = m_bottom;
+    p.num_mg = m_numMG;
+    p.iter_max = m_iterMax;
+    p.imin = m_imin;
+    p.eps = m_eps;
+    p.hang = m_hang;
+    p.norm_thresh = m_normThresh;
+    p.iter_min = m_iterMin;
+    return p;
+  }
 
   void checkRange(int l_max, int l_base) const {
     if (!m_h) MayDay::Error("GpuAMRMultiGrid: solve before define");
@@ -351,7 +840,8 @@ class GpuBackwardEuler {
     s.setLevels(a_phiOld, true);
     s.setLevels(a_source, false);
     int st = 0, it = 0;
-    GpuHierarchy::check(cmg_backward_euler(s.m_h, &s.m_p, a_dt, 1, a_zeroPhi ? 1 : 0, &st, &it));
+    const cmg_solve_params p = s.params();
+    GpuHierarchy::check(cmg_backward_euler(s.m_h, &p, a_dt, 1, a_zeroPhi ? 1 : 0, &st, &it));
     s.m_exitStatus = st;
     s.m_iterations = it;
     s.getPhi(a_phiNew);
@@ -376,7 +866,8 @@ class GpuAMRTGA {
     s.setLevels(a_phiOld, true);
     s.setLevels(a_source, false);
     int st[2] = {0, 0}, it[2] = {0, 0};
-    GpuHierarchy::check(cmg_tga(s.m_h, &s.m_p, a_dt, 1, st, it));
+    const cmg_solve_params p = s.params();
+    GpuHierarchy::check(cmg_tga(s.m_h, &p, a_dt, 1, st, it));
     s.m_exitStatus = st[1];
     s.m_iterations = it[1];
     s.getPhi(a_phiNew);

@@ -37,6 +37,8 @@ def test_dropin_matches_reference_solver(name):
     assert out["same_history_length"], out
     assert out["history_dev"] <= TOL, out
     assert out["phi_rel_dev"] <= TOL, out
+    # bit for bit
+    assert out["history_dev"] == 0.0 and out["phi_rel_dev"] == 0.0, out
     # computeAMRResidual through the drop-in reproduces the solve's last entry.
     assert out["gpu_final_residual"] == out["gpu_history_last"], out
 
@@ -102,3 +104,54 @@ def test_dropin_fineinterp_matches_reference(name):
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     out = json.loads(r.stdout.strip().splitlines()[-1])
     assert out["cells"] > 0 and out["max_abs_diff"] == 0.0, out
+
+
+OPS_CASES = {
+    "vc_3lev_16": "n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=-1",
+    "poisson_3lev_32": "n0=32 levels=3 maxbox=16 block=4 op=0 alpha=0 beta=1",
+    "helmholtz_2lev_16": "n0=16 levels=2 maxbox=8 block=4 op=0 alpha=1 beta=-1",
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(OPS_CASES))
+def test_each_operator_matches_reference_bit_for_bit(name):
+    """The reference's AMRPoissonOp / VCAMRPoissonOp2 and the GPU AMRLevelOps (cmg_chombo::GpuAMRPoissonOp) get
+    the same LevelData inputs, one method at a time: residual, applyOp, relax, preCond, the AMROperator /
+    AMRResidual family with coarse-fine interpolation and reflux, AMRRestrictS, assignCopier, zeroCovered,
+    AMRProlongS, AMRUpdateResidual, QuadCFInterp::coarseFineInterp (ghost cells), norms, dot products, BLAS-1,
+    and on every multigrid depth residual, relax, preCond, restrictResidual, prolongIncrement.  Every valid cell
+    of every output is equal (the operator family on levels with a finer level compares the cells not under it:
+    the reference's flux register also writes covered cells, which every caller discards)."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in check not built (make -C oracle dropin, needs the reference tree)")
+    r = subprocess.run([DROPIN] + OPS_CASES[name].split() + ["ops=1"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    ops = out["ops"]
+    names = {o["op"] for o in ops}
+    for needed in ("residual", "applyOp", "relax2", "preCond", "AMROperator", "AMRResidual", "AMRRestrictS",
+                   "assignCopier", "AMRProlongS", "AMRUpdateResidual", "coarseFineInterp", "restrictResidual",
+                   "prolongIncrement", "norm2", "dotProduct", "axby"):
+        assert needed in names, (needed, sorted(names))
+    bad = [o for o in ops if o["ndiff"] != 0]
+    assert not bad, bad
+    assert all(o["cells"] > 0 for o in ops), ops
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(OPS_CASES))
+def test_reference_amrmultigrid_over_gpu_operators(name):
+    """The reference's own AMRMultiGrid, unmodified, defined once with the reference factory and once with the
+    GPU factory (an AMRLevelOpFactory<LevelData<FArrayBox>>): identical exit status, iteration count, residual
+    history and phi, bit for bit."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in check not built (make -C oracle dropin, needs the reference tree)")
+    r = subprocess.run([DROPIN] + OPS_CASES[name].split() + ["amrmg=1"], capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["gpu_exit"] == out["cpu_exit"] == 1, out
+    assert out["gpu_iters"] == out["cpu_iters"], out
+    assert out["history_exact"], out
+    assert out["phi_ndiff"] == 0, out

@@ -1,11 +1,11 @@
 """FP64 GPU solve against the reference solve (golden fixtures from the
 reference's own AMRMultiGrid): same box layouts, same seeded inputs, same
-solver parameters.  The GPU path reproduces the reference's operation order,
-so phi must agree to 1e-12 relative L-infinity (relative to max|phi| on the
-level), every residual-history entry to 1e-12 of the initial residual (the
-scale of the solver's own stopping test, eps * r0), and the iteration count
-and exit status exactly.  Single-level solves are additionally required to be
-bit-identical to the reference."""
+solver parameters.  The GPU path reproduces the reference's operation order
+in every operator, so the solve is bit-identical: the same exit status and
+iteration count, every residual-history entry equal, and phi equal on every
+level (stored in full, or every sample_stride-th value of the large
+fixtures).  The 1e-12 bounds the north star states are checked first so that
+a failure shows how far apart the values are."""
 import numpy as np
 import pytest
 
@@ -34,20 +34,18 @@ def test_solve_matches_reference(cmg, name):
     assert len(hist) == len(ref_hist), (hist, ref_hist)
     dev = np.abs(hist - ref_hist) / ref_hist[0]
     assert dev.max() <= TOL, (hist, ref_hist)
-    if len(meta["boxes"]) == 1:
-        assert np.array_equal(hist, ref_hist)
+    assert np.array_equal(hist, ref_hist), (hist, ref_hist)
     for lev in range(len(meta["boxes"])):
         phi = h.phi(lev)
         scale = meta["phi_absmax"][lev]
         if meta["full"]:
             ref = arrays[f"phi{lev}"]
-            assert np.max(np.abs(phi - ref)) <= TOL * scale, (lev, np.max(np.abs(phi - ref)) / scale)
-            if len(meta["boxes"]) == 1:
-                assert np.array_equal(phi, ref)
+            got = phi
         else:
             ref = arrays[f"phi{lev}_sample"]
             got = phi[::meta["sample_stride"]]
-            assert np.max(np.abs(got - ref)) <= TOL * scale, (lev, np.max(np.abs(got - ref)) / scale)
+        assert np.max(np.abs(got - ref)) <= TOL * scale, (lev, np.max(np.abs(got - ref)) / scale)
+        assert np.array_equal(got, ref), (lev, int(np.sum(got != ref)), got.size)
     h.close()
 
 

@@ -18,7 +18,7 @@
 // Usage: cmg_oracle key=value ... out=<prefix>
 //   n0=64 levels=1 maxbox=32 block=8 fill=0.75 op=0|1 alpha=0 beta=1
 //   seed=20261203 thresh=0.1 pre=4 post=4 bottom=4 iters=100 eps=1e-10
-//   hang=1e-10 dumpphi=1
+//   hang=1e-10 dumpphi=1 plansonly=0 (1: write <prefix>.plans and stop)
 // Writes <prefix>.json (metadata, boxes, plans, residual history) and
 // <prefix>.bin (raw little-endian doubles: per level, per box in layout
 // order, valid cells x-fastest: rhs, phi, then for op=1 acoef and the three
@@ -140,6 +140,44 @@ int main(int argc, char** argv) {
   Vector<ProblemDomain>& domains = P.domains;
   Vector<Real>& dxs = P.dxs;
   Vector<DisjointBoxLayout>& grids = P.grids;
+  if (argi("plansonly", 0)) {
+    // Box layouts and copier plans only (no solve): <prefix>.plans, raw
+    // little-endian int32, per level the exchange plan then (levels >= 1)
+    // the coarsened-fine plan, each as a count followed by 14 ints per item
+    // (from, to, fromRegion lo/hi, toRegion lo/hi).
+    FILE* pf = std::fopen((out + ".plans").c_str(), "wb");
+    auto put = [&](const Copier& c) {
+      std::vector<int> v;
+      for (CopyIterator it(c, CopyIterator::LOCAL); it.ok(); ++it) {
+        const MotionItem& m = it();
+        v.push_back(m.fromIndex.intCode());
+        v.push_back(m.toIndex.intCode());
+        for (const Box* b : {&m.fromRegion, &m.toRegion}) {
+          for (int d = 0; d < 3; ++d) v.push_back(b->smallEnd(d));
+          for (int d = 0; d < 3; ++d) v.push_back(b->bigEnd(d));
+        }
+      }
+      int n = (int)(v.size() / 14);
+      std::fwrite(&n, sizeof(int), 1, pf);
+      std::fwrite(v.data(), sizeof(int), v.size(), pf);
+    };
+    for (int l = 0; l < nlev; ++l) {
+      Copier ex;
+      ex.exchangeDefine(grids[l], IntVect::Unit);
+      ex.trimEdges(grids[l], IntVect::Unit);
+      put(ex);
+      if (l > 0) {
+        DisjointBoxLayout cf;
+        coarsen(cf, grids[l], 2);
+        Copier c;
+        c.define(cf, grids[l - 1], IntVect::Zero);
+        put(c);
+      }
+    }
+    std::fclose(pf);
+    std::printf("oracle: plans of %d levels\n", nlev);
+    return 0;
+  }
   Vector<LDF*>& phi = P.phi;
   Vector<LDF*>& rhs = P.rhs;
   Vector<RefCountedPtr<LDF> >& aCoef = P.aCoef;

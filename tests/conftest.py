@@ -34,8 +34,8 @@ def golden(name):
     return meta, arrays
 
 
-# Fixtures whose GPU checks take minutes (the 149M-cell 256^3 workload); run
-# them with CMG_LARGE=1.
+# Fixtures skipped when CMG_LARGE=0 (the 149M-cell 256^3 workload, about half
+# a minute of GPU checks); they run by default.
 LARGE = {"config2_vc_3lev_256"}
 
 
@@ -44,10 +44,11 @@ LARGE = {"config2_vc_3lev_256"}
 OTHER_PATHS = ("bicgstab_", "heat_", "fineinterp_")
 
 
-def golden_names():
-    """The AMRMultiGrid fixtures."""
+def golden_names(include_large=False):
+    """The AMRMultiGrid fixtures (host-only checks pass include_large: they
+    are quick at every size)."""
     names = sorted(f[:-5] for f in os.listdir(GOLDEN) if f.endswith(".json") and not f.startswith(OTHER_PATHS))
-    if os.environ.get("CMG_LARGE") != "1":
+    if not include_large and os.environ.get("CMG_LARGE") == "0":
         names = [n for n in names if n not in LARGE]
     return names
 
@@ -55,15 +56,19 @@ def golden_names():
 def covered_mask(boxes, finer_boxes):
     """Valid cells of a level (boxes in layout order, x fastest) covered by the
     next finer level (ratio 2): the cells outside the composite solution."""
+    if not boxes:
+        return np.zeros(0, bool)
+    b = np.array(boxes)
+    lo, hi = b[:, :3].min(axis=0), b[:, 3:].max(axis=0)
+    n = hi - lo + 1
+    vol = np.zeros((n[2], n[1], n[0]), bool)
+    for f in finer_boxes:
+        flo = np.array(f[:3]) // 2 - lo
+        fhi = np.array(f[3:]) // 2 - lo
+        vol[flo[2]:fhi[2] + 1, flo[1]:fhi[1] + 1, flo[0]:fhi[0] + 1] = True
     masks = []
-    fine = [(np.array(b[:3]) // 2, np.array(b[3:]) // 2) for b in finer_boxes]
-    for b in boxes:
-        lo, hi = np.array(b[:3]), np.array(b[3:])
-        n = hi - lo + 1
-        m = np.zeros((n[2], n[1], n[0]), bool)
-        for flo, fhi in fine:
-            a, c = np.maximum(lo, flo), np.minimum(hi, fhi)
-            if np.all(a <= c):
-                m[a[2] - lo[2]:c[2] - lo[2] + 1, a[1] - lo[1]:c[1] - lo[1] + 1, a[0] - lo[0]:c[0] - lo[0] + 1] = True
-        masks.append(m.ravel())
-    return np.concatenate(masks) if masks else np.zeros(0, bool)
+    for x in boxes:
+        a = np.array(x[:3]) - lo
+        c = np.array(x[3:]) - lo
+        masks.append(vol[a[2]:c[2] + 1, a[1]:c[1] + 1, a[0]:c[0] + 1].ravel())
+    return np.concatenate(masks)

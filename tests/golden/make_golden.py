@@ -34,7 +34,7 @@ CASES = {
     "poisson_3lev_32": ("n0=32 levels=3 maxbox=16 op=0 alpha=0 beta=1", False),
     "vc_3lev_32": ("n0=32 levels=3 maxbox=16 op=1 alpha=1 beta=-1", False),
     "vc_2lev_64": ("n0=64 levels=2 maxbox=32 op=1 alpha=1 beta=-1", False),
-    "config0_poisson_64": ("n0=64 levels=1 maxbox=32 op=0 alpha=0 beta=1", False),
+    "config0_poisson_64": ("n0=64 levels=1 maxbox=32 op=0 alpha=0 beta=1", True),
     "config1_vc_3lev_128": ("n0=128 levels=3 maxbox=32 op=1 alpha=1 beta=-1", False),
     # the ~40M-cell mixed-precision workload: sparser samples keep the fixture small
     "config2_vc_3lev_256": ("n0=256 levels=3 maxbox=32 op=1 alpha=1 beta=-1", False, 1009),

@@ -1,12 +1,14 @@
 """Host geometry against the reference: base-level splitting and the Copier
 motion plans (exchange and coarsened-fine -> coarse) must match bit for bit,
 item for item, in order."""
+import os
+
 import numpy as np
 import pytest
 
-from conftest import golden, golden_names
+from conftest import GOLDEN, golden, golden_names
 
-CASES = golden_names()
+CASES = golden_names(include_large=True)
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -15,6 +17,13 @@ def test_domain_split_matches_reference(cmg, name):
     n0, maxbox, block = meta["n0"], meta["maxbox"], meta["block"]
     boxes = cmg.domain_split((0, 0, 0), (n0 - 1,) * 3, maxbox, block)
     assert [list(b) for b in boxes] == meta["boxes"][0]
+
+
+def plan_arrays(name):
+    """The complete reference plans of the benchmark-size fixtures, whose JSON
+    keeps only the plan sizes (tests/golden/make_golden_plans.py)."""
+    path = os.path.join(GOLDEN, name + "_plans.npz")
+    return dict(np.load(path)) if os.path.exists(path) else None
 
 
 def as_items(plan):
@@ -33,7 +42,9 @@ def test_exchange_plans_match_reference(cmg, name):
         if "exchange_plans" in meta:
             assert as_items(plan) == ref_items(meta["exchange_plans"][lev]), f"level {lev}"
         else:
-            assert len(plan) == meta["exchange_plan_sizes"][lev]
+            ref = plan_arrays(name)[f"exchange{lev}"]
+            assert len(plan) == meta["exchange_plan_sizes"][lev] == len(ref)
+            assert np.array_equal(np.asarray(plan, dtype=np.int64), ref.astype(np.int64)), f"level {lev}"
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -44,7 +55,9 @@ def test_coarse_fine_plans_match_reference(cmg, name):
         if "coarsened_fine_plans" in meta:
             assert as_items(plan) == ref_items(meta["coarsened_fine_plans"][lev - 1]), f"level {lev}"
         else:
-            assert len(plan) == meta["coarsened_fine_plan_sizes"][lev - 1]
+            ref = plan_arrays(name)[f"coarsened_fine{lev}"]
+            assert len(plan) == meta["coarsened_fine_plan_sizes"][lev - 1] == len(ref)
+            assert np.array_equal(np.asarray(plan, dtype=np.int64), ref.astype(np.int64)), f"level {lev}"
 
 
 def test_fine_levels_nest_in_coarse(cmg):

@@ -12,8 +12,6 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcmg.so")
 
-CMG_OK, CMG_EINVAL, CMG_ENOMEM, CMG_ECUDA, CMG_EINTERNAL = range(5)
-
 
 class CmgError(RuntimeError):
     def __init__(self, code, msg):
@@ -23,6 +21,10 @@ class CmgError(RuntimeError):
 
 class Box(ctypes.Structure):
     _fields_ = [("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3)]
+
+
+# Status codes (cmg.h).
+CMG_OK, CMG_EINVAL, CMG_ENOMEM, CMG_ECUDA, CMG_EINTERNAL, CMG_EDIVERGED, CMG_ETIMEOUT, CMG_ECANCELLED = range(8)
 
 
 class SolveParams(ctypes.Structure):
@@ -54,7 +56,9 @@ class Request(ctypes.Structure):
                 ("max_box", ctypes.c_int), ("block_factor", ctypes.c_int), ("fill_ratio", ctypes.c_double),
                 ("thresh", ctypes.c_double), ("seed", ctypes.c_uint64), ("op", ctypes.c_int),
                 ("alpha", ctypes.c_double), ("beta", ctypes.c_double), ("params", SolveParams),
-                ("mixed", ctypes.c_int), ("graphs", ctypes.c_int), ("device_tags", ctypes.c_int)]
+                ("mixed", ctypes.c_int), ("graphs", ctypes.c_int), ("device_tags", ctypes.c_int),
+                ("timeout", ctypes.c_double), ("cancel", ctypes.POINTER(ctypes.c_int)),
+                ("inject_nan_rhs", ctypes.c_int), ("inject_cancel_after", ctypes.c_int)]
 
 
 class RequestResult(ctypes.Structure):
@@ -64,7 +68,8 @@ class RequestResult(ctypes.Structure):
                 ("solve_seconds", ctypes.c_double), ("r0", ctypes.c_double), ("rfinal", ctypes.c_double),
                 ("grid_seconds", ctypes.c_double), ("build_seconds", ctypes.c_double),
                 ("fill_seconds", ctypes.c_double),
-                ("cells", ctypes.c_int64), ("device_bytes", ctypes.c_uint64), ("phi_hash", ctypes.c_uint64)]
+                ("cells", ctypes.c_int64), ("device_bytes", ctypes.c_uint64), ("phi_hash", ctypes.c_uint64),
+                ("estimate_bytes", ctypes.c_uint64), ("message", ctypes.c_char * 160)]
 
 
 def serve(requests, hbm_budget=120e9, max_inflight=16, open_loop=True):
@@ -82,12 +87,20 @@ def serve(requests, hbm_budget=120e9, max_inflight=16, open_loop=True):
         q.params = r.get("params") or solve_params(eps=r.get("eps", 1e-10))
         q.mixed, q.graphs = int(r.get("mixed", True)), int(r.get("graphs", True))
         q.device_tags = int(r.get("device_tags", False))
+        q.timeout = r.get("timeout", 0.0)
+        if r.get("cancel") is not None:  # a ctypes.c_int the caller may set while the call runs
+            q.cancel = ctypes.pointer(r["cancel"])
+        q.inject_nan_rhs = int(r.get("inject_nan_rhs", False))
+        q.inject_cancel_after = int(r.get("inject_cancel_after", -1))
     out = (RequestResult * max(n, 1))()
     wall = ctypes.c_double()
     _check(lib().cmg_serve(arr, n, ctypes.c_double(hbm_budget), int(max_inflight), int(open_loop), out,
                            ctypes.byref(wall)))
     keys = [f[0] for f in RequestResult._fields_]
-    return [{k: getattr(out[i], k) for k in keys} for i in range(n)], wall.value
+    res = [{k: getattr(out[i], k) for k in keys} for i in range(n)]
+    for r in res:
+        r["message"] = r["message"].decode(errors="replace")
+    return res, wall.value
 
 
 _lib = None
@@ -299,12 +312,15 @@ class Hierarchy:
         """AMRMultiGrid::solve on the device; mixed=True runs the FP32
         V-cycles inside FP64 iterative refinement (cmg_solve_mixed)."""
         p = params or solve_params()
-        hist = np.zeros(p.iter_max + 2, dtype=np.float64)
+        hist = np.zeros(max(p.iter_max, p.iter_min) + 2, dtype=np.float64)
         st, it, hl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         fn = lib().cmg_solve_mixed if mixed else lib().cmg_solve
-        _check(fn(self.h, ctypes.byref(p), int(zero_phi), ctypes.byref(st), ctypes.byref(it),
-                  _ptr(hist), len(hist), ctypes.byref(hl)))
-        return {"exit_status": st.value, "iterations": it.value, "history": hist[:hl.value].copy()}
+        rc = fn(self.h, ctypes.byref(p), int(zero_phi), ctypes.byref(st), ctypes.byref(it),
+                _ptr(hist), len(hist), ctypes.byref(hl))
+        if rc != CMG_EDIVERGED:
+            _check(rc)
+        return {"exit_status": st.value, "iterations": it.value, "history": hist[:min(hl.value, len(hist))].copy(),
+                "diverged": rc == CMG_EDIVERGED}
 
     def set_alpha_beta(self, alpha, beta):
         """TGAHelmOp::setAlphaAndBeta on every operator of the hierarchy (cmg_set_alpha_beta)."""

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -587,8 +588,6 @@ int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_infligh
     for (int i = 0; i < n; ++i) {
       const cmg_request& a = reqs[i];
       cmg::Request& r = rq[i];
-      if (a.n0 < 8 || a.levels < 1 || (a.op != 0 && a.op != 1) || a.block_factor < 1 || a.max_box < 0)
-        throw std::invalid_argument("cmg: invalid request");
       r.arrival = a.arrival;
       r.n0 = a.n0;
       r.levels = a.levels;
@@ -613,6 +612,10 @@ int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_infligh
       r.mixed = a.mixed != 0;
       r.graphs = a.graphs != 0;
       r.deviceTags = a.device_tags != 0;
+      r.timeout = a.timeout;
+      r.cancel = a.cancel;
+      r.injectNanRHS = a.inject_nan_rhs != 0;
+      r.injectCancelAfter = a.inject_cancel_after;
     }
     cmg::ServeOptions opt;
     opt.hbmBudget = hbm_budget;
@@ -639,6 +642,8 @@ int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_infligh
       o.build_seconds = a.buildSeconds;
       o.fill_seconds = a.fillSeconds;
       o.cells = a.cells;
+      o.estimate_bytes = a.estimate;
+      std::snprintf(o.message, sizeof(o.message), "%s", a.message.c_str());
       o.device_bytes = a.deviceBytes;
       o.phi_hash = a.phiHash;
     }

@@ -13,6 +13,7 @@
 #define CMG_SERVE_H
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "solver.H"
@@ -29,6 +30,13 @@ struct Request {
   SolveParams params;
   bool mixed = true, graphs = true;
   bool deviceTags = false;  // tagging pass of the grid generation on the device (tagging.H)
+  double timeout = 0;       // seconds after arrival to finish by (0: no limit)
+  const volatile int* cancel = nullptr;  // set non-zero by the caller (any thread) to cancel
+  // Host-side fault injection for tests: a NaN in the right-hand side of the
+  // finest level after the inputs are generated; cancellation after this
+  // many iterations (-1: never).
+  bool injectNanRHS = false;
+  int injectCancelAfter = -1;
 };
 
 struct RequestResult {
@@ -40,7 +48,9 @@ struct RequestResult {
   int64_t cells = 0;
   size_t deviceBytes = 0;
   uint64_t phiHash = 0;  // FNV-1a over the 64-bit words of phi on every level (valid cells)
-  int error = 0;
+  size_t estimate = 0;   // admission estimate of the device bytes
+  int error = 0;         // 0 or a CMG_* status (cmg.h)
+  std::string message;   // what went wrong when error != 0
 };
 
 struct ServeOptions {
@@ -49,7 +59,15 @@ struct ServeOptions {
   bool openLoop = true;      // release requests at their arrival times
 };
 
-// Runs every request; returns the wall time of the run in seconds.
+// Status codes of a request (the C ABI's CMG_* values).
+enum { REQ_OK = 0, REQ_EINVAL = 1, REQ_ENOMEM = 2, REQ_ECUDA = 3, REQ_EINTERNAL = 4, REQ_EDIVERGED = 5,
+       REQ_ETIMEOUT = 6, REQ_ECANCELLED = 7 };
+
+// Runs every request; returns the wall time of the run in seconds.  A
+// request that fails (invalid description, more memory than the whole
+// budget, a non-finite residual, its time limit, cancellation, an error
+// while it runs) gets its status and message and releases what it held; the
+// other requests are not affected.
 double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vector<RequestResult>& out);
 
 // Device bytes a request's hierarchy will hold, from its box lists (the

@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <string>
 #include <condition_variable>
 #include <cstring>
 #include <memory>
@@ -53,6 +55,31 @@ size_t estimateDeviceBytes(const std::vector<std::vector<Box>>& boxes, bool vc, 
   return (size_t)(bytes * 1.3) + (64u << 20);
 }
 
+namespace {
+
+// Failure of one request: its status and message.
+struct RequestError : std::runtime_error {
+  int code;
+  RequestError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// The description checks the C ABI used to apply to the whole call, now per
+// request (an invalid request fails alone).
+void validate(const Request& q) {
+  auto bad = [](const char* what) { throw RequestError(REQ_EINVAL, std::string("cmg: invalid request: ") + what); };
+  if (q.n0 < 8) bad("base size below 8");
+  if (q.levels < 1) bad("no levels");
+  if (q.op != 0 && q.op != 1) bad("operator is 0 (AMRPoissonOp) or 1 (VCAMRPoissonOp2)");
+  if (q.blockFactor < 1 || q.maxBox < 0) bad("blocking factor or maximum box size");
+  if (q.maxBox > 0 && q.maxBox % q.blockFactor != 0) bad("maximum box size not a multiple of the blocking factor");
+  if (q.n0 % q.blockFactor != 0) bad("base size not a multiple of the blocking factor");
+  const SolveParams& p = q.params;
+  if (p.pre < 0 || p.post < 0 || p.bottom < 0 || p.numMG < 1 || p.iterMax < 0) bad("solver parameters");
+  if (!(p.eps > 0) || !(q.timeout >= 0)) bad("tolerance or time limit");
+}
+
+}  // namespace
+
 double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vector<RequestResult>& out) {
   const size_t n = reqs.size();
   out.assign(n, RequestResult());
@@ -68,6 +95,7 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
   double used = 0;
   const Clock::time_point t0 = Clock::now();
   auto since = [&](Clock::time_point t) { return std::chrono::duration<double>(t - t0).count(); };
+  auto at = [&](double sec) { return t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(sec)); };
 
   auto work = [&]() {
     cudaSetDevice(dev);
@@ -80,12 +108,24 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
       }
       const Request& q = reqs[idx];
       RequestResult& r = out[idx];
-      if (opt.openLoop) std::this_thread::sleep_until(t0 + std::chrono::duration_cast<Clock::duration>(
-                                                                 std::chrono::duration<double>(q.arrival)));
+      if (opt.openLoop) std::this_thread::sleep_until(at(q.arrival));
+      const bool limited = q.timeout > 0;
+      const Clock::time_point deadline = at((opt.openLoop ? q.arrival : 0.0) + q.timeout);
+      // Why the request must stop now (0: it may go on).
+      auto stopCode = [&]() -> int {
+        if (q.cancel && *q.cancel) return REQ_ECANCELLED;
+        if (limited && Clock::now() >= deadline) return REQ_ETIMEOUT;
+        return REQ_OK;
+      };
+      auto stopError = [&](int code) {
+        throw RequestError(code, code == REQ_ECANCELLED ? "cmg: request cancelled" : "cmg: request time limit passed");
+      };
       double est = 0;
       bool reserved = false;
       cudaStream_t s = nullptr;
       try {
+        validate(q);
+        if (int c = stopCode()) stopError(c);
         const Clock::time_point ts = Clock::now();
         if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
           throw std::runtime_error("cmg: stream");
@@ -98,9 +138,22 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
         }
         r.gridSeconds = std::chrono::duration<double>(Clock::now() - ts).count();
         est = (double)estimateDeviceBytes(boxes, q.op == 1, q.mixed);
+        r.estimate = (size_t)est;
+        if (est > opt.hbmBudget)
+          throw RequestError(REQ_ENOMEM, "cmg: request needs about " + std::to_string((long long)est) +
+                                             " device bytes, more than the whole budget of " +
+                                             std::to_string((long long)opt.hbmBudget));
         {
+          // Admission: wait until the request fits beside the admitted ones,
+          // looking at cancellation and the time limit every 5 ms.
           std::unique_lock<std::mutex> lk(m);
-          cv.wait(lk, [&]() { return used + est <= opt.hbmBudget || used == 0; });
+          while (!(used + est <= opt.hbmBudget)) {
+            if (int c = stopCode()) {
+              lk.unlock();
+              stopError(c);
+            }
+            cv.wait_for(lk, std::chrono::milliseconds(5));
+          }
           used += est;
           reserved = true;
         }
@@ -118,12 +171,26 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
           const Clock::time_point tf = Clock::now();
           r.buildSeconds = std::chrono::duration<double>(tf - tb).count();
           S->fillSyntheticDevice(q.seed);
+          if (q.injectNanRHS) {
+            // one valid cell of the finest right-hand side made NaN
+            const int fl = S->numLevels() - 1;
+            const BoxDesc& b0 = S->level(fl).boxes[0];
+            const double nan = std::nan("");
+            if (cudaMemcpy(S->devRHS(fl) + cellIndex(b0, b0.lo[0], b0.lo[1], b0.lo[2]), &nan, sizeof(double),
+                           cudaMemcpyHostToDevice) != cudaSuccess)
+              throw std::runtime_error("cmg: fault injection copy");
+          }
           r.fillSeconds = std::chrono::duration<double>(Clock::now() - tf).count();
           S->setUseGraphs(q.graphs);
           const Clock::time_point tsolve = Clock::now();
           r.setupSeconds = std::chrono::duration<double>(tsolve - ts).count();
           r.started = since(tsolve);
-          SolveResult res = q.mixed ? S->solveMixed(q.params) : S->solve(q.params);
+          SolveParams sp = q.params;
+          sp.interrupt = [&](int iter) -> int {
+            if (q.injectCancelAfter >= 0 && iter >= q.injectCancelAfter) return REQ_ECANCELLED;
+            return stopCode();
+          };
+          SolveResult res = q.mixed ? S->solveMixed(sp) : S->solve(sp);
           const Clock::time_point tsolved = Clock::now();
           r.solveSeconds = std::chrono::duration<double>(tsolved - tsolve).count();
           r.solved = since(tsolved);
@@ -131,6 +198,10 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
           r.iterations = res.iterations;
           r.r0 = res.history.front();
           r.rfinal = res.history.back();
+          if (res.interrupted) stopError(res.interrupted);
+          if (res.diverged)
+            throw RequestError(REQ_EDIVERGED, "cmg: residual norm is not finite after " +
+                                                  std::to_string(res.iterations) + " iterations");
           uint64_t h = 1469598103934665603ULL;
           std::vector<double> phi;
           for (int l = 0; l < S->numLevels(); ++l) {
@@ -145,12 +216,23 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
         cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
         s = nullptr;
+      } catch (const RequestError& e) {
+        r.error = e.code;
+        r.message = e.what();
+      } catch (const std::bad_alloc& e) {
+        r.error = REQ_ENOMEM;
+        r.message = e.what();
+      } catch (const std::exception& e) {
+        const std::string w = e.what();
+        r.error = w.find("cudaMalloc") != std::string::npos ? REQ_ENOMEM : REQ_EINTERNAL;
+        r.message = w;
       } catch (...) {
-        r.error = 1;
-        if (s) {
-          cudaStreamSynchronize(s);
-          cudaStreamDestroy(s);
-        }
+        r.error = REQ_EINTERNAL;
+        r.message = "cmg: unknown error";
+      }
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
       }
       r.finished = since(Clock::now());
       if (reserved) {

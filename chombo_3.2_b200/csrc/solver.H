@@ -7,6 +7,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <map>
 #include <memory>
 #include <tuple>
@@ -31,12 +32,17 @@ struct SolveParams {
   int pre = 4, post = 4, bottom = 4, numMG = 1, iterMax = 100, imin = 5;
   double eps = 1e-10, hang = 1e-10, normThresh = 1e-30;
   int iterMin = -1;  // m_iterMin: iterate at least this often whatever the norms
+  // Checked on the host before the first iteration and after each one with
+  // the iterations done; a non-zero return ends the solve there and is kept
+  // in SolveResult::interrupted (cancellation and time limits of a server).
+  std::function<int(int)> interrupt;
 };
 
 struct SolveResult {
   int exitStatus = 0, iterations = 0;
   std::vector<double> history;  // composite max-norm residual, start of each iteration, then final
   bool diverged = false;        // a residual norm was NaN or infinite (the solve stopped there)
+  int interrupted = 0;          // the non-zero value SolveParams::interrupt returned, if it stopped the solve
 };
 
 // BiCGStab over the whole hierarchy preconditioned by AMR multigrid, as the

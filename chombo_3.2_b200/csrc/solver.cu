@@ -1436,7 +1436,8 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
   // and exit status are computed as for any other norm.
   bool finite = std::isfinite(rnorm);
   const bool graph = useGraphs_ && !profOn_;
-  while (finite && (goMin || (goIter && goRedu && goHang && goNorm))) {
+  if (p.interrupt) out.interrupted = p.interrupt(0);
+  while (finite && !out.interrupted && (goMin || (goIter && goRedu && goHang && goNorm))) {
     normLast = rnorm;
     if (graph) {
       cudaGraphExec_t exec = iterationGraph(mixed, ures, phi, rhs);
@@ -1454,6 +1455,7 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
     goHang = iter < p.imin || rnorm < (1 - p.hang) * normLast;
     goMin = iter < p.iterMin;
     finite = std::isfinite(rnorm);
+    if (p.interrupt) out.interrupted = p.interrupt(iter);
   }
   out.exitStatus = int(!goRedu) + int(!goIter) * 2 + int(!goHang) * 4 + int(!goNorm) * 8;
   out.iterations = iter;

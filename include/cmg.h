@@ -289,7 +289,8 @@ int cmg_synthetic_hierarchy_device(int n0, int nlevels, int max_box, int block_f
  * workers; each takes the next request in arrival order (released at its
  * arrival time when open_loop != 0, all at once otherwise), generates its
  * grids, waits until the device memory of the admitted hierarchies plus its
- * own estimate fits in hbm_budget bytes, builds the hierarchy on its own
+ * own estimate fits in hbm_budget bytes (a request whose estimate alone exceeds
+ * the budget fails with CMG_ENOMEM), builds the hierarchy on its own
  * stream, solves, reads phi back (hashed into phi_hash) and frees it.  The
  * solves of all admitted requests overlap on the device; requests share no
  * device data, so every result is the same alone and in the mix.  Times are
@@ -304,16 +305,32 @@ typedef struct cmg_request {
   cmg_solve_params params;
   int mixed, graphs;
   int device_tags; /* != 0: tag on the device (cmg_synthetic_hierarchy_device) */
+  double timeout;  /* seconds after arrival (after the start when open_loop == 0) to finish by; 0: none */
+  const volatile int* cancel; /* NULL, or a flag the caller may set from any thread to cancel the request */
+  /* Host-side fault injection (tests): a NaN in one cell of the finest
+   * right-hand side once the inputs are generated; cancellation after this
+   * many iterations (-1: never). */
+  int inject_nan_rhs, inject_cancel_after;
 } cmg_request;
 
 typedef struct cmg_request_result {
-  int exit_status, iterations, error;
+  int exit_status, iterations;
+  int error; /* 0, or the request's status: CMG_EINVAL (invalid description), CMG_ENOMEM (the request alone
+                exceeds the budget, or an allocation failed), CMG_EDIVERGED (a residual norm became NaN or
+                infinite), CMG_ETIMEOUT, CMG_ECANCELLED, CMG_ECUDA / CMG_EINTERNAL; see message */
   double admitted, started, solved, finished, setup_seconds, solve_seconds, r0, rfinal;
   double grid_seconds, build_seconds, fill_seconds; /* parts of setup_seconds */
   int64_t cells;
   uint64_t device_bytes, phi_hash;
+  uint64_t estimate_bytes; /* the admission estimate of the request's device memory */
+  char message[160];       /* empty, or what went wrong */
 } cmg_request_result;
 
+/* A failing request ends alone: it releases its memory and admission, and
+ * every other request runs as if it had not been there.  Cancellation and the
+ * time limit are looked at while a request waits for admission and between
+ * its solver iterations.  The call itself fails only on invalid arguments
+ * (null arrays, max_inflight < 1, a non-positive budget). */
 int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_inflight, int open_loop,
               cmg_request_result* out, double* wall_seconds);
 

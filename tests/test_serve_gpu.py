@@ -4,6 +4,8 @@ Every result must be the same alone and in the mix -- bit-identical phi
 (hash of every valid cell on every level), iteration count and final
 residual -- and a served request must reproduce the reference solve of the
 same seeded problem."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -34,12 +36,80 @@ def test_each_result_is_the_same_alone_and_in_the_mix(cmg):
 
 
 @pytest.mark.gpu
-def test_tight_budget_admits_one_at_a_time(cmg):
-    res, _ = cmg.serve(MIX[:3], hbm_budget=1.0, max_inflight=3, open_loop=False)
-    spans = sorted((r["admitted"], r["finished"]) for r in res)
-    for (a0, f0), (a1, _) in zip(spans, spans[1:]):
-        assert a1 >= f0 - 1e-3  # the next admission waits for the previous release
-    assert all(r["error"] == 0 and r["exit_status"] & 1 for r in res)
+def test_admission_keeps_the_budget(cmg):
+    """A budget that fits the largest request alone: the admitted estimates never add up to more than the
+    budget at any moment (a request waits for earlier ones to release theirs), and all finish."""
+    alone = [cmg.serve([r], max_inflight=1, open_loop=False)[0][0] for r in MIX[:4]]
+    est = [a["estimate_bytes"] for a in alone]
+    budget = float(max(est))
+    res, _ = cmg.serve(MIX[:4], hbm_budget=budget, max_inflight=4, open_loop=False)
+    assert all(r["error"] == 0 and r["exit_status"] & 1 for r in res), res
+    events = sorted([(r["admitted"], e) for r, e in zip(res, est)] + [(r["finished"], -e) for r, e in zip(res, est)],
+                    key=lambda t: (t[0], t[1]))
+    held = 0
+    for _, d in events:
+        held += d
+        assert held <= budget + 1, (held, budget)
+
+
+@pytest.mark.gpu
+def test_failing_requests_leave_the_others_unchanged(cmg):
+    """Host fault injection in the request stream: a NaN in a right-hand side (the solve stops with a non-finite
+    norm), an invalid description, a request larger than the whole memory budget, one cancelled before it
+    starts, one cancelled after two iterations, one whose time limit has passed.  Each fails with its own
+    status and a message; every good request in the same run gets the bit-identical result it gets alone."""
+    good = MIX[:4]
+    alone = [cmg.serve([r], max_inflight=1, open_loop=False)[0][0] for r in good]
+    budget = float(sum(a["estimate_bytes"] for a in alone)) * 1.5
+    cancelled = ctypes.c_int(1)
+    bad = [
+        (dict(good[0], inject_nan_rhs=True), cmg.CMG_EDIVERGED),
+        (dict(good[1], n0=30, block_factor=8), cmg.CMG_EINVAL),
+        (dict(n0=256, levels=3, max_box=32, op=1, alpha=1.0, beta=-1.0, seed=7, mixed=True), cmg.CMG_ENOMEM),
+        (dict(good[2], cancel=cancelled), cmg.CMG_ECANCELLED),
+        (dict(good[3], inject_cancel_after=2), cmg.CMG_ECANCELLED),
+        (dict(good[0], timeout=1e-9), cmg.CMG_ETIMEOUT),
+    ]
+    reqs = []
+    for i in range(max(len(good), len(bad))):
+        if i < len(bad):
+            reqs.append(bad[i][0])
+        if i < len(good):
+            reqs.append(good[i])
+    res, _ = cmg.serve(reqs, hbm_budget=budget, max_inflight=5, open_loop=False)
+    k = 0
+    for i in range(max(len(good), len(bad))):
+        if i < len(bad):
+            r, code = res[k], bad[i][1]
+            assert r["error"] == code, (i, r)
+            assert r["message"], r
+            if code == cmg.CMG_EDIVERGED:
+                assert not np.isfinite(r["rfinal"]), r
+            if i == 4:
+                assert r["iterations"] == 2, r
+            k += 1
+        if i < len(good):
+            r, a = res[k], alone[i]
+            assert r["error"] == 0, r
+            assert r["phi_hash"] == a["phi_hash"] and r["iterations"] == a["iterations"], (r, a)
+            k += 1
+
+
+@pytest.mark.gpu
+def test_nan_right_hand_side_reports_divergence(cmg):
+    """cmg_solve on a right-hand side holding a NaN: the max norm propagates the NaN (it is not dropped as a
+    max over doubles would), the solve stops with CMG_EDIVERGED and writes its outputs."""
+    meta, _ = golden("vc_3lev_16")
+    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+    h.fill_synthetic(meta["seed"])
+    rhs = h.get_rhs(2)
+    rhs[len(rhs) // 2] = np.nan
+    h.set_rhs(2, rhs)
+    assert np.isnan(h.residual_norm())
+    out = h.solve(cmg.solve_params())
+    assert out["diverged"] and out["iterations"] == 0
+    assert np.isnan(out["history"][0])
+    h.close()
 
 
 @pytest.mark.gpu

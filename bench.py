@@ -30,6 +30,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 ORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle")
 MLORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle_mlbicgstab")
 FIORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle_fineinterp")
+OMPORACLE = os.path.join(ROOT, "oracle", "_ref", "omp", "cmg_oracle")
 PROFILE_CLASSES = ["relax_finest", "residual_op", "ghost_fill", "bottom", "relax_other"]
 METRIC = "Poisson solves/s & p50/p99 latency at 1e-10 rel. residual; V-cycle HBM GB/s"
 WORKLOADS = {
@@ -205,6 +206,39 @@ def cpu_reference(meta, processes, repeats):
         per_step.append(len(ts) / max(ts) if ts else float("nan"))
     return {"per_step": per_step, "n_iter": n_iter, "processes": processes,
             "wall_step": [max(o[k]["seconds"] for o in outs if len(o) > k) for k in range(repeats)]}
+
+
+def cpu_reference_openmp(meta, threads):
+    """One reference solve at a time on all host cores: the oracle built with
+    the reference's OpenMP box loops (oracle/_ref/omp), OMP_NUM_THREADS =
+    threads, capped at 2 V-cycles and extrapolated like cpu_reference.  The
+    reference's own OpenMP code is only valid on single-level hierarchies:
+    LevelFluxRegister::reflux adds the fine registers through copyTo with an
+    AddOp that keeps LDOperator's threadSafe() == true, so the copy's motion
+    items run in parallel and items writing the same coarse cells lose
+    updates; multi-level solves then stagnate (measured with 8 threads: exit
+    status 4 instead of 1).  The timing is reported either way, with that
+    outcome stated."""
+    if not os.path.exists(OMPORACLE):
+        return None
+    boxfile = write_boxfile(meta)
+    n_iter = len(meta["residual_history"]) - 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    args = oracle_args(meta, boxfile, 2, 1)
+    args[0] = OMPORACLE
+    out = subprocess.run(args, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, env=env).stdout
+    reps = parse_repeats(out)
+    if not reps:
+        return None
+    solve_s = extrapolate(reps[0], n_iter)
+    single = len(meta["boxes"]) == 1
+    return {"value": 1.0 / solve_s, "unit": "solves/s", "cores": threads, "kind": "reference",
+            "sample": f"one reference solve with OMP_NUM_THREADS={threads} (the reference's OpenMP box loops), "
+                      f"capped at 2 of {n_iter} V-cycles, extrapolated to the full solve",
+            "valid": single,
+            "note": "single-level: the reference's OpenMP path converges as the serial one" if single else
+                    "multi-level: the reference's OpenMP reflux (LevelFluxRegister AddOp copy in parallel) loses "
+                    "flux-register updates and the solve stagnates, so this is the speed of an invalid solve"}
 
 
 def cpu_reference_bicgstab(meta, wl, processes):
@@ -796,10 +830,26 @@ def main():
                 "peak_kind": peak_kind, "launches": int(n_fine),
                 "avg_launch_us": 1000.0 * ms_fine / max(n_fine, 1),
                 "algorithmic_bytes_per_launch": bytes_fine / max(n_fine, 1)}
-    breakdown = {name: {"launches": int(v[0]) // n_prof, "ms_per_solve": v[1] / n_prof,
-                        "share": v[1] / prof_ms if prof_ms > 0 else 0.0,
-                        "gbs": (v[2] / 1e9) / (v[1] / 1e3) if v[1] > 0 and v[2] > 0 else None}
-                 for name, v in classes.items()}
+    breakdown = {}
+    for name, v in classes.items():
+        gbs = (v[2] / 1e9) / (v[1] / 1e3) if v[1] > 0 and v[2] > 0 else None
+        breakdown[name] = {"launches": int(v[0]) // n_prof, "ms_per_solve": v[1] / n_prof,
+                           "share": v[1] / prof_ms if prof_ms > 0 else 0.0, "gbs": gbs,
+                           "frac": gbs / peak if gbs else None}
+    # The whole V-cycle: algorithmic bytes of one V-cycle (cmg_vcycle_bytes:
+    # every relaxation colour pass, residual and operator pass of every level
+    # and multigrid depth, each array read once and each output written once)
+    # over the solve time per V-cycle (the solve's initial residual and norm
+    # reads included, so this is a lower bound on the V-cycle's own rate).
+    vbytes = None if bicg else h.vcycle_bytes(params)
+    vcycle = None
+    if vbytes:
+        vms = (total_ms / args.steps) / max(n_iter, 1)
+        vgbs = (vbytes / 1e9) / (vms / 1e3)
+        relaxed = sum(ncells[:-1]) * (params.pre + params.post) + ncells[-1] * (params.pre + params.post)
+        vcycle = {"algorithmic_bytes": vbytes, "ms": vms, "gbs": vgbs, "frac": vgbs / peak, "peak_kind": peak_kind,
+                  "cell_updates_per_s": relaxed / (vms / 1e3),
+                  "note": "solve time per V-cycle (initial residual and norm read-backs included)"}
     accuracy = None
     if mixed:
         # L-infinity deviation of the mixed-precision phi from the FP64
@@ -839,6 +889,9 @@ def main():
             cpu = {"value": res["per_step"][0], "unit": "solves/s", "cores": 1, "kind": "reference",
                    "sample": f"one single-thread reference solve capped at 2 of {res['n_iter']} V-cycles, "
                              f"extrapolated to the full solve (set-up + first + (n-1) x later V-cycle)"}
+    cpu_all = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not bicg:
+        cpu_all = cpu_reference_openmp(meta, os.cpu_count() or 1)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -851,7 +904,8 @@ def main():
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                        "cuda_graphs": not args.no_graphs},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-            "roofline": roofline, "breakdown": breakdown, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "roofline": roofline, "vcycle": vcycle, "breakdown": breakdown, "cpu_baseline": cpu,
+            "cpu_baseline_all_cores": cpu_all, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches, "launch_index_at_timed_start": launches0,
             "relax_variants": h.relax_variants(),
         }

@@ -696,7 +696,7 @@ def main():
     ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS) + ["config3", "config4", "fineinterp"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
-    ap.add_argument("--relax-mode", type=int, default=0, choices=[0, 1, 2],
+    ap.add_argument("--relax-mode", type=int, default=0, choices=[0, 1, 2, 3],
                     help="relaxation variant: 0 autotuned per level, 1 ghost fills, 2 in-pass ghosts")
     ap.add_argument("--batch", type=int, default=512, help="config3: number of hierarchies")
     ap.add_argument("--host-fill", action="store_true", help="config3: generate the inputs on the host")

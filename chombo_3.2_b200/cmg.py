@@ -371,7 +371,7 @@ class Hierarchy:
         a = (ctypes.c_float * max(n.value, 1))()
         b = (ctypes.c_float * max(n.value, 1))()
         _check(lib().cmg_relax_variants(self.h, v, a, b, n.value, ctypes.byref(n)))
-        names = {0: "fill", 1: "in-pass ghosts", 2: "one-block sweeps"}
+        names = {0: "fill", 1: "in-pass ghosts", 2: "one-block sweeps", 3: "fused sweeps"}
         return [{"variant": names.get(v[i], v[i]), "ms_fill": a[i], "ms_best_other": b[i]} for i in range(n.value)]
 
     def use_graphs(self, on=True):

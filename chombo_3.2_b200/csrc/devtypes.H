@@ -124,6 +124,15 @@ struct FaceRule {
   int src, kind;
 };
 
+// A colour-1 cell of a box that lies on a face whose ghost is an exchange
+// copy from another box (FR_COPY rule): the fused red-black sweep (one launch
+// per sweep, every box marching through its z slabs) cannot update it before
+// every box has finished its colour-0 cells, so a second launch does, from
+// this list.  q: the cell's index in its box, x fastest.
+struct DeferredCell {
+  int box, q;
+};
+
 // Device form of a ghost task: the task plus copies of its destination and
 // source box descriptors, so that a thread reaches its data after a single
 // table load.

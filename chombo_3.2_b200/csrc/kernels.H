@@ -28,6 +28,10 @@ struct LevelDev {
   int gcStart[2] = {0, 0}, gcExch[2] = {0, 0}, gcCF[2] = {0, 0};
   const FaceRule* faceRules = nullptr;    // LevelPlan::faceRules / faceOff
   const int* faceOff = nullptr;
+  const DeferredCell* deferred = nullptr; // LevelPlan::deferred
+  int nDeferred = 0;
+  const GhostCell* chGhost[2] = {nullptr, nullptr};  // LevelPlan::chunkGhost
+  const int* chGhostStart[2] = {nullptr, nullptr};
   const GhostTaskDev* zero = nullptr;
   int nZero = 0;
   const int* zeroStart = nullptr;
@@ -87,13 +91,23 @@ void scaleField(double* x, double scale, int64_t n, cudaStream_t s);
 // out[b] = sum of x*y over the valid cells of box b, accumulated in the
 // reference's order (FArrayBox::dotProduct: k, j, i with i fastest).
 void boxDots(const LevelDev& L, const double* x, const double* y, double* out, cudaStream_t s);
-// One colour pass of levelGSRB.  inlineGhosts: the neighbours beyond each
-// box come from the level's face-ghost rules, so no ghost fill is needed
-// before the pass; otherwise they are read from ghost cells filled by
-// ghostFill(withCF) just before.
+// One colour pass of levelGSRB.  inlineGhosts: every block first writes the
+// face ghosts its own cells read (LevelDev::chGhost, the entries of the fill
+// that would precede the pass), so no ghost fill is needed before the pass;
+// otherwise they are read from ghost cells filled by ghostFill(withCF) just
+// before.
 template <class T>
 void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, cudaStream_t s,
           bool inlineGhosts = false);
+// One whole red-black sweep (both colours) in two launches: every box
+// marches through its z slabs updating the colour-0 cells of slab k and then
+// the colour-1 cells of slab k - 1, each face coefficient and neighbour read
+// once for both colours; the face ghosts come from the level's fill rules
+// (no fill).  The colour-1 cells on exchange faces need other boxes' new
+// colour-0 values and are updated by the second launch (LevelDev::deferred).
+// Same values as gsrb() for colour 0 then colour 1.
+template <class T>
+void gsrbSweepFused(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s);
 // nsweeps red-black sweeps of a small level in a single one-block launch
 // (in-pass ghosts, block barriers between colour passes); same results.
 template <class T>

@@ -225,38 +225,54 @@ __device__ __forceinline__ T ghostValue(const FaceRule* __restrict__ rules, cons
   return T(gc.c1) * pc + T(gc.c2) * phi[r.src];
 }
 
+// Value of one ghost-fill entry (GhostCell) from the current field: the
+// arithmetic of k_ghostcells.
+template <class T>
+__device__ __forceinline__ T ghostCellValue(const GhostCell& g, const T* f, const GhostCoef& gc) {
+  const T v1 = f[g.s1];
+  if (g.s2 == -1) return v1;
+  if (g.s2 == -2) {
+    T zero = T(0);
+    return T(2) * zero - v1;
+  }
+  if (g.s2 == -3) return T(gc.flin) * v1;
+  return T(gc.c1) * v1 + T(gc.c2) * f[g.s2];
+}
+
 // GSRBLAPLACIAN / GSRBHELMHOLTZ (AMRPoissonOpF.ChF:51-198) and
-// GSRBHELMHOLTZVC3D (VCAMRPoissonOpF.ChF:57-125), one colour.  With face
-// rules, the neighbours beyond the box are evaluated from the rules instead
-// of read from ghost cells filled before the pass (same values, no fill).
-template <class T, int VC, bool INL>
+// GSRBHELMHOLTZVC3D (VCAMRPoissonOpF.ChF:57-125), one colour.  With PRE, the
+// block first writes the face ghosts its own cells read (the chunk's entries
+// of the fill that would precede the pass, pre[preStart[chunk] ..
+// preStart[chunk + 1])).  Those ghosts belong to the other colour, so no other
+// block writes their sources during the pass, and each is read only by the
+// one valid cell next to it, updated by this block after the barrier: the
+// values are the fill's.
+template <class T, int VC, bool PRE>
 __global__ void k_gsrb(const BoxDesc* boxes, const Chunk* chunks, T* phi, const T* rhs, int color, Scal sc,
                        const T* a, const T* b0, const T* b1, const T* b2, const T* lam,
-                       const FaceRule* __restrict__ rules, const int* __restrict__ faceOff, GhostCoef gc) {
+                       const GhostCell* __restrict__ pre, const int* __restrict__ preStart, GhostCoef gc) {
   Chunk ch = chunks[blockIdx.x];
   const BoxDesc bd = boxes[ch.box];
+  if (PRE) {
+    const int g1 = preStart[blockIdx.x + 1];
+    for (int q = preStart[blockIdx.x] + threadIdx.x; q < g1; q += blockDim.x) {
+      const GhostCell g = pre[q];
+      phi[g.dst] = ghostCellValue(g, phi, gc);
+    }
+    __syncthreads();
+  }
   int i, j, k;
   if (!colorCell(bd, ch.start + threadIdx.x, color, i, j, k)) return;
   const Stencil st = stencil(bd, i, j, k);
   const int64_t c = st.c;
   const T pc = phi[c];
   T v[6];
-  if (INL) {
-    const int b = ch.box;
-    v[0] = i == bd.hi[0] ? ghostValue(rules, faceOff, bd, b, 0, 1, i, j, k, pc, phi, gc) : phi[st.xp];
-    v[1] = i == bd.lo[0] ? ghostValue(rules, faceOff, bd, b, 0, -1, i, j, k, pc, phi, gc) : phi[st.xm];
-    v[2] = j == bd.hi[1] ? ghostValue(rules, faceOff, bd, b, 1, 1, i, j, k, pc, phi, gc) : phi[st.yp];
-    v[3] = j == bd.lo[1] ? ghostValue(rules, faceOff, bd, b, 1, -1, i, j, k, pc, phi, gc) : phi[st.ym];
-    v[4] = k == bd.hi[2] ? ghostValue(rules, faceOff, bd, b, 2, 1, i, j, k, pc, phi, gc) : phi[st.zp];
-    v[5] = k == bd.lo[2] ? ghostValue(rules, faceOff, bd, b, 2, -1, i, j, k, pc, phi, gc) : phi[st.zm];
-  } else {
-    v[0] = phi[st.xp];
-    v[1] = phi[st.xm];
-    v[2] = phi[st.yp];
-    v[3] = phi[st.ym];
-    v[4] = phi[st.zp];
-    v[5] = phi[st.zm];
-  }
+  v[0] = phi[st.xp];
+  v[1] = phi[st.xm];
+  v[2] = phi[st.yp];
+  v[3] = phi[st.ym];
+  v[4] = phi[st.zp];
+  v[5] = phi[st.zm];
   const T dxinv = T(sc.dxinv);
   if (VC) {
     T div = b0[st.xp] * (v[0] - pc) - b0[c] * (pc - v[1]) + b1[st.yp] * (v[2] - pc) - b1[c] * (pc - v[3]) +
@@ -320,6 +336,129 @@ __global__ void __launch_bounds__(1024) k_relax_block(const BoxDesc* boxes, cons
       }
       __syncthreads();
     }
+}
+
+// Neighbour value across a box face from its fill rule (the value the ghost
+// fill before the colour pass would have written, as in ghostValue).
+template <class T>
+__device__ __forceinline__ T ruleValue(const FaceRule& r, T pc, const T* phi, const GhostCoef& gc) {
+  if (r.kind == FR_COPY || r.kind == FR_FAB) return phi[r.src];
+  if (r.kind == FR_BC) {
+    T zero = T(0);
+    return T(2) * zero - pc;
+  }
+  if (r.kind == FR_CFLIN) return T(gc.flin) * pc;
+  return T(gc.c1) * pc + T(gc.c2) * phi[r.src];
+}
+
+// One cell of a red-black sweep with the neighbours beyond its box taken from
+// the face rules: the arithmetic of k_gsrb (GSRBHELMHOLTZVC3D,
+// GSRBLAPLACIAN, GSRBHELMHOLTZ).  With deferCopy, a cell with an exchange-copy
+// face ghost is left alone (its source box may not be done yet).
+template <class T, int VC>
+__device__ __forceinline__ void gsrbCell(const BoxDesc& bd, int b, int i, int j, int k, T* phi, const T* rhs,
+                                         const Scal& sc, const T* a, const T* b0, const T* b1, const T* b2,
+                                         const T* lam, const FaceRule* __restrict__ rules,
+                                         const int* __restrict__ faceOff, const GhostCoef& gc, bool deferCopy) {
+  const Stencil st = stencil(bd, i, j, k);
+  const int64_t c = st.c;
+  const int p[3] = {i, j, k};
+  const int nb[6] = {st.xp, st.xm, st.yp, st.ym, st.zp, st.zm};
+  FaceRule fr[6];
+  bool onFace[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const int d = f >> 1, side = (f & 1) ? 0 : 1;  // +d then -d
+    onFace[f] = side ? p[d] == bd.hi[d] : p[d] == bd.lo[d];
+    if (onFace[f]) {
+      const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+      fr[f] = rules[faceOff[6 * b + 2 * d + side] + (p[t0] - bd.lo[t0]) + (bd.hi[t0] - bd.lo[t0] + 1) * (p[t1] - bd.lo[t1])];
+      if (deferCopy && fr[f].kind == FR_COPY) return;
+    }
+  }
+  const T pc = phi[c];
+  T v[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) v[f] = onFace[f] ? ruleValue(fr[f], pc, phi, gc) : phi[nb[f]];
+  const T dxinv = T(sc.dxinv);
+  if (VC) {
+    T div = b0[st.xp] * (v[0] - pc) - b0[c] * (pc - v[1]) + b1[st.yp] * (v[2] - pc) - b1[c] * (pc - v[3]) +
+            b2[st.zp] * (v[4] - pc) - b2[c] * (pc - v[5]);
+    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * div * dxinv;
+    phi[c] = pc - lam[c] * (lofphi - rhs[c]);
+  } else if (sc.laplacian) {
+    T lphi = (v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) * dxinv;
+    phi[c] = T(sc.lambda) * (rhs[c] - lphi);
+  } else {
+    T lphi = ((v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) - T(2.0) * T(3) * pc) * dxinv;
+    T helmop = T(sc.alpha) * pc + T(sc.beta) * lphi;
+    phi[c] = pc + T(sc.lambda) * (helmop - rhs[c]);
+  }
+}
+
+// The fused sweep (gsrbSweepFused), first launch: one block per box marching
+// through its z slabs.  Step s updates the colour-0 cells of slab s, then
+// (after a barrier) the colour-1 cells of slab s - 1 except those with an
+// exchange-copy face ghost.  Every read is the value the reference's two
+// passes read: a colour-0 cell sees colour-1 neighbours not yet updated (slab
+// s - 1 is updated after the barrier, slabs s and s + 1 in later steps, the
+// other boxes' face cells only in the second launch), and a colour-1 cell sees
+// the new colour-0 values of slabs s - 2 .. s of its own box; its coarse-fine
+// and boundary ghosts use only its own box.  Part 2 of a step and part 1 of
+// the next touch disjoint cells (slab s - 1 colour 1 against slab s + 1 colour
+// 0 and its colour-1 neighbours in slabs s .. s + 2), so one barrier per step
+// suffices.  The face coefficients and phi of a slab are read by both colours
+// one step apart, from cache.
+template <class T, int VC>
+__global__ void __launch_bounds__(256) k_gsrb_march(const BoxDesc* boxes, T* phi, const T* rhs, Scal sc,
+                                                    const T* a, const T* b0, const T* b1, const T* b2,
+                                                    const T* lam, const FaceRule* __restrict__ rules,
+                                                    const int* __restrict__ faceOff, GhostCoef gc) {
+  const int b = blockIdx.x;
+  const BoxDesc bd = boxes[b];
+  const int nx = bd.hi[0] - bd.lo[0] + 1, ny = bd.hi[1] - bd.lo[1] + 1, nz = bd.hi[2] - bd.lo[2] + 1;
+  const int half = (nx + 1) / 2;
+  const int perSlab = half * ny;
+  for (int s = 0; s <= nz; ++s) {
+    if (s < nz) {
+      const int k = bd.lo[2] + s;
+      for (int q = threadIdx.x; q < perSlab; q += blockDim.x) {
+        const int r = fastDiv(q, half, bd.mHalf);
+        const int j = bd.lo[1] + r;
+        const int i = bd.lo[0] + ((bd.lo[0] + j + k) & 1) + 2 * (q - r * half);
+        if (i <= bd.hi[0]) gsrbCell<T, VC>(bd, b, i, j, k, phi, rhs, sc, a, b0, b1, b2, lam, rules, faceOff, gc, false);
+      }
+    }
+    __syncthreads();
+    if (s > 0) {
+      const int k = bd.lo[2] + s - 1;
+      for (int q = threadIdx.x; q < perSlab; q += blockDim.x) {
+        const int r = fastDiv(q, half, bd.mHalf);
+        const int j = bd.lo[1] + r;
+        const int i = bd.lo[0] + ((bd.lo[0] + j + k + 1) & 1) + 2 * (q - r * half);
+        if (i <= bd.hi[0]) gsrbCell<T, VC>(bd, b, i, j, k, phi, rhs, sc, a, b0, b1, b2, lam, rules, faceOff, gc, true);
+      }
+    }
+  }
+}
+
+// The fused sweep, second launch: the colour-1 cells with an exchange-copy
+// face ghost, now that every box has its new colour-0 values.
+template <class T, int VC>
+__global__ void __launch_bounds__(256) k_gsrb_deferred(const BoxDesc* boxes, const DeferredCell* cells, int n,
+                                                       T* phi, const T* rhs, Scal sc, const T* a, const T* b0,
+                                                       const T* b1, const T* b2, const T* lam,
+                                                       const FaceRule* __restrict__ rules,
+                                                       const int* __restrict__ faceOff, GhostCoef gc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const DeferredCell dc = cells[t];
+  const BoxDesc bd = boxes[dc.box];
+  const int nx = bd.hi[0] - bd.lo[0] + 1, ny = bd.hi[1] - bd.lo[1] + 1;
+  const int r = fastDiv(dc.q, nx, bd.mNx);
+  const int kk = fastDiv(r, ny, bd.mNy);
+  gsrbCell<T, VC>(bd, dc.box, bd.lo[0] + (dc.q - r * nx), bd.lo[1] + (r - kk * ny), bd.lo[2] + kk, phi, rhs, sc, a,
+                  b0, b1, b2, lam, rules, faceOff, gc, false);
 }
 
 // OPERATORLAPRES / OPERATORLAP (AMRPoissonOpF.ChF:287-377) and
@@ -1107,10 +1246,9 @@ void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, 
   Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
   const double dx = L.dx, dxc = L.dxCrse;
   GhostCoef gc{2 * (dxc - dx) / (dxc + dx), -(dxc - dx) / (dxc + 3 * dx), 1 - 2 * dx / (dx + dxc)};
-  const FaceRule* rules = L.faceRules;
   auto launch = [&](auto kern, const T* a, const T* b0, const T* b1, const T* b2, const T* lam) {
-    kern<<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, a, b0, b1, b2, lam, rules, L.faceOff,
-                             gc);
+    kern<<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, a, b0, b1, b2, lam,
+                             L.chGhost[color], L.chGhostStart[color], gc);
   };
   if (c.vc) {
     if (inlineGhosts)
@@ -1124,6 +1262,34 @@ void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, 
       launch(k_gsrb<T, 0, false>, nullptr, nullptr, nullptr, nullptr, nullptr);
   }
   CMG_LAUNCHED("gsrb");
+}
+
+template <class T>
+void gsrbSweepFused(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s) {
+  if (L.nbox == 0) return;
+  Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
+  const double dx = L.dx, dxc = L.dxCrse;
+  GhostCoef gc{2 * (dxc - dx) / (dxc + dx), -(dxc - dx) / (dxc + 3 * dx), 1 - 2 * dx / (dx + dxc)};
+  const int nd = L.nDeferred, db = (nd + 255) / 256;
+  if (c.vc) {
+    k_gsrb_march<T, 1><<<L.nbox, 256, 0, s>>>(L.boxes, phi, rhs, sc, c.a, c.b[0], c.b[1], c.b[2], c.lambda,
+                                              L.faceRules, L.faceOff, gc);
+    CMG_LAUNCHED("gsrbMarch");
+    if (nd > 0) {
+      k_gsrb_deferred<T, 1><<<db, 256, 0, s>>>(L.boxes, L.deferred, nd, phi, rhs, sc, c.a, c.b[0], c.b[1], c.b[2],
+                                               c.lambda, L.faceRules, L.faceOff, gc);
+      CMG_LAUNCHED("gsrbDeferred");
+    }
+  } else {
+    k_gsrb_march<T, 0><<<L.nbox, 256, 0, s>>>(L.boxes, phi, rhs, sc, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                              L.faceRules, L.faceOff, gc);
+    CMG_LAUNCHED("gsrbMarch");
+    if (nd > 0) {
+      k_gsrb_deferred<T, 0><<<db, 256, 0, s>>>(L.boxes, L.deferred, nd, phi, rhs, sc, nullptr, nullptr, nullptr,
+                                               nullptr, nullptr, L.faceRules, L.faceOff, gc);
+      CMG_LAUNCHED("gsrbDeferred");
+    }
+  }
 }
 
 template <class T>
@@ -1428,6 +1594,7 @@ void averageCoefficients(const LevelDev& F, const LevelDev& C, int r, const doub
   template void zeroCovered<T>(const LevelDev&, T*, cudaStream_t);                                         \
   template void gsrb<T>(const LevelDev&, T*, const T*, const Coef<T>&, int, cudaStream_t, bool);           \
   template void relaxBlock<T>(const LevelDev&, T*, const T*, const Coef<T>&, int, cudaStream_t);              \
+  template void gsrbSweepFused<T>(const LevelDev&, T*, const T*, const Coef<T>&, cudaStream_t);            \
   template void residual<T>(const LevelDev&, T*, const T*, const T*, const Coef<T>&, cudaStream_t);        \
   template void applyOp<T>(const LevelDev&, T*, const T*, const Coef<T>&, cudaStream_t);                   \
   template void negAdd<T>(const LevelDev&, T*, const T*, const T*, cudaStream_t);                          \

@@ -39,6 +39,13 @@ struct LevelPlan {
   // directions in increasing order; faceOff[6*b + 2*d + (side > 0)].
   std::vector<FaceRule> faceRules;
   std::vector<int> faceOff;
+  // Colour-1 cells on exchange faces (DeferredCell), box by box, x fastest.
+  std::vector<DeferredCell> deferred;
+  // Face ghosts read by each chunk of a colour pass (chunksColor[c]): the
+  // fill entries of chunk q are chunkGhost[c][chunkGhostStart[c][q] ..
+  // chunkGhostStart[c][q + 1]).
+  std::vector<GhostCell> chunkGhost[2];
+  std::vector<int> chunkGhostStart[2];
   std::vector<GhostTask> zeroCovered;  // covered by the next finer level
   std::vector<int> zeroStart;          // cumulative cell counts of zeroCovered
   std::vector<int> zeroBlock;

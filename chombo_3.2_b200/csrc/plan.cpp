@@ -104,6 +104,9 @@ void parallelItems(size_t n, F fn) {
     if (e) std::rethrow_exception(e);
 }
 
+void buildDeferred(LevelPlan& L);
+void buildChunkGhosts(LevelPlan& L);
+
 // Rules of every face-ghost cell from the level's ghost tasks (the fill with
 // coarse-fine values that precedes each relaxation pass).
 void buildFaceRules(LevelPlan& L) {
@@ -162,6 +165,100 @@ void buildFaceRules(LevelPlan& L) {
           }
         }
   });
+}
+
+// The colour-1 cells ((i+j+k) odd) with at least one face ghost filled by an
+// exchange copy, per box in x-fastest order (DeferredCell).
+void buildDeferred(LevelPlan& L) {
+  std::vector<std::vector<DeferredCell>> per(L.grids.size());
+  parallelItems(L.grids.size(), [&](size_t b) {
+    const Box& bx = L.grids[b];
+    const int nx = bx.size(0), ny = bx.size(1);
+    auto copyFace = [&](int d, int s, const IV& p) {
+      const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+      const FaceRule& r = L.faceRules[L.faceOff[6 * b + 2 * d + s] + (p[t0] - bx.lo[t0]) +
+                                      bx.size(t0) * (p[t1] - bx.lo[t1])];
+      return r.kind == FR_COPY;
+    };
+    for (int k = bx.lo[2]; k <= bx.hi[2]; ++k)
+      for (int j = bx.lo[1]; j <= bx.hi[1]; ++j)
+        for (int i = bx.lo[0]; i <= bx.hi[0]; ++i) {
+          if (((i + j + k) & 1) == 0) continue;
+          const IV p(i, j, k);
+          bool def = false;
+          for (int d = 0; d < 3 && !def; ++d) {
+            if (p[d] == bx.lo[d] && copyFace(d, 0, p)) def = true;
+            if (p[d] == bx.hi[d] && copyFace(d, 1, p)) def = true;
+          }
+          if (def)
+            per[b].push_back(DeferredCell{(int)b, (i - bx.lo[0]) + nx * ((j - bx.lo[1]) + ny * (k - bx.lo[2]))});
+        }
+  });
+  L.deferred.clear();
+  for (auto& v : per) L.deferred.insert(L.deferred.end(), v.begin(), v.end());
+}
+
+// Per-chunk face ghosts of the colour passes: for colour c, the ghost cells
+// of parity 1 - c that the cells of each colour-c chunk read, each as the
+// ghost-fill entry (GhostCell) of its face rule, grouped by chunk.  Every face
+// ghost is read by exactly one cell (the valid cell next to it), so the
+// groups are disjoint; FR_FAB faces have no fill and no entry.
+void buildChunkGhosts(LevelPlan& L) {
+  const size_t nb = L.grids.size();
+  for (int c = 0; c < 2; ++c) {
+    std::vector<std::vector<std::pair<int, GhostCell>>> per(nb);
+    parallelItems(nb, [&](size_t b) {
+      const Box& bx = L.grids[b];
+      const int half = (bx.size(0) + 1) / 2, ny = bx.size(1);
+      std::vector<std::pair<int, GhostCell>>& out = per[b];
+      for (int d = 0; d < 3; ++d) {
+        const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
+        for (int s = 0; s < 2; ++s) {
+          const FaceRule* r = &L.faceRules[L.faceOff[6 * b + 2 * d + s]];
+          for (int v = bx.lo[t1], q = 0; v <= bx.hi[t1]; ++v)
+            for (int u = bx.lo[t0]; u <= bx.hi[t0]; ++u, ++q) {
+              IV p;
+              p[d] = s ? bx.hi[d] : bx.lo[d];
+              p[t0] = u;
+              p[t1] = v;
+              if (((p[0] + p[1] + p[2]) & 1) != c || r[q].kind == FR_FAB) continue;
+              IV g = p;
+              g[d] += s ? 1 : -1;
+              const int dst = (int)cellOf(L, (int)b, g), adj = (int)cellOf(L, (int)b, p);
+              GhostCell e{dst, 0, 0};
+              switch (r[q].kind) {
+                case FR_COPY: e.s1 = r[q].src, e.s2 = -1; break;
+                case FR_BC: e.s1 = adj, e.s2 = -2; break;
+                case FR_CFLIN: e.s1 = adj, e.s2 = -3; break;
+                default: e.s1 = adj, e.s2 = r[q].src; break;  // FR_CFQUAD
+              }
+              const int par = (bx.lo[0] + p[1] + p[2] + c) & 1;
+              const int idx = ((p[1] - bx.lo[1]) + ny * (p[2] - bx.lo[2])) * half + (p[0] - bx.lo[0] - par) / 2;
+              out.push_back({idx, e});
+            }
+        }
+      }
+      std::stable_sort(out.begin(), out.end(),
+                       [](const std::pair<int, GhostCell>& x, const std::pair<int, GhostCell>& y) {
+                         return x.first / CHUNK < y.first / CHUNK;
+                       });
+    });
+    std::vector<GhostCell>& cells = L.chunkGhost[c];
+    std::vector<int>& start = L.chunkGhostStart[c];
+    cells.clear();
+    start.assign(1, 0);
+    for (size_t b = 0; b < nb; ++b) {
+      const Box& bx = L.grids[b];
+      const int64_t n = (int64_t)bx.size(1) * bx.size(2) * ((bx.size(0) + 1) / 2);
+      size_t at = 0;
+      for (int64_t ch = 0; ch * CHUNK < n; ++ch) {
+        while (at < per[b].size() && per[b][at].first / CHUNK == ch) cells.push_back(per[b][at++].second);
+        start.push_back((int)cells.size());
+      }
+      if (at != per[b].size()) throw std::logic_error("cmg: chunk ghost outside its box");
+    }
+    if (start.size() != L.chunksColor[c].size() + 1) throw std::logic_error("cmg: chunk ghost count mismatch");
+  }
 }
 
 std::vector<int> blockTasks(const std::vector<int>& start) {
@@ -270,6 +367,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
   }
   L.ghostBlock = blockTasks(L.ghostStart);
   buildFaceRules(L);
+  buildDeferred(L);
   if (L.nelem >= ((int64_t)1 << 31)) throw std::runtime_error("cmg: level too large for 32-bit ghost indices");
   // Flat lists: per parity the exchange and boundary tasks, then the
   // coarse-fine ones, each task's cells of that parity in k, j, i order.
@@ -345,6 +443,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     chunkCounts(L.chunksColor[0], (int)b, rows * half);
     chunkCounts(L.chunksColor[1], (int)b, rows * half);
   }
+  buildChunkGhosts(L);
 }
 
 int ownerOf(const LevelPlan& L, const IV& p) {

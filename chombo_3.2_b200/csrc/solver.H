@@ -240,6 +240,10 @@ class Solver {
                   int variant);
   // Levels up to this many cells may relax all sweeps in one one-block launch.
   static constexpr double kBlockRelaxMaxCells = 32768;
+  // Relaxation variants: 0 ghost fill before each colour pass, 1 face ghosts
+  // in the pass, 2 every sweep in one one-block launch, 3 fused sweeps
+  // (gsrbSweepFused: both colours per launch, boxes marching in z).
+  static constexpr int kRelaxVariants = 4;
   template <class T> void fill(const LevelDev& L, T* f, bool withCF, int par = -1);
   template <class T>
   void amrResidualLevel(int ilev, int lmax, T* const* res, T* const* phi, T* const* rhs);
@@ -273,11 +277,11 @@ class Solver {
   std::map<cudaGraphExec_t, long long> graphLaunches_;  // kernel launches per replay
   bool useGraphs_ = false;
   // Relaxation variant per AMR level / MG depth: ghost fill before each
-  // colour pass (0), face ghosts evaluated inside the pass (1), or every
-  // sweep in one one-block launch with in-pass ghosts (2).
+  // colour pass (0), face ghosts evaluated inside the pass (1), every sweep
+  // in one one-block launch with in-pass ghosts (2), or fused sweeps (3).
   std::vector<char> inlineA_, inlineM_;
   bool tuned_ = false;
-  int relaxMode_ = 0;  // 0: autotuned, 1: always fills, 2: always inline
+  int relaxMode_ = 0;  // 0: autotuned, 1: always fills, 2: always inline, 3: always fused
   std::vector<std::pair<float, float>> tuneMs_;
   void tuneRelaxation();
   double* hostScalars_ = nullptr;  // pinned: [0] norm read back, [1] bottom metric

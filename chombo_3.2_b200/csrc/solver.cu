@@ -157,6 +157,12 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
   d.gcells = upload(bufs_, p.gcells, s_);
   d.faceRules = upload(bufs_, p.faceRules, s_);
   d.faceOff = upload(bufs_, p.faceOff, s_);
+  d.deferred = upload(bufs_, p.deferred, s_);
+  for (int c = 0; c < 2; ++c) {
+    d.chGhost[c] = upload(bufs_, p.chunkGhost[c], s_);
+    d.chGhostStart[c] = upload(bufs_, p.chunkGhostStart[c], s_);
+  }
+  d.nDeferred = (int)p.deferred.size();
   for (int c = 0; c < 2; ++c) {
     d.gcStart[c] = p.gcStart[c];
     d.gcExch[c] = p.gcExch[c];
@@ -667,6 +673,13 @@ void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* ph
     timed(cls, bytes * 2 * n, [&]() { relaxBlock(L, phi, rhs, c, n, s_); });
     return;
   }
+  if (variant == 3) {
+    // Fused sweep: phi read and written once, rhs, a, lambda and the three
+    // face arrays read once per sweep (8 words VC, 3 constant coefficients).
+    const double sweepBytes = cells * sizeof(T) * (c.vc ? 8.0 : 3.0);
+    for (int it = 0; it < n; ++it) timed(cls, sweepBytes, [&]() { gsrbSweepFused(L, phi, rhs, c, s_); });
+    return;
+  }
   const bool inl = variant == 1;
   for (int it = 0; it < n; ++it)
     for (int color = 0; color <= 1; ++color) {
@@ -697,8 +710,9 @@ void Solver::relaxMG(int d, T* phi, const T* rhs, int n) {
 void Solver::tuneRelaxation() {
   tuned_ = true;
   tuneMs_.clear();
-  inlineA_.assign(amr_.size(), relaxMode_ == 2 ? 1 : 0);
-  inlineM_.assign(mg_.size(), relaxMode_ == 2 ? 1 : 0);
+  const char forced = relaxMode_ == 2 ? 1 : relaxMode_ == 3 ? 3 : 0;
+  inlineA_.assign(amr_.size(), forced);
+  inlineM_.assign(mg_.size(), forced);
   if (relaxMode_ != 0) return;
   cudaEvent_t e[3];
   for (auto& x : e) ck(cudaEventCreate(&x), "event");
@@ -721,23 +735,23 @@ void Solver::tuneRelaxation() {
   for (size_t l = 0; l < amr_.size(); ++l) {
     const double cells = (double)amr_[l].grids.numCells();
     Coef<double> c = coefAMR((int)l);
-    float t[3];
-    for (int v = 0; v < 3; ++v)
+    float t[kRelaxVariants];
+    for (int v = 0; v < kRelaxVariants; ++v)
       t[v] = (v == 2 && cells > kBlockRelaxMaxCells) ? 1e30f
                                                      : timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, v);
-    inlineA_[l] = (char)(std::min_element(t, t + 3) - t);
-    tuneMs_.push_back({t[0], std::min(t[1], t[2])});
+    inlineA_[l] = (char)(std::min_element(t, t + kRelaxVariants) - t);
+    tuneMs_.push_back({t[0], *std::min_element(t + 1, t + kRelaxVariants)});
     zeroField(amrDev_[l], lev_[l].corr);
   }
   for (size_t d = 0; d < mg_.size(); ++d) {
     const double cells = (double)mg_[d].grids.numCells();
     Coef<double> c = coefMG((int)d + 1);
-    float t[3];
-    for (int v = 0; v < 3; ++v)
+    float t[kRelaxVariants];
+    for (int v = 0; v < kRelaxVariants; ++v)
       t[v] = (v == 2 && cells > kBlockRelaxMaxCells) ? 1e30f
                                                      : timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, v);
-    inlineM_[d] = (char)(std::min_element(t, t + 3) - t);
-    tuneMs_.push_back({t[0], std::min(t[1], t[2])});
+    inlineM_[d] = (char)(std::min_element(t, t + kRelaxVariants) - t);
+    tuneMs_.push_back({t[0], *std::min_element(t + 1, t + kRelaxVariants)});
     zeroField(mgDev_[d], mgf_[d].corr);
   }
   profOn_ = prof;
@@ -849,7 +863,8 @@ std::vector<SolveResult> Solver::tga(const SolveParams& p, double dt, int nsteps
 }
 
 void Solver::setRelaxMode(int mode) {
-  if (mode < 0 || mode > 2) throw std::invalid_argument("cmg: relaxation mode is 0 (tuned), 1 (fills) or 2 (inline)");
+  if (mode < 0 || mode > 3)
+    throw std::invalid_argument("cmg: relaxation mode is 0 (tuned), 1 (fills), 2 (inline) or 3 (fused sweeps)");
   relaxMode_ = mode;
   tuned_ = false;
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);

@@ -112,11 +112,14 @@ int cmg_use_graphs(cmg_hierarchy* h, int on);
  * by a timing autotuner before the first solve (default); 1 = ghost fill
  * (exchange, boundary and coarse-fine values) before each colour pass, as the
  * reference's levelGSRB; 2 = the neighbours beyond each box evaluated inside
- * the pass from the same fill rules, no fill.  Identical results. */
+ * the pass from the same fill rules, no fill; 3 = fused sweeps: both colours
+ * of a sweep in one launch (every box marching through its z slabs, the
+ * colour-1 cells on faces shared with another box in a second launch), no
+ * fill.  Identical results. */
 int cmg_set_relax_mode(cmg_hierarchy* h, int mode);
 /* The relaxation variant of every AMR level, then every multigrid depth
  * (0 = ghost fills, 1 = in-pass ghosts, 2 = all sweeps in one one-block
- * launch, for levels of at most 32768 cells), with the autotuner's times in
+ * launch, for levels of at most 32768 cells, 3 = fused sweeps), with the autotuner's times in
  * ms for four sweeps with fills and with the best other variant (-1 when a
  * mode was forced); runs the tuner if it has not run.  n: entries. */
 int cmg_relax_variants(cmg_hierarchy* h, int* inline_out, float* ms_fill, float* ms_inline, int cap, int* n);

@@ -52,13 +52,15 @@ def test_graph_replay_is_bit_identical(cmg, name, mixed):
                                          ("vc_3lev_16", 2), ("poisson_1lev_32", 1), ("vc_1lev_32", 2)])
 def test_relaxation_variants_are_bit_identical(cmg, name, num_mg):
     """Ghost fill before each colour pass (mode 1), face ghosts evaluated in
-    the pass (mode 2) and the autotuned mix (mode 0) give the same bits, with
-    V-cycles and with W-cycles (num_mg=2), on one and on several levels."""
+    the pass (mode 2), fused sweeps (mode 3: both colours per launch, boxes
+    marching in z, exchange-face colour-1 cells in a second launch) and the
+    autotuned mix (mode 0) give the same bits, with V-cycles and with W-cycles
+    (num_mg=2), on one and on several levels, FP64 and mixed precision."""
     h, p, meta = make(cmg, name)
     p.num_mg = num_mg
     nlev = len(meta["boxes"])
     ref = None
-    for mode in (1, 2, 0):
+    for mode in (1, 2, 3, 0):
         h.set_relax_mode(mode)
         for mixed in (False, True):
             out = h.solve(p, mixed=mixed)
@@ -67,4 +69,21 @@ def test_relaxation_variants_are_bit_identical(cmg, name, num_mg):
                 ref = ref or {}
                 ref.setdefault(mixed, got)
             assert got == ref[mixed], (mode, mixed)
+    h.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["config1_vc_3lev_128", "vc_3lev_32"])
+def test_fused_sweeps_match_reference(cmg, name):
+    """Every level relaxed with fused sweeps (mode 3) reproduces the reference solve bit for bit."""
+    meta, arrays = golden(name)
+    h, p, _ = make(cmg, name)
+    h.set_relax_mode(3)
+    out = h.solve(p)
+    assert np.array_equal(out["history"], np.array(meta["residual_history"]))
+    for lev in range(len(meta["boxes"])):
+        phi = h.phi(lev)
+        ref = arrays[f"phi{lev}"] if meta["full"] else arrays[f"phi{lev}_sample"]
+        got = phi if meta["full"] else phi[::meta["sample_stride"]]
+        assert np.array_equal(got, ref), lev
     h.close()

@@ -834,7 +834,7 @@ int cmg_op_prolong_increment(cmg_hierarchy* h, int lev, double* phi, const doubl
 }
 
 int cmg_op_amr_operator(cmg_hierarchy* h, int level, int form, double* out, const double* phi_fine,
-                        const double* phi, const double* phi_coarse, const double* rhs) {
+                        double* phi, const double* phi_coarse, const double* rhs) {
   return guard([&]() {
     needPtr(out);
     opSolver(h, level).opAMROperator(level, out, phi_fine, phi, phi_coarse, rhs, form);

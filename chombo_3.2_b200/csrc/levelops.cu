@@ -283,6 +283,18 @@ void Solver::opStore(int lev, const double* f, double* host) {
   ck(cudaStreamSynchronize(s_), "operator sync");
 }
 
+// Every cell of device field f of level lev (valid and ghost) -> host
+// ghosted array.
+void Solver::opStoreGrown(int lev, const double* f, double* host) {
+  OpState& st = opState(lev);
+  const LevelDev& L = opDev(lev);
+  if (L.nbox == 0) return;
+  k_ghosted<<<L.nbox, 256, 0, s_>>>(L.boxes, st.off, const_cast<double*>(f), st.packed, 2);
+  ck(cudaGetLastError(), "operator gather");
+  ck(cudaMemcpyAsync(host, st.packed, st.size * sizeof(double), cudaMemcpyDeviceToHost, s_), "operator d2h");
+  ck(cudaStreamSynchronize(s_), "operator sync");
+}
+
 void Solver::opEnsureTuned() {
   if (!tuned_) tuneRelaxation();
 }
@@ -382,7 +394,7 @@ void Solver::opProlongIncrement(int lev, double* phi, const double* corrCoarse) 
 //   form 0: out = L(phi)           (applyOpI, plus reflux with phiFine),
 //   form 1: out = rhs - L(phi)     (the same, then axby(out, out, rhs, -1, 1)),
 //   form 2: out = rhs - L(phi)     (residualI: OPERATORLAPRES / VCCOMPUTERES3D).
-void Solver::opAMROperator(int l, double* out, const double* phiFine, const double* phi, const double* phiCoarse,
+void Solver::opAMROperator(int l, double* out, const double* phiFine, double* phi, const double* phiCoarse,
                            const double* rhs, int form) {
   if (l < 0 || l >= numLevels()) throw std::invalid_argument("cmg: AMR level out of range");
   if (phiCoarse && l == 0) throw std::invalid_argument("cmg: level 0 has no coarser level");
@@ -408,6 +420,7 @@ void Solver::opAMROperator(int l, double* out, const double* phiFine, const doub
     if (form == 1) negAdd(L, o, o, r, s_);
   }
   opStore(l, o, out);
+  opStoreGrown(l, f, phi);
 }
 
 // AMRPoissonOp::AMRRestrictS (AMRPoissonOp.cpp:877-919): the residual of
@@ -482,15 +495,9 @@ void Solver::opAMRUpdateResidual(int l, double* res, const double* corr, const d
 // whole (valid and ghost cells).
 void Solver::opCFInterp(int l, double* phi, const double* phiCoarse) {
   if (l < 1 || l >= numLevels()) throw std::invalid_argument("cmg: coarse-fine interpolation needs a level >= 1");
-  OpState& st = opState(l);
   double* f = opLoad(l, 0, phi);
   quadCF(amrDev_[l], f, opLoad(l - 1, 3, phiCoarse), s_);
-  const LevelDev& L = amrDev_[l];
-  if (L.nbox == 0) return;
-  k_ghosted<<<L.nbox, 256, 0, s_>>>(L.boxes, st.off, f, st.packed, 2);
-  ck(cudaGetLastError(), "operator gather");
-  ck(cudaMemcpyAsync(phi, st.packed, st.size * sizeof(double), cudaMemcpyDeviceToHost, s_), "operator d2h");
-  ck(cudaStreamSynchronize(s_), "operator sync");
+  opStoreGrown(l, f, phi);
 }
 
 // AMRLevelOp::zeroCovered (AMRMultiGrid.H:197-201): the valid cells of level

@@ -187,7 +187,7 @@ class Solver {
   void opPreCond(int lev, double* cor, const double* res);
   void opRestrictResidual(int lev, double* resCoarse, const double* phi, const double* rhs);
   void opProlongIncrement(int lev, double* phi, const double* corrCoarse);
-  void opAMROperator(int l, double* out, const double* phiFine, const double* phi, const double* phiCoarse,
+  void opAMROperator(int l, double* out, const double* phiFine, double* phi, const double* phiCoarse,
                      const double* rhs, int form);
   void opAMRRestrict(int l, double* resCoarsened, const double* residual, const double* corr,
                      const double* corrCoarse);
@@ -218,6 +218,7 @@ class Solver {
   void* uploadRaw(const void* src, size_t bytes);
   double* opLoad(int lev, int k, const double* host);
   void opStore(int lev, const double* f, double* host);
+  void opStoreGrown(int lev, const double* f, double* host);
   void opEnsureTuned();
   std::vector<double> opBoxValues(int lev, int nbox);
   const LevelDev& opDev(int lev) const;

@@ -411,9 +411,13 @@ int cmg_op_prolong_increment(cmg_hierarchy* h, int lev, double* phi, const doubl
  *   form 1: the same followed by out = rhs - out as axby(out, out, rhs, -1, 1)
  *           (AMRResidual, AMRResidualNC);
  *   form 2: out = rhs - L(phi) in residualI's own expression, phi_fine NULL
- *           (AMRResidualNF). */
+ *           (AMRResidualNF).
+ * Without phi_coarse the coarse-fine ghosts are phi's own (as the reference's
+ * applyOpI leaves them).  On return phi holds the ghost values the operator
+ * used (its valid cells unchanged): the reference fills the ghost cells of
+ * its const phi argument the same way. */
 int cmg_op_amr_operator(cmg_hierarchy* h, int level, int form, double* out, const double* phi_fine,
-                        const double* phi, const double* phi_coarse, const double* rhs);
+                        double* phi, const double* phi_coarse, const double* rhs);
 /* AMRLevelOp::AMRRestrictS (AMRPoissonOp.cpp:877-919), level >= 1: the
  * residual of `correction` against `residual` with coarse-fine ghosts from
  * coarse_correction (level - 1), averaged onto the coarsened-fine layout

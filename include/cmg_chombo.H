@@ -57,6 +57,7 @@
 #include "FluxBox.H"
 #include "LevelData.H"
 #include "LinearSolver.H"
+#include "LevelDataOps.H"
 #include "MayDay.H"
 #include "ProblemDomain.H"
 #include "RealVect.H"
@@ -171,7 +172,11 @@ class GpuAMRPoissonOp : public AMRLevelOp<LDF> {
   virtual void assignLocal(LDF& a_lhs, const LDF& a_rhs) {
     for (DataIterator dit = a_lhs.dataIterator(); dit.ok(); ++dit) a_lhs[dit].copy(a_rhs[dit]);
   }
+  // BLAS-1 on data of this level runs on the device; FASMultiGrid also hands
+  // the finest operator data of other depths (FASMultiGrid.H cycle), which
+  // goes to the reference's own LevelDataOps, as in the reference.
   virtual Real dotProduct(const LDF& a_1, const LDF& a_2) {
+    if (!mine(a_1)) return m_ops.dotProduct(a_1, a_2);
     in(a_1, m_a);
     in(a_2, m_b);
     double r = 0;
@@ -179,12 +184,14 @@ class GpuAMRPoissonOp : public AMRLevelOp<LDF> {
     return r;
   }
   virtual void incr(LDF& a_lhs, const LDF& a_x, Real a_scale) {
+    if (!mine(a_lhs)) return m_ops.incr(a_lhs, a_x, a_scale);
     in(a_lhs, m_o);
     in(a_x, m_a);
     check(cmg_op_incr(h(), m_lev, m_o.data(), m_a.data(), a_scale));
     outValid(m_o, a_lhs);
   }
   virtual void axby(LDF& a_lhs, const LDF& a_x, const LDF& a_y, Real a_a, Real a_b) {
+    if (!mine(a_lhs)) return m_ops.axby(a_lhs, a_x, a_y, a_a, a_b);
     in(a_x, m_a);
     in(a_y, m_b);
     out0(m_o);
@@ -192,11 +199,13 @@ class GpuAMRPoissonOp : public AMRLevelOp<LDF> {
     outValid(m_o, a_lhs);
   }
   virtual void scale(LDF& a_lhs, const Real& a_scale) {
+    if (!mine(a_lhs)) return m_ops.scale(a_lhs, a_scale);
     in(a_lhs, m_o);
     check(cmg_op_scale(h(), m_lev, m_o.data(), a_scale));
     outValid(m_o, a_lhs);
   }
   virtual Real norm(const LDF& a_x, int a_ord) {
+    if (!mine(a_x)) return CH_XD::norm(a_x, a_x.interval(), a_ord);
     in(a_x, m_a);
     double r = 0;
     check(cmg_op_norm(h(), m_lev, m_a.data(), a_ord, &r));
@@ -218,6 +227,20 @@ class GpuAMRPoissonOp : public AMRLevelOp<LDF> {
     in(a_residual, m_b);
     check(cmg_op_relax(h(), m_lev, m_a.data(), m_b.data(), a_iterations));
     outValid(m_a, a_correction);
+  }
+  // AMRPoissonOp::relaxNF (AMRPoissonOp.cpp:586-596): the inhomogeneous
+  // coarse-fine ghosts from a_phiCoarse, then relax.
+  virtual void relaxNF(LDF& a_phi, const LDF* a_phiCoarse, const LDF& a_rhs, int a_iterations) {
+    if (a_phiCoarse != NULL) coarseFineInterp(a_phi, *a_phiCoarse);
+    relax(a_phi, a_rhs, a_iterations);
+  }
+  // AMRPoissonOp::residualNF (AMRPoissonOp.cpp:238-254): homogeneous
+  // coarse-fine ghosts, or inhomogeneous ones from a_phiCoarse, then
+  // residualI (which keeps the coarse-fine ghosts a_phi holds).
+  virtual void residualNF(LDF& a_lhs, LDF& a_phi, const LDF* a_phiCoarse, const LDF& a_rhs,
+                          bool a_homogeneous = false) {
+    if (!a_homogeneous && a_phiCoarse != NULL) coarseFineInterp(a_phi, *a_phiCoarse);
+    residual(a_lhs, a_phi, a_rhs, a_homogeneous);
   }
   virtual void restrictResidual(LDF& a_resCoarse, LDF& a_phiFine, const LDF& a_rhsFine) {
     in(a_phiFine, m_a);
@@ -346,6 +369,9 @@ class GpuAMRPoissonOp : public AMRLevelOp<LDF> {
   Real m_dx;
   std::vector<double> m_a, m_b, m_c, m_o;
 
+  LevelDataOps<FArrayBox> m_ops;
+
+  bool mine(const LDF& a_ld) const { return sameBoxes(a_ld.disjointBoxLayout(), m_grids); }
   cmg_hierarchy* h() const;
   static void check(int rc) {
     if (rc != CMG_OK) MayDay::Error(cmg_last_error());
@@ -439,6 +465,11 @@ class GpuAMRPoissonOp : public AMRLevelOp<LDF> {
     check(cmg_op_amr_operator(h(), m_lev, a_form, m_o.data(), fine ? m_c.data() : nullptr, m_a.data(),
                               coarse ? m_d.data() : nullptr, a_rhs ? m_b.data() : nullptr));
     outValid(m_o, a_out);
+    // The reference fills the ghost cells of its const phi argument
+    // (coarse-fine, exchange, boundary) and later operators that apply the
+    // stencil without a coarse-fine fill (AMROperatorNC, residual with
+    // inhomogeneous boundaries) read them: keep them the same here.
+    unpackGrown(m_a, const_cast<LDF&>(a_phi));
   }
   std::vector<double> m_d;
 };

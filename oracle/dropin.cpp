@@ -14,7 +14,8 @@
 // fineinterp=1 (interpToFine) or 2 (pwcinterpToFine) for FineInterp; ops=1
 // for the operator-by-operator comparison of the reference's operators with
 // the GPU AMRLevelOps; amrmg=1 for the reference's AMRMultiGrid over the
-// reference factory and over the GPU factory; neumann=1 hands a Neumann BC
+// reference factory and over the GPU factory, amrmg=1 fas=1 for its
+// AMRFASMultiGrid the same way; neumann=1 hands a Neumann BC
 // to the GPU factory, which must refuse it)
 #include <cmath>
 #include <cstdio>
@@ -23,6 +24,7 @@
 #include <map>
 #include <string>
 
+#include "AMRFASMultiGrid.H"
 #include "AMRMultiGrid.H"
 #include "AMRPoissonOp.H"
 #include "AMRTGA.H"
@@ -647,12 +649,15 @@ static int opsCheck(OracleProblem& P, Vector<int>& rr) {
   return 0;
 }
 
-// The reference's own AMRMultiGrid, unmodified, defined once with the
-// reference's factory and once with the GPU factory (cmg_chombo's
-// AMRLevelOpFactory, whose operators run on the device one call at a time):
-// both solves print exit status, iteration count, residual history and phi
-// deviation as one JSON line.
+// The reference's own AMRMultiGrid (or, with fas=1, its AMRFASMultiGrid in
+// V-cycle mode), unmodified, defined once with the reference's factory and
+// once with the GPU factory (cmg_chombo's AMRLevelOpFactory, whose operators
+// run on the device one call at a time): both solves print exit status,
+// iteration count, residual history and phi deviation as one JSON line.
+// AMRFASMultiGrid calls no inspector, so its history is the final composite
+// residual alone.
 static int amrmgCheck(OracleProblem& P, Vector<int>& rr) {
+  const bool fas = argd("fas", 0) != 0;
   const int nlev = P.nlev, lmax = P.finest;
   const int pre = (int)argd("pre", 4), post = (int)argd("post", 4), bottom = (int)argd("bottom", 4);
   const int iters = (int)argd("iters", 100);
@@ -682,21 +687,24 @@ static int amrmgCheck(OracleProblem& P, Vector<int>& rr) {
     for (DataIterator dit = P.grids[l].dataIterator(); dit.ok(); ++dit) phiG[l]->operator[](dit()).setVal(0.0);
   }
   ResidualRecorder* recs[2];
-  int exitS[2];
+  int exitS[2], itersDone[2];
   for (int side = 0; side < 2; ++side) {
     BiCGStabSolver<LDF> bottomSolver;
     bottomSolver.m_verbosity = 0;
-    AMRMultiGrid<LDF> mg;
-    mg.define(P.domains[0], side == 0 ? *refFactory : *gpuFactory, &bottomSolver, nlev);
-    mg.setSolverParameters(pre, post, bottom, 1, iters, eps, hang, 1e-30);
-    mg.m_verbosity = 0;
+    AMRFASMultiGrid<LDF>* fmg = fas ? new AMRFASMultiGrid<LDF> : nullptr;
+    AMRMultiGrid<LDF>* mg = fas ? fmg : new AMRMultiGrid<LDF>;
+    mg->define(P.domains[0], side == 0 ? *refFactory : *gpuFactory, &bottomSolver, nlev);
+    mg->setSolverParameters(pre, post, bottom, 1, iters, eps, hang, 1e-30);
+    mg->m_verbosity = 0;
     RefCountedPtr<AMRMultiGridInspector<LDF> > insp(new ResidualRecorder);
-    mg.addInspector(insp);
-    mg.solve(side == 0 ? P.phi : phiG, P.rhs, lmax, 0, true);
+    mg->addInspector(insp);
+    mg->solve(side == 0 ? P.phi : phiG, P.rhs, lmax, 0, true);
     recs[side] = static_cast<ResidualRecorder*>(&(*insp));
-    recs[side]->norms.push_back(mg.computeAMRResidual(side == 0 ? P.phi : phiG, P.rhs, lmax, 0));
-    exitS[side] = mg.m_exitStatus;
+    recs[side]->norms.push_back(mg->computeAMRResidual(side == 0 ? P.phi : phiG, P.rhs, lmax, 0));
+    itersDone[side] = fas ? fmg->m_iter : (int)recs[side]->norms.size() - 1;
+    exitS[side] = mg->m_exitStatus;
     insp.neverDelete();
+    delete mg;
   }
   const bool sameLen = recs[0]->norms.size() == recs[1]->norms.size();
   bool histExact = sameLen;
@@ -707,12 +715,18 @@ static int amrmgCheck(OracleProblem& P, Vector<int>& rr) {
       maxHist = std::max(maxHist, std::fabs(recs[0]->norms[i] - recs[1]->norms[i]) / recs[0]->norms[0]);
     }
   long ndiff = 0;
-  for (int l = 0; l < nlev; ++l) ndiff += validDiff(*P.phi[l], *phiG[l]).ndiff;
-  std::printf("{\"amrmg\": 1, \"levels\": %d, \"cpu_exit\": %d, \"gpu_exit\": %d, \"cpu_iters\": %d, \"gpu_iters\": %d, "
+  std::string perLevel;
+  for (int l = 0; l < nlev; ++l) {
+    const long d = validDiff(*P.phi[l], *phiG[l]).ndiff;
+    ndiff += d;
+    perLevel += (l ? ", " : "") + std::to_string(d);
+  }
+  std::printf("{\"amrmg\": 1, \"fas\": %d, \"levels\": %d, \"cpu_exit\": %d, \"gpu_exit\": %d, \"cpu_iters\": %d, \"gpu_iters\": %d, "
               "\"same_history_length\": %s, \"history_exact\": %s, \"history_dev\": %.3e, \"phi_ndiff\": %ld, "
-              "\"phi_rel_dev\": %.3e}\n",
-              nlev, exitS[0], exitS[1], (int)recs[0]->norms.size() - 1, (int)recs[1]->norms.size() - 1,
-              sameLen ? "true" : "false", histExact ? "true" : "false", maxHist, ndiff, phiDeviation(P, phiG));
+              "\"phi_rel_dev\": %.3e, \"phi_ndiff_per_level\": [%s]}\n",
+              fas ? 1 : 0, nlev, exitS[0], exitS[1], itersDone[0], itersDone[1],
+              sameLen ? "true" : "false", histExact ? "true" : "false", maxHist, ndiff, phiDeviation(P, phiG),
+              perLevel.c_str());
   delete recs[0];
   delete recs[1];
   return 0;

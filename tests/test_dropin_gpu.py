@@ -155,3 +155,23 @@ def test_reference_amrmultigrid_over_gpu_operators(name):
     assert out["gpu_iters"] == out["cpu_iters"], out
     assert out["history_exact"], out
     assert out["phi_ndiff"] == 0, out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(OPS_CASES))
+def test_reference_amrfasmultigrid_over_gpu_operators(name):
+    """The reference's AMRFASMultiGrid (V-cycle mode, AMRFASMultiGrid.H), unmodified, over the reference factory
+    and over the GPU factory: it drives the operators through relaxNF, AMRRestrictS with and without the
+    residual, AMROperatorNC on the coarse level's own coarse-fine ghosts, AMRProlongS and the FASMultiGrid
+    depths below level 0.  Same exit status, iteration count, final composite residual and phi, bit for bit."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in check not built (make -C oracle dropin, needs the reference tree)")
+    r = subprocess.run([DROPIN] + OPS_CASES[name].split() + ["amrmg=1", "fas=1", "iters=12"], capture_output=True,
+                       text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["fas"] == 1
+    assert out["gpu_exit"] == out["cpu_exit"], out
+    assert out["gpu_iters"] == out["cpu_iters"] > 0, out
+    assert out["history_exact"], out
+    assert out["phi_ndiff"] == 0, out

@@ -25,6 +25,8 @@ class Box(ctypes.Structure):
 
 # Status codes (cmg.h).
 CMG_OK, CMG_EINVAL, CMG_ENOMEM, CMG_ECUDA, CMG_EINTERNAL, CMG_EDIVERGED, CMG_ETIMEOUT, CMG_ECANCELLED = range(8)
+# Homogeneous boundary types of a domain face (cmg_hierarchy_create_bc).
+BC_DIRICHLET, BC_NEUMANN = 0, 1
 
 
 class SolveParams(ctypes.Structure):
@@ -233,7 +235,9 @@ class FineInterp:
 class Hierarchy:
     """One AMR hierarchy with device-resident state (cmg_hierarchy)."""
 
-    def __init__(self, n0, level_boxes, op=0, alpha=0.0, beta=1.0, dx0=None):
+    def __init__(self, n0, level_boxes, op=0, alpha=0.0, beta=1.0, dx0=None, bc=None):
+        """bc: None (homogeneous Dirichlet on every face) or six face types, x-lo, x-hi, y-lo, y-hi, z-lo, z-hi,
+        each BC_DIRICHLET / BC_NEUMANN or the letters 'D' / 'N' (a string such as "NNNNND")."""
         L = lib()
         self.nlev = len(level_boxes)
         counts = (ctypes.c_int * self.nlev)(*[len(b) for b in level_boxes])
@@ -241,9 +245,15 @@ class Hierarchy:
         arr = boxes_array(flat)
         h = ctypes.c_void_p()
         dx0 = 1.0 / n0 if dx0 is None else dx0
-        _check(L.cmg_hierarchy_create((ctypes.c_int * 3)(0, 0, 0), (ctypes.c_int * 3)(n0 - 1, n0 - 1, n0 - 1),
-                                      ctypes.c_double(dx0), self.nlev, counts, arr, op, ctypes.c_double(alpha),
-                                      ctypes.c_double(beta), ctypes.byref(h)))
+        bcs = None
+        if bc is not None:
+            codes = [{"D": BC_DIRICHLET, "N": BC_NEUMANN}.get(x, x) if isinstance(x, str) else int(x) for x in bc]
+            if len(codes) != 6:
+                raise ValueError("bc needs six face types")
+            bcs = (ctypes.c_int * 6)(*codes)
+        _check(L.cmg_hierarchy_create_bc((ctypes.c_int * 3)(0, 0, 0), (ctypes.c_int * 3)(n0 - 1, n0 - 1, n0 - 1),
+                                         ctypes.c_double(dx0), self.nlev, counts, arr, op, ctypes.c_double(alpha),
+                                         ctypes.c_double(beta), bcs, ctypes.byref(h)))
         self.h = h
         self.op = op
 

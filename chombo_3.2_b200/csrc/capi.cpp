@@ -119,11 +119,23 @@ const char* cmg_last_error(void) { return g_err.c_str(); }
 
 int cmg_hierarchy_create(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels, const int* nboxes,
                          const cmg_box* boxes, int op, double alpha, double beta, cmg_hierarchy** out) {
+  return cmg_hierarchy_create_bc(domain_lo, domain_hi, dx0, nlevels, nboxes, boxes, op, alpha, beta, nullptr, out);
+}
+
+int cmg_hierarchy_create_bc(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
+                            const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta,
+                            const int bc[6], cmg_hierarchy** out) {
   return guard([&]() {
     if (!domain_lo || !domain_hi || !nboxes || !boxes || !out || nlevels < 1 || dx0 <= 0 || (op != 0 && op != 1))
       throw std::invalid_argument("cmg: invalid hierarchy description");
     *out = nullptr;
     cmg::HierarchyDesc d;
+    if (bc)
+      for (int f = 0; f < 6; ++f) {
+        if (bc[f] != CMG_BC_DIRICHLET && bc[f] != CMG_BC_NEUMANN)
+          throw std::invalid_argument("cmg: boundary type is CMG_BC_DIRICHLET or CMG_BC_NEUMANN");
+        d.bc[f] = bc[f];
+      }
     d.domain = cmg::Box(cmg::IV(domain_lo[0], domain_lo[1], domain_lo[2]), cmg::IV(domain_hi[0], domain_hi[1], domain_hi[2]));
     if (d.domain.empty()) throw std::invalid_argument("cmg: empty domain");
     d.dx0 = dx0;

@@ -87,7 +87,8 @@ enum GhostKind {
   G_BC = 1,        // homogeneous first-order Dirichlet: g = 2*0 - interior
   G_CFQUAD = 2,    // homogeneous quadratic CF: g = c1*phi(1 in) + c2*phi(2 in)
   G_CFLIN = 3,     // one-cell-wide box: g = f*phi(1 in)
-  G_ZERO = 4       // dst(cell) = 0 (covered cells before a norm)
+  G_ZERO = 4,      // dst(cell) = 0 (covered cells before a norm)
+  G_NEU = 5        // homogeneous Neumann: g = interior (NeumBC, BCFunc.cpp:217-236)
 };
 
 // Ghost cells handled by one thread block of the ghost kernel (each thread
@@ -100,7 +101,8 @@ struct GhostTask {
 };
 
 // One ghost cell of a level's ghost fill, as element indices: dst = src1
-// (s2 == -1, exchange copy), dst = 2*0 - src1 (s2 == -2, homogeneous
+// (s2 == -1, exchange copy or homogeneous Neumann face), dst = 2*0 - src1
+// (s2 == -2, homogeneous
 // Dirichlet face), dst = flin*src1 (s2 == -3, linear coarse-fine ghost of a
 // one-cell-wide box), dst = c1*src1 + c2*s2 (s2 >= 0, quadratic coarse-fine).
 struct GhostCell {
@@ -118,7 +120,8 @@ enum FaceRuleKind {
   FR_BC = 1,      // homogeneous Dirichlet: 2*0 - (the adjacent cell)
   FR_CFQUAD = 2,  // homogeneous quadratic CF: c1*(adjacent) + c2*f[src], src two cells inward
   FR_CFLIN = 3,   // linear CF of a one-cell-wide box: flin*(adjacent)
-  FR_FAB = 4      // no fill rule: the FAB ghost element src as it is
+  FR_FAB = 4,     // no fill rule: the FAB ghost element src as it is
+  FR_NEU = 5      // homogeneous Neumann: the adjacent cell itself
 };
 struct FaceRule {
   int src, kind;

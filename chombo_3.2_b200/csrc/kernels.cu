@@ -132,6 +132,8 @@ __global__ void __launch_bounds__(GHOST_THREADS) k_ghost(const GhostTaskDev* tas
     } else if (k == G_BC) {
       T zero = T(0);
       out = T(2) * zero - v1[u];
+    } else if (k == G_NEU) {
+      out = v1[u];
     } else if (k == G_CFLIN) {
       out = flin * v1[u];
     } else {
@@ -217,6 +219,7 @@ __device__ __forceinline__ T ghostValue(const FaceRule* __restrict__ rules, cons
   const FaceRule r = rules[faceOff[6 * b + 2 * d + (s > 0)] + (p[t0] - bd.lo[t0]) +
                            (bd.hi[t0] - bd.lo[t0] + 1) * (p[t1] - bd.lo[t1])];
   if (r.kind == FR_COPY || r.kind == FR_FAB) return phi[r.src];
+  if (r.kind == FR_NEU) return pc;
   if (r.kind == FR_BC) {
     T zero = T(0);
     return T(2) * zero - pc;
@@ -343,6 +346,7 @@ __global__ void __launch_bounds__(1024) k_relax_block(const BoxDesc* boxes, cons
 template <class T>
 __device__ __forceinline__ T ruleValue(const FaceRule& r, T pc, const T* phi, const GhostCoef& gc) {
   if (r.kind == FR_COPY || r.kind == FR_FAB) return phi[r.src];
+  if (r.kind == FR_NEU) return pc;
   if (r.kind == FR_BC) {
     T zero = T(0);
     return T(2) * zero - pc;

@@ -84,7 +84,10 @@ void buildFaceRules(LevelPlan& L);
 
 // Layout and ghost/chunk plans of one level (AMR level or multigrid depth).
 // dxCrse > 0 enables homogeneous coarse-fine ghost tasks on CF faces.
-void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse);
+// bc: homogeneous boundary type of each domain face (x-lo, x-hi, y-lo, y-hi,
+// z-lo, z-hi): 0 Dirichlet, 1 Neumann; nullptr for Dirichlet everywhere.
+void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse,
+                const int* bc = nullptr);
 // Coarse-fine interpolation tables of fine level F from coarse level C.
 void buildQuadCF(LevelPlan& F, const LevelPlan& C);
 // Coarse/fine box maps and zero-covered tasks (F fine, C coarse).

@@ -156,6 +156,8 @@ void buildFaceRules(LevelPlan& L) {
             r = FaceRule{(int)cellOf(L, t.src, g), FR_COPY};
           } else if (t.kind == G_BC) {
             r = FaceRule{0, FR_BC};
+          } else if (t.kind == G_NEU) {
+            r = FaceRule{0, FR_NEU};
           } else if (t.kind == G_CFLIN) {
             r = FaceRule{0, FR_CFLIN};
           } else if (t.kind == G_CFQUAD) {
@@ -229,6 +231,7 @@ void buildChunkGhosts(LevelPlan& L) {
               switch (r[q].kind) {
                 case FR_COPY: e.s1 = r[q].src, e.s2 = -1; break;
                 case FR_BC: e.s1 = adj, e.s2 = -2; break;
+                case FR_NEU: e.s1 = adj, e.s2 = -1; break;
                 case FR_CFLIN: e.s1 = adj, e.s2 = -3; break;
                 default: e.s1 = adj, e.s2 = r[q].src; break;  // FR_CFQUAD
               }
@@ -274,7 +277,7 @@ std::vector<int> blockTasks(const std::vector<int>& start) {
   return bt;
 }
 
-void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse) {
+void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse, const int* bc) {
   L.grids = grids;
   L.index.build(L.grids.boxes);
   L.domain = domain;
@@ -307,8 +310,9 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
   }
   L.nelem = off;
 
-  // Exchange items (Copier::exchangeDefine + trimEdges) and homogeneous
-  // Dirichlet faces (the driver's BC function: face ghosts outside the domain).
+  // Exchange items (Copier::exchangeDefine + trimEdges) and the physical
+  // boundary faces (face ghosts outside the domain): homogeneous Dirichlet, or
+  // homogeneous Neumann where bc[2 * dir + (side > 0)] is 1.
   L.ghost.clear();
   for (const Motion& m : exchangePlan(grids)) {
     GhostTask t{G_COPY, m.to, m.from, 0, 0, {}, {}};
@@ -324,7 +328,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
       for (int side = -1; side <= 1; side += 2) {
         Box g = grids[b].adjCell(d, side, 1);
         if (domain.contains(g)) continue;
-        GhostTask t{G_BC, (int)b, (int)b, d, side, {}, {}};
+        GhostTask t{bc && bc[2 * d + (side > 0)] == 1 ? G_NEU : G_BC, (int)b, (int)b, d, side, {}, {}};
         for (int k = 0; k < 3; ++k) {
           t.lo[k] = g.lo[k];
           t.hi[k] = g.hi[k];
@@ -414,7 +418,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
             int e[3] = {0, 0, 0};
             e[t.dir] = -t.side;
             g.s1 = (int)cellIndex(db, i + e[0], j + e[1], k + e[2]);
-            g.s2 = t.kind == G_BC ? -2 : t.kind == G_CFLIN ? -3
+            g.s2 = t.kind == G_NEU ? -1 : t.kind == G_BC ? -2 : t.kind == G_CFLIN ? -3
                                    : (int)cellIndex(db, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
           }
           L.gcells[at++] = g;
@@ -1022,11 +1026,11 @@ void buildBottom(const LevelPlan& L, BottomPlan& B) {
           if (t.kind == G_COPY) {
             src = cellIndex(L.boxes[t.src], i, j, k);
             B.gkind[g] = 0;
-          } else if (t.kind == G_BC) {
+          } else if (t.kind == G_BC || t.kind == G_NEU) {
             int e[3] = {0, 0, 0};
             e[t.dir] = -t.side;
             src = cellIndex(db, i + e[0], j + e[1], k + e[2]);
-            B.gkind[g] = 1;
+            B.gkind[g] = t.kind == G_BC ? 1 : 0;  // Neumann: a copy of the adjacent cell
           } else {
             throw std::runtime_error("cmg: coarse-fine ghost task on the bottom level");
           }

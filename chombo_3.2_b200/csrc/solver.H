@@ -26,6 +26,7 @@ struct HierarchyDesc {
   std::vector<std::vector<Box>> boxes;   // per AMR level, refinement ratio 2
   int vc = 0;                            // 0: AMRPoissonOp, 1: VCAMRPoissonOp2
   double alpha = 0.0, beta = 1.0;
+  int bc[6] = {0, 0, 0, 0, 0, 0};        // per domain face: 0 homogeneous Dirichlet, 1 homogeneous Neumann
 };
 
 struct SolveParams {

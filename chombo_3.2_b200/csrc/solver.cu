@@ -224,7 +224,7 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
     for (int l = 0; l < nlev; ++l)
       th.emplace_back([&, l]() {
         try {
-          buildLevel(amr_[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0);
+          buildLevel(amr_[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0, desc.bc);
         } catch (...) {
           err[l] = std::current_exception();
         }
@@ -233,7 +233,7 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
       th.emplace_back([&, d]() {
         try {
           const int c = mgc[d];
-          buildLevel(mg_[d], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0);
+          buildLevel(mg_[d], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0, desc.bc);
         } catch (...) {
           err[nlev + d] = std::current_exception();
         }

@@ -59,13 +59,26 @@ const char* cmg_last_error(void);
  * op = 1: VCAMRPoissonOp2, L = alpha a phi - beta div(b grad phi)
  * (VCAMRPoissonOp2Factory::define, AMRElliptic/VCAMRPoissonOp2.cpp:873-924).
  * Boundary conditions are homogeneous Dirichlet on every domain face
- * (the examples' ParseBC, releasedExamples/AMRPoisson/execCell/poissonSolve.cpp:76-119).
+ * (the examples' ParseBC, releasedExamples/AMRPoisson/execCell/poissonSolve.cpp:76-119);
+ * cmg_hierarchy_create_bc takes one per face.
  * Builds every plan (exchange copiers, coarse-fine stencils, flux registers,
  * multigrid levels: AMRMultiGrid::define, AMRMultiGrid.H:1292-1328) and
  * allocates all device state. */
 int cmg_hierarchy_create(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
                          const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta,
                          cmg_hierarchy** out);
+/* The same with a homogeneous boundary type per domain face, in the order
+ * x-lo, x-hi, y-lo, y-hi, z-lo, z-hi: CMG_BC_DIRICHLET (ghost = 2*0 - inside,
+ * DiriBC order 1 with value 0, BCFunc.cpp:294-354) or CMG_BC_NEUMANN (ghost =
+ * inside, NeumBC with value 0, BCFunc.cpp:217-236), as the AMRINS projection's
+ * pressure BC function sets them (walls and inflow Neumann, outflow
+ * Dirichlet).  bc == NULL is Dirichlet everywhere.  With Neumann on every
+ * face the operator is singular; the solver runs as the reference's does. */
+#define CMG_BC_DIRICHLET 0
+#define CMG_BC_NEUMANN 1
+int cmg_hierarchy_create_bc(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
+                            const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta,
+                            const int bc[6], cmg_hierarchy** out);
 int cmg_hierarchy_destroy(cmg_hierarchy* h);
 
 /* Sizes of the per-level data arrays. */

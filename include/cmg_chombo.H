@@ -75,17 +75,22 @@ struct GpuOpDescription {
   Vector<int> refRatios;
   Real coarsedx = 0, alpha = 0, beta = 1;
   int vc = 0;
+  int bc[6] = {0, 0, 0, 0, 0, 0};  // per domain face: CMG_BC_DIRICHLET or CMG_BC_NEUMANN (probeBoundary)
   Vector<RefCountedPtr<LDF> > aCoef;
   Vector<RefCountedPtr<LevelData<FluxBox> > > bCoef;
   bool defined = false;
 };
 
-// Rejects every boundary condition but the homogeneous Dirichlet one the
-// device solve applies (ghost = 2*0 - inside, BCFunc.cpp:294-354 with value
-// 0, order 1): on a slab two cells deep along each domain face the BC is
-// called inhomogeneous on distinct cell values, and every ghost across that
-// face must be minus the cell next to it.
-inline void requireHomogeneousDirichlet(BCHolder a_bc, const ProblemDomain& a_domain, Real a_dx) {
+// The boundary type of every domain face of a_bc, which the device solve
+// supports when it is homogeneous Dirichlet (ghost = 2*0 - inside,
+// BCFunc.cpp:294-354 with value 0, order 1) or homogeneous Neumann (ghost =
+// inside, BCFunc.cpp:217-236 with value 0), as the drivers' ParseBC and the
+// AMRINS projection's pressure BC function set them: on a slab two cells deep
+// along each domain face the BC is called inhomogeneous on distinct cell
+// values, and every ghost across that face must be minus the cell next to it
+// (Dirichlet) or equal to it (Neumann).  Anything else stops with
+// MayDay::Error.
+inline void probeBoundary(BCHolder a_bc, const ProblemDomain& a_domain, Real a_dx, int a_types[6]) {
   const Box& d = a_domain.domainBox();
   for (int dir = 0; dir < SpaceDim; ++dir)
     for (SideIterator sit; sit.ok(); ++sit) {
@@ -104,10 +109,16 @@ inline void requireHomogeneousDirichlet(BCHolder a_bc, const ProblemDomain& a_do
       a_bc(fab, valid, a_domain, a_dx, false);
       const Box ghost = adjCellBox(valid, dir, sit(), 1);
       const IntVect in = (sit() == Side::Lo ? 1 : -1) * BASISV(dir);
-      for (BoxIterator bit(ghost); bit.ok(); ++bit)
-        if (fab(bit(), 0) != -fab(bit() + in, 0))
-          MayDay::Error("cmg_chombo: the device operators support homogeneous Dirichlet boundary conditions only "
-                        "(ghost = -inside on every domain face); this BCHolder sets something else");
+      bool diri = true, neu = true;
+      for (BoxIterator bit(ghost); bit.ok(); ++bit) {
+        diri = diri && fab(bit(), 0) == -fab(bit() + in, 0);
+        neu = neu && fab(bit(), 0) == fab(bit() + in, 0);
+      }
+      if (!diri && !neu)
+        MayDay::Error("cmg_chombo: the device operators support homogeneous Dirichlet (ghost = -inside) and "
+                      "homogeneous Neumann (ghost = inside) boundary conditions only; this BCHolder sets "
+                      "something else on a domain face");
+      a_types[2 * dir + (sit() == Side::Hi ? 1 : 0)] = diri ? CMG_BC_DIRICHLET : CMG_BC_NEUMANN;
     }
 }
 
@@ -576,8 +587,8 @@ class GpuHierarchy {
       lo[dir] = db.smallEnd(dir);
       hi[dir] = db.bigEnd(dir);
     }
-    check(cmg_hierarchy_create(lo, hi, d.coarsedx, m_nlev, counts.data(), boxes.data(), d.vc, d.alpha, d.beta,
-                               &m_h));
+    check(cmg_hierarchy_create_bc(lo, hi, d.coarsedx, m_nlev, counts.data(), boxes.data(), d.vc, d.alpha, d.beta,
+                                  d.bc, &m_h));
     if (d.vc) {
       std::vector<double> buf;
       for (int l = 0; l < m_nlev; ++l) {
@@ -655,7 +666,7 @@ class GpuOpFactoryBase : public AMRLevelOpFactory<LDF> {
     m_d = a_d;
     m_bc = a_bc;
     m_shared.reset();
-    requireHomogeneousDirichlet(a_bc, a_d.coarseDomain, a_d.coarsedx);
+    probeBoundary(a_bc, a_d.coarseDomain, a_d.coarsedx, m_d.bc);
   }
   int levelOf(const ProblemDomain& a_domain) const {
     if (!m_d.defined) MayDay::Error("cmg_chombo: factory not defined");

@@ -106,6 +106,7 @@ int main(int argc, char** argv) {
     if (!eq) continue;
     g_args[std::string(argv[a], eq - argv[a])] = std::string(eq + 1);
   }
+  if (g_args.count("bc")) setFaceBC(g_args["bc"]);
   const int n0 = argi("n0", 64);
   const int numLevels = argi("levels", 1);
   const int maxBox = argi("maxbox", 32);
@@ -192,11 +193,11 @@ int main(int argc, char** argv) {
   VCAMRPoissonOp2Factory* vf = NULL;
   if (opType == 0) {
     pf = new AMRPoissonOpFactory;
-    pf->define(domains[0], fgrids, rr, dxs[0], &dirichletBC, alpha, beta);
+    pf->define(domains[0], fgrids, rr, dxs[0], &domainBC, alpha, beta);
     factory = pf;
   } else {
     vf = new VCAMRPoissonOp2Factory;
-    vf->define(domains[0], fgrids, rr, dxs[0], &dirichletBC, alpha, aCoef, beta, bCoef);
+    vf->define(domains[0], fgrids, rr, dxs[0], &domainBC, alpha, aCoef, beta, bCoef);
     factory = vf;
   }
   AMRMultiGrid<LDF>* solver = new AMRMultiGrid<LDF>();
@@ -238,6 +239,7 @@ int main(int argc, char** argv) {
   FILE* js = std::fopen((out + ".json").c_str(), "w");
   std::fprintf(js, "{\n\"n0\": %d, \"levels\": %d, \"maxbox\": %d, \"block\": %d, \"fill\": %.17g,\n", n0,
                nlev, maxBox, blockFactor, fillRatio);
+  std::fprintf(js, "\"bc\": \"%s\",\n", faceBCString().c_str());
   std::fprintf(js, "\"op\": %d, \"alpha\": %.17g, \"beta\": %.17g, \"seed\": %llu, \"thresh\": %.17g,\n", opType,
                alpha, beta, seed, thresh);
   std::fprintf(js, "\"pre\": %d, \"post\": %d, \"bottom\": %d, \"iters\": %d, \"eps\": %.17g, \"hang\": %.17g,\n",

@@ -15,8 +15,10 @@
 // for the operator-by-operator comparison of the reference's operators with
 // the GPU AMRLevelOps; amrmg=1 for the reference's AMRMultiGrid over the
 // reference factory and over the GPU factory, amrmg=1 fas=1 for its
-// AMRFASMultiGrid the same way; neumann=1 hands a Neumann BC
-// to the GPU factory, which must refuse it)
+// AMRFASMultiGrid the same way; bc=<six letters D/N> sets the homogeneous
+// Dirichlet / Neumann type of each domain face; bcprobe=1 prints the face
+// types the GPU factory reads off that BC function; badbc=1 hands an
+// inhomogeneous Dirichlet BC to the GPU factory, which must refuse it)
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -71,11 +73,11 @@ static int bicgstabCheck(OracleProblem& P, Vector<LDF*>& phiGpu, Vector<int>& rr
   RefCountedPtr<AMRLevelOpFactory<LDF> > factory;
   if (P.opType == 0) {
     AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   } else {
     VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   }
   for (int l = 0; l < nlev; ++l)
@@ -100,11 +102,11 @@ static int bicgstabCheck(OracleProblem& P, Vector<LDF*>& phiGpu, Vector<int>& rr
   gop.m_num_mg_smooth = mgSmooth;
   if (P.opType == 0) {
     cmg_chombo::GpuAMRPoissonOpFactory f;
-    f.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     gop.define(P.grids, rr, P.domains, dxv, f, 0);
   } else {
     cmg_chombo::GpuVCAMRPoissonOp2Factory f;
-    f.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     gop.define(P.grids, rr, P.domains, dxv, f, 0);
   }
   cmg_chombo::GpuMultilevelBiCGStabSolver gpu;
@@ -152,11 +154,11 @@ static int heatCheck(OracleProblem& P, Vector<LDF*>& phiGpu, Vector<int>& rr, bo
   RefCountedPtr<AMRLevelOpFactory<LDF> > factory;
   if (P.opType == 0) {
     AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   } else {
     VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   }
   BiCGStabSolver<LDF> bottomSolver;
@@ -186,10 +188,10 @@ static int heatCheck(OracleProblem& P, Vector<LDF*>& phiGpu, Vector<int>& rr, bo
   cmg_chombo::GpuAMRPoissonOpFactory pf;
   cmg_chombo::GpuVCAMRPoissonOp2Factory vf;
   if (P.opType == 0) {
-    pf.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    pf.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     gpu->define(P.domains[0], pf, &gpuBottom, nlev);
   } else {
-    vf.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    vf.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     gpu->define(P.domains[0], vf, &gpuBottom, nlev);
   }
   gpu->setSolverParameters(pre, post, bottom, 1, 100, eps, hang, 1e-30);
@@ -323,20 +325,20 @@ static int opsCheck(OracleProblem& P, Vector<int>& rr) {
   RefCountedPtr<AMRLevelOpFactory<LDF> > refFactory;
   if (P.opType == 0) {
     AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     refFactory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   } else {
     VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     refFactory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   }
   cmg_chombo::GpuAMRPoissonOpFactory gpf;
   cmg_chombo::GpuVCAMRPoissonOp2Factory gvf;
   cmg_chombo::GpuOpFactoryBase* gpuFactory = &gpf;
   if (P.opType == 0)
-    gpf.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    gpf.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
   else {
-    gvf.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    gvf.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     gpuFactory = &gvf;
   }
   std::vector<AMRLevelOp<LDF>*> ro(nlev), go(nlev);
@@ -665,20 +667,20 @@ static int amrmgCheck(OracleProblem& P, Vector<int>& rr) {
   RefCountedPtr<AMRLevelOpFactory<LDF> > refFactory;
   if (P.opType == 0) {
     AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     refFactory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   } else {
     VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     refFactory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   }
   cmg_chombo::GpuAMRPoissonOpFactory gpf;
   cmg_chombo::GpuVCAMRPoissonOp2Factory gvf;
   AMRLevelOpFactory<LDF>* gpuFactory = &gpf;
   if (P.opType == 0)
-    gpf.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    gpf.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
   else {
-    gvf.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    gvf.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     gpuFactory = &gvf;
   }
   Vector<LDF*> phiG(nlev);
@@ -732,16 +734,17 @@ static int amrmgCheck(OracleProblem& P, Vector<int>& rr) {
   return 0;
 }
 
-// A Neumann boundary condition (ghost = inside) handed to the GPU factory:
-// define() must stop with MayDay::Error, which aborts this program.
-static void neumannBC(FArrayBox& a_state, const Box& a_valid, const ProblemDomain& a_domain, Real a_dx,
-                      bool a_homogeneous) {
+// An inhomogeneous Dirichlet boundary condition (value 1 on every face,
+// ghost = 2*1 - inside) handed to the GPU factory: define() must stop with
+// MayDay::Error, which aborts this program.
+static void oneValue(Real*, int*, Side::LoHiSide*, Real* a_values) { a_values[0] = 1.; }
+static void inhomDirichletBC(FArrayBox& a_state, const Box& a_valid, const ProblemDomain& a_domain, Real a_dx,
+                             bool a_homogeneous) {
   for (int i = 0; i < CH_SPACEDIM; ++i)
     for (SideIterator sit; sit.ok(); ++sit) {
       Box g = adjCellBox(a_valid, i, sit(), 1);
       if (a_domain.domainBox().contains(g)) continue;
-      const IntVect in = (sit() == Side::Lo ? 1 : -1) * BASISV(i);
-      for (BoxIterator bit(g); bit.ok(); ++bit) a_state(bit(), 0) = a_state(bit() + in, 0);
+      DiriBC(a_state, a_valid, a_dx, a_homogeneous, oneValue, i, sit(), 1);
     }
 }
 
@@ -750,6 +753,7 @@ int main(int argc, char** argv) {
     const char* eq = std::strchr(argv[a], '=');
     if (eq) g_args[std::string(argv[a], eq - argv[a])] = std::string(eq + 1);
   }
+  if (g_args.count("bc")) setFaceBC(g_args["bc"]);
   OracleProblem P;
   P.n0 = (int)argd("n0", 16);
   P.numLevels = (int)argd("levels", 3);
@@ -773,10 +777,17 @@ int main(int argc, char** argv) {
   if (argd("fineinterp", 0) != 0) return fineInterpCheck(P, argd("fineinterp", 0) == 2);
   if (argd("ops", 0) != 0) return opsCheck(P, rr);
   if (argd("amrmg", 0) != 0) return amrmgCheck(P, rr);
-  if (argd("neumann", 0) != 0) {
+  if (argd("badbc", 0) != 0) {
     cmg_chombo::GpuAMRPoissonOpFactory f;
-    f.define(P.domains[0], P.grids, rr, P.dxs[0], &neumannBC, P.alpha, P.beta);
-    std::printf("{\"neumann_accepted\": true}\n");
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &inhomDirichletBC, P.alpha, P.beta);
+    std::printf("{\"inhomogeneous_accepted\": true}\n");
+    return 0;
+  }
+  if (argd("bcprobe", 0) != 0) {  // the face types the GPU factory reads off the problem's BC function
+    cmg_chombo::GpuAMRPoissonOpFactory f;
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
+    const int* t = f.description().bc;
+    std::printf("{\"bc_types\": [%d, %d, %d, %d, %d, %d]}\n", t[0], t[1], t[2], t[3], t[4], t[5]);
     return 0;
   }
 
@@ -784,11 +795,11 @@ int main(int argc, char** argv) {
   RefCountedPtr<AMRLevelOpFactory<LDF> > factory;
   if (P.opType == 0) {
     AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   } else {
     VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   }
   BiCGStabSolver<LDF> bottomSolver;
@@ -808,11 +819,11 @@ int main(int argc, char** argv) {
   BiCGStabSolver<LDF> gpuBottom;
   if (P.opType == 0) {
     cmg_chombo::GpuAMRPoissonOpFactory f;
-    f.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     gpu.define(P.domains[0], f, &gpuBottom, nlev);
   } else {
     cmg_chombo::GpuVCAMRPoissonOp2Factory f;
-    f.define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    f.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     gpu.define(P.domains[0], f, &gpuBottom, nlev);
   }
   gpu.setSolverParameters(pre, post, bottom, 1, iters, eps, hang, 1e-30);

@@ -55,6 +55,7 @@ int main(int argc, char** argv) {
     const char* eq = std::strchr(argv[a], '=');
     if (eq) g_args[std::string(argv[a], eq - argv[a])] = std::string(eq + 1);
   }
+  if (g_args.count("bc")) setFaceBC(g_args["bc"]);
   OracleProblem P;
   P.n0 = argi("n0", 32);
   P.numLevels = argi("levels", 1);
@@ -78,11 +79,11 @@ int main(int argc, char** argv) {
   AMRLevelOpFactory<LDF>* factory = NULL;
   if (P.opType == 0) {
     AMRPoissonOpFactory* f = new AMRPoissonOpFactory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     factory = f;
   } else {
     VCAMRPoissonOp2Factory* f = new VCAMRPoissonOp2Factory;
-    f->define(P.domains[0], P.grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     factory = f;
   }
   BiCGStabSolver<LDF> bottomSolver;

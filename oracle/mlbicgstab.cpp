@@ -47,6 +47,7 @@ int main(int argc, char** argv) {
     const char* eq = std::strchr(argv[a], '=');
     if (eq) g_args[std::string(argv[a], eq - argv[a])] = std::string(eq + 1);
   }
+  if (g_args.count("bc")) setFaceBC(g_args["bc"]);
   OracleProblem P;
   P.n0 = argi("n0", 32);
   P.numLevels = argi("levels", 1);
@@ -77,11 +78,11 @@ int main(int argc, char** argv) {
   RefCountedPtr<AMRLevelOpFactory<LDF> > factory;
   if (P.opType == 0) {
     AMRPoissonOpFactory* pf = new AMRPoissonOpFactory;
-    pf->define(domains[0], grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.beta);
+    pf->define(domains[0], grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(pf);
   } else {
     VCAMRPoissonOp2Factory* vf = new VCAMRPoissonOp2Factory;
-    vf->define(domains[0], grids, rr, P.dxs[0], &dirichletBC, P.alpha, P.aCoef, P.beta, P.bCoef);
+    vf->define(domains[0], grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(vf);
   }
   // Zero initial guess, ghost cells included (VCPoissonSolve.cpp:131-134).

@@ -39,17 +39,34 @@ typedef LevelData<FArrayBox> LDF;
 // the reference driver's ParseBC (execCell/poissonSolve.cpp:76-119).
 static void zeroValue(Real*, int*, Side::LoHiSide*, Real* a_values) { a_values[0] = 0.; }
 
-static void dirichletBC(FArrayBox& a_state, const Box& a_valid, const ProblemDomain& a_domain,
-                        Real a_dx, bool a_homogeneous) {
+// Homogeneous boundary type of each domain face (x-lo, x-hi, y-lo, y-hi,
+// z-lo, z-hi): 0 Dirichlet (the examples' ParseBC), 1 Neumann (walls and
+// inflow in the AMRINS projection's pressure BC function,
+// releasedExamples/AMRINS/BCutil/PhysBCUtil.cpp:427-473).  Set from the
+// bc=<six letters D/N> argument.
+static int g_faceBC[6] = {0, 0, 0, 0, 0, 0};
+static void setFaceBC(const std::string& a_s) {
+  for (int f = 0; f < 6; ++f) g_faceBC[f] = (f < (int)a_s.size() && a_s[f] == 'N') ? 1 : 0;
+}
+static std::string faceBCString() {
+  std::string s;
+  for (int f = 0; f < 6; ++f) s += g_faceBC[f] ? 'N' : 'D';
+  return s;
+}
+
+static void domainBC(FArrayBox& a_state, const Box& a_valid, const ProblemDomain& a_domain,
+                     Real a_dx, bool a_homogeneous) {
   if (!a_domain.domainBox().contains(a_state.box())) {
     for (int i = 0; i < CH_SPACEDIM; ++i) {
       if (!a_domain.isPeriodic(i)) {
-        Box lo = adjCellBox(a_valid, i, Side::Lo, 1);
-        Box hi = adjCellBox(a_valid, i, Side::Hi, 1);
-        if (!a_domain.domainBox().contains(lo))
-          DiriBC(a_state, a_valid, a_dx, true, zeroValue, i, Side::Lo, 1);
-        if (!a_domain.domainBox().contains(hi))
-          DiriBC(a_state, a_valid, a_dx, true, zeroValue, i, Side::Hi, 1);
+        for (SideIterator sit; sit.ok(); ++sit) {
+          Box g = adjCellBox(a_valid, i, sit(), 1);
+          if (a_domain.domainBox().contains(g)) continue;
+          if (g_faceBC[2 * i + (sit() == Side::Hi ? 1 : 0)])
+            NeumBC(a_state, a_valid, a_dx, true, zeroValue, i, sit());
+          else
+            DiriBC(a_state, a_valid, a_dx, true, zeroValue, i, sit(), 1);
+        }
       }
     }
   }

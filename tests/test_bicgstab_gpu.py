@@ -28,7 +28,7 @@ def params(cmg, meta):
 def test_bicgstab_matches_reference(cmg, name):
     meta, arrays = golden(name)
     base, _ = golden(meta["base"])
-    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"])
+    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"], bc=base.get("bc"))
     h.fill_synthetic(base["seed"])
     out = h.solve_bicgstab(params(cmg, meta))
     r0 = meta["initial_residual"]
@@ -56,7 +56,7 @@ def test_bicgstab_from_current_phi(cmg):
     """zero_phi=False starts from the phi in place: a converged phi converges again at once."""
     meta, _ = golden("bicgstab_vc_3lev_16")
     base, _ = golden(meta["base"])
-    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"])
+    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"], bc=base.get("bc"))
     h.fill_synthetic(base["seed"])
     p = params(cmg, meta)
     first = h.solve_bicgstab(p)
@@ -70,7 +70,7 @@ def test_bicgstab_graph_replay_is_bit_identical(cmg):
     """Each preconditioner call replayed from a captured CUDA graph gives the same bits as launching it."""
     meta, _ = golden("bicgstab_vc_3lev_16")
     base, _ = golden(meta["base"])
-    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"])
+    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"], bc=base.get("bc"))
     h.fill_synthetic(base["seed"])
     p = params(cmg, meta)
     plain = h.solve_bicgstab(p)

@@ -17,7 +17,7 @@ def test_device_inputs_match_host_inputs(cmg, name):
     nlev = len(meta["boxes"])
     res = []
     for device in (False, True):
-        h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+        h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"], bc=meta.get("bc"))
         h.fill_synthetic(meta["seed"], device=device)
         rhs = [h.get_rhs(l) for l in range(nlev)]
         out = h.solve(p)

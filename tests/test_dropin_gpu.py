@@ -110,6 +110,9 @@ OPS_CASES = {
     "vc_3lev_16": "n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=-1",
     "poisson_3lev_32": "n0=32 levels=3 maxbox=16 block=4 op=0 alpha=0 beta=1",
     "helmholtz_2lev_16": "n0=16 levels=2 maxbox=8 block=4 op=0 alpha=1 beta=-1",
+    # Neumann walls with a Dirichlet outflow face (the AMRINS projection's pressure BC) and mixed faces
+    "poisson_3lev_32_walls": "n0=32 levels=3 maxbox=16 block=4 op=0 alpha=0 beta=1 bc=NNNNND",
+    "vc_3lev_16_walls": "n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=-1 bc=NDNDNN",
 }
 
 

@@ -14,7 +14,7 @@ from test_fineinterp import CASES, coarse_input
 def setup(cmg, name):
     meta, arrays = golden(name)
     base, _ = golden(meta["base"])
-    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"])
+    h = cmg.Hierarchy(base["n0"], base["boxes"], op=base["op"], alpha=base["alpha"], beta=base["beta"], bc=base.get("bc"))
     lev = meta["level"]
     c = coarse_input(meta, base)
     if c is None:

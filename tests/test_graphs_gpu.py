@@ -11,7 +11,7 @@ from conftest import golden
 
 def make(cmg, name):
     meta, _ = golden(name)
-    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"], bc=meta.get("bc"))
     h.fill_synthetic(meta["seed"])
     p = cmg.solve_params(pre=meta["pre"], post=meta["post"], bottom=meta["bottom"], iter_max=meta["iters"],
                          eps=meta["eps"], hang=meta["hang"])
@@ -49,7 +49,8 @@ def test_graph_replay_is_bit_identical(cmg, name, mixed):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,num_mg", [("vc_3lev_16", 1), ("poisson_3lev_32", 1), ("helmholtz_2lev_16", 1),
-                                         ("vc_3lev_16", 2), ("poisson_1lev_32", 1), ("vc_1lev_32", 2)])
+                                         ("vc_3lev_16", 2), ("poisson_1lev_32", 1), ("vc_1lev_32", 2),
+                                         ("poisson_3lev_32_walls", 1), ("vc_3lev_16_walls", 2)])
 def test_relaxation_variants_are_bit_identical(cmg, name, num_mg):
     """Ghost fill before each colour pass (mode 1), face ghosts evaluated in
     the pass (mode 2), fused sweeps (mode 3: both colours per launch, boxes
@@ -73,7 +74,7 @@ def test_relaxation_variants_are_bit_identical(cmg, name, num_mg):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["config1_vc_3lev_128", "vc_3lev_32"])
+@pytest.mark.parametrize("name", ["config1_vc_3lev_128", "vc_3lev_32", "poisson_3lev_16_walls"])
 def test_fused_sweeps_match_reference(cmg, name):
     """Every level relaxed with fused sweeps (mode 3) reproduces the reference solve bit for bit."""
     meta, arrays = golden(name)

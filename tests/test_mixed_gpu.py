@@ -21,7 +21,7 @@ TOL_COVERED = 1e-6
 @pytest.mark.parametrize("name", golden_names())
 def test_mixed_matches_fp64_reference(cmg, name):
     meta, arrays = golden(name)
-    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"], bc=meta.get("bc"))
     h.fill_synthetic(meta["seed"])
     p = cmg.solve_params(pre=meta["pre"], post=meta["post"], bottom=meta["bottom"], iter_max=meta["iters"],
                          eps=meta["eps"], hang=meta["hang"])

@@ -15,7 +15,7 @@ TOL = 1e-12
 
 
 def solve_case(cmg, meta):
-    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"], bc=meta.get("bc"))
     h.fill_synthetic(meta["seed"])
     p = cmg.solve_params(pre=meta["pre"], post=meta["post"], bottom=meta["bottom"], iter_max=meta["iters"],
                          eps=meta["eps"], hang=meta["hang"])

@@ -100,7 +100,7 @@ def test_nan_right_hand_side_reports_divergence(cmg):
     """cmg_solve on a right-hand side holding a NaN: the max norm propagates the NaN (it is not dropped as a
     max over doubles would), the solve stops with CMG_EDIVERGED and writes its outputs."""
     meta, _ = golden("vc_3lev_16")
-    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"], bc=meta.get("bc"))
     h.fill_synthetic(meta["seed"])
     rhs = h.get_rhs(2)
     rhs[len(rhs) // 2] = np.nan

@@ -15,7 +15,7 @@ TOL = 1e-14
 
 def hierarchy(cmg, name):
     meta, _ = golden(name)
-    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+    h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"], bc=meta.get("bc"))
     h.fill_synthetic(meta["seed"])
     return h, meta
 

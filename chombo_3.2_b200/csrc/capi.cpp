@@ -328,6 +328,22 @@ int cmg_set_relax_mode(cmg_hierarchy* h, int mode) {
   });
 }
 
+int cmg_set_bottom_solver(cmg_hierarchy* h, const cmg_bottom_params* p) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (!p) throw std::invalid_argument("cmg: null argument");
+    cmg::BottomConfig c;
+    c.kind = p->kind;
+    c.imax = p->imax;
+    c.numRestarts = p->num_restarts;
+    c.normType = p->norm_type;
+    c.eps = p->eps;
+    c.hang = p->hang;
+    c.small = p->small;
+    h->solver->setBottomConfig(c);
+  });
+}
+
 int cmg_relax_variants(cmg_hierarchy* h, int* inline_out, float* ms_fill, float* ms_inline, int cap, int* n) {
   return guard([&]() {
     needLevel(h, 0);

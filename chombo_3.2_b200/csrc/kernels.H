@@ -147,7 +147,17 @@ template <class T> void maxNorm(const LevelDev& L, const T* f, double* out, cuda
 // (BottomPlan): slot tables, vectors r, r~, e, p, p~, s~, t, v, phi, rhs
 // (nv + ng doubles each), the compact coefficients of a variable-coefficient
 // operator, and a 2-int status (exit, iterations).
+// Which bottom solver runs and its public parameters: BiCGStabSolver
+// (BiCGStabSolver.H:165-182 defaults; its eps comes from the multigrid
+// solver's convergence metrics) or RelaxSolver (RelaxSolver.H:104-112
+// defaults, its own eps).  normType 2 or 0.
+struct BottomConfig {
+  int kind = 0;  // 0 BiCGStabSolver, 1 RelaxSolver
+  int imax = 80, numRestarts = 5, normType = 2;
+  double eps = 1e-6, hang = 1e-8, small = 1e-30, reps = 1e-12;
+};
 struct BottomWork {
+  BottomConfig cfg;
   int nv = 0, ng = 0, nbox = 0, ncol[2] = {0, 0};
   const int *fab = nullptr, *nb = nullptr, *col[2] = {nullptr, nullptr}, *boxStart = nullptr;
   const int *gsrc = nullptr, *gkind = nullptr;

@@ -983,6 +983,57 @@ __device__ double blkDot(const BottomArgs& A, const double* x, const double* y, 
 
 __device__ double blkNorm(const BottomArgs& A, const double* x) { return sqrt(blkDot(A, x, x, true)); }
 
+// The norm of type A.W.cfg.normType: 2 as above, 0 the largest |x| (a max,
+// so its order does not matter; NaN propagates).
+__device__ double blkNormType(const BottomArgs& A, const double* x) {
+  if (A.W.cfg.normType == 2) return blkNorm(A, x);
+  __shared__ double m;
+  if (threadIdx.x == 0) m = 0.0;
+  __syncthreads();
+  double v = 0.0;
+  for (int q = threadIdx.x; q < A.W.nv; q += blockDim.x) v = nanMax(v, fabs(x[q]));
+  for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMaxPos(&m, v);
+  __syncthreads();
+  const double r = m;
+  __syncthreads();
+  return r;
+}
+
+// RelaxSolver<T>::solve (AMRElliptic/RelaxSolver.H:128-186): repeated
+// preconditioner corrections e = preCond(r), phi += e, until the residual
+// norm falls below eps times the initial one, imax iterations or a hang.
+__device__ void relaxSolve(const BottomArgs& A) {
+  const BottomWork& W = A.W;
+  const int nc = W.nv + W.ng;
+  auto zeroAll = [&](double* x) {
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) x[q] = 0.0;
+    __syncthreads();
+  };
+  zeroAll(A.r);
+  blkOp(A, A.r, A.phi, A.rhs, 0);
+  double norm = blkNormType(A, A.r);
+  double minNorm = norm;
+  int iter = 0;
+  if (norm > 0.) {
+    const double initialNorm = norm;
+    while (iter < W.cfg.imax) {
+      zeroAll(A.e);
+      blkPrecond(A, A.e, A.r);
+      blkCells(A, [&](int q) { A.phi[q] = A.phi[q] + A.e[q] * 1.0; });
+      blkOp(A, A.r, A.phi, A.rhs, 0);
+      norm = blkNormType(A, A.r);
+      iter++;
+      if (norm < W.cfg.eps * initialNorm) break;
+      if (norm < minNorm)
+        minNorm = norm;
+      else if (norm * W.cfg.hang > minNorm)
+        break;
+    }
+  }
+  if (threadIdx.x == 0) W.status[0] = 0, W.status[1] = iter;
+}
+
 __device__ void bicgstab(const BottomArgs& A) {
   const BottomWork& W = A.W;
   const int nc = W.nv + W.ng;
@@ -1001,7 +1052,7 @@ __device__ void bicgstab(const BottomArgs& A) {
   int iter = 0, recount = 0, restarts = 0, status = 0;
   double rho[4] = {0, 0, 0, 0};
   double norm[2];
-  norm[0] = blkNorm(A, A.r);
+  norm[0] = blkNormType(A, A.r);
   double initial_norm = norm[0];
   const double initial_residual = norm[0];
   norm[1] = norm[0];
@@ -1039,7 +1090,7 @@ __device__ void bicgstab(const BottomArgs& A) {
     alpha[0] = rho[1] / m;
     if (fabs(m) > A.small * fabs(rho[1])) {
       incrV(A.r, A.v, -alpha[0]);
-      norm[0] = blkNorm(A, A.r);
+      norm[0] = blkNormType(A, A.r);
       incrV(A.e, A.pt, alpha[0]);
     } else {
       zeroAll(A.r);
@@ -1054,7 +1105,7 @@ __device__ void bicgstab(const BottomArgs& A) {
       omega[0] = tr / tt;
       incrV(A.e, A.st, omega[0]);
       incrV(A.r, A.t, -omega[0]);
-      norm[0] = blkNorm(A, A.r);
+      norm[0] = blkNormType(A, A.r);
     }
     if (norm[0] <= A.eps * initial_norm || norm[0] <= A.reps * initial_residual) {
       status = 1;
@@ -1071,7 +1122,7 @@ __device__ void bicgstab(const BottomArgs& A) {
           return;
         }
         blkOp(A, A.r, A.phi, A.rhs, 0);
-        norm[0] = blkNorm(A, A.r);
+        norm[0] = blkNormType(A, A.r);
         rho[1] = 0.0;
         rho[2] = 0.0;
         rho[3] = 0.0;
@@ -1097,7 +1148,10 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs A) {
     A.rhs[q] = A.rhsFab[W.fab[q]];
   }
   __syncthreads();
-  bicgstab(A);
+  if (W.cfg.kind == 1)
+    relaxSolve(A);
+  else
+    bicgstab(A);
   __syncthreads();
   for (int q = threadIdx.x; q < W.nv; q += blockDim.x) A.phiFab[W.fab[q]] = A.phi[q];
 }
@@ -1432,13 +1486,13 @@ void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<d
   A.v = w.v[7];
   A.phi = w.v[8];
   A.rhs = w.v[9];
-  A.eps = eps;
+  A.eps = w.cfg.kind == 1 ? w.cfg.eps : eps;  // RelaxSolver keeps its own tolerance
   A.metric = metric;
-  A.reps = 1.0e-12;
-  A.hang = 1e-8;
-  A.small = 1.0e-30;
-  A.imax = 80;
-  A.numRestarts = 5;
+  A.reps = w.cfg.reps;
+  A.hang = w.cfg.hang;
+  A.small = w.cfg.small;
+  A.imax = w.cfg.imax;
+  A.numRestarts = w.cfg.numRestarts;
   // AMRPoissonOp::preCond multiplier (AMRPoissonOp.cpp:304-329).
   A.mult = 1.0 / (c.alpha - 2.0 * 3 * c.beta / (L.dx * L.dx));
   k_bottom<<<1, 1024, w.nbox * sizeof(double), s>>>(A);

@@ -169,6 +169,9 @@ class Solver {
   // 1 ghost fill before every colour pass, 2 face ghosts evaluated inside the
   // pass.  All three give identical results.
   void setRelaxMode(int mode);
+  // The bottom solver of the multigrid levels below level 0 (BottomConfig).
+  void setBottomConfig(const BottomConfig& c);
+  const BottomConfig& bottomConfig() const { return bottom_.cfg; }
   // The variant of every AMR level then every multigrid depth (1: inline),
   // and the tuner's sweep times (ms; empty when a mode was forced).
   void relaxVariants(std::vector<int>& inl, std::vector<float>& msFill, std::vector<float>& msInline);

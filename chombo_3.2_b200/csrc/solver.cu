@@ -862,6 +862,18 @@ std::vector<SolveResult> Solver::tga(const SolveParams& p, double dt, int nsteps
   return out;
 }
 
+void Solver::setBottomConfig(const BottomConfig& c) {
+  if (c.kind != 0 && c.kind != 1) throw std::invalid_argument("cmg: bottom solver is BiCGStab (0) or relaxation (1)");
+  if (c.normType != 0 && c.normType != 2) throw std::invalid_argument("cmg: bottom solver norm type is 0 or 2");
+  if (c.imax < 0 || c.numRestarts < 0) throw std::invalid_argument("cmg: negative bottom solver iteration limit");
+  bottom_.cfg = c;
+  // captured bottom launches hold the old parameters
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  graphs_.clear();
+  for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
+  precondGraphs_.clear();
+}
+
 void Solver::setRelaxMode(int mode) {
   if (mode < 0 || mode > 3)
     throw std::invalid_argument("cmg: relaxation mode is 0 (tuned), 1 (fills), 2 (inline) or 3 (fused sweeps)");

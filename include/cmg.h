@@ -124,12 +124,30 @@ int cmg_use_graphs(cmg_hierarchy* h, int on);
 /* Relaxation variant (no counterpart in the reference): 0 = chosen per level
  * by a timing autotuner before the first solve (default); 1 = ghost fill
  * (exchange, boundary and coarse-fine values) before each colour pass, as the
- * reference's levelGSRB; 2 = the neighbours beyond each box evaluated inside
- * the pass from the same fill rules, no fill; 3 = fused sweeps: both colours
+ * reference's levelGSRB; 2 = no separate fill: every block of a colour pass
+ * first writes the face ghosts its own cells read (the same fill entries),
+ * then updates its cells; 3 = fused sweeps: both colours
  * of a sweep in one launch (every box marching through its z slabs, the
  * colour-1 cells on faces shared with another box in a second launch), no
  * fill.  Identical results. */
 int cmg_set_relax_mode(cmg_hierarchy* h, int mode);
+
+/* The bottom solver of the deepest multigrid level, as the LinearSolver
+ * AMRMultiGrid::define is given: CMG_BOTTOM_BICGSTAB (BiCGStabSolver,
+ * BiCGStabSolver.H:199-515; the default, with its defaults imax 80,
+ * num_restarts 5, norm_type 2, hang 1e-8, small 1e-30; its tolerance is the
+ * one the multigrid solve hands it, so eps is not read) or CMG_BOTTOM_RELAX
+ * (RelaxSolver, RelaxSolver.H:128-186: imax corrections by the operator's
+ * preconditioner, stopping below eps times the initial residual norm or on a
+ * hang; its defaults imax 40, norm_type 2, eps 1e-6, hang 0, the bottom of the
+ * AMRINS projection solves).  norm_type 2 or 0. */
+#define CMG_BOTTOM_BICGSTAB 0
+#define CMG_BOTTOM_RELAX 1
+typedef struct cmg_bottom_params {
+  int kind, imax, num_restarts, norm_type;
+  double eps, hang, small;
+} cmg_bottom_params;
+int cmg_set_bottom_solver(cmg_hierarchy* h, const cmg_bottom_params* p);
 /* The relaxation variant of every AMR level, then every multigrid depth
  * (0 = ghost fills, 1 = in-pass ghosts, 2 = all sweeps in one one-block
  * launch, for levels of at most 32768 cells, 3 = fused sweeps), with the autotuner's times in

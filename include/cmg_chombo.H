@@ -18,14 +18,17 @@
 // Scope, each checked with MayDay::Error like the reference's own checks:
 //   - refinement ratio 2 between all levels, non-periodic domain, serial
 //     (every box local), one component;
-//   - homogeneous Dirichlet boundary conditions on the domain faces (the
-//     examples' ParseBC with value 0, order 1).  The factories' define()
+//   - homogeneous Dirichlet or homogeneous Neumann boundary conditions, one
+//     type per domain face (the examples' ParseBC with value 0, order 1; the
+//     AMRINS projection's walls and outflow).  The factories' define()
 //     probes the BCHolder: on a two-cell slab along each of the six domain
 //     faces it calls the BC (inhomogeneous) and requires every face ghost to
-//     be minus the cell inside it; any other condition (Neumann, a non-zero
-//     Dirichlet value, a higher-order stencil) is rejected there;
-//   - the bottom solver must be a BiCGStabSolver (its device restatement runs
-//     with the reference's default parameters);
+//     be minus the cell inside it (Dirichlet) or equal to it (Neumann); any
+//     other condition (a non-zero value, a higher-order stencil) is rejected
+//     there;
+//   - the bottom solver is a BiCGStabSolver or a RelaxSolver; its public
+//     parameters (m_imax, m_numRestarts, m_normType 2 or 0, m_eps of the
+//     RelaxSolver, m_hang, m_small) are read when each solve starts;
 //   - solve over all levels: l_base = 0 and l_max = numLevels - 1.
 // Only valid cells of phi are written; ghost cells are left as they were.
 //
@@ -61,6 +64,7 @@
 #include "MayDay.H"
 #include "ProblemDomain.H"
 #include "RealVect.H"
+#include "RelaxSolver.H"
 #include "RefCountedPtr.H"
 #include "cmg.h"
 
@@ -796,6 +800,7 @@ class GpuAMRMultiGrid : private GpuHierarchy {
     setLevels(a_rhs, false);
     if (!a_zeroPhi) setLevels(a_phi, true);
     const cmg_solve_params p = params();
+    applyBottom();
     m_history.assign(std::max(p.iter_max, p.iter_min) + 2, 0.0);
     int st = 0, it = 0, hl = 0;
     const int rc = cmg_solve(m_h, &p, a_zeroPhi ? 1 : 0, &st, &it, m_history.data(), (int)m_history.size(), &hl);
@@ -854,10 +859,33 @@ class GpuAMRMultiGrid : private GpuHierarchy {
 
   void defineWith(const ProblemDomain& a_coarseDomain, const GpuOpDescription& d, LinearSolver<LDF>* a_bottom,
                   int a_numLevels) {
-    if (a_bottom && !dynamic_cast<BiCGStabSolver<LDF>*>(a_bottom))
-      MayDay::Error("GpuAMRMultiGrid: the device solve uses BiCGStab as its bottom solver");
+    if (a_bottom && !dynamic_cast<BiCGStabSolver<LDF>*>(a_bottom) && !dynamic_cast<RelaxSolver<LDF>*>(a_bottom))
+      MayDay::Error("GpuAMRMultiGrid: the device bottom solver is a BiCGStabSolver or a RelaxSolver");
+    m_bottomSolver = a_bottom;
     defineFrom(a_coarseDomain, d, a_numLevels);
   }
+
+  // The bottom solver's public parameters, read when a solve starts (as the
+  // reference reads them inside its solve).
+  void applyBottom() {
+    cmg_bottom_params b = {CMG_BOTTOM_BICGSTAB, 80, 5, 2, 1e-6, 1e-8, 1e-30};
+    if (BiCGStabSolver<LDF>* s = dynamic_cast<BiCGStabSolver<LDF>*>(m_bottomSolver)) {
+      b.imax = s->m_imax;
+      b.num_restarts = s->m_numRestarts;
+      b.norm_type = s->m_normType;
+      b.hang = s->m_hang;
+      b.small = s->m_small;
+    } else if (RelaxSolver<LDF>* r = dynamic_cast<RelaxSolver<LDF>*>(m_bottomSolver)) {
+      b.kind = CMG_BOTTOM_RELAX;
+      b.imax = r->m_imax;
+      b.num_restarts = 0;
+      b.norm_type = r->m_normType;
+      b.eps = r->m_eps;
+      b.hang = r->m_hang;
+    }
+    check(cmg_set_bottom_solver(m_h, &b));
+  }
+  LinearSolver<LDF>* m_bottomSolver = nullptr;
 };
 
 // The reference's heat solvers over the GPU solve: BackwardEuler

@@ -35,6 +35,7 @@
 #include "FineInterp.H"
 #include "MultilevelLinearOp.H"
 #include "QuadCFInterp.H"
+#include "RelaxSolver.H"
 #include "VCAMRPoissonOp2.H"
 #include "cmg_chombo.H"
 #include "problem.H"
@@ -651,6 +652,20 @@ static int opsCheck(OracleProblem& P, Vector<int>& rr) {
   return 0;
 }
 
+// The bottom solver the multigrid solves are given: the reference's
+// BiCGStabSolver, or with relaxbottom=1 its RelaxSolver (the AMRINS
+// projection's bottom solver, CCProjector.cpp:1056-1058), defaults kept.
+static LinearSolver<LDF>* newBottom() {
+  if (argd("relaxbottom", 0) != 0) {
+    RelaxSolver<LDF>* r = new RelaxSolver<LDF>;
+    r->m_verbosity = 0;
+    return r;
+  }
+  BiCGStabSolver<LDF>* b = new BiCGStabSolver<LDF>;
+  b->m_verbosity = 0;
+  return b;
+}
+
 // The reference's own AMRMultiGrid (or, with fas=1, its AMRFASMultiGrid in
 // V-cycle mode), unmodified, defined once with the reference's factory and
 // once with the GPU factory (cmg_chombo's AMRLevelOpFactory, whose operators
@@ -691,11 +706,10 @@ static int amrmgCheck(OracleProblem& P, Vector<int>& rr) {
   ResidualRecorder* recs[2];
   int exitS[2], itersDone[2];
   for (int side = 0; side < 2; ++side) {
-    BiCGStabSolver<LDF> bottomSolver;
-    bottomSolver.m_verbosity = 0;
+    LinearSolver<LDF>* bottomSolver = newBottom();
     AMRFASMultiGrid<LDF>* fmg = fas ? new AMRFASMultiGrid<LDF> : nullptr;
     AMRMultiGrid<LDF>* mg = fas ? fmg : new AMRMultiGrid<LDF>;
-    mg->define(P.domains[0], side == 0 ? *refFactory : *gpuFactory, &bottomSolver, nlev);
+    mg->define(P.domains[0], side == 0 ? *refFactory : *gpuFactory, bottomSolver, nlev);
     mg->setSolverParameters(pre, post, bottom, 1, iters, eps, hang, 1e-30);
     mg->m_verbosity = 0;
     RefCountedPtr<AMRMultiGridInspector<LDF> > insp(new ResidualRecorder);
@@ -707,6 +721,7 @@ static int amrmgCheck(OracleProblem& P, Vector<int>& rr) {
     exitS[side] = mg->m_exitStatus;
     insp.neverDelete();
     delete mg;
+    delete bottomSolver;
   }
   const bool sameLen = recs[0]->norms.size() == recs[1]->norms.size();
   bool histExact = sameLen;
@@ -802,10 +817,9 @@ int main(int argc, char** argv) {
     f->define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.aCoef, P.beta, P.bCoef);
     factory = RefCountedPtr<AMRLevelOpFactory<LDF> >(f);
   }
-  BiCGStabSolver<LDF> bottomSolver;
-  bottomSolver.m_verbosity = 0;
+  LinearSolver<LDF>* bottomSolver = newBottom();
   AMRMultiGrid<LDF> cpu;
-  cpu.define(P.domains[0], *factory, &bottomSolver, nlev);
+  cpu.define(P.domains[0], *factory, bottomSolver, nlev);
   cpu.setSolverParameters(pre, post, bottom, 1, iters, eps, hang, 1e-30);
   cpu.m_verbosity = 0;
   RefCountedPtr<AMRMultiGridInspector<LDF> > insp(new ResidualRecorder);
@@ -816,7 +830,8 @@ int main(int argc, char** argv) {
 
   // The same calls on the GPU drop-in.
   cmg_chombo::GpuAMRMultiGrid gpu;
-  BiCGStabSolver<LDF> gpuBottom;
+  LinearSolver<LDF>* gpuBottomPtr = newBottom();
+  LinearSolver<LDF>& gpuBottom = *gpuBottomPtr;
   if (P.opType == 0) {
     cmg_chombo::GpuAMRPoissonOpFactory f;
     f.define(P.domains[0], P.grids, rr, P.dxs[0], &domainBC, P.alpha, P.beta);

@@ -21,6 +21,12 @@ CASES = {
     "poisson_3lev_16": "n0=16 levels=3 maxbox=8 block=4 op=0 alpha=0 beta=1",
     "helmholtz_2lev_16": "n0=16 levels=2 maxbox=8 block=4 op=0 alpha=1 beta=-1",
     "vc_1lev_32": "n0=32 levels=1 maxbox=16 op=1 alpha=1 beta=-1",
+    # the AMRINS projection's solves (CCProjector::defineMultiGrid, CCProjector.cpp:1872-1957): a composite
+    # Poisson problem with AMRPoissonOpFactory, Neumann walls and a Dirichlet outflow face, a RelaxSolver bottom
+    # and m_eps 1e-10
+    "projection_3lev_32": "n0=32 levels=3 maxbox=16 block=4 op=0 alpha=0 beta=1 bc=NNNNND relaxbottom=1 eps=1e-10",
+    "projection_2lev_16_relax": "n0=16 levels=2 maxbox=8 block=4 op=0 alpha=0 beta=1 bc=NDNNNN relaxbottom=1",
+    "vc_3lev_16_walls": "n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=-1 bc=NDNDNN",
 }
 
 
@@ -113,6 +119,7 @@ OPS_CASES = {
     # Neumann walls with a Dirichlet outflow face (the AMRINS projection's pressure BC) and mixed faces
     "poisson_3lev_32_walls": "n0=32 levels=3 maxbox=16 block=4 op=0 alpha=0 beta=1 bc=NNNNND",
     "vc_3lev_16_walls": "n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=-1 bc=NDNDNN",
+    "projection_3lev_32": "n0=32 levels=3 maxbox=16 block=4 op=0 alpha=0 beta=1 bc=NNNNND relaxbottom=1",
 }
 
 

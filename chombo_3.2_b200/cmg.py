@@ -424,3 +424,66 @@ class Hierarchy:
         r = ctypes.c_double()
         _check(lib().cmg_vcycle_bytes(self.h, ctypes.byref(p), ctypes.byref(r)))
         return r.value
+
+
+class Forest(Hierarchy):
+    """A forest (cmg_forest_create): several hierarchies with the same n0, level count, operator and boundary
+    types, whose level-0 layouts coarsen alike, solved together (one launch per V-cycle operation for all of
+    them).  `hierarchies` is a list of per-hierarchy level box lists.  Level data is the hierarchies' data one
+    after the other; phi(k, level) and set_rhs(k, level, data) address one hierarchy."""
+
+    def __init__(self, n0, hierarchies, op=0, alpha=0.0, beta=1.0, dx0=None, bc=None):
+        L = lib()
+        self.nh = len(hierarchies)
+        self.nlev = len(hierarchies[0])
+        counts = [len(lev) for hb in hierarchies for lev in hb]
+        if len(counts) != self.nh * self.nlev:
+            raise ValueError("every hierarchy of a forest has the same number of levels")
+        arr = boxes_array([b for hb in hierarchies for lev in hb for b in lev])
+        bcs = None
+        if bc is not None:
+            bcs = (ctypes.c_int * 6)(*[{"D": BC_DIRICHLET, "N": BC_NEUMANN}.get(x, x) if isinstance(x, str)
+                                       else int(x) for x in bc])
+        h = ctypes.c_void_p()
+        dx0 = 1.0 / n0 if dx0 is None else dx0
+        _check(L.cmg_forest_create(self.nh, (ctypes.c_int * 3)(0, 0, 0), (ctypes.c_int * 3)(n0 - 1, n0 - 1, n0 - 1),
+                                   ctypes.c_double(dx0), self.nlev, (ctypes.c_int * len(counts))(*counts), arr, op,
+                                   ctypes.c_double(alpha), ctypes.c_double(beta), bcs, ctypes.byref(h)))
+        self.h = h
+        self.op = op
+
+    def cells(self, k, level):
+        n = ctypes.c_int64()
+        _check(lib().cmg_forest_cells(self.h, k, level, ctypes.byref(n)))
+        return n.value
+
+    def _slice(self, k, level):
+        a = sum(self.cells(j, level) for j in range(k))
+        return slice(a, a + self.cells(k, level))
+
+    def fill_synthetic(self, seeds, device=True):
+        """The device generator of every hierarchy with its own seed (cmg_forest_fill_synthetic)."""
+        if not device:
+            raise ValueError("a forest fills its synthetic inputs on the device")
+        arr = (ctypes.c_uint64 * self.nh)(*seeds)
+        _check(lib().cmg_forest_fill_synthetic(self.h, arr))
+
+    def phi(self, k, level):
+        return Hierarchy.phi(self, level)[self._slice(k, level)].copy()
+
+    def set_rhs(self, k, level, data):
+        full = self.get_rhs(level)
+        full[self._slice(k, level)] = np.asarray(data, dtype=np.float64)
+        Hierarchy.set_rhs(self, level, full)
+
+    def solve(self, params=None, zero_phi=True, mixed=False):
+        """Every hierarchy's AMRMultiGrid solve at once (cmg_forest_solve): a list of per-hierarchy results."""
+        p = params or solve_params()
+        st = (ctypes.c_int * self.nh)()
+        it = (ctypes.c_int * self.nh)()
+        fn = (ctypes.c_double * self.nh)()
+        rc = lib().cmg_forest_solve(self.h, ctypes.byref(p), int(zero_phi), int(mixed), st, it, fn)
+        if rc != CMG_EDIVERGED:
+            _check(rc)
+        return [{"exit_status": st[k], "iterations": it[k], "final_norm": fn[k], "diverged": rc == CMG_EDIVERGED}
+                for k in range(self.nh)]

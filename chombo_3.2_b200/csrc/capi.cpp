@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -122,60 +123,134 @@ int cmg_hierarchy_create(const int domain_lo[3], const int domain_hi[3], double 
   return cmg_hierarchy_create_bc(domain_lo, domain_hi, dx0, nlevels, nboxes, boxes, op, alpha, beta, nullptr, out);
 }
 
+namespace {
+cmg::SolveParams solverParams(const cmg_solve_params* p);
+}
+
+// The checked description of one hierarchy (cmg_hierarchy_create_bc's
+// arguments); boxes of nlevels levels, counts in nboxes.
+static cmg::HierarchyDesc makeDesc(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
+                                   const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta,
+                                   const int bc[6]) {
+  if (!domain_lo || !domain_hi || !nboxes || !boxes || nlevels < 1 || dx0 <= 0 || (op != 0 && op != 1))
+    throw std::invalid_argument("cmg: invalid hierarchy description");
+  cmg::HierarchyDesc d;
+  if (bc)
+    for (int f = 0; f < 6; ++f) {
+      if (bc[f] != CMG_BC_DIRICHLET && bc[f] != CMG_BC_NEUMANN)
+        throw std::invalid_argument("cmg: boundary type is CMG_BC_DIRICHLET or CMG_BC_NEUMANN");
+      d.bc[f] = bc[f];
+    }
+  d.domain = cmg::Box(cmg::IV(domain_lo[0], domain_lo[1], domain_lo[2]), cmg::IV(domain_hi[0], domain_hi[1], domain_hi[2]));
+  if (d.domain.empty()) throw std::invalid_argument("cmg: empty domain");
+  d.dx0 = dx0;
+  d.vc = op;
+  d.alpha = alpha;
+  d.beta = beta;
+  int k = 0;
+  cmg::Box dom = d.domain;
+  for (int l = 0; l < nlevels; ++l) {
+    if (nboxes[l] < 1) throw std::invalid_argument("cmg: a level has no boxes");
+    if (l > 0) dom = dom.refine(2);
+    std::vector<cmg::Box> v;
+    for (int b = 0; b < nboxes[l]; ++b, ++k) {
+      cmg::Box bx = toBox(boxes[k]);
+      if (bx.empty() || !dom.contains(bx)) throw std::invalid_argument("cmg: box empty or outside its level domain");
+      if (l > 0 && !bx.coarsenable(2)) throw std::invalid_argument("cmg: fine box not coarsenable by 2");
+      v.push_back(bx);
+    }
+    std::vector<cmg::Box> sorted = v;
+    std::sort(sorted.begin(), sorted.end());
+    for (size_t i = 0; i < sorted.size(); ++i)
+      for (size_t j = i + 1; j < sorted.size() && sorted[j].lo[0] <= sorted[i].hi[0]; ++j)
+        if (sorted[i].intersects(sorted[j])) throw std::invalid_argument("cmg: boxes of a level overlap");
+    d.boxes.push_back(v);
+  }
+  return d;
+}
+
+// A handle around a new Solver on its own stream.
+static cmg_hierarchy* newHandle(const cmg::HierarchyDesc& d,
+                                const std::function<cmg::Solver*(cudaStream_t)>& make) {
+  cmg_hierarchy* h = new cmg_hierarchy;
+  h->desc = d;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete h;
+    throw std::runtime_error(std::string("cmg: stream: ") + cudaGetErrorString(e));
+  }
+  try {
+    h->solver = make(h->stream);
+  } catch (...) {
+    cudaStreamDestroy(h->stream);
+    delete h;
+    throw;
+  }
+  return h;
+}
+
 int cmg_hierarchy_create_bc(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
                             const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta,
                             const int bc[6], cmg_hierarchy** out) {
   return guard([&]() {
-    if (!domain_lo || !domain_hi || !nboxes || !boxes || !out || nlevels < 1 || dx0 <= 0 || (op != 0 && op != 1))
-      throw std::invalid_argument("cmg: invalid hierarchy description");
+    if (!out) throw std::invalid_argument("cmg: invalid hierarchy description");
     *out = nullptr;
-    cmg::HierarchyDesc d;
-    if (bc)
-      for (int f = 0; f < 6; ++f) {
-        if (bc[f] != CMG_BC_DIRICHLET && bc[f] != CMG_BC_NEUMANN)
-          throw std::invalid_argument("cmg: boundary type is CMG_BC_DIRICHLET or CMG_BC_NEUMANN");
-        d.bc[f] = bc[f];
-      }
-    d.domain = cmg::Box(cmg::IV(domain_lo[0], domain_lo[1], domain_lo[2]), cmg::IV(domain_hi[0], domain_hi[1], domain_hi[2]));
-    if (d.domain.empty()) throw std::invalid_argument("cmg: empty domain");
-    d.dx0 = dx0;
-    d.vc = op;
-    d.alpha = alpha;
-    d.beta = beta;
-    int k = 0;
-    cmg::Box dom = d.domain;
-    for (int l = 0; l < nlevels; ++l) {
-      if (nboxes[l] < 1) throw std::invalid_argument("cmg: a level has no boxes");
-      if (l > 0) dom = dom.refine(2);
-      std::vector<cmg::Box> v;
-      for (int b = 0; b < nboxes[l]; ++b, ++k) {
-        cmg::Box bx = toBox(boxes[k]);
-        if (bx.empty() || !dom.contains(bx)) throw std::invalid_argument("cmg: box empty or outside its level domain");
-        if (l > 0 && !bx.coarsenable(2)) throw std::invalid_argument("cmg: fine box not coarsenable by 2");
-        v.push_back(bx);
-      }
-      std::vector<cmg::Box> sorted = v;
-      std::sort(sorted.begin(), sorted.end());
-      for (size_t i = 0; i < sorted.size(); ++i)
-        for (size_t j = i + 1; j < sorted.size() && sorted[j].lo[0] <= sorted[i].hi[0]; ++j)
-          if (sorted[i].intersects(sorted[j])) throw std::invalid_argument("cmg: boxes of a level overlap");
-      d.boxes.push_back(v);
+    const cmg::HierarchyDesc d = makeDesc(domain_lo, domain_hi, dx0, nlevels, nboxes, boxes, op, alpha, beta, bc);
+    *out = newHandle(d, [&](cudaStream_t s) { return new cmg::Solver(d, s); });
+  });
+}
+
+int cmg_forest_create(int nh, const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
+                      const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta, const int bc[6],
+                      cmg_hierarchy** out) {
+  return guard([&]() {
+    if (!out || nh < 1 || nlevels < 1 || !nboxes || !boxes) throw std::invalid_argument("cmg: invalid forest");
+    *out = nullptr;
+    std::vector<cmg::HierarchyDesc> descs;
+    size_t at = 0;
+    for (int k = 0; k < nh; ++k) {
+      descs.push_back(makeDesc(domain_lo, domain_hi, dx0, nlevels, nboxes + (size_t)k * nlevels, boxes + at, op,
+                               alpha, beta, bc));
+      for (int l = 0; l < nlevels; ++l) at += nboxes[(size_t)k * nlevels + l];
     }
-    cmg_hierarchy* h = new cmg_hierarchy;
-    h->desc = d;
-    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-      delete h;
-      throw std::runtime_error(std::string("cmg: stream: ") + cudaGetErrorString(e));
+    *out = newHandle(descs[0], [&](cudaStream_t s) { return new cmg::Solver(descs, s); });
+  });
+}
+
+int cmg_forest_size(const cmg_hierarchy* h, int* nh) {
+  return guard([&]() {
+    if (!h || !h->solver || !nh) throw std::invalid_argument("cmg: null argument");
+    *nh = h->solver->numHierarchies();
+  });
+}
+
+int cmg_forest_cells(const cmg_hierarchy* h, int k, int level, int64_t* out) {
+  return guard([&]() {
+    if (!h || !h->solver || !out) throw std::invalid_argument("cmg: null argument");
+    *out = h->solver->hierarchyCells(k, level);
+  });
+}
+
+int cmg_forest_fill_synthetic(cmg_hierarchy* h, const uint64_t* seeds) {
+  return guard([&]() {
+    if (!h || !h->solver || !seeds) throw std::invalid_argument("cmg: null argument");
+    h->solver->fillSyntheticForest(std::vector<uint64_t>(seeds, seeds + h->solver->numHierarchies()));
+  });
+}
+
+int cmg_forest_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int mixed, int* exit_status,
+                     int* iterations, double* final_norm) {
+  return guard([&]() {
+    if (!h || !h->solver || !p || !exit_status || !iterations) throw std::invalid_argument("cmg: null argument");
+    const std::vector<cmg::SolveResult> r = h->solver->solveForest(solverParams(p), zero_phi != 0, mixed != 0);
+    int diverged = -1;
+    for (size_t k = 0; k < r.size(); ++k) {
+      exit_status[k] = r[k].exitStatus;
+      iterations[k] = r[k].iterations;
+      if (final_norm) final_norm[k] = r[k].history.back();
+      if (r[k].diverged && diverged < 0) diverged = r[k].iterations;
     }
-    try {
-      h->solver = new cmg::Solver(d, h->stream);
-    } catch (...) {
-      cudaStreamDestroy(h->stream);
-      delete h;
-      throw;
-    }
-    *out = h;
+    if (diverged >= 0) throw Diverged(diverged);
   });
 }
 

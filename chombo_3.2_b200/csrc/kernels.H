@@ -26,6 +26,12 @@ struct LevelDev {
   int nCellsExchBC = 0, nCellsGhost = 0;
   const GhostCell* gcells = nullptr;     // flat ghost-cell lists (LevelPlan::gcells)
   int gcStart[2] = {0, 0}, gcExch[2] = {0, 0}, gcCF[2] = {0, 0};
+  // forest levels (several hierarchies, LevelPlan::boxHier / hierStart):
+  // hierarchy of each box and first element of each hierarchy; null and 1
+  // for one hierarchy
+  const int* boxHier = nullptr;
+  const int64_t* hierStart = nullptr;
+  int nh = 1;
   const FaceRule* faceRules = nullptr;    // LevelPlan::faceRules / faceOff
   const int* faceOff = nullptr;
   const DeferredCell* deferred = nullptr; // LevelPlan::deferred
@@ -140,8 +146,13 @@ template <class T> void incr(const LevelDev& L, T* lhs, const T* x, double scale
 void incrMixed(const LevelDev& L, double* lhs, const float* x, cudaStream_t s);
 // dst[q] = src[q] for every element of a level array (valid and ghost cells).
 template <class D, class S> void convert(D* dst, const S* src, int64_t n, cudaStream_t s);
-// Max |f| over valid cells, folded into *out (device scalar) with max().
+// Max |f| over valid cells, folded into *out (device scalar) with max();
+// on a forest level into out[k] for each hierarchy k.
 template <class T> void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s);
+// lhs += x (flat, like incr / incrMixed) on the element ranges of the
+// hierarchies k of a forest level with active[k] != 0 only.
+template <class T, class X>
+void incrActive(const LevelDev& L, T* lhs, const X* x, const int* active, cudaStream_t s);
 
 // Bottom BiCGStab state in the compact slot space of the bottom level
 // (BottomPlan): slot tables, vectors r, r~, e, p, p~, s~, t, v, phi, rhs
@@ -157,7 +168,6 @@ struct BottomConfig {
   double eps = 1e-6, hang = 1e-8, small = 1e-30, reps = 1e-12;
 };
 struct BottomWork {
-  BottomConfig cfg;
   int nv = 0, ng = 0, nbox = 0, ncol[2] = {0, 0};
   const int *fab = nullptr, *nb = nullptr, *col[2] = {nullptr, nullptr}, *boxStart = nullptr;
   const int *gsrc = nullptr, *gkind = nullptr;
@@ -165,14 +175,17 @@ struct BottomWork {
   double *a = nullptr, *b[3] = {nullptr, nullptr, nullptr}, *lam = nullptr;
   int* status = nullptr;
 };
-// BiCGStab bottom solve of L(phi) = rhs (homogeneous boundary conditions) on
-// one level, one thread block, reference summation order.  eps and metric are
-// the tolerance and convergence metric AMRMultiGrid hands its bottom solver
-// (the metric read from device memory when the kernel runs, so a captured
-// launch serves every solve).  phi and rhs are level fields; the
-// coefficients come from w.
-void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
-                 double eps, const double* metric, cudaStream_t s);
+// Bottom solve (BiCGStab or relaxation, cfg) of L(phi) = rhs (homogeneous
+// boundary conditions) on one level, one thread block per hierarchy
+// (works[0 .. nworks), device memory; several for a forest), reference
+// summation order.  eps and metrics[k] are the tolerance and convergence
+// metric AMRMultiGrid hands hierarchy k's bottom solver (the metric read
+// from device memory when the kernel runs, so a captured launch serves every
+// solve).  phi and rhs are level fields; the coefficients come from the
+// works.  maxBoxes: the largest box count of a work.
+void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork* works,
+                 int nworks, int maxBoxes, const BottomConfig& cfg, double eps, const double* metrics,
+                 cudaStream_t s);
 // dst[slot] = fab[w.fab[slot]] for every slot of the bottom level.
 void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream_t s);
 
@@ -180,6 +193,10 @@ void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream
 // face arrays b when not null), the same formulas as synthetic.H.
 void fillSyntheticLevel(const LevelDev& L, uint64_t seed, double* rhs, double* a, double* const b[3],
                         cudaStream_t s);
+// The same over boxes [box0, box1) whose chunks are [ch0, ch1) of L.chAll
+// (one hierarchy of a forest level).
+void fillSyntheticBoxes(const LevelDev& L, uint64_t seed, double* rhs, double* a, double* const b[3], int box0,
+                        int box1, int ch0, int ch1, cudaStream_t s);
 // lambda of the variable-coefficient relaxation on one level
 // (VCAMRPoissonOp2::resetLambda with SUMFACES).
 void lambdaLevel(const LevelDev& L, const double* a, const double* const b[3], double alpha, double beta,

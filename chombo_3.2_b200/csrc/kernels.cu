@@ -637,6 +637,38 @@ __global__ void k_maxnorm(const BoxDesc* boxes, const Chunk* chunks, int nchunks
   }
 }
 
+// The max-norm of a forest level, one chunk per block, folded into the
+// norm of the chunk's hierarchy.
+template <class T>
+__global__ void k_maxnorm_hier(const BoxDesc* boxes, const Chunk* chunks, const int* boxHier, const T* f,
+                               double* out) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  double v = 0.0;
+  int i, j, k;
+  if (allCell(bd, ch.start + threadIdx.x, i, j, k)) v = fabs((double)f[cellIndex(bd, i, j, k)]);
+  for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __shared__ double red[CHUNK / 32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < CHUNK / 32 ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) atomicMaxPos(out + boxHier[ch.box], fabs(v));
+  }
+}
+
+// lhs += x over hierarchy blockIdx.y's element range of a forest level, if
+// that hierarchy is still iterating (k_incr_flat's arithmetic).
+template <class T, class X>
+__global__ void k_incr_active(T* lhs, const X* x, const int64_t* hierStart, const int* active) {
+  const int h = blockIdx.y;
+  if (!active[h]) return;
+  const int64_t a = hierStart[h], b = hierStart[h + 1];
+  for (int64_t q = a + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < b; q += (int64_t)gridDim.x * blockDim.x)
+    lhs[q] = lhs[q] + T(x[q]) * T(1.0);
+}
+
 // RESTRICTRES / RESTRICTRESVC3D (AMRPoissonOpF.ChF:394-438,
 // VCAMRPoissonOpF.ChF:337-413): res_c accumulates (rhs - L phi)/8 over its 8
 // fine cells in fine k-j-i order, starting from zero.
@@ -850,6 +882,7 @@ struct BottomArgs {
   double eps, reps, hang, small, mult;
   const double* metric;  // device scalar: the solve's initial residual norm
   int imax, numRestarts;
+  BottomConfig cfg;
 };
 
 // Exchange copies and homogeneous Dirichlet values of every ghost slot.
@@ -986,7 +1019,7 @@ __device__ double blkNorm(const BottomArgs& A, const double* x) { return sqrt(bl
 // The norm of type A.W.cfg.normType: 2 as above, 0 the largest |x| (a max,
 // so its order does not matter; NaN propagates).
 __device__ double blkNormType(const BottomArgs& A, const double* x) {
-  if (A.W.cfg.normType == 2) return blkNorm(A, x);
+  if (A.cfg.normType == 2) return blkNorm(A, x);
   __shared__ double m;
   if (threadIdx.x == 0) m = 0.0;
   __syncthreads();
@@ -1017,17 +1050,17 @@ __device__ void relaxSolve(const BottomArgs& A) {
   int iter = 0;
   if (norm > 0.) {
     const double initialNorm = norm;
-    while (iter < W.cfg.imax) {
+    while (iter < A.cfg.imax) {
       zeroAll(A.e);
       blkPrecond(A, A.e, A.r);
       blkCells(A, [&](int q) { A.phi[q] = A.phi[q] + A.e[q] * 1.0; });
       blkOp(A, A.r, A.phi, A.rhs, 0);
       norm = blkNormType(A, A.r);
       iter++;
-      if (norm < W.cfg.eps * initialNorm) break;
+      if (norm < A.cfg.eps * initialNorm) break;
       if (norm < minNorm)
         minNorm = norm;
-      else if (norm * W.cfg.hang > minNorm)
+      else if (norm * A.cfg.hang > minNorm)
         break;
     }
   }
@@ -1140,15 +1173,30 @@ __device__ void bicgstab(const BottomArgs& A) {
   if (threadIdx.x == 0) W.status[0] = status, W.status[1] = iter;
 }
 
-__global__ void __launch_bounds__(1024) k_bottom(BottomArgs A) {
+// One block per hierarchy of the level: block k solves with works[k] and
+// metrics[k], the rest of the arguments shared.
+__global__ void __launch_bounds__(1024) k_bottom(BottomArgs A0, const BottomWork* works, const double* metrics) {
+  BottomArgs A = A0;
+  A.W = works[blockIdx.x];
+  A.metric = metrics + blockIdx.x;
   const BottomWork& W = A.W;
+  A.r = W.v[0];
+  A.rt = W.v[1];
+  A.e = W.v[2];
+  A.p = W.v[3];
+  A.pt = W.v[4];
+  A.st = W.v[5];
+  A.t = W.v[6];
+  A.v = W.v[7];
+  A.phi = W.v[8];
+  A.rhs = W.v[9];
   const int nc = W.nv + W.ng;
   for (int q = threadIdx.x; q < nc; q += blockDim.x) {
     A.phi[q] = A.phiFab[W.fab[q]];
     A.rhs[q] = A.rhsFab[W.fab[q]];
   }
   __syncthreads();
-  if (W.cfg.kind == 1)
+  if (A.cfg.kind == 1)
     relaxSolve(A);
   else
     bicgstab(A);
@@ -1456,6 +1504,11 @@ void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s) {
 template <class T>
 void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s) {
   if (L.nAll == 0) return;
+  if (L.boxHier) {
+    k_maxnorm_hier<T><<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, L.boxHier, f, out);
+    CMG_LAUNCHED("maxNorm");
+    return;
+  }
   // One chunk per block (lowest latency) up to 4096 chunks; beyond, a
   // grid of 4096 blocks striding over them.
   const int blocks = std::min(L.nAll, 4096);
@@ -1467,35 +1520,26 @@ void maxNorm(const LevelDev& L, const T* f, double* out, cudaStream_t s) {
 long long launchCount() { return g_launches.load(std::memory_order_relaxed); }
 void addLaunches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
-void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork& w,
-                 double eps, const double* metric, cudaStream_t s) {
+void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork* works,
+                 int nworks, int maxBoxes, const BottomConfig& cfg, double eps, const double* metrics,
+                 cudaStream_t s) {
+  if (nworks == 0) return;
   BottomArgs A;
-  A.W = w;
   A.boxes = L.boxes;
   A.sc = scalars(L.dx, c.alpha, c.beta, c.vc);
   A.vc = c.vc;
   A.phiFab = phi;
   A.rhsFab = rhs;
-  A.r = w.v[0];
-  A.rt = w.v[1];
-  A.e = w.v[2];
-  A.p = w.v[3];
-  A.pt = w.v[4];
-  A.st = w.v[5];
-  A.t = w.v[6];
-  A.v = w.v[7];
-  A.phi = w.v[8];
-  A.rhs = w.v[9];
-  A.eps = w.cfg.kind == 1 ? w.cfg.eps : eps;  // RelaxSolver keeps its own tolerance
-  A.metric = metric;
-  A.reps = w.cfg.reps;
-  A.hang = w.cfg.hang;
-  A.small = w.cfg.small;
-  A.imax = w.cfg.imax;
-  A.numRestarts = w.cfg.numRestarts;
+  A.cfg = cfg;
+  A.eps = cfg.kind == 1 ? cfg.eps : eps;  // RelaxSolver keeps its own tolerance
+  A.reps = cfg.reps;
+  A.hang = cfg.hang;
+  A.small = cfg.small;
+  A.imax = cfg.imax;
+  A.numRestarts = cfg.numRestarts;
   // AMRPoissonOp::preCond multiplier (AMRPoissonOp.cpp:304-329).
   A.mult = 1.0 / (c.alpha - 2.0 * 3 * c.beta / (L.dx * L.dx));
-  k_bottom<<<1, 1024, w.nbox * sizeof(double), s>>>(A);
+  k_bottom<<<nworks, 1024, maxBoxes * sizeof(double), s>>>(A, works, metrics);
   CMG_LAUNCHED("bottomSolve");
 }
 
@@ -1511,6 +1555,17 @@ void incrMixed(const LevelDev& L, double* lhs, const float* x, cudaStream_t s) {
   k_incr_flat<double, float><<<flatBlocks(L.nelem), 256, 0, s>>>(lhs, x, 1.0, L.nelem);
   CMG_LAUNCHED("incrMixed");
 }
+
+template <class T, class X>
+void incrActive(const LevelDev& L, T* lhs, const X* x, const int* active, cudaStream_t s) {
+  if (L.nelem == 0) return;
+  const int64_t per = (L.nelem + L.nh - 1) / L.nh;
+  const int bx = (int)std::max<int64_t>(1, std::min<int64_t>((per + 255) / 256, 64));
+  k_incr_active<T, X><<<dim3(bx, L.nh), 256, 0, s>>>(lhs, x, L.hierStart, active);
+  CMG_LAUNCHED("incrActive");
+}
+template void incrActive<double, double>(const LevelDev&, double*, const double*, const int*, cudaStream_t);
+template void incrActive<double, float>(const LevelDev&, double*, const float*, const int*, cudaStream_t);
 
 template <class D, class S>
 void convert(D* dst, const S* src, int64_t n, cudaStream_t s) {
@@ -1618,13 +1673,18 @@ __global__ void k_avg_faces(const BoxDesc* fboxes, const BoxDesc* cboxes, int r,
 
 void fillSyntheticLevel(const LevelDev& L, uint64_t seed, double* rhs, double* a, double* const b[3],
                         cudaStream_t s) {
+  fillSyntheticBoxes(L, seed, rhs, a, b, 0, L.nbox, 0, L.nAll, s);
+}
+
+void fillSyntheticBoxes(const LevelDev& L, uint64_t seed, double* rhs, double* a, double* const b[3], int box0,
+                        int box1, int ch0, int ch1, cudaStream_t s) {
   cmg_synth::Problem prob(seed);
-  if (L.nAll == 0) return;
-  k_fill_cells<<<L.nAll, CHUNK, 0, s>>>(L.boxes, L.chAll, L.dx, prob.bumps, prob.acoef, rhs, a);
+  if (ch1 <= ch0) return;
+  k_fill_cells<<<ch1 - ch0, CHUNK, 0, s>>>(L.boxes, L.chAll + ch0, L.dx, prob.bumps, prob.acoef, rhs, a);
   CMG_LAUNCHED("fillCells");
-  if (!b) return;
+  if (!b || box1 <= box0) return;
   for (int d = 0; d < 3; ++d) {
-    k_fill_faces<<<L.nbox, 256, 0, s>>>(L.boxes, L.dx, d, prob.bcoef, b[d]);
+    k_fill_faces<<<box1 - box0, 256, 0, s>>>(L.boxes + box0, L.dx, d, prob.bcoef, b[d]);
     CMG_LAUNCHED("fillFaces");
   }
 }

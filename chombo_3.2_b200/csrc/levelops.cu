@@ -220,6 +220,7 @@ int64_t Solver::opCoarsenedSize(int l) const {
 // in the ghosted host format (and, for AMR levels >= 1, in the coarsened-fine
 // format), a host staging buffer, and level-sized device fields.
 Solver::OpState& Solver::opState(int lev) {
+  needSingle();
   auto it = opStates_.find(lev);
   if (it != opStates_.end()) return *it->second;
   const LevelPlan& p = opPlan(lev);

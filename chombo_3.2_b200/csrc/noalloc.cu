@@ -127,6 +127,7 @@ struct DeviceScope {
 // kernels and order as Solver::computeAMRResidual, level pointers kept on
 // the stack and the max-norm reduced through the static scratch.
 double Solver::residualNormStatic(double* scratch) {
+  needSingle();
   const int nlev = numLevels(), lmax = nlev - 1;
   if (nlev > NOALLOC_MAX_LEVELS)
     throw std::invalid_argument("cmg: residual_norm_noalloc: more than 16 levels (static scratch limit)");

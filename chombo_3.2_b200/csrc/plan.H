@@ -63,6 +63,10 @@ struct LevelPlan {
   std::vector<RefluxCell> rfCells;
   std::vector<RefluxCoarseTerm> rfCoarse;
   std::vector<RefluxFineGroup> rfFine;
+  // Forest levels (mergeLevels): hierarchy of each box, first element of each
+  // hierarchy (one more entry: nelem).  Empty for one hierarchy.
+  std::vector<int> boxHier;
+  std::vector<int64_t> hierStart;
 };
 
 // Compact indexing of the bottom level for the one-block BiCGStab: valid
@@ -107,6 +111,15 @@ std::vector<int> blockTasks(const std::vector<int>& start);
 
 // Finds the box of L containing p, or -1.
 int ownerOf(const LevelPlan& L, const IV& p);
+
+// The same level of several hierarchies as one level (a forest level):
+// parts[k] placed at element offset elemOff[k] and box offset boxOff[k];
+// coarseElemOff / coarseBoxOff (the next coarser level's part offsets) shift
+// the coarse-fine tables, fineElemOff (the next finer level's) the flux
+// register; nullptr where the level has no such neighbour.
+void mergeLevels(const std::vector<const LevelPlan*>& parts, const std::vector<int64_t>& elemOff,
+                 const std::vector<int>& boxOff, const std::vector<int64_t>* coarseElemOff,
+                 const std::vector<int>* coarseBoxOff, const std::vector<int64_t>* fineElemOff, LevelPlan& out);
 
 }  // namespace cmg
 

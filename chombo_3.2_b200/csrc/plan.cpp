@@ -1042,3 +1042,177 @@ void buildBottom(const LevelPlan& L, BottomPlan& B) {
 }
 
 }  // namespace cmg
+
+namespace cmg {
+
+// ------------------------------------------------------------------ forests
+// A forest level is the disjoint union of the same level of several
+// hierarchies: their boxes one hierarchy after the other, each hierarchy's
+// FABs in one contiguous element range.  Every table of a LevelPlan refers to
+// boxes, elements, chunks or pool entries of its own level (or of the next
+// coarser or finer level), so the union is the concatenation of the parts
+// with those indices shifted; the hierarchies never share a cell, and every
+// kernel over the union does, box by box, what it does over each part.
+void mergeLevels(const std::vector<const LevelPlan*>& parts, const std::vector<int64_t>& elemOff,
+                 const std::vector<int>& boxOff, const std::vector<int64_t>* coarseElemOff,
+                 const std::vector<int>* coarseBoxOff, const std::vector<int64_t>* fineElemOff, LevelPlan& out) {
+  const size_t K = parts.size();
+  if (K == 0) throw std::invalid_argument("cmg: empty forest");
+  const LevelPlan& p0 = *parts[0];
+  out = LevelPlan();
+  out.domain = p0.domain;
+  out.dx = p0.dx;
+  out.dxCrse = p0.dxCrse;
+  auto shiftCell = [](GhostCell g, int64_t eo) {
+    g.dst += (int)eo;
+    g.s1 += (int)eo;
+    if (g.s2 >= 0) g.s2 += (int)eo;
+    return g;
+  };
+  auto shiftTask = [](GhostTask t, int bo) {
+    t.dst += bo;
+    t.src += bo;
+    return t;
+  };
+  // boxes, grids, elements, chunks
+  for (size_t k = 0; k < K; ++k) {
+    const LevelPlan& p = *parts[k];
+    if (p.dx != p0.dx || p.dxCrse != p0.dxCrse) throw std::invalid_argument("cmg: forest levels differ in dx");
+    for (BoxDesc d : p.boxes) {
+      d.off += elemOff[k];
+      out.boxes.push_back(d);
+    }
+    out.grids.boxes.insert(out.grids.boxes.end(), p.grids.boxes.begin(), p.grids.boxes.end());
+    out.nelem += p.nelem;
+    for (Chunk c : p.chunksAll) out.chunksAll.push_back(Chunk{c.box + boxOff[k], c.start});
+    for (int c = 0; c < 2; ++c)
+      for (Chunk ch : p.chunksColor[c]) out.chunksColor[c].push_back(Chunk{ch.box + boxOff[k], ch.start});
+    for (DeferredCell d : p.deferred) out.deferred.push_back(DeferredCell{d.box + boxOff[k], d.q});
+  }
+  if (out.nelem >= ((int64_t)1 << 31)) throw std::runtime_error("cmg: forest level too large for 32-bit indices");
+  for (size_t k = 0; k < K; ++k) {
+    out.hierStart.push_back(elemOff[k]);
+    out.boxHier.insert(out.boxHier.end(), parts[k]->boxes.size(), (int)k);
+  }
+  out.hierStart.push_back(out.nelem);
+  // ghost tasks: every part's exchange and boundary tasks, then every part's
+  // coarse-fine tasks (the order the fills rely on)
+  for (int pass = 0; pass < 2; ++pass)
+    for (size_t k = 0; k < K; ++k) {
+      const LevelPlan& p = *parts[k];
+      const size_t a = pass == 0 ? 0 : (size_t)p.nExchBC, b = pass == 0 ? (size_t)p.nExchBC : p.ghost.size();
+      for (size_t t = a; t < b; ++t) out.ghost.push_back(shiftTask(p.ghost[t], boxOff[k]));
+      if (pass == 0) out.nExchBC += p.nExchBC;
+    }
+  out.ghostStart.assign(1, 0);
+  out.slotStart.assign(1, 0);
+  for (const GhostTask& t : out.ghost) {
+    const int64_t c = (int64_t)(t.hi[0] - t.lo[0] + 1) * (t.hi[1] - t.lo[1] + 1) * (t.hi[2] - t.lo[2] + 1);
+    out.ghostStart.push_back(out.ghostStart.back() + (int)c);
+    out.slotStart.push_back(out.slotStart.back() + (int)colourSlots(t.lo, t.hi, parityAxis(t.lo, t.hi)));
+  }
+  out.ghostBlock = blockTasks(out.ghostStart);
+  out.slotBlock = blockTasks(out.slotStart);
+  // flat ghost cells: per parity all exchange+boundary parts, then all CF parts
+  for (int par = 0; par < 2; ++par) {
+    out.gcStart[par] = (int)out.gcells.size();
+    for (int cf = 0; cf < 2; ++cf)
+      for (size_t k = 0; k < K; ++k) {
+        const LevelPlan& p = *parts[k];
+        const int a = p.gcStart[par] + (cf ? p.gcExch[par] : 0);
+        const int n = cf ? p.gcCF[par] : p.gcExch[par];
+        for (int q = a; q < a + n; ++q) out.gcells.push_back(shiftCell(p.gcells[q], elemOff[k]));
+        (cf ? out.gcCF[par] : out.gcExch[par]) += n;
+      }
+  }
+  // face rules, per-chunk ghosts
+  for (size_t k = 0; k < K; ++k) {
+    const LevelPlan& p = *parts[k];
+    const int rbase = (int)out.faceRules.size();
+    for (FaceRule r : p.faceRules) {
+      if (r.kind == FR_COPY || r.kind == FR_CFQUAD || r.kind == FR_FAB) r.src += (int)elemOff[k];
+      out.faceRules.push_back(r);
+    }
+    for (size_t q = 0; q + 1 < p.faceOff.size(); ++q) out.faceOff.push_back(p.faceOff[q] + rbase);
+    for (int c = 0; c < 2; ++c) {
+      const int gbase = (int)out.chunkGhost[c].size();
+      for (const GhostCell& g : p.chunkGhost[c]) out.chunkGhost[c].push_back(shiftCell(g, elemOff[k]));
+      for (size_t q = 0; q + 1 < p.chunkGhostStart[c].size(); ++q)
+        out.chunkGhostStart[c].push_back(p.chunkGhostStart[c][q] + gbase);
+    }
+  }
+  out.faceOff.push_back((int)out.faceRules.size());
+  for (int c = 0; c < 2; ++c) out.chunkGhostStart[c].push_back((int)out.chunkGhost[c].size());
+  // zeroing of the cells under the finer level
+  for (size_t k = 0; k < K; ++k)
+    for (const GhostTask& t : parts[k]->zeroCovered) out.zeroCovered.push_back(shiftTask(t, boxOff[k]));
+  out.zeroStart.assign(1, 0);
+  for (const GhostTask& t : out.zeroCovered)
+    out.zeroStart.push_back(out.zeroStart.back() +
+                            (t.hi[0] - t.lo[0] + 1) * (t.hi[1] - t.lo[1] + 1) * (t.hi[2] - t.lo[2] + 1));
+  out.zeroBlock = blockTasks(out.zeroStart);
+  // coarse-fine interpolation and coarse/fine maps (coarser level indices)
+  if (coarseElemOff) {
+    for (size_t k = 0; k < K; ++k) {
+      const LevelPlan& p = *parts[k];
+      const int64_t eoC = (*coarseElemOff)[k];
+      const int coarseBase = (int)out.cfCoarse.size(), poolBase = (int)out.cfOff.size();
+      for (CFCoarse e : p.cfCoarse) {
+        e.cc += eoC;
+        for (int q = 0; q < 2; ++q) {
+          if (e.d1[q].kind) e.d1[q].start += poolBase;
+          if (e.d2[q].kind) e.d2[q].start += poolBase;
+        }
+        if (e.mx.kind) e.mx.start += poolBase;
+        out.cfCoarse.push_back(e);
+      }
+      for (CFFine f : p.cfFine) {
+        f.g += elemOff[k];
+        f.pa += elemOff[k];
+        f.pb += elemOff[k];
+        f.coarse += coarseBase;
+        out.cfFine.push_back(f);
+      }
+      out.cfW.insert(out.cfW.end(), p.cfW.begin(), p.cfW.end());
+      for (int64_t o : p.cfOff) out.cfOff.push_back(o + eoC);
+      const int itemBase = (int)out.toCoarse.size();
+      for (CoarseFineItem it : p.toCoarse) {
+        it.cbox += (*coarseBoxOff)[k];
+        it.fbox += boxOff[k];
+        out.toCoarse.push_back(it);
+      }
+      for (Chunk c : p.toCoarseChunksF) out.toCoarseChunksF.push_back(Chunk{c.box + itemBase, c.start});
+      for (Chunk c : p.toCoarseChunksC) out.toCoarseChunksC.push_back(Chunk{c.box + itemBase, c.start});
+    }
+  }
+  // flux-register correction from the finer level (finer level indices)
+  if (fineElemOff) {
+    for (size_t k = 0; k < K; ++k) {
+      const LevelPlan& p = *parts[k];
+      const int64_t eoF = (*fineElemOff)[k];
+      const int cbase = (int)out.rfCoarse.size(), fbase = (int)out.rfFine.size();
+      for (RefluxCell rc : p.rfCells) {
+        rc.c += elemOff[k];
+        rc.start += cbase;
+        rc.fstart += fbase;
+        out.rfCells.push_back(rc);
+      }
+      for (RefluxCoarseTerm t : p.rfCoarse) {
+        t.hi += elemOff[k];
+        t.lo += elemOff[k];
+        if (t.bface >= 0) t.bface += elemOff[k];
+        out.rfCoarse.push_back(t);
+      }
+      for (RefluxFineGroup g : p.rfFine) {
+        for (int q = 0; q < 4; ++q) {
+          g.hi[q] += eoF;
+          g.lo[q] += eoF;
+          if (g.bface[q] >= 0) g.bface[q] += eoF;
+        }
+        out.rfFine.push_back(g);
+      }
+    }
+  }
+}
+
+}  // namespace cmg

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <functional>
+#include <stdexcept>
 #include <map>
 #include <memory>
 #include <tuple>
@@ -80,7 +81,28 @@ struct DevBuf {
 class Solver {
  public:
   Solver(const HierarchyDesc& d, cudaStream_t stream);
+  // A forest of hierarchies solved together: every level and multigrid depth
+  // holds the boxes of all of them (one kernel launch per operation for the
+  // whole forest), each hierarchy with its own convergence test and bottom
+  // solve.  Level data (setRHS, getPhi, ...) is the hierarchies' data one
+  // after the other.
+  Solver(const std::vector<HierarchyDesc>& descs, cudaStream_t stream);
   ~Solver();
+  int numHierarchies() const { return nh_; }
+  // The single-hierarchy solves and operators refuse a forest.
+  void needSingle() const {
+    if (nh_ > 1) throw std::invalid_argument("cmg: a forest is solved with cmg_forest_solve only");
+  }
+  // Valid cells of hierarchy k on level l (forest level data is ordered by
+  // hierarchy).
+  int64_t hierarchyCells(int k, int l) const;
+  // Each hierarchy's solve, all of them advancing together: an iteration
+  // runs for every hierarchy, and phi of a hierarchy whose stopping rule has
+  // ended its solve is no longer changed, so each result is the one its own
+  // solve gives.  Mixed: FP32 V-cycles inside FP64 refinement.
+  std::vector<SolveResult> solveForest(const SolveParams& p, bool zeroPhi, bool mixed);
+  // fillSyntheticDevice for every hierarchy with its own seed.
+  void fillSyntheticForest(const std::vector<uint64_t>& seeds);
   int numLevels() const { return (int)amr_.size(); }
   const LevelPlan& level(int l) const { return amr_[l]; }
   int numMGDepths() const { return (int)mg_.size(); }
@@ -171,7 +193,7 @@ class Solver {
   void setRelaxMode(int mode);
   // The bottom solver of the multigrid levels below level 0 (BottomConfig).
   void setBottomConfig(const BottomConfig& c);
-  const BottomConfig& bottomConfig() const { return bottom_.cfg; }
+  const BottomConfig& bottomConfig() const { return bottomCfg_; }
   // The variant of every AMR level then every multigrid depth (1: inline),
   // and the tuner's sweep times (ms; empty when a mode was forced).
   void relaxVariants(std::vector<int>& inl, std::vector<float>& msFill, std::vector<float>& msInline);
@@ -255,6 +277,7 @@ class Solver {
   double computeAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);
   void launchAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs, int lmax);
   double readNorm();
+  std::vector<double> readNorms();  // one per hierarchy
   SolveResult solveImpl(const SolveParams& p, bool zeroPhi, bool mixed);
   void iterationBody(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi, std::vector<double*>& rhs);
   cudaGraphExec_t iterationGraph(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi,
@@ -345,7 +368,14 @@ class Solver {
   std::vector<FieldsT<float>> lev32_, mgf32_;  // FP32 V-cycle fields (allocated on first solveMixed)
   bool have32_ = false, coef32Stale_ = true;
   std::vector<std::unique_ptr<DevBuf>> bufs_;
-  BottomWork bottom_;
+  std::vector<BottomWork> bottoms_;         // one per hierarchy (one unless a forest)
+  const BottomWork* dBottoms_ = nullptr;    // the same in device memory
+  int maxBottomBoxes_ = 1;
+  BottomConfig bottomCfg_;
+  int nh_ = 1;                              // hierarchies (a forest: more than one)
+  int* dActive_ = nullptr;                  // per hierarchy: still iterating (forest solves)
+  int* hostActive_ = nullptr;               // pinned staging of dActive_
+  void setup(const std::vector<BottomPlan>& bps);
   double* dNorm_ = nullptr;
   int64_t bottomCells_ = 0;
   SolveParams sp_;

@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <exception>
 #include <thread>
@@ -194,13 +195,17 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
   d.rfF = upload(bufs_, p.rfFine, s_);
   d.dx = p.dx;
   d.dxCrse = p.dxCrse;
+  d.boxHier = upload(bufs_, p.boxHier, s_);
+  d.hierStart = upload(bufs_, p.hierStart, s_);
+  d.nh = p.hierStart.empty() ? 1 : (int)p.hierStart.size() - 1;
 }
 
-Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
-    : s_(stream), own_(stream), desc_(desc), alpha0_(desc.alpha), beta0_(desc.beta) {
+// Host plans of one hierarchy: its AMR levels, the multigrid depths below
+// level 0 and the plans between consecutive AMR levels.
+static void hierarchyPlans(const HierarchyDesc& desc, std::vector<LevelPlan>& amr, std::vector<LevelPlan>& mg) {
   const int nlev = (int)desc.boxes.size();
   if (nlev < 1) throw std::runtime_error("cmg: hierarchy needs at least one level");
-  amr_.resize(nlev);
+  amr.resize(nlev);
   // Host plans, one thread per level and then one per level pair (each pair
   // writes distinct members of its two levels).
   std::vector<Box> doms(nlev);
@@ -217,14 +222,14 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
   const Layout g0(desc.boxes[0]);
   std::vector<int> mgc;
   for (int c = 2; g0.coarsenable(c * 2); c *= 2) mgc.push_back(c);
-  mg_.resize(mgc.size());
+  mg.resize(mgc.size());
   {
     std::vector<std::exception_ptr> err(nlev + mgc.size());
     std::vector<std::thread> th;
     for (int l = 0; l < nlev; ++l)
       th.emplace_back([&, l]() {
         try {
-          buildLevel(amr_[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0, desc.bc);
+          buildLevel(amr[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0, desc.bc);
         } catch (...) {
           err[l] = std::current_exception();
         }
@@ -233,7 +238,7 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
       th.emplace_back([&, d]() {
         try {
           const int c = mgc[d];
-          buildLevel(mg_[d], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0, desc.bc);
+          buildLevel(mg[d], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0, desc.bc);
         } catch (...) {
           err[nlev + d] = std::current_exception();
         }
@@ -248,9 +253,9 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
     for (int l = 1; l < nlev; ++l)
       th.emplace_back([&, l]() {
         try {
-          buildQuadCF(amr_[l], amr_[l - 1]);
-          buildCoarseFine(amr_[l], amr_[l - 1]);
-          buildReflux(amr_[l - 1], amr_[l], desc.vc != 0);
+          buildQuadCF(amr[l], amr[l - 1]);
+          buildCoarseFine(amr[l], amr[l - 1]);
+          buildReflux(amr[l - 1], amr[l], desc.vc != 0);
         } catch (...) {
           err[l] = std::current_exception();
         }
@@ -259,6 +264,102 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
     for (auto& e : err)
       if (e) std::rethrow_exception(e);
   }
+}
+
+Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
+    : s_(stream), own_(stream), desc_(desc), alpha0_(desc.alpha), beta0_(desc.beta) {
+  hierarchyPlans(desc, amr_, mg_);
+  std::vector<BottomPlan> bps(1);
+  buildBottom(mg_.empty() ? amr_[0] : mg_.back(), bps[0]);
+  setup(bps);
+}
+
+// A forest: hierarchies with the same domain, cell size, level count,
+// operator and boundary types (and so the same multigrid depths when their
+// level-0 layouts coarsen alike) planned one by one and merged level by level
+// (mergeLevels).  Each keeps its own bottom solve; the solve loop keeps a
+// residual norm, a stopping rule and an iteration count per hierarchy.
+Solver::Solver(const std::vector<HierarchyDesc>& descs, cudaStream_t stream)
+    : s_(stream), own_(stream), desc_(descs.at(0)), alpha0_(descs[0].alpha), beta0_(descs[0].beta) {
+  const size_t K = descs.size();
+  const HierarchyDesc& d0 = descs[0];
+  for (const HierarchyDesc& d : descs) {
+    bool same = d.domain.lo == d0.domain.lo && d.domain.hi == d0.domain.hi && d.dx0 == d0.dx0 &&
+                d.boxes.size() == d0.boxes.size() && d.vc == d0.vc && d.alpha == d0.alpha && d.beta == d0.beta;
+    for (int f = 0; f < 6; ++f) same = same && d.bc[f] == d0.bc[f];
+    if (!same)
+      throw std::invalid_argument("cmg: the hierarchies of a forest need the same domain, dx, level count, operator "
+                                  "and boundary types");
+  }
+  std::vector<std::vector<LevelPlan>> amrP(K), mgP(K);
+  {
+    std::vector<std::exception_ptr> err(K);
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(K, 8));
+    std::vector<std::thread> th;
+    std::atomic<size_t> next{0};
+    for (size_t t = 0; t < nt; ++t)
+      th.emplace_back([&]() {
+        for (size_t k = next++; k < K; k = next++) try {
+            hierarchyPlans(descs[k], amrP[k], mgP[k]);
+          } catch (...) {
+            err[k] = std::current_exception();
+          }
+      });
+    for (auto& t : th) t.join();
+    for (auto& e : err)
+      if (e) std::rethrow_exception(e);
+  }
+  const size_t nlev = amrP[0].size(), nd = mgP[0].size();
+  for (size_t k = 0; k < K; ++k)
+    if (mgP[k].size() != nd)
+      throw std::invalid_argument("cmg: the hierarchies of a forest need the same multigrid depths (level-0 boxes "
+                                  "that coarsen alike)");
+  // element and box offsets of every part, level by level
+  auto offsets = [&](const std::vector<std::vector<LevelPlan>>& P, size_t l, std::vector<int64_t>& eo,
+                     std::vector<int>& bo) {
+    eo.assign(K, 0);
+    bo.assign(K, 0);
+    int64_t e = 0;
+    int b = 0;
+    for (size_t k = 0; k < K; ++k) {
+      eo[k] = e;
+      bo[k] = b;
+      e += P[k][l].nelem;
+      b += (int)P[k][l].boxes.size();
+    }
+  };
+  std::vector<std::vector<int64_t>> eoA(nlev), eoM(nd);
+  std::vector<std::vector<int>> boA(nlev), boM(nd);
+  for (size_t l = 0; l < nlev; ++l) offsets(amrP, l, eoA[l], boA[l]);
+  for (size_t d = 0; d < nd; ++d) offsets(mgP, d, eoM[d], boM[d]);
+  amr_.resize(nlev);
+  mg_.resize(nd);
+  for (size_t l = 0; l < nlev; ++l) {
+    std::vector<const LevelPlan*> parts;
+    for (size_t k = 0; k < K; ++k) parts.push_back(&amrP[k][l]);
+    mergeLevels(parts, eoA[l], boA[l], l > 0 ? &eoA[l - 1] : nullptr, l > 0 ? &boA[l - 1] : nullptr,
+                l + 1 < nlev ? &eoA[l + 1] : nullptr, amr_[l]);
+    desc_.boxes[l] = amr_[l].grids.boxes;
+  }
+  for (size_t d = 0; d < nd; ++d) {
+    std::vector<const LevelPlan*> parts;
+    for (size_t k = 0; k < K; ++k) parts.push_back(&mgP[k][d]);
+    mergeLevels(parts, eoM[d], boM[d], nullptr, nullptr, nullptr, mg_[d]);
+  }
+  // each hierarchy's bottom level, its slots moved to the merged elements
+  std::vector<BottomPlan> bps(K);
+  for (size_t k = 0; k < K; ++k) {
+    buildBottom(nd == 0 ? amrP[k][0] : mgP[k][nd - 1], bps[k]);
+    const int64_t eo = nd == 0 ? eoA[0][k] : eoM[nd - 1][k];
+    for (int& f : bps[k].fab) f += (int)eo;
+  }
+  setup(bps);
+}
+
+void Solver::setup(const std::vector<BottomPlan>& bps) {
+  const HierarchyDesc& desc = desc_;
+  const int nlev = (int)amr_.size();
+  nh_ = (int)bps.size();
   bottomCells_ = desc.domain.numPts();
   for (size_t d = 0; d < mg_.size(); ++d) bottomCells_ /= 8;
 
@@ -293,34 +394,43 @@ Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
       mgf_[d].lambda = alloc(n);
     }
   }
-  // Bottom solve in the compact slot space of the deepest level.
-  const LevelPlan& bl = mg_.empty() ? amr_[0] : mg_.back();
-  BottomPlan bp;
-  buildBottom(bl, bp);
-  const size_t nc = (size_t)bp.nv + bp.ng;
-  bottom_.nv = bp.nv;
-  bottom_.ng = bp.ng;
-  bottom_.nbox = (int)bl.boxes.size();
-  bottom_.fab = upload(bufs_, bp.fab, s_);
-  bottom_.nb = upload(bufs_, bp.nb, s_);
-  for (int c = 0; c < 2; ++c) {
-    bottom_.col[c] = upload(bufs_, bp.color[c], s_);
-    bottom_.ncol[c] = (int)bp.color[c].size();
+  // Bottom solves in the compact slot space of the deepest level, one per
+  // hierarchy.
+  bottoms_.resize(bps.size());
+  maxBottomBoxes_ = 1;
+  for (size_t k = 0; k < bps.size(); ++k) {
+    const BottomPlan& bp = bps[k];
+    BottomWork& w = bottoms_[k];
+    const size_t nc = (size_t)bp.nv + bp.ng;
+    w.nv = bp.nv;
+    w.ng = bp.ng;
+    w.nbox = (int)bp.boxStart.size() - 1;
+    maxBottomBoxes_ = std::max(maxBottomBoxes_, w.nbox);
+    w.fab = upload(bufs_, bp.fab, s_);
+    w.nb = upload(bufs_, bp.nb, s_);
+    for (int c = 0; c < 2; ++c) {
+      w.col[c] = upload(bufs_, bp.color[c], s_);
+      w.ncol[c] = (int)bp.color[c].size();
+    }
+    w.boxStart = upload(bufs_, bp.boxStart, s_);
+    w.gsrc = upload(bufs_, bp.gsrc, s_);
+    w.gkind = upload(bufs_, bp.gkind, s_);
+    for (int q = 0; q < 10; ++q) w.v[q] = alloc(nc);
+    if (desc.vc) {
+      w.a = alloc(nc);
+      for (int d = 0; d < 3; ++d) w.b[d] = alloc(nc);
+      w.lam = alloc(nc);
+    }
+    bufs_.emplace_back(new DevBuf(4 * sizeof(int), s_));
+    w.status = (int*)bufs_.back()->p;
   }
-  bottom_.boxStart = upload(bufs_, bp.boxStart, s_);
-  bottom_.gsrc = upload(bufs_, bp.gsrc, s_);
-  bottom_.gkind = upload(bufs_, bp.gkind, s_);
-  for (int k = 0; k < 10; ++k) bottom_.v[k] = alloc(nc);
-  if (desc.vc) {
-    bottom_.a = alloc(nc);
-    for (int d = 0; d < 3; ++d) bottom_.b[d] = alloc(nc);
-    bottom_.lam = alloc(nc);
-  }
-  bufs_.emplace_back(new DevBuf(4 * sizeof(int), s_));
-  bottom_.status = (int*)bufs_.back()->p;
-  dNorm_ = alloc(1);
-  dMetric_ = alloc(1);
-  ck(cudaMallocHost((void**)&hostScalars_, 2 * sizeof(double)), "pinned scalars");
+  dBottoms_ = upload(bufs_, bottoms_, s_);
+  dNorm_ = alloc(nh_);
+  dMetric_ = alloc(nh_);
+  bufs_.emplace_back(new DevBuf(nh_ * sizeof(int), s_));
+  dActive_ = (int*)bufs_.back()->p;
+  ck(cudaMallocHost((void**)&hostScalars_, (2 + 2 * nh_) * sizeof(double)), "pinned scalars");
+  ck(cudaMallocHost((void**)&hostActive_, nh_ * sizeof(int)), "pinned flags");
   if (desc.vc) {
     hostA_.resize(nlev);
     for (int d = 0; d < 3; ++d) hostB_[d].resize(nlev);
@@ -333,6 +443,7 @@ Solver::~Solver() {
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
   for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
   if (hostScalars_) cudaFreeHost(hostScalars_);
+  if (hostActive_) cudaFreeHost(hostActive_);
   if (hostBoxSums_) cudaFreeHost(hostBoxSums_);
 }
 
@@ -558,9 +669,11 @@ void Solver::finalizeCoefficients() {
   coef32Stale_ = true;
   // Compact copies of the bottom level's coefficients for the bottom solve.
   Coef<double> cb = coefMG((int)mg_.size());
-  gatherSlots(bottom_, cb.a, bottom_.a, s_);
-  for (int k = 0; k < 3; ++k) gatherSlots(bottom_, cb.b[k], bottom_.b[k], s_);
-  gatherSlots(bottom_, cb.lambda, bottom_.lam, s_);
+  for (BottomWork& w : bottoms_) {
+    gatherSlots(w, cb.a, w.a, s_);
+    for (int k = 0; k < 3; ++k) gatherSlots(w, cb.b[k], w.b[k], s_);
+    gatherSlots(w, cb.lambda, w.lam, s_);
+  }
   ck(cudaStreamSynchronize(s_), "bottom coefficients");
 }
 
@@ -577,11 +690,62 @@ void Solver::fillSyntheticDevice(uint64_t seed) {
     }
     coef32Stale_ = true;
     Coef<double> cb = coefMG((int)mg_.size());
-    gatherSlots(bottom_, cb.a, bottom_.a, s_);
-    for (int k = 0; k < 3; ++k) gatherSlots(bottom_, cb.b[k], bottom_.b[k], s_);
-    gatherSlots(bottom_, cb.lambda, bottom_.lam, s_);
+    for (BottomWork& w : bottoms_) {
+      gatherSlots(w, cb.a, w.a, s_);
+      for (int k = 0; k < 3; ++k) gatherSlots(w, cb.b[k], w.b[k], s_);
+      gatherSlots(w, cb.lambda, w.lam, s_);
+    }
   }
   ck(cudaStreamSynchronize(s_), "device inputs");
+}
+
+void Solver::fillSyntheticForest(const std::vector<uint64_t>& seeds) {
+  if ((int)seeds.size() != nh_) throw std::invalid_argument("cmg: one seed per hierarchy");
+  for (int l = 0; l < numLevels(); ++l) {
+    const LevelPlan& p = amr_[l];
+    for (int k = 0; k < nh_; ++k) {
+      // boxes and chunks of hierarchy k (both ordered by hierarchy)
+      int b0 = 0, b1 = 0, c0 = 0, c1 = 0;
+      if (nh_ == 1) {
+        b1 = (int)p.boxes.size();
+        c1 = (int)p.chunksAll.size();
+      } else {
+        b0 = (int)(std::lower_bound(p.boxHier.begin(), p.boxHier.end(), k) - p.boxHier.begin());
+        b1 = (int)(std::upper_bound(p.boxHier.begin(), p.boxHier.end(), k) - p.boxHier.begin());
+        auto byBox = [](const Chunk& c, int b) { return c.box < b; };
+        c0 = (int)(std::lower_bound(p.chunksAll.begin(), p.chunksAll.end(), b0, byBox) - p.chunksAll.begin());
+        c1 = (int)(std::lower_bound(p.chunksAll.begin(), p.chunksAll.end(), b1, byBox) - p.chunksAll.begin());
+      }
+      fillSyntheticBoxes(amrDev_[l], seeds[k], lev_[l].rhs, desc_.vc ? lev_[l].a : nullptr,
+                         desc_.vc ? lev_[l].b : nullptr, b0, b1, c0, c1, s_);
+    }
+  }
+  if (desc_.vc) {
+    for (int l = 0; l < numLevels(); ++l)
+      lambdaLevel(amrDev_[l], lev_[l].a, lev_[l].b, desc_.alpha, desc_.beta, lev_[l].lambda, s_);
+    for (size_t d = 0; d < mg_.size(); ++d) {
+      averageCoefficients(amrDev_[0], mgDev_[d], 2 << d, lev_[0].a, lev_[0].b, mgf_[d].a, mgf_[d].b, s_);
+      lambdaLevel(mgDev_[d], mgf_[d].a, mgf_[d].b, desc_.alpha, desc_.beta, mgf_[d].lambda, s_);
+    }
+    coef32Stale_ = true;
+    Coef<double> cb = coefMG((int)mg_.size());
+    for (BottomWork& w : bottoms_) {
+      gatherSlots(w, cb.a, w.a, s_);
+      for (int k = 0; k < 3; ++k) gatherSlots(w, cb.b[k], w.b[k], s_);
+      gatherSlots(w, cb.lambda, w.lam, s_);
+    }
+  }
+  ck(cudaStreamSynchronize(s_), "device inputs");
+}
+
+int64_t Solver::hierarchyCells(int k, int l) const {
+  if (k < 0 || k >= nh_ || l < 0 || l >= numLevels()) throw std::invalid_argument("cmg: hierarchy or level out of range");
+  const LevelPlan& p = amr_[l];
+  if (nh_ == 1) return p.grids.numCells();
+  int64_t n = 0;
+  for (size_t b = 0; b < p.boxes.size(); ++b)
+    if (p.boxHier[b] == k) n += p.grids.boxes[b].numPts();
+  return n;
 }
 
 Coef<double> Solver::coefAMR(int l) const {
@@ -779,7 +943,7 @@ void Solver::setAlphaAndBeta(double alpha, double beta) {
       lambdaLevel(amrDev_[l], lev_[l].a, lev_[l].b, desc_.alpha, desc_.beta, lev_[l].lambda, s_);
     for (size_t d = 0; d < mg_.size(); ++d)
       lambdaLevel(mgDev_[d], mgf_[d].a, mgf_[d].b, desc_.alpha, desc_.beta, mgf_[d].lambda, s_);
-    gatherSlots(bottom_, coefMG((int)mg_.size()).lambda, bottom_.lam, s_);
+    for (BottomWork& w : bottoms_) gatherSlots(w, coefMG((int)mg_.size()).lambda, w.lam, s_);
     coef32Stale_ = true;
   } else {
     desc_.alpha = alpha * alpha0_;
@@ -789,6 +953,7 @@ void Solver::setAlphaAndBeta(double alpha, double beta) {
 }
 
 std::vector<SolveResult> Solver::backwardEuler(const SolveParams& p, double dt, int nsteps, bool zeroPhi) {
+  needSingle();
   if (nsteps < 0) throw std::invalid_argument("cmg: negative step count");
   const int nlev = numLevels();
   if (src_.empty()) {
@@ -810,6 +975,7 @@ std::vector<SolveResult> Solver::backwardEuler(const SolveParams& p, double dt, 
 }
 
 std::vector<SolveResult> Solver::tga(const SolveParams& p, double dt, int nsteps) {
+  needSingle();
   if (nsteps < 0) throw std::invalid_argument("cmg: negative step count");
   const int nlev = numLevels();
   // AMRTGA::setMu (AMRTGA.H:351-366).
@@ -866,7 +1032,7 @@ void Solver::setBottomConfig(const BottomConfig& c) {
   if (c.kind != 0 && c.kind != 1) throw std::invalid_argument("cmg: bottom solver is BiCGStab (0) or relaxation (1)");
   if (c.normType != 0 && c.normType != 2) throw std::invalid_argument("cmg: bottom solver norm type is 0 or 2");
   if (c.imax < 0 || c.numRestarts < 0) throw std::invalid_argument("cmg: negative bottom solver iteration limit");
-  bottom_.cfg = c;
+  bottomCfg_ = c;
   // captured bottom launches hold the old parameters
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
   graphs_.clear();
@@ -933,7 +1099,7 @@ double Solver::computeAMRResidual(std::vector<double*>& res, std::vector<double*
 // into dNorm_ (no host synchronisation, so it can be captured).
 void Solver::launchAMRResidual(std::vector<double*>& res, std::vector<double*>& phi, std::vector<double*>& rhs,
                                int lmax) {
-  ck(cudaMemsetAsync(dNorm_, 0, sizeof(double), s_), "norm reset");
+  ck(cudaMemsetAsync(dNorm_, 0, nh_ * sizeof(double), s_), "norm reset");
   for (int ilev = 0; ilev <= lmax; ++ilev) {
     amrResidualLevel<double>(ilev, lmax, res.data(), phi.data(), rhs.data());
     if (ilev != lmax) zeroCovered(amrDev_[ilev], res[ilev], s_);
@@ -949,13 +1115,22 @@ double Solver::readNorm() {
   return hostScalars_[0];
 }
 
+std::vector<double> Solver::readNorms() {
+  double* h = hostScalars_ + 2;
+  ck(cudaMemcpyAsync(h, dNorm_, nh_ * sizeof(double), cudaMemcpyDeviceToHost, s_), "norm d2h");
+  ck(cudaStreamSynchronize(s_), "norm sync");
+  return std::vector<double>(h, h + nh_);
+}
+
 // BiCGStab bottom solve in FP64 whatever the V-cycle's precision: an FP32
 // V-cycle hands its correction and residual over through the FP64 fields of
 // the bottom level (free during the FP32 cycle) and takes the result back.
 template <>
 void Solver::bottom<double>(int depth, double* corr, double* res) {
   const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
-  timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr, res, coefMG(depth), bottom_, sp_.eps, dMetric_, s_); });
+  timed(P_BOTTOM, 0.0, [&]() {
+    bottomSolve(L, corr, res, coefMG(depth), dBottoms_, nh_, maxBottomBoxes_, bottomCfg_, sp_.eps, dMetric_, s_);
+  });
 }
 template <>
 void Solver::bottom<float>(int depth, float* corr, float* res) {
@@ -964,7 +1139,9 @@ void Solver::bottom<float>(int depth, float* corr, float* res) {
   double* res64 = depth == 0 ? lev_[0].res : mgf_[depth - 1].res;
   convert(corr64, corr, L.nelem, s_);
   convert(res64, res, L.nelem, s_);
-  timed(P_BOTTOM, 0.0, [&]() { bottomSolve(L, corr64, res64, coefMG(depth), bottom_, sp_.eps, dMetric_, s_); });
+  timed(P_BOTTOM, 0.0, [&]() {
+    bottomSolve(L, corr64, res64, coefMG(depth), dBottoms_, nh_, maxBottomBoxes_, bottomCfg_, sp_.eps, dMetric_, s_);
+  });
   convert(corr, corr64, L.nelem, s_);
 }
 
@@ -1241,6 +1418,7 @@ void Solver::mlPreCond(MLVec& cor, MLVec& res, const MLSolveParams& p) {
 }
 
 void Solver::interpToFine(int l, bool pwc) {
+  needSingle();
   if (l < 1 || l >= numLevels()) throw std::invalid_argument("cmg: fine interpolation needs a level in 1..finest");
   if (fineInterp_.size() < amr_.size()) fineInterp_.resize(amr_.size());
   if (!fineInterp_[l])
@@ -1255,6 +1433,7 @@ void Solver::interpToFine(int l, bool pwc) {
 }
 
 MLSolveResult Solver::solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroPhi) {
+  needSingle();
   if (p.mgIters < 0 || p.mgSmooth < 0 || p.imax < 0 || p.numRestarts < 0)
     throw std::invalid_argument("cmg: invalid BiCGStab parameters");
   if (!tuned_) tuneRelaxation();
@@ -1390,6 +1569,7 @@ MLSolveResult Solver::solveMultilevelBiCGStab(const MLSolveParams& p, bool zeroP
 }
 
 double Solver::residualNorm() {
+  needSingle();
   int lmax = numLevels() - 1;
   std::vector<double*> res(lmax + 1), phi(lmax + 1), rhs(lmax + 1);
   for (int l = 0; l <= lmax; ++l) {
@@ -1414,10 +1594,15 @@ SolveResult Solver::solveMixed(const SolveParams& p, bool zeroPhi) { return solv
 void Solver::iterationBody(bool mixed, std::vector<double*>& ures, std::vector<double*>& phi,
                            std::vector<double*>& rhs) {
   const int lmax = numLevels() - 1;
+  // A forest changes phi only for the hierarchies still iterating (dActive_).
+  const bool forest = nh_ > 1;
   if (!mixed) {
     amrVCycle<double>(lmax, lmax);
     for (int l = 0; l <= lmax; ++l) {
-      incr(amrDev_[l], lev_[l].phi, lev_[l].ucorr, 1.0, s_);
+      if (forest)
+        incrActive(amrDev_[l], lev_[l].phi, (const double*)lev_[l].ucorr, dActive_, s_);
+      else
+        incr(amrDev_[l], lev_[l].phi, lev_[l].ucorr, 1.0, s_);
       zeroField(amrDev_[l], lev_[l].ucorr);
     }
   } else {
@@ -1426,12 +1611,18 @@ void Solver::iterationBody(bool mixed, std::vector<double*>& ures, std::vector<d
       zeroField(amrDev_[l], lev32_[l].ucorr);
     }
     amrVCycle<float>(lmax, lmax);
-    for (int l = 0; l <= lmax; ++l) incrMixed(amrDev_[l], lev_[l].phi, lev32_[l].ucorr, s_);
+    for (int l = 0; l <= lmax; ++l) {
+      if (forest)
+        incrActive(amrDev_[l], lev_[l].phi, (const float*)lev32_[l].ucorr, dActive_, s_);
+      else
+        incrMixed(amrDev_[l], lev_[l].phi, lev32_[l].ucorr, s_);
+    }
   }
   launchAMRResidual(ures, phi, rhs, lmax);
 }
 
 SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
+  needSingle();
   if (!tuned_) tuneRelaxation();
   if (mixed) ensure32();
   sp_ = p;
@@ -1487,6 +1678,82 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
   out.exitStatus = int(!goRedu) + int(!goIter) * 2 + int(!goHang) * 4 + int(!goNorm) * 8;
   out.iterations = iter;
   out.diverged = !finite;
+  return out;
+}
+
+// AMRMultiGrid::solve for every hierarchy of a forest together: the loop of
+// solveImpl with one norm, stopping rule and iteration count per hierarchy;
+// an iteration runs while any hierarchy goes on, and only the going ones
+// take its correction.
+std::vector<SolveResult> Solver::solveForest(const SolveParams& p, bool zeroPhi, bool mixed) {
+  if (!tuned_) tuneRelaxation();
+  if (mixed) ensure32();
+  sp_ = p;
+  const int lmax = numLevels() - 1, K = nh_;
+  std::vector<SolveResult> out(K);
+  std::vector<double*> ures(lmax + 1), phi(lmax + 1), rhs(lmax + 1);
+  for (int l = 0; l <= lmax; ++l) {
+    zeroField(amrDev_[l], lev_[l].ucorr);
+    zeroField(amrDev_[l], lev_[l].ures);
+    if (zeroPhi) zeroField(amrDev_[l], lev_[l].phi);
+    ures[l] = lev_[l].ures;
+    phi[l] = lev_[l].phi;
+    rhs[l] = lev_[l].rhs;
+  }
+  launchAMRResidual(ures, phi, rhs, lmax);
+  const std::vector<double> r0 = readNorms();
+  std::vector<double> rnorm = r0, normLast(K);
+  // each hierarchy's bottom solver gets its own initial norm as its metric
+  for (int k = 0; k < K; ++k) hostScalars_[2 + k] = r0[k];
+  ck(cudaMemcpyAsync(dMetric_, hostScalars_ + 2, K * sizeof(double), cudaMemcpyHostToDevice, s_), "metric");
+  std::vector<char> goNorm(K), goRedu(K), goIter(K), goHang(K), goMin(K), finite(K), going(K);
+  int interrupted = 0;
+  auto update = [&](int k, int iter) {
+    goNorm[k] = rnorm[k] > p.normThresh;
+    goRedu[k] = rnorm[k] > p.eps * r0[k];
+    goIter[k] = iter < p.iterMax;
+    goHang[k] = iter < p.imin || rnorm[k] < (1 - p.hang) * normLast[k];
+    goMin[k] = iter < p.iterMin;
+    finite[k] = std::isfinite(rnorm[k]);
+    going[k] = finite[k] && !interrupted && (goMin[k] || (goIter[k] && goRedu[k] && goHang[k] && goNorm[k]));
+  };
+  if (p.interrupt) interrupted = p.interrupt(0);
+  for (int k = 0; k < K; ++k) {
+    normLast[k] = 2 * r0[k];
+    out[k].history.push_back(rnorm[k]);
+    update(k, 0);
+  }
+  const bool graph = useGraphs_ && !profOn_;
+  int iter = 0;
+  while (std::any_of(going.begin(), going.end(), [](char g) { return g != 0; })) {
+    for (int k = 0; k < K; ++k) {
+      hostActive_[k] = going[k];
+      if (going[k]) normLast[k] = rnorm[k];
+    }
+    ck(cudaMemcpyAsync(dActive_, hostActive_, K * sizeof(int), cudaMemcpyHostToDevice, s_), "active flags");
+    if (graph) {
+      cudaGraphExec_t exec = iterationGraph(mixed, ures, phi, rhs);
+      ck(cudaGraphLaunch(exec, s_), "graph launch");
+      addLaunches(graphLaunches_[exec]);
+    } else {
+      iterationBody(mixed, ures, phi, rhs);
+    }
+    const std::vector<double> r = readNorms();
+    iter++;
+    if (p.interrupt) interrupted = p.interrupt(iter);
+    for (int k = 0; k < K; ++k) {
+      if (!hostActive_[k]) continue;
+      rnorm[k] = r[k];
+      out[k].iterations = iter;
+      out[k].history.push_back(rnorm[k]);
+      update(k, iter);
+    }
+  }
+  for (int k = 0; k < K; ++k) {
+    out[k].exitStatus = int(!goRedu[k]) + int(!goIter[k]) * 2 + int(!goHang[k]) * 4 + int(!goNorm[k]) * 8;
+    out[k].diverged = !finite[k];
+    out[k].interrupted = interrupted;
+  }
   return out;
 }
 

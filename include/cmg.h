@@ -81,6 +81,35 @@ int cmg_hierarchy_create_bc(const int domain_lo[3], const int domain_hi[3], doub
                             const int bc[6], cmg_hierarchy** out);
 int cmg_hierarchy_destroy(cmg_hierarchy* h);
 
+/* A forest: nh hierarchies with the same level-0 domain, dx0, level count,
+ * operator and boundary types, whose level-0 layouts coarsen alike (the same
+ * multigrid depths), solved together: every operation of a V-cycle is one
+ * launch over the boxes of all of them (their levels concatenated, each
+ * hierarchy in its own element range), the bottom solves one thread block per
+ * hierarchy.  nboxes holds nh * nlevels counts (hierarchy by hierarchy, level
+ * by level) and boxes the boxes in that order.  The handle is a hierarchy
+ * whose level data (cmg_set_rhs, cmg_get_phi, ...) is the hierarchies' data
+ * one after the other (cmg_forest_cells gives each part); solve it with
+ * cmg_forest_solve.  The single-hierarchy solves, operators and FineInterp
+ * refuse a forest with CMG_EINVAL. */
+int cmg_forest_create(int nh, const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
+                      const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta, const int bc[6],
+                      cmg_hierarchy** out);
+int cmg_forest_size(const cmg_hierarchy* h, int* nh);
+/* Valid cells of hierarchy k on a level. */
+int cmg_forest_cells(const cmg_hierarchy* h, int k, int level, int64_t* out);
+/* cmg_fill_synthetic (device generator) of every hierarchy, seeds[k] for hierarchy k. */
+int cmg_forest_fill_synthetic(cmg_hierarchy* h, const uint64_t* seeds);
+/* AMRMultiGrid::solve of every hierarchy of the forest at once (mixed != 0:
+ * FP32 V-cycles in FP64 refinement, as cmg_solve_mixed): each hierarchy keeps
+ * its own residual norm, stopping rule and bottom-solver metric, and its phi
+ * takes no correction after its own stop, so exit_status[k], iterations[k]
+ * and phi of hierarchy k are those of its own solve.  final_norm (may be
+ * NULL): each hierarchy's last composite residual norm.  CMG_EDIVERGED when a
+ * hierarchy's norm became non-finite (the others' results are written). */
+int cmg_forest_solve(cmg_hierarchy* h, const cmg_solve_params* p, int zero_phi, int mixed, int* exit_status,
+                     int* iterations, double* final_norm);
+
 /* Sizes of the per-level data arrays. */
 int cmg_num_levels(const cmg_hierarchy* h, int* out);
 int cmg_num_boxes(const cmg_hierarchy* h, int level, int* out);

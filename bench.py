@@ -440,6 +440,8 @@ def run_batch(args):
         h.fill_synthetic(sp["seed"], device=not args.host_fill)
         return h
 
+    if args.forest:
+        return run_batch_forest(args, cmg, specs, params, pool)
     for w0 in range(0, len(specs), wave):
         hs = list(pool.map(build, specs[w0:w0 + wave]))
         cells += sum(sum(h.num_cells(l) for l in range(h.nlev)) for h in hs)
@@ -489,6 +491,76 @@ def run_batch(args):
         "plain_fp64_one_at_a_time": {"value": base, "unit": "solves/s", "ratio": value / base},
         "vcycles_mixed_mean": float(np.mean(iters_mixed)), "vcycles_fp64_mean": float(np.mean(iters_fp64)),
         "not_converged": not_converged,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_batch_forest(args, cmg, specs, params, pool):
+    """Batching with forests: the problems grouped by (base size, max box, operator), each group one forest
+    (cmg_forest_create: its hierarchies' levels merged, one kernel launch per V-cycle operation for the whole
+    group, a bottom-solve block per hierarchy, per-hierarchy stopping), the forests solved concurrently on
+    their own streams, FP32 V-cycles inside FP64 refinement.  Every hierarchy's result is the one its own
+    solve gives (tests/test_forest_gpu.py)."""
+    import torch
+    groups = {}
+    for sp in specs:
+        groups.setdefault((sp["n0"], sp["max_box"], sp["op"]), []).append(sp)
+    cap = max(1, args.forest_size)
+    parts = []
+    for key in sorted(groups):
+        g = groups[key]
+        for a in range(0, len(g), cap):
+            parts.append(g[a:a + cap])
+
+    def build(part):
+        sp0 = part[0]
+        hb = [cmg.synthetic_hierarchy(sp["n0"], sp["levels"], sp["max_box"], sp["block_factor"], sp["fill_ratio"],
+                                      sp["seed"], sp["thresh"]) for sp in part]
+        f = cmg.Forest(sp0["n0"], hb, op=sp0["op"], alpha=sp0["alpha"], beta=sp0["beta"])
+        f.fill_synthetic([sp["seed"] for sp in part])
+        f.use_graphs(True)
+        f.set_relax_mode(args.relax_mode)
+        return f
+
+    forests = list(pool.map(build, parts))
+    cells = sum(sum(f.num_cells(l) for l in range(f.nlev)) for f in forests)
+    # first solve of each forest: autotuning and graph capture, not timed
+    list(pool.map(lambda f: f.solve(params, mixed=True), forests))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    outs = list(pool.map(lambda f: f.solve(params, mixed=True), forests))
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    res = [o for out in outs for o in out]
+    iters = [o["iterations"] for o in res]
+    not_converged = sum(1 for o in res if not (o["exit_status"] & 1))
+    for f in forests:
+        f.close()
+    value = len(specs) / t_batch
+    cpu = None
+    if not args.no_cpu_baseline:
+        procs = max(1, min(os.cpu_count() or 1, 8))
+        sample = specs[::16]
+        r = cpu_reference_sample(cmg, sample, procs)
+        if r:
+            cpu = {"value": r[0], "unit": "solves/s", "cores": procs, "kind": "reference",
+                   "sample": f"{len(sample)} of the {len(specs)} problems (every 16th), full reference solves to "
+                             f"1e-10, {procs} at a time on the host cores; rate = problems / wall time "
+                             f"({r[1]:.1f} s)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": 1000.0 * t_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"{len(specs)} independent 2-level hierarchies, base 32^3-128^3 log-uniform (x16), "
+                               "max box 16/24/32, Poisson or VC Helmholtz, rel. residual 1e-10",
+                   "batching": f"{len(forests)} forests (hierarchies grouped by base size, max box and operator, "
+                               f"at most {cap} per forest), solved concurrently on {args.inflight} host threads, "
+                               "one stream per forest",
+                   "cells": cells, "relax_mode": args.relax_mode,
+                   "timing": "wall clock around one solve of every forest (all resident; host set-up, autotuning "
+                             "and graph capture in an untimed first solve)"},
+        "cpu_baseline": cpu,
+        "vcycles_mixed_mean": float(np.mean(iters)), "not_converged": not_converged,
     }
     print(json.dumps(line), flush=True)
 
@@ -701,6 +773,8 @@ def main():
     ap.add_argument("--batch", type=int, default=512, help="config3: number of hierarchies")
     ap.add_argument("--host-fill", action="store_true", help="config3: generate the inputs on the host")
     ap.add_argument("--wave", type=int, default=128, help="config3: hierarchies resident at once")
+    ap.add_argument("--forest", type=int, default=1, help="config3: 1 = batch the problems in forests")
+    ap.add_argument("--forest-size", type=int, default=64, help="config3: most hierarchies in one forest")
     ap.add_argument("--inflight", type=int, default=16, help="config3/4: concurrent solves")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="config4: arrival rates (req/s)")
     ap.add_argument("--host-tags", action="store_true", help="config4: tag for grid generation on the host")

@@ -633,6 +633,10 @@ int cmg_residual_norm_noalloc(cmg_hierarchy* h, double* out) {
   });
 }
 
+int cmg_residual_norm_noalloc_forget(void) {
+  return guard([&]() { cmg::forgetNoAllocScratch(); });
+}
+
 static int syntheticHierarchyImpl(int n0, int nlevels, int max_box, int block_factor, double fill_ratio,
                                   uint64_t seed, double thresh, int* nlevels_out, int* nboxes, cmg_box* boxes,
                                   int cap, int* ntotal, bool device) {

@@ -13,6 +13,8 @@ enum { NOALLOC_MAX_BOXES = 4096, NOALLOC_MAX_LEVELS = 16, NOALLOC_MAX_DEVICES = 
 // Composite residual max-norm of the hierarchy's current phi and rhs, same
 // value as Solver::residualNorm, allocating no memory on success.
 double residualNormNoAlloc(Solver& S);
+// Drops the scratch addresses found so far (after a device reset).
+void forgetNoAllocScratch();
 
 }  // namespace cmg
 

@@ -67,6 +67,15 @@ double* scratchFor(int dev) {
   return g_scratchPtr[dev];
 }
 
+}  // namespace
+
+void forgetNoAllocScratch() {
+  std::lock_guard<std::mutex> lock(g_setupMutex);
+  for (double*& p : g_scratchPtr) p = nullptr;
+}
+
+namespace {
+
 enum { NT = 256 };
 
 // max(a, b) that keeps a NaN from either side (fmax drops it), so that a

@@ -288,9 +288,13 @@ int cmg_fine_interp_is_fused(const cmg_fine_interp* fi, int* out);
  * cudaGetSymbolAddress (that device made current); make it before any stream
  * capture begins on the device.  Every call zeroes the running maximum
  * itself.  Calls that overlap in time on one device share the scratch and
- * race: serialise them. */
+ * race: serialise them.  The address found is kept for the process; a
+ * caller that resets a device (cudaDeviceReset) calls
+ * cmg_residual_norm_noalloc_forget() afterwards, and its next call on that
+ * device looks the scratch up again (outside any capture, as a first call). */
 #define CMG_NOALLOC_MAX_BOXES 4096
 int cmg_residual_norm_noalloc(cmg_hierarchy* h, double* out);
+int cmg_residual_norm_noalloc_forget(void);
 
 /* Fills rhs (all levels) and, for op = 1, a and b from the seeded synthetic
  * workload recipe (Gaussian bumps; exp of a random Fourier series), then

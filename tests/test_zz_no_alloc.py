@@ -76,3 +76,14 @@ def test_rejects_level_beyond_scratch(cmg):
     # The rejected call launched nothing; the ordinary entry point still works.
     assert np.isfinite(h.residual_norm())
     h.close()
+
+
+@pytest.mark.gpu
+def test_forgotten_scratch_is_looked_up_again(cmg):
+    """cmg_residual_norm_noalloc_forget drops the cached scratch address (for a caller that reset the device);
+    the next call looks it up again and gives the same value."""
+    h, _ = hierarchy(cmg, "vc_3lev_16")
+    before = h.residual_norm_noalloc()
+    assert cmg.lib().cmg_residual_norm_noalloc_forget() == cmg.CMG_OK
+    assert h.residual_norm_noalloc() == before
+    h.close()

@@ -522,7 +522,9 @@ def run_batch_forest(args, cmg, specs, params, pool):
         f.set_relax_mode(args.relax_mode)
         return f
 
+    t_build = time.perf_counter()
     forests = list(pool.map(build, parts))
+    t_build = time.perf_counter() - t_build
     cells = sum(sum(f.num_cells(l) for l in range(f.nlev)) for f in forests)
     # first solve of each forest: autotuning and graph capture, not timed
     list(pool.map(lambda f: f.solve(params, mixed=True), forests))
@@ -561,8 +563,61 @@ def run_batch_forest(args, cmg, specs, params, pool):
                              "and graph capture in an untimed first solve)"},
         "cpu_baseline": cpu,
         "vcycles_mixed_mean": float(np.mean(iters)), "not_converged": not_converged,
+        "host_setup_s": t_build,
     }
+    if getattr(args, "quiet_line", False):
+        return line
     print(json.dumps(line), flush=True)
+
+
+def extra_workloads(args, cmg):
+    """The precision and batching workloads measured in the default run, so that their numbers come from the
+    same run as the headline: config 2 (3-level 256^3 VC Helmholtz, 149M cells, FP32 V-cycles in FP64
+    refinement, 3 timed solves after one warm-up, CUDA events on the solver's stream) and config 3 (512
+    independent 2-level hierarchies in forests, wall clock around one solve of every forest)."""
+    import concurrent.futures as cf
+    import torch
+    out = {}
+    try:
+        meta = golden_meta(WORKLOADS["config2"]["golden"])
+        h = cmg.Hierarchy(meta["n0"], meta["boxes"], op=meta["op"], alpha=meta["alpha"], beta=meta["beta"])
+        h.fill_synthetic(meta["seed"])
+        p = cmg.solve_params(pre=meta["pre"], post=meta["post"], bottom=meta["bottom"], iter_max=meta["iters"],
+                             eps=meta["eps"], hang=meta["hang"])
+        h.use_graphs(True)
+        o = h.solve(p, mixed=True)
+        stream = torch.cuda.ExternalStream(h.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        n = 3
+        for _ in range(n):
+            o = h.solve(p, mixed=True)
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b) / n
+        out["config2"] = {"workload": WORKLOADS["config2"]["name"], "value": 1000.0 / ms, "unit": "solves/s",
+                          "ms_per_solve": ms, "fp64_refinement_steps": o["iterations"],
+                          "exit_status": o["exit_status"], "reference_vcycles": len(meta["residual_history"]) - 1,
+                          "cells": sum(h.num_cells(l) for l in range(len(meta["boxes"]))), "dtype": "f32+f64",
+                          "timing": "CUDA events on the solver's stream around 3 solves after one untimed solve"}
+        h.close()
+    except Exception as e:  # reported, not fatal: the headline line stands on its own
+        out["config2"] = {"error": str(e)[:300]}
+    try:
+        specs = batch_specs(512, 20261203)
+        pool = cf.ThreadPoolExecutor(max_workers=16)
+        a2 = argparse.Namespace(**vars(args))
+        a2.forest_size, a2.inflight, a2.relax_mode, a2.no_cpu_baseline, a2.quiet_line = 64, 16, 0, True, True
+        line = run_batch_forest(a2, cmg, specs, cmg.solve_params(eps=1e-10), pool)
+        out["config3"] = {k: line[k] for k in ("value", "unit", "ms_per_step", "vcycles_mixed_mean", "not_converged",
+                                               "host_setup_s", "dtype")}
+        out["config3"]["workload"] = line["config"]["workload"]
+        out["config3"]["batching"] = line["config"]["batching"]
+        out["config3"]["timing"] = line["config"]["timing"]
+    except Exception as e:
+        out["config3"] = {"error": str(e)[:300]}
+    return out
 
 
 def fineinterp_reference(meta, repeat):
@@ -774,6 +829,8 @@ def main():
     ap.add_argument("--host-fill", action="store_true", help="config3: generate the inputs on the host")
     ap.add_argument("--wave", type=int, default=128, help="config3: hierarchies resident at once")
     ap.add_argument("--forest", type=int, default=1, help="config3: 1 = batch the problems in forests")
+    ap.add_argument("--extras", type=int, default=1,
+                    help="config1, one GPU: also measure config 2 (mixed) and config 3 (forests) in the same run")
     ap.add_argument("--forest-size", type=int, default=64, help="config3: most hierarchies in one forest")
     ap.add_argument("--inflight", type=int, default=16, help="config3/4: concurrent solves")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="config4: arrival rates (req/s)")
@@ -985,11 +1042,14 @@ def main():
         }
         if accuracy:
             line["accuracy"] = accuracy
+    h.close()
+    if rank == 0:
+        if world == 1 and args.workload == "config1" and args.extras:
+            line["extra_workloads"] = extra_workloads(args, cmg)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    h.close()
 
 
 if __name__ == "__main__":

@@ -142,6 +142,11 @@ template <class T> void reflux(const LevelDev& C, T* lofphiC, const T* phiC, con
 // lhs += scale * x (LevelDataOps::incr); valid cells as the reference, ghost
 // slots too (refilled before any read).
 template <class T> void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s);
+// lhs += x, then x = lhs (the increment and the copy back of AMRVCycle's
+// post-smoothing), in one pass over whole level arrays.
+template <class T> void incrCopy(const LevelDev& L, T* lhs, T* x, cudaStream_t s);
+// lhs += x, then x = 0, in one pass over whole level arrays.
+template <class T> void incrZero(const LevelDev& L, T* lhs, T* x, cudaStream_t s);
 // lhs += x over valid cells, an FP32 correction added to an FP64 field.
 void incrMixed(const LevelDev& L, double* lhs, const float* x, cudaStream_t s);
 // dst[q] = src[q] for every element of a level array (valid and ghost cells).

@@ -732,22 +732,51 @@ __global__ void k_average(const BoxDesc* fboxes, const BoxDesc* cboxes, const Co
   coarse[cellIndex(cboxes[it.cbox], I, J, K)] = T(0.125) * sum;
 }
 
-// AMRProlongS (AMRPoissonOp.cpp:959-990): fine += coarse(i/2).
+// AMRProlongS (AMRPoissonOp.cpp:959-990): fine += coarse(i/2).  One thread
+// per coarse cell of an item (chunks over the items' coarse cells, x
+// fastest) updates its eight fine cells: the coarse value is read once, the
+// eight fine loads are independent, and for each of the eight child offsets
+// a warp's threads touch consecutive slots of one colour half.
 template <class T>
 __global__ void k_prolongamr(const BoxDesc* fboxes, const BoxDesc* cboxes, const CoarseFineItem* items,
                              const Chunk* chunks, T* fine, const T* coarse) {
   Chunk ch = chunks[blockIdx.x];
   const CoarseFineItem it = items[ch.box];
   const int q = ch.start + threadIdx.x;
-  // fine cells of the item's region in x-fastest order: a warp covers a fine
-  // row segment and the coarse row segment above it
-  const int fnx = 2 * (it.hi[0] - it.lo[0] + 1), fny = 2 * (it.hi[1] - it.lo[1] + 1);
-  const int fnz = 2 * (it.hi[2] - it.lo[2] + 1);
-  if (q >= fnx * fny * fnz) return;
-  const int r = q / fnx, fi = q - r * fnx, fk = r / fny, fj = r - fk * fny;
-  const int I = it.lo[0] + (fi >> 1), J = it.lo[1] + (fj >> 1), K = it.lo[2] + (fk >> 1);
-  int64_t f = cellIndex(fboxes[it.fbox], 2 * it.lo[0] + fi, 2 * it.lo[1] + fj, 2 * it.lo[2] + fk);
-  fine[f] = fine[f] + coarse[cellIndex(cboxes[it.cbox], I, J, K)];
+  const int nx = it.hi[0] - it.lo[0] + 1, ny = it.hi[1] - it.lo[1] + 1, nz = it.hi[2] - it.lo[2] + 1;
+  if (q >= nx * ny * nz) return;
+  const int r = q / nx, kk = r / ny;
+  const int I = it.lo[0] + (q - r * nx), J = it.lo[1] + (r - kk * ny), K = it.lo[2] + kk;
+  const BoxDesc fb = fboxes[it.fbox];
+  const T c = coarse[cellIndex(cboxes[it.cbox], I, J, K)];
+  int64_t f[8];
+  T v[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) f[n] = cellIndex(fb, 2 * I + (n & 1), 2 * J + ((n >> 1) & 1), 2 * K + (n >> 2));
+#pragma unroll
+  for (int n = 0; n < 8; ++n) v[n] = fine[f[n]];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) fine[f[n]] = v[n] + c;
+}
+
+// lhs = lhs + x * 1 (k_incr_flat's arithmetic), then x = the new lhs: the
+// increment followed by a copy back, in one pass.
+template <class T>
+__global__ void k_incr_copy_flat(T* lhs, T* x, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    const T v = lhs[q] + x[q] * T(1.0);
+    lhs[q] = v;
+    x[q] = v;
+  }
+}
+
+// lhs = lhs + x * 1, then x = 0: the increment followed by zeroing x.
+template <class T>
+__global__ void k_incr_zero_flat(T* lhs, T* x, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    lhs[q] = lhs[q] + x[q] * T(1.0);
+    x[q] = T(0);
+  }
 }
 
 // QuadCFStencil derivatives (AMRTools/QuadCFStencil.cpp:33-260).
@@ -1464,7 +1493,7 @@ void averageAMR(const LevelDev& F, const LevelDev& C, T* coarse, const T* fine, 
 template <class T>
 void prolongAMR(const LevelDev& F, const LevelDev& C, T* fine, const T* coarse, cudaStream_t s) {
   if (F.nItemChF == 0) return;
-  k_prolongamr<T><<<F.nItemChF, CHUNK, 0, s>>>(F.boxes, C.boxes, F.items, F.itemChF, fine, coarse);
+  k_prolongamr<T><<<F.nItemChC, CHUNK, 0, s>>>(F.boxes, C.boxes, F.items, F.itemChC, fine, coarse);
   CMG_LAUNCHED("prolongAMR");
 }
 
@@ -1499,6 +1528,20 @@ void incr(const LevelDev& L, T* lhs, const T* x, double scale, cudaStream_t s) {
   if (L.nelem == 0) return;
   k_incr_flat<T, T><<<flatBlocks(L.nelem), 256, 0, s>>>(lhs, x, T(scale), L.nelem);
   CMG_LAUNCHED("incr");
+}
+
+template <class T>
+void incrCopy(const LevelDev& L, T* lhs, T* x, cudaStream_t s) {
+  if (L.nelem == 0) return;
+  k_incr_copy_flat<T><<<flatBlocks(L.nelem), 256, 0, s>>>(lhs, x, L.nelem);
+  CMG_LAUNCHED("incrCopy");
+}
+
+template <class T>
+void incrZero(const LevelDev& L, T* lhs, T* x, cudaStream_t s) {
+  if (L.nelem == 0) return;
+  k_incr_zero_flat<T><<<flatBlocks(L.nelem), 256, 0, s>>>(lhs, x, L.nelem);
+  CMG_LAUNCHED("incrZero");
 }
 
 template <class T>
@@ -1724,6 +1767,8 @@ void averageCoefficients(const LevelDev& F, const LevelDev& C, int r, const doub
   template void quadCF<T>(const LevelDev&, T*, const T*, cudaStream_t);                                    \
   template void reflux<T>(const LevelDev&, T*, const T*, const T*, const Coef<T>&, const Coef<T>&,         \
                           cudaStream_t);                                                                   \
+  template void incrCopy<T>(const LevelDev&, T*, T*, cudaStream_t);                                         \
+  template void incrZero<T>(const LevelDev&, T*, T*, cudaStream_t);                                         \
   template void incr<T>(const LevelDev&, T*, const T*, double, cudaStream_t);                              \
   template void maxNorm<T>(const LevelDev&, const T*, double*, cudaStream_t);
 

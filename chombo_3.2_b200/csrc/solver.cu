@@ -1229,8 +1229,7 @@ void Solver::amrVCycle(int ilev, int lmax) {
   timed(P_OP, amr_[ilev].grids.numCells() * w * (desc_.vc ? 7.0 : 3.0), [&]() { residual(L, f.res, f.corr, f.res, coefA<T>(ilev), s_); });
   zeroField(L, f.ucorr);
   relaxAMR(ilev, f.ucorr, f.res, sp_.post);
-  incr(L, f.corr, f.ucorr, 1.0, s_);
-  copyField(L, f.ucorr, f.corr);
+  incrCopy(L, f.corr, f.ucorr, s_);  // corr += ucorr; ucorr = corr
 }
 
 template void Solver::amrVCycle<double>(int, int);
@@ -1612,8 +1611,8 @@ void Solver::iterationBody(bool mixed, std::vector<double*>& ures, std::vector<d
       if (forest)
         incrActive(amrDev_[l], lev_[l].phi, (const double*)lev_[l].ucorr, dActive_, s_);
       else
-        incr(amrDev_[l], lev_[l].phi, lev_[l].ucorr, 1.0, s_);
-      zeroField(amrDev_[l], lev_[l].ucorr);
+        incrZero(amrDev_[l], lev_[l].phi, lev_[l].ucorr, s_);  // phi += ucorr; ucorr = 0
+      if (forest) zeroField(amrDev_[l], lev_[l].ucorr);
     }
   } else {
     for (int l = 0; l <= lmax; ++l) {

@@ -51,6 +51,8 @@ struct LevelDev {
   const CFCoarse* cfC = nullptr;
   const CFFine* cfF = nullptr;
   int nCfF = 0;
+  int nCfC = 0;                 // coarse cells of the interpolation (cfC entries)
+  double* cfTmp = nullptr;      // 6 values per cfC entry (derivatives and the coarse value), T-typed
   const double* cfW = nullptr;
   const int64_t* cfOff = nullptr;
   // coarse/fine maps to the coarser level

@@ -619,12 +619,26 @@ template <class T>
 __global__ void k_maxnorm(const BoxDesc* boxes, const Chunk* chunks, int nchunks, const T* f, double* out) {
   // Blocks stride over the chunks (one chunk each when the grid covers
   // them), so a large level sends one atomic per block, not per chunk.
+  // Up to four chunks per step, their table loads and values issued
+  // together (the max does not depend on the order).
   double v = 0.0;
-  for (int cix = blockIdx.x; cix < nchunks; cix += gridDim.x) {
-    Chunk ch = chunks[cix];
-    const BoxDesc bd = boxes[ch.box];
-    int i, j, k;
-    if (allCell(bd, ch.start + threadIdx.x, i, j, k)) v = nanMax(v, fabs((double)f[cellIndex(bd, i, j, k)]));
+  for (int c0 = blockIdx.x; c0 < nchunks; c0 += 4 * gridDim.x) {
+    int64_t at[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      at[u] = -1;
+      const int cix = c0 + u * gridDim.x;
+      if (cix >= nchunks) continue;
+      const Chunk ch = chunks[cix];
+      const BoxDesc bd = boxes[ch.box];
+      int i, j, k;
+      if (allCell(bd, ch.start + threadIdx.x, i, j, k)) at[u] = cellIndex(bd, i, j, k);
+    }
+    double x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[u] = at[u] >= 0 ? fabs((double)f[at[u]]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v = nanMax(v, x[u]);
   }
   for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
   __shared__ double red[CHUNK / 32];
@@ -809,28 +823,42 @@ __device__ __forceinline__ T cfMixed(const CFDeriv& d, const double* w, const in
   return v / (dxc * dxc);
 }
 
-// QuadCFInterp::getPhiStar + interpOnIVS (AMRTools/QuadCFInterp.cpp:569-839):
-// phistar from the coarse Taylor expansion, then the quadratic through
-// phistar and two fine cells, in the Fortran (packed face,
+// QuadCFInterp::getPhiStar + interpOnIVS (AMRTools/QuadCFInterp.cpp:569-839),
+// in two launches.  First, per coarse cell under a coarse-fine face: the
+// tangential first and second derivatives, the mixed derivative and the
+// coarse value (six values into tmp); every fine ghost over that coarse cell
+// (four on a face) reads them instead of gathering the stencils again.
+template <class T>
+__global__ void k_cf_coarse(const CFCoarse* coarse, int n, const double* w, const int64_t* off, const T* phiC, T h,
+                            T* tmp) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const CFCoarse cc = coarse[t];
+  const T dxc = T(2) * h;
+  T* o = tmp + 6 * (int64_t)t;
+  o[0] = cfFirst(cc.d1[0], w, off, phiC, dxc);
+  o[1] = cfSecond(cc.d2[0], w, off, phiC, dxc);
+  o[2] = cfFirst(cc.d1[1], w, off, phiC, dxc);
+  o[3] = cfSecond(cc.d2[1], w, off, phiC, dxc);
+  o[4] = cfMixed(cc.mx, w, off, phiC, dxc);
+  o[5] = phiC[cc.cc];
+}
+
+// Second, per fine ghost: phistar from the coarse Taylor expansion, then the
+// quadratic through phistar and two fine cells, in the Fortran (packed face,
 // QuadCFInterpF.ChF:9-48) or C++ (unpacked face) arithmetic.
 template <class T>
-__global__ void k_quadcf(const CFFine* fine, int n, const CFCoarse* coarse, const double* w, const int64_t* off,
-                         T* phiF, const T* phiC, T h) {
+__global__ void k_quadcf(const CFFine* fine, int n, const T* tmp, T* phiF, T h) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const CFFine e = fine[t];
-  const CFCoarse cc = coarse[e.coarse];
-  const T dxc = T(2) * h;
-  T s1 = cfFirst(cc.d1[0], w, off, phiC, dxc);
-  T c1 = cfSecond(cc.d2[0], w, off, phiC, dxc);
-  T s2 = cfFirst(cc.d1[1], w, off, phiC, dxc);
-  T c2 = cfSecond(cc.d2[1], w, off, phiC, dxc);
-  T mx = cfMixed(cc.mx, w, off, phiC, dxc);
+  const T* c = tmp + 6 * (int64_t)e.coarse;
+  const T s1 = c[0], c1 = c[1], s2 = c[2], c2 = c[3], mx = c[4];
   const T x1 = T(e.x1), x2 = T(e.x2);
   T update1 = x1 * s1 + T(0.5) * x1 * x1 * c1;
   T update2 = x2 * s2 + T(0.5) * x2 * x2 * c2;
   T update3 = x1 * x2 * mx;
-  T ps = phiC[cc.cc] + update1 + update2 + update3;
+  T ps = c[5] + update1 + update2 + update3;
   T pa = phiF[e.pa], pb = phiF[e.pb];
   T r;
   if (e.packed) {
@@ -1500,8 +1528,10 @@ void prolongAMR(const LevelDev& F, const LevelDev& C, T* fine, const T* coarse, 
 template <class T>
 void quadCF(const LevelDev& F, T* phiF, const T* phiC, cudaStream_t s) {
   if (F.nCfF == 0) return;
-  int nb = (F.nCfF + 127) / 128;
-  k_quadcf<T><<<nb, 128, 0, s>>>(F.cfF, F.nCfF, F.cfC, F.cfW, F.cfOff, phiF, phiC, T(F.dx));
+  T* tmp = reinterpret_cast<T*>(F.cfTmp);
+  k_cf_coarse<T><<<(F.nCfC + 127) / 128, 128, 0, s>>>(F.cfC, F.nCfC, F.cfW, F.cfOff, phiC, T(F.dx), tmp);
+  CMG_LAUNCHED("quadCFCoarse");
+  k_quadcf<T><<<(F.nCfF + 127) / 128, 128, 0, s>>>(F.cfF, F.nCfF, tmp, phiF, T(F.dx));
   CMG_LAUNCHED("quadCF");
 }
 

@@ -180,6 +180,8 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
     d.nColor[c] = (int)p.chunksColor[c].size();
   }
   d.cfC = upload(bufs_, p.cfCoarse, s_);
+  d.nCfC = (int)p.cfCoarse.size();
+  if (d.nCfC > 0) d.cfTmp = alloc(6 * (size_t)d.nCfC);
   d.cfF = upload(bufs_, p.cfFine, s_);
   d.nCfF = (int)p.cfFine.size();
   d.cfW = upload(bufs_, p.cfW, s_);

@@ -785,12 +785,14 @@ def run_serving(args):
                 "mean_setup_ms": 1000.0 * float(np.mean([r["setup_seconds"] for r, _ in res])),
                 "mean_solve_ms": 1000.0 * float(np.mean([r["solve_seconds"] for r, _ in res])),
                 "mean_grid_ms": 1000.0 * float(np.mean([r["grid_seconds"] for r, _ in res])),
-                "mean_build_ms": 1000.0 * float(np.mean([r["build_seconds"] for r, _ in res]))}
+                "mean_build_ms": 1000.0 * float(np.mean([r["build_seconds"] for r, _ in res])),
+                "batched_requests": sum(1 for r, _ in res if r["batch_size"] > 1)}
 
     per_rate = {}
     for rate in rates:
         reqs = stream(rate, args.requests, int(rate))
-        res, wall = cmg.serve(reqs, hbm_budget=120e9, max_inflight=args.inflight, open_loop=True)
+        res, wall = cmg.serve(reqs, hbm_budget=120e9, max_inflight=args.inflight, open_loop=True,
+                              batch_window=args.batch_window, max_batch=16)
         per_rate[str(int(rate))] = stats(list(zip(res, [q["arrival"] for q in reqs])), wall)
     # The plain FP64 GPU solve, one request at a time, on the first rate's stream.
     reqs = stream(rates[0], args.requests, int(rates[0]))
@@ -807,7 +809,8 @@ def run_serving(args):
                                "(x16), Poisson or VC Helmholtz, tolerance 1e-8 or 1e-10, 120 GB budget",
                    "requests_per_rate": args.requests, "workers": args.inflight,
                    "latency": "arrival to phi on the host, including grid generation and set-up",
-                   "tagging": "host" if args.host_tags else "device"},
+                   "tagging": "host" if args.host_tags else "device",
+                   "batch_window_s": args.batch_window},
         "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "per_rate": per_rate,
         "plain_fp64_one_at_a_time": base,
     }
@@ -829,6 +832,8 @@ def main():
     ap.add_argument("--host-fill", action="store_true", help="config3: generate the inputs on the host")
     ap.add_argument("--wave", type=int, default=128, help="config3: hierarchies resident at once")
     ap.add_argument("--forest", type=int, default=1, help="config3: 1 = batch the problems in forests")
+    ap.add_argument("--batch-window", type=float, default=0.0,
+                    help="config4: seconds a request waits for others of its class to be solved with it")
     ap.add_argument("--extras", type=int, default=1,
                     help="config1, one GPU: also measure config 2 (mixed) and config 3 (forests) in the same run")
     ap.add_argument("--forest-size", type=int, default=64, help="config3: most hierarchies in one forest")

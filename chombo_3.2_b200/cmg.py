@@ -71,11 +71,12 @@ class RequestResult(ctypes.Structure):
                 ("grid_seconds", ctypes.c_double), ("build_seconds", ctypes.c_double),
                 ("fill_seconds", ctypes.c_double),
                 ("cells", ctypes.c_int64), ("device_bytes", ctypes.c_uint64), ("phi_hash", ctypes.c_uint64),
-                ("estimate_bytes", ctypes.c_uint64), ("message", ctypes.c_char * 160)]
+                ("estimate_bytes", ctypes.c_uint64), ("batch_size", ctypes.c_int), ("message", ctypes.c_char * 160)]
 
 
-def serve(requests, hbm_budget=120e9, max_inflight=16, open_loop=True):
-    """Runs cmg_serve over a list of dicts with Request fields; returns (results, wall seconds)."""
+def serve(requests, hbm_budget=120e9, max_inflight=16, open_loop=True, batch_window=0.0, max_batch=16):
+    """Runs cmg_serve over a list of dicts with Request fields; returns (results, wall seconds).  batch_window > 0:
+    cmg_serve_batched, requests of one class in flight together solved as one forest."""
     n = len(requests)
     arr = (Request * max(n, 1))()
     for i, r in enumerate(requests):
@@ -96,8 +97,12 @@ def serve(requests, hbm_budget=120e9, max_inflight=16, open_loop=True):
         q.inject_cancel_after = int(r.get("inject_cancel_after", -1))
     out = (RequestResult * max(n, 1))()
     wall = ctypes.c_double()
-    _check(lib().cmg_serve(arr, n, ctypes.c_double(hbm_budget), int(max_inflight), int(open_loop), out,
-                           ctypes.byref(wall)))
+    if batch_window > 0:
+        _check(lib().cmg_serve_batched(arr, n, ctypes.c_double(hbm_budget), int(max_inflight), int(open_loop),
+                                       ctypes.c_double(batch_window), int(max_batch), out, ctypes.byref(wall)))
+    else:
+        _check(lib().cmg_serve(arr, n, ctypes.c_double(hbm_budget), int(max_inflight), int(open_loop), out,
+                               ctypes.byref(wall)))
     keys = [f[0] for f in RequestResult._fields_]
     res = [{k: getattr(out[i], k) for k in keys} for i in range(n)]
     for r in res:

@@ -688,8 +688,14 @@ int cmg_synthetic_hierarchy_device(int n0, int nlevels, int max_box, int block_f
 
 int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_inflight, int open_loop,
               cmg_request_result* out, double* wall_seconds) {
+  return cmg_serve_batched(reqs, n, hbm_budget, max_inflight, open_loop, 0.0, 1, out, wall_seconds);
+}
+
+int cmg_serve_batched(const cmg_request* reqs, int n, double hbm_budget, int max_inflight, int open_loop,
+                      double batch_window, int max_batch, cmg_request_result* out, double* wall_seconds) {
   return guard([&]() {
-    if ((!reqs && n > 0) || (!out && n > 0) || n < 0 || max_inflight < 1 || !(hbm_budget > 0))
+    if ((!reqs && n > 0) || (!out && n > 0) || n < 0 || max_inflight < 1 || !(hbm_budget > 0) ||
+        !(batch_window >= 0) || max_batch < 1)
       throw std::invalid_argument("cmg: invalid serve arguments");
     std::vector<cmg::Request> rq(n);
     for (int i = 0; i < n; ++i) {
@@ -728,6 +734,8 @@ int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_infligh
     opt.hbmBudget = hbm_budget;
     opt.maxInflight = max_inflight;
     opt.openLoop = open_loop != 0;
+    opt.batchWindow = batch_window;
+    opt.maxBatch = max_batch;
     std::vector<cmg::RequestResult> res;
     double wall = cmg::serve(rq, opt, res);
     if (wall_seconds) *wall_seconds = wall;
@@ -747,6 +755,7 @@ int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_infligh
       o.rfinal = a.rfinal;
       o.grid_seconds = a.gridSeconds;
       o.build_seconds = a.buildSeconds;
+      o.batch_size = a.batchSize;
       o.fill_seconds = a.fillSeconds;
       o.cells = a.cells;
       o.estimate_bytes = a.estimate;

@@ -189,10 +189,11 @@ struct BottomWork {
 // metric AMRMultiGrid hands hierarchy k's bottom solver (the metric read
 // from device memory when the kernel runs, so a captured launch serves every
 // solve).  phi and rhs are level fields; the coefficients come from the
-// works.  maxBoxes: the largest box count of a work.
+// works.  maxBoxes: the largest box count of a work.  epsPer (device, may be
+// null): a BiCGStab tolerance per hierarchy in place of eps.
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork* works,
                  int nworks, int maxBoxes, const BottomConfig& cfg, double eps, const double* metrics,
-                 cudaStream_t s);
+                 cudaStream_t s, const double* epsPer = nullptr);
 // dst[slot] = fab[w.fab[slot]] for every slot of the bottom level.
 void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream_t s);
 

@@ -940,6 +940,7 @@ struct BottomArgs {
   const double* metric;  // device scalar: the solve's initial residual norm
   int imax, numRestarts;
   BottomConfig cfg;
+  const double* epsPer;  // per block (hierarchy) tolerance of a BiCGStab bottom, or null
 };
 
 // Exchange copies and homogeneous Dirichlet values of every ghost slot.
@@ -1236,6 +1237,7 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs A0, const BottomWork
   BottomArgs A = A0;
   A.W = works[blockIdx.x];
   A.metric = metrics + blockIdx.x;
+  if (A0.epsPer && A0.cfg.kind == 0) A.eps = A0.epsPer[blockIdx.x];
   const BottomWork& W = A.W;
   A.r = W.v[0];
   A.rt = W.v[1];
@@ -1595,7 +1597,7 @@ void addLaunches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxe
 
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork* works,
                  int nworks, int maxBoxes, const BottomConfig& cfg, double eps, const double* metrics,
-                 cudaStream_t s) {
+                 cudaStream_t s, const double* epsPer) {
   if (nworks == 0) return;
   BottomArgs A;
   A.boxes = L.boxes;
@@ -1605,6 +1607,7 @@ void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<d
   A.rhsFab = rhs;
   A.cfg = cfg;
   A.eps = cfg.kind == 1 ? cfg.eps : eps;  // RelaxSolver keeps its own tolerance
+  A.epsPer = epsPer;
   A.reps = cfg.reps;
   A.hang = cfg.hang;
   A.small = cfg.small;

@@ -39,7 +39,8 @@ struct LevelPlan {
   // directions in increasing order; faceOff[6*b + 2*d + (side > 0)].
   std::vector<FaceRule> faceRules;
   std::vector<int> faceOff;
-  // Colour-1 cells on exchange faces (DeferredCell), box by box, x fastest.
+  // Colour-1 cells on exchange faces (DeferredCell), box by box, x fastest;
+  // empty until the fused sweep asks for them (buildDeferred).
   std::vector<DeferredCell> deferred;
   // Face ghosts read by each chunk of a colour pass (chunksColor[c]): the
   // fill entries of chunk q are chunkGhost[c][chunkGhostStart[c][q] ..
@@ -85,6 +86,12 @@ void buildBottom(const LevelPlan& L, BottomPlan& B);
 
 // Face-ghost rules of a level from its ghost tasks (LevelPlan::faceRules).
 void buildFaceRules(LevelPlan& L);
+// The colour-1 cells on exchange faces (LevelPlan::deferred), for the fused
+// sweep; built on demand, after the face rules.
+void buildDeferred(LevelPlan& L);
+// Levels of at most this many cells get the per-chunk ghost lists of the
+// prefill relaxation variant (LevelPlan::chunkGhost).
+constexpr int64_t kPrefillMaxCells = int64_t(1) << 22;
 
 // Layout and ghost/chunk plans of one level (AMR level or multigrid depth).
 // dxCrse > 0 enables homogeneous coarse-fine ghost tasks on CF faces.

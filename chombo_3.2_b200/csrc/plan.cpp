@@ -176,25 +176,27 @@ void buildDeferred(LevelPlan& L) {
   parallelItems(L.grids.size(), [&](size_t b) {
     const Box& bx = L.grids[b];
     const int nx = bx.size(0), ny = bx.size(1);
-    auto copyFace = [&](int d, int s, const IV& p) {
+    // Only face cells can qualify: walk the six faces (cells on an edge come
+    // up on two or three of them, hence the sort and unique below).
+    std::vector<int> qs;
+    for (int d = 0; d < 3; ++d) {
       const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;
-      const FaceRule& r = L.faceRules[L.faceOff[6 * b + 2 * d + s] + (p[t0] - bx.lo[t0]) +
-                                      bx.size(t0) * (p[t1] - bx.lo[t1])];
-      return r.kind == FR_COPY;
-    };
-    for (int k = bx.lo[2]; k <= bx.hi[2]; ++k)
-      for (int j = bx.lo[1]; j <= bx.hi[1]; ++j)
-        for (int i = bx.lo[0]; i <= bx.hi[0]; ++i) {
-          if (((i + j + k) & 1) == 0) continue;
-          const IV p(i, j, k);
-          bool def = false;
-          for (int d = 0; d < 3 && !def; ++d) {
-            if (p[d] == bx.lo[d] && copyFace(d, 0, p)) def = true;
-            if (p[d] == bx.hi[d] && copyFace(d, 1, p)) def = true;
+      for (int s = 0; s < 2; ++s) {
+        const FaceRule* r = &L.faceRules[L.faceOff[6 * b + 2 * d + s]];
+        for (int v = bx.lo[t1], q = 0; v <= bx.hi[t1]; ++v)
+          for (int u = bx.lo[t0]; u <= bx.hi[t0]; ++u, ++q) {
+            IV p;
+            p[d] = s ? bx.hi[d] : bx.lo[d];
+            p[t0] = u;
+            p[t1] = v;
+            if (((p[0] + p[1] + p[2]) & 1) == 0 || r[q].kind != FR_COPY) continue;
+            qs.push_back((p[0] - bx.lo[0]) + nx * ((p[1] - bx.lo[1]) + ny * (p[2] - bx.lo[2])));
           }
-          if (def)
-            per[b].push_back(DeferredCell{(int)b, (i - bx.lo[0]) + nx * ((j - bx.lo[1]) + ny * (k - bx.lo[2]))});
-        }
+      }
+    }
+    std::sort(qs.begin(), qs.end());
+    qs.erase(std::unique(qs.begin(), qs.end()), qs.end());
+    for (int q : qs) per[b].push_back(DeferredCell{(int)b, q});
   });
   L.deferred.clear();
   for (auto& v : per) L.deferred.insert(L.deferred.end(), v.begin(), v.end());
@@ -371,7 +373,6 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
   }
   L.ghostBlock = blockTasks(L.ghostStart);
   buildFaceRules(L);
-  buildDeferred(L);
   if (L.nelem >= ((int64_t)1 << 31)) throw std::runtime_error("cmg: level too large for 32-bit ghost indices");
   // Flat lists: per parity the exchange and boundary tasks, then the
   // coarse-fine ones, each task's cells of that parity in k, j, i order.
@@ -447,7 +448,10 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     chunkCounts(L.chunksColor[0], (int)b, rows * half);
     chunkCounts(L.chunksColor[1], (int)b, rows * half);
   }
-  buildChunkGhosts(L);
+  // The prefill variant's per-chunk lists only where that variant can win
+  // (latency-bound levels): on larger levels the separate fill is as fast,
+  // and the lists would add as much host work and memory as the fill lists.
+  if (grids.numCells() <= kPrefillMaxCells) buildChunkGhosts(L);
 }
 
 int ownerOf(const LevelPlan& L, const IV& p) {
@@ -1125,7 +1129,9 @@ void mergeLevels(const std::vector<const LevelPlan*>& parts, const std::vector<i
         (cf ? out.gcCF[par] : out.gcExch[par]) += n;
       }
   }
-  // face rules, per-chunk ghosts
+  // face rules, per-chunk ghosts (kept only when every part has them)
+  bool chunkLists = true;
+  for (size_t k = 0; k < K; ++k) chunkLists = chunkLists && !parts[k]->chunkGhostStart[0].empty();
   for (size_t k = 0; k < K; ++k) {
     const LevelPlan& p = *parts[k];
     const int rbase = (int)out.faceRules.size();
@@ -1134,7 +1140,7 @@ void mergeLevels(const std::vector<const LevelPlan*>& parts, const std::vector<i
       out.faceRules.push_back(r);
     }
     for (size_t q = 0; q + 1 < p.faceOff.size(); ++q) out.faceOff.push_back(p.faceOff[q] + rbase);
-    for (int c = 0; c < 2; ++c) {
+    for (int c = 0; c < 2 && chunkLists; ++c) {
       const int gbase = (int)out.chunkGhost[c].size();
       for (const GhostCell& g : p.chunkGhost[c]) out.chunkGhost[c].push_back(shiftCell(g, elemOff[k]));
       for (size_t q = 0; q + 1 < p.chunkGhostStart[c].size(); ++q)
@@ -1142,7 +1148,7 @@ void mergeLevels(const std::vector<const LevelPlan*>& parts, const std::vector<i
     }
   }
   out.faceOff.push_back((int)out.faceRules.size());
-  for (int c = 0; c < 2; ++c) out.chunkGhostStart[c].push_back((int)out.chunkGhost[c].size());
+  for (int c = 0; c < 2 && chunkLists; ++c) out.chunkGhostStart[c].push_back((int)out.chunkGhost[c].size());
   // zeroing of the cells under the finer level
   for (size_t k = 0; k < K; ++k)
     for (const GhostTask& t : parts[k]->zeroCovered) out.zeroCovered.push_back(shiftTask(t, boxOff[k]));

@@ -49,6 +49,7 @@ struct RequestResult {
   size_t deviceBytes = 0;
   uint64_t phiHash = 0;  // FNV-1a over the 64-bit words of phi on every level (valid cells)
   size_t estimate = 0;   // admission estimate of the device bytes
+  int batchSize = 1;     // requests solved together with this one (one forest), itself included
   int error = 0;         // 0 or a CMG_* status (cmg.h)
   std::string message;   // what went wrong when error != 0
 };
@@ -57,6 +58,15 @@ struct ServeOptions {
   double hbmBudget = 120e9;  // bytes of device memory the admitted hierarchies may hold
   int maxInflight = 16;      // worker threads, each owning one hierarchy at a time
   bool openLoop = true;      // release requests at their arrival times
+  // Batching V-cycles across requests: a request of the same class as one
+  // admitted less than batchWindow seconds earlier (same problem recipe,
+  // operator, precision and solver parameters but the tolerance) joins it,
+  // and up to maxBatch of them are solved as one forest (Solver's forest
+  // constructor: one launch per V-cycle operation for all of them, each with
+  // its own tolerance, stopping rule, time limit and cancellation).  0: every
+  // request alone.
+  double batchWindow = 0;
+  int maxBatch = 16;
 };
 
 // Status codes of a request (the C ABI's CMG_* values).

@@ -11,6 +11,9 @@
 #include <mutex>
 #include <stdexcept>
 #include <thread>
+#include <functional>
+#include <map>
+#include <cstdio>
 
 #include "meshrefine.H"
 #include "synthfill.H"
@@ -78,6 +81,27 @@ void validate(const Request& q) {
   if (!(p.eps > 0) || !(q.timeout >= 0)) bad("tolerance or time limit");
 }
 
+// What requests must share to be solved as one forest: the problem recipe
+// (so the same level-0 layout and multigrid depths), operator, precision and
+// every solver parameter but the tolerance (each member keeps its own).
+std::string classKey(const Request& q) {
+  const SolveParams& p = q.params;
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), "%d %d %d %d %.17g %.17g %d %.17g %.17g %d %d %d %d %d %d %d %d %.17g %.17g %d",
+                q.n0, q.levels, q.maxBox, q.blockFactor, q.fillRatio, q.thresh, q.op, q.alpha, q.beta, (int)q.mixed,
+                (int)q.graphs, p.pre, p.post, p.bottom, p.numMG, p.iterMax, p.imin, p.hang, p.normThresh, p.iterMin);
+  return buf;
+}
+
+// Requests waiting to be solved together (ServeOptions::batchWindow).
+struct Batch {
+  std::vector<size_t> members;                  // request indices, the first is the leader
+  std::vector<std::vector<std::vector<Box>>> boxes;
+  std::vector<Clock::time_point> starts;        // when each member's own processing began
+  Clock::time_point deadline;
+  bool closed = false, done = false;
+};
+
 }  // namespace
 
 double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vector<RequestResult>& out) {
@@ -96,6 +120,126 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
   const Clock::time_point t0 = Clock::now();
   auto since = [&](Clock::time_point t) { return std::chrono::duration<double>(t - t0).count(); };
   auto at = [&](double sec) { return t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(sec)); };
+  // Why request q must stop now (0: it may go on).
+  auto stopFor = [&](const Request& q) -> int {
+    if (q.cancel && *q.cancel) return REQ_ECANCELLED;
+    if (q.timeout > 0 && Clock::now() >= at((opt.openLoop ? q.arrival : 0.0) + q.timeout)) return REQ_ETIMEOUT;
+    return REQ_OK;
+  };
+  auto stopMessage = [](int code) {
+    return std::string(code == REQ_ECANCELLED ? "cmg: request cancelled" : "cmg: request time limit passed");
+  };
+  std::mutex bm;
+  std::condition_variable bcv;
+  std::map<std::string, std::shared_ptr<Batch>> openBatches;
+
+  // One forest for the members of a batch, on the leader's stream: every
+  // member's result (or error) is written here.
+  auto runBatch = [&](Batch& b, cudaStream_t s) {
+    const size_t K = b.members.size();
+    const Request& q0 = reqs[b.members[0]];
+    try {
+      std::vector<HierarchyDesc> descs(K);
+      for (size_t k = 0; k < K; ++k) {
+        const Request& q = reqs[b.members[k]];
+        HierarchyDesc& d = descs[k];
+        d.domain = Box(IV(0, 0, 0), IV(q.n0 - 1, q.n0 - 1, q.n0 - 1));
+        d.dx0 = 1.0 / q.n0;
+        d.boxes = b.boxes[k];
+        d.vc = q.op;
+        d.alpha = q.alpha;
+        d.beta = q.beta;
+      }
+      const Clock::time_point tb = Clock::now();
+      std::unique_ptr<Solver> S(new Solver(descs, s));
+      const Clock::time_point tf = Clock::now();
+      std::vector<uint64_t> seeds;
+      for (size_t k = 0; k < K; ++k) seeds.push_back(reqs[b.members[k]].seed);
+      S->fillSyntheticForest(seeds);
+      const int fl = S->numLevels() - 1;
+      int box0 = 0;
+      for (size_t k = 0; k < K; ++k) {
+        if (reqs[b.members[k]].injectNanRHS) {
+          // one valid cell of member k's finest right-hand side made NaN
+          const BoxDesc& bd = S->level(fl).boxes[box0];
+          const double nan = std::nan("");
+          if (cudaMemcpy(S->devRHS(fl) + cellIndex(bd, bd.lo[0], bd.lo[1], bd.lo[2]), &nan, sizeof(double),
+                         cudaMemcpyHostToDevice) != cudaSuccess)
+            throw std::runtime_error("cmg: fault injection copy");
+        }
+        box0 += (int)b.boxes[k][fl].size();
+      }
+      S->setUseGraphs(q0.graphs);
+      const Clock::time_point tsolve = Clock::now();
+      std::vector<double> eps;
+      std::vector<std::function<int(int)>> ints;
+      for (size_t k = 0; k < K; ++k) {
+        const Request* q = &reqs[b.members[k]];
+        eps.push_back(q->params.eps);
+        ints.push_back([q, &stopFor](int iter) -> int {
+          if (q->injectCancelAfter >= 0 && iter >= q->injectCancelAfter) return REQ_ECANCELLED;
+          return stopFor(*q);
+        });
+      }
+      const std::vector<SolveResult> res = S->solveForest(q0.params, true, q0.mixed, &eps, &ints);
+      const Clock::time_point tsolved = Clock::now();
+      std::vector<uint64_t> hash(K, 1469598103934665603ULL);
+      std::vector<int64_t> cells(K, 0);
+      std::vector<double> phi;
+      for (int l = 0; l < S->numLevels(); ++l) {
+        phi.resize(S->numValidCells(l));
+        S->getPhi(l, phi.data(), false);
+        size_t at0 = 0;
+        for (size_t k = 0; k < K; ++k) {
+          const int64_t nk = S->hierarchyCells((int)k, l);
+          hash[k] = fnv1a(phi.data() + at0, (size_t)nk, hash[k]);
+          cells[k] += nk;
+          at0 += (size_t)nk;
+        }
+      }
+      const size_t bytes = S->deviceBytes();
+      for (size_t k = 0; k < K; ++k) {
+        RequestResult& r = out[b.members[k]];
+        r.batchSize = (int)K;
+        r.buildSeconds = std::chrono::duration<double>(tf - tb).count();
+        r.fillSeconds = std::chrono::duration<double>(tsolve - tf).count();
+        r.setupSeconds = std::chrono::duration<double>(tsolve - b.starts[k]).count();
+        r.started = since(tsolve);
+        r.solved = since(tsolved);
+        r.solveSeconds = std::chrono::duration<double>(tsolved - tsolve).count();
+        r.exitStatus = res[k].exitStatus;
+        r.iterations = res[k].iterations;
+        r.r0 = res[k].history.front();
+        r.rfinal = res[k].history.back();
+        r.cells = cells[k];
+        r.deviceBytes = bytes / K;
+        if (res[k].interrupted) {
+          r.error = res[k].interrupted;
+          r.message = stopMessage(res[k].interrupted);
+        } else if (res[k].diverged) {
+          r.error = REQ_EDIVERGED;
+          r.message = "cmg: residual norm is not finite after " + std::to_string(res[k].iterations) + " iterations";
+        } else {
+          r.phiHash = hash[k];
+        }
+      }
+      cudaStreamSynchronize(s);
+    } catch (...) {
+      std::string w = "cmg: unknown error";
+      try {
+        throw;
+      } catch (const std::exception& e) {
+        w = e.what();
+      } catch (...) {
+      }
+      for (size_t k = 0; k < K; ++k) {
+        RequestResult& r = out[b.members[k]];
+        r.batchSize = (int)K;
+        r.error = w.find("cudaMalloc") != std::string::npos ? REQ_ENOMEM : REQ_EINTERNAL;
+        r.message = w;
+      }
+    }
+  };
 
   auto work = [&]() {
     cudaSetDevice(dev);
@@ -158,6 +302,58 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
           reserved = true;
         }
         r.admitted = since(Clock::now());
+        bool batched = false;
+        if (opt.batchWindow > 0 && opt.maxBatch > 1) {
+          // Join the open batch of this request's class, or open one and lead it.
+          const std::string key = classKey(q);
+          std::shared_ptr<Batch> b;
+          bool leader = false;
+          {
+            std::unique_lock<std::mutex> lk(bm);
+            auto it = openBatches.find(key);
+            if (it != openBatches.end() && !it->second->closed) {
+              b = it->second;
+              b->members.push_back(idx);
+              b->boxes.push_back(boxes);
+              b->starts.push_back(ts);
+              if ((int)b->members.size() >= opt.maxBatch) {
+                b->closed = true;
+                openBatches.erase(it);
+              }
+              bcv.notify_all();
+            } else {
+              b = std::make_shared<Batch>();
+              b->members.push_back(idx);
+              b->boxes.push_back(boxes);
+              b->starts.push_back(ts);
+              b->deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(
+                                               std::chrono::duration<double>(opt.batchWindow));
+              openBatches[key] = b;
+              leader = true;
+              while (!b->closed && Clock::now() < b->deadline) bcv.wait_until(lk, b->deadline);
+              if (!b->closed) {
+                b->closed = true;
+                auto it2 = openBatches.find(key);
+                if (it2 != openBatches.end() && it2->second == b) openBatches.erase(it2);
+              }
+            }
+            if (!leader) {
+              while (!b->done) bcv.wait(lk);
+              batched = true;
+            }
+          }
+          if (leader && b->members.size() > 1) {
+            runBatch(*b, s);
+            {
+              std::lock_guard<std::mutex> lk(bm);
+              b->done = true;
+            }
+            bcv.notify_all();
+            batched = true;
+          }
+          if (batched && r.error) throw RequestError(r.error, r.message);
+        }
+        if (!batched) {
         HierarchyDesc d;
         d.domain = Box(IV(0, 0, 0), IV(q.n0 - 1, q.n0 - 1, q.n0 - 1));
         d.dx0 = 1.0 / q.n0;
@@ -213,6 +409,7 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
           r.phiHash = h;
           r.deviceBytes = S->deviceBytes();
         }
+        }  // the request alone
         cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
         s = nullptr;

@@ -100,7 +100,11 @@ class Solver {
   // runs for every hierarchy, and phi of a hierarchy whose stopping rule has
   // ended its solve is no longer changed, so each result is the one its own
   // solve gives.  Mixed: FP32 V-cycles inside FP64 refinement.
-  std::vector<SolveResult> solveForest(const SolveParams& p, bool zeroPhi, bool mixed);
+  // epsPer: a tolerance per hierarchy in place of p.eps; interrupts: a hook
+  // per hierarchy (as SolveParams::interrupt, ending that hierarchy's solve).
+  std::vector<SolveResult> solveForest(const SolveParams& p, bool zeroPhi, bool mixed,
+                                       const std::vector<double>* epsPer = nullptr,
+                                       const std::vector<std::function<int(int)>>* interrupts = nullptr);
   // fillSyntheticDevice for every hierarchy with its own seed.
   void fillSyntheticForest(const std::vector<uint64_t>& seeds);
   int numLevels() const { return (int)amr_.size(); }
@@ -191,6 +195,8 @@ class Solver {
   // 1 ghost fill before every colour pass, 2 face ghosts evaluated inside the
   // pass.  All three give identical results.
   void setRelaxMode(int mode);
+  // Builds and uploads the fused sweep's deferred-cell lists (once).
+  void ensureDeferred();
   // The bottom solver of the multigrid levels below level 0 (BottomConfig).
   void setBottomConfig(const BottomConfig& c);
   const BottomConfig& bottomConfig() const { return bottomCfg_; }
@@ -374,6 +380,7 @@ class Solver {
   BottomConfig bottomCfg_;
   int nh_ = 1;                              // hierarchies (a forest: more than one)
   int* dActive_ = nullptr;                  // per hierarchy: still iterating (forest solves)
+  double* dEps_ = nullptr;                  // per hierarchy: bottom-solver tolerance (forest solves)
   int* hostActive_ = nullptr;               // pinned staging of dActive_
   void setup(const std::vector<BottomPlan>& bps);
   double* dNorm_ = nullptr;

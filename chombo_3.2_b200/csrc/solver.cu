@@ -429,9 +429,10 @@ void Solver::setup(const std::vector<BottomPlan>& bps) {
   dBottoms_ = upload(bufs_, bottoms_, s_);
   dNorm_ = alloc(nh_);
   dMetric_ = alloc(nh_);
+  if (nh_ > 1) dEps_ = alloc(nh_);
   bufs_.emplace_back(new DevBuf(nh_ * sizeof(int), s_));
   dActive_ = (int*)bufs_.back()->p;
-  ck(cudaMallocHost((void**)&hostScalars_, (2 + 2 * nh_) * sizeof(double)), "pinned scalars");
+  ck(cudaMallocHost((void**)&hostScalars_, (2 + 3 * nh_) * sizeof(double)), "pinned scalars");
   ck(cudaMallocHost((void**)&hostActive_, nh_ * sizeof(int)), "pinned flags");
   if (desc.vc) {
     hostA_.resize(nlev);
@@ -846,7 +847,8 @@ void Solver::relaxLevel(const LevelDev& L, double cells, const Coef<T>& c, T* ph
     for (int it = 0; it < n; ++it) timed(cls, sweepBytes, [&]() { gsrbSweepFused(L, phi, rhs, c, s_); });
     return;
   }
-  const bool inl = variant == 1;
+  // without per-chunk lists (large levels) the prefill variant is the fill one
+  const bool inl = variant == 1 && (L.chGhost[0] != nullptr || L.nColor[0] == 0);
   for (int it = 0; it < n; ++it)
     for (int color = 0; color <= 1; ++color) {
       if (!inl) fill(L, phi, true, 1 - color);
@@ -887,6 +889,15 @@ void Solver::tuneRelaxation() {
   tuned_ = true;
   tuneMs_.clear();
   const char forced = relaxMode_ == 2 ? 1 : relaxMode_ == 3 ? 3 : 0;
+  if (forced == 3) ensureDeferred();
+  // The variants the tuner compares on a level: the prefill one where the
+  // level has its per-chunk lists, the one-block one on small levels; the
+  // fused sweep (slower on every level measured) only when forced.
+  auto offered = [&](const LevelDev& L, double cells, int v) {
+    if (v == 1) return L.chGhost[0] != nullptr;
+    if (v == 2) return cells <= kBlockRelaxMaxCells;
+    return v != 3;
+  };
   inlineA_.assign(amr_.size(), forced);
   inlineM_.assign(mg_.size(), forced);
   if (relaxMode_ != 0) return;
@@ -913,8 +924,7 @@ void Solver::tuneRelaxation() {
     Coef<double> c = coefAMR((int)l);
     float t[kRelaxVariants];
     for (int v = 0; v < kRelaxVariants; ++v)
-      t[v] = (v == 2 && cells > kBlockRelaxMaxCells) ? 1e30f
-                                                     : timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, v);
+      t[v] = offered(amrDev_[l], cells, v) ? timeOne(amrDev_[l], cells, c, lev_[l].corr, lev_[l].res, v) : 1e30f;
     inlineA_[l] = (char)pickVariant(t, kRelaxVariants);
     tuneMs_.push_back({t[0], *std::min_element(t + 1, t + kRelaxVariants)});
     zeroField(amrDev_[l], lev_[l].corr);
@@ -924,8 +934,7 @@ void Solver::tuneRelaxation() {
     Coef<double> c = coefMG((int)d + 1);
     float t[kRelaxVariants];
     for (int v = 0; v < kRelaxVariants; ++v)
-      t[v] = (v == 2 && cells > kBlockRelaxMaxCells) ? 1e30f
-                                                     : timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, v);
+      t[v] = offered(mgDev_[d], cells, v) ? timeOne(mgDev_[d], cells, c, mgf_[d].corr, mgf_[d].res, v) : 1e30f;
     inlineM_[d] = (char)pickVariant(t, kRelaxVariants);
     tuneMs_.push_back({t[0], *std::min_element(t + 1, t + kRelaxVariants)});
     zeroField(mgDev_[d], mgf_[d].corr);
@@ -1052,6 +1061,18 @@ void Solver::setBottomConfig(const BottomConfig& c) {
   precondGraphs_.clear();
 }
 
+void Solver::ensureDeferred() {
+  auto one = [&](LevelPlan& p, LevelDev& d) {
+    if (d.deferred || p.grids.size() == 0) return;
+    buildDeferred(p);
+    d.deferred = upload(bufs_, p.deferred, s_);
+    d.nDeferred = (int)p.deferred.size();
+  };
+  for (size_t l = 0; l < amr_.size(); ++l) one(amr_[l], amrDev_[l]);
+  for (size_t d = 0; d < mg_.size(); ++d) one(mg_[d], mgDev_[d]);
+  ck(cudaStreamSynchronize(s_), "deferred lists");
+}
+
 void Solver::setRelaxMode(int mode) {
   if (mode < 0 || mode > 3)
     throw std::invalid_argument("cmg: relaxation mode is 0 (tuned), 1 (fills), 2 (inline) or 3 (fused sweeps)");
@@ -1141,7 +1162,8 @@ template <>
 void Solver::bottom<double>(int depth, double* corr, double* res) {
   const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
   timed(P_BOTTOM, 0.0, [&]() {
-    bottomSolve(L, corr, res, coefMG(depth), dBottoms_, nh_, maxBottomBoxes_, bottomCfg_, sp_.eps, dMetric_, s_);
+    bottomSolve(L, corr, res, coefMG(depth), dBottoms_, nh_, maxBottomBoxes_, bottomCfg_, sp_.eps, dMetric_, s_,
+                dEps_);
   });
 }
 template <>
@@ -1152,7 +1174,8 @@ void Solver::bottom<float>(int depth, float* corr, float* res) {
   convert(corr64, corr, L.nelem, s_);
   convert(res64, res, L.nelem, s_);
   timed(P_BOTTOM, 0.0, [&]() {
-    bottomSolve(L, corr64, res64, coefMG(depth), dBottoms_, nh_, maxBottomBoxes_, bottomCfg_, sp_.eps, dMetric_, s_);
+    bottomSolve(L, corr64, res64, coefMG(depth), dBottoms_, nh_, maxBottomBoxes_, bottomCfg_, sp_.eps, dMetric_,
+                s_, dEps_);
   });
   convert(corr, corr64, L.nelem, s_);
 }
@@ -1696,7 +1719,9 @@ SolveResult Solver::solveImpl(const SolveParams& p, bool zeroPhi, bool mixed) {
 // solveImpl with one norm, stopping rule and iteration count per hierarchy;
 // an iteration runs while any hierarchy goes on, and only the going ones
 // take its correction.
-std::vector<SolveResult> Solver::solveForest(const SolveParams& p, bool zeroPhi, bool mixed) {
+std::vector<SolveResult> Solver::solveForest(const SolveParams& p, bool zeroPhi, bool mixed,
+                                             const std::vector<double>* epsPer,
+                                             const std::vector<std::function<int(int)>>* interrupts) {
   if (!tuned_) tuneRelaxation();
   if (mixed) ensure32();
   sp_ = p;
@@ -1714,21 +1739,37 @@ std::vector<SolveResult> Solver::solveForest(const SolveParams& p, bool zeroPhi,
   launchAMRResidual(ures, phi, rhs, lmax);
   const std::vector<double> r0 = readNorms();
   std::vector<double> rnorm = r0, normLast(K);
-  // each hierarchy's bottom solver gets its own initial norm as its metric
-  for (int k = 0; k < K; ++k) hostScalars_[2 + k] = r0[k];
+  if (epsPer && (int)epsPer->size() != K) throw std::invalid_argument("cmg: one tolerance per hierarchy");
+  if (interrupts && (int)interrupts->size() != K) throw std::invalid_argument("cmg: one interrupt per hierarchy");
+  auto epsOf = [&](int k) { return epsPer ? (*epsPer)[k] : p.eps; };
+  // each hierarchy's bottom solver gets its own initial norm as its metric,
+  // and its own tolerance
+  for (int k = 0; k < K; ++k) {
+    hostScalars_[2 + k] = r0[k];
+    hostScalars_[2 + K + k] = epsOf(k);
+  }
   ck(cudaMemcpyAsync(dMetric_, hostScalars_ + 2, K * sizeof(double), cudaMemcpyHostToDevice, s_), "metric");
+  if (K > 1)
+    ck(cudaMemcpyAsync(dEps_, hostScalars_ + 2 + K, K * sizeof(double), cudaMemcpyHostToDevice, s_), "tolerances");
   std::vector<char> goNorm(K), goRedu(K), goIter(K), goHang(K), goMin(K), finite(K), going(K);
+  std::vector<int> own(K, 0);  // a hierarchy's own interrupt code
   int interrupted = 0;
   auto update = [&](int k, int iter) {
     goNorm[k] = rnorm[k] > p.normThresh;
-    goRedu[k] = rnorm[k] > p.eps * r0[k];
+    goRedu[k] = rnorm[k] > epsOf(k) * r0[k];
     goIter[k] = iter < p.iterMax;
     goHang[k] = iter < p.imin || rnorm[k] < (1 - p.hang) * normLast[k];
     goMin[k] = iter < p.iterMin;
     finite[k] = std::isfinite(rnorm[k]);
-    going[k] = finite[k] && !interrupted && (goMin[k] || (goIter[k] && goRedu[k] && goHang[k] && goNorm[k]));
+    going[k] = finite[k] && !interrupted && !own[k] && (goMin[k] || (goIter[k] && goRedu[k] && goHang[k] && goNorm[k]));
   };
-  if (p.interrupt) interrupted = p.interrupt(0);
+  auto poll = [&](int iter) {
+    if (p.interrupt && !interrupted) interrupted = p.interrupt(iter);
+    if (interrupts)
+      for (int k = 0; k < K; ++k)
+        if (!own[k] && (iter == 0 || going[k]) && (*interrupts)[k]) own[k] = (*interrupts)[k](iter);
+  };
+  poll(0);
   for (int k = 0; k < K; ++k) {
     normLast[k] = 2 * r0[k];
     out[k].history.push_back(rnorm[k]);
@@ -1751,7 +1792,7 @@ std::vector<SolveResult> Solver::solveForest(const SolveParams& p, bool zeroPhi,
     }
     const std::vector<double> r = readNorms();
     iter++;
-    if (p.interrupt) interrupted = p.interrupt(iter);
+    poll(iter);
     for (int k = 0; k < K; ++k) {
       if (!hostActive_[k]) continue;
       rnorm[k] = r[k];
@@ -1763,7 +1804,7 @@ std::vector<SolveResult> Solver::solveForest(const SolveParams& p, bool zeroPhi,
   for (int k = 0; k < K; ++k) {
     out[k].exitStatus = int(!goRedu[k]) + int(!goIter[k]) * 2 + int(!goHang[k]) * 4 + int(!goNorm[k]) * 8;
     out[k].diverged = !finite[k];
-    out[k].interrupted = interrupted;
+    out[k].interrupted = own[k] ? own[k] : interrupted;
   }
   return out;
 }

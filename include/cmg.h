@@ -390,6 +390,7 @@ typedef struct cmg_request_result {
   int64_t cells;
   uint64_t device_bytes, phi_hash;
   uint64_t estimate_bytes; /* the admission estimate of the request's device memory */
+  int batch_size;          /* requests solved together with this one (cmg_serve_batched), itself included */
   char message[160];       /* empty, or what went wrong */
 } cmg_request_result;
 
@@ -400,6 +401,16 @@ typedef struct cmg_request_result {
  * (null arrays, max_inflight < 1, a non-positive budget). */
 int cmg_serve(const cmg_request* reqs, int n, double hbm_budget, int max_inflight, int open_loop,
               cmg_request_result* out, double* wall_seconds);
+/* cmg_serve with V-cycles batched across requests: a request admitted less
+ * than batch_window seconds after another of its class (the same problem
+ * recipe, operator, precision and solver parameters; tolerances may differ)
+ * joins it, and up to max_batch such requests are solved as one forest
+ * (cmg_forest_create), each keeping its own tolerance, stopping rule, time
+ * limit, cancellation and status; the first waits at most batch_window for
+ * the others.  A request without a partner is solved alone, as cmg_serve
+ * does.  Each result is the request's own solve, bit for bit. */
+int cmg_serve_batched(const cmg_request* reqs, int n, double hbm_budget, int max_inflight, int open_loop,
+                      double batch_window, int max_batch, cmg_request_result* out, double* wall_seconds);
 
 /* Algorithmic bytes moved per V-cycle (roofline numerator). */
 int cmg_vcycle_bytes(const cmg_hierarchy* h, const cmg_solve_params* p, double* out);

@@ -126,3 +126,48 @@ def test_served_request_reproduces_reference_solve(cmg):
     assert r["exit_status"] == meta["exit_status"]
     assert r["iterations"] == len(hist) - 1
     assert abs(r["rfinal"] - hist[-1]) <= 1e-12 * hist[0]
+
+
+BATCH = [
+    # one class (same recipe, operator, precision, parameters), different seeds and tolerances
+    dict(n0=32, levels=2, max_box=16, op=0, alpha=0.0, beta=1.0, seed=201, mixed=True, eps=1e-10),
+    dict(n0=32, levels=2, max_box=16, op=0, alpha=0.0, beta=1.0, seed=202, mixed=True, eps=1e-8),
+    dict(n0=32, levels=2, max_box=16, op=0, alpha=0.0, beta=1.0, seed=203, mixed=True, eps=1e-10),
+    # another class
+    dict(n0=48, levels=2, max_box=24, op=1, alpha=1.0, beta=-1.0, seed=204, mixed=False, eps=1e-10),
+    dict(n0=48, levels=2, max_box=24, op=1, alpha=1.0, beta=-1.0, seed=205, mixed=False, eps=1e-8),
+    # a class of one
+    dict(n0=64, levels=1, max_box=32, op=0, alpha=1.0, beta=-1.0, seed=206, mixed=True, eps=1e-10),
+]
+
+
+@pytest.mark.gpu
+def test_batched_requests_give_their_own_results(cmg):
+    """cmg_serve_batched: requests of one class in flight together are solved as one forest, each with its own
+    tolerance; every result (phi hash, iterations, final norm, exit status) is the one the request gets alone,
+    and the batch sizes show that the classes were batched."""
+    alone = [cmg.serve([r], max_inflight=1, open_loop=False)[0][0] for r in BATCH]
+    for a in alone:
+        assert a["error"] == 0 and a["exit_status"] & 1, a
+    res, _ = cmg.serve(BATCH, max_inflight=len(BATCH), open_loop=False, batch_window=0.5, max_batch=8)
+    for a, b in zip(alone, res):
+        assert b["error"] == 0, b
+        assert b["phi_hash"] == a["phi_hash"], (a, b)
+        assert (b["iterations"], b["exit_status"], b["rfinal"]) == (a["iterations"], a["exit_status"], a["rfinal"])
+    assert [b["batch_size"] for b in res] == [3, 3, 3, 2, 2, 1], [b["batch_size"] for b in res]
+
+
+@pytest.mark.gpu
+def test_failures_inside_a_batch_stay_with_their_request(cmg):
+    """A NaN right-hand side and a cancellation after two iterations inside one batch: those two members fail
+    with their own status, the others in the same forest keep their own results."""
+    base = dict(n0=32, levels=2, max_box=16, op=0, alpha=0.0, beta=1.0, mixed=True, eps=1e-10)
+    reqs = [dict(base, seed=301), dict(base, seed=302, inject_nan_rhs=True), dict(base, seed=303),
+            dict(base, seed=304, inject_cancel_after=2)]
+    alone = [cmg.serve([r], max_inflight=1, open_loop=False)[0][0] for r in (reqs[0], reqs[2])]
+    res, _ = cmg.serve(reqs, max_inflight=len(reqs), open_loop=False, batch_window=0.5, max_batch=8)
+    assert all(r["batch_size"] == 4 for r in res), [r["batch_size"] for r in res]
+    assert res[1]["error"] == cmg.CMG_EDIVERGED, res[1]
+    assert res[3]["error"] == cmg.CMG_ECANCELLED and res[3]["iterations"] == 2, res[3]
+    for a, b in zip(alone, (res[0], res[2])):
+        assert b["error"] == 0 and b["phi_hash"] == a["phi_hash"] and b["iterations"] == a["iterations"]

@@ -225,6 +225,21 @@ class FineInterp:
         _check(lib().cmg_fine_interp_run(self.h, _ptr(a), _ptr(out), 0, int(pwc)))
         return out
 
+    def interp_to_fine_device(self, coarse_ptr, fine_ptr, pwc=False):
+        """The same from and into device memory (cmg_fine_interp_run with on_device=1), in the order of the
+        object's stream (set_stream)."""
+        _check(lib().cmg_fine_interp_run(self.h, ctypes.c_void_p(coarse_ptr), ctypes.c_void_p(fine_ptr), 1,
+                                         int(pwc)))
+
+    def set_stream(self, stream):
+        """Runs later interpolations on `stream` (a cudaStream_t as an int; 0/None: the object's own)."""
+        _check(lib().cmg_fine_interp_set_stream(self.h, ctypes.c_void_p(stream or None)))
+
+    def is_fused(self):
+        out = ctypes.c_int()
+        _check(lib().cmg_fine_interp_is_fused(self.h, ctypes.byref(out)))
+        return bool(out.value)
+
     def close(self):
         if self.h:
             _check(lib().cmg_fine_interp_destroy(self.h))

@@ -130,6 +130,7 @@ def test_large_boxes_take_the_two_kernel_path(cmg):
     assert np.array_equal(h.phi(1), want)
     h.close()
     fi = cmg.FineInterp((0, 0, 0, 63, 63, 63), fine_boxes, coarse_boxes)
+    assert not fi.is_fused()
     assert np.array_equal(fi.interp_to_fine(c), want)
     fi.close()
 
@@ -149,3 +150,41 @@ def test_staging_above_48kb_takes_the_shared_memory_opt_in(cmg):
     h.interp_to_fine(1)
     assert np.array_equal(h.phi(1), want)
     h.close()
+    fi = cmg.FineInterp((0, 0, 0, 63, 63, 63), fine_boxes, coarse_boxes)
+    assert fi.is_fused()
+    assert np.array_equal(fi.interp_to_fine(c), want)
+    assert np.array_equal(fi.interp_to_fine(c, pwc=True), fine_interp_numpy(coarse_boxes, c, fine_boxes, 32, 1))
+    fi.close()
+
+
+@pytest.mark.gpu
+def test_device_pointers_in_stream_order(cmg):
+    """cmg_fine_interp_run with device pointers (torch tensors): the coarse data are produced on a caller's
+    stream and the object runs on that stream (cmg_fine_interp_set_stream), so no synchronisation is needed in
+    between; then on the object's own stream after the caller's stream is waited on.  Both equal the host-array
+    path bit for bit, on the fused and on the two-kernel path."""
+    import torch
+    import make_golden_fineinterp as mg
+    coarse_boxes = sorted((x, y, z, x + 15, y + 15, z + 15) for z in (0, 16) for y in (0, 16) for x in (0, 16))
+    for fine_boxes in ([(8, 8, 8, 39, 39, 39)], [(8, 8, 8, 55, 55, 55), (56, 0, 0, 63, 7, 7)]):
+        c = mg.seeded_field(coarse_boxes, 32, 79)
+        fi = cmg.FineInterp((0, 0, 0, 63, 63, 63), fine_boxes, coarse_boxes)
+        want = fi.interp_to_fine(c)
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            dc = torch.from_numpy(c).to("cuda", non_blocking=False) * 1.0   # produced on s
+            df = torch.zeros(fi.nfine, dtype=torch.float64, device="cuda")
+        fi.set_stream(s.cuda_stream)
+        fi.interp_to_fine_device(dc.data_ptr(), df.data_ptr())
+        s.synchronize()
+        assert np.array_equal(df.cpu().numpy(), want)
+        # back on the object's own stream: the caller finishes its producer first
+        fi.set_stream(None)
+        with torch.cuda.stream(s):
+            dc2 = dc * 1.0
+            df2 = torch.zeros_like(df)
+        s.synchronize()
+        fi.interp_to_fine_device(dc2.data_ptr(), df2.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(df2.cpu().numpy(), want)
+        fi.close()

@@ -26,7 +26,7 @@ class Box(ctypes.Structure):
 # Status codes (cmg.h).
 CMG_OK, CMG_EINVAL, CMG_ENOMEM, CMG_ECUDA, CMG_EINTERNAL, CMG_EDIVERGED, CMG_ETIMEOUT, CMG_ECANCELLED = range(8)
 # Homogeneous boundary types of a domain face (cmg_hierarchy_create_bc).
-BC_DIRICHLET, BC_NEUMANN = 0, 1
+BC_DIRICHLET, BC_NEUMANN, BC_PERIODIC = 0, 1, 2
 
 
 class SolveParams(ctypes.Structure):
@@ -195,6 +195,15 @@ def layout_exchange_plan(boxes):
     return _plan(lib().cmg_layout_exchange_plan, arr, len(boxes))
 
 
+def layout_exchange_plan_periodic(boxes, domain, periodic):
+    """Exchange plan on ``domain`` (lo, hi) with the directions in ``periodic``
+    (three flags) wrapping around."""
+    arr = boxes_array(boxes)
+    dom = boxes_array([tuple(domain)])
+    per = np.asarray([1 if p else 0 for p in periodic], dtype=np.int32)
+    return _plan(lib().cmg_layout_exchange_plan_periodic, arr, len(boxes), dom, _ptr(per))
+
+
 def layout_coarse_fine_plan(fine, coarse):
     fa, ca = boxes_array(fine), boxes_array(coarse)
     return _plan(lib().cmg_layout_coarse_fine_plan, fa, len(fine), ca, len(coarse))
@@ -257,7 +266,8 @@ class Hierarchy:
 
     def __init__(self, n0, level_boxes, op=0, alpha=0.0, beta=1.0, dx0=None, bc=None):
         """bc: None (homogeneous Dirichlet on every face) or six face types, x-lo, x-hi, y-lo, y-hi, z-lo, z-hi,
-        each BC_DIRICHLET / BC_NEUMANN or the letters 'D' / 'N' (a string such as "NNNNND")."""
+        each BC_DIRICHLET / BC_NEUMANN / BC_PERIODIC or the letters 'D' / 'N' / 'P' (a string such as "NNNNND";
+        periodic directions on both faces, one-level hierarchies)."""
         L = lib()
         self.nlev = len(level_boxes)
         counts = (ctypes.c_int * self.nlev)(*[len(b) for b in level_boxes])
@@ -267,7 +277,8 @@ class Hierarchy:
         dx0 = 1.0 / n0 if dx0 is None else dx0
         bcs = None
         if bc is not None:
-            codes = [{"D": BC_DIRICHLET, "N": BC_NEUMANN}.get(x, x) if isinstance(x, str) else int(x) for x in bc]
+            letters = {"D": BC_DIRICHLET, "N": BC_NEUMANN, "P": BC_PERIODIC}
+            codes = [letters.get(x, x) if isinstance(x, str) else int(x) for x in bc]
             if len(codes) != 6:
                 raise ValueError("bc needs six face types")
             bcs = (ctypes.c_int * 6)(*codes)
@@ -462,7 +473,7 @@ class Forest(Hierarchy):
         arr = boxes_array([b for hb in hierarchies for lev in hb for b in lev])
         bcs = None
         if bc is not None:
-            bcs = (ctypes.c_int * 6)(*[{"D": BC_DIRICHLET, "N": BC_NEUMANN}.get(x, x) if isinstance(x, str)
+            bcs = (ctypes.c_int * 6)(*[{"D": BC_DIRICHLET, "N": BC_NEUMANN, "P": BC_PERIODIC}.get(x, x) if isinstance(x, str)
                                        else int(x) for x in bc])
         h = ctypes.c_void_p()
         dx0 = 1.0 / n0 if dx0 is None else dx0

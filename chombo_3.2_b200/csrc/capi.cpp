@@ -137,10 +137,15 @@ static cmg::HierarchyDesc makeDesc(const int domain_lo[3], const int domain_hi[3
   cmg::HierarchyDesc d;
   if (bc)
     for (int f = 0; f < 6; ++f) {
-      if (bc[f] != CMG_BC_DIRICHLET && bc[f] != CMG_BC_NEUMANN)
-        throw std::invalid_argument("cmg: boundary type is CMG_BC_DIRICHLET or CMG_BC_NEUMANN");
-      d.bc[f] = bc[f];
+      if (bc[f] != CMG_BC_DIRICHLET && bc[f] != CMG_BC_NEUMANN && bc[f] != CMG_BC_PERIODIC)
+        throw std::invalid_argument("cmg: boundary type is CMG_BC_DIRICHLET, CMG_BC_NEUMANN or CMG_BC_PERIODIC");
+      if ((bc[f] == CMG_BC_PERIODIC) != (bc[f ^ 1] == CMG_BC_PERIODIC))
+        throw std::invalid_argument("cmg: a periodic direction is periodic on both of its faces");
+      d.bc[f] = bc[f] == CMG_BC_PERIODIC ? 0 : bc[f];
+      d.periodic[f / 2] = bc[f] == CMG_BC_PERIODIC;
     }
+  if (nlevels > 1 && (d.periodic[0] || d.periodic[1] || d.periodic[2]))
+    throw std::invalid_argument("cmg: periodic domains are supported on one-level hierarchies");
   d.domain = cmg::Box(cmg::IV(domain_lo[0], domain_lo[1], domain_lo[2]), cmg::IV(domain_hi[0], domain_hi[1], domain_hi[2]));
   if (d.domain.empty()) throw std::invalid_argument("cmg: empty domain");
   d.dx0 = dx0;
@@ -1059,6 +1064,23 @@ int cmg_layout_exchange_plan(const cmg_box* boxes, int nbox, int* items14, int c
     std::vector<cmg::Box> v;
     for (int b = 0; b < nbox; ++b) v.push_back(toBox(boxes[b]));
     auto plan = cmg::exchangePlan(cmg::Layout(v));
+    *n = (int)plan.size();
+    if (items14) {
+      if (cap < (int)plan.size()) throw std::invalid_argument("cmg: item buffer too small");
+      for (size_t i = 0; i < plan.size(); ++i)
+        putMotion(items14 + 14 * i, plan[i].from, plan[i].to, plan[i].fromRegion, plan[i].toRegion);
+    }
+  });
+}
+
+int cmg_layout_exchange_plan_periodic(const cmg_box* boxes, int nbox, const cmg_box* domain, const int* periodic,
+                                      int* items14, int cap, int* n) {
+  return guard([&]() {
+    if (!boxes || nbox < 1 || !domain || !periodic || !n) throw std::invalid_argument("cmg: invalid box list");
+    std::vector<cmg::Box> v;
+    for (int b = 0; b < nbox; ++b) v.push_back(toBox(boxes[b]));
+    const bool per[3] = {periodic[0] != 0, periodic[1] != 0, periodic[2] != 0};
+    auto plan = cmg::exchangePlan(cmg::Layout(v), toBox(*domain), per);
     *n = (int)plan.size();
     if (items14) {
       if (cap < (int)plan.size()) throw std::invalid_argument("cmg: item buffer too small");

@@ -98,6 +98,7 @@ enum { GHOST_THREADS = 256, GHOST_PER_THREAD = 1, GHOST_PER_BLOCK = GHOST_THREAD
 struct GhostTask {
   int kind, dst, src, dir, side;  // side = -1 (low) or +1 (high)
   int lo[3], hi[3];
+  int shift[3];  // exchange from a periodic image: the source cell is (i,j,k) - shift
 };
 
 // One ghost cell of a level's ghost fill, as element indices: dst = src1
@@ -143,6 +144,7 @@ struct GhostTaskDev {
   BoxDesc dst, src;
   int kind, dir, side;
   int lo[3], hi[3];
+  int shift[3];  // GhostTask::shift
   int ax;  // one-colour enumeration steps by 2 along this axis (first with extent > 1)
 };
 

@@ -240,6 +240,9 @@ struct Motion {
 // Copier::exchangeDefine + trimEdges (BoxTools/Copier.cpp:1464-1516,142-177)
 // for one ghost layer, non-periodic domain.
 std::vector<Motion> exchangePlan(const Layout& g);
+// The same with the periodic images of the domain in the directions where
+// periodic[d] (fromRegion in the source box's own coordinates).
+std::vector<Motion> exchangePlan(const Layout& g, const Box& domain, const bool* periodic);
 // Copier::define(src, dest, ghost=0) local plan (BoxTools/Copier.cpp:903-1110).
 std::vector<Motion> copyPlan(const Layout& src, const Layout& dst);
 // Spatial index of a box list: the boxes overlapping each block of B^3

@@ -4,23 +4,63 @@
 
 namespace cmg {
 
-std::vector<Motion> exchangePlan(const Layout& g) {
+std::vector<Motion> exchangePlan(const Layout& g) { return exchangePlan(g, Box(), nullptr); }
+
+std::vector<Motion> exchangePlan(const Layout& g, const Box& domain, const bool* periodic) {
   // Neighbours of box b are the other boxes meeting grow(b,1), in index order
-  // (DisjointBoxLayout::computeNeighbors, BoxTools/DisjointBoxLayout.cpp:174-254).
-  // An item is kept by trimEdges when its region touches a face ghost layer.
+  // (DisjointBoxLayout::computeNeighbors, BoxTools/DisjointBoxLayout.cpp:174-254),
+  // found through a spatial index.  In a periodic direction the domain's
+  // images shifted by +-its length are neighbours too, listed after the
+  // direct ones by source box and then by shift, the shifts ordered with x
+  // outermost (ShiftIterator::computeShifts, BoxTools/ProblemDomain.cpp:45-110):
+  // their items copy from the source box at region - shift.  An item is kept
+  // by trimEdges when its region touches a face ghost layer.
   std::vector<Motion> plan;
   const size_t n = g.size();
+  std::vector<IV> shifts;
+  if (periodic) {
+    const int r[3] = {periodic[0] ? 1 : 0, periodic[1] ? 1 : 0, periodic[2] ? 1 : 0};
+    for (int x = -r[0]; x <= r[0]; ++x)
+      for (int y = -r[1]; y <= r[1]; ++y)
+        for (int z = -r[2]; z <= r[2]; ++z)
+          if (x || y || z) shifts.push_back(IV(x * domain.size(0), y * domain.size(1), z * domain.size(2)));
+  }
+  BoxIndex index;
+  index.build(g.boxes);
+  std::vector<int> hits;
+  struct Image {
+    int nb, shift;
+    Motion m;
+  };
+  std::vector<Image> images;
+  auto kept = [&](size_t b, const Box& region) {
+    for (int d = 0; d < 3; ++d)
+      if (g[b].grow(d, 1).intersects(region)) return true;
+    return false;
+  };
   for (size_t b = 0; b < n; ++b) {
-    Box bghost = g[b].grow(1);
-    for (size_t nb = 0; nb < n; ++nb) {
-      if (nb == b) continue;
-      const Box& nbox = g[nb];
-      if (!bghost.intersects(nbox)) continue;
-      Box region = nbox & bghost;
-      bool keep = false;
-      for (int d = 0; d < 3 && !keep; ++d) keep = g[b].grow(d, 1).intersects(region);
-      if (keep) plan.push_back(Motion{(int)nb, (int)b, region, region});
+    const Box bghost = g[b].grow(1);
+    index.query(g.boxes, bghost, hits);
+    for (int nb : hits) {
+      if (nb == (int)b) continue;
+      const Box region = g[nb] & bghost;
+      if (!region.empty() && kept(b, region)) plan.push_back(Motion{nb, (int)b, region, region});
     }
+    if (shifts.empty() || domain.contains(bghost)) continue;
+    images.clear();
+    for (size_t k = 0; k < shifts.size(); ++k) {
+      const IV& sh = shifts[k];
+      const IV back(-sh[0], -sh[1], -sh[2]);
+      index.query(g.boxes, bghost.shift(back), hits);
+      for (int nb : hits) {
+        const Box region = g[nb].shift(sh) & bghost;
+        if (!region.empty() && kept(b, region))
+          images.push_back(Image{nb, (int)k, Motion{nb, (int)b, region.shift(back), region}});
+      }
+    }
+    std::sort(images.begin(), images.end(),
+              [](const Image& a, const Image& c) { return a.nb != c.nb ? a.nb < c.nb : a.shift < c.shift; });
+    for (const Image& im : images) plan.push_back(im.m);
   }
   return plan;
 }

@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(GHOST_THREADS) k_ghost(const GhostTaskDev* tas
     kind[u] = t.kind;
     dst[u] = cellIndex(t.dst, c[0], c[1], c[2]);
     if (t.kind == G_COPY) {
-      s1[u] = cellIndex(t.src, c[0], c[1], c[2]);
+      s1[u] = cellIndex(t.src, c[0] - t.shift[0], c[1] - t.shift[1], c[2] - t.shift[2]);
     } else if (t.kind != G_ZERO) {
       int e[3] = {0, 0, 0};
       e[t.dir] = -t.side;  // one cell inward

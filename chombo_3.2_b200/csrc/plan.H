@@ -97,8 +97,10 @@ constexpr int64_t kPrefillMaxCells = int64_t(1) << 22;
 // dxCrse > 0 enables homogeneous coarse-fine ghost tasks on CF faces.
 // bc: homogeneous boundary type of each domain face (x-lo, x-hi, y-lo, y-hi,
 // z-lo, z-hi): 0 Dirichlet, 1 Neumann; nullptr for Dirichlet everywhere.
+// periodic: per direction, the domain repeats (exchange from its images, no
+// boundary values); nullptr for none.
 void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse,
-                const int* bc = nullptr);
+                const int* bc = nullptr, const bool* periodic = nullptr);
 // Coarse-fine interpolation tables of fine level F from coarse level C.
 void buildQuadCF(LevelPlan& F, const LevelPlan& C);
 // Coarse/fine box maps and zero-covered tasks (F fine, C coarse).

@@ -153,7 +153,7 @@ void buildFaceRules(LevelPlan& L) {
           if (q < 0) continue;
           FaceRule& r = L.faceRules[q];
           if (t.kind == G_COPY) {
-            r = FaceRule{(int)cellOf(L, t.src, g), FR_COPY};
+            r = FaceRule{(int)cellOf(L, t.src, g - IV(t.shift[0], t.shift[1], t.shift[2])), FR_COPY};
           } else if (t.kind == G_BC) {
             r = FaceRule{0, FR_BC};
           } else if (t.kind == G_NEU) {
@@ -279,7 +279,8 @@ std::vector<int> blockTasks(const std::vector<int>& start) {
   return bt;
 }
 
-void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse, const int* bc) {
+void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx, double dxCrse, const int* bc,
+                const bool* periodic) {
   L.grids = grids;
   L.index.build(L.grids.boxes);
   L.domain = domain;
@@ -316,8 +317,9 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
   // boundary faces (face ghosts outside the domain): homogeneous Dirichlet, or
   // homogeneous Neumann where bc[2 * dir + (side > 0)] is 1.
   L.ghost.clear();
-  for (const Motion& m : exchangePlan(grids)) {
-    GhostTask t{G_COPY, m.to, m.from, 0, 0, {}, {}};
+  for (const Motion& m : exchangePlan(grids, domain, periodic)) {
+    GhostTask t{G_COPY, m.to, m.from, 0, 0, {}, {}, {}};
+    for (int k = 0; k < 3; ++k) t.shift[k] = m.toRegion.lo[k] - m.fromRegion.lo[k];
     for (int k = 0; k < 3; ++k) {
       t.lo[k] = m.toRegion.lo[k];
       t.hi[k] = m.toRegion.hi[k];
@@ -328,9 +330,10 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     if (domain.contains(grids[b].grow(1))) continue;
     for (int d = 0; d < 3; ++d)
       for (int side = -1; side <= 1; side += 2) {
+        if (periodic && periodic[d]) continue;  // filled from the periodic image
         Box g = grids[b].adjCell(d, side, 1);
         if (domain.contains(g)) continue;
-        GhostTask t{bc && bc[2 * d + (side > 0)] == 1 ? G_NEU : G_BC, (int)b, (int)b, d, side, {}, {}};
+        GhostTask t{bc && bc[2 * d + (side > 0)] == 1 ? G_NEU : G_BC, (int)b, (int)b, d, side, {}, {}, {}};
         for (int k = 0; k < 3; ++k) {
           t.lo[k] = g.lo[k];
           t.hi[k] = g.hi[k];
@@ -413,7 +416,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
           GhostCell g;
           g.dst = (int)cellIndex(db, i, j, k);
           if (t.kind == G_COPY) {
-            g.s1 = (int)cellIndex(L.boxes[t.src], i, j, k);
+            g.s1 = (int)cellIndex(L.boxes[t.src], i - t.shift[0], j - t.shift[1], k - t.shift[2]);
             g.s2 = -1;
           } else {
             int e[3] = {0, 0, 0};
@@ -1028,7 +1031,7 @@ void buildBottom(const LevelPlan& L, BottomPlan& B) {
           const int g = it->second - B.nv;
           int64_t src;
           if (t.kind == G_COPY) {
-            src = cellIndex(L.boxes[t.src], i, j, k);
+            src = cellIndex(L.boxes[t.src], i - t.shift[0], j - t.shift[1], k - t.shift[2]);
             B.gkind[g] = 0;
           } else if (t.kind == G_BC || t.kind == G_NEU) {
             int e[3] = {0, 0, 0};

@@ -28,6 +28,7 @@ struct HierarchyDesc {
   int vc = 0;                            // 0: AMRPoissonOp, 1: VCAMRPoissonOp2
   double alpha = 0.0, beta = 1.0;
   int bc[6] = {0, 0, 0, 0, 0, 0};        // per domain face: 0 homogeneous Dirichlet, 1 homogeneous Neumann
+  bool periodic[3] = {false, false, false};  // per direction (one-level hierarchies)
 };
 
 struct SolveParams {

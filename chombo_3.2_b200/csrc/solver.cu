@@ -132,6 +132,7 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
       GhostTaskDev& o = out[i];
       o.dst = p.boxes[t.dst];
       o.src = p.boxes[t.src];
+      for (int k = 0; k < 3; ++k) o.shift[k] = t.shift[k];
       o.kind = t.kind;
       o.dir = t.dir;
       o.side = t.side;
@@ -207,6 +208,8 @@ void Solver::uploadLevel(const LevelPlan& p, LevelDev& d) {
 static void hierarchyPlans(const HierarchyDesc& desc, std::vector<LevelPlan>& amr, std::vector<LevelPlan>& mg) {
   const int nlev = (int)desc.boxes.size();
   if (nlev < 1) throw std::runtime_error("cmg: hierarchy needs at least one level");
+  if (nlev > 1 && (desc.periodic[0] || desc.periodic[1] || desc.periodic[2]))
+    throw std::invalid_argument("cmg: periodic domains are supported on one-level hierarchies");
   amr.resize(nlev);
   // Host plans, one thread per level and then one per level pair (each pair
   // writes distinct members of its two levels).
@@ -231,7 +234,8 @@ static void hierarchyPlans(const HierarchyDesc& desc, std::vector<LevelPlan>& am
     for (int l = 0; l < nlev; ++l)
       th.emplace_back([&, l]() {
         try {
-          buildLevel(amr[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0, desc.bc);
+          buildLevel(amr[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0, desc.bc,
+                     desc.periodic);
         } catch (...) {
           err[l] = std::current_exception();
         }
@@ -240,7 +244,7 @@ static void hierarchyPlans(const HierarchyDesc& desc, std::vector<LevelPlan>& am
       th.emplace_back([&, d]() {
         try {
           const int c = mgc[d];
-          buildLevel(mg[d], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0, desc.bc);
+          buildLevel(mg[d], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0, desc.bc, desc.periodic);
         } catch (...) {
           err[nlev + d] = std::current_exception();
         }
@@ -289,6 +293,7 @@ Solver::Solver(const std::vector<HierarchyDesc>& descs, cudaStream_t stream)
     bool same = d.domain.lo == d0.domain.lo && d.domain.hi == d0.domain.hi && d.dx0 == d0.dx0 &&
                 d.boxes.size() == d0.boxes.size() && d.vc == d0.vc && d.alpha == d0.alpha && d.beta == d0.beta;
     for (int f = 0; f < 6; ++f) same = same && d.bc[f] == d0.bc[f];
+    for (int k = 0; k < 3; ++k) same = same && d.periodic[k] == d0.periodic[k];
     if (!same)
       throw std::invalid_argument("cmg: the hierarchies of a forest need the same domain, dx, level count, operator "
                                   "and boundary types");

@@ -76,6 +76,10 @@ int cmg_hierarchy_create(const int domain_lo[3], const int domain_hi[3], double 
  * face the operator is singular; the solver runs as the reference's does. */
 #define CMG_BC_DIRICHLET 0
 #define CMG_BC_NEUMANN 1
+/* A periodic direction (both of its faces; ProblemDomain's periodicity):
+ * ghost cells beyond the domain come from the domain's periodic image.
+ * One-level hierarchies only (CMG_EINVAL otherwise). */
+#define CMG_BC_PERIODIC 2
 int cmg_hierarchy_create_bc(const int domain_lo[3], const int domain_hi[3], double dx0, int nlevels,
                             const int* nboxes, const cmg_box* boxes, int op, double alpha, double beta,
                             const int bc[6], cmg_hierarchy** out);
@@ -322,6 +326,12 @@ int cmg_coarse_fine_plan(const cmg_hierarchy* h, int level, int* items14, int ca
 /* Host-only variants (no device state): the same plans for a box list given
  * directly, in layout order after sorting. */
 int cmg_layout_exchange_plan(const cmg_box* boxes, int nbox, int* items14, int cap, int* n);
+/* The exchange plan of a box list on a domain with periodic directions
+ * (periodic[d] nonzero): items from the domain's periodic images carry a
+ * fromRegion shifted by the domain length against their toRegion
+ * (Copier::define over ProblemDomain's shift iterator, BoxTools/Copier.cpp:903-1110). */
+int cmg_layout_exchange_plan_periodic(const cmg_box* boxes, int nbox, const cmg_box* domain, const int* periodic,
+                                      int* items14, int cap, int* n);
 int cmg_layout_coarse_fine_plan(const cmg_box* fine, int nfine, const cmg_box* coarse, int ncoarse, int* items14,
                                 int cap, int* n);
 

@@ -79,7 +79,7 @@ struct GpuOpDescription {
   Vector<int> refRatios;
   Real coarsedx = 0, alpha = 0, beta = 1;
   int vc = 0;
-  int bc[6] = {0, 0, 0, 0, 0, 0};  // per domain face: CMG_BC_DIRICHLET or CMG_BC_NEUMANN (probeBoundary)
+  int bc[6] = {0, 0, 0, 0, 0, 0};  // per domain face: CMG_BC_DIRICHLET, _NEUMANN or _PERIODIC (probeBoundary)
   Vector<RefCountedPtr<LDF> > aCoef;
   Vector<RefCountedPtr<LevelData<FluxBox> > > bCoef;
   bool defined = false;
@@ -98,6 +98,12 @@ inline void probeBoundary(BCHolder a_bc, const ProblemDomain& a_domain, Real a_d
   const Box& d = a_domain.domainBox();
   for (int dir = 0; dir < SpaceDim; ++dir)
     for (SideIterator sit; sit.ok(); ++sit) {
+      if (a_domain.isPeriodic(dir)) {
+        // The operators never apply a BC across a periodic face: its ghost
+        // cells are exchanged from the domain's periodic image.
+        a_types[2 * dir + (sit() == Side::Hi ? 1 : 0)] = CMG_BC_PERIODIC;
+        continue;
+      }
       Box valid = d;
       const int w = std::min(2, d.size(dir));
       if (sit() == Side::Lo)
@@ -565,8 +571,8 @@ class GpuHierarchy {
     if (a_numLevels < 1 || a_numLevels > d.grids.size()) MayDay::Error("cmg_chombo: bad number of levels");
     for (int l = 0; l + 1 < a_numLevels; ++l)
       if (d.refRatios[l] != 2) MayDay::Error("cmg_chombo: refinement ratio 2 only");
-    for (int dir = 0; dir < SpaceDim; ++dir)
-      if (a_coarseDomain.isPeriodic(dir)) MayDay::Error("cmg_chombo: periodic domains are not supported");
+    if (a_coarseDomain.isPeriodic() && a_numLevels > 1)
+      MayDay::Error("cmg_chombo: periodic domains are supported for one-level hierarchies only");
     m_d = d;
     m_nlev = a_numLevels;
     std::vector<int> counts;

@@ -42,15 +42,19 @@ static void zeroValue(Real*, int*, Side::LoHiSide*, Real* a_values) { a_values[0
 // Homogeneous boundary type of each domain face (x-lo, x-hi, y-lo, y-hi,
 // z-lo, z-hi): 0 Dirichlet (the examples' ParseBC), 1 Neumann (walls and
 // inflow in the AMRINS projection's pressure BC function,
-// releasedExamples/AMRINS/BCutil/PhysBCUtil.cpp:427-473).  Set from the
-// bc=<six letters D/N> argument.
+// releasedExamples/AMRINS/BCutil/PhysBCUtil.cpp:427-473), 2 periodic (the
+// direction's ProblemDomain periodicity; both faces of a direction).  Set
+// from the bc=<six letters D/N/P> argument.
 static int g_faceBC[6] = {0, 0, 0, 0, 0, 0};
 static void setFaceBC(const std::string& a_s) {
-  for (int f = 0; f < 6; ++f) g_faceBC[f] = (f < (int)a_s.size() && a_s[f] == 'N') ? 1 : 0;
+  for (int f = 0; f < 6; ++f) {
+    const char c = f < (int)a_s.size() ? a_s[f] : 'D';
+    g_faceBC[f] = c == 'N' ? 1 : c == 'P' ? 2 : 0;
+  }
 }
 static std::string faceBCString() {
   std::string s;
-  for (int f = 0; f < 6; ++f) s += g_faceBC[f] ? 'N' : 'D';
+  for (int f = 0; f < 6; ++f) s += g_faceBC[f] == 1 ? 'N' : g_faceBC[f] == 2 ? 'P' : 'D';
   return s;
 }
 
@@ -126,7 +130,7 @@ inline int buildProblem(OracleProblem& P) {
   Vector<int> refRatios(std::max(numLevels, 2), 2);
   Vector<ProblemDomain> domains(numLevels);
   Vector<Real> dxs(numLevels);
-  bool periodic[CH_SPACEDIM] = {false, false, false};
+  bool periodic[CH_SPACEDIM] = {g_faceBC[0] == 2, g_faceBC[2] == 2, g_faceBC[4] == 2};
   domains[0] = ProblemDomain(IntVect::Zero, (n0 - 1) * IntVect::Unit, periodic);
   dxs[0] = 1.0 / n0;
   for (int l = 1; l < numLevels; ++l) {

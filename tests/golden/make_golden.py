@@ -37,6 +37,10 @@ CASES = {
     "vc_3lev_16_walls": ("n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=-1 bc=NDNDNN", True),
     "helmholtz_2lev_16_neumann": ("n0=16 levels=2 maxbox=8 block=4 op=0 alpha=1 beta=-1 bc=NNNNNN", True),
     "poisson_3lev_32_walls": ("n0=32 levels=3 maxbox=16 op=0 alpha=0 beta=1 bc=NNNNND", False),
+    # periodic directions (one-level hierarchies), the published Proto AMRPoisson configuration's operator
+    "helmholtz_1lev_32_periodic": ("n0=32 levels=1 maxbox=16 op=0 alpha=1 beta=-0.1 bc=PPPPPP", True),
+    "vc_1lev_32_periodic": ("n0=32 levels=1 maxbox=16 op=1 alpha=1 beta=-1 bc=PPPPPP", True),
+    "helmholtz_1lev_32_ppnndd": ("n0=32 levels=1 maxbox=16 op=0 alpha=1 beta=-0.1 bc=PPNNDD", True),
     "vc_3lev_32": ("n0=32 levels=3 maxbox=16 op=1 alpha=1 beta=-1", False),
     "vc_2lev_64": ("n0=64 levels=2 maxbox=32 op=1 alpha=1 beta=-1", False),
     "config0_poisson_64": ("n0=64 levels=1 maxbox=32 op=0 alpha=0 beta=1", True),

@@ -47,3 +47,17 @@ def test_null_hierarchy_is_an_error(cmg):
     lib = cmg.lib()
     out = ctypes.c_int64()
     assert lib.cmg_num_cells(None, 0, ctypes.byref(out)) == cmg.CMG_EINVAL
+
+
+def test_hierarchy_create_rejects_half_periodic_direction(cmg):
+    with pytest.raises(cmg.CmgError) as e:
+        cmg.Hierarchy(16, [[(0, 0, 0, 15, 15, 15)]], bc="PDNNDD")
+    assert e.value.code == cmg.CMG_EINVAL
+
+
+def test_hierarchy_create_rejects_periodic_amr(cmg):
+    # periodic directions on one-level hierarchies only; refused before any device work
+    with pytest.raises(cmg.CmgError) as e:
+        cmg.Hierarchy(16, [[(0, 0, 0, 15, 15, 15)], [(8, 8, 8, 15, 15, 15)]], bc="PPPPPP")
+    assert e.value.code == cmg.CMG_EINVAL
+    assert "one-level" in str(e.value)

@@ -31,11 +31,12 @@ def test_inhomogeneous_boundary_condition_is_refused():
     assert "homogeneous Neumann (ghost = inside) boundary conditions only" in (r.stdout + r.stderr)
 
 
-@pytest.mark.parametrize("faces", ["DDDDDD", "NNNNND", "NDNDNN", "NNNNNN"])
+@pytest.mark.parametrize("faces", ["DDDDDD", "NNNNND", "NDNDNN", "NNNNNN", "PPPPPP", "PPNNDD", "DNPPNN"])
 def test_face_types_are_read_off_the_bc_function(faces):
+    """Periodic directions come from the ProblemDomain (the BC function is not called across them)."""
     need_dropin()
     r = subprocess.run([DROPIN] + BASE + ["bcprobe=1", "bc=" + faces], capture_output=True, text=True,
                        timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     out = json.loads(r.stdout.strip().splitlines()[-1])
-    assert out["bc_types"] == [1 if c == "N" else 0 for c in faces]
+    assert out["bc_types"] == [{"D": 0, "N": 1, "P": 2}[c] for c in faces]

@@ -27,6 +27,9 @@ CASES = {
     "projection_3lev_32": "n0=32 levels=3 maxbox=16 block=4 op=0 alpha=0 beta=1 bc=NNNNND relaxbottom=1 eps=1e-10",
     "projection_2lev_16_relax": "n0=16 levels=2 maxbox=8 block=4 op=0 alpha=0 beta=1 bc=NDNNNN relaxbottom=1",
     "vc_3lev_16_walls": "n0=16 levels=3 maxbox=8 block=4 op=1 alpha=1 beta=-1 bc=NDNDNN",
+    # one-level periodic domains (ProblemDomain periodic in every direction, or in x and y)
+    "helmholtz_1lev_32_periodic": "n0=32 levels=1 maxbox=16 op=0 alpha=1 beta=-0.1 bc=PPPPPP",
+    "vc_1lev_32_ppnndd": "n0=32 levels=1 maxbox=16 op=1 alpha=1 beta=-1 bc=PPNNDD",
 }
 
 

@@ -31,7 +31,8 @@ needs_oracle = pytest.mark.skipif(not os.path.exists(ORACLE), reason="oracle not
 
 @needs_oracle
 @pytest.mark.parametrize("name", ["poisson_1lev_32", "helmholtz_1lev_32", "vc_1lev_32", "poisson_3lev_16",
-                                  "helmholtz_2lev_16", "vc_3lev_16"])
+                                  "helmholtz_2lev_16", "vc_3lev_16", "poisson_3lev_16_walls", "vc_3lev_16_walls",
+                                  "helmholtz_1lev_32_periodic", "helmholtz_1lev_32_ppnndd", "vc_1lev_32_periodic"])
 def test_oracle_reproduces_golden(tmp_path, name):
     meta, arrays = golden(name)
     out = str(tmp_path / name)

@@ -617,7 +617,48 @@ def extra_workloads(args, cmg):
         out["config3"]["timing"] = line["config"]["timing"]
     except Exception as e:
         out["config3"] = {"error": str(e)[:300]}
+    try:
+        out["helmholtz_512_periodic"] = published_vcycle(cmg)
+    except Exception as e:
+        out["helmholtz_512_periodic"] = {"error": str(e)[:300]}
     return out
+
+
+def published_vcycle(cmg):
+    """The configuration of the reference's one published AMRPoisson timing: a single level 512^3 on the unit
+    domain, periodic in every direction, domainSplit into 32^3 boxes (block factor 8), alpha = 1, beta = -0.1,
+    4 smoothings per relaxation (releasedExamples/Proto/Poisson/doc/proto_poisson.tex:18-55 and
+    exec/periodic.inputs), 1.223 s per V-cycle on a 32-core Haswell node.  Seeded synthetic right-hand side; one
+    untimed solve, then one timed solve in CUDA events on the solver's stream, divided by its V-cycle count (each
+    V-cycle is followed by the residual and its max norm, as in the example's loop)."""
+    import torch
+    n0 = 512
+    boxes = cmg.domain_split((0, 0, 0), (n0 - 1,) * 3, 32, 8)
+    h = cmg.Hierarchy(n0, [boxes], op=0, alpha=1.0, beta=-0.1, bc="PPPPPP")
+    try:
+        h.fill_synthetic(20261203)
+        p = cmg.solve_params(pre=4, post=4, bottom=4, iter_max=100, eps=1e-10, hang=1e-10)
+        h.use_graphs(True)
+        h.solve(p)
+        stream = torch.cuda.ExternalStream(h.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        o = h.solve(p)
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        nv = max(o["iterations"], 1)
+        vb = h.vcycle_bytes(p)
+        peak = measured_peaks()[0]
+        return {"workload": "single level 512^3 periodic Helmholtz (alpha 1, beta -0.1), 4096 boxes of 32^3, "
+                            "4 smoothings", "ms_per_vcycle": ms / nv, "vcycles": o["iterations"],
+                "exit_status": o["exit_status"], "ms_per_solve": ms, "cells": h.num_cells(0),
+                "vcycle_gbs": vb / (ms / nv) / 1e6, "vcycle_frac": vb / (ms / nv) / 1e6 / peak,
+                "published_s_per_vcycle": 1.223, "published_hardware": "1 Cori Haswell node, 32 MPI ranks",
+                "dtype": "f64", "timing": "CUDA events on the solver's stream around one solve after an untimed one"}
+    finally:
+        h.close()
 
 
 def fineinterp_reference(meta, repeat):

@@ -53,6 +53,12 @@ def solve_params(pre=4, post=4, bottom=4, num_mg=1, iter_max=100, imin=5, eps=1e
     return SolveParams(pre, post, bottom, num_mg, iter_max, imin, eps, hang, norm_thresh, iter_min)
 
 
+class BottomParams(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("imax", ctypes.c_int), ("num_restarts", ctypes.c_int),
+                ("norm_type", ctypes.c_int), ("eps", ctypes.c_double), ("hang", ctypes.c_double),
+                ("small", ctypes.c_double)]
+
+
 class Request(ctypes.Structure):
     _fields_ = [("arrival", ctypes.c_double), ("n0", ctypes.c_int), ("levels", ctypes.c_int),
                 ("max_box", ctypes.c_int), ("block_factor", ctypes.c_int), ("fill_ratio", ctypes.c_double),
@@ -404,6 +410,23 @@ class Hierarchy:
 
     def set_relax_mode(self, mode):
         _check(lib().cmg_set_relax_mode(self.h, int(mode)))
+
+    def set_bottom_solver(self, kind=0, imax=None, num_restarts=5, norm_type=2, eps=1e-6, hang=None, small=1e-30):
+        """kind 0 BiCGStabSolver (defaults imax 80, hang 1e-8), 1 RelaxSolver (defaults imax 40, hang 0)."""
+        if imax is None:
+            imax = 80 if kind == 0 else 40
+        if hang is None:
+            hang = 1e-8 if kind == 0 else 0.0
+        p = BottomParams(int(kind), int(imax), int(num_restarts), int(norm_type), float(eps), float(hang),
+                         float(small))
+        _check(lib().cmg_set_bottom_solver(self.h, ctypes.byref(p)))
+
+    def set_bottom_grid(self, mode):
+        """-1 automatic, 0 one block per hierarchy, 1 the whole device; returns whether the grid-wide bottom
+        solve is in use."""
+        on = ctypes.c_int()
+        _check(lib().cmg_set_bottom_grid(self.h, int(mode), ctypes.byref(on)))
+        return bool(on.value)
 
     def relax_variants(self):
         n = ctypes.c_int()

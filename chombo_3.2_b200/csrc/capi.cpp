@@ -408,6 +408,14 @@ int cmg_set_relax_mode(cmg_hierarchy* h, int mode) {
   });
 }
 
+int cmg_set_bottom_grid(cmg_hierarchy* h, int mode, int* on_grid) {
+  return guard([&]() {
+    needLevel(h, 0);
+    h->solver->setBottomGrid(mode);
+    if (on_grid) *on_grid = h->solver->bottomOnGrid() ? 1 : 0;
+  });
+}
+
 int cmg_set_bottom_solver(cmg_hierarchy* h, const cmg_bottom_params* p) {
   return guard([&]() {
     needLevel(h, 0);

@@ -177,10 +177,11 @@ struct BottomConfig {
 struct BottomWork {
   int nv = 0, ng = 0, nbox = 0, ncol[2] = {0, 0};
   const int *fab = nullptr, *nb = nullptr, *col[2] = {nullptr, nullptr}, *boxStart = nullptr;
-  const int *gsrc = nullptr, *gkind = nullptr;
+  const int* nbv = nullptr;  // 6 per valid slot: face neighbour value source (BottomPlan::nbv)
   double* v[10] = {};
   double *a = nullptr, *b[3] = {nullptr, nullptr, nullptr}, *lam = nullptr;
   int* status = nullptr;
+  double *gpart = nullptr, *gpart2 = nullptr, *gscal = nullptr;  // sums of a grid-wide solve
 };
 // Bottom solve (BiCGStab or relaxation, cfg) of L(phi) = rhs (homogeneous
 // boundary conditions) on one level, one thread block per hierarchy
@@ -190,10 +191,16 @@ struct BottomWork {
 // from device memory when the kernel runs, so a captured launch serves every
 // solve).  phi and rhs are level fields; the coefficients come from the
 // works.  maxBoxes: the largest box count of a work.  epsPer (device, may be
-// null): a BiCGStab tolerance per hierarchy in place of eps.
+// null): a BiCGStab tolerance per hierarchy in place of eps.  gridBlocks > 0
+// (one work only, its gpart/gpart2/gscal set): the whole solve as one
+// cooperative launch of that many blocks instead of one block.
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork* works,
                  int nworks, int maxBoxes, const BottomConfig& cfg, double eps, const double* metrics,
-                 cudaStream_t s, const double* epsPer = nullptr);
+                 cudaStream_t s, const double* epsPer = nullptr, int gridBlocks = 0);
+// Blocks of a grid-wide bottom solve of nv valid cells (bounded by what is
+// co-resident on the device), and threads per block.
+int bottomGridBlocks(int nv);
+int bottomGridThreads();
 // dst[slot] = fab[w.fab[slot]] for every slot of the bottom level.
 void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream_t s);
 

@@ -7,10 +7,14 @@
 #include <cstdio>
 #include <stdexcept>
 
+#include <cooperative_groups.h>
+
 #include "kernels.H"
 #include "synthdev.H"
 #include "plan.H"
 #include "synthetic.H"
+
+namespace cg = cooperative_groups;
 
 namespace cmg {
 
@@ -920,14 +924,23 @@ __global__ void k_reflux(const RefluxCell* cells, int n, const RefluxCoarseTerm*
 }
 
 // ---------------------------------------------------------------- bottom
-// BiCGStabSolver<T>::solve (AMRElliptic/BiCGStabSolver.H:199-515) on the
-// deepest multigrid level, run by one thread block so that every dot product
-// and norm is summed in the reference's order: per box in x-fastest order
-// (FArrayBox::dotProduct, FArrayBox.cpp:260-280; FArrayBox::sumPow pencil
-// order, FArrayBox.cpp:168-209), then box by box.  All vectors live in the
-// bottom level's compact slot space (valid cells, then the face ghosts the
-// stencil reads; BottomPlan), a few tens of KB that stay in L1, and every
-// pass is one flat loop over a precomputed slot list.
+// BiCGStabSolver<T>::solve (AMRElliptic/BiCGStabSolver.H:199-515) and
+// RelaxSolver<T>::solve (RelaxSolver.H:128-186) on the deepest multigrid
+// level, every dot product and norm summed in the reference's order: per box
+// in x-fastest order (FArrayBox::dotProduct, FArrayBox.cpp:260-280;
+// FArrayBox::sumPow pencil order, FArrayBox.cpp:168-209), then box by box
+// from zero.  The vectors live in the bottom level's compact slot space (its
+// valid cells, BottomPlan).  A stencil read of a face ghost goes straight to
+// the valid cell that the level's exchange or boundary condition copies
+// there (nbv: the source slot, or -(slot + 1) for a homogeneous Dirichlet
+// ghost, read as 0 - value the way the BC writes it).  A ghost is only read
+// while its source is not written (a colour pass reads the other colour; an
+// operator apply writes another vector), so the value read is the one an
+// exchange just before the pass would have left there.
+// Two ways to run: one thread block per hierarchy (BlkCtx: forests and
+// small levels), or the whole grid of one cooperative launch for one
+// hierarchy with a large bottom level (GridCtx), its phases separated by
+// grid barriers and its sums folded by block 0 from shared memory.
 struct BottomArgs {
   BottomWork W;
   const BoxDesc* boxes;
@@ -943,177 +956,227 @@ struct BottomArgs {
   const double* epsPer;  // per block (hierarchy) tolerance of a BiCGStab bottom, or null
 };
 
-// Exchange copies and homogeneous Dirichlet values of every ghost slot.
-__device__ void blkGhost(const BottomArgs& A, double* f) {
-  const BottomWork& W = A.W;
-  for (int g = threadIdx.x; g < W.ng; g += blockDim.x) {
-    const int kind = W.gkind[g];
-    if (kind == 0) {
-      f[W.nv + g] = f[W.gsrc[g]];
-    } else if (kind == 1) {
-      double zero = 0.0;
-      f[W.nv + g] = 2.0 * zero - f[W.gsrc[g]];
+constexpr int kBottomGridThreads = 256;
+constexpr int kBottomStage = 2048;  // doubles per fold chunk staged in shared memory (grid)
+
+// In-order fold of p[0..n): a sum from zero, or a NaN-keeping max from zero.
+__device__ __forceinline__ double foldRun(double acc, const double* p, int n, bool mx) {
+  if (mx) {
+    for (int b = 0; b < n; ++b) acc = nanMax(acc, p[b]);
+  } else {
+    for (int b = 0; b < n; ++b) acc += p[b];
+  }
+  return acc;
+}
+
+struct BlkCtx {
+  double* part;   // per-box partials (dynamic shared memory)
+  double* part2;  // a second set, for two sums folded together
+  double* scal;   // 8 rotating broadcast slots (shared)
+  int k;
+  __device__ int tid() const { return threadIdx.x; }
+  __device__ int nthr() const { return blockDim.x; }
+  __device__ void sync() const { __syncthreads(); }
+  // Folds part[0..n) (and part2 when two) once every thread has written its
+  // partials; every thread gets the results.  A broadcast slot is written
+  // again only four folds later, after every thread has read it.
+  __device__ void reduce(int n, bool two, bool mx, double& r1, double& r2) {
+    __syncthreads();
+    const int s = k;
+    k = (k + 2) & 7;
+    if (threadIdx.x == 0) scal[s] = foldRun(0.0, part, n, mx);
+    if (two && threadIdx.x == 32) scal[s + 1] = foldRun(0.0, part2, n, mx);
+    __syncthreads();
+    r1 = scal[s];
+    if (two) r2 = scal[s + 1];
+  }
+};
+
+struct GridCtx {
+  double* part;   // per-box partials (global)
+  double* part2;
+  double* scal;   // 8 rotating broadcast slots (global)
+  double* stage;  // 2 x kBottomStage doubles of shared memory
+  int k;
+  __device__ int tid() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+  __device__ int nthr() const { return gridDim.x * blockDim.x; }
+  __device__ void sync() const { cg::this_grid().sync(); }
+  __device__ void reduce(int n, bool two, bool mx, double& r1, double& r2) {
+    cg::this_grid().sync();
+    const int s = k;
+    k = (k + 2) & 7;
+    if (blockIdx.x == 0) {
+      double a1 = 0.0, a2 = 0.0;
+      for (int base = 0; base < n; base += kBottomStage) {
+        const int m = min(kBottomStage, n - base);
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+          stage[i] = __ldcg(part + base + i);
+          if (two) stage[kBottomStage + i] = __ldcg(part2 + base + i);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) a1 = foldRun(a1, stage, m, mx);
+        if (two && threadIdx.x == 32) a2 = foldRun(a2, stage + kBottomStage, m, mx);
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) scal[s] = a1;
+      if (two && threadIdx.x == 32) scal[s + 1] = a2;
+    }
+    cg::this_grid().sync();
+    r1 = __ldcg(scal + s);
+    if (two) r2 = __ldcg(scal + s + 1);
+  }
+};
+
+template <class C, class F>
+__device__ __forceinline__ void bCells(C& c, int n, F fn) {
+  for (int q = c.tid(); q < n; q += c.nthr()) fn(q);
+  c.sync();
+}
+
+// A face neighbour's value: the slot itself, or 0 - the source of a
+// homogeneous Dirichlet ghost.
+__device__ __forceinline__ double gval(const double* f, int v) { return v >= 0 ? f[v] : 0.0 - f[-v - 1]; }
+
+// The partial sum of box b: x.y in x-fastest order, or sumPow(2) of x.
+__device__ double boxPartial(const BottomArgs& A, int b, const double* x, const double* y, bool pencil) {
+  const BoxDesc bd = A.boxes[b];
+  const int nx = bd.hi[0] - bd.lo[0] + 1, ny = bd.hi[1] - bd.lo[1] + 1, nz = bd.hi[2] - bd.lo[2] + 1;
+  const int s0 = A.W.boxStart[b];
+  double s = 0.0;
+  if (!pencil) {
+    for (int q = s0; q < s0 + nx * ny * nz; ++q) s += x[q] * y[q];
+  } else {
+    // sumPow(p=2): per-x accumulation over pencils, then across x.
+    for (int i = 0; i < nx; ++i) {
+      double acc = 0.0;
+      bool first = true;
+      for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j) {
+          double v = x[s0 + i + nx * (j + ny * k)];
+          acc = first ? v * v : acc + v * v;
+          first = false;
+        }
+      s = (i == 0) ? acc : s + acc;
     }
   }
-  __syncthreads();
+  return s;
 }
 
-template <class F>
-__device__ void blkCells(const BottomArgs& A, F fn) {
-  for (int q = threadIdx.x; q < A.W.nv; q += blockDim.x) fn(q);
-  __syncthreads();
+template <class C>
+__device__ double bDot(C& c, const BottomArgs& A, const double* x, const double* y, bool pencil) {
+  for (int b = c.tid(); b < A.W.nbox; b += c.nthr()) c.part[b] = boxPartial(A, b, x, y, pencil);
+  double r, unused;
+  c.reduce(A.W.nbox, false, false, r, unused);
+  return r;
 }
 
-__device__ __forceinline__ Stencil slotStencil(const BottomWork& W, int q) {
-  const int* n = W.nb + 6 * q;
-  Stencil st;
-  st.c = q;
-  st.xp = n[0];
-  st.xm = n[1];
-  st.yp = n[2];
-  st.ym = n[3];
-  st.zp = n[4];
-  st.zm = n[5];
-  return st;
+// x1.y1 and x2.y2, each in the reference's order, folded side by side.
+template <class C>
+__device__ void bDot2(C& c, const BottomArgs& A, const double* x1, const double* y1, const double* x2,
+                      const double* y2, double& r1, double& r2) {
+  for (int b = c.tid(); b < A.W.nbox; b += c.nthr()) {
+    c.part[b] = boxPartial(A, b, x1, y1, false);
+    c.part2[b] = boxPartial(A, b, x2, y2, false);
+  }
+  c.reduce(A.W.nbox, true, false, r1, r2);
 }
 
-__device__ void blkGsrb(const BottomArgs& A, double* phi, const double* rhs, int color) {
+// The norm of type A.cfg.normType: 2 the reference-ordered sqrt(sumPow),
+// 0 the largest |x| (a max, so its order does not matter; NaN propagates).
+template <class C>
+__device__ double bNormType(C& c, const BottomArgs& A, const double* x) {
+  if (A.cfg.normType == 2) return sqrt(bDot(c, A, x, x, true));
+  double v = 0.0;
+  for (int q = c.tid(); q < A.W.nv; q += c.nthr()) v = nanMax(v, fabs(x[q]));
+  for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) c.part[c.tid() >> 5] = v;
+  double r, unused;
+  c.reduce(c.nthr() >> 5, false, true, r, unused);
+  return r;
+}
+
+// One colour of levelGSRB, face ghosts read from their sources.
+template <class C>
+__device__ void bGsrb(C& c, const BottomArgs& A, double* phi, const double* rhs, int color) {
   const BottomWork& W = A.W;
   const int* list = W.col[color];
-  for (int idx = threadIdx.x; idx < W.ncol[color]; idx += blockDim.x) {
-    const Stencil st = slotStencil(W, list[idx]);
-    const int64_t c = st.c;
-    const double dxinv = A.sc.dxinv;
+  const double dxinv = A.sc.dxinv;
+  for (int idx = c.tid(); idx < W.ncol[color]; idx += c.nthr()) {
+    const int q = list[idx];
+    const int* n = W.nbv + 6 * q;
+    const double pxp = gval(phi, n[0]), pxm = gval(phi, n[1]), pyp = gval(phi, n[2]), pym = gval(phi, n[3]),
+                 pzp = gval(phi, n[4]), pzm = gval(phi, n[5]);
+    const double pc = phi[q];
     if (A.vc) {
-      double pc = phi[c];
-      double lofphi = A.sc.alpha * W.a[c] * pc - A.sc.beta * vcDiv(phi, W.b[0], W.b[1], W.b[2], st) * dxinv;
-      phi[c] = pc - W.lam[c] * (lofphi - rhs[c]);
+      const int* o = W.nb + 6 * q;
+      const double div = W.b[0][o[0]] * (pxp - pc) - W.b[0][q] * (pc - pxm) + W.b[1][o[2]] * (pyp - pc) -
+                         W.b[1][q] * (pc - pym) + W.b[2][o[4]] * (pzp - pc) - W.b[2][q] * (pc - pzm);
+      const double lofphi = A.sc.alpha * W.a[q] * pc - A.sc.beta * div * dxinv;
+      phi[q] = pc - W.lam[q] * (lofphi - rhs[q]);
     } else if (A.sc.laplacian) {
-      double lphi = nbrSum(phi, st) * dxinv;
-      phi[c] = A.sc.lambda * (rhs[c] - lphi);
+      const double lphi = (pxp + pxm + pyp + pym + pzp + pzm) * dxinv;
+      phi[q] = A.sc.lambda * (rhs[q] - lphi);
     } else {
-      double pc = phi[c];
-      double lphi = (nbrSum(phi, st) - 2.0 * 3 * pc) * dxinv;
-      double helmop = A.sc.alpha * pc + A.sc.beta * lphi;
-      phi[c] = pc + A.sc.lambda * (helmop - rhs[c]);
+      const double lphi = (pxp + pxm + pyp + pym + pzp + pzm - 2.0 * 3 * pc) * dxinv;
+      const double helmop = A.sc.alpha * pc + A.sc.beta * lphi;
+      phi[q] = pc + A.sc.lambda * (helmop - rhs[q]);
     }
   }
-  __syncthreads();
+  c.sync();
 }
 
-// levelGSRB: per colour a ghost fill then the colour update.
-__device__ void blkRelax(const BottomArgs& A, double* phi, const double* rhs, int nit) {
+template <class C>
+__device__ void bRelax(C& c, const BottomArgs& A, double* phi, const double* rhs, int nit) {
   for (int it = 0; it < nit; ++it)
-    for (int color = 0; color <= 1; ++color) {
-      blkGhost(A, phi);
-      blkGsrb(A, phi, rhs, color);
-    }
+    for (int color = 0; color <= 1; ++color) bGsrb(c, A, phi, rhs, color);
 }
 
-// residual (mode 0) or applyOp (mode 1) after a ghost fill.
-__device__ void blkOp(const BottomArgs& A, double* r, double* phi, const double* rhs, int mode) {
-  blkGhost(A, phi);
+// residual (mode 0) or applyOp (mode 1) into every valid slot of r.
+template <class C>
+__device__ void bOp(C& c, const BottomArgs& A, double* r, const double* phi, const double* rhs, int mode) {
   const double dxinv = A.sc.dxinv;
   const BottomWork& W = A.W;
-  blkCells(A, [&](int q) {
-    const Stencil st = slotStencil(W, q);
-    double pc = phi[q];
+  bCells(c, W.nv, [&](int q) {
+    const int* n = W.nbv + 6 * q;
+    const double pxp = gval(phi, n[0]), pxm = gval(phi, n[1]), pyp = gval(phi, n[2]), pym = gval(phi, n[3]),
+                 pzp = gval(phi, n[4]), pzm = gval(phi, n[5]);
+    const double pc = phi[q];
     if (A.vc) {
-      double lofphi = A.sc.alpha * W.a[q] * pc - A.sc.beta * vcDiv(phi, W.b[0], W.b[1], W.b[2], st) * dxinv;
+      const int* o = W.nb + 6 * q;
+      const double div = W.b[0][o[0]] * (pxp - pc) - W.b[0][q] * (pc - pxm) + W.b[1][o[2]] * (pyp - pc) -
+                         W.b[1][q] * (pc - pym) + W.b[2][o[4]] * (pzp - pc) - W.b[2][q] * (pc - pzm);
+      const double lofphi = A.sc.alpha * W.a[q] * pc - A.sc.beta * div * dxinv;
       r[q] = mode == 0 ? rhs[q] - lofphi : lofphi;
     } else {
-      double lap = (nbrSum(phi, st) - 6.0 * pc) * dxinv;
+      const double lap = (pxp + pxm + pyp + pym + pzp + pzm - 6.0 * pc) * dxinv;
       r[q] = mode == 0 ? -(A.sc.alpha * pc) - A.sc.beta * lap + rhs[q] : A.sc.alpha * pc + A.sc.beta * lap;
     }
   });
 }
 
-__device__ void blkPrecond(const BottomArgs& A, double* out, const double* in) {
-  blkCells(A, [&](int q) { out[q] = A.vc ? in[q] * A.W.lam[q] : in[q] * A.mult; });
-  blkRelax(A, out, in, 2);
-}
-
-__device__ double blkDot(const BottomArgs& A, const double* x, const double* y, bool pencil) {
-  extern __shared__ double spart[];
-  const BottomWork& W = A.W;
-  for (int b = threadIdx.x; b < W.nbox; b += blockDim.x) {
-    const BoxDesc bd = A.boxes[b];
-    const int nx = bd.hi[0] - bd.lo[0] + 1, ny = bd.hi[1] - bd.lo[1] + 1, nz = bd.hi[2] - bd.lo[2] + 1;
-    const int s0 = W.boxStart[b];
-    double s = 0.0;
-    if (!pencil) {
-      for (int q = s0; q < s0 + nx * ny * nz; ++q) s += x[q] * y[q];
-    } else {
-      // sumPow(p=2): per-x accumulation over pencils, then across x.
-      for (int i = 0; i < nx; ++i) {
-        double acc = 0.0;
-        bool first = true;
-        for (int k = 0; k < nz; ++k)
-          for (int j = 0; j < ny; ++j) {
-            double v = x[s0 + i + nx * (j + ny * k)];
-            acc = first ? v * v : acc + v * v;
-            first = false;
-          }
-        s = (i == 0) ? acc : s + acc;
-      }
-    }
-    spart[b] = s;
-  }
-  __syncthreads();
-  __shared__ double tot;
-  if (threadIdx.x == 0) {
-    double v = 0.0;
-    for (int b = 0; b < W.nbox; ++b) v += spart[b];
-    tot = v;
-  }
-  __syncthreads();
-  double r = tot;
-  __syncthreads();
-  return r;
-}
-
-__device__ double blkNorm(const BottomArgs& A, const double* x) { return sqrt(blkDot(A, x, x, true)); }
-
-// The norm of type A.W.cfg.normType: 2 as above, 0 the largest |x| (a max,
-// so its order does not matter; NaN propagates).
-__device__ double blkNormType(const BottomArgs& A, const double* x) {
-  if (A.cfg.normType == 2) return blkNorm(A, x);
-  __shared__ double m;
-  if (threadIdx.x == 0) m = 0.0;
-  __syncthreads();
-  double v = 0.0;
-  for (int q = threadIdx.x; q < A.W.nv; q += blockDim.x) v = nanMax(v, fabs(x[q]));
-  for (int o = 16; o > 0; o >>= 1) v = nanMax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0) atomicMaxPos(&m, v);
-  __syncthreads();
-  const double r = m;
-  __syncthreads();
-  return r;
+template <class C>
+__device__ void bPrecond(C& c, const BottomArgs& A, double* out, const double* in) {
+  bCells(c, A.W.nv, [&](int q) { out[q] = A.vc ? in[q] * A.W.lam[q] : in[q] * A.mult; });
+  bRelax(c, A, out, in, 2);
 }
 
 // RelaxSolver<T>::solve (AMRElliptic/RelaxSolver.H:128-186): repeated
 // preconditioner corrections e = preCond(r), phi += e, until the residual
 // norm falls below eps times the initial one, imax iterations or a hang.
-__device__ void relaxSolve(const BottomArgs& A) {
+template <class C>
+__device__ void bRelaxSolve(C& c, const BottomArgs& A) {
   const BottomWork& W = A.W;
-  const int nc = W.nv + W.ng;
-  auto zeroAll = [&](double* x) {
-    for (int q = threadIdx.x; q < nc; q += blockDim.x) x[q] = 0.0;
-    __syncthreads();
-  };
-  zeroAll(A.r);
-  blkOp(A, A.r, A.phi, A.rhs, 0);
-  double norm = blkNormType(A, A.r);
+  bOp(c, A, A.r, A.phi, A.rhs, 0);
+  double norm = bNormType(c, A, A.r);
   double minNorm = norm;
   int iter = 0;
   if (norm > 0.) {
     const double initialNorm = norm;
     while (iter < A.cfg.imax) {
-      zeroAll(A.e);
-      blkPrecond(A, A.e, A.r);
-      blkCells(A, [&](int q) { A.phi[q] = A.phi[q] + A.e[q] * 1.0; });
-      blkOp(A, A.r, A.phi, A.rhs, 0);
-      norm = blkNormType(A, A.r);
+      bPrecond(c, A, A.e, A.r);
+      bCells(c, W.nv, [&](int q) { A.phi[q] = A.phi[q] + A.e[q] * 1.0; });
+      bOp(c, A, A.r, A.phi, A.rhs, 0);
+      norm = bNormType(c, A, A.r);
       iter++;
       if (norm < A.cfg.eps * initialNorm) break;
       if (norm < minNorm)
@@ -1122,28 +1185,23 @@ __device__ void relaxSolve(const BottomArgs& A) {
         break;
     }
   }
-  if (threadIdx.x == 0) W.status[0] = 0, W.status[1] = iter;
+  if (c.tid() == 0) W.status[0] = 0, W.status[1] = iter;
 }
 
-__device__ void bicgstab(const BottomArgs& A) {
+template <class C>
+__device__ void bBicgstab(C& c, const BottomArgs& A) {
   const BottomWork& W = A.W;
-  const int nc = W.nv + W.ng;
-  auto zeroAll = [&](double* x) {
-    for (int q = threadIdx.x; q < nc; q += blockDim.x) x[q] = 0.0;
-    __syncthreads();
-  };
-  auto copyValid = [&](double* d, const double* s) { blkCells(A, [&](int q) { d[q] = s[q]; }); };
-  auto incrV = [&](double* y, const double* x, double sc) { blkCells(A, [&](int q) { y[q] = y[q] + x[q] * sc; }); };
-  zeroAll(A.r);
-  blkOp(A, A.r, A.phi, A.rhs, 0);
-  copyValid(A.rt, A.r);
-  zeroAll(A.e);
-  zeroAll(A.pt);
-  zeroAll(A.st);
+  const int nv = W.nv;
+  auto zeroV = [&](double* x) { bCells(c, nv, [&](int q) { x[q] = 0.0; }); };
+  auto copyV = [&](double* d, const double* s) { bCells(c, nv, [&](int q) { d[q] = s[q]; }); };
+  auto incrV = [&](double* y, const double* x, double sc) { bCells(c, nv, [&](int q) { y[q] = y[q] + x[q] * sc; }); };
+  bOp(c, A, A.r, A.phi, A.rhs, 0);
+  copyV(A.rt, A.r);
+  zeroV(A.e);
   int iter = 0, recount = 0, restarts = 0, status = 0;
   double rho[4] = {0, 0, 0, 0};
   double norm[2];
-  norm[0] = blkNormType(A, A.r);
+  norm[0] = bNormType(c, A, A.r);
   double initial_norm = norm[0];
   const double initial_residual = norm[0];
   norm[1] = norm[0];
@@ -1159,44 +1217,52 @@ __device__ void bicgstab(const BottomArgs& A) {
     omega[1] = omega[0];
     rho[3] = rho[2];
     rho[2] = rho[1];
-    rho[1] = blkDot(A, A.rt, A.r, false);
+    rho[1] = bDot(c, A, A.rt, A.r, false);
     if (rho[1] == 0.0) {
       incrV(A.phi, A.e, 1.0);
-      if (threadIdx.x == 0) W.status[0] = 2, W.status[1] = iter;
+      if (c.tid() == 0) W.status[0] = 2, W.status[1] = iter;
       return;
     }
     if (init) {
-      copyValid(A.p, A.r);
+      copyV(A.p, A.r);
       init = false;
     } else {
+      // p = beta p; p -= beta omega v; p += r (one pass, each element in that order)
       beta[1] = (rho[1] / rho[2]) * (alpha[1] / omega[1]);
-      blkCells(A, [&](int q) { A.p[q] = A.p[q] * beta[1]; });
-      incrV(A.p, A.v, -beta[1] * omega[1]);
-      incrV(A.p, A.r, 1.0);
+      const double b1 = beta[1], bo = -beta[1] * omega[1];
+      bCells(c, nv, [&](int q) {
+        double x = A.p[q] * b1;
+        x = x + A.v[q] * bo;
+        A.p[q] = x + A.r[q] * 1.0;
+      });
     }
-    blkPrecond(A, A.pt, A.p);
-    zeroAll(A.v);
-    blkOp(A, A.v, A.pt, nullptr, 1);
-    double m = blkDot(A, A.rt, A.v, false);
+    bPrecond(c, A, A.pt, A.p);
+    bOp(c, A, A.v, A.pt, nullptr, 1);
+    double m = bDot(c, A, A.rt, A.v, false);
     alpha[0] = rho[1] / m;
     if (fabs(m) > A.small * fabs(rho[1])) {
-      incrV(A.r, A.v, -alpha[0]);
-      norm[0] = blkNormType(A, A.r);
-      incrV(A.e, A.pt, alpha[0]);
+      const double a0 = alpha[0];
+      bCells(c, nv, [&](int q) {
+        A.r[q] = A.r[q] + A.v[q] * -a0;
+        A.e[q] = A.e[q] + A.pt[q] * a0;
+      });
+      norm[0] = bNormType(c, A, A.r);
     } else {
-      zeroAll(A.r);
+      zeroV(A.r);
       norm[0] = 0.0;
     }
     if (norm[0] > A.eps * initial_norm && norm[0] > A.reps * initial_residual) {
-      blkPrecond(A, A.st, A.r);
-      zeroAll(A.t);
-      blkOp(A, A.t, A.st, nullptr, 1);
-      double tr = blkDot(A, A.t, A.r, false);
-      double tt = blkDot(A, A.t, A.t, false);
+      bPrecond(c, A, A.st, A.r);
+      bOp(c, A, A.t, A.st, nullptr, 1);
+      double tr, tt;
+      bDot2(c, A, A.t, A.r, A.t, A.t, tr, tt);
       omega[0] = tr / tt;
-      incrV(A.e, A.st, omega[0]);
-      incrV(A.r, A.t, -omega[0]);
-      norm[0] = blkNormType(A, A.r);
+      const double w0 = omega[0];
+      bCells(c, nv, [&](int q) {
+        A.e[q] = A.e[q] + A.st[q] * w0;
+        A.r[q] = A.r[q] + A.t[q] * -w0;
+      });
+      norm[0] = bNormType(c, A, A.r);
     }
     if (norm[0] <= A.eps * initial_norm || norm[0] <= A.reps * initial_residual) {
       status = 1;
@@ -1209,35 +1275,30 @@ __device__ void bicgstab(const BottomArgs& A) {
         recount = 0;
         incrV(A.phi, A.e, 1.0);
         if (restarts == A.numRestarts) {
-          if (threadIdx.x == 0) W.status[0] = 3, W.status[1] = iter;
+          if (c.tid() == 0) W.status[0] = 3, W.status[1] = iter;
           return;
         }
-        blkOp(A, A.r, A.phi, A.rhs, 0);
-        norm[0] = blkNormType(A, A.r);
+        bOp(c, A, A.r, A.phi, A.rhs, 0);
+        norm[0] = bNormType(c, A, A.r);
         rho[1] = 0.0;
         rho[2] = 0.0;
         rho[3] = 0.0;
         alpha[0] = 0;
         beta[0] = 0;
         omega[0] = 0;
-        copyValid(A.rt, A.r);
-        zeroAll(A.e);
+        copyV(A.rt, A.r);
+        zeroV(A.e);
         restarts++;
         init = true;
       }
     }
   }
   incrV(A.phi, A.e, 1.0);
-  if (threadIdx.x == 0) W.status[0] = status, W.status[1] = iter;
+  if (c.tid() == 0) W.status[0] = status, W.status[1] = iter;
 }
 
-// One block per hierarchy of the level: block k solves with works[k] and
-// metrics[k], the rest of the arguments shared.
-__global__ void __launch_bounds__(1024) k_bottom(BottomArgs A0, const BottomWork* works, const double* metrics) {
-  BottomArgs A = A0;
-  A.W = works[blockIdx.x];
-  A.metric = metrics + blockIdx.x;
-  if (A0.epsPer && A0.cfg.kind == 0) A.eps = A0.epsPer[blockIdx.x];
+template <class C>
+__device__ void bottomRun(C& c, BottomArgs& A) {
   const BottomWork& W = A.W;
   A.r = W.v[0];
   A.rt = W.v[1];
@@ -1249,18 +1310,49 @@ __global__ void __launch_bounds__(1024) k_bottom(BottomArgs A0, const BottomWork
   A.v = W.v[7];
   A.phi = W.v[8];
   A.rhs = W.v[9];
-  const int nc = W.nv + W.ng;
-  for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+  bCells(c, W.nv, [&](int q) {
     A.phi[q] = A.phiFab[W.fab[q]];
     A.rhs[q] = A.rhsFab[W.fab[q]];
-  }
-  __syncthreads();
+  });
   if (A.cfg.kind == 1)
-    relaxSolve(A);
+    bRelaxSolve(c, A);
   else
-    bicgstab(A);
-  __syncthreads();
-  for (int q = threadIdx.x; q < W.nv; q += blockDim.x) A.phiFab[W.fab[q]] = A.phi[q];
+    bBicgstab(c, A);
+  c.sync();
+  for (int q = c.tid(); q < W.nv; q += c.nthr()) A.phiFab[W.fab[q]] = A.phi[q];
+}
+
+// One block per hierarchy of the level: block k solves with works[k] and
+// metrics[k], the rest of the arguments shared.
+__global__ void __launch_bounds__(1024) k_bottom(BottomArgs A0, const BottomWork* works, const double* metrics) {
+  extern __shared__ double spart[];
+  __shared__ double scal[8];
+  BottomArgs A = A0;
+  A.W = works[blockIdx.x];
+  A.metric = metrics + blockIdx.x;
+  if (A0.epsPer && A0.cfg.kind == 0) A.eps = A0.epsPer[blockIdx.x];
+  BlkCtx c;
+  c.part = spart;
+  c.part2 = spart + max(A.W.nbox, 32);
+  c.scal = scal;
+  c.k = 0;
+  bottomRun(c, A);
+}
+
+// One hierarchy, the whole grid (cooperative launch).
+__global__ void __launch_bounds__(kBottomGridThreads) k_bottom_grid(BottomArgs A, const BottomWork* works,
+                                                                    const double* metrics) {
+  __shared__ double stage[2 * kBottomStage];
+  A.W = works[0];
+  A.metric = metrics;
+  if (A.epsPer && A.cfg.kind == 0) A.eps = A.epsPer[0];
+  GridCtx c;
+  c.part = A.W.gpart;
+  c.part2 = A.W.gpart2;
+  c.scal = A.W.gscal;
+  c.stage = stage;
+  c.k = 0;
+  bottomRun(c, A);
 }
 
 __global__ void k_gather_slots(const int* fab, int n, const double* src, double* dst) {
@@ -1597,7 +1689,7 @@ void addLaunches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxe
 
 void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<double>& c, const BottomWork* works,
                  int nworks, int maxBoxes, const BottomConfig& cfg, double eps, const double* metrics,
-                 cudaStream_t s, const double* epsPer) {
+                 cudaStream_t s, const double* epsPer, int gridBlocks) {
   if (nworks == 0) return;
   BottomArgs A;
   A.boxes = L.boxes;
@@ -1615,9 +1707,40 @@ void bottomSolve(const LevelDev& L, double* phi, const double* rhs, const Coef<d
   A.numRestarts = cfg.numRestarts;
   // AMRPoissonOp::preCond multiplier (AMRPoissonOp.cpp:304-329).
   A.mult = 1.0 / (c.alpha - 2.0 * 3 * c.beta / (L.dx * L.dx));
-  k_bottom<<<nworks, 1024, maxBoxes * sizeof(double), s>>>(A, works, metrics);
+  if (gridBlocks > 0) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(gridBlocks);
+    lc.blockDim = dim3(kBottomGridThreads);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    check(cudaLaunchKernelEx(&lc, k_bottom_grid, A, works, metrics), "bottomSolve (grid)");
+    CMG_LAUNCHED("bottomSolve");
+    return;
+  }
+  const size_t smem = 2 * (size_t)std::max(maxBoxes, 32) * sizeof(double);
+  if (smem > 48 * 1024) {
+    if (smem > 200 * 1024) throw std::runtime_error("cmg: bottom level with too many boxes for one block");
+    check(cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "bottom smem");
+  }
+  k_bottom<<<nworks, 1024, smem, s>>>(A, works, metrics);
   CMG_LAUNCHED("bottomSolve");
 }
+
+int bottomGridBlocks(int nv) {
+  int dev = 0, sms = 0, occ = 0;
+  check(cudaGetDevice(&dev), "device");
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bottom_grid, kBottomGridThreads, 0), "occupancy");
+  const int want = (nv + kBottomGridThreads - 1) / kBottomGridThreads;
+  return std::max(1, std::min(want, sms * std::max(occ, 1)));
+}
+
+int bottomGridThreads() { return kBottomGridThreads; }
 
 void gatherSlots(const BottomWork& w, const double* fab, double* dst, cudaStream_t s) {
   const int n = w.nv + w.ng;

@@ -70,10 +70,11 @@ struct LevelPlan {
   std::vector<int64_t> hierStart;
 };
 
-// Compact indexing of the bottom level for the one-block BiCGStab: valid
-// cells first (box by box, x fastest, the reference's summation order), then
-// the face-ghost slots the 7-point stencil reads.  Every vector of the bottom
-// solve lives in this compact space, small enough to stay in L1.
+// Compact indexing of the bottom level for the bottom solve: valid cells
+// first (box by box, x fastest, the reference's summation order), then the
+// face-ghost slots the 7-point stencil reads (where the face coefficients of
+// a variable-coefficient operator are gathered).  The solve's vectors hold
+// the valid slots; a ghost's value is read from its source through nbv.
 struct BottomPlan {
   int nv = 0, ng = 0;            // valid cells, ghost slots
   std::vector<int> fab;          // FAB element index of every slot (nv + ng)
@@ -81,6 +82,8 @@ struct BottomPlan {
   std::vector<int> color[2];     // valid slots of each colour
   std::vector<int> boxStart;     // first valid slot of each box (nbox + 1)
   std::vector<int> gsrc, gkind;  // per ghost slot: source slot, 0 copy / 1 Dirichlet / 2 untouched
+  std::vector<int> nbv;          // 6 per valid cell: the neighbour's value source, a valid slot s
+                                 // (read as is) or -(s + 1) (a Dirichlet ghost: 0 - value)
 };
 void buildBottom(const LevelPlan& L, BottomPlan& B);
 

@@ -1046,6 +1046,19 @@ void buildBottom(const LevelPlan& L, BottomPlan& B) {
           B.gsrc[g] = s2->second;
         }
   }
+  // Every face ghost the stencil reads has a source (level 0 covers its
+  // domain), so the solve reads the source directly.
+  B.nbv.resize(B.nb.size());
+  for (size_t i = 0; i < B.nb.size(); ++i) {
+    const int n = B.nb[i];
+    if (n < B.nv) {
+      B.nbv[i] = n;
+      continue;
+    }
+    const int g = n - B.nv;
+    if (B.gkind[g] == 2) throw std::runtime_error("cmg: bottom level face ghost with no source");
+    B.nbv[i] = B.gkind[g] == 0 ? B.gsrc[g] : -(B.gsrc[g] + 1);
+  }
 }
 
 }  // namespace cmg

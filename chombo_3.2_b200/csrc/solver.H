@@ -200,6 +200,13 @@ class Solver {
   void ensureDeferred();
   // The bottom solver of the multigrid levels below level 0 (BottomConfig).
   void setBottomConfig(const BottomConfig& c);
+  // How the bottom solve runs: -1 automatic (the whole device for one
+  // hierarchy whose bottom level has at least kBottomGridMinCells cells,
+  // else one block per hierarchy), 0 one block, 1 the whole device (one
+  // hierarchy only).  The results are the same bit for bit.
+  void setBottomGrid(int mode);
+  bool bottomOnGrid() const { return bottomGrid_ > 0; }
+  static constexpr int kBottomGridMinCells = 4096;
   const BottomConfig& bottomConfig() const { return bottomCfg_; }
   // The variant of every AMR level then every multigrid depth (1: inline),
   // and the tuner's sweep times (ms; empty when a mode was forced).
@@ -378,6 +385,7 @@ class Solver {
   std::vector<BottomWork> bottoms_;         // one per hierarchy (one unless a forest)
   const BottomWork* dBottoms_ = nullptr;    // the same in device memory
   int maxBottomBoxes_ = 1;
+  int bottomGrid_ = 0;  // blocks of the grid-wide bottom solve, 0 for one block per hierarchy
   BottomConfig bottomCfg_;
   int nh_ = 1;                              // hierarchies (a forest: more than one)
   int* dActive_ = nullptr;                  // per hierarchy: still iterating (forest solves)

@@ -420,8 +420,7 @@ void Solver::setup(const std::vector<BottomPlan>& bps) {
       w.ncol[c] = (int)bp.color[c].size();
     }
     w.boxStart = upload(bufs_, bp.boxStart, s_);
-    w.gsrc = upload(bufs_, bp.gsrc, s_);
-    w.gkind = upload(bufs_, bp.gkind, s_);
+    w.nbv = upload(bufs_, bp.nbv, s_);
     for (int q = 0; q < 10; ++q) w.v[q] = alloc(nc);
     if (desc.vc) {
       w.a = alloc(nc);
@@ -432,6 +431,7 @@ void Solver::setup(const std::vector<BottomPlan>& bps) {
     w.status = (int*)bufs_.back()->p;
   }
   dBottoms_ = upload(bufs_, bottoms_, s_);
+  setBottomGrid(-1);
   dNorm_ = alloc(nh_);
   dMetric_ = alloc(nh_);
   if (nh_ > 1) dEps_ = alloc(nh_);
@@ -1066,6 +1066,30 @@ void Solver::setBottomConfig(const BottomConfig& c) {
   precondGraphs_.clear();
 }
 
+void Solver::setBottomGrid(int mode) {
+  if (mode < -1 || mode > 1) throw std::invalid_argument("cmg: bottom grid mode is -1 (automatic), 0 or 1");
+  // One hierarchy with a large bottom level: the solve spreads over the
+  // device in one cooperative launch (below that, one block is faster).
+  int blocks = 0;
+  if (nh_ == 1 && mode != 0 && (mode == 1 || bottoms_[0].nv >= kBottomGridMinCells)) {
+    BottomWork& w = bottoms_[0];
+    blocks = bottomGridBlocks(w.nv);
+    if (!w.gscal) {
+      const int nPart = std::max(w.nbox, blocks * bottomGridThreads() / 32);
+      w.gpart = alloc(nPart);
+      w.gpart2 = alloc(nPart);
+      w.gscal = alloc(8);
+      dBottoms_ = upload(bufs_, bottoms_, s_);
+    }
+  }
+  if (blocks == bottomGrid_) return;
+  bottomGrid_ = blocks;
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  graphs_.clear();
+  for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
+  precondGraphs_.clear();
+}
+
 void Solver::ensureDeferred() {
   auto one = [&](LevelPlan& p, LevelDev& d) {
     if (d.deferred || p.grids.size() == 0) return;
@@ -1168,7 +1192,7 @@ void Solver::bottom<double>(int depth, double* corr, double* res) {
   const LevelDev& L = depth == 0 ? amrDev_[0] : mgDev_[depth - 1];
   timed(P_BOTTOM, 0.0, [&]() {
     bottomSolve(L, corr, res, coefMG(depth), dBottoms_, nh_, maxBottomBoxes_, bottomCfg_, sp_.eps, dMetric_, s_,
-                dEps_);
+                dEps_, bottomGrid_);
   });
 }
 template <>
@@ -1180,7 +1204,7 @@ void Solver::bottom<float>(int depth, float* corr, float* res) {
   convert(res64, res, L.nelem, s_);
   timed(P_BOTTOM, 0.0, [&]() {
     bottomSolve(L, corr64, res64, coefMG(depth), dBottoms_, nh_, maxBottomBoxes_, bottomCfg_, sp_.eps, dMetric_,
-                s_, dEps_);
+                s_, dEps_, bottomGrid_);
   });
   convert(corr, corr64, L.nelem, s_);
 }

@@ -181,6 +181,13 @@ typedef struct cmg_bottom_params {
   double eps, hang, small;
 } cmg_bottom_params;
 int cmg_set_bottom_solver(cmg_hierarchy* h, const cmg_bottom_params* p);
+/* Where the bottom solve runs: -1 automatic (the default: across the whole
+ * device in one cooperative launch for a single hierarchy whose bottom level
+ * has at least 4096 cells, else one thread block per hierarchy), 0 one thread
+ * block per hierarchy, 1 the whole device (single hierarchies only; a forest
+ * keeps one block per hierarchy).  Identical results.  *on_grid (may be
+ * null) receives 1 when the grid-wide solve is in use. */
+int cmg_set_bottom_grid(cmg_hierarchy* h, int mode, int* on_grid);
 /* The relaxation variant of every AMR level, then every multigrid depth
  * (0 = ghost fills, 1 = in-pass ghosts, 2 = all sweeps in one one-block
  * launch, for levels of at most 32768 cells, 3 = fused sweeps), with the autotuner's times in

@@ -41,6 +41,9 @@ CASES = {
     "helmholtz_1lev_32_periodic": ("n0=32 levels=1 maxbox=16 op=0 alpha=1 beta=-0.1 bc=PPPPPP", True),
     "vc_1lev_32_periodic": ("n0=32 levels=1 maxbox=16 op=1 alpha=1 beta=-1 bc=PPPPPP", True),
     "helmholtz_1lev_32_ppnndd": ("n0=32 levels=1 maxbox=16 op=0 alpha=1 beta=-0.1 bc=PPNNDD", True),
+    # 4096 boxes of 4^3: the bottom level (32^3 in 4096 boxes of 2^3) is large enough for the grid-wide bottom solve
+    "helmholtz_1lev_64_periodic_box4": ("n0=64 levels=1 maxbox=4 block=4 op=0 alpha=1 beta=-0.1 bc=PPPPPP", False),
+    "vc_1lev_64_box4": ("n0=64 levels=1 maxbox=4 block=4 op=1 alpha=1 beta=-1", False),
     "vc_3lev_32": ("n0=32 levels=3 maxbox=16 op=1 alpha=1 beta=-1", False),
     "vc_2lev_64": ("n0=64 levels=2 maxbox=32 op=1 alpha=1 beta=-1", False),
     "config0_poisson_64": ("n0=64 levels=1 maxbox=32 op=0 alpha=0 beta=1", True),

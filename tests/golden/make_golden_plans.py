@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 ORACLE = os.path.join(ROOT, "oracle", "_ref", "cmg_oracle")
 
-CASES = ["config1_vc_3lev_128", "config2_vc_3lev_256"]
+CASES = ["config1_vc_3lev_128", "config2_vc_3lev_256", "helmholtz_1lev_64_periodic_box4", "vc_1lev_64_box4"]
 
 
 def run_case(name):

@@ -296,6 +296,116 @@ __global__ void k_gsrb(const BoxDesc* boxes, const Chunk* chunks, T* phi, const 
   }
 }
 
+// One GSRB update (k_gsrb's arithmetic) from loaded values: v the six
+// neighbours (+x, -x, +y, -y, +z, -z), f the face coefficients
+// (b0[+x], b0[c], b1[+y], b1[c], b2[+z], b2[c]) of a VC operator.
+template <class T, int VC>
+__device__ __forceinline__ T gsrbValue(const Scal& sc, T pc, T rh, const T* v, T av, T lv, const T* f) {
+  const T dxinv = T(sc.dxinv);
+  if (VC) {
+    T div = f[0] * (v[0] - pc) - f[1] * (pc - v[1]) + f[2] * (v[2] - pc) - f[3] * (pc - v[3]) + f[4] * (v[4] - pc) -
+            f[5] * (pc - v[5]);
+    T lofphi = T(sc.alpha) * av * pc - T(sc.beta) * div * dxinv;
+    return pc - lv * (lofphi - rh);
+  } else if (sc.laplacian) {
+    T lphi = (v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) * dxinv;
+    return T(sc.lambda) * (rh - lphi);
+  } else {
+    T lphi = ((v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) - T(2.0) * T(3) * pc) * dxinv;
+    T helmop = T(sc.alpha) * pc + T(sc.beta) * lphi;
+    return pc + T(sc.lambda) * (helmop - rh);
+  }
+}
+
+// The one-colour pass of k_gsrb (ghosts filled before the pass) with two
+// cells per thread: colour indices q and q + 1 of the chunk, which for an
+// even number of colour cells per row are neighbours in one row (i and
+// i + 2), sharing the enumeration, the index arithmetic and the x-neighbour
+// between them (phi[oth + xo] is +x of the first and -x of the second).  A
+// pair split across rows (odd rows) takes the second cell's own indices.
+// All loads come before both stores (cells of one colour read only the other
+// colour and themselves), so the two updates are those of k_gsrb.
+template <class T, int VC>
+__device__ __forceinline__ void gsrbOne(const BoxDesc& bd, int i, int j, int k, T* phi, const T* rhs, const Scal& sc,
+                                        const T* a, const T* b0, const T* b1, const T* b2, const T* lam) {
+  const Stencil s = stencil(bd, i, j, k);
+  const T v[6] = {phi[s.xp], phi[s.xm], phi[s.yp], phi[s.ym], phi[s.zp], phi[s.zm]};
+  T f[6], av = T(0), lv = T(0);
+  if (VC) {
+    av = a[s.c];
+    lv = lam[s.c];
+    f[0] = b0[s.xp];
+    f[1] = b0[s.c];
+    f[2] = b1[s.yp];
+    f[3] = b1[s.c];
+    f[4] = b2[s.zp];
+    f[5] = b2[s.c];
+  }
+  phi[s.c] = gsrbValue<T, VC>(sc, phi[s.c], rhs[s.c], v, av, lv, f);
+}
+
+// The one-colour pass of k_gsrb (ghosts filled before the pass) with two
+// cells per thread: colour indices q and q + 1 of the chunk, which for an
+// even number of colour cells per row are neighbours in one row (i and
+// i + 2), sharing the enumeration, the index arithmetic and the x-neighbour
+// between them (phi[oth + xo] is +x of the first and -x of the second).  A
+// pair split across rows (odd rows) updates its cells one by one.  All loads
+// of a pair come before its stores (cells of one colour read only the other
+// colour and themselves), so the updates are those of k_gsrb.
+template <class T, int VC>
+__global__ void __launch_bounds__(CHUNK / 2) k_gsrb_pair(const BoxDesc* boxes, const Chunk* chunks, T* phi,
+                                                         const T* rhs, int color, Scal sc, const T* a, const T* b0,
+                                                         const T* b1, const T* b2, const T* lam) {
+  const Chunk ch = chunks[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  const int q = ch.start + 2 * threadIdx.x;
+  const int nx = bd.hi[0] - bd.lo[0] + 1, ny = bd.hi[1] - bd.lo[1] + 1, nz = bd.hi[2] - bd.lo[2] + 1;
+  const int half = (nx + 1) / 2;
+  const int r = fastDiv(q, half, bd.mHalf);
+  if (r >= ny * nz) return;
+  const int kk = fastDiv(r, ny, bd.mNy);
+  const int j = bd.lo[1] + (r - kk * ny), k = bd.lo[2] + kk;
+  const int m = q - r * half;
+  const int i = bd.lo[0] + ((bd.lo[0] + j + k + color) & 1) + 2 * m;
+  if (m + 1 < half && i + 2 <= bd.hi[0]) {
+    // both cells in this row
+    const Stencil st = stencil(bd, i, j, k);
+    const int c = st.c;
+    const T pc0 = phi[c], pc1 = phi[c + 1];
+    const T rh0 = rhs[c], rh1 = rhs[c + 1];
+    const T xm = phi[st.xm], xc = phi[st.xp], xp = phi[st.xp + 1];
+    const T v0[6] = {xc, xm, phi[st.yp], phi[st.ym], phi[st.zp], phi[st.zm]};
+    const T v1[6] = {xp, xc, phi[st.yp + 1], phi[st.ym + 1], phi[st.zp + 1], phi[st.zm + 1]};
+    T av0 = T(0), av1 = T(0), lv0 = T(0), lv1 = T(0), f0[6], f1[6];
+    if (VC) {
+      av0 = a[c];
+      av1 = a[c + 1];
+      lv0 = lam[c];
+      lv1 = lam[c + 1];
+      f0[0] = b0[st.xp];
+      f0[1] = b0[c];
+      f0[2] = b1[st.yp];
+      f0[3] = b1[c];
+      f0[4] = b2[st.zp];
+      f0[5] = b2[c];
+      f1[0] = b0[st.xp + 1];
+      f1[1] = b0[c + 1];
+      f1[2] = b1[st.yp + 1];
+      f1[3] = b1[c + 1];
+      f1[4] = b2[st.zp + 1];
+      f1[5] = b2[c + 1];
+    }
+    const T n0 = gsrbValue<T, VC>(sc, pc0, rh0, v0, av0, lv0, f0);
+    const T n1 = gsrbValue<T, VC>(sc, pc1, rh1, v1, av1, lv1, f1);
+    phi[c] = n0;
+    phi[c + 1] = n1;
+    return;
+  }
+  if (i <= bd.hi[0]) gsrbOne<T, VC>(bd, i, j, k, phi, rhs, sc, a, b0, b1, b2, lam);
+  int i1, j1, k1;
+  if (colorCell(bd, q + 1, color, i1, j1, k1)) gsrbOne<T, VC>(bd, i1, j1, k1, phi, rhs, sc, a, b0, b1, b2, lam);
+}
+
 // n red-black sweeps of a small level in one launch: one block walks every
 // cell of a colour (ghosts from their rules), synchronises, and goes on to
 // the next colour and sweep -- the launches of 2n colour passes replaced by
@@ -1507,16 +1617,19 @@ void gsrb(const LevelDev& L, T* phi, const T* rhs, const Coef<T>& c, int color, 
     kern<<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, a, b0, b1, b2, lam,
                              L.chGhost[color], L.chGhostStart[color], gc);
   };
+  auto launchPair = [&](auto kern, const T* a, const T* b0, const T* b1, const T* b2, const T* lam) {
+    kern<<<n, CHUNK / 2, 0, s>>>(L.boxes, L.chColor[color], phi, rhs, color, sc, a, b0, b1, b2, lam);
+  };
   if (c.vc) {
     if (inlineGhosts)
       launch(k_gsrb<T, 1, true>, c.a, c.b[0], c.b[1], c.b[2], c.lambda);
     else
-      launch(k_gsrb<T, 1, false>, c.a, c.b[0], c.b[1], c.b[2], c.lambda);
+      launchPair(k_gsrb_pair<T, 1>, c.a, c.b[0], c.b[1], c.b[2], c.lambda);
   } else {
     if (inlineGhosts)
       launch(k_gsrb<T, 0, true>, nullptr, nullptr, nullptr, nullptr, nullptr);
     else
-      launch(k_gsrb<T, 0, false>, nullptr, nullptr, nullptr, nullptr, nullptr);
+      launchPair(k_gsrb_pair<T, 0>, nullptr, nullptr, nullptr, nullptr, nullptr);
   }
   CMG_LAUNCHED("gsrb");
 }

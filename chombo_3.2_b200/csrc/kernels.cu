@@ -580,36 +580,98 @@ __global__ void __launch_bounds__(256) k_gsrb_deferred(const BoxDesc* boxes, con
 }
 
 // OPERATORLAPRES / OPERATORLAP (AMRPoissonOpF.ChF:287-377) and
-// VCCOMPUTERES3D / VCCOMPUTEOP3D (VCAMRPoissonOpF.ChF:148-312).
-// mode 0: r = rhs - L(phi) (residual form), mode 1: r = L(phi).
-// Each block takes half a colour chunk of both colours: threads 0-127 the
-// colour-0 cells of 128 consecutive slots, threads 128-255 the colour-1 cells
-// of the same slots (the two colour chunk lists of a box have the same
-// boundaries).  Every warp reads one colour half of each array, and the
-// block's two halves read each other's cells as neighbours from L1.
+// VCCOMPUTERES3D / VCCOMPUTEOP3D (VCAMRPoissonOpF.ChF:148-312) value of one
+// cell from loaded values (v and f as in gsrbValue).  MODE 0: r = rhs - L(phi)
+// (residual form), MODE 1: r = L(phi).
 template <class T, int VC, int MODE>
-__global__ void k_op(const BoxDesc* boxes, const Chunk* ch0, const Chunk* ch1, T* r, const T* phi, const T* rhs,
-                     Scal sc, const T* a, const T* b0, const T* b1, const T* b2) {
-  const int color = threadIdx.x >= CHUNK / 2;
-  Chunk ch = (color ? ch1 : ch0)[blockIdx.x >> 1];
-  const BoxDesc bd = boxes[ch.box];
-  int i, j, k;
-  if (!colorCell(bd, ch.start + (blockIdx.x & 1) * (CHUNK / 2) + (threadIdx.x & (CHUNK / 2 - 1)), color, i, j, k))
-    return;
-  const Stencil st = stencil(bd, i, j, k);
-  const int64_t c = st.c;
+__device__ __forceinline__ T opValue(const Scal& sc, T pc, T rh, const T* v, T av, const T* f) {
   const T dxinv = T(sc.dxinv);
-  T pc = phi[c];
   if (VC) {
-    T lofphi = T(sc.alpha) * a[c] * pc - T(sc.beta) * vcDiv(phi, b0, b1, b2, st) * dxinv;
-    r[c] = MODE == 0 ? rhs[c] - lofphi : lofphi;
+    T div = f[0] * (v[0] - pc) - f[1] * (pc - v[1]) + f[2] * (v[2] - pc) - f[3] * (pc - v[3]) + f[4] * (v[4] - pc) -
+            f[5] * (pc - v[5]);
+    T lofphi = T(sc.alpha) * av * pc - T(sc.beta) * div * dxinv;
+    return MODE == 0 ? rh - lofphi : lofphi;
   } else {
-    T lap = (nbrSum(phi, st) - T(6) * pc) * dxinv;
-    if (MODE == 0)
-      r[c] = -(T(sc.alpha) * pc) - T(sc.beta) * lap + rhs[c];
-    else
-      r[c] = T(sc.alpha) * pc + T(sc.beta) * lap;
+    T lap = ((v[0] + v[1] + v[2] + v[3] + v[4] + v[5]) - T(6) * pc) * dxinv;
+    return MODE == 0 ? -(T(sc.alpha) * pc) - T(sc.beta) * lap + rh : T(sc.alpha) * pc + T(sc.beta) * lap;
   }
+}
+
+template <class T, int VC, int MODE>
+__device__ __forceinline__ void opOne(const BoxDesc& bd, int i, int j, int k, T* r, const T* phi, const T* rhs,
+                                      const Scal& sc, const T* a, const T* b0, const T* b1, const T* b2) {
+  const Stencil s = stencil(bd, i, j, k);
+  const T v[6] = {phi[s.xp], phi[s.xm], phi[s.yp], phi[s.ym], phi[s.zp], phi[s.zm]};
+  T f[6], av = T(0);
+  if (VC) {
+    av = a[s.c];
+    f[0] = b0[s.xp];
+    f[1] = b0[s.c];
+    f[2] = b1[s.yp];
+    f[3] = b1[s.c];
+    f[4] = b2[s.zp];
+    f[5] = b2[s.c];
+  }
+  r[s.c] = opValue<T, VC, MODE>(sc, phi[s.c], MODE == 0 ? rhs[s.c] : T(0), v, av, f);
+}
+
+// The operator / residual over both colours with two same-row cells per
+// thread (as k_gsrb_pair): threads 0-127 take the colour-0 cells of one
+// colour chunk, threads 128-255 the colour-1 cells of the chunk with the same
+// boundaries, so a block reads both colour halves of the same slots and each
+// half finds its neighbours in the other's lines.
+template <class T, int VC, int MODE>
+__global__ void __launch_bounds__(CHUNK) k_op_pair(const BoxDesc* boxes, const Chunk* ch0, const Chunk* ch1, T* r,
+                                                   const T* phi, const T* rhs, Scal sc, const T* a, const T* b0,
+                                                   const T* b1, const T* b2) {
+  const int color = threadIdx.x >= CHUNK / 2;
+  const Chunk ch = (color ? ch1 : ch0)[blockIdx.x];
+  const BoxDesc bd = boxes[ch.box];
+  const int q = ch.start + 2 * (threadIdx.x & (CHUNK / 2 - 1));
+  const int nx = bd.hi[0] - bd.lo[0] + 1, ny = bd.hi[1] - bd.lo[1] + 1, nz = bd.hi[2] - bd.lo[2] + 1;
+  const int half = (nx + 1) / 2;
+  const int rr = fastDiv(q, half, bd.mHalf);
+  if (rr >= ny * nz) return;
+  const int kk = fastDiv(rr, ny, bd.mNy);
+  const int j = bd.lo[1] + (rr - kk * ny), k = bd.lo[2] + kk;
+  const int m = q - rr * half;
+  const int i = bd.lo[0] + ((bd.lo[0] + j + k + color) & 1) + 2 * m;
+  if (m + 1 < half && i + 2 <= bd.hi[0]) {
+    const Stencil st = stencil(bd, i, j, k);
+    const int c = st.c;
+    const T pc0 = phi[c], pc1 = phi[c + 1];
+    T rh0 = T(0), rh1 = T(0);
+    if (MODE == 0) {
+      rh0 = rhs[c];
+      rh1 = rhs[c + 1];
+    }
+    const T xm = phi[st.xm], xc = phi[st.xp], xp = phi[st.xp + 1];
+    const T v0[6] = {xc, xm, phi[st.yp], phi[st.ym], phi[st.zp], phi[st.zm]};
+    const T v1[6] = {xp, xc, phi[st.yp + 1], phi[st.ym + 1], phi[st.zp + 1], phi[st.zm + 1]};
+    T av0 = T(0), av1 = T(0), f0[6], f1[6];
+    if (VC) {
+      av0 = a[c];
+      av1 = a[c + 1];
+      f0[0] = b0[st.xp];
+      f0[1] = b0[c];
+      f0[2] = b1[st.yp];
+      f0[3] = b1[c];
+      f0[4] = b2[st.zp];
+      f0[5] = b2[c];
+      f1[0] = b0[st.xp + 1];
+      f1[1] = b0[c + 1];
+      f1[2] = b1[st.yp + 1];
+      f1[3] = b1[c + 1];
+      f1[4] = b2[st.zp + 1];
+      f1[5] = b2[c + 1];
+    }
+    r[c] = opValue<T, VC, MODE>(sc, pc0, rh0, v0, av0, f0);
+    r[c + 1] = opValue<T, VC, MODE>(sc, pc1, rh1, v1, av1, f1);
+    return;
+  }
+  if (i <= bd.hi[0]) opOne<T, VC, MODE>(bd, i, j, k, r, phi, rhs, sc, a, b0, b1, b2);
+  int i1, j1, k1;
+  if (colorCell(bd, q + 1, color, i1, j1, k1)) opOne<T, VC, MODE>(bd, i1, j1, k1, r, phi, rhs, sc, a, b0, b1, b2);
 }
 
 template <class T>
@@ -1666,13 +1728,13 @@ template <class T>
 void residual(const LevelDev& L, T* r, const T* phi, const T* rhs, const Coef<T>& c, cudaStream_t s) {
   if (L.nAll == 0) return;
   Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
-  const int n = 2 * L.nColor[0];
+  const int n = L.nColor[0];
   if (c.vc)
-    k_op<T, 1, 0><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], r, phi, rhs, sc, c.a, c.b[0], c.b[1],
-                                      c.b[2]);
+    k_op_pair<T, 1, 0><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], r, phi, rhs, sc, c.a, c.b[0],
+                                           c.b[1], c.b[2]);
   else
-    k_op<T, 0, 0><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], r, phi, rhs, sc, nullptr, nullptr,
-                                      nullptr, nullptr);
+    k_op_pair<T, 0, 0><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], r, phi, rhs, sc, nullptr, nullptr,
+                                           nullptr, nullptr);
   CMG_LAUNCHED("residual");
 }
 
@@ -1680,13 +1742,13 @@ template <class T>
 void applyOp(const LevelDev& L, T* lofphi, const T* phi, const Coef<T>& c, cudaStream_t s) {
   if (L.nAll == 0) return;
   Scal sc = scalars(L.dx, c.alpha, c.beta, c.vc);
-  const int n = 2 * L.nColor[0];
+  const int n = L.nColor[0];
   if (c.vc)
-    k_op<T, 1, 1><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], lofphi, phi, nullptr, sc, c.a, c.b[0],
-                                      c.b[1], c.b[2]);
+    k_op_pair<T, 1, 1><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], lofphi, phi, nullptr, sc, c.a,
+                                           c.b[0], c.b[1], c.b[2]);
   else
-    k_op<T, 0, 1><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], lofphi, phi, nullptr, sc, nullptr,
-                                      nullptr, nullptr, nullptr);
+    k_op_pair<T, 0, 1><<<n, CHUNK, 0, s>>>(L.boxes, L.chColor[0], L.chColor[1], lofphi, phi, nullptr, sc, nullptr,
+                                           nullptr, nullptr, nullptr);
   CMG_LAUNCHED("applyOp");
 }
 

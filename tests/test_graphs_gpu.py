@@ -50,13 +50,16 @@ def test_graph_replay_is_bit_identical(cmg, name, mixed):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,num_mg", [("vc_3lev_16", 1), ("poisson_3lev_32", 1), ("helmholtz_2lev_16", 1),
                                          ("vc_3lev_16", 2), ("poisson_1lev_32", 1), ("vc_1lev_32", 2),
-                                         ("poisson_3lev_32_walls", 1), ("vc_3lev_16_walls", 2)])
+                                         ("poisson_3lev_32_walls", 1), ("vc_3lev_16_walls", 2),
+                                         ("helmholtz_1lev_32_periodic", 1), ("helmholtz_1lev_32_ppnndd", 2),
+                                         ("helmholtz_1lev_64_periodic_box4", 1)])
 def test_relaxation_variants_are_bit_identical(cmg, name, num_mg):
     """Ghost fill before each colour pass (mode 1), face ghosts evaluated in
     the pass (mode 2), fused sweeps (mode 3: both colours per launch, boxes
     marching in z, exchange-face colour-1 cells in a second launch) and the
     autotuned mix (mode 0) give the same bits, with V-cycles and with W-cycles
-    (num_mg=2), on one and on several levels, FP64 and mixed precision."""
+    (num_mg=2), on one and on several levels, FP64 and mixed precision, on
+    walled and periodic domains."""
     h, p, meta = make(cmg, name)
     p.num_mg = num_mg
     nlev = len(meta["boxes"])

@@ -1001,9 +1001,9 @@ def main():
         traffic = t["dram_bytes_per_launch"] if t else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": f"k_gsrb<{'float' if mixed else 'double'},{meta['op']}>: one red-black colour pass over "
-                          "the finest AMR level (two launches per sweep; the one-colour ghost fill between them is "
-                          "timed separately)",
+                "kernel": f"k_gsrb_pair<{'float' if mixed else 'double'},{meta['op']}>: one red-black colour pass "
+                          "over the finest AMR level (two launches per sweep; the one-colour ghost fill between them "
+                          "is timed separately)",
                 "peak_kind": peak_kind, "launches": int(n_fine),
                 "avg_launch_us": 1000.0 * ms_fine / max(n_fine, 1),
                 "algorithmic_bytes_per_launch": bytes_fine / max(n_fine, 1)}

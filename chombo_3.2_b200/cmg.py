@@ -411,6 +411,12 @@ class Hierarchy:
     def set_relax_mode(self, mode):
         _check(lib().cmg_set_relax_mode(self.h, int(mode)))
 
+    def setup_seconds(self):
+        """(plan building, device set-up) host seconds of the hierarchy's creation."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(lib().cmg_setup_seconds(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def set_bottom_solver(self, kind=0, imax=None, num_restarts=5, norm_type=2, eps=1e-6, hang=None, small=1e-30):
         """kind 0 BiCGStabSolver (defaults imax 80, hang 1e-8), 1 RelaxSolver (defaults imax 40, hang 0)."""
         if imax is None:

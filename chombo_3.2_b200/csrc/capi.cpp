@@ -408,6 +408,14 @@ int cmg_set_relax_mode(cmg_hierarchy* h, int mode) {
   });
 }
 
+int cmg_setup_seconds(const cmg_hierarchy* h, double* plans, double* device) {
+  return guard([&]() {
+    needLevel(h, 0);
+    if (plans) *plans = h->solver->planSeconds();
+    if (device) *device = h->solver->deviceSeconds();
+  });
+}
+
 int cmg_set_bottom_grid(cmg_hierarchy* h, int mode, int* on_grid) {
   return guard([&]() {
     needLevel(h, 0);

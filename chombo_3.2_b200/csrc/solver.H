@@ -199,6 +199,10 @@ class Solver {
   // Builds and uploads the fused sweep's deferred-cell lists (once).
   void ensureDeferred();
   // The bottom solver of the multigrid levels below level 0 (BottomConfig).
+  // Host seconds of the constructor: plan building, then device set-up
+  // (allocation, uploads, coefficient fills); 0 for a forest.
+  double planSeconds() const { return planSeconds_; }
+  double deviceSeconds() const { return deviceSeconds_; }
   void setBottomConfig(const BottomConfig& c);
   // How the bottom solve runs: -1 automatic (the whole device for one
   // hierarchy whose bottom level has at least kBottomGridMinCells cells,
@@ -385,7 +389,8 @@ class Solver {
   std::vector<BottomWork> bottoms_;         // one per hierarchy (one unless a forest)
   const BottomWork* dBottoms_ = nullptr;    // the same in device memory
   int maxBottomBoxes_ = 1;
-  int bottomGrid_ = 0;  // blocks of the grid-wide bottom solve, 0 for one block per hierarchy
+  int bottomGrid_ = 0;
+  double planSeconds_ = 0, deviceSeconds_ = 0;  // blocks of the grid-wide bottom solve, 0 for one block per hierarchy
   BottomConfig bottomCfg_;
   int nh_ = 1;                              // hierarchies (a forest: more than one)
   int* dActive_ = nullptr;                  // per hierarchy: still iterating (forest solves)

@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <mutex>
 #include <exception>
@@ -274,10 +275,14 @@ static void hierarchyPlans(const HierarchyDesc& desc, std::vector<LevelPlan>& am
 
 Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
     : s_(stream), own_(stream), desc_(desc), alpha0_(desc.alpha), beta0_(desc.beta) {
+  const auto t0 = std::chrono::steady_clock::now();
   hierarchyPlans(desc, amr_, mg_);
   std::vector<BottomPlan> bps(1);
   buildBottom(mg_.empty() ? amr_[0] : mg_.back(), bps[0]);
+  const auto t1 = std::chrono::steady_clock::now();
   setup(bps);
+  planSeconds_ = std::chrono::duration<double>(t1 - t0).count();
+  deviceSeconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
 }
 
 // A forest: hierarchies with the same domain, cell size, level count,

@@ -432,6 +432,10 @@ int cmg_serve_batched(const cmg_request* reqs, int n, double hbm_budget, int max
 /* Algorithmic bytes moved per V-cycle (roofline numerator). */
 int cmg_vcycle_bytes(const cmg_hierarchy* h, const cmg_solve_params* p, double* out);
 
+/* Host seconds cmg_hierarchy_create spent building the plans (layouts,
+ * exchange, coarse-fine, flux-register and bottom tables) and setting up the
+ * device (allocation, uploads); either pointer may be null. */
+int cmg_setup_seconds(const cmg_hierarchy* h, double* plans, double* device);
 /* The CUDA stream every call of this hierarchy runs on (cudaStream_t). */
 int cmg_get_stream(const cmg_hierarchy* h, void** stream);
 /* Streams (no counterpart in the reference, whose calls are synchronous host

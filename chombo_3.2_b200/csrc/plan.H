@@ -89,12 +89,18 @@ void buildBottom(const LevelPlan& L, BottomPlan& B);
 
 // Face-ghost rules of a level from its ghost tasks (LevelPlan::faceRules).
 void buildFaceRules(LevelPlan& L);
+// buildFaceRules unless the level has them; true when it built them.
+bool ensureFaceRules(LevelPlan& L);
 // The colour-1 cells on exchange faces (LevelPlan::deferred), for the fused
 // sweep; built on demand, after the face rules.
 void buildDeferred(LevelPlan& L);
 // Levels of at most this many cells get the per-chunk ghost lists of the
 // prefill relaxation variant (LevelPlan::chunkGhost).
 constexpr int64_t kPrefillMaxCells = int64_t(1) << 22;
+// Levels up to this many cells get their face rules with the plan (the
+// one-block relaxation uses them); larger ones only when the fused sweep asks
+// for them (ensureFaceRules).
+constexpr int64_t kFaceRulesEagerCells = 32768;
 
 // Layout and ghost/chunk plans of one level (AMR level or multigrid depth).
 // dxCrse > 0 enables homogeneous coarse-fine ghost tasks on CF faces.

@@ -107,6 +107,12 @@ void parallelItems(size_t n, F fn) {
 void buildDeferred(LevelPlan& L);
 void buildChunkGhosts(LevelPlan& L);
 
+bool ensureFaceRules(LevelPlan& L) {
+  if (!L.faceOff.empty() || L.grids.size() == 0) return false;
+  buildFaceRules(L);
+  return true;
+}
+
 // Rules of every face-ghost cell from the level's ghost tasks (the fill with
 // coarse-fine values that precedes each relaxation pass).
 void buildFaceRules(LevelPlan& L) {
@@ -375,7 +381,9 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     L.ghostStart.push_back(L.ghostStart.back() + (int)c);
   }
   L.ghostBlock = blockTasks(L.ghostStart);
-  buildFaceRules(L);
+  L.faceRules.clear();
+  L.faceOff.clear();
+  if (grids.numCells() <= kFaceRulesEagerCells) buildFaceRules(L);
   if (L.nelem >= ((int64_t)1 << 31)) throw std::runtime_error("cmg: level too large for 32-bit ghost indices");
   // Flat lists: per parity the exchange and boundary tasks, then the
   // coarse-fine ones, each task's cells of that parity in k, j, i order.
@@ -454,7 +462,10 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
   // The prefill variant's per-chunk lists only where that variant can win
   // (latency-bound levels): on larger levels the separate fill is as fast,
   // and the lists would add as much host work and memory as the fill lists.
-  if (grids.numCells() <= kPrefillMaxCells) buildChunkGhosts(L);
+  if (grids.numCells() <= kPrefillMaxCells) {
+    ensureFaceRules(L);  // the per-chunk lists are made from the face rules
+    buildChunkGhosts(L);
+  }
 }
 
 int ownerOf(const LevelPlan& L, const IV& p) {
@@ -1145,17 +1156,20 @@ void mergeLevels(const std::vector<const LevelPlan*>& parts, const std::vector<i
         (cf ? out.gcCF[par] : out.gcExch[par]) += n;
       }
   }
-  // face rules, per-chunk ghosts (kept only when every part has them)
-  bool chunkLists = true;
+  // face rules, per-chunk ghosts (each kept only when every part has them;
+  // face rules missing here are built on the merged plan when asked for)
+  bool chunkLists = true, rules = true;
   for (size_t k = 0; k < K; ++k) chunkLists = chunkLists && !parts[k]->chunkGhostStart[0].empty();
+  for (size_t k = 0; k < K; ++k) rules = rules && (!parts[k]->faceOff.empty() || parts[k]->grids.size() == 0);
   for (size_t k = 0; k < K; ++k) {
     const LevelPlan& p = *parts[k];
     const int rbase = (int)out.faceRules.size();
     for (FaceRule r : p.faceRules) {
+      if (!rules) break;
       if (r.kind == FR_COPY || r.kind == FR_CFQUAD || r.kind == FR_FAB) r.src += (int)elemOff[k];
       out.faceRules.push_back(r);
     }
-    for (size_t q = 0; q + 1 < p.faceOff.size(); ++q) out.faceOff.push_back(p.faceOff[q] + rbase);
+    for (size_t q = 0; rules && q + 1 < p.faceOff.size(); ++q) out.faceOff.push_back(p.faceOff[q] + rbase);
     for (int c = 0; c < 2 && chunkLists; ++c) {
       const int gbase = (int)out.chunkGhost[c].size();
       for (const GhostCell& g : p.chunkGhost[c]) out.chunkGhost[c].push_back(shiftCell(g, elemOff[k]));
@@ -1163,7 +1177,7 @@ void mergeLevels(const std::vector<const LevelPlan*>& parts, const std::vector<i
         out.chunkGhostStart[c].push_back(p.chunkGhostStart[c][q] + gbase);
     }
   }
-  out.faceOff.push_back((int)out.faceRules.size());
+  if (rules) out.faceOff.push_back((int)out.faceRules.size());
   for (int c = 0; c < 2 && chunkLists; ++c) out.chunkGhostStart[c].push_back((int)out.chunkGhost[c].size());
   // zeroing of the cells under the finer level
   for (size_t k = 0; k < K; ++k)

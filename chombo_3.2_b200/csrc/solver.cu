@@ -1098,6 +1098,10 @@ void Solver::setBottomGrid(int mode) {
 void Solver::ensureDeferred() {
   auto one = [&](LevelPlan& p, LevelDev& d) {
     if (d.deferred || p.grids.size() == 0) return;
+    if (ensureFaceRules(p)) {
+      d.faceRules = upload(bufs_, p.faceRules, s_);
+      d.faceOff = upload(bufs_, p.faceOff, s_);
+    }
     buildDeferred(p);
     d.deferred = upload(bufs_, p.deferred, s_);
     d.nDeferred = (int)p.deferred.size();

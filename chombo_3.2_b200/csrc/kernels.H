@@ -176,6 +176,7 @@ struct BottomConfig {
 };
 struct BottomWork {
   int nv = 0, ng = 0, nbox = 0, ncol[2] = {0, 0};
+  int maxBoxCells = 0;  // cells of the largest box
   const int *fab = nullptr, *nb = nullptr, *col[2] = {nullptr, nullptr}, *boxStart = nullptr;
   const int* nbv = nullptr;  // 6 per valid slot: face neighbour value source (BottomPlan::nbv)
   double* v[10] = {};

@@ -1142,6 +1142,7 @@ __device__ __forceinline__ double foldRun(double acc, const double* p, int n, bo
 }
 
 struct BlkCtx {
+  static constexpr bool kGrid = false;
   double* part;   // per-box partials (dynamic shared memory)
   double* part2;  // a second set, for two sums folded together
   double* scal;   // 8 rotating broadcast slots (shared)
@@ -1165,6 +1166,7 @@ struct BlkCtx {
 };
 
 struct GridCtx {
+  static constexpr bool kGrid = true;
   double* part;   // per-box partials (global)
   double* part2;
   double* scal;   // 8 rotating broadcast slots (global)
@@ -1360,16 +1362,76 @@ __device__ void bRelaxSolve(C& c, const BottomArgs& A) {
   if (c.tid() == 0) W.status[0] = 0, W.status[1] = iter;
 }
 
+// On the grid, boxes of at most this many cells have their element-wise
+// updates and their partial sums done by one thread each, with no barrier in
+// between (in one block a barrier costs less than the serialised updates).
+constexpr int kBoxWiseCells = 64;
+
+// r += v * sv and e += w * sw on every valid slot, then the norm of r (and,
+// with rtr, the reference-ordered rt.r, folded beside it): the two sums a
+// BiCGStab half step ends with.
+template <class C>
+__device__ double bUpdateNorm(C& c, const BottomArgs& A, const double* v, double sv, const double* w, double sw,
+                              double* rtr) {
+  const BottomWork& W = A.W;
+  if (C::kGrid && A.cfg.normType == 2 && W.maxBoxCells <= kBoxWiseCells) {
+    for (int b = c.tid(); b < W.nbox; b += c.nthr()) {
+      for (int q = W.boxStart[b]; q < W.boxStart[b + 1]; ++q) {
+        A.r[q] = A.r[q] + v[q] * sv;
+        A.e[q] = A.e[q] + w[q] * sw;
+      }
+      c.part[b] = boxPartial(A, b, A.r, A.r, true);
+      if (rtr) c.part2[b] = boxPartial(A, b, A.rt, A.r, false);
+    }
+    double n2, d = 0.0;
+    c.reduce(W.nbox, rtr != nullptr, false, n2, d);
+    if (rtr) *rtr = d;
+    return sqrt(n2);
+  }
+  bCells(c, W.nv, [&](int q) {
+    A.r[q] = A.r[q] + v[q] * sv;
+    A.e[q] = A.e[q] + w[q] * sw;
+  });
+  const double n = bNormType(c, A, A.r);
+  if (rtr) *rtr = bDot(c, A, A.rt, A.r, false);
+  return n;
+}
+
+// p from r (init) or p = (p beta + v (-beta omega)) + r, then the
+// preconditioner pt = preCond(p): the two share their first pass.
+template <class C>
+__device__ void bDirection(C& c, const BottomArgs& A, bool init, double b1, double bo) {
+  const BottomWork& W = A.W;
+  bCells(c, W.nv, [&](int q) {
+    double x;
+    if (init) {
+      x = A.r[q];
+    } else {
+      x = A.p[q] * b1;
+      x = x + A.v[q] * bo;
+      x = x + A.r[q] * 1.0;
+    }
+    A.p[q] = x;
+    A.pt[q] = A.vc ? x * W.lam[q] : x * A.mult;
+  });
+  bRelax(c, A, A.pt, A.p, 2);
+}
+
 template <class C>
 __device__ void bBicgstab(C& c, const BottomArgs& A) {
   const BottomWork& W = A.W;
   const int nv = W.nv;
   auto zeroV = [&](double* x) { bCells(c, nv, [&](int q) { x[q] = 0.0; }); };
-  auto copyV = [&](double* d, const double* s) { bCells(c, nv, [&](int q) { d[q] = s[q]; }); };
   auto incrV = [&](double* y, const double* x, double sc) { bCells(c, nv, [&](int q) { y[q] = y[q] + x[q] * sc; }); };
+  // rt = r, e = 0 in one pass
+  auto restartVectors = [&]() {
+    bCells(c, nv, [&](int q) {
+      A.rt[q] = A.r[q];
+      A.e[q] = 0.0;
+    });
+  };
   bOp(c, A, A.r, A.phi, A.rhs, 0);
-  copyV(A.rt, A.r);
-  zeroV(A.e);
+  restartVectors();
   int iter = 0, recount = 0, restarts = 0, status = 0;
   double rho[4] = {0, 0, 0, 0};
   double norm[2];
@@ -1379,6 +1441,9 @@ __device__ void bBicgstab(C& c, const BottomArgs& A) {
   norm[1] = norm[0];
   double alpha[2] = {0, 0}, beta[2] = {0, 0}, omega[2] = {0, 0};
   bool init = true;
+  // rt.r of the current r when the last half step folded it beside its norm
+  bool haveRho = false;
+  double rhoNext = 0.0;
   const double metric = *A.metric;
   if (metric > 0) initial_norm = metric;
   while ((iter < A.imax && norm[0] > A.eps * norm[1]) && (norm[1] > 0)) {
@@ -1389,36 +1454,27 @@ __device__ void bBicgstab(C& c, const BottomArgs& A) {
     omega[1] = omega[0];
     rho[3] = rho[2];
     rho[2] = rho[1];
-    rho[1] = bDot(c, A, A.rt, A.r, false);
+    rho[1] = haveRho ? rhoNext : bDot(c, A, A.rt, A.r, false);
+    haveRho = false;
     if (rho[1] == 0.0) {
       incrV(A.phi, A.e, 1.0);
       if (c.tid() == 0) W.status[0] = 2, W.status[1] = iter;
       return;
     }
-    if (init) {
-      copyV(A.p, A.r);
-      init = false;
-    } else {
-      // p = beta p; p -= beta omega v; p += r (one pass, each element in that order)
+    double b1 = 0.0, bo = 0.0;
+    if (!init) {
       beta[1] = (rho[1] / rho[2]) * (alpha[1] / omega[1]);
-      const double b1 = beta[1], bo = -beta[1] * omega[1];
-      bCells(c, nv, [&](int q) {
-        double x = A.p[q] * b1;
-        x = x + A.v[q] * bo;
-        A.p[q] = x + A.r[q] * 1.0;
-      });
+      b1 = beta[1];
+      bo = -beta[1] * omega[1];
     }
-    bPrecond(c, A, A.pt, A.p);
+    bDirection(c, A, init, b1, bo);
+    init = false;
     bOp(c, A, A.v, A.pt, nullptr, 1);
     double m = bDot(c, A, A.rt, A.v, false);
     alpha[0] = rho[1] / m;
     if (fabs(m) > A.small * fabs(rho[1])) {
       const double a0 = alpha[0];
-      bCells(c, nv, [&](int q) {
-        A.r[q] = A.r[q] + A.v[q] * -a0;
-        A.e[q] = A.e[q] + A.pt[q] * a0;
-      });
-      norm[0] = bNormType(c, A, A.r);
+      norm[0] = bUpdateNorm(c, A, A.v, -a0, A.pt, a0, nullptr);
     } else {
       zeroV(A.r);
       norm[0] = 0.0;
@@ -1430,11 +1486,8 @@ __device__ void bBicgstab(C& c, const BottomArgs& A) {
       bDot2(c, A, A.t, A.r, A.t, A.t, tr, tt);
       omega[0] = tr / tt;
       const double w0 = omega[0];
-      bCells(c, nv, [&](int q) {
-        A.e[q] = A.e[q] + A.st[q] * w0;
-        A.r[q] = A.r[q] + A.t[q] * -w0;
-      });
-      norm[0] = bNormType(c, A, A.r);
+      norm[0] = bUpdateNorm(c, A, A.t, -w0, A.st, w0, &rhoNext);
+      haveRho = true;
     }
     if (norm[0] <= A.eps * initial_norm || norm[0] <= A.reps * initial_residual) {
       status = 1;
@@ -1458,8 +1511,8 @@ __device__ void bBicgstab(C& c, const BottomArgs& A) {
         alpha[0] = 0;
         beta[0] = 0;
         omega[0] = 0;
-        copyV(A.rt, A.r);
-        zeroV(A.e);
+        restartVectors();
+        haveRho = false;
         restarts++;
         init = true;
       }

@@ -417,6 +417,7 @@ void Solver::setup(const std::vector<BottomPlan>& bps) {
     w.nv = bp.nv;
     w.ng = bp.ng;
     w.nbox = (int)bp.boxStart.size() - 1;
+    for (int b = 0; b < w.nbox; ++b) w.maxBoxCells = std::max(w.maxBoxCells, bp.boxStart[b + 1] - bp.boxStart[b]);
     maxBottomBoxes_ = std::max(maxBottomBoxes_, w.nbox);
     w.fab = upload(bufs_, bp.fab, s_);
     w.nb = upload(bufs_, bp.nb, s_);

@@ -91,6 +91,10 @@ void buildBottom(const LevelPlan& L, BottomPlan& B);
 void buildFaceRules(LevelPlan& L);
 // buildFaceRules unless the level has them; true when it built them.
 bool ensureFaceRules(LevelPlan& L);
+// The per-chunk face-ghost lists of the prefill relaxation variant
+// (LevelPlan::chunkGhost, and the face rules they are made from) on levels of
+// at most kPrefillMaxCells cells that lack them; true when it built them.
+bool ensureChunkGhosts(LevelPlan& L);
 // The colour-1 cells on exchange faces (LevelPlan::deferred), for the fused
 // sweep; built on demand, after the face rules.
 void buildDeferred(LevelPlan& L);

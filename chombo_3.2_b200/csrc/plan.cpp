@@ -459,13 +459,18 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     chunkCounts(L.chunksColor[0], (int)b, rows * half);
     chunkCounts(L.chunksColor[1], (int)b, rows * half);
   }
-  // The prefill variant's per-chunk lists only where that variant can win
-  // (latency-bound levels): on larger levels the separate fill is as fast,
-  // and the lists would add as much host work and memory as the fill lists.
-  if (grids.numCells() <= kPrefillMaxCells) {
-    ensureFaceRules(L);  // the per-chunk lists are made from the face rules
-    buildChunkGhosts(L);
-  }
+  // The prefill variant's per-chunk lists are built when the relaxation
+  // tuner asks for them (ensureChunkGhosts).
+}
+
+bool ensureChunkGhosts(LevelPlan& L) {
+  // Only where that variant can win (latency-bound levels): on larger levels
+  // the separate fill is as fast, and the lists would add as much host work
+  // and memory as the fill lists.
+  if (!L.chunkGhostStart[0].empty() || L.grids.size() == 0 || L.grids.numCells() > kPrefillMaxCells) return false;
+  ensureFaceRules(L);  // the per-chunk lists are made from the face rules
+  buildChunkGhosts(L);
+  return true;
 }
 
 int ownerOf(const LevelPlan& L, const IV& p) {
@@ -639,13 +644,16 @@ void buildQuadCFBox(const LevelPlan& F, const LevelPlan& C, const OwnerIndex& ow
   std::vector<int> hits;
   const double dxf = F.dx;
   const double dxc = 2 * dxf;
-  auto pushPool = [&](const std::vector<IV>& cells, const std::vector<double>* w) {
+  auto pushCells = [&](const IV* cells, size_t n, const double* w) {
     int start = (int)out.off.size();
-    for (size_t i = 0; i < cells.size(); ++i) {
+    for (size_t i = 0; i < n; ++i) {
       out.off.push_back(owner.cell(cells[i]));
-      out.w.push_back(w ? (*w)[i] : 0.0);
+      out.w.push_back(w ? w[i] : 0.0);
     }
     return start;
+  };
+  auto pushPool = [&](const std::vector<IV>& cells, const std::vector<double>* w) {
+    return pushCells(cells.data(), cells.size(), w ? w->data() : nullptr);
   };
   const Box& fbox = F.grids[fb];
   for (int d = 0; d < 3; ++d) {
@@ -703,12 +711,14 @@ void buildQuadCFBox(const LevelPlan& F, const LevelPlan& C, const OwnerIndex& ow
         if (standard.contains(c)) {
           for (int k = 0; k < 2; ++k) {
             IV ek = IV::basis(t[k]);
-            e.d1[k] = CFDeriv{1, 2, pushPool({c - ek, c + ek}, nullptr)};
-            e.d2[k] = CFDeriv{1, 3, pushPool({c - ek, c + ek, c}, nullptr)};
+            const IV d1[2] = {c - ek, c + ek}, d2[3] = {c - ek, c + ek, c};
+            e.d1[k] = CFDeriv{1, 2, pushCells(d1, 2, nullptr)};
+            e.d2[k] = CFDeriv{1, 3, pushCells(d2, 3, nullptr)};
           }
           // computeMixedDerivative: basex = e(t[0]), basey = e(t[1]).
           IV bx = IV::basis(t[0]), by = IV::basis(t[1]);
-          e.mx = CFDeriv{1, 4, pushPool({c + bx + by, c - bx + by, c + bx - by, c - bx - by}, nullptr)};
+          const IV mx[4] = {c + bx + by, c - bx + by, c + bx - by, c - bx - by};
+          e.mx = CFDeriv{1, 4, pushCells(mx, 4, nullptr)};
         } else {
           const CoarseStencils& cs = irr[i];
           for (int k = 0; k < 2; ++k) {

@@ -170,6 +170,7 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
         box0 += (int)b.boxes[k][fl].size();
       }
       S->setUseGraphs(q0.graphs);
+      S->setRelaxMode(1);  // one solve per hierarchy: no autotuning (see below)
       const Clock::time_point tsolve = Clock::now();
       std::vector<double> eps;
       std::vector<std::function<int(int)>> ints;
@@ -378,6 +379,11 @@ double serve(const std::vector<Request>& reqs, const ServeOptions& opt, std::vec
           }
           r.fillSeconds = std::chrono::duration<double>(Clock::now() - tf).count();
           S->setUseGraphs(q.graphs);
+          // A served hierarchy is solved once: the relaxation autotuner's
+          // timing sweeps (and the per-chunk lists it would build) cost more
+          // than the variants it can pick save, so every level keeps the
+          // ghost-fill variant.
+          S->setRelaxMode(1);
           const Clock::time_point tsolve = Clock::now();
           r.setupSeconds = std::chrono::duration<double>(tsolve - ts).count();
           r.started = since(tsolve);

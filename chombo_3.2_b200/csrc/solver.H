@@ -198,6 +198,9 @@ class Solver {
   void setRelaxMode(int mode);
   // Builds and uploads the fused sweep's deferred-cell lists (once).
   void ensureDeferred();
+  // Builds and uploads the prefill variant's per-chunk ghost lists (once, on
+  // the levels small enough for them).
+  void ensureChunkGhosts();
   // The bottom solver of the multigrid levels below level 0 (BottomConfig).
   // Host seconds of the constructor: plan building, then device set-up
   // (allocation, uploads, coefficient fills); 0 for a forest.

@@ -901,6 +901,7 @@ void Solver::tuneRelaxation() {
   tuneMs_.clear();
   const char forced = relaxMode_ == 2 ? 1 : relaxMode_ == 3 ? 3 : 0;
   if (forced == 3) ensureDeferred();
+  if (relaxMode_ == 0 || relaxMode_ == 2) ensureChunkGhosts();
   // The variants the tuner compares on a level: the prefill one where the
   // level has its per-chunk lists, the one-block one on small levels; the
   // fused sweep (slower on every level measured) only when forced.
@@ -1094,6 +1095,24 @@ void Solver::setBottomGrid(int mode) {
   graphs_.clear();
   for (auto& kv : precondGraphs_) cudaGraphExecDestroy(kv.second);
   precondGraphs_.clear();
+}
+
+void Solver::ensureChunkGhosts() {
+  auto one = [&](LevelPlan& p, LevelDev& d) {
+    const bool hadRules = !p.faceOff.empty();
+    if (!cmg::ensureChunkGhosts(p)) return;
+    if (!hadRules) {
+      d.faceRules = upload(bufs_, p.faceRules, s_);
+      d.faceOff = upload(bufs_, p.faceOff, s_);
+    }
+    for (int c = 0; c < 2; ++c) {
+      d.chGhost[c] = upload(bufs_, p.chunkGhost[c], s_);
+      d.chGhostStart[c] = upload(bufs_, p.chunkGhostStart[c], s_);
+    }
+  };
+  for (size_t l = 0; l < amr_.size(); ++l) one(amr_[l], amrDev_[l]);
+  for (size_t d = 0; d < mg_.size(); ++d) one(mg_[d], mgDev_[d]);
+  ck(cudaStreamSynchronize(s_), "chunk ghost lists");
 }
 
 void Solver::ensureDeferred() {

@@ -624,41 +624,110 @@ def extra_workloads(args, cmg):
     return out
 
 
-def published_vcycle(cmg):
+def published_vcycle(cmg, n0=512, steps=1, warmup=1, relax_mode=0, graphs=True):
     """The configuration of the reference's one published AMRPoisson timing: a single level 512^3 on the unit
     domain, periodic in every direction, domainSplit into 32^3 boxes (block factor 8), alpha = 1, beta = -0.1,
     4 smoothings per relaxation (releasedExamples/Proto/Poisson/doc/proto_poisson.tex:18-55 and
-    exec/periodic.inputs), 1.223 s per V-cycle on a 32-core Haswell node.  Seeded synthetic right-hand side; one
-    untimed solve, then one timed solve in CUDA events on the solver's stream, divided by its V-cycle count (each
-    V-cycle is followed by the residual and its max norm, as in the example's loop)."""
+    exec/periodic.inputs), 1.223 s per V-cycle on a 32-core Haswell node (n0 other than 512: the same recipe at
+    that size).  Seeded synthetic right-hand side; warmup untimed solves, then `steps` timed solves in CUDA events
+    on the solver's stream, divided by their V-cycle count (each V-cycle is followed by the residual and its max
+    norm, as in the example's loop)."""
     import torch
-    n0 = 512
     boxes = cmg.domain_split((0, 0, 0), (n0 - 1,) * 3, 32, 8)
     h = cmg.Hierarchy(n0, [boxes], op=0, alpha=1.0, beta=-0.1, bc="PPPPPP")
     try:
         h.fill_synthetic(20261203)
         p = cmg.solve_params(pre=4, post=4, bottom=4, iter_max=100, eps=1e-10, hang=1e-10)
-        h.use_graphs(True)
-        h.solve(p)
+        h.set_relax_mode(relax_mode)
+        h.use_graphs(graphs)
+        for _ in range(max(warmup, 1)):
+            h.solve(p)
         stream = torch.cuda.ExternalStream(h.stream())
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         a.record(stream)
-        o = h.solve(p)
+        for _ in range(steps):
+            o = h.solve(p)
         b.record(stream)
         b.synchronize()
-        ms = a.elapsed_time(b)
+        ms = a.elapsed_time(b) / steps
         nv = max(o["iterations"], 1)
         vb = h.vcycle_bytes(p)
         peak = measured_peaks()[0]
-        return {"workload": "single level 512^3 periodic Helmholtz (alpha 1, beta -0.1), 4096 boxes of 32^3, "
-                            "4 smoothings", "ms_per_vcycle": ms / nv, "vcycles": o["iterations"],
+        return {"workload": f"single level {n0}^3 periodic Helmholtz (alpha 1, beta -0.1), {len(boxes)} boxes of "
+                            "32^3, 4 smoothings", "ms_per_vcycle": ms / nv, "vcycles": o["iterations"],
                 "exit_status": o["exit_status"], "ms_per_solve": ms, "cells": h.num_cells(0),
                 "vcycle_gbs": vb / (ms / nv) / 1e6, "vcycle_frac": vb / (ms / nv) / 1e6 / peak,
-                "published_s_per_vcycle": 1.223, "published_hardware": "1 Cori Haswell node, 32 MPI ranks",
-                "dtype": "f64", "timing": "CUDA events on the solver's stream around one solve after an untimed one"}
+                "published_s_per_vcycle": 1.223 if n0 == 512 else None,
+                "published_hardware": "1 Cori Haswell node, 32 MPI ranks", "dtype": "f64",
+                "timing": f"CUDA events on the solver's stream around {steps} solve(s) after {max(warmup, 1)} "
+                          "untimed"}
     finally:
         h.close()
+
+
+def periodic_reference(cmg, n0, n_iter, threads):
+    """The reference on the periodic configuration: the oracle built with the reference's OpenMP box loops (valid
+    on one level), OMP_NUM_THREADS = threads, capped at 2 V-cycles; returns seconds per (steady) V-cycle, the
+    set-up, and the full solve extrapolated to n_iter V-cycles."""
+    if not os.path.exists(OMPORACLE):
+        return None
+    boxes = cmg.domain_split((0, 0, 0), (n0 - 1,) * 3, 32, 8)
+    meta = {"n0": n0, "boxes": [[list(b) for b in boxes]], "maxbox": 32, "block": 8, "op": 0, "alpha": 1.0,
+            "beta": -0.1, "seed": 20261203, "pre": 4, "post": 4, "bottom": 4, "eps": 1e-10, "hang": 1e-10}
+    boxfile = write_boxfile(meta)
+    a = oracle_args(meta, boxfile, 2, 1) + ["bc=PPPPPP"]
+    a[0] = OMPORACLE
+    out = subprocess.run(a, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+                         env=dict(os.environ, OMP_NUM_THREADS=str(threads))).stdout
+    reps = parse_repeats(out)
+    if not reps:
+        return None
+    its = reps[0]["iterations"]
+    return {"s_per_vcycle": its[-1], "setup_s": reps[0]["setup"], "solve_s": extrapolate(reps[0], n_iter),
+            "cores": threads}
+
+
+def run_periodic(args):
+    """--workload periodic: the published configuration (published_vcycle) as its own line."""
+    cmg = load_cmg()
+    r = published_vcycle(cmg, n0=args.n0, steps=args.steps, warmup=args.warmup, relax_mode=args.relax_mode,
+                         graphs=not args.no_graphs)
+    line = {"metric": METRIC, "value": 1000.0 / r["ms_per_solve"], "unit": "solves/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_solve"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": r["workload"]}, "gpu_launches": cmg.launch_count()}
+    line.update({k: r[k] for k in ("ms_per_vcycle", "vcycles", "exit_status", "cells", "vcycle_gbs", "vcycle_frac",
+                                   "published_s_per_vcycle", "published_hardware", "timing")})
+    if not args.no_cpu_baseline:
+        ref = periodic_reference(cmg, args.n0, r["vcycles"], os.cpu_count() or 1)
+        if ref:
+            line["cpu_baseline"] = {"value": 1.0 / ref["solve_s"], "unit": "solves/s", "cores": ref["cores"],
+                                    "kind": "reference", "s_per_vcycle": ref["s_per_vcycle"],
+                                    "sample": f"one reference solve with OMP_NUM_THREADS={ref['cores']} (single "
+                                              "level: the reference's OpenMP box loops are valid), capped at 2 "
+                                              f"V-cycles, extrapolated to the solve's {r['vcycles']}"}
+    print(json.dumps(line))
+
+
+def run_periodic_reference(args):
+    """--impl reference of --workload periodic: periodic_reference on all host cores, as its own line."""
+    cmg = load_cmg()
+    n_iter = 6  # V-cycles of this solve to 1e-10 (the GPU solve reproduces the reference's history bit for bit)
+    ref = periodic_reference(cmg, args.n0, n_iter, os.cpu_count() or 1)
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/omp/cmg_oracle is not built"}))
+        return
+    v = 1.0 / ref["solve_s"]
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": 1,
+                      "steps": 1, "warmup": 0, "ms_per_step": 1000.0 * ref["solve_s"], "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": f"single level {args.n0}^3 periodic Helmholtz (alpha 1, beta -0.1), "
+                                             "boxes of 32^3, 4 smoothings"},
+                      "s_per_vcycle": ref["s_per_vcycle"], "setup_s": ref["setup_s"],
+                      "cpu_baseline": {"value": v, "unit": "solves/s", "cores": ref["cores"], "kind": "reference",
+                                       "sample": "one solve capped at 2 V-cycles, extrapolated to 6"},
+                      "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
 def fineinterp_reference(meta, repeat):
@@ -864,7 +933,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS) + ["config3", "config4", "fineinterp"])
+    ap.add_argument("--workload", default="config1",
+                    choices=sorted(WORKLOADS) + ["config3", "config4", "fineinterp", "periodic"])
+    ap.add_argument("--n0", type=int, default=512, help="periodic: base size (512: the published configuration)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="launch every kernel instead of replaying graphs")
     ap.add_argument("--relax-mode", type=int, default=0, choices=[0, 1, 2, 3],
@@ -885,6 +956,8 @@ def main():
     args = ap.parse_args()
     if args.workload == "fineinterp":
         return run_fineinterp(args)
+    if args.workload == "periodic":
+        return run_periodic_reference(args) if args.impl == "reference" else run_periodic(args)
     if args.workload in ("config3", "config4"):
         if args.impl == "reference":
             return run_reference_batch(args)

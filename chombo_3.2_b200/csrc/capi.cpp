@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/cmg.h"
+#include "hostpool.H"
 #include "fineinterp.H"
 #include "meshrefine.H"
 #include "noalloc.H"
@@ -103,13 +104,7 @@ void putMotion(int* o, int from, int to, const cmg::Box& fr, const cmg::Box& tr)
 
 template <class F>
 void parallelBoxes(size_t nbox, F fn) {
-  unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> th;
-  for (unsigned t = 0; t < nt; ++t)
-    th.emplace_back([&, t]() {
-      for (size_t b = t; b < nbox; b += nt) fn(b);
-    });
-  for (auto& x : th) x.join();
+  hostParallel(nbox, [&](size_t b) { fn(b); });
 }
 
 }  // namespace

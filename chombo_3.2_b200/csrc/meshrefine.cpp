@@ -5,6 +5,8 @@
 // result).
 #include "meshrefine.H"
 
+#include "hostpool.H"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -118,13 +120,7 @@ Box minBoxOf(const IV* begin, const IV* end) {
 
 template <class F>
 void parallelFor(size_t n, F fn) {
-  unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> th;
-  for (unsigned t = 0; t < nt; ++t)
-    th.emplace_back([&, t]() {
-      for (size_t i = t; i < n; i += nt) fn(i);
-    });
-  for (auto& x : th) x.join();
+  hostParallel(n, [&](size_t i) { fn(i); });
 }
 
 // Coarse cells of cdom that contain a member of s.  Planes of coarse cells

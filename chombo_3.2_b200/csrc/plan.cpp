@@ -2,6 +2,8 @@
 // reproduces; the kernels then apply these tables without any geometry logic.
 #include "plan.H"
 
+#include "hostpool.H"
+
 #include <atomic>
 #include <exception>
 #include <thread>
@@ -79,29 +81,11 @@ static int64_t faceSlot(const LevelPlan& L, size_t b, const IV& g, int& dir, int
          (int64_t)bx.size(t0) * (g[t1] - bx.lo[t1]);
 }
 
-// Runs fn(i) for every i in [0, n) on up to 16 host threads; the items must
+// Runs fn(i) for every i in [0, n) on the host thread pool; the items must
 // write disjoint data.
 template <class F>
 void parallelItems(size_t n, F fn) {
-  const size_t nt = std::min<size_t>(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
-  if (nt <= 1) {
-    for (size_t i = 0; i < n; ++i) fn(i);
-    return;
-  }
-  std::atomic<size_t> next{0};
-  std::vector<std::exception_ptr> err(nt);
-  std::vector<std::thread> th;
-  for (size_t t = 0; t < nt; ++t)
-    th.emplace_back([&, t]() {
-      try {
-        for (size_t i = next++; i < n; i = next++) fn(i);
-      } catch (...) {
-        err[t] = std::current_exception();
-      }
-    });
-  for (auto& x : th) x.join();
-  for (auto& e : err)
-    if (e) std::rethrow_exception(e);
+  hostParallel(n, [&](size_t i) { fn(i); });
 }
 
 void buildDeferred(LevelPlan& L);
@@ -786,23 +770,7 @@ void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
   cfineIndex.build(cfine.boxes);
   const size_t nb = F.grids.size();
   std::vector<QuadCFPart> parts(nb);
-  std::vector<std::exception_ptr> err(nb);
-  const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> th;
-  std::atomic<size_t> next{0};
-  for (unsigned t = 0; t < nt; ++t)
-    th.emplace_back([&]() {
-      for (size_t fb = next++; fb < nb; fb = next++) {
-        try {
-          buildQuadCFBox(F, C, owner, cfine, cfineIndex, fb, parts[fb]);
-        } catch (...) {
-          err[fb] = std::current_exception();
-        }
-      }
-    });
-  for (auto& x : th) x.join();
-  for (auto& e : err)
-    if (e) std::rethrow_exception(e);
+  parallelItems(nb, [&](size_t fb) { buildQuadCFBox(F, C, owner, cfine, cfineIndex, fb, parts[fb]); });
   size_t nc = 0, nf = 0, np = 0;
   for (const QuadCFPart& p : parts) {
     nc += p.coarse.size();

@@ -4,6 +4,7 @@
 #include <thread>
 #include <vector>
 
+#include "hostpool.H"
 #include "synthetic.H"
 
 namespace cmg {
@@ -12,13 +13,7 @@ namespace {
 
 template <class F>
 void parallelBoxes(size_t nbox, F fn) {
-  unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> th;
-  for (unsigned t = 0; t < nt; ++t)
-    th.emplace_back([&, t]() {
-      for (size_t b = t; b < nbox; b += nt) fn(b);
-    });
-  for (auto& x : th) x.join();
+  hostParallel(nbox, [&](size_t b) { fn(b); });
 }
 
 }  // namespace

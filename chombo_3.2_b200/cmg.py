@@ -232,11 +232,16 @@ class FineInterp:
         self.nfine = sum((b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1) for b in fine_boxes)
         self.ncoarse = sum((b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1) for b in coarse_boxes)
 
-    def interp_to_fine(self, coarse, pwc=False):
+    def interp_to_fine(self, coarse, pwc=False, out=None):
+        """Host arrays in and out; out (float64, nfine cells, contiguous) is filled and returned when given,
+        else a new array."""
         a = np.ascontiguousarray(coarse, dtype=np.float64)
         if a.size != self.ncoarse:
             raise ValueError(f"coarse data has {a.size} cells, the coarse layout {self.ncoarse}")
-        out = np.empty(self.nfine, dtype=np.float64)
+        if out is None:
+            out = np.empty(self.nfine, dtype=np.float64)
+        elif out.dtype != np.float64 or out.size != self.nfine or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a contiguous float64 array of {self.nfine} cells")
         _check(lib().cmg_fine_interp_run(self.h, _ptr(a), _ptr(out), 0, int(pwc)))
         return out
 

@@ -403,8 +403,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     const BoxDesc& db = L.boxes[t.dst];
     for (int k = t.lo[2]; k <= t.hi[2]; ++k)
       for (int j = t.lo[1]; j <= t.hi[1]; ++j)
-        for (int i = t.lo[0]; i <= t.hi[0]; ++i) {
-          if (((i + j + k) & 1) != par) continue;
+        for (int i = t.lo[0] + ((t.lo[0] + j + k + par) & 1); i <= t.hi[0]; i += 2) {  // cells of parity par
           GhostCell g;
           g.dst = (int)cellIndex(db, i, j, k);
           if (t.kind == G_COPY) {

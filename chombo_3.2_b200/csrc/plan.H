@@ -5,6 +5,8 @@
 #ifndef CMG_PLAN_H
 #define CMG_PLAN_H
 
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "devtypes.H"
@@ -13,6 +15,31 @@
 namespace cmg {
 
 enum { CHUNK = 256 };
+
+// Allocator whose resize leaves new elements uninitialised: the largest
+// plan tables (coarse-fine stencils, flux registers) are resized once and
+// filled by their builders on host threads, so each page is first touched by
+// the thread that writes it instead of by one thread zeroing them all.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U>&) {}
+  template <class U>
+  void construct(U* p) noexcept {
+    ::new ((void*)p) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new ((void*)p) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using PlanVec = std::vector<T, NoInitAlloc<T>>;
 
 struct LevelPlan {
   Layout grids;
@@ -32,7 +59,7 @@ struct LevelPlan {
   std::vector<int> slotStart, slotBlock;
   // The ghost fill cell by cell: [colour 0 exchange+BC | colour 0 CF |
   // colour 1 exchange+BC | colour 1 CF], each group in task order.
-  std::vector<GhostCell> gcells;
+  PlanVec<GhostCell> gcells;
   int gcStart[2] = {0, 0}, gcExch[2] = {0, 0}, gcCF[2] = {0, 0};
   // Face-ghost rules for relaxation without ghost fills: per box, six faces
   // (direction-major, low side first), each over its two tangential
@@ -52,18 +79,18 @@ struct LevelPlan {
   std::vector<int> zeroBlock;
   std::vector<Chunk> chunksAll, chunksColor[2];
   // Coarse-fine interpolation from the next coarser level (levels >= 1).
-  std::vector<CFCoarse> cfCoarse;
-  std::vector<CFFine> cfFine;
-  std::vector<double> cfW;
-  std::vector<int64_t> cfOff;
+  PlanVec<CFCoarse> cfCoarse;
+  PlanVec<CFFine> cfFine;
+  PlanVec<double> cfW;
+  PlanVec<int64_t> cfOff;
   // Maps to the next coarser level (levels >= 1): items in coarse index space.
   std::vector<CoarseFineItem> toCoarse;
   std::vector<Chunk> toCoarseChunksF;  // chunks over fine cells of items
   std::vector<Chunk> toCoarseChunksC;  // chunks over coarse cells of items
   // Flux-register correction of this level from the next finer level.
-  std::vector<RefluxCell> rfCells;
-  std::vector<RefluxCoarseTerm> rfCoarse;
-  std::vector<RefluxFineGroup> rfFine;
+  PlanVec<RefluxCell> rfCells;
+  PlanVec<RefluxCoarseTerm> rfCoarse;
+  PlanVec<RefluxFineGroup> rfFine;
   // Forest levels (mergeLevels): hierarchy of each box, first element of each
   // hierarchy (one more entry: nelem).  Empty for one hierarchy.
   std::vector<int> boxHier;

@@ -336,7 +336,9 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
   // AMRElliptic/AMRPoissonOp.cpp:1598-1671).  A packed face is one box; an
   // unpacked face is emitted cell by cell with the same formula.
   if (dxCrse > 0) {
-    for (size_t b = 0; b < grids.size(); ++b)
+    // each box's faces on a host thread, appended in box order
+    std::vector<std::vector<GhostTask>> perBox(grids.size());
+    parallelItems(grids.size(), [&](size_t b) {
       for (int d = 0; d < 3; ++d)
         for (int side = -1; side <= 1; side += 2) {
           CellSet s;
@@ -354,9 +356,11 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
               t.lo[k] = r.lo[k];
               t.hi[k] = r.hi[k];
             }
-            L.ghost.push_back(t);
+            perBox[b].push_back(t);
           }
         }
+    });
+    for (const auto& v : perBox) L.ghost.insert(L.ghost.end(), v.begin(), v.end());
   }
 
   L.ghostStart.assign(1, 0);
@@ -397,7 +401,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
       L.gcCF[par] = (int)(pos - L.gcStart[par] - L.gcExch[par]);
     }
     start[2 * ntask] = pos;
-    L.gcells.assign((size_t)pos, GhostCell{0, 0, 0});
+    L.gcells.resize((size_t)pos);  // every entry is written below
   }
   auto emit = [&](const GhostTask& t, int par, int64_t at) {
     const BoxDesc& db = L.boxes[t.dst];
@@ -770,34 +774,39 @@ void buildQuadCF(LevelPlan& F, const LevelPlan& C) {
   const size_t nb = F.grids.size();
   std::vector<QuadCFPart> parts(nb);
   parallelItems(nb, [&](size_t fb) { buildQuadCFBox(F, C, owner, cfine, cfineIndex, fb, parts[fb]); });
-  size_t nc = 0, nf = 0, np = 0;
-  for (const QuadCFPart& p : parts) {
-    nc += p.coarse.size();
-    nf += p.fine.size();
-    np += p.off.size();
-  }
-  F.cfCoarse.reserve(nc);
-  F.cfFine.reserve(nf);
-  F.cfW.reserve(np);
-  F.cfOff.reserve(np);
+  // Concatenation: every part's ranges from prefix sums, then the parts
+  // copied (and their indices shifted) on host threads.
+  std::vector<size_t> c0(nb + 1, 0), f0(nb + 1, 0), p0(nb + 1, 0);
   for (size_t fb = 0; fb < nb; ++fb) {
+    c0[fb + 1] = c0[fb] + parts[fb].coarse.size();
+    f0[fb + 1] = f0[fb] + parts[fb].fine.size();
+    p0[fb + 1] = p0[fb] + parts[fb].off.size();
+  }
+  F.cfCoarse.resize(c0[nb]);
+  F.cfFine.resize(f0[nb]);
+  F.cfW.resize(p0[nb]);
+  F.cfOff.resize(p0[nb]);
+  parallelItems(nb, [&](size_t fb) {
     QuadCFPart& p = parts[fb];
-    const int coarseBase = (int)F.cfCoarse.size(), poolBase = (int)F.cfOff.size();
-    for (CFCoarse e : p.coarse) {
+    const int coarseBase = (int)c0[fb], poolBase = (int)p0[fb];
+    for (size_t i = 0; i < p.coarse.size(); ++i) {
+      CFCoarse e = p.coarse[i];
       for (int k = 0; k < 2; ++k) {
         if (e.d1[k].kind) e.d1[k].start += poolBase;
         if (e.d2[k].kind) e.d2[k].start += poolBase;
       }
       if (e.mx.kind) e.mx.start += poolBase;
-      F.cfCoarse.push_back(e);
+      F.cfCoarse[c0[fb] + i] = e;
     }
-    for (CFFine f : p.fine) {
+    for (size_t i = 0; i < p.fine.size(); ++i) {
+      CFFine f = p.fine[i];
       f.coarse += coarseBase;
-      F.cfFine.push_back(f);
+      F.cfFine[f0[fb] + i] = f;
     }
-    F.cfW.insert(F.cfW.end(), p.w.begin(), p.w.end());
-    F.cfOff.insert(F.cfOff.end(), p.off.begin(), p.off.end());
-  }
+    std::copy(p.w.begin(), p.w.end(), F.cfW.begin() + p0[fb]);
+    std::copy(p.off.begin(), p.off.end(), F.cfOff.begin() + p0[fb]);
+    p = QuadCFPart();
+  });
 }
 
 }  // namespace cmg
@@ -954,16 +963,29 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
       out.cells.push_back(rc);
     }
   });
-  for (Part& p : parts) {
-    const int cbase = (int)C.rfCoarse.size(), fbase = (int)C.rfFine.size();
-    for (RefluxCell rc : p.cells) {
-      rc.start += cbase;
-      rc.fstart += fbase;
-      C.rfCells.push_back(rc);
-    }
-    C.rfCoarse.insert(C.rfCoarse.end(), p.co.begin(), p.co.end());
-    C.rfFine.insert(C.rfFine.end(), p.fi.begin(), p.fi.end());
+  // Concatenation from prefix sums, the parts copied on host threads.
+  const size_t np = parts.size();
+  std::vector<size_t> n0(np + 1, 0), t0(np + 1, 0), g0(np + 1, 0);
+  for (size_t k = 0; k < np; ++k) {
+    n0[k + 1] = n0[k] + parts[k].cells.size();
+    t0[k + 1] = t0[k] + parts[k].co.size();
+    g0[k + 1] = g0[k] + parts[k].fi.size();
   }
+  C.rfCells.resize(n0[np]);
+  C.rfCoarse.resize(t0[np]);
+  C.rfFine.resize(g0[np]);
+  parallelItems(np, [&](size_t k) {
+    Part& p = parts[k];
+    for (size_t i = 0; i < p.cells.size(); ++i) {
+      RefluxCell rc = p.cells[i];
+      rc.start += (int)t0[k];
+      rc.fstart += (int)g0[k];
+      C.rfCells[n0[k] + i] = rc;
+    }
+    std::copy(p.co.begin(), p.co.end(), C.rfCoarse.begin() + t0[k]);
+    std::copy(p.fi.begin(), p.fi.end(), C.rfFine.begin() + g0[k]);
+    p = Part();
+  });
 }
 
 void buildBottom(const LevelPlan& L, BottomPlan& B) {

@@ -2,6 +2,8 @@
 // behaviour each function reproduces.
 #include "geom.H"
 
+#include "hostpool.H"
+
 namespace cmg {
 
 std::vector<Motion> exchangePlan(const Layout& g) { return exchangePlan(g, Box(), nullptr); }
@@ -27,27 +29,29 @@ std::vector<Motion> exchangePlan(const Layout& g, const Box& domain, const bool*
   }
   BoxIndex index;
   index.build(g.boxes);
-  std::vector<int> hits;
   struct Image {
     int nb, shift;
     Motion m;
   };
-  std::vector<Image> images;
   auto kept = [&](size_t b, const Box& region) {
     for (int d = 0; d < 3; ++d)
       if (g[b].grow(d, 1).intersects(region)) return true;
     return false;
   };
-  for (size_t b = 0; b < n; ++b) {
+  // each box's items on a host thread, concatenated in box order
+  std::vector<std::vector<Motion>> perBox(n);
+  hostParallel(n, [&](size_t b) {
+    std::vector<int> hits;
+    std::vector<Image> images;
+    std::vector<Motion>& out = perBox[b];
     const Box bghost = g[b].grow(1);
     index.query(g.boxes, bghost, hits);
     for (int nb : hits) {
       if (nb == (int)b) continue;
       const Box region = g[nb] & bghost;
-      if (!region.empty() && kept(b, region)) plan.push_back(Motion{nb, (int)b, region, region});
+      if (!region.empty() && kept(b, region)) out.push_back(Motion{nb, (int)b, region, region});
     }
-    if (shifts.empty() || domain.contains(bghost)) continue;
-    images.clear();
+    if (shifts.empty() || domain.contains(bghost)) return;
     for (size_t k = 0; k < shifts.size(); ++k) {
       const IV& sh = shifts[k];
       const IV back(-sh[0], -sh[1], -sh[2]);
@@ -60,8 +64,12 @@ std::vector<Motion> exchangePlan(const Layout& g, const Box& domain, const bool*
     }
     std::sort(images.begin(), images.end(),
               [](const Image& a, const Image& c) { return a.nb != c.nb ? a.nb < c.nb : a.shift < c.shift; });
-    for (const Image& im : images) plan.push_back(im.m);
-  }
+    for (const Image& im : images) out.push_back(im.m);
+  });
+  size_t total = 0;
+  for (const auto& v : perBox) total += v.size();
+  plan.reserve(total);
+  for (const auto& v : perBox) plan.insert(plan.end(), v.begin(), v.end());
   return plan;
 }
 

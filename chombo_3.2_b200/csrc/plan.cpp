@@ -387,7 +387,8 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
       }
     return n;
   };
-  std::vector<int64_t> start(2 * ntask + 1, 0);
+  std::vector<int64_t> start(2 * ntask + 1, 0), count(2 * ntask, 0);
+  parallelItems(2 * ntask, [&](size_t q) { count[q] = parityCount(L.ghost[q % ntask], (int)(q / ntask)); });
   {
     int64_t pos = 0;
     for (int par = 0; par < 2; ++par) {
@@ -395,7 +396,7 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
       for (size_t t = 0; t < ntask; ++t) {
         if (t == (size_t)L.nExchBC) L.gcExch[par] = (int)(pos - L.gcStart[par]);
         start[par * ntask + t] = pos;
-        pos += parityCount(L.ghost[t], par);
+        pos += count[par * ntask + t];
       }
       if (ntask <= (size_t)L.nExchBC) L.gcExch[par] = (int)(pos - L.gcStart[par]);
       L.gcCF[par] = (int)(pos - L.gcStart[par] - L.gcExch[par]);

@@ -858,8 +858,8 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
   C.rfCoarse.clear();
   C.rfFine.clear();
   Layout cfine = F.grids.coarsen(2);
-  CellSet covered(C.domain, false);
-  for (const Box& b : cfine.boxes) covered.set(b, true);
+  BoxIndex cfineIndex;
+  cfineIndex.build(cfine.boxes);
   // Coarse boxes are independent: each builds its cells with pool starts
   // relative to its own pools on a host thread; the parts are concatenated
   // in box order (the same tables as one pass over the boxes).
@@ -872,12 +872,14 @@ void buildReflux(LevelPlan& C, const LevelPlan& F, bool vc) {
   parallelItems(C.grids.size(), [&](size_t cb) {
     Part& out = parts[cb];
     const Box& cbox = C.grids[cb];
-    // coarsened fine boxes next to this coarse box, in fine box order
-    std::vector<size_t> near;
-    const Box grown = cbox.grow(1);
-    for (size_t f = 0; f < cfine.size(); ++f)
-      if (cfine[f].intersects(grown)) near.push_back(f);
-    if (near.empty()) return;
+    // coarsened fine boxes next to this coarse box, in fine box order, and
+    // the cells of this box they cover
+    std::vector<int> hits;
+    cfineIndex.query(cfine.boxes, cbox.grow(1), hits);
+    if (hits.empty()) return;
+    const std::vector<size_t> near(hits.begin(), hits.end());
+    CellSet covered(cbox, false);
+    for (size_t f : near) covered.set(cfine[f], true);
     // Per coarse cell of this box (first-touch order): its coarse terms and
     // fine groups.
     std::vector<int> slotOf((size_t)cbox.numPts(), -1);

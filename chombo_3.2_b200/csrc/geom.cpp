@@ -74,13 +74,21 @@ std::vector<Motion> exchangePlan(const Layout& g, const Box& domain, const bool*
 }
 
 std::vector<Motion> copyPlan(const Layout& src, const Layout& dst) {
+  // per destination box, the source boxes meeting it in index order (through
+  // a spatial index, on host threads), concatenated in destination order
+  BoxIndex index;
+  index.build(src.boxes);
+  std::vector<std::vector<Motion>> perBox(dst.size());
+  hostParallel(dst.size(), [&](size_t d) {
+    std::vector<int> hits;
+    index.query(src.boxes, dst[d], hits);
+    for (int s : hits) {
+      Box r = dst[d] & src[s];
+      if (!r.empty()) perBox[d].push_back(Motion{s, (int)d, r, r});
+    }
+  });
   std::vector<Motion> plan;
-  for (size_t d = 0; d < dst.size(); ++d)
-    for (size_t s = 0; s < src.size(); ++s)
-      if (dst[d].intersects(src[s])) {
-        Box r = dst[d] & src[s];
-        plan.push_back(Motion{(int)s, (int)d, r, r});
-      }
+  for (const auto& v : perBox) plan.insert(plan.end(), v.begin(), v.end());
   return plan;
 }
 

@@ -1,0 +1,59 @@
+// Field-wise hash of every host plan table (ghost lists, face rules, per-chunk
+// ghosts, coarse-fine stencils, flux registers, copy items, chunks) of three
+// synthetic hierarchies: a regression check that the plan builders produce the
+// tables the device solve was verified with.
+#include <cstdio>
+#include <cstdint>
+#include <cstring>
+#include "geom.H"
+#include "plan.H"
+#include "meshrefine.H"
+using namespace cmg;
+struct H {
+  uint64_t h = 1469598103934665603ULL;
+  void add(const void* p, size_t n) { const unsigned char* c = (const unsigned char*)p; for (size_t i = 0; i < n; ++i) { h ^= c[i]; h *= 1099511628211ULL; } }
+  template <class T> void v(const T& x) { add(&x, sizeof(T)); }
+};
+static void hashLevel(H& h, const LevelPlan& L) {
+  for (auto& g : L.gcells) { h.v(g.dst); h.v(g.s1); h.v(g.s2); }
+  for (int p = 0; p < 2; ++p) { h.v(L.gcStart[p]); h.v(L.gcExch[p]); h.v(L.gcCF[p]); }
+  for (auto& r : L.faceRules) { h.v(r.src); h.v(r.kind); }
+  for (int x : L.faceOff) h.v(x);
+  for (int c = 0; c < 2; ++c) { for (auto& g : L.chunkGhost[c]) { h.v(g.dst); h.v(g.s1); h.v(g.s2); } for (int x : L.chunkGhostStart[c]) h.v(x); }
+  for (auto& e : L.cfCoarse) { h.v(e.cc); for (int k = 0; k < 2; ++k) { h.v(e.d1[k].kind); h.v(e.d1[k].n); h.v(e.d1[k].start); h.v(e.d2[k].kind); h.v(e.d2[k].n); h.v(e.d2[k].start); } h.v(e.mx.kind); h.v(e.mx.n); h.v(e.mx.start); }
+  for (auto& f : L.cfFine) { h.v(f.g); h.v(f.pa); h.v(f.pb); h.v(f.x1); h.v(f.x2); h.v(f.coarse); h.v(f.packed); }
+  for (double w : L.cfW) h.v(w);
+  for (int64_t o : L.cfOff) h.v(o);
+  for (auto& c : L.rfCells) { h.v(c.c); h.v(c.nco); h.v(c.nfi); h.v(c.start); h.v(c.fstart); }
+  for (auto& t : L.rfCoarse) { h.v(t.hi); h.v(t.lo); h.v(t.bface); h.v(t.dir); h.v(t.sgn); }
+  for (auto& g : L.rfFine) { for (int k = 0; k < 4; ++k) { h.v(g.hi[k]); h.v(g.lo[k]); h.v(g.bface[k]); } h.v(g.dir); h.v(g.scale); }
+  for (auto& t : L.ghost) { h.v(t.kind); h.v(t.dst); h.v(t.src); h.v(t.dir); h.v(t.side); for (int k = 0; k < 3; ++k) { h.v(t.lo[k]); h.v(t.hi[k]); h.v(t.shift[k]); } }
+  for (auto& c : L.toCoarse) { h.v(c.cbox); h.v(c.fbox); for (int k = 0; k < 3; ++k) { h.v(c.lo[k]); h.v(c.hi[k]); } }
+  for (auto& c : L.chunksColor[0]) { h.v(c.box); h.v(c.start); }
+}
+int main() {
+  struct Case { int n0, nl; } cases[] = {{32, 3}, {64, 3}, {128, 3}};
+  for (auto cs : cases) {
+    auto boxes = syntheticHierarchy(cs.n0, cs.nl, 32, 8, 0.75, 20261203, 0.1);
+    const int nl = (int)boxes.size();
+    std::vector<LevelPlan> amr(nl);
+    Box dom(IV(0, 0, 0), IV(cs.n0 - 1, cs.n0 - 1, cs.n0 - 1));
+    double dx = 1.0 / cs.n0;
+    for (int l = 0; l < nl; ++l) {
+      buildLevel(amr[l], Layout(boxes[l]), dom, dx, l ? 2 * dx : 0.0, nullptr, nullptr);
+      ensureChunkGhosts(amr[l]);
+      ensureFaceRules(amr[l]);
+      dom = dom.refine(2);
+      dx /= 2;
+    }
+    for (int l = 1; l < nl; ++l) {
+      buildQuadCF(amr[l], amr[l - 1]);
+      buildCoarseFine(amr[l], amr[l - 1]);
+      buildReflux(amr[l - 1], amr[l], true);
+    }
+    H h;
+    for (auto& L : amr) hashLevel(h, L);
+    printf("n0 %d levels %d hash %016llx\n", cs.n0, nl, (unsigned long long)h.h);
+  }
+  return 0;
+}

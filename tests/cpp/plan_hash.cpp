@@ -55,5 +55,42 @@ int main() {
     for (auto& L : amr) hashLevel(h, L);
     printf("n0 %d levels %d hash %016llx\n", cs.n0, nl, (unsigned long long)h.h);
   }
+  // one periodic level (64^3 in 64 boxes of 16^3, periodic in x and y) with
+  // its multigrid depths and the bottom plan of the deepest
+  {
+    const bool per[3] = {true, true, false};
+    const int bc[6] = {0, 0, 0, 0, 1, 0};
+    Box dom(IV(0, 0, 0), IV(63, 63, 63));
+    Layout g0(domainSplit(dom, 16, 8));
+    H h;
+    LevelPlan L0;
+    buildLevel(L0, g0, dom, 1.0 / 64, 0.0, bc, per);
+    ensureChunkGhosts(L0);
+    ensureFaceRules(L0);
+    hashLevel(h, L0);
+    LevelPlan last;
+    int depths = 0;
+    for (int c = 2; g0.coarsenable(c * 2); c *= 2, ++depths) {
+      LevelPlan M;
+      buildLevel(M, g0.coarsen(c), dom.coarsen(c), c / 64.0, 0.0, bc, per);
+      ensureChunkGhosts(M);
+      ensureFaceRules(M);
+      hashLevel(h, M);
+      last = M;
+    }
+    BottomPlan B;
+    buildBottom(depths ? last : L0, B);
+    h.v(B.nv);
+    h.v(B.ng);
+    for (int x : B.fab) h.v(x);
+    for (int x : B.nb) h.v(x);
+    for (int c = 0; c < 2; ++c)
+      for (int x : B.color[c]) h.v(x);
+    for (int x : B.boxStart) h.v(x);
+    for (int x : B.gsrc) h.v(x);
+    for (int x : B.gkind) h.v(x);
+    for (int x : B.nbv) h.v(x);
+    printf("periodic64 depths %d hash %016llx\n", depths, (unsigned long long)h.h);
+  }
   return 0;
 }

@@ -1,6 +1,7 @@
 """Regression check of the host plan builders: a field-wise hash of every plan table (ghost lists, face rules,
 per-chunk ghosts, coarse-fine stencils, flux registers, coarse-fine copy items, chunks) of three synthetic
-hierarchies (32^3, 64^3 and 128^3 bases, three levels) must stay what it was when the device solve was last
+hierarchies (32^3, 64^3 and 128^3 bases, three levels) and of a periodic 64^3 level with its multigrid depths and
+bottom plan must stay what it was when the device solve was last
 verified against the reference with these tables.  Speed-ups of the builders (threads, indexes, allocation) must
 leave these hashes unchanged; a change of the tables themselves needs the GPU parity suite and a new hash."""
 import os
@@ -24,3 +25,5 @@ def test_plan_tables_unchanged(tmp_path):
     assert out.returncode == 0, out.stderr[-2000:]
     got = {int(line.split()[1]): line.split()[5] for line in out.stdout.splitlines() if line.startswith("n0 ")}
     assert got == EXPECTED, got
+    periodic = [line.split()[-1] for line in out.stdout.splitlines() if line.startswith("periodic64")]
+    assert periodic == ["d4c2228b1e0c650f"], periodic

@@ -475,7 +475,7 @@ int ownerOf(const LevelPlan& L, const IV& p) {
 // lies in at most one box.
 struct OwnerIndex {
   const LevelPlan* L;
-  int B = 1;
+  int B = 1, sh = 0;  // block edge B = 2^sh
   IV org, n;
   std::vector<int> own;
   explicit OwnerIndex(const LevelPlan& lp) : L(&lp) {
@@ -483,6 +483,7 @@ struct OwnerIndex {
     for (const Box& b : lp.grids.boxes)
       for (int d = 0; d < 3; ++d)
         while (B > 1 && ((b.lo[d] % B) != 0 || ((b.hi[d] + 1) % B) != 0)) B /= 2;
+    while ((1 << sh) < B) ++sh;
     Box dom = lp.domain;
     for (int d = 0; d < 3; ++d) {
       org[d] = floordiv(dom.lo[d], B);
@@ -499,8 +500,9 @@ struct OwnerIndex {
   size_t slot(const IV& q) const {
     return (size_t)(q[0] - org[0]) + (size_t)n[0] * ((size_t)(q[1] - org[1]) + (size_t)n[1] * (q[2] - org[2]));
   }
+  // floor(p / B) by an arithmetic shift (also for negative p)
   int find(const IV& p) const {
-    IV q(floordiv(p[0], B), floordiv(p[1], B), floordiv(p[2], B));
+    IV q(p[0] >> sh, p[1] >> sh, p[2] >> sh);
     for (int d = 0; d < 3; ++d)
       if (q[d] < org[d] || q[d] >= org[d] + n[d]) return -1;
     return own[slot(q)];

@@ -5,14 +5,13 @@
 // method it performs.
 #include "solver.H"
 #include "fineinterp.H"
+#include "hostpool.H"
 
 #include <cstdint>
 #include <algorithm>
 #include <chrono>
-#include <atomic>
 #include <mutex>
 #include <exception>
-#include <thread>
 
 #include <cmath>
 #include <cstdio>
@@ -229,48 +228,24 @@ static void hierarchyPlans(const HierarchyDesc& desc, std::vector<LevelPlan>& am
   std::vector<int> mgc;
   for (int c = 2; g0.coarsenable(c * 2); c *= 2) mgc.push_back(c);
   mg.resize(mgc.size());
-  {
-    std::vector<std::exception_ptr> err(nlev + mgc.size());
-    std::vector<std::thread> th;
-    for (int l = 0; l < nlev; ++l)
-      th.emplace_back([&, l]() {
-        try {
-          buildLevel(amr[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0, desc.bc,
-                     desc.periodic);
-        } catch (...) {
-          err[l] = std::current_exception();
-        }
-      });
-    for (size_t d = 0; d < mgc.size(); ++d)
-      th.emplace_back([&, d]() {
-        try {
-          const int c = mgc[d];
-          buildLevel(mg[d], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0, desc.bc, desc.periodic);
-        } catch (...) {
-          err[nlev + d] = std::current_exception();
-        }
-      });
-    for (auto& t : th) t.join();
-    for (auto& e : err)
-      if (e) std::rethrow_exception(e);
-  }
-  {
-    std::vector<std::exception_ptr> err(nlev);
-    std::vector<std::thread> th;
-    for (int l = 1; l < nlev; ++l)
-      th.emplace_back([&, l]() {
-        try {
-          buildQuadCF(amr[l], amr[l - 1]);
-          buildCoarseFine(amr[l], amr[l - 1]);
-          buildReflux(amr[l - 1], amr[l], desc.vc != 0);
-        } catch (...) {
-          err[l] = std::current_exception();
-        }
-      });
-    for (auto& t : th) t.join();
-    for (auto& e : err)
-      if (e) std::rethrow_exception(e);
-  }
+  // Levels and multigrid depths, then the coarse-fine tables of each level
+  // pair, as items of the host pool (each item loops over its boxes on the
+  // same pool).
+  hostParallel(nlev + mgc.size(), [&](size_t i) {
+    if (i < (size_t)nlev) {
+      const int l = (int)i;
+      buildLevel(amr[l], Layout(desc.boxes[l]), doms[l], dxs[l], l > 0 ? dxs[l - 1] : 0.0, desc.bc, desc.periodic);
+    } else {
+      const int c = mgc[i - nlev];
+      buildLevel(mg[i - nlev], g0.coarsen(c), desc.domain.coarsen(c), desc.dx0 * c, 0.0, desc.bc, desc.periodic);
+    }
+  });
+  hostParallel(nlev > 1 ? nlev - 1 : 0, [&](size_t i) {
+    const int l = (int)i + 1;
+    buildQuadCF(amr[l], amr[l - 1]);
+    buildCoarseFine(amr[l], amr[l - 1]);
+    buildReflux(amr[l - 1], amr[l], desc.vc != 0);
+  });
 }
 
 Solver::Solver(const HierarchyDesc& desc, cudaStream_t stream)
@@ -304,23 +279,7 @@ Solver::Solver(const std::vector<HierarchyDesc>& descs, cudaStream_t stream)
                                   "and boundary types");
   }
   std::vector<std::vector<LevelPlan>> amrP(K), mgP(K);
-  {
-    std::vector<std::exception_ptr> err(K);
-    const size_t nt = std::max<size_t>(1, std::min<size_t>(K, 8));
-    std::vector<std::thread> th;
-    std::atomic<size_t> next{0};
-    for (size_t t = 0; t < nt; ++t)
-      th.emplace_back([&]() {
-        for (size_t k = next++; k < K; k = next++) try {
-            hierarchyPlans(descs[k], amrP[k], mgP[k]);
-          } catch (...) {
-            err[k] = std::current_exception();
-          }
-      });
-    for (auto& t : th) t.join();
-    for (auto& e : err)
-      if (e) std::rethrow_exception(e);
-  }
+  hostParallel(K, [&](size_t k) { hierarchyPlans(descs[k], amrP[k], mgP[k]); });
   const size_t nlev = amrP[0].size(), nd = mgP[0].size();
   for (size_t k = 0; k < K; ++k)
     if (mgP[k].size() != nd)

@@ -8,6 +8,7 @@
 #include "geom.H"
 #include "plan.H"
 #include "meshrefine.H"
+#include "hostpool.H"
 using namespace cmg;
 struct H {
   uint64_t h = 1469598103934665603ULL;
@@ -39,18 +40,25 @@ int main() {
     std::vector<LevelPlan> amr(nl);
     Box dom(IV(0, 0, 0), IV(cs.n0 - 1, cs.n0 - 1, cs.n0 - 1));
     double dx = 1.0 / cs.n0;
-    for (int l = 0; l < nl; ++l) {
-      buildLevel(amr[l], Layout(boxes[l]), dom, dx, l ? 2 * dx : 0.0, nullptr, nullptr);
+    std::vector<Box> doms(nl, dom);
+    std::vector<double> dxs(nl, dx);
+    for (int l = 1; l < nl; ++l) {
+      doms[l] = doms[l - 1].refine(2);
+      dxs[l] = dxs[l - 1] / 2;
+    }
+    // levels, then level pairs, as items of the host pool (the solver's
+    // order), each item looping over its boxes on the same pool
+    hostParallel(nl, [&](size_t l) {
+      buildLevel(amr[l], Layout(boxes[l]), doms[l], dxs[l], l ? dxs[l - 1] : 0.0, nullptr, nullptr);
       ensureChunkGhosts(amr[l]);
       ensureFaceRules(amr[l]);
-      dom = dom.refine(2);
-      dx /= 2;
-    }
-    for (int l = 1; l < nl; ++l) {
+    });
+    hostParallel(nl - 1, [&](size_t i) {
+      const int l = (int)i + 1;
       buildQuadCF(amr[l], amr[l - 1]);
       buildCoarseFine(amr[l], amr[l - 1]);
       buildReflux(amr[l - 1], amr[l], true);
-    }
+    });
     H h;
     for (auto& L : amr) hashLevel(h, L);
     printf("n0 %d levels %d hash %016llx\n", cs.n0, nl, (unsigned long long)h.h);

@@ -26,9 +26,14 @@ void chunkCounts(std::vector<Chunk>& out, int box, int64_t n) {
 bool faceCFSet(const LevelPlan& L, const Box& b, int d, int side, CellSet& out) {
   Box edge = b.adjCell(d, side, 1) & L.domain;
   if (edge.empty()) return false;
-  out.define(edge, true);
   std::vector<int> hits;
   L.index.query(L.grids.boxes, edge, hits);
+  // The boxes of a level are disjoint: the layer is covered (no cell set
+  // needed) when their overlaps with it add up to its size.
+  int64_t covered = 0;
+  for (int k : hits) covered += (L.grids[k] & edge).numPts();
+  if (covered == edge.numPts()) return false;
+  out.define(edge, true);
   for (int k : hits) out.subtract(L.grids[k]);
   return !out.empty();
 }

@@ -409,25 +409,40 @@ void buildLevel(LevelPlan& L, const Layout& grids, const Box& domain, double dx,
     start[2 * ntask] = pos;
     L.gcells.resize((size_t)pos);  // every entry is written below
   }
+  // Along a row the cells of one parity are two apart in x, so each of their
+  // indices (and their sources', shifted by a fixed offset) is the previous
+  // one plus 1 (cellIndex: same colour half, colour slot + 1).
   auto emit = [&](const GhostTask& t, int par, int64_t at) {
     const BoxDesc& db = L.boxes[t.dst];
+    int e[3] = {0, 0, 0};
+    if (t.kind != G_COPY) e[t.dir] = -t.side;
+    const int s2fixed = t.kind == G_NEU ? -1 : t.kind == G_BC ? -2 : t.kind == G_CFLIN ? -3 : 0;
     for (int k = t.lo[2]; k <= t.hi[2]; ++k)
-      for (int j = t.lo[1]; j <= t.hi[1]; ++j)
-        for (int i = t.lo[0] + ((t.lo[0] + j + k + par) & 1); i <= t.hi[0]; i += 2) {  // cells of parity par
-          GhostCell g;
-          g.dst = (int)cellIndex(db, i, j, k);
-          if (t.kind == G_COPY) {
-            g.s1 = (int)cellIndex(L.boxes[t.src], i - t.shift[0], j - t.shift[1], k - t.shift[2]);
-            g.s2 = -1;
+      for (int j = t.lo[1]; j <= t.hi[1]; ++j) {
+        const int i0 = t.lo[0] + ((t.lo[0] + j + k + par) & 1);  // the row's first cell of parity par
+        if (i0 > t.hi[0]) continue;
+        const int n = (t.hi[0] - i0) / 2 + 1;
+        const int d0 = (int)cellIndex(db, i0, j, k);
+        int a0, b0 = -1, bstep = 0;
+        if (t.kind == G_COPY) {
+          a0 = (int)cellIndex(L.boxes[t.src], i0 - t.shift[0], j - t.shift[1], k - t.shift[2]);
+        } else {
+          a0 = (int)cellIndex(db, i0 + e[0], j + e[1], k + e[2]);
+          if (s2fixed) {
+            b0 = s2fixed;
           } else {
-            int e[3] = {0, 0, 0};
-            e[t.dir] = -t.side;
-            g.s1 = (int)cellIndex(db, i + e[0], j + e[1], k + e[2]);
-            g.s2 = t.kind == G_NEU ? -1 : t.kind == G_BC ? -2 : t.kind == G_CFLIN ? -3
-                                   : (int)cellIndex(db, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
+            b0 = (int)cellIndex(db, i0 + 2 * e[0], j + 2 * e[1], k + 2 * e[2]);
+            bstep = 1;
           }
-          L.gcells[at++] = g;
         }
+        GhostCell* g = &L.gcells[at];
+        for (int m = 0; m < n; ++m) {
+          g[m].dst = d0 + m;
+          g[m].s1 = a0 + m;
+          g[m].s2 = b0 + bstep * m;
+        }
+        at += n;
+      }
     if (at != start[par * ntask + (&t - L.ghost.data()) + 1] && (size_t)(&t - L.ghost.data()) + 1 < ntask)
       throw std::logic_error("cmg: ghost-cell count mismatch");
   };

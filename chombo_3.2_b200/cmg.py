@@ -80,6 +80,13 @@ class RequestResult(ctypes.Structure):
                 ("estimate_bytes", ctypes.c_uint64), ("batch_size", ctypes.c_int), ("message", ctypes.c_char * 160)]
 
 
+def host_blocks(release=False):
+    """Bytes of freed host plan-table blocks kept for reuse by later plans; release=True gives them back first."""
+    kept = ctypes.c_size_t()
+    _check(lib().cmg_host_blocks(1 if release else 0, ctypes.byref(kept)))
+    return kept.value
+
+
 def serve(requests, hbm_budget=120e9, max_inflight=16, open_loop=True, batch_window=0.0, max_batch=16):
     """Runs cmg_serve over a list of dicts with Request fields; returns (results, wall seconds).  batch_window > 0:
     cmg_serve_batched, requests of one class in flight together solved as one forest."""

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/cmg.h"
+#include "hostmem.H"
 #include "hostpool.H"
 #include "fineinterp.H"
 #include "meshrefine.H"
@@ -408,6 +409,13 @@ int cmg_setup_seconds(const cmg_hierarchy* h, double* plans, double* device) {
     needLevel(h, 0);
     if (plans) *plans = h->solver->planSeconds();
     if (device) *device = h->solver->deviceSeconds();
+  });
+}
+
+int cmg_host_blocks(int release, size_t* kept) {
+  return guard([&]() {
+    if (release) cmg::hostBlockRelease();
+    if (kept) *kept = cmg::hostBlockKept();
   });
 }
 

@@ -11,6 +11,7 @@
 
 #include "devtypes.H"
 #include "geom.H"
+#include "hostmem.H"
 
 namespace cmg {
 
@@ -19,7 +20,9 @@ enum { CHUNK = 256 };
 // Allocator whose resize leaves new elements uninitialised: the largest
 // plan tables (coarse-fine stencils, flux registers) are resized once and
 // filled by their builders on host threads, so each page is first touched by
-// the thread that writes it instead of by one thread zeroing them all.
+// the thread that writes it instead of by one thread zeroing them all.  Their
+// storage comes from the kept large blocks (hostBlockAlloc), so plans built
+// after others were freed reuse mapped pages.
 template <class T>
 struct NoInitAlloc : std::allocator<T> {
   template <class U>
@@ -27,6 +30,8 @@ struct NoInitAlloc : std::allocator<T> {
     using other = NoInitAlloc<U>;
   };
   NoInitAlloc() = default;
+  T* allocate(size_t n) { return static_cast<T*>(hostBlockAlloc(n * sizeof(T))); }
+  void deallocate(T* p, size_t n) { hostBlockFree(p, n * sizeof(T)); }
   template <class U>
   NoInitAlloc(const NoInitAlloc<U>&) {}
   template <class U>

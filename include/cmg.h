@@ -14,6 +14,7 @@
 #ifndef CMG_H
 #define CMG_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -436,6 +437,12 @@ int cmg_vcycle_bytes(const cmg_hierarchy* h, const cmg_solve_params* p, double* 
  * exchange, coarse-fine, flux-register and bottom tables) and setting up the
  * device (allocation, uploads); either pointer may be null. */
 int cmg_setup_seconds(const cmg_hierarchy* h, double* plans, double* device);
+/* Host plan tables of 1 MiB or more take their storage from blocks that are
+ * kept, once freed, for later plans (up to min(8 GiB, physical memory / 8)),
+ * so a process that creates hierarchy after hierarchy reuses mapped pages.
+ * *kept (may be null) receives the bytes held; release != 0 first gives
+ * them all back to the system. */
+int cmg_host_blocks(int release, size_t* kept);
 /* The CUDA stream every call of this hierarchy runs on (cudaStream_t). */
 int cmg_get_stream(const cmg_hierarchy* h, void** stream);
 /* Streams (no counterpart in the reference, whose calls are synchronous host

@@ -17,7 +17,7 @@ def test_plan_tables_unchanged(tmp_path):
     exe = str(tmp_path / "plan_hash")
     srcs = [os.path.join(ROOT, "tests", "cpp", "plan_hash.cpp")] + [os.path.join(SRC, f) for f in
                                                                     ("plan.cpp", "geom.cpp", "meshrefine.cpp",
-                                                                     "hostpool.cpp")]
+                                                                     "hostpool.cpp", "hostmem.cpp")]
     r = subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-I", SRC, "-I", "/usr/local/cuda/include",
                         "-o", exe] + srcs + ["-lpthread"], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
